@@ -1,0 +1,400 @@
+#!/usr/bin/env python
+"""Benchmark of the Beams lighted volume renderer hot path on B200.
+
+One step = one frame of the exact path at the 512^3 noise / 1024x1024 / M = 256
+configuration: the light march that builds the 257^3
+transmittance map (K1) and the view march that shades by it (K2), with the
+field already resident in HBM. Synthetic seeded input; the 512 MiB field is
+larger than L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (the path does not shard across GPUs: there
+is no exchange step), launched by torch.distributed.run; value is the total over
+ranks divided by the slowest rank's time.
+
+The line carries:
+  value       lit samples/s over the timed frames (map build + view march),
+  ms_per_step frame time (ms/frame),
+  e2e         the same metric through the C ABI with host buffers: every step
+              uploads the field from pinned host memory and reads the image back,
+  roofline    the dominant kernel's algorithmic bytes / its CUDA-event time,
+              against the measured HBM copy bandwidth,
+  cpu_baseline the CPU oracle (the reference algorithm, OpenMP) on a bounded
+              sample of the same frame, extrapolated to a full frame.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "lit samples/s & ms/frame @1024² on 1 B200; MLP vs exact shadow at ≥45 dB PSNR"
+UNIT = "lit samples/s"
+BYTES_LIGHT_SAMPLE = 32    # 8 field corners, float32
+BYTES_MAP_VERTEX = 4       # one float32 opacity written per vertex
+BYTES_LIT_SAMPLE = 64      # 8 field corners + 8 map corners, float32
+BYTES_PIXEL = 16           # RGBA float32 written per ray
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel: str):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summaries, if any.
+    Lines look like: `traffic_bytes_per_launch[k_light_march]: 123456`."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    pat = re.compile(rf"traffic_bytes_per_launch\[{re.escape(kernel)}\]:\s*([0-9.eE+]+)")
+    for name in sorted(os.listdir(d)):
+        if not name.endswith((".md", ".txt")):
+            continue
+        with open(os.path.join(d, name)) as f:
+            m = pat.search(f.read())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while the timed region runs."""
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+               0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+    def __init__(self, device_index: int, period_s: float = 0.02):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self.period = period_s
+        self._stop = threading.Event()
+        self._h = None
+        try:
+            import pynvml as N
+            N.nvmlInit()
+            self.N = N
+            self._h = self._handle(device_index)
+            self.max_mhz = N.nvmlDeviceGetMaxClockInfo(self._h, N.NVML_CLOCK_SM)
+        except Exception as e:  # no NVML: report the absence, not a guess
+            self.error = str(e)
+
+    def _handle(self, idx):
+        import torch
+        N = self.N
+        try:
+            uuid = str(torch.cuda.get_device_properties(idx).uuid)
+            return N.nvmlDeviceGetHandleByUUID(("GPU-" + uuid) if not uuid.startswith("GPU-") else uuid)
+        except Exception:
+            return N.nvmlDeviceGetHandleByIndex(idx)
+
+    def _run(self):
+        N = self.N
+        while not self._stop.is_set():
+            try:
+                self.samples.append(N.nvmlDeviceGetClockInfo(self._h, N.NVML_CLOCK_SM))
+                r = N.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for bit, name in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self._h is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._h is not None:
+            self._t.join()
+
+    def summary(self):
+        if self._h is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "note": "NVML unavailable"}
+        busy = [s for s in self.samples if s > 0]
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons - {"gpu_idle"}), "samples": len(self.samples)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def build_scene(config: int):
+    from pilot_b200 import scenes
+    return scenes.config1() if config == 1 else scenes.config0()
+
+
+def workload_desc(s, config: int):
+    return {"workload": f"config{config}: {s.dims[0]}^3 {s.kind} f32 field, {s.width}x{s.height} image, "
+                        f"M={s.map_m} map ({s.map_m + 1}^3 vertices), view step 0.5 voxel, light step "
+                        f"|extent|/128, alpha cut {s.cutoff}, {'point' if s.light_kind == 0 else 'directional'} light",
+            "field": list(s.dims), "image": [s.width, s.height], "map_cells": s.map_m,
+            "l2": "inputs larger than L2 (512 MiB field > 126 MB L2); no flush" if config == 1 else
+                  "field 8 MiB fits L2: per-step L2 flush",
+            "form": "exact"}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline / reference arm: the oracle (the reference algorithm restated in
+# C++, float32 as the reference computes) on the host cores.
+# ---------------------------------------------------------------------------
+def cpu_sample_frame(scene, field, map_values, budget_s: float, threads: int, rng_seed: int = 0):
+    """Times the oracle on a bounded sample of one frame and extrapolates.
+
+    Light march: a random subset of map vertices. View march: every S-th image
+    row (full width), shading by map_values (the shading only scales colour, so
+    the work does not depend on the map's values). Returns per-frame estimates."""
+    from oracle.oracle import Oracle
+    o = Oracle(scene, field=field, threads=threads)
+    pd = scene.map_m + 1
+    nvert = pd ** 3
+    rng = np.random.default_rng(rng_seed)
+    # calibrate on a small pilot, then size the sample to the budget
+    pilot = rng.choice(nvert, min(nvert, 4096), replace=False)
+    t0 = time.perf_counter()
+    o.light_march_ids(pilot)
+    per_vertex = (time.perf_counter() - t0) / pilot.size
+    t0 = time.perf_counter()
+    row = scene.height // 2
+    o.view_march(map_values, window=(0, row, scene.width, 1))
+    per_row = time.perf_counter() - t0
+    nv = int(min(nvert, max(4096, 0.6 * budget_s / max(per_vertex, 1e-9))))
+    nrows = int(min(scene.height, max(1, 0.4 * budget_s / max(per_row, 1e-9))))
+    ids = rng.choice(nvert, nv, replace=False)
+    t0 = time.perf_counter()
+    _, light_samples = o.light_march_ids(ids)
+    t_light = time.perf_counter() - t0
+    rows = np.linspace(0, scene.height - 1, nrows).round().astype(int)
+    t0 = time.perf_counter()
+    lit = 0
+    for y in rows:
+        _, l = o.view_march(map_values, window=(0, int(y), scene.width, 1))
+        lit += l
+    t_view = time.perf_counter() - t0
+    frame_s = t_light * nvert / nv + t_view * scene.height / nrows
+    lit_frame = lit * scene.height / nrows
+    return {"frame_s": frame_s, "lit_per_frame": lit_frame, "value": lit_frame / frame_s,
+            "sample": f"{nv} of {nvert} map vertices (random) + {nrows} of {scene.height} image rows; "
+                      f"timed {t_light + t_view:.1f} s, extrapolated to one frame",
+            "t_light_s": t_light, "t_view_s": t_view, "light_samples_sampled": light_samples}
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    from oracle.oracle import noise_field
+    threads = os.cpu_count() or 1
+    s = build_scene(args.config)
+    if s.kind == "noise":
+        field = noise_field(s.dims, s.params, s.octaves, s.base_freq, threads=threads)
+    else:
+        field = s.field_numpy()
+    zero_map = np.zeros((s.map_m + 1,) * 3, np.float32)
+    per_step = max(1.0, min(10.0, 150.0 / max(1, args.steps + args.warmup)))
+    results = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_sample_frame(s, field, zero_map, per_step, threads, rng_seed=i)
+        if i >= args.warmup:
+            results.append(r)
+    frame_s = float(np.mean([r["frame_s"] for r in results]))
+    lit = float(np.mean([r["lit_per_frame"] for r in results]))
+    value = lit / frame_s
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": frame_s * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded gradient noise generated on the CPU)",
+            "config": workload_desc(s, args.config),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": results[-1]["sample"] + "; the reference cannot be built here (VTK-m, "
+                                       "MPI absent), so its algorithm runs as the project's C++ restatement"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from pilot_b200 import beams as B
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    stream = torch.cuda.current_stream()
+    s = build_scene(args.config)
+    fd = s.field_device()
+    r = B.Renderer(local, stream=stream.cuda_stream)
+    r.set_volume(fd, origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+    s.configure(r)
+    cam = s.camera()
+    out = torch.empty((s.height, s.width, 4), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda") if args.config != 1 else None
+
+    _, t0 = r.render(cam, out=out, timings=True)          # counts for one frame (deterministic)
+    lit_frame, light_frame = t0["lit_samples"], t0["light_samples"]
+    launches_per_frame = t0["kernel_launches"]
+    r.set_reuse_shadow_map(True)   # the explicit build below is the frame's map; render reuses it
+
+    def frame(evs=None):
+        if flush is not None:
+            flush.zero_()
+        if evs:
+            evs[0].record(stream)
+        r.build_shadow_map(timings=False)
+        if evs:
+            evs[1].record(stream)
+        r.render(cam, out=out, timings=False)
+        if evs:
+            evs[2].record(stream)
+
+    for _ in range(args.warmup):
+        frame()
+    torch.cuda.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    with sampler:
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for i in range(args.steps):
+            frame(evs[i])
+        stop.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    total_ms = start.elapsed_time(stop)
+    if flush is not None:  # the flush is not part of a frame
+        total_ms = sum(e[0].elapsed_time(e[2]) for e in evs)
+    k1_ms = sum(e[0].elapsed_time(e[1]) for e in evs) / args.steps
+    k2_ms = sum(e[1].elapsed_time(e[2]) for e in evs) / args.steps
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * args.steps * lit_frame / (max_ms / 1e3)
+
+    # roofline of the dominant kernel
+    peak, peak_kind = measured_peaks()
+    nvert = (s.map_m + 1) ** 3
+    npix = s.width * s.height
+    k1_bytes = light_frame * BYTES_LIGHT_SAMPLE + nvert * BYTES_MAP_VERTEX
+    k2_bytes = lit_frame * BYTES_LIT_SAMPLE + npix * BYTES_PIXEL
+    if k1_ms >= k2_ms:
+        kname, kbytes, kms = "k_light_march", k1_bytes, k1_ms
+    else:
+        kname, kbytes, kms = "k_view_march", k2_bytes, k2_ms
+    achieved = kbytes / (kms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": profiled_traffic(kname),
+                "algorithmic_bytes_per_launch": kbytes,
+                "bytes_model": "light sample 32 B + 4 B/vertex; lit sample 64 B + 16 B/pixel",
+                "k_light_march_ms": k1_ms, "k_view_march_ms": k2_ms,
+                "k_light_march_GBps": k1_bytes / (k1_ms / 1e3) / 1e9,
+                "k_view_march_GBps": k2_bytes / (k2_ms / 1e3) / 1e9}
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        host_field = fd.cpu().pin_memory()
+        host_out = torch.empty((s.height, s.width, 4), dtype=torch.float32).pin_memory()
+        r.set_reuse_shadow_map(False)
+        for _ in range(2):
+            r.set_volume(host_field, dims=s.dims, origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+            r.render(cam, out=host_out, timings=False)
+        ne = max(3, min(args.steps, 20))
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(ne):
+            r.set_volume(host_field, dims=s.dims, origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+            r.render(cam, out=host_out, timings=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * ne * lit_frame / (float(te.item()) / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(host_field.numel() * 4 + s.tf.nbytes),
+               "d2h_bytes_per_step": int(host_out.numel() * 4),
+               "ms_per_step": float(te.item()) / ne,
+               "path": "beams_set_volume(pinned host field) + beams_render(pinned host image) per step"}
+        r.set_reuse_shadow_map(True)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        field = fd.cpu().numpy()
+        gpu_map = r.get_shadow_map(nvert).reshape((s.map_m + 1,) * 3)
+        c = cpu_sample_frame(s, field, gpu_map, args.cpu_budget, threads)
+        cpu = {"value": c["value"], "unit": UNIT, "cores": threads, "kind": "port", "sample": c["sample"],
+               "ms_per_frame": c["frame_s"] * 1e3}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded 4-octave gradient noise, generated on the device)",
+                "config": dict(workload_desc(s, args.config), parallelism=f"replicas x{world}"),
+                "ms_per_frame": max_ms / args.steps, "map_build_ms": k1_ms, "view_march_ms": k2_ms,
+                "lit_samples_per_frame": lit_frame, "light_samples_per_frame": light_frame,
+                "gpu_launches": launches_per_frame * args.steps,
+                "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": sampler.summary()}
+        print(json.dumps(line), flush=True)
+    r.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=1, choices=[0, 1])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work for cpu_baseline")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up frames
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

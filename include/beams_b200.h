@@ -1,0 +1,179 @@
+/*
+ * beams_b200.h — C ABI of the B200-native Beams lighted volume renderer.
+ *
+ * The library replaces the hot path behind beams::rendering::MapperLightedVolume
+ * (beams/rendering/MapperLightedVolume.h:16-62) and LightedVolumeRenderer
+ * (beams/rendering/LightedVolumeRenderer.h:20-101): the light-space march that
+ * builds the (M+1)^3 transmittance ("opacity") map and the view-ray march that
+ * samples the field, applies the transfer function, shades by the map and
+ * composites front to back.
+ *
+ * Conventions
+ *  - Every entry point returns a beams_status; no C++ exception crosses the ABI.
+ *    The reference throws vtkm::cont::ErrorBadValue at the matching places.
+ *  - Caller-owned inputs are copied unless the struct says on_device=1, in which
+ *    case the device pointer is borrowed until the next set_* call or destroy.
+ *  - One renderer per host thread. All GPU work is ordered on the stream given
+ *    to beams_create (NULL = the legacy default stream).
+ *  - Pixel (x, y) is stored at rgba[4*(y*width + x)], y = 0 is the bottom row.
+ */
+#ifndef BEAMS_B200_H
+#define BEAMS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BEAMS_ABI_VERSION 1
+
+typedef enum beams_status {
+  BEAMS_OK = 0,
+  BEAMS_ERR_INVALID_ARG = 1,
+  BEAMS_ERR_UNSUPPORTED = 2,
+  BEAMS_ERR_CUDA = 3,
+  BEAMS_ERR_OOM = 4,
+  BEAMS_ERR_TIMEOUT = 5,
+  BEAMS_ERR_CONFIG = 6,
+  BEAMS_ERR_INTERNAL = 7,
+  BEAMS_ERR_STATE = 8
+} beams_status;
+
+typedef enum beams_dtype { BEAMS_F32 = 0, BEAMS_BF16 = 1, BEAMS_F16 = 2 } beams_dtype;
+typedef enum beams_assoc { BEAMS_ASSOC_POINTS = 0, BEAMS_ASSOC_CELLS = 1 } beams_assoc;
+
+/* Render forms. EXACT is the reference algorithm in FP32. PRECISION stores the
+ * field (BF16/F16, chosen by the volume dtype) and the map (F16) in 16 bits and
+ * accumulates optical depth in FP32 with Kahan compensation. MLP replaces the
+ * map build and lookup by a trained transmittance network. */
+typedef enum beams_form { BEAMS_FORM_EXACT = 0, BEAMS_FORM_PRECISION = 1, BEAMS_FORM_MLP = 2 } beams_form;
+
+/* A structured scalar volume on a uniform grid. The renderer builds the same
+ * float32 rectilinear coordinate arrays the reference scenes build
+ * (origin + i*spacing, beams/sources/Spheres.cxx:144-156). */
+typedef struct beams_volume {
+  const void* data;     /* dims[0]*dims[1]*dims[2] values, x fastest */
+  int dtype;            /* beams_dtype */
+  int dims[3];          /* point dimensions */
+  double origin[3];
+  double spacing[3];
+  double range[2];      /* scalar range used to normalise (SetData's scalarRange) */
+  int assoc;            /* beams_assoc */
+  int on_device;        /* 1: data is a device pointer on the renderer's device */
+} beams_volume;
+
+/* Pinhole camera; rays through pixel centres. */
+typedef struct beams_camera {
+  double position[3];
+  double look_at[3];
+  double up[3];
+  double fov_y_deg;
+  int width;
+  int height;
+} beams_camera;
+
+/* Filled by beams_render when a non-NULL pointer is given (the call then
+ * synchronises the stream). Times are CUDA-event times on the renderer stream. */
+typedef struct beams_timings {
+  float map_build_ms;          /* light march (Phase 1 in the reference) */
+  float view_march_ms;         /* slab + view march (Phase 4) */
+  float composite_ms;          /* brick composite / copy-out (Phase 5) */
+  float total_ms;
+  unsigned long long light_samples;  /* light-march samples evaluated */
+  unsigned long long lit_samples;    /* view samples composited */
+  unsigned long long rays_hit;       /* view rays that entered the volume */
+  unsigned long long mlp_samples;    /* view samples shaded by the MLP */
+  int map_vertices;                  /* (M+1)^3 of the map built this frame, 0 if reused */
+  int fallback_tiles;                /* MLP form: tiles that used the exact map */
+  int kernel_launches;               /* kernels this call launched */
+} beams_timings;
+
+typedef struct beams_renderer beams_renderer;
+
+/* ---- lifetime ------------------------------------------------------------ */
+/* Replaces MapperLightedVolume::MapperLightedVolume() (MapperLightedVolume.cxx:47-50)
+ * and its InternalsType (MapperLightedVolume.cxx:27-45). */
+beams_status beams_create(beams_renderer** out, int device, void* cuda_stream);
+/* Replaces MapperLightedVolume::~MapperLightedVolume() (MapperLightedVolume.cxx:52). */
+beams_status beams_destroy(beams_renderer* r);
+/* Last error text of this renderer (thread-local text when r is NULL). */
+const char* beams_last_error(const beams_renderer* r);
+int beams_abi_version(void);
+
+/* ---- scene setters --------------------------------------------------------- */
+/* Replaces LightedVolumeRenderer::SetData (LightedVolumeRenderer.cxx:766-779),
+ * called from MapperLightedVolume::RenderCells (MapperLightedVolume.cxx:160-161). */
+beams_status beams_set_volume(beams_renderer* r, const beams_volume* v);
+/* Replaces LightedVolumeRenderer::SetColorMap (LightedVolumeRenderer.cxx:761-764):
+ * n RGBA entries, already sampled from the colour table. */
+beams_status beams_set_color_map(beams_renderer* r, const float* rgba, int n);
+/* Replaces MapperLightedVolume::SetShadowMapSize (MapperLightedVolume.cxx:101-104). */
+beams_status beams_set_shadow_map_size(beams_renderer* r, int mx, int my, int mz);
+/* Replaces MapperLightedVolume::SetUseShadowMap (MapperLightedVolume.cxx:96-99). */
+beams_status beams_set_use_shadow_map(beams_renderer* r, int enable);
+/* Replaces MapperLightedVolume::ClearLights (MapperLightedVolume.cxx:81-84). */
+beams_status beams_clear_lights(beams_renderer* r);
+/* Replaces MapperLightedVolume::AddLight with a PointLight (MapperLightedVolume.cxx:76-79,
+ * LightedVolumeRenderer.cxx:835-841): light colour = color * intensity. Only the
+ * first light shades, as in the reference (TransmittanceMap.h:591-592). */
+beams_status beams_add_point_light(beams_renderer* r, const double pos[3], const float color[3],
+                                   float intensity);
+/* Extension (no reference counterpart; the reference has point lights only,
+ * beams/rendering/PointLight.h:16-30): a directional light travelling along dir. */
+beams_status beams_add_directional_light(beams_renderer* r, const double dir[3], const float color[3],
+                                         float intensity);
+/* Replaces MapperLightedVolume::SetSampleDistance (MapperLightedVolume.cxx:316-319) and
+ * LightedVolumeRenderer::SetSampleDistance (LightedVolumeRenderer.cxx:1374-1379).
+ * d <= 0 returns BEAMS_ERR_INVALID_ARG, where the reference throws. */
+beams_status beams_set_sample_distance(beams_renderer* r, float d);
+/* Early-termination threshold on accumulated alpha. The reference breaks at
+ * alpha >= 1.0 (LightedVolumeRenderer.cxx:491-492); 1.0 is the default. */
+beams_status beams_set_termination_alpha(beams_renderer* r, float alpha);
+/* Light-march step count over the volume diagonal; the reference fixes 128
+ * (TransmittanceMap.h:584-585), which is the default. */
+beams_status beams_set_light_steps(beams_renderer* r, float steps);
+/* Slab test precision for view rays: 1 (default) = FP64 t_enter/t_exit,
+ * 0 = the reference's FP32 rcp_safe form (LightedVolumeRenderer.cxx:644-718). */
+beams_status beams_set_slab_fp64(beams_renderer* r, int enable);
+/* Keep the last map when its inputs (volume, colour map, light, map size) did not
+ * change. Off by default: the reference rebuilds the map every frame. */
+beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable);
+/* Replaces MapperLightedVolume::SetCompositeBackground (MapperLightedVolume.cxx:321-324):
+ * blend rgb over an opaque background colour after compositing. Off by default. */
+beams_status beams_set_background(beams_renderer* r, int enable, const float rgba[4]);
+/* Selects the render form (beams_form). opts: NULL, or for BEAMS_FORM_MLP a
+ * const beams_mlp_options*. */
+beams_status beams_set_form(beams_renderer* r, int form, const void* opts);
+
+/* ---- render --------------------------------------------------------------- */
+/* Replaces MapperLightedVolume::RenderCells (MapperLightedVolume.cxx:114-193):
+ * map build (Phase 1/3) + view march (Phase 4) + copy-out (Phase 5).
+ * rgba_out holds width*height*4 floats, premultiplied RGBA, on the host unless
+ * out_on_device. t may be NULL (then nothing synchronises). */
+beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgba_out,
+                          int out_on_device, beams_timings* t);
+
+/* Map access for tests and tools: copies the current (M+1)^3 float32 map
+ * (x fastest) to dst (host or device). Returns BEAMS_ERR_STATE before a build. */
+beams_status beams_get_shadow_map(beams_renderer* r, float* dst, size_t count, int dst_on_device);
+/* Builds the map only (Phase 1), without a view march. */
+beams_status beams_build_shadow_map(beams_renderer* r, beams_timings* t);
+
+/* ---- scene generation (synthetic inputs; device-side) ----------------------- */
+/* Fills a float32 field (x fastest, n[0]*n[1]*n[2] values) on the device with a sum
+ * of Gaussian blobs: params = nblobs x {cx, cy, cz, sigma, amplitude} in domain
+ * units [0,1]^3; the result is normalised to [0,1] when normalise != 0. */
+beams_status beams_generate_blobs(float* dev_out, const int n[3], const float* params, int nblobs,
+                                  int normalise, void* cuda_stream);
+/* Gradient (Perlin-style) noise, octaves summed with lacunarity and gain, then
+ * remapped to [0,1]. perm: 256 bytes (a permutation of 0..255). */
+beams_status beams_generate_noise(float* dev_out, const int n[3], const unsigned char* perm,
+                                  int octaves, float base_freq, float lacunarity, float gain,
+                                  void* cuda_stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BEAMS_B200_H */

@@ -1,0 +1,89 @@
+/*
+ * beams_oracle.h — CPU oracle for the Beams lighted volume renderer hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This is the checker: a plain C++ restatement of the
+ * reference worklets, used by the tests, by smoke() and as the CPU baseline.
+ * Nothing in the product library links, loads or calls it.
+ *
+ * Parity is UNPINNED: the reference ships no tests, golden images or fixtures,
+ * and it cannot be built here (VTK-m 1.9, MPI, fmt and toml++ are absent and its
+ * driver's Run() body is commented out). The restatement follows the reference
+ * source line by line; the few VTK-m internals it relies on are restated from
+ * their published definitions (see beams_oracle.cpp).
+ *
+ * Two modes share one template: "f32" repeats the reference's float32 arithmetic
+ * (no FMA contraction, IEEE division and sqrt), "f64" is the same algorithm in
+ * double precision and is the accuracy yardstick.
+ */
+#ifndef BEAMS_ORACLE_H
+#define BEAMS_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_scene {
+  const float* field;   /* point field, x fastest */
+  int dims[3];          /* point dims */
+  double origin[3];
+  double spacing[3];
+  double range[2];
+  const float* tf;      /* tf_n x RGBA */
+  int tf_n;
+  int light_kind;       /* 0 point, 1 directional */
+  double light[3];      /* position, or travel direction */
+  float light_color[3];
+  float light_intensity;
+  int map_m[3];         /* cells per axis of the map */
+  int use_map;
+  float sample_distance;/* <= 0: |extent| / 200 (LightedVolumeRenderer.cxx:815-819) */
+  float alpha_cutoff;   /* reference: 1.0 */
+  float light_steps;    /* reference: 128 */
+  int slab_fp64;        /* 1: slab test in double, rounded to float (f32 mode) */
+  double cam_pos[3];
+  double cam_look[3];
+  double cam_up[3];
+  double fov_y_deg;
+  int width;
+  int height;
+} oracle_scene;
+
+/* Light march over every map vertex ((M+1)^3, x fastest). */
+int oracle_light_march_f32(const oracle_scene* s, float* map_out, int threads, uint64_t* samples);
+int oracle_light_march_f64(const oracle_scene* s, double* map_out, int threads, uint64_t* samples);
+/* Light march over a list of flat vertex ids only (bounded CPU samples). */
+int oracle_light_march_ids_f32(const oracle_scene* s, const int64_t* ids, int64_t n, float* out,
+                               int threads, uint64_t* samples);
+int oracle_light_march_ids_f64(const oracle_scene* s, const int64_t* ids, int64_t n, double* out,
+                               int threads, uint64_t* samples);
+/* Transmittance 1 - o at arbitrary points (march from the light to each point). */
+int oracle_light_march_points_f64(const oracle_scene* s, const double* pts, int64_t n,
+                                  const double* light_pos, double* opacity_out, int threads);
+
+/* View march over the pixel window [x0,x0+w) x [y0,y0+h); rgba_out is w*h*4.
+ * map may be NULL when use_map == 0. lazy != 0: ignore map and compute the map
+ * vertices a lookup needs on demand (memoised). */
+int oracle_view_march_f32(const oracle_scene* s, const float* map, int x0, int y0, int w, int h,
+                          float* rgba_out, int threads, uint64_t* lit_samples);
+int oracle_view_march_f64(const oracle_scene* s, const double* map, int x0, int y0, int w, int h,
+                          double* rgba_out, int threads, uint64_t* lit_samples);
+int oracle_view_march_lazy_f64(const oracle_scene* s, int x0, int y0, int w, int h, int stride,
+                               double* rgba_out, int threads, uint64_t* lit_samples);
+
+/* Per-pixel slab test (t_enter, t_exit; miss -> t_enter = -1). */
+int oracle_ray_setup_f32(const oracle_scene* s, int x, int y, float out[8]);
+
+/* Gradient-noise field (x fastest), remapped to [0,1]; the reference arm's input. */
+int oracle_generate_noise(float* out, int nx, int ny, int nz, const unsigned char* perm, int octaves,
+                          float f0, float lac, float gain, int threads);
+
+/* Sort-last "over" of B premultiplied RGBA images in the given order
+ * (MapperLightedVolume.cxx:284-297). */
+int oracle_composite_f32(const float* images, int nimages, int npix, const int* order,
+                         float* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

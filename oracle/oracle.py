@@ -1,0 +1,166 @@
+"""ctypes access to the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+The oracle is the checker and the CPU baseline; the product never imports it.
+Parity is unpinned: the reference has no golden data and cannot be built here,
+so the oracle is a line-by-line restatement of the reference worklets (see
+beams_oracle.cpp for the cited lines and the VTK-m definitions it restates).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import build_oracle
+
+_lib = None
+
+
+class OracleScene(C.Structure):
+    _fields_ = [("field", C.c_void_p), ("dims", C.c_int * 3), ("origin", C.c_double * 3),
+                ("spacing", C.c_double * 3), ("range", C.c_double * 2), ("tf", C.c_void_p), ("tf_n", C.c_int),
+                ("light_kind", C.c_int), ("light", C.c_double * 3), ("light_color", C.c_float * 3),
+                ("light_intensity", C.c_float), ("map_m", C.c_int * 3), ("use_map", C.c_int),
+                ("sample_distance", C.c_float), ("alpha_cutoff", C.c_float), ("light_steps", C.c_float),
+                ("slab_fp64", C.c_int), ("cam_pos", C.c_double * 3), ("cam_look", C.c_double * 3),
+                ("cam_up", C.c_double * 3), ("fov_y_deg", C.c_double), ("width", C.c_int), ("height", C.c_int)]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = build_oracle.build()
+        L = C.CDLL(str(path))
+        P, S = C.c_void_p, C.POINTER(OracleScene)
+        u64p = C.POINTER(C.c_uint64)
+        for name, args in {
+            "oracle_light_march_f32": [S, P, C.c_int, u64p],
+            "oracle_light_march_f64": [S, P, C.c_int, u64p],
+            "oracle_light_march_ids_f32": [S, P, C.c_int64, P, C.c_int, u64p],
+            "oracle_light_march_ids_f64": [S, P, C.c_int64, P, C.c_int, u64p],
+            "oracle_light_march_points_f64": [S, P, C.c_int64, P, P, C.c_int],
+            "oracle_view_march_f32": [S, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
+            "oracle_view_march_f64": [S, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
+            "oracle_view_march_lazy_f64": [S, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
+            "oracle_ray_setup_f32": [S, C.c_int, C.c_int, P],
+            "oracle_composite_f32": [P, C.c_int, C.c_int, P, P],
+            "oracle_generate_noise": [P, C.c_int, C.c_int, C.c_int, P, C.c_int, C.c_float, C.c_float,
+                                      C.c_float, C.c_int],
+        }.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Oracle:
+    """Oracle bound to one scene and one field array (z, y, x) float32."""
+
+    def __init__(self, scene, field: np.ndarray | None = None, threads: int = 0):
+        self.scene = scene
+        self.field = np.ascontiguousarray(scene.field_numpy() if field is None else field, np.float32)
+        self.tf = np.ascontiguousarray(scene.tf, np.float32)
+        self.threads = threads
+        s = scene
+        self.cs = OracleScene(
+            _p(self.field), (C.c_int * 3)(*s.dims), (C.c_double * 3)(*s.origin), (C.c_double * 3)(*s.spacing),
+            (C.c_double * 2)(*s.value_range), _p(self.tf), self.tf.shape[0], s.light_kind,
+            (C.c_double * 3)(*s.light), (C.c_float * 3)(*s.light_color), s.light_intensity,
+            (C.c_int * 3)(s.map_m, s.map_m, s.map_m), int(s.use_map), s.sample_distance, s.cutoff,
+            s.light_steps, int(s.slab_fp64), (C.c_double * 3)(*s.cam_pos), (C.c_double * 3)(*s.cam_look),
+            (C.c_double * 3)(*s.cam_up), s.fov_y_deg, s.width, s.height)
+
+    @property
+    def map_shape(self):
+        m = self.scene.map_m + 1
+        return (m, m, m)
+
+    def light_march(self, fp64: bool = False):
+        out = np.empty(self.map_shape, np.float64 if fp64 else np.float32)
+        ns = C.c_uint64()
+        fn = lib().oracle_light_march_f64 if fp64 else lib().oracle_light_march_f32
+        if fn(C.byref(self.cs), _p(out), self.threads, C.byref(ns)):
+            raise RuntimeError("oracle light march rejected the scene")
+        return out, ns.value
+
+    def light_march_ids(self, ids: np.ndarray, fp64: bool = False):
+        ids = np.ascontiguousarray(ids, np.int64)
+        out = np.empty(ids.shape[0], np.float64 if fp64 else np.float32)
+        ns = C.c_uint64()
+        fn = lib().oracle_light_march_ids_f64 if fp64 else lib().oracle_light_march_ids_f32
+        if fn(C.byref(self.cs), _p(ids), ids.shape[0], _p(out), self.threads, C.byref(ns)):
+            raise RuntimeError("oracle light march rejected the scene")
+        return out, ns.value
+
+    def point_opacity(self, pts: np.ndarray, light_pos: np.ndarray | None = None):
+        pts = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+        out = np.empty(pts.shape[0], np.float64)
+        lp = None if light_pos is None else np.ascontiguousarray(light_pos, np.float64).reshape(-1, 3)
+        if lib().oracle_light_march_points_f64(C.byref(self.cs), _p(pts), pts.shape[0],
+                                               None if lp is None else _p(lp), _p(out), self.threads):
+            raise RuntimeError("oracle point march rejected the scene")
+        return out
+
+    def view_march(self, map_values=None, window=None, fp64: bool = False):
+        s = self.scene
+        x0, y0, w, h = window if window is not None else (0, 0, s.width, s.height)
+        dt = np.float64 if fp64 else np.float32
+        out = np.zeros((h, w, 4), dt)
+        if s.use_map and map_values is None:
+            map_values, _ = self.light_march(fp64)
+        mp = None if map_values is None else np.ascontiguousarray(map_values, dt)
+        lit = C.c_uint64()
+        fn = lib().oracle_view_march_f64 if fp64 else lib().oracle_view_march_f32
+        if fn(C.byref(self.cs), None if mp is None else _p(mp), x0, y0, w, h, _p(out), self.threads,
+              C.byref(lit)):
+            raise RuntimeError("oracle view march rejected the scene")
+        return out, lit.value
+
+    def view_march_lazy_f64(self, window, stride: int = 1):
+        x0, y0, w, h = window
+        ow, oh = -(-w // stride), -(-h // stride)
+        out = np.zeros((oh, ow, 4), np.float64)
+        lit = C.c_uint64()
+        if lib().oracle_view_march_lazy_f64(C.byref(self.cs), x0, y0, w, h, stride, _p(out), self.threads,
+                                            C.byref(lit)):
+            raise RuntimeError("oracle lazy view march rejected the scene")
+        return out, lit.value
+
+    def ray_setup(self, x: int, y: int):
+        out = np.zeros(8, np.float32)
+        lib().oracle_ray_setup_f32(C.byref(self.cs), x, y, _p(out))
+        return out
+
+
+def composite(images: np.ndarray, order) -> np.ndarray:
+    """Sort-last over of premultiplied RGBA images (MapperLightedVolume.cxx:284-297)."""
+    imgs = np.ascontiguousarray(images, np.float32)
+    n = imgs.shape[0]
+    npix = imgs[0].size // 4
+    order = np.ascontiguousarray(order, np.int32)
+    out = np.zeros(imgs.shape[1:], np.float32)
+    if lib().oracle_composite_f32(_p(imgs), n, npix, _p(order), _p(out)):
+        raise RuntimeError("oracle composite rejected the input")
+    return out
+
+
+def noise_field(dims, perm, octaves=4, base_freq=4.0, lacunarity=2.0, gain=0.5, threads=0) -> np.ndarray:
+    """Gradient-noise field on the CPU (z, y, x), the same float32 operations as the
+    library's device generator."""
+    nx, ny, nz = dims
+    out = np.empty((nz, ny, nx), np.float32)
+    perm = np.ascontiguousarray(perm, np.uint8)
+    if lib().oracle_generate_noise(_p(out), nx, ny, nz, _p(perm), octaves, base_freq, lacunarity, gain, threads):
+        raise RuntimeError("oracle noise generator rejected the arguments")
+    return out
+
+
+def psnr(a: np.ndarray, b: np.ndarray) -> float:
+    mse = float(np.mean((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2))
+    return float("inf") if mse == 0 else 10.0 * np.log10(1.0 / mse)

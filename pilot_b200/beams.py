@@ -1,0 +1,320 @@
+"""ctypes binding of libbeams_b200.so and a mirror of the reference's mapper API.
+
+``Renderer`` is a thin 1:1 wrapper of the C ABI (include/beams_b200.h).
+``MapperLightedVolume`` mirrors beams::rendering::MapperLightedVolume
+(beams/rendering/MapperLightedVolume.h:16-62): the same setter names, the same
+argument meaning, the same error behaviour (the reference throws
+vtkm::cont::ErrorBadValue; this raises BeamsError with the library's message).
+
+There is no fallback: importing this module fails loudly when the CUDA library
+has not been built, and every render runs the CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_LIB_PATH = Path(__file__).resolve().parent / "lib" / "libbeams_b200.so"
+
+BEAMS_OK = 0
+STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "UNSUPPORTED", 3: "CUDA", 4: "OOM", 5: "TIMEOUT",
+                6: "CONFIG", 7: "INTERNAL", 8: "STATE"}
+F32, BF16, F16 = 0, 1, 2
+ASSOC_POINTS, ASSOC_CELLS = 0, 1
+FORM_EXACT, FORM_PRECISION, FORM_MLP = 0, 1, 2
+
+
+class BeamsError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class Volume(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("dtype", C.c_int), ("dims", C.c_int * 3),
+                ("origin", C.c_double * 3), ("spacing", C.c_double * 3), ("range", C.c_double * 2),
+                ("assoc", C.c_int), ("on_device", C.c_int)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("position", C.c_double * 3), ("look_at", C.c_double * 3), ("up", C.c_double * 3),
+                ("fov_y_deg", C.c_double), ("width", C.c_int), ("height", C.c_int)]
+
+
+class Timings(C.Structure):
+    _fields_ = [("map_build_ms", C.c_float), ("view_march_ms", C.c_float), ("composite_ms", C.c_float),
+                ("total_ms", C.c_float), ("light_samples", C.c_ulonglong), ("lit_samples", C.c_ulonglong),
+                ("rays_hit", C.c_ulonglong), ("mlp_samples", C.c_ulonglong), ("map_vertices", C.c_int),
+                ("fallback_tiles", C.c_int), ("kernel_launches", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    """Loads the CUDA library (raises when it is missing: there is no CPU path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not _LIB_PATH.exists():
+        raise ImportError(f"{_LIB_PATH} is missing: run pilot_b200/build.py (there is no CPU fallback)")
+    L = C.CDLL(str(_LIB_PATH))
+    P = C.c_void_p
+    sig = {
+        "beams_abi_version": ([], C.c_int),
+        "beams_last_error": ([P], C.c_char_p),
+        "beams_create": ([C.POINTER(P), C.c_int, P], C.c_int),
+        "beams_destroy": ([P], C.c_int),
+        "beams_set_volume": ([P, C.POINTER(Volume)], C.c_int),
+        "beams_set_color_map": ([P, P, C.c_int], C.c_int),
+        "beams_set_shadow_map_size": ([P, C.c_int, C.c_int, C.c_int], C.c_int),
+        "beams_set_use_shadow_map": ([P, C.c_int], C.c_int),
+        "beams_clear_lights": ([P], C.c_int),
+        "beams_add_point_light": ([P, P, P, C.c_float], C.c_int),
+        "beams_add_directional_light": ([P, P, P, C.c_float], C.c_int),
+        "beams_set_sample_distance": ([P, C.c_float], C.c_int),
+        "beams_set_termination_alpha": ([P, C.c_float], C.c_int),
+        "beams_set_light_steps": ([P, C.c_float], C.c_int),
+        "beams_set_slab_fp64": ([P, C.c_int], C.c_int),
+        "beams_set_reuse_shadow_map": ([P, C.c_int], C.c_int),
+        "beams_set_background": ([P, C.c_int, P], C.c_int),
+        "beams_set_form": ([P, C.c_int, P], C.c_int),
+        "beams_render": ([P, C.POINTER(Camera), P, C.c_int, C.POINTER(Timings)], C.c_int),
+        "beams_get_shadow_map": ([P, P, C.c_size_t, C.c_int], C.c_int),
+        "beams_build_shadow_map": ([P, C.POINTER(Timings)], C.c_int),
+        "beams_generate_blobs": ([P, P, P, C.c_int, C.c_int, P], C.c_int),
+        "beams_generate_noise": ([P, P, P, C.c_int, C.c_float, C.c_float, C.c_float, P], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def exported_symbols():
+    """Names the header declares; used by the load test."""
+    hdr = Path(__file__).resolve().parent.parent / "include" / "beams_b200.h"
+    import re
+    text = hdr.read_text()
+    return sorted(set(re.findall(r"^\s*(?:beams_status|const char\*|int)\s+(beams_\w+)\s*\(", text, re.M)))
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(C.c_void_p)
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return a
+
+
+def _d3(v):
+    return (C.c_double * 3)(*[float(x) for x in v])
+
+
+def _f3(v):
+    return (C.c_float * 3)(*[float(x) for x in v])
+
+
+class Renderer:
+    """1:1 wrapper of the beams_* C ABI."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self._L = lib()
+        h = C.c_void_p()
+        self._check(self._L.beams_create(C.byref(h), int(device), C.c_void_p(stream) if stream else None), None)
+        self._h = h
+        self._keep = []
+
+    def _check(self, st, h="self"):
+        if st != BEAMS_OK:
+            hh = self._h if h == "self" else h
+            msg = self._L.beams_last_error(hh)
+            raise BeamsError(st, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.beams_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- setters --------------------------------------------------------------
+    def set_volume(self, data, dims=None, origin=(0, 0, 0), spacing=None, value_range=None,
+                   dtype=F32, assoc=ASSOC_POINTS):
+        """data: numpy array (z, y, x) on the host, or a torch CUDA tensor."""
+        on_device = 0
+        if isinstance(data, np.ndarray):
+            arr = np.ascontiguousarray(data)
+            if dims is None:
+                nz, ny, nx = arr.shape
+                dims = (nx, ny, nz) if assoc == ASSOC_POINTS else (nx + 1, ny + 1, nz + 1)
+            if dtype == F32:
+                arr = arr.astype(np.float32, copy=False)
+            self._keep_host = arr
+            ptr = arr.ctypes.data_as(C.c_void_p)
+        else:  # torch tensor
+            on_device = 1 if data.is_cuda else 0
+            if dims is None:
+                nz, ny, nx = data.shape
+                dims = (nx, ny, nz) if assoc == ASSOC_POINTS else (nx + 1, ny + 1, nz + 1)
+            ptr = C.c_void_p(data.data_ptr())
+            self._keep_dev = data
+        if spacing is None:
+            spacing = tuple(1.0 / (d - 1) for d in dims)
+        if value_range is None:
+            value_range = (0.0, 1.0)
+        v = Volume(ptr, dtype, (C.c_int * 3)(*dims), _d3(origin), _d3(spacing),
+                   (C.c_double * 2)(*value_range), assoc, on_device)
+        self._check(self._L.beams_set_volume(self._h, C.byref(v)))
+
+    def set_color_map(self, rgba):
+        t = np.ascontiguousarray(rgba, dtype=np.float32).reshape(-1, 4)
+        self._check(self._L.beams_set_color_map(self._h, _ptr(t), t.shape[0]))
+
+    def set_shadow_map_size(self, mx, my=None, mz=None):
+        my = mx if my is None else my
+        mz = mx if mz is None else mz
+        self._check(self._L.beams_set_shadow_map_size(self._h, int(mx), int(my), int(mz)))
+
+    def set_use_shadow_map(self, on: bool):
+        self._check(self._L.beams_set_use_shadow_map(self._h, int(bool(on))))
+
+    def clear_lights(self):
+        self._check(self._L.beams_clear_lights(self._h))
+
+    def add_point_light(self, pos, color=(1, 1, 1), intensity=1.0):
+        self._check(self._L.beams_add_point_light(self._h, _d3(pos), _f3(color), float(intensity)))
+
+    def add_directional_light(self, direction, color=(1, 1, 1), intensity=1.0):
+        self._check(self._L.beams_add_directional_light(self._h, _d3(direction), _f3(color), float(intensity)))
+
+    def set_sample_distance(self, d):
+        self._check(self._L.beams_set_sample_distance(self._h, float(d)))
+
+    def set_termination_alpha(self, a):
+        self._check(self._L.beams_set_termination_alpha(self._h, float(a)))
+
+    def set_light_steps(self, s):
+        self._check(self._L.beams_set_light_steps(self._h, float(s)))
+
+    def set_slab_fp64(self, on: bool):
+        self._check(self._L.beams_set_slab_fp64(self._h, int(bool(on))))
+
+    def set_reuse_shadow_map(self, on: bool):
+        self._check(self._L.beams_set_reuse_shadow_map(self._h, int(bool(on))))
+
+    def set_background(self, on: bool, rgba=(1, 1, 1, 1)):
+        c = (C.c_float * 4)(*rgba)
+        self._check(self._L.beams_set_background(self._h, int(bool(on)), c))
+
+    def set_form(self, form: int, opts=None):
+        self._check(self._L.beams_set_form(self._h, int(form), opts))
+
+    # -- render ---------------------------------------------------------------
+    @staticmethod
+    def camera(position, look_at, up, fov_y_deg, width, height) -> Camera:
+        return Camera(_d3(position), _d3(look_at), _d3(up), float(fov_y_deg), int(width), int(height))
+
+    def render(self, cam: Camera, out=None, timings=True):
+        """Renders into out (numpy (H,W,4) float32 host array or torch CUDA tensor)."""
+        if out is None:
+            out = np.zeros((cam.height, cam.width, 4), np.float32)
+        on_dev = 0 if isinstance(out, np.ndarray) else int(out.is_cuda)
+        t = Timings() if timings else None
+        self._check(self._L.beams_render(self._h, C.byref(cam), _ptr(out), on_dev,
+                                         C.byref(t) if t is not None else None))
+        return out, (t.as_dict() if t is not None else None)
+
+    def build_shadow_map(self, timings=True):
+        """Phase 1 only. With timings=False nothing synchronises."""
+        t = Timings() if timings else None
+        self._check(self._L.beams_build_shadow_map(self._h, C.byref(t) if t is not None else None))
+        return t.as_dict() if t is not None else None
+
+    def get_shadow_map(self, count):
+        m = np.empty(count, np.float32)
+        self._check(self._L.beams_get_shadow_map(self._h, _ptr(m), m.size, 0))
+        return m
+
+
+class MapperLightedVolume:
+    """Mirror of beams::rendering::MapperLightedVolume over the C ABI.
+
+    Reference: beams/rendering/MapperLightedVolume.h:16-62, .cxx:47-324.
+    RenderCells takes the field, its bounds and range, a camera and returns the
+    premultiplied RGBA canvas (the reference writes a CanvasRayTracer).
+    """
+
+    def __init__(self, device: int = 0):
+        self._r = Renderer(device)
+        self._width = self._height = None
+        self._sample_distance = -1.0  # DEFAULT_SAMPLE_DISTANCE (MapperLightedVolume.cxx:19)
+        self._color_map = None
+
+    def SetCanvas(self, width: int, height: int):
+        self._width, self._height = int(width), int(height)
+
+    def SetShadowMapSize(self, size):
+        sx, sy, sz = (size, size, size) if np.isscalar(size) else size
+        self._r.set_shadow_map_size(sx, sy, sz)
+
+    def SetUseShadowMap(self, use: bool):
+        self._r.set_use_shadow_map(use)
+
+    def AddLight(self, position, color=(1, 1, 1), intensity=1.0):
+        self._r.add_point_light(position, color, intensity)
+
+    def ClearLights(self):
+        self._r.clear_lights()
+
+    def SetSampleDistance(self, d: float):
+        # Stored; validated when rendering, like the reference (LightedVolumeRenderer.cxx:1374-1379).
+        self._sample_distance = float(d)
+
+    def SetCompositeBackground(self, on: bool, rgba=(1, 1, 1, 1)):
+        self._r.set_background(on, rgba)
+
+    def SetDensityScale(self, s: float):
+        self._density_scale = float(s)  # stored, never read (as in the reference)
+
+    def SetActiveColorTable(self, rgba_table):
+        self._color_map = np.asarray(rgba_table, np.float32).reshape(-1, 4)
+
+    def RenderCells(self, field, origin, spacing, scalar_range, camera: dict, assoc=ASSOC_POINTS):
+        if self._width is None:
+            raise BeamsError(1, "Ray Tracer: no canvas set")
+        if self._color_map is None:
+            raise BeamsError(8, "no active color table")
+        if self._sample_distance != -1.0:
+            self._r.set_sample_distance(self._sample_distance)
+        self._r.set_volume(field, origin=origin, spacing=spacing, value_range=scalar_range, assoc=assoc)
+        self._r.set_color_map(self._color_map)
+        cam = Renderer.camera(camera["position"], camera["look_at"], camera.get("up", (0, 1, 0)),
+                              camera.get("fov_y_deg", 30.0), self._width, self._height)
+        img, t = self._r.render(cam)
+        self.last_timings = t
+        return img
+
+    @property
+    def renderer(self) -> Renderer:
+        return self._r

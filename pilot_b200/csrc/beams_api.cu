@@ -1,0 +1,566 @@
+// beams_api.cu — the C ABI (include/beams_b200.h): renderer state, parameter
+// derivation and frame orchestration. Host code only; kernels live in k_*.cu.
+//
+// Phase structure of one frame follows LightedVolumeRenderer::RenderOnDevice
+// (beams/rendering/LightedVolumeRenderer.cxx:910-1372): the map is built once
+// (the reference's Phase 3 re-runs Phase 1 from zero opacity when there is a
+// single block, :1210-1256, which yields the same map), then the view march.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/beams_b200.h"
+#include "beams_params.h"
+#include "kernels.h"
+#include "renderer.h"
+
+using beams::Counters;
+using beams::ExactGeo;
+
+namespace {
+thread_local std::string g_tls_error;
+}
+
+namespace beams {
+
+beams_status fail(beams_renderer* r, beams_status s, const std::string& msg) {
+  if (r) r->err = msg;
+  else g_tls_error = msg;
+  return s;
+}
+
+beams_status cuda_fail(beams_renderer* r, cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();  // clear a sticky-free error so the next call starts clean
+  return fail(r, e == cudaErrorMemoryAllocation ? BEAMS_ERR_OOM : BEAMS_ERR_CUDA, m);
+}
+
+beams_status ensure_buffer(beams_renderer* r, void** buf, size_t* cap, size_t bytes, const char* what) {
+  if (*cap >= bytes && *buf) return BEAMS_OK;
+  if (*buf) {
+    cudaFree(*buf);
+    *buf = nullptr;
+    *cap = 0;
+  }
+  cudaError_t e = cudaMalloc(buf, bytes);
+  if (e != cudaSuccess) {
+    *buf = nullptr;
+    return cuda_fail(r, e, what);
+  }
+  *cap = bytes;
+  return BEAMS_OK;
+}
+
+static bool finite3(const double* v) {
+  return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]);
+}
+
+// Derives the kernel parameters exactly as the reference derives them
+// (float32 arithmetic; see the cited lines in beams_params.h).
+beams_status make_geo(beams_renderer* r, const beams_camera* cam, ExactGeo& g) {
+  std::memset(&g, 0, sizeof(g));
+  const beams_volume& v = r->vol;
+  for (int d = 0; d < 3; ++d) {
+    g.n[d] = v.dims[d];
+    g.org[d] = (float)v.origin[d];
+    g.h[d] = (float)v.spacing[d];
+    g.invh[d] = 1.f / g.h[d];
+    g.minp[d] = g.org[d] + g.h[d] * 0.f;
+    g.maxp[d] = g.org[d] + g.h[d] * (float)(v.dims[d] - 1);
+    g.bmin[d] = (double)g.minp[d];
+    g.bmax[d] = (double)g.maxp[d];
+  }
+  const float fmin = (float)v.range[0], fmax = (float)v.range[1];
+  g.min_scalar = fmin;
+  g.inv_delta = ((fmax - fmin) != 0.f) ? 1.f / (fmax - fmin) : fmin;
+  g.tf_n = r->tf_n;
+  float ma = 0.f;
+  for (int i = 0; i < r->tf_n; ++i) {
+    const float a = r->tf[4 * i + 3];
+    ma = (ma < a) ? a : ma;
+  }
+  g.max_alpha = ma;
+  float ext[3];
+  for (int d = 0; d < 3; ++d) ext[d] = (float)(g.bmax[d] - g.bmin[d]);
+  g.extent_mag = std::sqrt(ext[0] * ext[0] + ext[1] * ext[1] + ext[2] * ext[2]);
+  for (int d = 0; d < 3; ++d) {
+    g.pd[d] = r->map_m[d] + 1;
+    g.morig[d] = (float)g.bmin[d];
+    g.msp[d] = ext[d] / (float)r->map_m[d];
+    g.minv[d] = 1.f / g.msp[d];
+  }
+  g.sd = (r->sample_distance > 0.f) ? r->sample_distance : g.extent_mag / 200.f;
+  g.mesh_eps = g.extent_mag * 0.0001f;
+  g.step = g.extent_mag / r->light_steps;
+  g.cutoff = r->cutoff;
+  g.light_budget = (int)(g.extent_mag / g.step) + 8;
+  g.dir_dist = 2.f * g.extent_mag;
+  if (!r->lights.empty()) {
+    const Light& L = r->lights[0];
+    g.light_kind = L.kind;
+    for (int d = 0; d < 3; ++d) g.light_color[d] = L.color[d] * L.intensity;
+    if (L.kind == 0) {
+      for (int d = 0; d < 3; ++d) g.light[d] = (float)L.v[d];
+    } else {
+      const double len = std::sqrt(L.v[0] * L.v[0] + L.v[1] * L.v[1] + L.v[2] * L.v[2]);
+      for (int d = 0; d < 3; ++d) g.light[d] = (float)(L.v[d] / len);
+    }
+  }
+  g.slab_fp64 = r->slab_fp64;
+  g.use_map = r->use_map ? 1 : 0;
+  g.assoc_cells = (v.assoc == BEAMS_ASSOC_CELLS) ? 1 : 0;
+  if (cam) {
+    double f[3], rr[3], u[3];
+    for (int d = 0; d < 3; ++d) f[d] = cam->look_at[d] - cam->position[d];
+    const double fl = std::sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+    for (int d = 0; d < 3; ++d) f[d] /= fl;
+    const double* up = cam->up;
+    rr[0] = f[1] * up[2] - f[2] * up[1];
+    rr[1] = f[2] * up[0] - f[0] * up[2];
+    rr[2] = f[0] * up[1] - f[1] * up[0];
+    const double rl = std::sqrt(rr[0] * rr[0] + rr[1] * rr[1] + rr[2] * rr[2]);
+    if (!(fl > 0) || !(rl > 0)) return fail(r, BEAMS_ERR_INVALID_ARG, "camera: degenerate view or up vector");
+    for (int d = 0; d < 3; ++d) rr[d] /= rl;
+    u[0] = rr[1] * f[2] - rr[2] * f[1];
+    u[1] = rr[2] * f[0] - rr[0] * f[2];
+    u[2] = rr[0] * f[1] - rr[1] * f[0];
+    const double th = std::tan(cam->fov_y_deg * M_PI / 360.0);
+    const double aspect = (double)cam->width / (double)cam->height;
+    for (int d = 0; d < 3; ++d) {
+      g.cam_pos[d] = (float)cam->position[d];
+      g.cf[d] = (float)f[d];
+      g.cr[d] = (float)rr[d];
+      g.cu[d] = (float)u[d];
+    }
+    g.kx = (float)(2.0 * th * aspect / cam->width);
+    g.cx = (float)(th * aspect);
+    g.ky = (float)(2.0 * th / cam->height);
+    g.cy = (float)th;
+    g.width = cam->width;
+    g.height = cam->height;
+  }
+  return BEAMS_OK;
+}
+
+beams_status validate_camera(beams_renderer* r, const beams_camera* cam) {
+  if (!cam) return fail(r, BEAMS_ERR_INVALID_ARG, "camera is NULL");
+  if (cam->width < 1 || cam->height < 1 || cam->width > 16384 || cam->height > 16384)
+    return fail(r, BEAMS_ERR_INVALID_ARG, "camera: width/height must be in [1, 16384]");
+  if (!(cam->fov_y_deg > 0.0 && cam->fov_y_deg < 180.0))
+    return fail(r, BEAMS_ERR_INVALID_ARG, "camera: fov_y_deg must be in (0, 180)");
+  if (!finite3(cam->position) || !finite3(cam->look_at) || !finite3(cam->up))
+    return fail(r, BEAMS_ERR_INVALID_ARG, "camera: non-finite vector");
+  return BEAMS_OK;
+}
+
+// Key of the inputs a map depends on; a cached map is reused only on a match.
+static void map_key(const beams_renderer* r, MapKey& k) {
+  std::memset(&k, 0, sizeof(k));
+  k.volume_version = r->volume_version;
+  k.tf_version = r->tf_version;
+  for (int d = 0; d < 3; ++d) k.m[d] = r->map_m[d];
+  k.steps = r->light_steps;
+  k.form = r->form;
+  if (!r->lights.empty()) {
+    k.light_kind = r->lights[0].kind;
+    for (int d = 0; d < 3; ++d) k.light[d] = r->lights[0].v[d];
+  }
+}
+
+beams_status build_map(beams_renderer* r, const ExactGeo& g, int& launches, bool& built) {
+  built = false;
+  MapKey key;
+  map_key(r, key);
+  if (r->reuse_map && r->map_valid && std::memcmp(&key, &r->map_key, sizeof(key)) == 0) return BEAMS_OK;
+  const size_t nvert = (size_t)g.pd[0] * g.pd[1] * g.pd[2];
+  beams_status s = ensure_buffer(r, (void**)&r->d_map, &r->map_cap, nvert * sizeof(float), "allocating map");
+  if (s != BEAMS_OK) return s;
+  r->map_valid = false;
+  cudaError_t e = launch_light_march_f32(g, (const float*)r->d_field, r->d_tf, r->d_map, r->d_cnt, r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "light_march launch");
+  ++launches;
+  r->map_key = key;
+  r->map_valid = true;
+  r->map_count = nvert;
+  built = true;
+  return BEAMS_OK;
+}
+
+beams_status check_ready(beams_renderer* r) {
+  if (!r->has_volume) return fail(r, BEAMS_ERR_STATE, "no volume set (beams_set_volume)");
+  if (r->tf_n < 1) return fail(r, BEAMS_ERR_STATE, "no colour map set (beams_set_color_map)");
+  if (r->use_map && r->vol.assoc == BEAMS_ASSOC_POINTS && r->lights.empty())
+    return fail(r, BEAMS_ERR_STATE, "shadow map enabled but no light added");
+  if (r->form == BEAMS_FORM_EXACT && r->vol.dtype != BEAMS_F32)
+    return fail(r, BEAMS_ERR_UNSUPPORTED, "the exact form needs a float32 volume");
+  return BEAMS_OK;
+}
+
+}  // namespace beams
+
+using namespace beams;
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int beams_abi_version(void) { return BEAMS_ABI_VERSION; }
+
+const char* beams_last_error(const beams_renderer* r) {
+  return r ? r->err.c_str() : g_tls_error.c_str();
+}
+
+beams_status beams_create(beams_renderer** out, int device, void* stream) {
+  if (!out) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDeviceCount");
+  if (device < 0 || device >= ndev) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "device index out of range");
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaSetDevice");
+  beams_renderer* r = new beams_renderer();
+  r->device = device;
+  r->stream = (cudaStream_t)stream;
+  for (int i = 0; i < 4; ++i) {
+    e = cudaEventCreate(&r->ev[i]);
+    if (e != cudaSuccess) {
+      delete r;
+      return cuda_fail(nullptr, e, "cudaEventCreate");
+    }
+  }
+  e = cudaMalloc((void**)&r->d_cnt, sizeof(Counters));
+  if (e != cudaSuccess) {
+    delete r;
+    return cuda_fail(nullptr, e, "allocating counters");
+  }
+  e = cudaMemset(r->d_cnt, 0, sizeof(Counters));
+  if (e != cudaSuccess) {
+    delete r;
+    return cuda_fail(nullptr, e, "clearing counters");
+  }
+  *out = r;
+  return BEAMS_OK;
+}
+
+beams_status beams_destroy(beams_renderer* r) {
+  if (!r) return BEAMS_OK;
+  cudaSetDevice(r->device);
+  cudaStreamSynchronize(r->stream);
+  delete r;
+  return BEAMS_OK;
+}
+
+beams_status beams_set_volume(beams_renderer* r, const beams_volume* v) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  if (!v || !v->data) return fail(r, BEAMS_ERR_INVALID_ARG, "volume or volume data is NULL");
+  if (v->dtype != BEAMS_F32 && v->dtype != BEAMS_BF16 && v->dtype != BEAMS_F16)
+    return fail(r, BEAMS_ERR_INVALID_ARG, "volume dtype must be F32, BF16 or F16");
+  if (v->assoc != BEAMS_ASSOC_POINTS && v->assoc != BEAMS_ASSOC_CELLS)
+    return fail(r, BEAMS_ERR_INVALID_ARG, "volume assoc must be POINTS or CELLS");
+  for (int d = 0; d < 3; ++d) {
+    if (v->dims[d] < 2 || v->dims[d] > 8192)
+      return fail(r, BEAMS_ERR_INVALID_ARG, "volume dims must be in [2, 8192] (point dimensions)");
+    if (!(v->spacing[d] > 0.0) || !std::isfinite(v->spacing[d]) || !std::isfinite(v->origin[d]))
+      return fail(r, BEAMS_ERR_INVALID_ARG, "volume spacing must be positive and finite");
+  }
+  if (!std::isfinite(v->range[0]) || !std::isfinite(v->range[1]))
+    return fail(r, BEAMS_ERR_INVALID_ARG, "volume range must be finite");
+  cudaSetDevice(r->device);
+  const size_t elem = (v->dtype == BEAMS_F32) ? 4 : 2;
+  size_t count = (size_t)v->dims[0] * v->dims[1] * v->dims[2];
+  if (v->assoc == BEAMS_ASSOC_CELLS) count = (size_t)(v->dims[0] - 1) * (v->dims[1] - 1) * (v->dims[2] - 1);
+  const size_t bytes = count * elem;
+  if (v->on_device) {
+    r->d_field = v->data;
+  } else {
+    beams_status s = ensure_buffer(r, &r->d_field_owned, &r->field_cap, bytes, "allocating volume");
+    if (s != BEAMS_OK) return s;
+    cudaError_t e = cudaMemcpyAsync(r->d_field_owned, v->data, bytes, cudaMemcpyHostToDevice, r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "copying volume to device");
+    r->d_field = r->d_field_owned;
+  }
+  r->vol = *v;
+  r->vol.data = r->d_field;
+  r->vol.on_device = 1;
+  r->field_bytes = bytes;
+  r->has_volume = true;
+  ++r->volume_version;
+  return BEAMS_OK;
+}
+
+beams_status beams_set_color_map(beams_renderer* r, const float* rgba, int n) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  if (!rgba || n < 1 || n > 1024) return fail(r, BEAMS_ERR_INVALID_ARG, "colour map needs 1..1024 RGBA entries");
+  for (int i = 0; i < 4 * n; ++i)
+    if (!std::isfinite(rgba[i])) return fail(r, BEAMS_ERR_INVALID_ARG, "colour map has a non-finite entry");
+  cudaSetDevice(r->device);
+  r->tf.assign(rgba, rgba + 4 * n);
+  beams_status s = ensure_buffer(r, (void**)&r->d_tf, &r->tf_cap, sizeof(float) * 4 * 1024, "allocating colour map");
+  if (s != BEAMS_OK) return s;
+  cudaError_t e = cudaMemcpyAsync(r->d_tf, r->tf.data(), sizeof(float) * 4 * n, cudaMemcpyHostToDevice, r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "copying colour map");
+  r->tf_n = n;
+  ++r->tf_version;
+  return BEAMS_OK;
+}
+
+beams_status beams_set_shadow_map_size(beams_renderer* r, int mx, int my, int mz) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  if (mx < 1 || my < 1 || mz < 1 || mx > 2047 || my > 2047 || mz > 2047)
+    return fail(r, BEAMS_ERR_INVALID_ARG, "shadow map size must be in [1, 2047] cells per axis");
+  r->map_m[0] = mx;
+  r->map_m[1] = my;
+  r->map_m[2] = mz;
+  return BEAMS_OK;
+}
+
+beams_status beams_set_use_shadow_map(beams_renderer* r, int enable) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  r->use_map = enable != 0;
+  return BEAMS_OK;
+}
+
+beams_status beams_clear_lights(beams_renderer* r) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  r->lights.clear();
+  return BEAMS_OK;
+}
+
+static beams_status add_light(beams_renderer* r, int kind, const double v[3], const float color[3], float intensity) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  if (!v || !color || !finite3(v) || !std::isfinite(intensity) || !std::isfinite(color[0]) ||
+      !std::isfinite(color[1]) || !std::isfinite(color[2]))
+    return fail(r, BEAMS_ERR_INVALID_ARG, "light: non-finite or NULL argument");
+  if (kind == 1 && v[0] == 0.0 && v[1] == 0.0 && v[2] == 0.0)
+    return fail(r, BEAMS_ERR_INVALID_ARG, "directional light: zero direction");
+  Light L;
+  L.kind = kind;
+  for (int d = 0; d < 3; ++d) {
+    L.v[d] = v[d];
+    L.color[d] = color[d];
+  }
+  L.intensity = intensity;
+  r->lights.push_back(L);
+  return BEAMS_OK;
+}
+
+beams_status beams_add_point_light(beams_renderer* r, const double pos[3], const float color[3], float intensity) {
+  return add_light(r, 0, pos, color, intensity);
+}
+
+beams_status beams_add_directional_light(beams_renderer* r, const double dir[3], const float color[3],
+                                         float intensity) {
+  return add_light(r, 1, dir, color, intensity);
+}
+
+beams_status beams_set_sample_distance(beams_renderer* r, float d) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  if (!(d > 0.f) || !std::isfinite(d)) return fail(r, BEAMS_ERR_INVALID_ARG, "Sample distance must be positive.");
+  r->sample_distance = d;
+  return BEAMS_OK;
+}
+
+beams_status beams_set_termination_alpha(beams_renderer* r, float a) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  if (!(a > 0.f) || !std::isfinite(a)) return fail(r, BEAMS_ERR_INVALID_ARG, "termination alpha must be positive");
+  r->cutoff = a;
+  return BEAMS_OK;
+}
+
+beams_status beams_set_light_steps(beams_renderer* r, float steps) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  if (!(steps >= 1.f && steps <= 65536.f)) return fail(r, BEAMS_ERR_INVALID_ARG, "light steps must be in [1, 65536]");
+  r->light_steps = steps;
+  return BEAMS_OK;
+}
+
+beams_status beams_set_slab_fp64(beams_renderer* r, int enable) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  r->slab_fp64 = enable != 0;
+  return BEAMS_OK;
+}
+
+beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  r->reuse_map = enable != 0;
+  return BEAMS_OK;
+}
+
+beams_status beams_set_background(beams_renderer* r, int enable, const float rgba[4]) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  r->bg = enable != 0;
+  if (rgba)
+    for (int i = 0; i < 4; ++i) r->bg_rgba[i] = rgba[i];
+  return BEAMS_OK;
+}
+
+beams_status beams_set_form(beams_renderer* r, int form, const void* opts) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  (void)opts;
+  if (form != BEAMS_FORM_EXACT) return fail(r, BEAMS_ERR_UNSUPPORTED, "form not available in this build");
+  r->form = form;
+  return BEAMS_OK;
+}
+
+beams_status beams_build_shadow_map(beams_renderer* r, beams_timings* t) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  beams_status s = check_ready(r);
+  if (s != BEAMS_OK) return s;
+  if (r->lights.empty()) return fail(r, BEAMS_ERR_STATE, "no light added");
+  cudaSetDevice(r->device);
+  ExactGeo g;
+  s = make_geo(r, nullptr, g);
+  if (s != BEAMS_OK) return s;
+  cudaError_t e = cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "clearing counters");
+  cudaEventRecord(r->ev[0], r->stream);
+  int launches = 0;
+  bool built = false;
+  const bool keep = r->reuse_map;
+  r->reuse_map = false;
+  s = build_map(r, g, launches, built);
+  r->reuse_map = keep;
+  if (s != BEAMS_OK) return s;
+  cudaEventRecord(r->ev[1], r->stream);
+  if (t) {
+    std::memset(t, 0, sizeof(*t));
+    e = cudaStreamSynchronize(r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "light march");
+    Counters c;
+    e = cudaMemcpy(&c, r->d_cnt, sizeof(c), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(r, e, "reading counters");
+    cudaEventElapsedTime(&t->map_build_ms, r->ev[0], r->ev[1]);
+    t->total_ms = t->map_build_ms;
+    t->light_samples = c.light_samples;
+    t->map_vertices = built ? (int)r->map_count : 0;
+    t->kernel_launches = launches;
+  }
+  return BEAMS_OK;
+}
+
+beams_status beams_get_shadow_map(beams_renderer* r, float* dst, size_t count, int dst_on_device) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  if (!r->map_valid) return fail(r, BEAMS_ERR_STATE, "no map has been built");
+  if (!dst || count < r->map_count) return fail(r, BEAMS_ERR_INVALID_ARG, "destination too small for the map");
+  cudaSetDevice(r->device);
+  cudaError_t e = cudaMemcpyAsync(dst, r->d_map, r->map_count * sizeof(float),
+                                  dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, r->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "copying map");
+  return BEAMS_OK;
+}
+
+beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgba_out, int out_on_device,
+                          beams_timings* t) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  beams_status s = validate_camera(r, cam);
+  if (s != BEAMS_OK) return s;
+  if (!rgba_out) return fail(r, BEAMS_ERR_INVALID_ARG, "rgba_out is NULL");
+  s = check_ready(r);
+  if (s != BEAMS_OK) return s;
+  cudaSetDevice(r->device);
+  ExactGeo g;
+  s = make_geo(r, cam, g);
+  if (s != BEAMS_OK) return s;
+  int launches = 0;
+  cudaError_t e = cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "clearing counters");
+  cudaEventRecord(r->ev[0], r->stream);
+  bool built = false;
+  const bool need_map = r->use_map && r->vol.assoc == BEAMS_ASSOC_POINTS;
+  if (need_map) {
+    s = build_map(r, g, launches, built);
+    if (s != BEAMS_OK) return s;
+  }
+  cudaEventRecord(r->ev[1], r->stream);
+  const size_t npix = (size_t)cam->width * cam->height;
+  float4* dst = (float4*)rgba_out;
+  const bool direct = out_on_device && (((uintptr_t)rgba_out & 15) == 0);
+  if (!direct) {
+    s = ensure_buffer(r, (void**)&r->d_rgba, &r->rgba_cap, npix * sizeof(float4), "allocating image");
+    if (s != BEAMS_OK) return s;
+    dst = r->d_rgba;
+  }
+  e = launch_view_march_f32(g, (const float*)r->d_field, r->d_tf, need_map ? r->d_map : nullptr, dst, r->d_cnt,
+                            r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "view_march launch");
+  ++launches;
+  cudaEventRecord(r->ev[2], r->stream);
+  if (!direct) {
+    e = cudaMemcpyAsync(rgba_out, dst, npix * sizeof(float4),
+                        out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "copying image out");
+  }
+  cudaEventRecord(r->ev[3], r->stream);
+  if (t) {
+    std::memset(t, 0, sizeof(*t));
+    e = cudaStreamSynchronize(r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "render");
+    Counters c;
+    e = cudaMemcpy(&c, r->d_cnt, sizeof(c), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(r, e, "reading counters");
+    cudaEventElapsedTime(&t->map_build_ms, r->ev[0], r->ev[1]);
+    cudaEventElapsedTime(&t->view_march_ms, r->ev[1], r->ev[2]);
+    cudaEventElapsedTime(&t->composite_ms, r->ev[2], r->ev[3]);
+    cudaEventElapsedTime(&t->total_ms, r->ev[0], r->ev[3]);
+    t->light_samples = c.light_samples;
+    t->lit_samples = c.lit_samples;
+    t->rays_hit = c.rays_hit;
+    t->mlp_samples = c.mlp_samples;
+    t->map_vertices = built ? (int)r->map_count : 0;
+    t->kernel_launches = launches;
+  } else if (!out_on_device) {
+    // The caller reads rgba_out on return.
+    e = cudaStreamSynchronize(r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "render");
+  }
+  return BEAMS_OK;
+}
+
+beams_status beams_generate_blobs(float* dev_out, const int n[3], const float* params, int nblobs, int normalise,
+                                  void* stream) {
+  if (!dev_out || !n || !params || nblobs < 1 || nblobs > 4096)
+    return fail(nullptr, BEAMS_ERR_INVALID_ARG, "generate_blobs: bad argument");
+  if (n[0] < 2 || n[1] < 2 || n[2] < 2) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "generate_blobs: dims < 2");
+  cudaStream_t st = (cudaStream_t)stream;
+  float* d_prm = nullptr;
+  unsigned* d_mm = nullptr;
+  cudaError_t e = cudaMalloc((void**)&d_prm, sizeof(float) * 5 * nblobs);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d_mm, 2 * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_prm, params, sizeof(float) * 5 * nblobs, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = launch_generate_blobs(dev_out, n, d_prm, nblobs, st);
+  if (e == cudaSuccess && normalise)
+    e = launch_normalise01(dev_out, (int64_t)n[0] * n[1] * n[2], d_mm, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(d_prm);
+  cudaFree(d_mm);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "generate_blobs");
+  return BEAMS_OK;
+}
+
+beams_status beams_generate_noise(float* dev_out, const int n[3], const unsigned char* perm, int octaves,
+                                  float base_freq, float lacunarity, float gain, void* stream) {
+  if (!dev_out || !n || !perm || octaves < 1 || octaves > 16)
+    return fail(nullptr, BEAMS_ERR_INVALID_ARG, "generate_noise: bad argument");
+  if (n[0] < 2 || n[1] < 2 || n[2] < 2) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "generate_noise: dims < 2");
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned char* d_perm = nullptr;
+  unsigned* d_mm = nullptr;
+  cudaError_t e = cudaMalloc((void**)&d_perm, 256);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d_mm, 2 * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_perm, perm, 256, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = launch_generate_noise(dev_out, n, d_perm, octaves, base_freq, lacunarity, gain, st);
+  if (e == cudaSuccess) e = launch_normalise01(dev_out, (int64_t)n[0] * n[1] * n[2], d_mm, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(d_perm);
+  cudaFree(d_mm);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "generate_noise");
+  return BEAMS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,54 @@
+// beams_params.h — kernel parameter blocks, derived on the host from the scene
+// exactly as the reference derives them (float32 arithmetic, no contraction).
+#pragma once
+#include <stdint.h>
+
+namespace beams {
+
+// Everything the exact light and view marches need, passed by value.
+struct ExactGeo {
+  // Field grid. Rectilinear coordinates are generated, not stored:
+  // coord(d, i) = org[d] + h[d] * float(i), the float32 ArrayHandleCounting the
+  // reference scenes build (beams/sources/Spheres.cxx:144-156).
+  int n[3];
+  float org[3], h[3], invh[3];  // invh only seeds the cell search
+  float minp[3], maxp[3];       // coord(d,0), coord(d,n-1)
+  double bmin[3], bmax[3];      // vtkm::Bounds of the coordinates (double)
+  float min_scalar, inv_delta;  // LightedVolumeRenderer.cxx:331-334
+  // Transfer function (RGBA table in global memory, staged to shared memory).
+  int tf_n;
+  float max_alpha;              // TransmittanceMap.h:515-525
+  // Map grid: (M+1)^3 vertices over the field bounds (TransmittanceMap.h:550-563).
+  int pd[3];
+  float morig[3], msp[3], minv[3];
+  float light_color[3];         // Color * Intensity (LightedVolumeRenderer.cxx:840)
+  float extent_mag;             // BoundsMagnitude (beams/Math.h:13-21)
+  float sd;                     // view sample distance
+  float mesh_eps;               // |extent| * 1e-4 (LightedVolumeRenderer.cxx:1261)
+  float step;                   // light step |extent| / steps (TransmittanceMap.h:584-585)
+  float cutoff;                 // early-termination alpha
+  int light_kind;               // 0 point, 1 directional
+  float light[3];               // position, or normalised travel direction
+  float dir_dist;               // directional light: per-vertex origin distance
+  int light_budget;             // iteration cap of one light ray
+  // Camera (pinhole, pixel centres).
+  float cam_pos[3], cf[3], cr[3], cu[3];
+  float kx, cx, ky, cy;
+  int width, height;
+  int slab_fp64;
+  int use_map;
+  int assoc_cells;
+};
+
+// Counters written by the kernels (one atomic per warp).
+struct Counters {
+  unsigned long long light_samples;
+  unsigned long long lit_samples;
+  unsigned long long rays_hit;
+  unsigned long long mlp_samples;
+  unsigned long long fallback_tiles;
+  unsigned long long errors;
+  unsigned long long pad[2];
+};
+
+}  // namespace beams

@@ -1,0 +1,235 @@
+// exact_device.cuh — device restatement of the reference's per-sample math.
+//
+// Every translation unit that includes this header is compiled with
+// -fmad=false: a*b+c stays two IEEE roundings, as in the reference's x86-64
+// build, and the explicit fmaf() calls below are the only fused operations
+// (lcl's lerp uses std::fma). Division and sqrtf are IEEE (no fast-math).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "beams_params.h"
+
+namespace beams {
+
+// vtkm::Min / vtkm::Max on the host are std::min / std::max.
+template <typename T> __device__ __forceinline__ T mn(T a, T b) { return (b < a) ? b : a; }
+template <typename T> __device__ __forceinline__ T mx(T a, T b) { return (a < b) ? b : a; }
+__device__ __forceinline__ float clamp01(float x) { return x < 0.f ? 0.f : (x > 1.f ? 1.f : x); }
+
+// lcl::internal::lerp(a, b, t) = fma(t, b, fma(-t, a, a)).
+__device__ __forceinline__ float lerp_lcl(float a, float b, float t) {
+  return fmaf(t, b, fmaf(-t, a, a));
+}
+
+// vtkm::exec::CellInterpolate on a hexahedron (lcl trilinear, VTK corner order).
+__device__ __forceinline__ float hex_interp(const float v[8], float px, float py, float pz) {
+  const float vbf = lerp_lcl(v[0], v[1], px);
+  const float vbb = lerp_lcl(v[3], v[2], px);
+  const float vtf = lerp_lcl(v[4], v[5], px);
+  const float vtb = lerp_lcl(v[7], v[6], px);
+  const float vb = lerp_lcl(vbf, vbb, py);
+  const float vt = lerp_lcl(vtf, vtb, py);
+  return lerp_lcl(vb, vt, pz);
+}
+
+// Rectilinear coordinate i on axis d (float32 counting array).
+__device__ __forceinline__ float coord(const ExactGeo& g, int d, int i) {
+  return g.org[d] + g.h[d] * (float)i;
+}
+
+__device__ __forceinline__ float vtx_coord(const ExactGeo& g, int d, int i) {
+  return g.morig[d] + g.msp[d] * (float)i;
+}
+
+// Field loads. The exact form reads float32; the precision form reads 16-bit.
+template <typename FieldT> struct FieldLoad;
+template <> struct FieldLoad<float> {
+  static __device__ __forceinline__ float ld(const float* __restrict__ f, int64_t i) { return __ldg(f + i); }
+};
+
+// SegmentAABB (Intersections.cxx:9-48). The slab ratios are formed in double
+// because vtkm::Bounds holds doubles, then stored to float.
+__device__ __forceinline__ void segment_aabb(const ExactGeo& g, const float a[3], const float b[3],
+                                             float& tmin, float& tmax) {
+  float dir[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+  const float len = sqrtf(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+  dir[0] = dir[0] / len;
+  dir[1] = dir[1] / len;
+  dir[2] = dir[2] / len;
+  tmin = 0.f;
+  tmax = __int_as_float(0x7f800000);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float t0 = (float)((g.bmin[d] - (double)a[d]) / (double)dir[d]);
+    const float t1 = (float)((g.bmax[d] - (double)a[d]) / (double)dir[d]);
+    tmin = mx(tmin, mn(t0, t1));
+    tmax = mn(tmax, mx(t0, t1));
+  }
+  if (tmin < 0.f) tmin = 1e-4f;
+  if (tmax > len) tmax = len;
+}
+
+// Map vertex position (uniform point coordinates of the opacity map).
+__device__ __forceinline__ void map_vertex(const ExactGeo& g, int64_t id, float V[3]) {
+  const int64_t px = g.pd[0], pxy = (int64_t)g.pd[0] * g.pd[1];
+  const int64_t k = id / pxy;
+  const int64_t r = id - k * pxy;
+  const int64_t j = r / px;
+  const int64_t i = r - j * px;
+  V[0] = vtx_coord(g, 0, (int)i);
+  V[1] = vtx_coord(g, 1, (int)j);
+  V[2] = vtx_coord(g, 2, (int)k);
+}
+
+__device__ __forceinline__ void light_origin(const ExactGeo& g, const float V[3], float L[3]) {
+  if (g.light_kind == 0) {
+    L[0] = g.light[0];
+    L[1] = g.light[1];
+    L[2] = g.light[2];
+  } else {
+    L[0] = V[0] - g.light[0] * g.dir_dist;
+    L[1] = V[1] - g.light[1] * g.dir_dist;
+    L[2] = V[2] - g.light[2] * g.dir_dist;
+  }
+}
+
+// Light-march cell search: RectilinearMeshOracle's binary search
+// (RectilinearMeshOracle.h:154-176) returns the smallest cell c with
+// val <= coord(c+1). A seeded guess plus a bounded fix-up finds the same cell.
+__device__ __forceinline__ int find_cell_bsearch(const ExactGeo& g, int d, float val) {
+  const int cmax = g.n[d] - 2;
+  int c = (int)((val - g.org[d]) * g.invh[d]);
+  c = c < 0 ? 0 : (c > cmax ? cmax : c);
+  for (int it = 0; it < 4 && c > 0 && val <= coord(g, d, c); ++it) --c;
+  for (int it = 0; it < 4 && c < cmax && val > coord(g, d, c + 1); ++it) ++c;
+  // The seed is within one cell of the answer; these loops only run when the
+  // spacing is not uniform enough for that (never for counting coordinates).
+  while (c > 0 && val <= coord(g, d, c)) --c;
+  while (c < cmax && val > coord(g, d, c + 1)) ++c;
+  return c;
+}
+
+// View-march cell search: RectilinearLocator::LocateCell (LightedVolumeRenderer.cxx:119-165)
+// walks to the unique cell with coord(c) <= p < coord(c+1).
+__device__ __forceinline__ int find_cell_walk(const ExactGeo& g, int d, float p) {
+  const int cmax = g.n[d] - 2;
+  int c = (int)((p - g.org[d]) * g.invh[d]);
+  c = c < 0 ? 0 : (c > cmax ? cmax : c);
+  for (int it = 0; it < 4 && c > 0 && p < coord(g, d, c); ++it) --c;
+  for (int it = 0; it < 4 && c < cmax && p >= coord(g, d, c + 1); ++it) ++c;
+  while (c > 0 && p < coord(g, d, c)) --c;
+  while (c < cmax && p >= coord(g, d, c + 1)) ++c;
+  return c;
+}
+
+// TF index of the light march (TransmittanceMap.h:322-326), saturating.
+__device__ __forceinline__ int tf_index_clamped(float fi, int n1) {
+  if (fi > -1.f && fi < (float)(n1 + 1)) {
+    int idx = (int)fi;
+    return idx < 0 ? 0 : (idx > n1 ? n1 : idx);
+  }
+  return (fi >= (float)(n1 + 1)) ? n1 : 0;
+}
+
+// Pinhole camera ray through pixel centre (x, y).
+__device__ __forceinline__ void camera_ray(const ExactGeo& g, int x, int y, float o[3], float d[3]) {
+  const float sx = ((float)x + 0.5f) * g.kx - g.cx;
+  const float sy = ((float)y + 0.5f) * g.ky - g.cy;
+  float v[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) v[k] = (g.cf[k] + sx * g.cr[k]) + sy * g.cu[k];
+  const float len = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    d[k] = v[k] / len;
+    o[k] = g.cam_pos[k];
+  }
+}
+
+// CalcRayStart (LightedVolumeRenderer.cxx:644-718) in S = float (the reference)
+// or S = double (t_enter/t_exit set up in FP64, then rounded to float).
+template <typename S>
+__device__ __forceinline__ bool slab_t(const S o[3], const S d[3], const double bmin[3],
+                                       const double bmax[3], S& minD, S& maxD) {
+  S lo[3], hi[3];
+  const S eps = (sizeof(S) == 4) ? (S)1e-8f : (S)1e-8;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const S inv = S(1) / ((fabs(d[k]) < eps) ? eps : d[k]);
+    const S od = o[k] * inv;
+    lo[k] = (S)bmin[k] * inv - od;
+    hi[k] = (S)bmax[k] * inv - od;
+  }
+  minD = mx(mx(mx(mn(lo[1], hi[1]), mn(lo[0], hi[0])), mn(lo[2], hi[2])), minD);
+  const S exitD = mn(mn(mx(lo[1], hi[1]), mx(lo[0], hi[0])), mx(lo[2], hi[2]));
+  maxD = mn(maxD, exitD);
+  return !(maxD < minD);
+}
+
+__device__ __forceinline__ bool ray_setup(const ExactGeo& g, int x, int y, float o[3], float d[3],
+                                          float& minD, float& maxD) {
+  camera_ray(g, x, y, o, d);
+  if (g.slab_fp64) {
+    const double od[3] = {(double)o[0], (double)o[1], (double)o[2]};
+    const double dd[3] = {(double)d[0], (double)d[1], (double)d[2]};
+    double lo = 0.0, hi = __longlong_as_double(0x7ff0000000000000ull);
+    const bool hit = slab_t<double>(od, dd, g.bmin, g.bmax, lo, hi);
+    minD = (float)lo;
+    maxD = (float)hi;
+    return hit;
+  }
+  minD = 0.f;
+  maxD = __int_as_float(0x7f800000);
+  return slab_t<float>(o, d, g.bmin, g.bmax, minD, maxD);
+}
+
+__device__ __forceinline__ bool inside_vol(const ExactGeo& g, const float p[3]) {
+  return !(p[0] < g.minp[0] || p[0] > g.maxp[0] || p[1] < g.minp[1] || p[1] > g.maxp[1] ||
+           p[2] < g.minp[2] || p[2] > g.maxp[2]);
+}
+
+// TransmittanceLocator::LocateCell + GetEstimateUsingVerticesT
+// (TransmittanceMap.h:93-112, :200-229): map opacity at p.
+template <typename MapT>
+__device__ __forceinline__ float map_opacity(const ExactGeo& g, const MapT* __restrict__ map,
+                                             const float p[3]);
+
+template <>
+__device__ __forceinline__ float map_opacity<float>(const ExactGeo& g, const float* __restrict__ map,
+                                                    const float p[3]) {
+  int c[3];
+  float pc[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    float t = (p[d] - g.morig[d]) * g.minv[d];
+    if (t < 0.f) t = 0.f;
+    if (t >= (float)(g.pd[d] - 1)) t = (float)(g.pd[d] - 2);
+    c[d] = (int)t;
+    const float lo = vtx_coord(g, d, c[d]);
+    const float hi = vtx_coord(g, d, c[d] + 1);
+    pc[d] = (p[d] - lo) / (hi - lo);
+  }
+  const int64_t px = g.pd[0], pxy = (int64_t)g.pd[0] * g.pd[1];
+  const int64_t i0 = (int64_t)c[2] * pxy + (int64_t)c[1] * px + c[0];
+  float v[8];
+  v[0] = __ldg(map + i0);
+  v[1] = __ldg(map + i0 + 1);
+  v[2] = __ldg(map + i0 + 1 + px);
+  v[3] = __ldg(map + i0 + px);
+  v[4] = __ldg(map + i0 + pxy);
+  v[5] = __ldg(map + i0 + pxy + 1);
+  v[6] = __ldg(map + i0 + pxy + 1 + px);
+  v[7] = __ldg(map + i0 + pxy + px);
+  return hex_interp(v, pc[0], pc[1], pc[2]);
+}
+
+// Warp-aggregated counter increment (one atomic per warp). Must be reached by
+// all 32 lanes of the warp (kernels keep out-of-range lanes alive with v = 0);
+// blocks are one-dimensional.
+__device__ __forceinline__ void warp_add(unsigned long long* dst, unsigned v) {
+  const unsigned s = __reduce_add_sync(0xffffffffu, v);
+  if ((threadIdx.x & 31) == 0 && s) atomicAdd(dst, (unsigned long long)s);
+}
+
+}  // namespace beams

@@ -1,0 +1,99 @@
+// renderer.h — the opaque beams_renderer behind the C ABI.
+//
+// Mirrors the state of MapperLightedVolume::InternalsType
+// (beams/rendering/MapperLightedVolume.cxx:27-45) and LightedVolumeRenderer
+// (beams/rendering/LightedVolumeRenderer.h:231-261), with device buffers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/beams_b200.h"
+#include "beams_params.h"
+
+namespace beams {
+
+struct Light {
+  int kind = 0;  // 0 point, 1 directional
+  double v[3] = {0, 0, 0};
+  float color[3] = {1, 1, 1};
+  float intensity = 1.f;
+};
+
+struct MapKey {
+  unsigned long long volume_version;
+  unsigned long long tf_version;
+  int m[3];
+  float steps;
+  int form;
+  int light_kind;
+  double light[3];
+};
+
+}  // namespace beams
+
+struct beams_renderer {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  // volume (SetData)
+  bool has_volume = false;
+  beams_volume vol{};
+  void* d_field_owned = nullptr;
+  size_t field_cap = 0;
+  const void* d_field = nullptr;
+  size_t field_bytes = 0;
+  unsigned long long volume_version = 0;
+
+  // colour map (SetColorMap)
+  std::vector<float> tf;
+  float4* d_tf = nullptr;
+  size_t tf_cap = 0;
+  int tf_n = 0;
+  unsigned long long tf_version = 0;
+
+  // lights, map and march settings; defaults are the reference's
+  // (LightedVolumeRenderer.cxx:752-759: shadow map on, 16^3, sample distance -1).
+  std::vector<beams::Light> lights;
+  int map_m[3] = {16, 16, 16};
+  bool use_map = true;
+  float sample_distance = -1.f;
+  float cutoff = 1.f;
+  float light_steps = 128.f;
+  int slab_fp64 = 1;
+  bool reuse_map = false;
+  bool bg = false;
+  float bg_rgba[4] = {1.f, 1.f, 1.f, 1.f};
+  int form = BEAMS_FORM_EXACT;
+
+  // transmittance map
+  float* d_map = nullptr;
+  size_t map_cap = 0;
+  size_t map_count = 0;
+  bool map_valid = false;
+  beams::MapKey map_key{};
+
+  // image + counters + timing
+  float4* d_rgba = nullptr;
+  size_t rgba_cap = 0;
+  beams::Counters* d_cnt = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+  ~beams_renderer() {
+    if (d_field_owned) cudaFree(d_field_owned);
+    if (d_tf) cudaFree(d_tf);
+    if (d_map) cudaFree(d_map);
+    if (d_rgba) cudaFree(d_rgba);
+    if (d_cnt) cudaFree(d_cnt);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
+namespace beams {
+beams_status fail(beams_renderer* r, beams_status s, const std::string& msg);
+beams_status cuda_fail(beams_renderer* r, cudaError_t e, const char* what);
+beams_status ensure_buffer(beams_renderer* r, void** buf, size_t* cap, size_t bytes, const char* what);
+}  // namespace beams

@@ -1,0 +1,161 @@
+"""Known-answer tests of the CPU oracle (no GPU).
+
+The reference ships no tests or golden data, so these closed forms pin the
+reference behaviours the oracle restates:
+  * light march advances before it samples, composites o += (1-o)a with
+    a = TF alpha / max alpha (TransmittanceMap.h:299-331);
+  * view march premultiplies c.a by (1 - C.a) and accumulates C.a += c.a
+    (LightedVolumeRenderer.cxx:464-481), so a constant field gives
+    C.a = 1 - (1-a)^k after k samples;
+  * the slab test returns the analytic entry/exit (LightedVolumeRenderer.cxx:644-718);
+  * the TF index truncates (LightedVolumeRenderer.cxx:453-454).
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle, composite, psnr
+from pilot_b200 import scenes
+
+
+def const_scene(value=0.45, n=16, m=8, light=(0.013, 0.021, 1.0), image=16, cutoff=1e9, use_map=True):
+    s = scenes.small(0, n=n, image=image, m=m, light_kind=1, cutoff=1.0)
+    s.light = light
+    s.cutoff = cutoff
+    s.use_map = use_map
+    s.array = np.full((n, n, n), value, np.float32)
+    return s
+
+
+def tf_alpha(s, value):
+    idx = int(np.float32(value) * np.float32(s.tf.shape[0] - 1))
+    return float(s.tf[idx, 3]), float(s.tf[:, 3].max())
+
+
+def test_light_march_constant_field_closed_form():
+    s = const_scene()
+    o = Oracle(s)
+    m, ns = o.light_march(fp64=True)
+    a, amax = tf_alpha(s, 0.45)
+    an = a / amax
+    assert ns > 0
+    # every vertex value is 1 - (1 - a/maxa)^k for an integer k >= 0
+    k = np.log1p(-m) / np.log1p(-an)
+    assert np.allclose(k, np.round(k), atol=1e-6), "map values are not whole powers of (1 - a)"
+    # nearly +z light: k grows with z (samples from the entry face to the vertex)
+    kz = np.round(k).mean(axis=(1, 2))
+    assert np.all(np.diff(kz) >= 0) and kz[-1] > kz[0]
+    # advance-then-sample: a vertex at depth z gets floor(z/step)+1 samples while the
+    # next position is still inside (z axis, light along +z)
+    ext = np.sqrt(3.0)
+    step = ext / 128
+    z = np.arange(s.map_m + 1) / s.map_m
+    expect = np.minimum(np.floor(z / step) + 1, np.floor(1.0 / step))
+    interior = np.round(k)[:, s.map_m // 2, s.map_m // 2]
+    assert np.max(np.abs(interior - expect)) <= 1
+
+
+def test_view_march_constant_field_alpha_is_whole_power():
+    s = const_scene(use_map=False, image=12)
+    o = Oracle(s)
+    img, lit = o.view_march(None, fp64=True)
+    a, _ = tf_alpha(s, 0.45)
+    alpha = img[..., 3]
+    assert lit > 0 and np.all(alpha > 0)
+    k = np.log1p(-alpha) / np.log1p(-a)
+    assert np.allclose(k, np.round(k), atol=1e-6)
+    # premultiplied colour: rgb = tf_rgb * alpha with no shadowing
+    idx = int(np.float32(0.45) * np.float32(255))
+    assert np.allclose(img[..., :3], s.tf[idx, :3][None, None, :] * alpha[..., None], atol=1e-9)
+
+
+def test_empty_transfer_function_renders_nothing():
+    s = scenes.small(1, n=16, image=16, m=6)
+    s.tf = s.tf.copy()
+    s.tf[:, 3] = 0
+    o = Oracle(s)
+    m, _ = o.light_march()
+    img, _ = o.view_march(m)
+    assert np.all(m == 0)
+    assert np.all(img == 0)
+
+
+def test_slab_analytic_entry_exit():
+    s = scenes.small(0, n=16, image=9, m=4)
+    s.cam_pos, s.cam_look, s.cam_up = (0.5, 0.5, 2.0), (0.5, 0.5, 0.5), (0.0, 1.0, 0.0)
+    for fp64 in (True, False):
+        s.slab_fp64 = fp64
+        o = Oracle(s)
+        r = o.ray_setup(4, 4)  # centre pixel of a 9x9 image looks straight down -z
+        assert np.allclose(r[3:6], [0, 0, -1], atol=1e-7)
+        assert abs(r[6] - 1.0) < 1e-6 and abs(r[7] - 2.0) < 1e-6
+    # a ray that misses the box is flagged with t_enter = -1
+    s.cam_look = (5.0, 5.0, 2.0 - 1e-3)
+    s.cam_up = (0.0, 0.0, 1.0)
+    o = Oracle(s)
+    assert o.ray_setup(4, 4)[6] == -1.0
+
+
+def test_single_opaque_block_casts_shadow_column():
+    n, m = 24, 12
+    f = np.zeros((n, n, n), np.float32)
+    f[8:16, 8:16, 8:16] = 1.0  # opaque cube in the middle
+    s = scenes.small(0, n=n, image=16, m=m, light_kind=1)
+    s.light = (0.0, 0.0, 1.0)  # light travels along +z
+    s.array = f
+    o = Oracle(s)
+    mp, _ = o.light_march(fp64=True)
+    c = m // 2
+    assert mp[m, c, c] > 0.99          # behind the block (far z face) is dark
+    assert mp[0, c, c] == 0.0          # the entry face sees the light
+    assert mp[m, 0, 0] < 1e-6          # outside the shadow column
+    assert mp[m, c, 1] < mp[m, c, c]
+
+
+def test_truncating_tf_index():
+    # 0.7 * 255 = 178.5 -> index 178 (truncation, not rounding)
+    s = const_scene(value=0.7, use_map=False, image=4)
+    tf = np.zeros_like(s.tf)
+    tf[178] = (1, 0, 0, 0.5)
+    tf[179] = (0, 1, 0, 0.5)
+    s.tf = tf
+    img, _ = Oracle(s).view_march(None, fp64=True)
+    assert np.all(img[..., 0] > 0) and np.all(img[..., 1] == 0)
+
+
+def test_fp32_mode_tracks_fp64():
+    s = scenes.small(2, n=24, image=40, m=12)
+    o = Oracle(s)
+    m32, _ = o.light_march()
+    m64, _ = o.light_march(fp64=True)
+    assert np.max(np.abs(m32 - m64)) < 1e-3
+    i32, l32 = o.view_march(m32)
+    i64, l64 = o.view_march(m64, fp64=True)
+    assert psnr(i32, i64) > 60
+    assert abs(l32 - l64) <= 0.01 * l64
+
+
+def test_directional_light_matches_far_point_light():
+    s = scenes.small(3, n=20, image=8, m=8, light_kind=1)
+    d = np.array(s.light) / np.linalg.norm(s.light)
+    mdir, _ = Oracle(s).light_march(fp64=True)
+    far = np.array([0.5, 0.5, 0.5]) - d * 1e4 * np.sqrt(3)
+    s.light_kind, s.light = 0, tuple(far)
+    mpt, _ = Oracle(s).light_march(fp64=True)
+    # sample positions differ (per-vertex origin vs one far origin): compare loosely
+    assert np.mean(np.abs(mdir - mpt)) < 0.02
+
+
+def test_composite_over_order():
+    a = np.array([[[0.5, 0, 0, 0.5]]], np.float32)
+    b = np.array([[[0, 0.8, 0, 0.8]]], np.float32)
+    out = composite(np.stack([a, b]), [0, 1])
+    assert np.allclose(out[0, 0], [0.5, 0.4, 0, 0.9])
+    out2 = composite(np.stack([a, b]), [1, 0])
+    assert np.allclose(out2[0, 0], [0.1, 0.8, 0, 0.9])
+
+
+def test_oracle_rejects_bad_scene():
+    s = scenes.small(0, n=16, image=8, m=4)
+    s.light_steps = 0
+    with pytest.raises(RuntimeError):
+        Oracle(s).light_march()

@@ -259,6 +259,7 @@ def run_ours(args):
     out = torch.empty((s.height, s.width, 4), dtype=torch.float32, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda") if args.config != 1 else None
 
+    r.render(cam, out=out, timings=True)                  # builds the cell tables and quad field
     _, t0 = r.render(cam, out=out, timings=True)          # counts for one frame (deterministic)
     lit_frame, light_frame = t0["lit_samples"], t0["light_samples"]
     launches_per_frame = t0["kernel_launches"]

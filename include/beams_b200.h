@@ -161,6 +161,14 @@ beams_status beams_get_shadow_map(beams_renderer* r, float* dst, size_t count, i
 /* Builds the map only (Phase 1), without a view march. */
 beams_status beams_build_shadow_map(beams_renderer* r, beams_timings* t);
 
+/* ---- diagnostics ------------------------------------------------------------ */
+/* Checks, on the device, the kernels' correctly rounded division (Markstein's
+ * correction on a tabulated reciprocal) against IEEE division for every cell
+ * width of the counting coordinates origin + i*spacing (ncells cells) and
+ * `samples` numerators per width. No reference counterpart (test support). */
+beams_status beams_selftest_division(float origin, float spacing, int ncells, int samples,
+                                     unsigned long long* checked, unsigned long long* mismatches);
+
 /* ---- scene generation (synthetic inputs; device-side) ----------------------- */
 /* Fills a float32 field (x fastest, n[0]*n[1]*n[2] values) on the device with a sum
  * of Gaussian blobs: params = nblobs x {cx, cy, cz, sigma, amplitude} in domain

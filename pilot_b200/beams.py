@@ -89,6 +89,8 @@ def lib():
         "beams_get_shadow_map": ([P, P, C.c_size_t, C.c_int], C.c_int),
         "beams_build_shadow_map": ([P, C.POINTER(Timings)], C.c_int),
         "beams_generate_blobs": ([P, P, P, C.c_int, C.c_int, P], C.c_int),
+        "beams_selftest_division": ([C.c_float, C.c_float, C.c_int, C.c_int, C.POINTER(C.c_ulonglong),
+                                     C.POINTER(C.c_ulonglong)], C.c_int),
         "beams_generate_noise": ([P, P, P, C.c_int, C.c_float, C.c_float, C.c_float, P], C.c_int),
     }
     for name, (args, res) in sig.items():
@@ -255,6 +257,16 @@ class Renderer:
         m = np.empty(count, np.float32)
         self._check(self._L.beams_get_shadow_map(self._h, _ptr(m), m.size, 0))
         return m
+
+
+def selftest_division(origin: float, spacing: float, ncells: int, samples: int):
+    """(checked, mismatches) of the kernels' division against IEEE division."""
+    L = lib()
+    chk, bad = C.c_ulonglong(), C.c_ulonglong()
+    st = L.beams_selftest_division(origin, spacing, ncells, samples, C.byref(chk), C.byref(bad))
+    if st != BEAMS_OK:
+        raise BeamsError(st, L.beams_last_error(None).decode())
+    return chk.value, bad.value
 
 
 class MapperLightedVolume:

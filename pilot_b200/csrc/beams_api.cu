@@ -95,6 +95,9 @@ beams_status make_geo(beams_renderer* r, const beams_camera* cam, ExactGeo& g) {
     g.minv[d] = 1.f / g.msp[d];
   }
   g.sd = (r->sample_distance > 0.f) ? r->sample_distance : g.extent_mag / 200.f;
+  // Bounds every view ray's iteration count (and so the kernel's run time).
+  if (!(g.extent_mag / g.sd <= 1.0e6f))
+    return fail(r, BEAMS_ERR_INVALID_ARG, "sample distance is below 1e-6 of the volume diagonal");
   g.mesh_eps = g.extent_mag * 0.0001f;
   g.step = g.extent_mag / r->light_steps;
   g.cutoff = r->cutoff;
@@ -111,6 +114,16 @@ beams_status make_geo(beams_renderer* r, const beams_camera* cam, ExactGeo& g) {
       for (int d = 0; d < 3; ++d) g.light[d] = (float)(L.v[d] / len);
     }
   }
+  int off = 0;
+  for (int d = 0; d < 3; ++d) {
+    g.ax_off[d] = off;
+    off += g.n[d] - 1;
+  }
+  for (int d = 0; d < 3; ++d) {
+    g.max_off[d] = off;
+    off += r->map_m[d];
+  }
+  g.ntab = off;
   g.slab_fp64 = r->slab_fp64;
   g.use_map = r->use_map ? 1 : 0;
   g.assoc_cells = (v.assoc == BEAMS_ASSOC_CELLS) ? 1 : 0;
@@ -172,6 +185,33 @@ static void map_key(const beams_renderer* r, MapKey& k) {
   }
 }
 
+// Builds the derived layouts the kernels read: cell tables (per frame geometry)
+// and, for point fields, the 4-corner quad copy of the field.
+beams_status prepare_layouts(beams_renderer* r, const ExactGeo& g, int& launches) {
+  const unsigned long long key[4] = {r->volume_version, (unsigned long long)r->map_m[0],
+                                     (unsigned long long)r->map_m[1], (unsigned long long)r->map_m[2]};
+  if (std::memcmp(key, r->tab_key, sizeof(key)) != 0) {
+    beams_status s = ensure_buffer(r, (void**)&r->d_tab, &r->tab_cap, (size_t)g.ntab * sizeof(float4),
+                                   "allocating cell tables");
+    if (s != BEAMS_OK) return s;
+    cudaError_t e = launch_build_tables(g, r->d_tab, r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "cell table build");
+    ++launches;
+    std::memcpy(r->tab_key, key, sizeof(key));
+  }
+  if (r->vol.assoc == BEAMS_ASSOC_POINTS && r->quads_version != r->volume_version) {
+    const size_t nq = (size_t)(g.n[0] - 1) * (g.n[1] - 1) * g.n[2];
+    beams_status s = ensure_buffer(r, (void**)&r->d_quads, &r->quads_cap, nq * sizeof(float4),
+                                   "allocating quad field");
+    if (s != BEAMS_OK) return s;
+    cudaError_t e = launch_build_quads((const float*)r->d_field, r->d_quads, g.n, r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "quad field build");
+    ++launches;
+    r->quads_version = r->volume_version;
+  }
+  return BEAMS_OK;
+}
+
 beams_status build_map(beams_renderer* r, const ExactGeo& g, int& launches, bool& built) {
   built = false;
   MapKey key;
@@ -181,7 +221,7 @@ beams_status build_map(beams_renderer* r, const ExactGeo& g, int& launches, bool
   beams_status s = ensure_buffer(r, (void**)&r->d_map, &r->map_cap, nvert * sizeof(float), "allocating map");
   if (s != BEAMS_OK) return s;
   r->map_valid = false;
-  cudaError_t e = launch_light_march_f32(g, (const float*)r->d_field, r->d_tf, r->d_map, r->d_cnt, r->stream);
+  cudaError_t e = launch_light_march_f32(g, r->d_quads, r->d_tab, r->d_tf, r->d_map, r->d_cnt, r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "light_march launch");
   ++launches;
   r->map_key = key;
@@ -198,6 +238,13 @@ beams_status check_ready(beams_renderer* r) {
     return fail(r, BEAMS_ERR_STATE, "shadow map enabled but no light added");
   if (r->form == BEAMS_FORM_EXACT && r->vol.dtype != BEAMS_F32)
     return fail(r, BEAMS_ERR_UNSUPPORTED, "the exact form needs a float32 volume");
+  const double nq = (double)(r->vol.dims[0] - 1) * (r->vol.dims[1] - 1) * r->vol.dims[2];
+  if (nq >= 4294967296.0) return fail(r, BEAMS_ERR_UNSUPPORTED, "volume too large for 32-bit cell indexing");
+  const double nv = (double)(r->map_m[0] + 1) * (r->map_m[1] + 1) * (r->map_m[2] + 1);
+  if (nv >= 2147483648.0) return fail(r, BEAMS_ERR_UNSUPPORTED, "shadow map too large (vertices >= 2^31)");
+  const int ntab = r->vol.dims[0] + r->vol.dims[1] + r->vol.dims[2] - 3 + r->map_m[0] + r->map_m[1] + r->map_m[2];
+  if ((size_t)(ntab + 1024) * 16 > 200 * 1024)
+    return fail(r, BEAMS_ERR_UNSUPPORTED, "volume/map axes too long for the shared-memory cell tables");
   return BEAMS_OK;
 }
 
@@ -421,6 +468,8 @@ beams_status beams_build_shadow_map(beams_renderer* r, beams_timings* t) {
   cudaEventRecord(r->ev[0], r->stream);
   int launches = 0;
   bool built = false;
+  s = prepare_layouts(r, g, launches);
+  if (s != BEAMS_OK) return s;
   const bool keep = r->reuse_map;
   r->reuse_map = false;
   s = build_map(r, g, launches, built);
@@ -472,6 +521,8 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
   if (e != cudaSuccess) return cuda_fail(r, e, "clearing counters");
   cudaEventRecord(r->ev[0], r->stream);
   bool built = false;
+  s = prepare_layouts(r, g, launches);
+  if (s != BEAMS_OK) return s;
   const bool need_map = r->use_map && r->vol.assoc == BEAMS_ASSOC_POINTS;
   if (need_map) {
     s = build_map(r, g, launches, built);
@@ -486,8 +537,8 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
     if (s != BEAMS_OK) return s;
     dst = r->d_rgba;
   }
-  e = launch_view_march_f32(g, (const float*)r->d_field, r->d_tf, need_map ? r->d_map : nullptr, dst, r->d_cnt,
-                            r->stream);
+  e = launch_view_march_f32(g, (const float*)r->d_field, r->d_quads, r->d_tab, r->d_tf, need_map ? r->d_map : nullptr,
+                            dst, r->d_cnt, r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "view_march launch");
   ++launches;
   cudaEventRecord(r->ev[2], r->stream);
@@ -519,6 +570,23 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
     e = cudaStreamSynchronize(r->stream);
     if (e != cudaSuccess) return cuda_fail(r, e, "render");
   }
+  return BEAMS_OK;
+}
+
+beams_status beams_selftest_division(float origin, float spacing, int ncells, int samples,
+                                     unsigned long long* checked, unsigned long long* mismatches) {
+  if (ncells < 1 || samples < 4 || !checked || !mismatches || !(spacing > 0.f))
+    return fail(nullptr, BEAMS_ERR_INVALID_ARG, "selftest_division: bad argument");
+  unsigned long long* d = nullptr;
+  cudaError_t e = cudaMalloc((void**)&d, 2 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(d, 0, 2 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = launch_selftest_division(origin, spacing, ncells, samples, d, nullptr);
+  unsigned long long h[2] = {0, 0};
+  if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "selftest_division");
+  *mismatches = h[0];
+  *checked = h[1];
   return BEAMS_OK;
 }
 

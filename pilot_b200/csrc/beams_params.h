@@ -38,6 +38,11 @@ struct ExactGeo {
   int slab_fp64;
   int use_map;
   int assoc_cells;
+  // Cell tables: per axis, one float4 {lo, hi, RN(1/(hi-lo)), 0} per cell, field
+  // axes first (n-1 cells each), then map axes (M cells each).
+  int ax_off[3];   // offset of field axis d in the table
+  int max_off[3];  // offset of map axis d in the table
+  int ntab;        // total table entries
 };
 
 // Counters written by the kernels (one atomic per warp).
@@ -48,7 +53,9 @@ struct Counters {
   unsigned long long mlp_samples;
   unsigned long long fallback_tiles;
   unsigned long long errors;
-  unsigned long long pad[2];
+  unsigned int tiles_light;   // persistent-block work counters (zeroed per frame)
+  unsigned int tiles_view;
+  unsigned long long pad;
 };
 
 }  // namespace beams

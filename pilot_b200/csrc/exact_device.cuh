@@ -94,32 +94,47 @@ __device__ __forceinline__ void light_origin(const ExactGeo& g, const float V[3]
   }
 }
 
+// Correctly rounded division x / w given r = RN(1/w), after Markstein's
+// theorem (P. Markstein, "Computation of elementary functions on the IBM
+// RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990): with r the
+// correctly rounded reciprocal and q a faithful quotient, the residual
+// e = x - q*w is exact under fma and RN(q + e*r) is the correctly rounded
+// quotient. One refinement makes q faithful, the second rounds it. Valid for
+// normal operands whose quotient neither overflows nor underflows, which
+// holds for the parametric coordinates here (|x| <= 2w, w a cell width);
+// beams_selftest(BEAMS_SELFTEST_DIVISION) checks it against IEEE division.
+__device__ __forceinline__ float div_rn_markstein(float x, float w, float r) {
+  float q = x * r;
+  float e = fmaf(-q, w, x);
+  q = fmaf(e, r, q);
+  e = fmaf(-q, w, x);
+  return fmaf(e, r, q);
+}
+
+// Cell tables: T[c] = {coord(c), coord(c+1), RN(1/(coord(c+1)-coord(c))), 0}.
+//
 // Light-march cell search: RectilinearMeshOracle's binary search
 // (RectilinearMeshOracle.h:154-176) returns the smallest cell c with
 // val <= coord(c+1). A seeded guess plus a bounded fix-up finds the same cell.
-__device__ __forceinline__ int find_cell_bsearch(const ExactGeo& g, int d, float val) {
-  const int cmax = g.n[d] - 2;
-  int c = (int)((val - g.org[d]) * g.invh[d]);
+__device__ __forceinline__ int find_cell_bsearch_t(const float4* T, int cmax, float org, float invh,
+                                                   float val, float4& e) {
+  int c = (int)((val - org) * invh);
   c = c < 0 ? 0 : (c > cmax ? cmax : c);
-  for (int it = 0; it < 4 && c > 0 && val <= coord(g, d, c); ++it) --c;
-  for (int it = 0; it < 4 && c < cmax && val > coord(g, d, c + 1); ++it) ++c;
-  // The seed is within one cell of the answer; these loops only run when the
-  // spacing is not uniform enough for that (never for counting coordinates).
-  while (c > 0 && val <= coord(g, d, c)) --c;
-  while (c < cmax && val > coord(g, d, c + 1)) ++c;
+  e = T[c];
+  while (c > 0 && val <= e.x) e = T[--c];
+  while (c < cmax && val > e.y) e = T[++c];
   return c;
 }
 
 // View-march cell search: RectilinearLocator::LocateCell (LightedVolumeRenderer.cxx:119-165)
 // walks to the unique cell with coord(c) <= p < coord(c+1).
-__device__ __forceinline__ int find_cell_walk(const ExactGeo& g, int d, float p) {
-  const int cmax = g.n[d] - 2;
-  int c = (int)((p - g.org[d]) * g.invh[d]);
+__device__ __forceinline__ int find_cell_walk_t(const float4* T, int cmax, float org, float invh, float p,
+                                                float4& e) {
+  int c = (int)((p - org) * invh);
   c = c < 0 ? 0 : (c > cmax ? cmax : c);
-  for (int it = 0; it < 4 && c > 0 && p < coord(g, d, c); ++it) --c;
-  for (int it = 0; it < 4 && c < cmax && p >= coord(g, d, c + 1); ++it) ++c;
-  while (c > 0 && p < coord(g, d, c)) --c;
-  while (c < cmax && p >= coord(g, d, c + 1)) ++c;
+  e = T[c];
+  while (c > 0 && p < e.x) e = T[--c];
+  while (c < cmax && p >= e.y) e = T[++c];
   return c;
 }
 
@@ -190,14 +205,9 @@ __device__ __forceinline__ bool inside_vol(const ExactGeo& g, const float p[3]) 
 }
 
 // TransmittanceLocator::LocateCell + GetEstimateUsingVerticesT
-// (TransmittanceMap.h:93-112, :200-229): map opacity at p.
-template <typename MapT>
-__device__ __forceinline__ float map_opacity(const ExactGeo& g, const MapT* __restrict__ map,
-                                             const float p[3]);
-
-template <>
-__device__ __forceinline__ float map_opacity<float>(const ExactGeo& g, const float* __restrict__ map,
-                                                    const float p[3]) {
+// (TransmittanceMap.h:93-112, :200-229): map opacity at p. MT = map cell tables.
+__device__ __forceinline__ float map_opacity_t(const ExactGeo& g, const float4* MT, const float* __restrict__ map,
+                                               const float p[3]) {
   int c[3];
   float pc[3];
 #pragma unroll
@@ -206,23 +216,35 @@ __device__ __forceinline__ float map_opacity<float>(const ExactGeo& g, const flo
     if (t < 0.f) t = 0.f;
     if (t >= (float)(g.pd[d] - 1)) t = (float)(g.pd[d] - 2);
     c[d] = (int)t;
-    const float lo = vtx_coord(g, d, c[d]);
-    const float hi = vtx_coord(g, d, c[d] + 1);
-    pc[d] = (p[d] - lo) / (hi - lo);
+    const float4 e = MT[g.max_off[d] + c[d]];
+    pc[d] = div_rn_markstein(p[d] - e.x, e.y - e.x, e.z);
   }
-  const int64_t px = g.pd[0], pxy = (int64_t)g.pd[0] * g.pd[1];
-  const int64_t i0 = (int64_t)c[2] * pxy + (int64_t)c[1] * px + c[0];
+  const unsigned px = (unsigned)g.pd[0], pxy = (unsigned)g.pd[0] * (unsigned)g.pd[1];
+  const float* m = map + ((unsigned)c[2] * pxy + (unsigned)c[1] * px + (unsigned)c[0]);
   float v[8];
-  v[0] = __ldg(map + i0);
-  v[1] = __ldg(map + i0 + 1);
-  v[2] = __ldg(map + i0 + 1 + px);
-  v[3] = __ldg(map + i0 + px);
-  v[4] = __ldg(map + i0 + pxy);
-  v[5] = __ldg(map + i0 + pxy + 1);
-  v[6] = __ldg(map + i0 + pxy + 1 + px);
-  v[7] = __ldg(map + i0 + pxy + px);
+  v[0] = __ldg(m);
+  v[1] = __ldg(m + 1);
+  v[2] = __ldg(m + 1 + px);
+  v[3] = __ldg(m + px);
+  v[4] = __ldg(m + pxy);
+  v[5] = __ldg(m + pxy + 1);
+  v[6] = __ldg(m + pxy + 1 + px);
+  v[7] = __ldg(m + pxy + px);
   return hex_interp(v, pc[0], pc[1], pc[2]);
 }
+
+// Quad layout of a point field: Q[z][y][x] = {f(x,y,z), f(x+1,y,z), f(x,y+1,z),
+// f(x+1,y+1,z)} for x < nx-1, y < ny-1, so one cell is two 16-byte loads
+// (z and z+1). VTK corner order 0..7 = lo.x lo.y lo.w lo.z hi.x hi.y hi.w hi.z.
+template <typename Q> struct QuadLoad;
+template <> struct QuadLoad<float4> {
+  static __device__ __forceinline__ void cell(const float4* __restrict__ q, unsigned qi, unsigned qz, float v[8]) {
+    const float4 a = __ldg(q + qi);
+    const float4 b = __ldg(q + qi + qz);
+    v[0] = a.x; v[1] = a.y; v[2] = a.w; v[3] = a.z;
+    v[4] = b.x; v[5] = b.y; v[6] = b.w; v[7] = b.z;
+  }
+};
 
 // Warp-aggregated counter increment (one atomic per warp). Must be reached by
 // all 32 lanes of the warp (kernels keep out-of-range lanes alive with v = 0);

@@ -9,6 +9,13 @@
 //   TransmittanceMapEstimator::GetEstimateUsingVertices (TransmittanceMap.h:166-197).
 // K2c view_march_cells: SamplerCellAssoc::operator() (LightedVolumeRenderer.cxx:540-641).
 //
+// Both marches are instruction-bound (the field and map are served from L1/L2),
+// so the layout is chosen to cut instructions per sample:
+//  * the field is read as 4-corner quads (two 16-byte loads per cell);
+//  * per-axis cell tables {lo, hi, RN(1/(hi-lo))} live in shared memory, so a
+//    cell search is one guess plus rare fix-ups, and the parametric division is
+//    Markstein's correction on the tabulated reciprocal;
+//  * blocks are persistent and take 256-ray tiles from an atomic counter.
 // Compiled with -fmad=false (see exact_device.cuh).
 #include <cuda_runtime.h>
 
@@ -18,23 +25,52 @@
 namespace beams {
 
 constexpr int kMaxTF = 1024;
+constexpr int kThreads = 256;
+
+// Loads the cell tables (and nothing else) into shared memory.
+__device__ __forceinline__ void load_tables(float4* s_tab, const float4* __restrict__ tab, int ntab) {
+  for (int i = threadIdx.x; i < ntab; i += blockDim.x) s_tab[i] = tab[i];
+}
+
+// Next 256-item tile of a persistent block, or -1 when the work is done.
+__device__ __forceinline__ int next_tile(unsigned* counter, int ntiles, int* s_tile) {
+  __syncthreads();
+  if (threadIdx.x == 0) *s_tile = (int)atomicAdd(counter, 1u);
+  __syncthreads();
+  const int t = *s_tile;
+  return t < ntiles ? t : -1;
+}
 
 // ---------------------------------------------------------------------------
 // K1
 // ---------------------------------------------------------------------------
-template <typename FieldT>
-__global__ void __launch_bounds__(256) k_light_march(const ExactGeo g, const FieldT* __restrict__ field,
-                                                     const float4* __restrict__ tf,
-                                                     float* __restrict__ map, int64_t nvert,
-                                                     Counters* __restrict__ cnt) {
-  __shared__ float s_a[kMaxTF];  // TF alpha / max alpha (TransmittanceMap.h:329)
+template <typename QuadT>
+__global__ void __launch_bounds__(kThreads) k_light_march(const ExactGeo g, const QuadT* __restrict__ quads,
+                                                          const float4* __restrict__ tab,
+                                                          const float4* __restrict__ tf,
+                                                          float* __restrict__ map, int nvert,
+                                                          Counters* __restrict__ cnt) {
+  extern __shared__ float4 s_dyn[];
+  float4* s_tab = s_dyn;                        // g.ntab entries
+  float* s_a = (float*)(s_dyn + g.ntab);        // TF alpha / max alpha (TransmittanceMap.h:329)
+  __shared__ int s_tile;
+  load_tables(s_tab, tab, g.ntab);
   for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x)
     s_a[i] = (g.max_alpha > 0.f) ? tf[i].w / g.max_alpha : 0.f;
-  __syncthreads();
 
-  const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const float4* T0 = s_tab + g.ax_off[0];
+  const float4* T1 = s_tab + g.ax_off[1];
+  const float4* T2 = s_tab + g.ax_off[2];
+  const int cm0 = g.n[0] - 2, cm1 = g.n[1] - 2, cm2 = g.n[2] - 2;
+  const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
+  const int n1 = g.tf_n - 1;
+  const int ntiles = (nvert + kThreads - 1) / kThreads;
   unsigned ns = 0;
-  if (id < nvert) {
+
+  for (int tile = next_tile(&cnt->tiles_light, ntiles, &s_tile); tile >= 0;
+       tile = next_tile(&cnt->tiles_light, ntiles, &s_tile)) {
+    const int id = tile * kThreads + threadIdx.x;
+    if (id >= nvert) continue;
     float V[3], L[3];
     map_vertex(g, id, V);
     light_origin(g, V, L);
@@ -47,8 +83,6 @@ __global__ void __launch_bounds__(256) k_light_march(const ExactGeo g, const Fie
     float s[3] = {st[0], st[1], st[2]};
     const float len2 = (tmax - tmin) * (tmax - tmin);
     const float sdx = g.step * dir[0], sdy = g.step * dir[1], sdz = g.step * dir[2];
-    const int n1 = g.tf_n - 1;
-    const int64_t nx = g.n[0], nxy = (int64_t)g.n[0] * g.n[1];
     float o = 0.f;
     for (int b = g.light_budget; b > 0; --b) {
       const float q0 = s[0] - st[0], q1 = s[1] - st[1], q2 = s[2] - st[2];
@@ -57,26 +91,16 @@ __global__ void __launch_bounds__(256) k_light_march(const ExactGeo g, const Fie
       s[1] = s[1] + sdy;
       s[2] = s[2] + sdz;
       if (!inside_vol(g, s)) break;
-      int c[3];
-      float pc[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        c[d] = find_cell_bsearch(g, d, s[d]);
-        const float lo = coord(g, d, c[d]);
-        const float hi = coord(g, d, c[d] + 1);
-        pc[d] = (s[d] - lo) / (hi - lo);
-      }
-      const int64_t i0 = (int64_t)c[2] * nxy + (int64_t)c[1] * nx + c[0];
+      float4 e0, e1, e2;
+      const int c0 = find_cell_bsearch_t(T0, cm0, g.org[0], g.invh[0], s[0], e0);
+      const int c1 = find_cell_bsearch_t(T1, cm1, g.org[1], g.invh[1], s[1], e1);
+      const int c2 = find_cell_bsearch_t(T2, cm2, g.org[2], g.invh[2], s[2], e2);
+      const float px = div_rn_markstein(s[0] - e0.x, e0.y - e0.x, e0.z);
+      const float py = div_rn_markstein(s[1] - e1.x, e1.y - e1.x, e1.z);
+      const float pz = div_rn_markstein(s[2] - e2.x, e2.y - e2.x, e2.z);
       float vals[8];
-      vals[0] = FieldLoad<FieldT>::ld(field, i0);
-      vals[1] = FieldLoad<FieldT>::ld(field, i0 + 1);
-      vals[2] = FieldLoad<FieldT>::ld(field, i0 + 1 + nx);
-      vals[3] = FieldLoad<FieldT>::ld(field, i0 + nx);
-      vals[4] = FieldLoad<FieldT>::ld(field, i0 + nxy);
-      vals[5] = FieldLoad<FieldT>::ld(field, i0 + nxy + 1);
-      vals[6] = FieldLoad<FieldT>::ld(field, i0 + nxy + 1 + nx);
-      vals[7] = FieldLoad<FieldT>::ld(field, i0 + nxy + nx);
-      float scalar = hex_interp(vals, pc[0], pc[1], pc[2]);
+      QuadLoad<QuadT>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qz, vals);
+      float scalar = hex_interp(vals, px, py, pz);
       scalar = (scalar - g.min_scalar) * g.inv_delta;
       const int idx = tf_index_clamped(scalar * (float)n1, n1);
       o = o + (1.f - o) * s_a[idx];
@@ -92,24 +116,23 @@ __global__ void __launch_bounds__(256) k_light_march(const ExactGeo g, const Fie
 // ---------------------------------------------------------------------------
 // K2 (point field)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void tile_pixel(const ExactGeo& g, int& x, int& y) {
-  // 16x16-pixel blocks of 8 warps; each warp owns an 8x4 tile.
+__device__ __forceinline__ void tile_pixel(int tiles_x, int tile, int& x, int& y) {
+  // 16x16-pixel tiles of 8 warps; each warp owns an 8x4 patch.
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int tiles_x = (g.width + 15) >> 4;
-  const int bx = blockIdx.x % tiles_x, by = blockIdx.x / tiles_x;
+  const int bx = tile % tiles_x, by = tile / tiles_x;
   x = (bx << 4) + ((w & 1) << 3) + (lane & 7);
   y = (by << 4) + ((w >> 1) << 2) + (lane >> 3);
 }
 
-template <typename FieldT, bool USE_MAP>
-__device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const FieldT* __restrict__ field,
-                                                 const float4* s_tf, const float* __restrict__ map,
-                                                 int x, int y, float4& color, unsigned& lit,
-                                                 unsigned& hit) {
+template <typename QuadT, bool USE_MAP>
+__device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT* __restrict__ quads,
+                                                 const float4* s_tab, const float4* s_tf,
+                                                 const float* __restrict__ map, int x, int y, float4& color,
+                                                 unsigned& lit, unsigned& hit) {
   color = make_float4(0.f, 0.f, 0.f, 0.f);
   float o[3], d[3], minD, maxD;
   if (!ray_setup(g, x, y, o, d, minD, maxD)) return;
-  hit = 1;
+  hit += 1;
   const float qd = (maxD - minD) / g.sd;
   long long budget = (qd < 1e9f) ? (long long)qd + 16 : 1000000000ll;
   float dist = minD + g.mesh_eps;
@@ -121,6 +144,7 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const FieldT
     p[2] = o[2] + dist * d[2];
   }
   const float sdx = g.sd * d[0], sdy = g.sd * d[1], sdz = g.sd * d[2];
+  const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
   float bl[3] = {0.f, 0.f, 0.f};
   bool newCell = true;
   float tx = 0.f, ty = 0.f, tz = 0.f;
@@ -128,7 +152,6 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const FieldT
   int c[3] = {0, 0, 0};
   float inv[3] = {0.f, 0.f, 0.f};
   const int n1 = g.tf_n - 1;
-  const int64_t nx = g.n[0], nxy = (int64_t)g.n[0] * g.n[1];
   while (inside_vol(g, p) && dist < maxD && budget-- > 0) {
     const float mint = mn(tx, mn(ty, tz));
     const float maxt = mx(tx, mx(ty, tz));
@@ -136,27 +159,27 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const FieldT
     if (newCell) {
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
+        const float4* T = s_tab + g.ax_off[k];
+        float4 e;
         if (p[k] == g.maxp[k]) {
           c[k] = g.n[k] - 2;  // the reference leaves invSpacing[k] unchanged here
+          e = T[c[k]];
         } else {
-          c[k] = find_cell_walk(g, k, p[k]);
-          inv[k] = 1.f / (coord(g, k, c[k] + 1) - coord(g, k, c[k]));
+          c[k] = find_cell_walk_t(T, g.n[k] - 2, g.org[k], g.invh[k], p[k], e);
+          inv[k] = e.z;  // 1.f / (coord(c+1) - coord(c)), IEEE
         }
-        bl[k] = coord(g, k, c[k]);
+        bl[k] = e.x;
       }
-      const int64_t i0 = (int64_t)c[2] * nxy + (int64_t)c[1] * nx + c[0];
-      s0 = FieldLoad<FieldT>::ld(field, i0);
-      const float s1 = FieldLoad<FieldT>::ld(field, i0 + 1);
-      const float s2 = FieldLoad<FieldT>::ld(field, i0 + 1 + nx);
-      s3 = FieldLoad<FieldT>::ld(field, i0 + nx);
-      s4 = FieldLoad<FieldT>::ld(field, i0 + nxy);
-      const float s5 = FieldLoad<FieldT>::ld(field, i0 + nxy + 1);
-      const float s6 = FieldLoad<FieldT>::ld(field, i0 + nxy + 1 + nx);
-      s7 = FieldLoad<FieldT>::ld(field, i0 + nxy + nx);
-      s6m7 = s6 - s7;
-      s5m4 = s5 - s4;
-      s1m0 = s1 - s0;
-      s2m3 = s2 - s3;
+      float v[8];
+      QuadLoad<QuadT>::cell(quads, (unsigned)c[2] * qz + (unsigned)c[1] * qx + (unsigned)c[0], qz, v);
+      s0 = v[0];
+      s3 = v[3];
+      s4 = v[4];
+      s7 = v[7];
+      s6m7 = v[6] - v[7];
+      s5m4 = v[5] - v[4];
+      s1m0 = v[1] - v[0];
+      s2m3 = v[2] - v[3];
       tx = (p[0] - bl[0]) * inv[0];
       ty = (p[1] - bl[1]) * inv[1];
       tz = (p[2] - bl[2]) * inv[2];
@@ -176,7 +199,7 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const FieldT
       float sc0 = tfc.x, sc1 = tfc.y, sc2 = tfc.z;
       const float sa = tfc.w * (1.f - color.w);
       if (USE_MAP) {
-        const float tr = 1.f - map_opacity<float>(g, map, p);
+        const float tr = 1.f - map_opacity_t(g, s_tab, map, p);
         sc0 = sc0 * (tr * g.light_color[0]);
         sc1 = sc1 * (tr * g.light_color[1]);
         sc2 = sc2 * (tr * g.light_color[2]);
@@ -201,22 +224,31 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const FieldT
   }
 }
 
-template <typename FieldT, bool USE_MAP>
-__global__ void __launch_bounds__(256) k_view_march(const ExactGeo g, const FieldT* __restrict__ field,
-                                                    const float4* __restrict__ tf,
-                                                    const float* __restrict__ map,
-                                                    float4* __restrict__ out,
-                                                    Counters* __restrict__ cnt) {
-  __shared__ float4 s_tf[kMaxTF];
+template <typename QuadT, bool USE_MAP>
+__global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const QuadT* __restrict__ quads,
+                                                         const float4* __restrict__ tab,
+                                                         const float4* __restrict__ tf,
+                                                         const float* __restrict__ map,
+                                                         float4* __restrict__ out,
+                                                         Counters* __restrict__ cnt) {
+  extern __shared__ float4 s_dyn[];
+  float4* s_tab = s_dyn;
+  float4* s_tf = s_dyn + g.ntab;
+  __shared__ int s_tile;
+  load_tables(s_tab, tab, g.ntab);
   for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) s_tf[i] = tf[i];
-  __syncthreads();
-  int x, y;
-  tile_pixel(g, x, y);
+  const int tiles_x = (g.width + 15) >> 4;
+  const int ntiles = tiles_x * ((g.height + 15) >> 4);
   unsigned lit = 0, hit = 0;
-  if (x < g.width && y < g.height) {
-    float4 color;
-    view_march_pixel<FieldT, USE_MAP>(g, field, s_tf, map, x, y, color, lit, hit);
-    out[(int64_t)y * g.width + x] = color;
+  for (int tile = next_tile(&cnt->tiles_view, ntiles, &s_tile); tile >= 0;
+       tile = next_tile(&cnt->tiles_view, ntiles, &s_tile)) {
+    int x, y;
+    tile_pixel(tiles_x, tile, x, y);
+    if (x < g.width && y < g.height) {
+      float4 color;
+      view_march_pixel<QuadT, USE_MAP>(g, quads, s_tab, s_tf, map, x, y, color, lit, hit);
+      out[(size_t)y * g.width + x] = color;
+    }
   }
   warp_add(&cnt->lit_samples, lit);
   warp_add(&cnt->rays_hit, hit);
@@ -226,22 +258,30 @@ __global__ void __launch_bounds__(256) k_view_march(const ExactGeo g, const Fiel
 // K2c (cell field, unlit)
 // ---------------------------------------------------------------------------
 template <typename FieldT>
-__global__ void __launch_bounds__(256) k_view_march_cells(const ExactGeo g,
-                                                          const FieldT* __restrict__ field,
-                                                          const float4* __restrict__ tf,
-                                                          float4* __restrict__ out,
-                                                          Counters* __restrict__ cnt) {
-  __shared__ float4 s_tf[kMaxTF];
+__global__ void __launch_bounds__(kThreads) k_view_march_cells(const ExactGeo g,
+                                                               const FieldT* __restrict__ field,
+                                                               const float4* __restrict__ tab,
+                                                               const float4* __restrict__ tf,
+                                                               float4* __restrict__ out,
+                                                               Counters* __restrict__ cnt) {
+  extern __shared__ float4 s_dyn[];
+  float4* s_tab = s_dyn;
+  float4* s_tf = s_dyn + g.ntab;
+  __shared__ int s_tile;
+  load_tables(s_tab, tab, g.ntab);
   for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) s_tf[i] = tf[i];
-  __syncthreads();
-  int x, y;
-  tile_pixel(g, x, y);
+  const int tiles_x = (g.width + 15) >> 4;
+  const int ntiles = tiles_x * ((g.height + 15) >> 4);
   unsigned lit = 0, hit = 0;
-  if (x < g.width && y < g.height) {
+  for (int tile = next_tile(&cnt->tiles_view, ntiles, &s_tile); tile >= 0;
+       tile = next_tile(&cnt->tiles_view, ntiles, &s_tile)) {
+    int x, y;
+    tile_pixel(tiles_x, tile, x, y);
+    if (!(x < g.width && y < g.height)) continue;
     float4 color = make_float4(0.f, 0.f, 0.f, 0.f);
     float o[3], d[3], minD, maxD;
     if (ray_setup(g, x, y, o, d, minD, maxD)) {
-      hit = 1;
+      hit += 1;
       const float qd = (maxD - minD) / g.sd;
       long long budget = (qd < 1e9f) ? (long long)qd + 16 : 1000000000ll;
       float dist = minD + g.mesh_eps;
@@ -260,7 +300,7 @@ __global__ void __launch_bounds__(256) k_view_march_cells(const ExactGeo g,
       float inv[3] = {0.f, 0.f, 0.f};
       int c[3] = {0, 0, 0};
       const int n1 = g.tf_n - 1;
-      const int64_t cx = g.n[0] - 1, cxy = (int64_t)(g.n[0] - 1) * (g.n[1] - 1);
+      const unsigned cx = (unsigned)(g.n[0] - 1), cxy = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
       while (inside_vol(g, p) && dist < maxD && budget-- > 0) {
         const float mint = mn(tx, mn(ty, tz));
         const float maxt = mx(tx, mx(ty, tz));
@@ -268,15 +308,18 @@ __global__ void __launch_bounds__(256) k_view_march_cells(const ExactGeo g,
         if (newCell) {
 #pragma unroll
           for (int k = 0; k < 3; ++k) {
+            const float4* T = s_tab + g.ax_off[k];
+            float4 e;
             if (p[k] == g.maxp[k]) {
               c[k] = g.n[k] - 2;
+              e = T[c[k]];
             } else {
-              c[k] = find_cell_walk(g, k, p[k]);
-              inv[k] = 1.f / (coord(g, k, c[k] + 1) - coord(g, k, c[k]));
+              c[k] = find_cell_walk_t(T, g.n[k] - 2, g.org[k], g.invh[k], p[k], e);
+              inv[k] = e.z;
             }
-            bl[k] = coord(g, k, c[k]);
+            bl[k] = e.x;
           }
-          const int64_t cid = (int64_t)c[2] * cxy + (int64_t)c[1] * cx + c[0];
+          const unsigned cid = (unsigned)c[2] * cxy + (unsigned)c[1] * cx + (unsigned)c[0];
           const float v = FieldLoad<FieldT>::ld(field, cid);
           const float nsv = (v - g.min_scalar) * g.inv_delta;
           sc = s_tf[tf_index_clamped(nsv * (float)n1, n1)];
@@ -305,33 +348,164 @@ __global__ void __launch_bounds__(256) k_view_march_cells(const ExactGeo g,
       color.z = mn(color.z, 1.f);
       color.w = mn(color.w, 1.f);
     }
-    out[(int64_t)y * g.width + x] = color;
+    out[(size_t)y * g.width + x] = color;
   }
   warp_add(&cnt->lit_samples, lit);
   warp_add(&cnt->rays_hit, hit);
 }
 
 // ---------------------------------------------------------------------------
+// layout builders
+// ---------------------------------------------------------------------------
+// Cell tables: field axes then map axes, each entry {lo, hi, RN(1/(hi-lo)), 0}
+// with lo/hi the same float expressions the marches compare against.
+__global__ void k_build_tables(const ExactGeo g, float4* __restrict__ tab) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.ntab) return;
+  float lo, hi;
+  if (i < g.max_off[0]) {
+    const int d = (i >= g.ax_off[2]) ? 2 : (i >= g.ax_off[1] ? 1 : 0);
+    const int c = i - g.ax_off[d];
+    lo = coord(g, d, c);
+    hi = coord(g, d, c + 1);
+  } else {
+    const int d = (i >= g.max_off[2]) ? 2 : (i >= g.max_off[1] ? 1 : 0);
+    const int c = i - g.max_off[d];
+    lo = vtx_coord(g, d, c);
+    hi = vtx_coord(g, d, c + 1);
+  }
+  tab[i] = make_float4(lo, hi, 1.f / (hi - lo), 0.f);
+}
+
+__global__ void k_build_quads(const float* __restrict__ f, float4* __restrict__ q, int nx, int ny, int nz) {
+  const unsigned qx = nx - 1, qxy = (unsigned)(nx - 1) * (ny - 1);
+  const size_t total = (size_t)qxy * nz;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const unsigned z = (unsigned)(i / qxy);
+    const unsigned r = (unsigned)(i - (size_t)z * qxy);
+    const unsigned y = r / qx, x = r - y * qx;
+    const float* b = f + ((size_t)z * ny + y) * nx + x;
+    q[i] = make_float4(__ldg(b), __ldg(b + 1), __ldg(b + nx), __ldg(b + nx + 1));
+  }
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-cudaError_t launch_light_march_f32(const ExactGeo& g, const float* field, const float4* tf,
-                                   float* map, Counters* cnt, cudaStream_t st) {
-  const int64_t nvert = (int64_t)g.pd[0] * g.pd[1] * g.pd[2];
-  const int64_t blocks = (nvert + 255) / 256;
-  k_light_march<float><<<(unsigned)blocks, 256, 0, st>>>(g, field, tf, map, nvert, cnt);
+static int g_num_sms = 0;
+static int num_sms() {
+  if (!g_num_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+template <typename K>
+static cudaError_t persistent_grid(K kernel, size_t smem, int ntiles, int& grid) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  grid = num_sms() * per_sm;
+  if (grid > ntiles) grid = ntiles;
+  if (grid < 1) grid = 1;
+  return cudaSuccess;
+}
+
+cudaError_t launch_build_tables(const ExactGeo& g, float4* tab, cudaStream_t st) {
+  k_build_tables<<<(g.ntab + 255) / 256, 256, 0, st>>>(g, tab);
   return cudaGetLastError();
 }
 
-cudaError_t launch_view_march_f32(const ExactGeo& g, const float* field, const float4* tf,
-                                  const float* map, float4* out, Counters* cnt, cudaStream_t st) {
-  const int blocks = ((g.width + 15) >> 4) * ((g.height + 15) >> 4);
+cudaError_t launch_build_quads(const float* field, float4* quads, const int n[3], cudaStream_t st) {
+  const size_t total = (size_t)(n[0] - 1) * (n[1] - 1) * n[2];
+  size_t blocks = (total + 255) / 256;
+  const size_t cap = (size_t)num_sms() * 16;
+  k_build_quads<<<(unsigned)(blocks < cap ? blocks : cap), 256, 0, st>>>(field, quads, n[0], n[1], n[2]);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
+                                   float* map, Counters* cnt, cudaStream_t st) {
+  const int nvert = g.pd[0] * g.pd[1] * g.pd[2];
+  const size_t smem = (size_t)g.ntab * sizeof(float4) + (size_t)g.tf_n * sizeof(float);
+  const int ntiles = (nvert + kThreads - 1) / kThreads;
+  int grid = 0;
+  cudaError_t e = persistent_grid(k_light_march<float4>, smem, ntiles, grid);
+  if (e != cudaSuccess) return e;
+  k_light_march<float4><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, map, nvert, cnt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_view_march_f32(const ExactGeo& g, const float* field, const float4* quads, const float4* tab,
+                                  const float4* tf, const float* map, float4* out, Counters* cnt, cudaStream_t st) {
+  const size_t smem = ((size_t)g.ntab + (size_t)g.tf_n) * sizeof(float4);
+  const int ntiles = ((g.width + 15) >> 4) * ((g.height + 15) >> 4);
+  int grid = 0;
+  cudaError_t e;
   if (g.assoc_cells) {
-    k_view_march_cells<float><<<blocks, 256, 0, st>>>(g, field, tf, out, cnt);
+    e = persistent_grid(k_view_march_cells<float>, smem, ntiles, grid);
+    if (e != cudaSuccess) return e;
+    k_view_march_cells<float><<<grid, kThreads, smem, st>>>(g, field, tab, tf, out, cnt);
   } else if (g.use_map) {
-    k_view_march<float, true><<<blocks, 256, 0, st>>>(g, field, tf, map, out, cnt);
+    e = persistent_grid(k_view_march<float4, true>, smem, ntiles, grid);
+    if (e != cudaSuccess) return e;
+    k_view_march<float4, true><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, map, out, cnt);
   } else {
-    k_view_march<float, false><<<blocks, 256, 0, st>>>(g, field, tf, nullptr, out, cnt);
+    e = persistent_grid(k_view_march<float4, false>, smem, ntiles, grid);
+    if (e != cudaSuccess) return e;
+    k_view_march<float4, false><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, nullptr, out, cnt);
   }
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// self-test: Markstein division against IEEE division on counting coordinates
+// ---------------------------------------------------------------------------
+__global__ void k_selftest_division(float org, float h, int ncells, int samples, unsigned long long* bad,
+                                    unsigned long long* checked) {
+  unsigned nb = 0, nc = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)ncells * samples;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i / samples);
+    const unsigned k = (unsigned)(i - (long long)c * samples);
+    const float lo = org + h * (float)c;
+    const float hi = org + h * (float)(c + 1);
+    const float w = hi - lo;
+    const float r = 1.f / w;
+    // x spans [-w/2, 3w/2]: a Weyl sequence over the interval plus exact end points.
+    float x;
+    if (k == 0) x = 0.f;
+    else if (k == 1) x = w;
+    else if (k == 2) x = w * 0.5f;
+    else {
+      const float u = (float)((k * 2654435769u) >> 8) * (1.f / 16777216.f);
+      x = (u * 2.f - 0.5f) * w;
+    }
+    const float ref = x / w;  // IEEE (prec-div)
+    const float got = div_rn_markstein(x, w, r);
+    nb += (__float_as_uint(ref) != __float_as_uint(got)) ? 1u : 0u;
+    nc += 1u;
+  }
+  const unsigned sb = __reduce_add_sync(0xffffffffu, nb), sc = __reduce_add_sync(0xffffffffu, nc);
+  if ((threadIdx.x & 31) == 0) {
+    if (sb) atomicAdd(bad, (unsigned long long)sb);
+    atomicAdd(checked, (unsigned long long)sc);
+  }
+}
+
+cudaError_t launch_selftest_division(float org, float h, int ncells, int samples, unsigned long long* d_out,
+                                     cudaStream_t st) {
+  const long long total = (long long)ncells * samples;
+  long long blocks = (total + 255) / 256;
+  const long long cap = (long long)num_sms() * 32;
+  k_selftest_division<<<(unsigned)(blocks < cap ? blocks : cap), 256, 0, st>>>(org, h, ncells, samples, d_out,
+                                                                              d_out + 1);
   return cudaGetLastError();
 }
 

@@ -7,10 +7,14 @@
 
 namespace beams {
 
-cudaError_t launch_light_march_f32(const ExactGeo& g, const float* field, const float4* tf,
+cudaError_t launch_build_tables(const ExactGeo& g, float4* tab, cudaStream_t st);
+cudaError_t launch_build_quads(const float* field, float4* quads, const int n[3], cudaStream_t st);
+cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    float* map, Counters* cnt, cudaStream_t st);
-cudaError_t launch_view_march_f32(const ExactGeo& g, const float* field, const float4* tf,
-                                  const float* map, float4* out, Counters* cnt, cudaStream_t st);
+cudaError_t launch_view_march_f32(const ExactGeo& g, const float* field, const float4* quads, const float4* tab,
+                                  const float4* tf, const float* map, float4* out, Counters* cnt, cudaStream_t st);
+cudaError_t launch_selftest_division(float org, float h, int ncells, int samples, unsigned long long* d_out,
+                                     cudaStream_t st);
 
 cudaError_t launch_generate_blobs(float* out, const int n[3], const float* d_params, int nblobs,
                                   cudaStream_t st);

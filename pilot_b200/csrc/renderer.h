@@ -75,6 +75,14 @@ struct beams_renderer {
   bool map_valid = false;
   beams::MapKey map_key{};
 
+  // derived layouts: 4-corner quads of the field, per-axis cell tables
+  float4* d_quads = nullptr;
+  size_t quads_cap = 0;
+  unsigned long long quads_version = 0;  // volume_version the quads were built from
+  float4* d_tab = nullptr;
+  size_t tab_cap = 0;
+  unsigned long long tab_key[4] = {0, 0, 0, 0};  // volume_version, map m[3] packed
+
   // image + counters + timing
   float4* d_rgba = nullptr;
   size_t rgba_cap = 0;
@@ -85,6 +93,8 @@ struct beams_renderer {
     if (d_field_owned) cudaFree(d_field_owned);
     if (d_tf) cudaFree(d_tf);
     if (d_map) cudaFree(d_map);
+    if (d_quads) cudaFree(d_quads);
+    if (d_tab) cudaFree(d_tab);
     if (d_rgba) cudaFree(d_rgba);
     if (d_cnt) cudaFree(d_cnt);
     for (auto& e : ev)

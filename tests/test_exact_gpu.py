@@ -55,6 +55,18 @@ def test_small_scene_parity(cuda_device, cfg):
           f"PSNR vs f64 {psnr(img, i64):.1f} dB")
 
 
+@pytest.mark.parametrize("n", [24, 129, 257, 513, 1025])
+def test_markstein_division_matches_ieee(cuda_device, n):
+    """The kernels' parametric-coordinate division equals IEEE division for every
+    cell width of the counting coordinates (0, 1/(n-1)) and 2^16 numerators each."""
+    checked, bad = B.selftest_division(0.0, 1.0 / (n - 1), n - 1, 1 << 16)
+    assert checked == (n - 1) << 16 and bad == 0
+    # map axes: spacing = extent / M
+    for m in (16, 128, 256, 512):
+        checked, bad = B.selftest_division(0.0, 1.0 / m, m, 1 << 14)
+        assert bad == 0
+
+
 def test_slab_fp32_reference_mode(cuda_device):
     s = scenes.small(4, n=32, image=80, m=16, kind="blobs")
     s.slab_fp64 = False

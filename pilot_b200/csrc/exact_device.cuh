@@ -111,18 +111,22 @@ __device__ __forceinline__ float div_rn_markstein(float x, float w, float r) {
   return fmaf(e, r, q);
 }
 
-// Cell tables: T[c] = {coord(c), coord(c+1), RN(1/(coord(c+1)-coord(c))), 0}.
+// Cell tables: T[c] = {coord(c), coord(c+1), coord(c+1)-coord(c), RN(1/(coord(c+1)-coord(c)))}.
 //
 // Light-march cell search: RectilinearMeshOracle's binary search
 // (RectilinearMeshOracle.h:154-176) returns the smallest cell c with
-// val <= coord(c+1). A seeded guess plus a bounded fix-up finds the same cell.
+// val <= coord(c+1). The seed (val - org) / h is that cell for counting
+// coordinates except within an ulp of a cell face, where the bounded walk
+// below settles it. At c == 0 a point on the lower face stays in cell 0 and
+// inside the volume val <= coord(cmax+1), so one test per side suffices.
 __device__ __forceinline__ int find_cell_bsearch_t(const float4* T, int cmax, float org, float invh,
                                                    float val, float4& e) {
-  int c = (int)((val - org) * invh);
-  c = c < 0 ? 0 : (c > cmax ? cmax : c);
+  int c = (int)fminf(fmaxf((val - org) * invh, 0.f), (float)cmax);
   e = T[c];
-  while (c > 0 && val <= e.x) e = T[--c];
-  while (c < cmax && val > e.y) e = T[++c];
+  if (val <= e.x || val > e.y) {
+    while (c > 0 && val <= e.x) e = T[--c];
+    while (c < cmax && val > e.y) e = T[++c];
+  }
   return c;
 }
 
@@ -130,21 +134,20 @@ __device__ __forceinline__ int find_cell_bsearch_t(const float4* T, int cmax, fl
 // walks to the unique cell with coord(c) <= p < coord(c+1).
 __device__ __forceinline__ int find_cell_walk_t(const float4* T, int cmax, float org, float invh, float p,
                                                 float4& e) {
-  int c = (int)((p - org) * invh);
-  c = c < 0 ? 0 : (c > cmax ? cmax : c);
+  int c = (int)fminf(fmaxf((p - org) * invh, 0.f), (float)cmax);
   e = T[c];
-  while (c > 0 && p < e.x) e = T[--c];
-  while (c < cmax && p >= e.y) e = T[++c];
+  if (p < e.x || p >= e.y) {
+    while (c > 0 && p < e.x) e = T[--c];
+    while (c < cmax && p >= e.y) e = T[++c];
+  }
   return c;
 }
 
-// TF index of the light march (TransmittanceMap.h:322-326), saturating.
+// TF index of the light march (TransmittanceMap.h:322-326): truncate, clamp to
+// [0, n1]; saturating, NaN -> 0. Clamping in float first gives the same index:
+// (-1, 0) truncates to 0 either way and [n1, n1+1) to n1.
 __device__ __forceinline__ int tf_index_clamped(float fi, int n1) {
-  if (fi > -1.f && fi < (float)(n1 + 1)) {
-    int idx = (int)fi;
-    return idx < 0 ? 0 : (idx > n1 ? n1 : idx);
-  }
-  return (fi >= (float)(n1 + 1)) ? n1 : 0;
+  return (int)fminf(fmaxf(fi, 0.f), (float)n1);
 }
 
 // Pinhole camera ray through pixel centre (x, y).
@@ -217,7 +220,7 @@ __device__ __forceinline__ float map_opacity_t(const ExactGeo& g, const float4* 
     if (t >= (float)(g.pd[d] - 1)) t = (float)(g.pd[d] - 2);
     c[d] = (int)t;
     const float4 e = MT[g.max_off[d] + c[d]];
-    pc[d] = div_rn_markstein(p[d] - e.x, e.y - e.x, e.z);
+    pc[d] = div_rn_markstein(p[d] - e.x, e.z, e.w);
   }
   const unsigned px = (unsigned)g.pd[0], pxy = (unsigned)g.pd[0] * (unsigned)g.pd[1];
   const float* m = map + ((unsigned)c[2] * pxy + (unsigned)c[1] * px + (unsigned)c[0]);

@@ -32,31 +32,23 @@ __device__ __forceinline__ void load_tables(float4* s_tab, const float4* __restr
   for (int i = threadIdx.x; i < ntab; i += blockDim.x) s_tab[i] = tab[i];
 }
 
-// Next 256-item tile of a persistent block, or -1 when the work is done.
-__device__ __forceinline__ int next_tile(unsigned* counter, int ntiles, int* s_tile) {
-  __syncthreads();
-  if (threadIdx.x == 0) *s_tile = (int)atomicAdd(counter, 1u);
-  __syncthreads();
-  const int t = *s_tile;
-  return t < ntiles ? t : -1;
-}
-
 // ---------------------------------------------------------------------------
 // K1
 // ---------------------------------------------------------------------------
 template <typename QuadT>
-__global__ void __launch_bounds__(kThreads) k_light_march(const ExactGeo g, const QuadT* __restrict__ quads,
+__global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, const QuadT* __restrict__ quads,
                                                           const float4* __restrict__ tab,
                                                           const float4* __restrict__ tf,
                                                           float* __restrict__ map, int nvert,
                                                           Counters* __restrict__ cnt) {
   extern __shared__ float4 s_dyn[];
-  float4* s_tab = s_dyn;                        // g.ntab entries
-  float* s_a = (float*)(s_dyn + g.ntab);        // TF alpha / max alpha (TransmittanceMap.h:329)
-  __shared__ int s_tile;
-  load_tables(s_tab, tab, g.ntab);
+  const int nfield = g.max_off[0];             // field-axis table entries only
+  float4* s_tab = s_dyn;
+  float* s_a = (float*)(s_dyn + nfield);       // TF alpha / max alpha (TransmittanceMap.h:329)
+  load_tables(s_tab, tab, nfield);
   for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x)
     s_a[i] = (g.max_alpha > 0.f) ? tf[i].w / g.max_alpha : 0.f;
+  __syncthreads();
 
   const float4* T0 = s_tab + g.ax_off[0];
   const float4* T1 = s_tab + g.ax_off[1];
@@ -64,12 +56,16 @@ __global__ void __launch_bounds__(kThreads) k_light_march(const ExactGeo g, cons
   const int cm0 = g.n[0] - 2, cm1 = g.n[1] - 2, cm2 = g.n[2] - 2;
   const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
   const int n1 = g.tf_n - 1;
-  const int ntiles = (nvert + kThreads - 1) / kThreads;
+  // Warps take 32-vertex tiles round-robin: no block barriers inside the march,
+  // and the tiles in flight sweep the vertex array in order.
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int ntiles = (nvert + 31) >> 5;
   unsigned ns = 0;
 
-  for (int tile = next_tile(&cnt->tiles_light, ntiles, &s_tile); tile >= 0;
-       tile = next_tile(&cnt->tiles_light, ntiles, &s_tile)) {
-    const int id = tile * kThreads + threadIdx.x;
+  for (int tile = warp; tile < ntiles; tile += nwarps) {
+    const int id = (tile << 5) + lane;
     if (id >= nvert) continue;
     float V[3], L[3];
     map_vertex(g, id, V);
@@ -83,29 +79,51 @@ __global__ void __launch_bounds__(kThreads) k_light_march(const ExactGeo g, cons
     float s[3] = {st[0], st[1], st[2]};
     const float len2 = (tmax - tmin) * (tmax - tmin);
     const float sdx = g.step * dir[0], sdy = g.step * dir[1], sdz = g.step * dir[2];
-    float o = 0.f;
-    for (int b = g.light_budget; b > 0; --b) {
+    // The sample positions do not depend on the opacity, so sample k+1 is
+    // located and its loads issued before sample k is composited (the loads of
+    // two samples are in flight per ray). The break conditions are evaluated
+    // in the reference's order for every sample; only o == 1 ends the march
+    // early, after which the prefetched sample is discarded.
+    int b = g.light_budget;
+    auto gen = [&](float v8[8], float pc[3]) -> bool {
+      if (b-- <= 0) return false;
       const float q0 = s[0] - st[0], q1 = s[1] - st[1], q2 = s[2] - st[2];
-      if (!(q0 * q0 + q1 * q1 + q2 * q2 <= len2)) break;
+      if (!(q0 * q0 + q1 * q1 + q2 * q2 <= len2)) return false;
       s[0] = s[0] + sdx;
       s[1] = s[1] + sdy;
       s[2] = s[2] + sdz;
-      if (!inside_vol(g, s)) break;
+      if (!inside_vol(g, s)) return false;
       float4 e0, e1, e2;
       const int c0 = find_cell_bsearch_t(T0, cm0, g.org[0], g.invh[0], s[0], e0);
       const int c1 = find_cell_bsearch_t(T1, cm1, g.org[1], g.invh[1], s[1], e1);
       const int c2 = find_cell_bsearch_t(T2, cm2, g.org[2], g.invh[2], s[2], e2);
-      const float px = div_rn_markstein(s[0] - e0.x, e0.y - e0.x, e0.z);
-      const float py = div_rn_markstein(s[1] - e1.x, e1.y - e1.x, e1.z);
-      const float pz = div_rn_markstein(s[2] - e2.x, e2.y - e2.x, e2.z);
-      float vals[8];
-      QuadLoad<QuadT>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qz, vals);
-      float scalar = hex_interp(vals, px, py, pz);
-      scalar = (scalar - g.min_scalar) * g.inv_delta;
-      const int idx = tf_index_clamped(scalar * (float)n1, n1);
-      o = o + (1.f - o) * s_a[idx];
-      ++ns;
+      QuadLoad<QuadT>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qz, v8);
+      // pcoords = (p - min) / (max - min) (RectilinearMeshOracle.h:189-192)
+      pc[0] = div_rn_markstein(s[0] - e0.x, e0.z, e0.w);
+      pc[1] = div_rn_markstein(s[1] - e1.x, e1.z, e1.w);
+      pc[2] = div_rn_markstein(s[2] - e2.x, e2.z, e2.w);
+      return true;
+    };
+    float o = 0.f;
+    float va[8], pa[3], vb[8], pb[3];
+    bool ok = gen(va, pa);
+    while (ok) {
+      const bool okb = gen(vb, pb);
+      {
+        float scalar = hex_interp(va, pa[0], pa[1], pa[2]);
+        scalar = (scalar - g.min_scalar) * g.inv_delta;
+        o = o + (1.f - o) * s_a[tf_index_clamped(scalar * (float)n1, n1)];
+        ++ns;
+      }
       // o == 1 is a fixed point of o + (1-o)a: the remaining samples cannot change it.
+      if (o == 1.f || !okb) break;
+      ok = gen(va, pa);
+      {
+        float scalar = hex_interp(vb, pb[0], pb[1], pb[2]);
+        scalar = (scalar - g.min_scalar) * g.inv_delta;
+        o = o + (1.f - o) * s_a[tf_index_clamped(scalar * (float)n1, n1)];
+        ++ns;
+      }
       if (o == 1.f) break;
     }
     map[id] = o;
@@ -116,12 +134,19 @@ __global__ void __launch_bounds__(kThreads) k_light_march(const ExactGeo g, cons
 // ---------------------------------------------------------------------------
 // K2 (point field)
 // ---------------------------------------------------------------------------
+// 8x4-pixel warp tiles; tiles_x = ceil(width / 8).
 __device__ __forceinline__ void tile_pixel(int tiles_x, int tile, int& x, int& y) {
-  // 16x16-pixel tiles of 8 warps; each warp owns an 8x4 patch.
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31;
   const int bx = tile % tiles_x, by = tile / tiles_x;
-  x = (bx << 4) + ((w & 1) << 3) + (lane & 7);
-  y = (by << 4) + ((w >> 1) << 2) + (lane >> 3);
+  x = (bx << 3) + (lane & 7);
+  y = (by << 2) + (lane >> 3);
+}
+
+// Next warp tile from the frame's counter (one atomic per warp tile).
+__device__ __forceinline__ int next_warp_tile(unsigned* counter) {
+  unsigned t = 0;
+  if ((threadIdx.x & 31) == 0) t = atomicAdd(counter, 1u);
+  return (int)__shfl_sync(0xffffffffu, t, 0);
 }
 
 template <typename QuadT, bool USE_MAP>
@@ -166,7 +191,7 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT*
           e = T[c[k]];
         } else {
           c[k] = find_cell_walk_t(T, g.n[k] - 2, g.org[k], g.invh[k], p[k], e);
-          inv[k] = e.z;  // 1.f / (coord(c+1) - coord(c)), IEEE
+          inv[k] = e.w;  // 1.f / (coord(c+1) - coord(c)), IEEE
         }
         bl[k] = e.x;
       }
@@ -234,14 +259,13 @@ __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const
   extern __shared__ float4 s_dyn[];
   float4* s_tab = s_dyn;
   float4* s_tf = s_dyn + g.ntab;
-  __shared__ int s_tile;
   load_tables(s_tab, tab, g.ntab);
   for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) s_tf[i] = tf[i];
-  const int tiles_x = (g.width + 15) >> 4;
-  const int ntiles = tiles_x * ((g.height + 15) >> 4);
+  __syncthreads();
+  const int tiles_x = (g.width + 7) >> 3;
+  const int ntiles = tiles_x * ((g.height + 3) >> 2);
   unsigned lit = 0, hit = 0;
-  for (int tile = next_tile(&cnt->tiles_view, ntiles, &s_tile); tile >= 0;
-       tile = next_tile(&cnt->tiles_view, ntiles, &s_tile)) {
+  for (int tile = next_warp_tile(&cnt->tiles_view); tile < ntiles; tile = next_warp_tile(&cnt->tiles_view)) {
     int x, y;
     tile_pixel(tiles_x, tile, x, y);
     if (x < g.width && y < g.height) {
@@ -267,14 +291,13 @@ __global__ void __launch_bounds__(kThreads) k_view_march_cells(const ExactGeo g,
   extern __shared__ float4 s_dyn[];
   float4* s_tab = s_dyn;
   float4* s_tf = s_dyn + g.ntab;
-  __shared__ int s_tile;
   load_tables(s_tab, tab, g.ntab);
   for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) s_tf[i] = tf[i];
-  const int tiles_x = (g.width + 15) >> 4;
-  const int ntiles = tiles_x * ((g.height + 15) >> 4);
+  __syncthreads();
+  const int tiles_x = (g.width + 7) >> 3;
+  const int ntiles = tiles_x * ((g.height + 3) >> 2);
   unsigned lit = 0, hit = 0;
-  for (int tile = next_tile(&cnt->tiles_view, ntiles, &s_tile); tile >= 0;
-       tile = next_tile(&cnt->tiles_view, ntiles, &s_tile)) {
+  for (int tile = next_warp_tile(&cnt->tiles_view); tile < ntiles; tile = next_warp_tile(&cnt->tiles_view)) {
     int x, y;
     tile_pixel(tiles_x, tile, x, y);
     if (!(x < g.width && y < g.height)) continue;
@@ -315,7 +338,7 @@ __global__ void __launch_bounds__(kThreads) k_view_march_cells(const ExactGeo g,
               e = T[c[k]];
             } else {
               c[k] = find_cell_walk_t(T, g.n[k] - 2, g.org[k], g.invh[k], p[k], e);
-              inv[k] = e.z;
+              inv[k] = e.w;
             }
             bl[k] = e.x;
           }
@@ -357,7 +380,7 @@ __global__ void __launch_bounds__(kThreads) k_view_march_cells(const ExactGeo g,
 // ---------------------------------------------------------------------------
 // layout builders
 // ---------------------------------------------------------------------------
-// Cell tables: field axes then map axes, each entry {lo, hi, RN(1/(hi-lo)), 0}
+// Cell tables: field axes then map axes, each entry {lo, hi, hi-lo, RN(1/(hi-lo))}
 // with lo/hi the same float expressions the marches compare against.
 __global__ void k_build_tables(const ExactGeo g, float4* __restrict__ tab) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -374,7 +397,8 @@ __global__ void k_build_tables(const ExactGeo g, float4* __restrict__ tab) {
     lo = vtx_coord(g, d, c);
     hi = vtx_coord(g, d, c + 1);
   }
-  tab[i] = make_float4(lo, hi, 1.f / (hi - lo), 0.f);
+  const float w = hi - lo;
+  tab[i] = make_float4(lo, hi, w, 1.f / w);
 }
 
 __global__ void k_build_quads(const float* __restrict__ f, float4* __restrict__ q, int nx, int ny, int nz) {
@@ -433,7 +457,7 @@ cudaError_t launch_build_quads(const float* field, float4* quads, const int n[3]
 cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    float* map, Counters* cnt, cudaStream_t st) {
   const int nvert = g.pd[0] * g.pd[1] * g.pd[2];
-  const size_t smem = (size_t)g.ntab * sizeof(float4) + (size_t)g.tf_n * sizeof(float);
+  const size_t smem = (size_t)g.max_off[0] * sizeof(float4) + (size_t)g.tf_n * sizeof(float);
   const int ntiles = (nvert + kThreads - 1) / kThreads;
   int grid = 0;
   cudaError_t e = persistent_grid(k_light_march<float4>, smem, ntiles, grid);
@@ -445,7 +469,7 @@ cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const
 cudaError_t launch_view_march_f32(const ExactGeo& g, const float* field, const float4* quads, const float4* tab,
                                   const float4* tf, const float* map, float4* out, Counters* cnt, cudaStream_t st) {
   const size_t smem = ((size_t)g.ntab + (size_t)g.tf_n) * sizeof(float4);
-  const int ntiles = ((g.width + 15) >> 4) * ((g.height + 15) >> 4);
+  const int ntiles = (((g.width + 7) >> 3) * ((g.height + 3) >> 2) + 7) / 8;  // 8 warp tiles per block
   int grid = 0;
   cudaError_t e;
   if (g.assoc_cells) {

@@ -161,6 +161,32 @@ beams_status beams_get_shadow_map(beams_renderer* r, float* dst, size_t count, i
 /* Builds the map only (Phase 1), without a view march. */
 beams_status beams_build_shadow_map(beams_renderer* r, beams_timings* t);
 
+/* ---- render without device allocation ---------------------------------------- */
+/* No counterpart in the reference: an addition for callers that may not
+ * allocate device memory themselves (a plugin or custom call inside another
+ * framework that owns all GPU memory through its own allocator, or a frame loop
+ * that must not stall on cudaMalloc/cudaFree, which can synchronise the device).
+ * Renders one frame like beams_create + set_* + beams_render with a point light,
+ * the reference's 128 light steps and the FP64 slab, into rgba_out_device
+ * (width*height*4 floats, 16-byte aligned), asynchronously on cuda_stream.
+ * Inputs stay the caller's: vol must be a float32 point field with on_device = 1,
+ * tf_rgba_device holds tf_n (<= 1024) RGBA entries on the device, 16-byte aligned.
+ * It calls no cudaMalloc or cudaFree: its only scratch, the frame's
+ * (map_cells+1)^3 transmittance map, lives in one static device array sized for
+ * map_cells <= BEAMS_NOALLOC_MAX_MAP_CELLS (129^3 floats, 8.6 MB), which every
+ * device that loads the library holds until exit; larger map_cells is rejected
+ * with BEAMS_ERR_INVALID_ARG. The first call on each device looks up that
+ * array's device address (cudaGetSymbolAddress), so make the first call on a
+ * device outside any stream capture. All calls share the one array: calls that
+ * overlap on the GPU (other streams, other threads) race and corrupt each
+ * other's maps; serialise them. Each call rewrites every map entry it reads, so
+ * no clearing is needed between calls. Errors: beams_last_error(NULL). */
+#define BEAMS_NOALLOC_MAX_MAP_CELLS 128
+beams_status beams_render_noalloc(const beams_volume* vol, const float* tf_rgba_device, int tf_n,
+                                  const double light_pos[3], const float light_color[3], float light_intensity,
+                                  int map_cells, float sample_distance, float termination_alpha,
+                                  const beams_camera* cam, float* rgba_out_device, void* cuda_stream);
+
 /* ---- diagnostics ------------------------------------------------------------ */
 /* Checks, on the device, the kernels' correctly rounded division (Markstein's
  * correction on a tabulated reciprocal) against IEEE division for every cell

@@ -147,6 +147,23 @@ beams_status beams_set_background(beams_renderer* r, int enable, const float rgb
  * const beams_mlp_options*. */
 beams_status beams_set_form(beams_renderer* r, int form, const void* opts);
 
+/* ---- multi-block scenes (sort-last on one GPU) ------------------------------- */
+/* Replaces the reference's one-block-per-rank decomposition: SetData of each
+ * rank's block plus the BoundsMap of all blocks (BoundsMap.cxx:93-127). After this
+ * call beams_render runs the reference's five phases on the device: Phase 1 local
+ * maps, Phases 2-3 cross-block shadow stitching (LightedVolumeRenderer.cxx:968-1256,
+ * TransmittanceMap.h:342-513: each other block's map opacity at the light
+ * segment's exit point, over-composited in exit order, then the local march
+ * re-run from that prefix), Phase 4 a view march per block clipped to its
+ * bounds, and Phase 5 the depth-ordered over composite of the block images
+ * (MapperLightedVolume.cxx:215-303). Blocks are float32 point fields; neighbours
+ * share their face plane. Up to 32 blocks. beams_set_volume leaves this mode. */
+beams_status beams_set_bricks(beams_renderer* r, const beams_volume* bricks, int nbricks);
+/* Copies brick `brick`'s map after the last render: stage 0 = Phase 1 (local),
+ * stage 1 = stitched. For tests and tools. */
+beams_status beams_get_brick_map(beams_renderer* r, int brick, int stage, float* dst, size_t count,
+                                 int dst_on_device);
+
 /* ---- render --------------------------------------------------------------- */
 /* Replaces MapperLightedVolume::RenderCells (MapperLightedVolume.cxx:114-193):
  * map build (Phase 1/3) + view march (Phase 4) + copy-out (Phase 5).

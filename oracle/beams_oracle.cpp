@@ -203,7 +203,7 @@ inline T field_at(const Geo<T>& g, int64_t j) {
 
 // Marches from light origin L to destination P; returns the accumulated opacity.
 template <typename T>
-T light_march_point(const Geo<T>& g, const T L[3], const T P[3], uint64_t& nsamples) {
+T light_march_point(const Geo<T>& g, const T L[3], const T P[3], uint64_t& nsamples, T o0 = T(0)) {
   T v[3] = {P[0] - L[0], P[1] - L[1], P[2] - L[2]};
   const T rs = T(1) / std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
   const T dir[3] = {v[0] * rs, v[1] * rs, v[2] * rs};
@@ -213,7 +213,7 @@ T light_march_point(const Geo<T>& g, const T L[3], const T P[3], uint64_t& nsamp
   T sl[3] = {start[0], start[1], start[2]};
   const T len2 = (tmax - tmin) * (tmax - tmin);
   const int N1 = g.tf_n - 1;
-  T o = T(0);
+  T o = o0;
   // Budget: the loop below advances by step each iteration inside the box.
   int budget = (int)(g.extent_mag / g.step) + 8;
   while (budget-- > 0) {
@@ -295,7 +295,17 @@ T vertex_opacity(const Geo<T>& g, int64_t id, uint64_t& ns) {
 // ---- map lookup (TransmittanceMap.h:93-112 LocateCell, :166-197 estimator) -----
 
 template <typename T, typename MapGet>
+inline T map_opacity_at(const Geo<T>& g, const T p[3], MapGet get);
+
+template <typename T, typename MapGet>
 inline void map_estimate(const Geo<T>& g, const T p[3], MapGet get, T est[3]) {
+  const T tr = T(1) - map_opacity_at(g, p, get);
+  for (int d = 0; d < 3; ++d) est[d] = tr * g.light_color[d];
+}
+
+// GetEstimateUsingVerticesT (TransmittanceMap.h:200-229): map opacity at p.
+template <typename T, typename MapGet>
+inline T map_opacity_at(const Geo<T>& g, const T p[3], MapGet get) {
   int64_t c[3];
   for (int d = 0; d < 3; ++d) {
     T t = (p[d] - g.morig[d]) * g.minv[d];
@@ -320,9 +330,7 @@ inline void map_estimate(const Geo<T>& g, const T p[3], MapGet get, T est[3]) {
   v[5] = get(i0 + pxy + 1);
   v[6] = get(i0 + pxy + 1 + px);
   v[7] = get(i0 + pxy + px);
-  const T opacity = hex_interp(v, pc[0], pc[1], pc[2]);
-  const T tr = T(1) - opacity;
-  for (int d = 0; d < 3; ++d) est[d] = tr * g.light_color[d];
+  return hex_interp(v, pc[0], pc[1], pc[2]);
 }
 
 // ---- camera + slab (LightedVolumeRenderer.cxx:644-718) --------------------------
@@ -578,6 +586,142 @@ int view_march(const oracle_scene* s, const T* map, int x0, int y0, int w, int h
 
 }  // namespace
 
+
+// ---- multi-block rendering (the reference's sort-last path on one host) ----------
+//
+// Phase 1: each block marches its own map from zero (TransmittanceMap.h:565-621).
+// Phases 2-3 (LightedVolumeRenderer.cxx:968-1256, TransmittanceMap.h:342-513):
+// for every vertex, each other block the segment light->vertex crosses
+// (SegmentAABB hit, glancing hits included) contributes its Phase-1 map opacity
+// at the segment's exit point (RayT = tMax); the contributions are
+// over-composited in increasing RayT and the local march is re-run starting
+// from that prefix. Phase 4: each block renders the full image clipped to its
+// own bounds. Phase 5 (MapperLightedVolume.cxx:215-303): images are composited
+// front to back in increasing |camera - block centre|.
+namespace {
+
+template <typename T>
+int render_bricks(const oracle_scene* sc, int nb, T* maps_local, T* maps_final, T* imgs, T* rgba, int threads,
+                  uint64_t* lit_out) {
+  if (nb < 1 || !rgba) return 1;
+  for (int b = 0; b < nb; ++b)
+    if (!valid(&sc[b])) return 1;
+  std::vector<Geo<T>> G(nb);
+  for (int b = 0; b < nb; ++b) build_geo(&sc[b], G[b]);
+  std::vector<std::vector<T>> local(nb), fin(nb);
+  for (int b = 0; b < nb; ++b) {
+    const int64_t nv = (int64_t)G[b].pd[0] * G[b].pd[1] * G[b].pd[2];
+    local[b].resize(nv);
+    fin[b].resize(nv);
+    const Geo<T>& g = G[b];
+    T* dst = local[b].data();
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(nthreads(threads))
+    for (int64_t id = 0; id < nv; ++id) {
+      uint64_t ns = 0;
+      dst[id] = vertex_opacity(g, id, ns);
+    }
+  }
+  for (int b = 0; b < nb; ++b) {
+    const int64_t nv = (int64_t)G[b].pd[0] * G[b].pd[1] * G[b].pd[2];
+    const Geo<T>& g = G[b];
+    T* dst = fin[b].data();
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(nthreads(threads))
+    for (int64_t id = 0; id < nv; ++id) {
+      T V[3], L[3];
+      map_vertex(g, id, V);
+      light_origin(g, V, L);
+      T v[3] = {V[0] - L[0], V[1] - L[1], V[2] - L[2]};
+      const T rs = T(1) / std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      const T dir[3] = {v[0] * rs, v[1] * rs, v[2] * rs};
+      struct Hit { T t; int blk; T op; };
+      Hit hits[64];
+      int nh = 0;
+      for (int c = 0; c < nb && nh < 64; ++c) {
+        if (c == b) continue;
+        T tmin, tmax;
+        segment_aabb(L, V, G[c], tmin, tmax);
+        if (!(tmin <= tmax)) continue;
+        const T P[3] = {L[0] + dir[0] * tmax, L[1] + dir[1] * tmax, L[2] + dir[2] * tmax};
+        const T* mc = local[c].data();
+        const T op = map_opacity_at(G[c], P, [mc](int64_t i) -> T { return mc[i]; });
+        hits[nh++] = Hit{tmax, c, op};
+      }
+      // HitSort (TransmittanceMap.h:371-385): increasing RayT; ties by block id.
+      for (int i = 1; i < nh; ++i)
+        for (int j = i; j > 0 && (hits[j].t < hits[j - 1].t ||
+                                  (hits[j].t == hits[j - 1].t && hits[j].blk < hits[j - 1].blk)); --j)
+          std::swap(hits[j], hits[j - 1]);
+      T o = T(0);
+      for (int i = 0; i < nh; ++i) o = o + (T(1) - o) * hits[i].op;
+      uint64_t ns = 0;
+      dst[id] = light_march_point(g, L, V, ns, o);
+    }
+  }
+  const int W = sc[0].width, H = sc[0].height;
+  const int64_t npx = (int64_t)W * H;
+  std::vector<T> img((size_t)nb * npx * 4);
+  uint64_t lit = 0;
+  for (int b = 0; b < nb; ++b) {
+    const Geo<T>& g = G[b];
+    const T* mp = fin[b].data();
+    auto get = [mp](int64_t i) -> T { return mp[i]; };
+    T* out = img.data() + (size_t)b * npx * 4;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads(threads)) reduction(+ : lit)
+    for (int64_t i = 0; i < npx; ++i) {
+      const int yy = (int)(i / W), xx = (int)(i - (int64_t)yy * W);
+      T c[4];
+      uint64_t l = 0;
+      march_pixel(g, xx, yy, get, c, l);
+      lit += l;
+      for (int k = 0; k < 4; ++k) out[4 * i + k] = c[k];
+    }
+  }
+  // depth order: |camera - block centre| in float (MapperLightedVolume.cxx:221-241)
+  std::vector<std::pair<float, int>> order;
+  const float cam[3] = {(float)sc[0].cam_pos[0], (float)sc[0].cam_pos[1], (float)sc[0].cam_pos[2]};
+  for (int b = 0; b < nb; ++b) {
+    float c3[3];
+    for (int d = 0; d < 3; ++d) c3[d] = (float)((G[b].bmin[d] + G[b].bmax[d]) * 0.5);
+    const float dx = cam[0] - c3[0], dy = cam[1] - c3[1], dz = cam[2] - c3[2];
+    order.push_back({std::sqrt(dx * dx + dy * dy + dz * dz), b});
+  }
+  std::stable_sort(order.begin(), order.end(),
+                   [](const std::pair<float, int>& l, const std::pair<float, int>& r) { return l.first < r.first; });
+  const T* first = img.data() + (size_t)order[0].second * npx * 4;
+  for (int64_t i = 0; i < 4 * npx; ++i) rgba[i] = first[i];
+  for (int k = 1; k < nb; ++k) {
+    const T* bimg = img.data() + (size_t)order[k].second * npx * 4;
+    for (int64_t j = 0; j < npx; ++j) {
+      T* a = rgba + 4 * j;
+      const T* bb = bimg + 4 * j;
+      a[0] = a[0] + bb[0] * (T(1) - a[3]);
+      a[1] = a[1] + bb[1] * (T(1) - a[3]);
+      a[2] = a[2] + bb[2] * (T(1) - a[3]);
+      a[3] = a[3] + bb[3] * (T(1) - a[3]);
+    }
+  }
+  size_t off = 0;
+  for (int b = 0; b < nb; ++b) {
+    if (maps_local) std::copy(local[b].begin(), local[b].end(), maps_local + off);
+    if (maps_final) std::copy(fin[b].begin(), fin[b].end(), maps_final + off);
+    off += local[b].size();
+  }
+  if (imgs) std::copy(img.begin(), img.end(), imgs);
+  if (lit_out) *lit_out = lit;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int oracle_render_bricks_f32(const oracle_scene* scenes, int nbricks, float* maps_local, float* maps_final,
+                                        float* brick_images, float* rgba, int threads, uint64_t* lit) {
+  return render_bricks<float>(scenes, nbricks, maps_local, maps_final, brick_images, rgba, threads, lit);
+}
+extern "C" int oracle_render_bricks_f64(const oracle_scene* scenes, int nbricks, double* maps_local,
+                                        double* maps_final, double* brick_images, double* rgba, int threads,
+                                        uint64_t* lit) {
+  return render_bricks<double>(scenes, nbricks, maps_local, maps_final, brick_images, rgba, threads, lit);
+}
 
 // ---- synthetic inputs on the CPU (the reference arm's field) ---------------------
 // Same float32 operation sequence as the library's device generator

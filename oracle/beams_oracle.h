@@ -74,6 +74,15 @@ int oracle_view_march_lazy_f64(const oracle_scene* s, int x0, int y0, int w, int
 /* Per-pixel slab test (t_enter, t_exit; miss -> t_enter = -1). */
 int oracle_ray_setup_f32(const oracle_scene* s, int x, int y, float out[8]);
 
+/* Multi-block render: scenes[b] describes block b (its own field, dims, origin,
+ * spacing; camera, light, TF, map size shared). Outputs (each optional except
+ * rgba): per-block Phase-1 maps and stitched final maps concatenated in block
+ * order, per-block images (nbricks*W*H*4), the depth-ordered composite. */
+int oracle_render_bricks_f32(const oracle_scene* scenes, int nbricks, float* maps_local, float* maps_final,
+                             float* brick_images, float* rgba, int threads, uint64_t* lit);
+int oracle_render_bricks_f64(const oracle_scene* scenes, int nbricks, double* maps_local, double* maps_final,
+                             double* brick_images, double* rgba, int threads, uint64_t* lit);
+
 /* Gradient-noise field (x fastest), remapped to [0,1]; the reference arm's input. */
 int oracle_generate_noise(float* out, int nx, int ny, int nz, const unsigned char* perm, int octaves,
                           float f0, float lac, float gain, int threads);

@@ -47,6 +47,8 @@ def lib():
             "oracle_composite_f32": [P, C.c_int, C.c_int, P, P],
             "oracle_generate_noise": [P, C.c_int, C.c_int, C.c_int, P, C.c_int, C.c_float, C.c_float,
                                       C.c_float, C.c_int],
+            "oracle_render_bricks_f32": [P, C.c_int, P, P, P, P, C.c_int, u64p],
+            "oracle_render_bricks_f64": [P, C.c_int, P, P, P, P, C.c_int, u64p],
         }.items():
             f = getattr(L, name)
             f.argtypes = args
@@ -136,6 +138,26 @@ class Oracle:
         out = np.zeros(8, np.float32)
         lib().oracle_ray_setup_f32(C.byref(self.cs), x, y, _p(out))
         return out
+
+
+def render_bricks(bricks, fp64: bool = False, threads: int = 0):
+    """Multi-block render of a list of brick scenes (scenes.split_bricks).
+    Returns (rgba, brick_images, local_maps, final_maps, lit)."""
+    orcs = [Oracle(b, threads=threads) for b in bricks]
+    arr = (OracleScene * len(bricks))(*[o.cs for o in orcs])
+    dt = np.float64 if fp64 else np.float32
+    W, H = bricks[0].width, bricks[0].height
+    nverts = [int(np.prod(o.map_shape)) for o in orcs]
+    local = np.zeros(sum(nverts), dt)
+    final = np.zeros(sum(nverts), dt)
+    imgs = np.zeros((len(bricks), H, W, 4), dt)
+    rgba = np.zeros((H, W, 4), dt)
+    lit = C.c_uint64()
+    fn = lib().oracle_render_bricks_f64 if fp64 else lib().oracle_render_bricks_f32
+    if fn(C.cast(arr, C.c_void_p), len(bricks), _p(local), _p(final), _p(imgs), _p(rgba), threads, C.byref(lit)):
+        raise RuntimeError("oracle brick render rejected the scenes")
+    split = np.cumsum(nverts)[:-1]
+    return rgba, imgs, np.split(local, split), np.split(final, split), lit.value
 
 
 def composite(images: np.ndarray, order) -> np.ndarray:

@@ -91,6 +91,8 @@ def lib():
         "beams_generate_blobs": ([P, P, P, C.c_int, C.c_int, P], C.c_int),
         "beams_selftest_division": ([C.c_float, C.c_float, C.c_int, C.c_int, C.POINTER(C.c_ulonglong),
                                      C.POINTER(C.c_ulonglong)], C.c_int),
+        "beams_set_bricks": ([P, P, C.c_int], C.c_int),
+        "beams_get_brick_map": ([P, C.c_int, C.c_int, P, C.c_size_t, C.c_int], C.c_int),
         "beams_generate_noise": ([P, P, P, C.c_int, C.c_float, C.c_float, C.c_float, P], C.c_int),
     }
     for name, (args, res) in sig.items():
@@ -188,6 +190,29 @@ class Renderer:
         v = Volume(ptr, dtype, (C.c_int * 3)(*dims), _d3(origin), _d3(spacing),
                    (C.c_double * 2)(*value_range), assoc, on_device)
         self._check(self._L.beams_set_volume(self._h, C.byref(v)))
+
+    def set_bricks(self, bricks):
+        """bricks: list of (array (z,y,x) float32 numpy or torch CUDA tensor, origin, spacing, value_range)."""
+        vols = (Volume * len(bricks))()
+        self._keep_bricks = []
+        for i, (data, origin, spacing, vrange) in enumerate(bricks):
+            if isinstance(data, np.ndarray):
+                arr = np.ascontiguousarray(data, np.float32)
+                self._keep_bricks.append(arr)
+                ptr, on_dev = arr.ctypes.data_as(C.c_void_p), 0
+                nz, ny, nx = arr.shape
+            else:
+                self._keep_bricks.append(data)
+                ptr, on_dev = C.c_void_p(data.data_ptr()), int(data.is_cuda)
+                nz, ny, nx = data.shape
+            vols[i] = Volume(ptr, F32, (C.c_int * 3)(nx, ny, nz), _d3(origin), _d3(spacing),
+                             (C.c_double * 2)(*vrange), ASSOC_POINTS, on_dev)
+        self._check(self._L.beams_set_bricks(self._h, C.cast(vols, C.c_void_p), len(bricks)))
+
+    def get_brick_map(self, brick: int, stage: int, count: int):
+        m = np.empty(count, np.float32)
+        self._check(self._L.beams_get_brick_map(self._h, brick, stage, _ptr(m), m.size, 0))
+        return m
 
     def set_color_map(self, rgba):
         t = np.ascontiguousarray(rgba, dtype=np.float32).reshape(-1, 4)

@@ -7,6 +7,7 @@
 // single block, :1210-1256, which yields the same map), then the view march.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -62,9 +63,8 @@ static bool finite3(const double* v) {
 
 // Derives the kernel parameters exactly as the reference derives them
 // (float32 arithmetic; see the cited lines in beams_params.h).
-beams_status make_geo(beams_renderer* r, const beams_camera* cam, ExactGeo& g) {
+beams_status make_geo_vol(beams_renderer* r, const beams_volume& v, const beams_camera* cam, ExactGeo& g) {
   std::memset(&g, 0, sizeof(g));
-  const beams_volume& v = r->vol;
   for (int d = 0; d < 3; ++d) {
     g.n[d] = v.dims[d];
     g.org[d] = (float)v.origin[d];
@@ -160,6 +160,10 @@ beams_status make_geo(beams_renderer* r, const beams_camera* cam, ExactGeo& g) {
   return BEAMS_OK;
 }
 
+beams_status make_geo(beams_renderer* r, const beams_camera* cam, ExactGeo& g) {
+  return make_geo_vol(r, r->vol, cam, g);
+}
+
 beams_status validate_camera(beams_renderer* r, const beams_camera* cam) {
   if (!cam) return fail(r, BEAMS_ERR_INVALID_ARG, "camera is NULL");
   if (cam->width < 1 || cam->height < 1 || cam->width > 16384 || cam->height > 16384)
@@ -183,6 +187,33 @@ static void map_key(const beams_renderer* r, MapKey& k) {
     k.light_kind = r->lights[0].kind;
     for (int d = 0; d < 3; ++d) k.light[d] = r->lights[0].v[d];
   }
+}
+
+// Derived layouts of one field: cell tables and (point fields) the quad copy.
+static beams_status prepare_layouts_for(beams_renderer* r, const ExactGeo& g, int assoc, const void* d_field,
+                                        unsigned long long version, float4** d_tab, size_t* tab_cap,
+                                        unsigned long long tab_key[4], float4** d_quads, size_t* quads_cap,
+                                        unsigned long long* quads_version, int& launches) {
+  const unsigned long long key[4] = {version, (unsigned long long)r->map_m[0], (unsigned long long)r->map_m[1],
+                                     (unsigned long long)r->map_m[2]};
+  if (std::memcmp(key, tab_key, sizeof(key)) != 0) {
+    beams_status s = ensure_buffer(r, (void**)d_tab, tab_cap, (size_t)g.ntab * sizeof(float4), "allocating cell tables");
+    if (s != BEAMS_OK) return s;
+    cudaError_t e = launch_build_tables(g, *d_tab, r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "cell table build");
+    ++launches;
+    std::memcpy(tab_key, key, sizeof(key));
+  }
+  if (assoc == BEAMS_ASSOC_POINTS && *quads_version != version) {
+    const size_t nq = (size_t)(g.n[0] - 1) * (g.n[1] - 1) * g.n[2];
+    beams_status s = ensure_buffer(r, (void**)d_quads, quads_cap, nq * sizeof(float4), "allocating quad field");
+    if (s != BEAMS_OK) return s;
+    cudaError_t e = launch_build_quads((const float*)d_field, *d_quads, g.n, r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "quad field build");
+    ++launches;
+    *quads_version = version;
+  }
+  return BEAMS_OK;
 }
 
 // Builds the derived layouts the kernels read: cell tables (per frame geometry)
@@ -231,7 +262,29 @@ beams_status build_map(beams_renderer* r, const ExactGeo& g, int& launches, bool
   return BEAMS_OK;
 }
 
+static beams_status check_sizes(beams_renderer* r, const beams_volume& v) {
+  const double nq = (double)(v.dims[0] - 1) * (v.dims[1] - 1) * v.dims[2];
+  if (nq >= 4294967296.0) return fail(r, BEAMS_ERR_UNSUPPORTED, "volume too large for 32-bit cell indexing");
+  const double nv = (double)(r->map_m[0] + 1) * (r->map_m[1] + 1) * (r->map_m[2] + 1);
+  if (nv >= 2147483648.0) return fail(r, BEAMS_ERR_UNSUPPORTED, "shadow map too large (vertices >= 2^31)");
+  const int ntab = v.dims[0] + v.dims[1] + v.dims[2] - 3 + r->map_m[0] + r->map_m[1] + r->map_m[2];
+  if ((size_t)(ntab + 1024) * 16 > 200 * 1024)
+    return fail(r, BEAMS_ERR_UNSUPPORTED, "volume/map axes too long for the shared-memory cell tables");
+  return BEAMS_OK;
+}
+
 beams_status check_ready(beams_renderer* r) {
+  if (r->brick_mode) {
+    if (r->bricks.empty()) return fail(r, BEAMS_ERR_STATE, "no bricks set (beams_set_bricks)");
+    if (r->tf_n < 1) return fail(r, BEAMS_ERR_STATE, "no colour map set (beams_set_color_map)");
+    if (r->use_map && r->lights.empty()) return fail(r, BEAMS_ERR_STATE, "shadow map enabled but no light added");
+    if (r->form != BEAMS_FORM_EXACT) return fail(r, BEAMS_ERR_UNSUPPORTED, "bricks render in the exact form only");
+    for (auto& b : r->bricks) {
+      beams_status s = check_sizes(r, b.vol);
+      if (s != BEAMS_OK) return s;
+    }
+    return BEAMS_OK;
+  }
   if (!r->has_volume) return fail(r, BEAMS_ERR_STATE, "no volume set (beams_set_volume)");
   if (r->tf_n < 1) return fail(r, BEAMS_ERR_STATE, "no colour map set (beams_set_color_map)");
   if (r->use_map && r->vol.assoc == BEAMS_ASSOC_POINTS && r->lights.empty())
@@ -245,6 +298,136 @@ beams_status check_ready(beams_renderer* r) {
   const int ntab = r->vol.dims[0] + r->vol.dims[1] + r->vol.dims[2] - 3 + r->map_m[0] + r->map_m[1] + r->map_m[2];
   if ((size_t)(ntab + 1024) * 16 > 200 * 1024)
     return fail(r, BEAMS_ERR_UNSUPPORTED, "volume/map axes too long for the shared-memory cell tables");
+  return BEAMS_OK;
+}
+
+// One frame of a multi-block scene: Phase 1 local maps, Phases 2-3 stitched
+// maps, Phase 4 per-brick view marches, Phase 5 depth-ordered composite.
+beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* out, int& launches) {
+  const int nb = (int)r->bricks.size();
+  std::vector<ExactGeo> G(nb);
+  for (int b = 0; b < nb; ++b) {
+    Brick& B = r->bricks[b];
+    beams_status s = make_geo_vol(r, B.vol, cam, G[b]);
+    if (s != BEAMS_OK) return s;
+    s = prepare_layouts_for(r, G[b], B.vol.assoc, B.d_field, B.version, &B.d_tab, &B.tab_cap, B.tab_key,
+                            &B.d_quads, &B.quads_cap, &B.quads_version, launches);
+    if (s != BEAMS_OK) return s;
+  }
+  const size_t npix = (size_t)cam->width * cam->height;
+  beams_status s = ensure_buffer(r, (void**)&r->d_brick_imgs, &r->brick_imgs_cap, (size_t)nb * npix * sizeof(float4),
+                                 "allocating brick images");
+  if (s != BEAMS_OK) return s;
+  cudaError_t e;
+  if (r->use_map) {
+    std::vector<BrickRef> refs(nb);
+    for (int b = 0; b < nb; ++b) {
+      Brick& B = r->bricks[b];
+      const size_t nv = (size_t)G[b].pd[0] * G[b].pd[1] * G[b].pd[2];
+      s = ensure_buffer(r, (void**)&B.d_map_local, &B.local_cap, nv * sizeof(float), "allocating brick map");
+      if (s == BEAMS_OK) s = ensure_buffer(r, (void**)&B.d_map_final, &B.final_cap, nv * sizeof(float), "allocating brick map");
+      if (s != BEAMS_OK) return s;
+      B.map_count = nv;
+      e = launch_light_march_f32(G[b], B.d_quads, B.d_tab, r->d_tf, B.d_map_local, r->d_cnt, r->stream);
+      if (e != cudaSuccess) return cuda_fail(r, e, "brick light march");
+      ++launches;
+      BrickRef& R = refs[b];
+      for (int d = 0; d < 3; ++d) {
+        R.bmin[d] = G[b].bmin[d];
+        R.bmax[d] = G[b].bmax[d];
+        R.morig[d] = G[b].morig[d];
+        R.msp[d] = G[b].msp[d];
+        R.minv[d] = G[b].minv[d];
+        R.pd[d] = G[b].pd[d];
+      }
+      R.map = B.d_map_local;
+    }
+    s = ensure_buffer(r, (void**)&r->d_refs, &r->refs_cap, nb * sizeof(BrickRef), "allocating brick table");
+    if (s != BEAMS_OK) return s;
+    e = cudaMemcpyAsync(r->d_refs, refs.data(), nb * sizeof(BrickRef), cudaMemcpyHostToDevice, r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "copying brick table");
+    for (int b = 0; b < nb; ++b) {
+      Brick& B = r->bricks[b];
+      e = launch_light_march_f32(G[b], B.d_quads, B.d_tab, r->d_tf, B.d_map_final, r->d_cnt, r->stream, r->d_refs,
+                                 nb, b);
+      if (e != cudaSuccess) return cuda_fail(r, e, "brick stitch march");
+      ++launches;
+    }
+  }
+  cudaEventRecord(r->ev[1], r->stream);
+  for (int b = 0; b < nb; ++b) {
+    Brick& B = r->bricks[b];
+    e = cudaMemsetAsync(&r->d_cnt->tiles_view, 0, sizeof(unsigned), r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "clearing tile counter");
+    e = launch_view_march_f32(G[b], (const float*)B.d_field, B.d_quads, B.d_tab, r->d_tf,
+                              r->use_map ? B.d_map_final : nullptr, r->d_brick_imgs + (size_t)b * npix, r->d_cnt,
+                              r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "brick view march");
+    ++launches;
+  }
+  cudaEventRecord(r->ev[2], r->stream);
+  // Depth order: |camera - block centre| in float (MapperLightedVolume.cxx:221-241).
+  std::vector<std::pair<float, int>> order;
+  const float cp[3] = {(float)cam->position[0], (float)cam->position[1], (float)cam->position[2]};
+  for (int b = 0; b < nb; ++b) {
+    float c3[3];
+    for (int d = 0; d < 3; ++d) c3[d] = (float)((G[b].bmin[d] + G[b].bmax[d]) * 0.5);
+    const float dx = cp[0] - c3[0], dy = cp[1] - c3[1], dz = cp[2] - c3[2];
+    order.push_back({std::sqrt(dx * dx + dy * dy + dz * dz), b});
+  }
+  std::stable_sort(order.begin(), order.end(),
+                   [](const std::pair<float, int>& l, const std::pair<float, int>& q) { return l.first < q.first; });
+  int idx[kMaxBricks];
+  for (int b = 0; b < nb; ++b) idx[b] = order[b].second;
+  e = launch_composite(r->d_brick_imgs, nb, npix, idx, out, r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "brick composite");
+  ++launches;
+  return BEAMS_OK;
+}
+
+// beams_render for a multi-block scene: output handling and timings around render_bricks.
+beams_status render_bricks_frame(beams_renderer* r, const beams_camera* cam, float* rgba_out, int out_on_device,
+                                 beams_timings* t, int& launches) {
+  const size_t npix = (size_t)cam->width * cam->height;
+  float4* dst = (float4*)rgba_out;
+  const bool direct = out_on_device && (((uintptr_t)rgba_out & 15) == 0);
+  beams_status s;
+  if (!direct) {
+    s = ensure_buffer(r, (void**)&r->d_rgba, &r->rgba_cap, npix * sizeof(float4), "allocating image");
+    if (s != BEAMS_OK) return s;
+    dst = r->d_rgba;
+  }
+  s = render_bricks(r, cam, dst, launches);
+  if (s != BEAMS_OK) return s;
+  cudaError_t e;
+  if (!direct) {
+    e = cudaMemcpyAsync(rgba_out, dst, npix * sizeof(float4),
+                        out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "copying image out");
+  }
+  cudaEventRecord(r->ev[3], r->stream);
+  if (t) {
+    std::memset(t, 0, sizeof(*t));
+    e = cudaStreamSynchronize(r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "render");
+    Counters c;
+    e = cudaMemcpy(&c, r->d_cnt, sizeof(c), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(r, e, "reading counters");
+    cudaEventElapsedTime(&t->map_build_ms, r->ev[0], r->ev[1]);
+    cudaEventElapsedTime(&t->view_march_ms, r->ev[1], r->ev[2]);
+    cudaEventElapsedTime(&t->composite_ms, r->ev[2], r->ev[3]);
+    cudaEventElapsedTime(&t->total_ms, r->ev[0], r->ev[3]);
+    t->light_samples = c.light_samples;
+    t->lit_samples = c.lit_samples;
+    t->rays_hit = c.rays_hit;
+    size_t nv = 0;
+    for (auto& b : r->bricks) nv += r->use_map ? b.map_count : 0;
+    t->map_vertices = (int)nv;
+    t->kernel_launches = launches;
+  } else if (!out_on_device) {
+    e = cudaStreamSynchronize(r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "render");
+  }
   return BEAMS_OK;
 }
 
@@ -336,6 +519,7 @@ beams_status beams_set_volume(beams_renderer* r, const beams_volume* v) {
   r->vol.on_device = 1;
   r->field_bytes = bytes;
   r->has_volume = true;
+  r->brick_mode = false;
   ++r->volume_version;
   return BEAMS_OK;
 }
@@ -514,13 +698,14 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
   if (s != BEAMS_OK) return s;
   cudaSetDevice(r->device);
   ExactGeo g;
-  s = make_geo(r, cam, g);
+  s = make_geo_vol(r, r->brick_mode ? r->bricks[0].vol : r->vol, cam, g);
   if (s != BEAMS_OK) return s;
   int launches = 0;
   cudaError_t e = cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "clearing counters");
   cudaEventRecord(r->ev[0], r->stream);
   bool built = false;
+  if (r->brick_mode) return render_bricks_frame(r, cam, rgba_out, out_on_device, t, launches);
   s = prepare_layouts(r, g, launches);
   if (s != BEAMS_OK) return s;
   const bool need_map = r->use_map && r->vol.assoc == BEAMS_ASSOC_POINTS;
@@ -570,6 +755,64 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
     e = cudaStreamSynchronize(r->stream);
     if (e != cudaSuccess) return cuda_fail(r, e, "render");
   }
+  return BEAMS_OK;
+}
+
+beams_status beams_set_bricks(beams_renderer* r, const beams_volume* bricks, int nbricks) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  if (!bricks || nbricks < 1 || nbricks > kMaxBricks)
+    return fail(r, BEAMS_ERR_INVALID_ARG, "bricks: need 1..32 volumes");
+  for (int b = 0; b < nbricks; ++b) {
+    const beams_volume& v = bricks[b];
+    if (!v.data || v.dtype != BEAMS_F32 || v.assoc != BEAMS_ASSOC_POINTS)
+      return fail(r, BEAMS_ERR_INVALID_ARG, "bricks: each brick must be a float32 point field");
+    for (int d = 0; d < 3; ++d)
+      if (v.dims[d] < 2 || v.dims[d] > 8192 || !(v.spacing[d] > 0.0) || !std::isfinite(v.spacing[d]) ||
+          !std::isfinite(v.origin[d]))
+        return fail(r, BEAMS_ERR_INVALID_ARG, "bricks: bad dims/origin/spacing");
+    if (!std::isfinite(v.range[0]) || !std::isfinite(v.range[1]))
+      return fail(r, BEAMS_ERR_INVALID_ARG, "bricks: range must be finite");
+  }
+  cudaSetDevice(r->device);
+  for (auto& b : r->bricks) b.release();
+  r->bricks.assign(nbricks, Brick());
+  for (int b = 0; b < nbricks; ++b) {
+    Brick& B = r->bricks[b];
+    const beams_volume& v = bricks[b];
+    const size_t bytes = (size_t)v.dims[0] * v.dims[1] * v.dims[2] * sizeof(float);
+    if (v.on_device) {
+      B.d_field = v.data;
+    } else {
+      beams_status s = ensure_buffer(r, &B.d_field_owned, &B.field_cap, bytes, "allocating brick field");
+      if (s != BEAMS_OK) return s;
+      cudaError_t e = cudaMemcpyAsync(B.d_field_owned, v.data, bytes, cudaMemcpyHostToDevice, r->stream);
+      if (e != cudaSuccess) return cuda_fail(r, e, "copying brick field");
+      B.d_field = B.d_field_owned;
+    }
+    B.vol = v;
+    B.vol.data = B.d_field;
+    B.vol.on_device = 1;
+    B.version = ++r->brick_counter;
+  }
+  r->brick_mode = true;
+  r->map_valid = false;
+  return BEAMS_OK;
+}
+
+beams_status beams_get_brick_map(beams_renderer* r, int brick, int stage, float* dst, size_t count,
+                                 int dst_on_device) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  if (!r->brick_mode || brick < 0 || brick >= (int)r->bricks.size())
+    return fail(r, BEAMS_ERR_INVALID_ARG, "no such brick");
+  Brick& B = r->bricks[brick];
+  const float* src = stage ? B.d_map_final : B.d_map_local;
+  if (!src || B.map_count == 0) return fail(r, BEAMS_ERR_STATE, "brick map not built yet");
+  if (!dst || count < B.map_count) return fail(r, BEAMS_ERR_INVALID_ARG, "destination too small for the map");
+  cudaSetDevice(r->device);
+  cudaError_t e = cudaMemcpyAsync(dst, src, B.map_count * sizeof(float),
+                                  dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, r->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "copying brick map");
   return BEAMS_OK;
 }
 

@@ -45,6 +45,17 @@ struct ExactGeo {
   int ntab;        // total table entries
 };
 
+// What the stitch kernel needs of every other brick (multi-block scenes): its
+// bounds (for SegmentAABB) and its Phase-1 map with that map's geometry.
+struct BrickRef {
+  double bmin[3], bmax[3];
+  float morig[3], msp[3], minv[3];
+  int pd[3];
+  const float* map;
+};
+
+constexpr int kMaxBricks = 32;
+
 // Counters written by the kernels (one atomic per warp).
 struct Counters {
   unsigned long long light_samples;

@@ -50,8 +50,8 @@ template <> struct FieldLoad<float> {
 
 // SegmentAABB (Intersections.cxx:9-48). The slab ratios are formed in double
 // because vtkm::Bounds holds doubles, then stored to float.
-__device__ __forceinline__ void segment_aabb(const ExactGeo& g, const float a[3], const float b[3],
-                                             float& tmin, float& tmax) {
+__device__ __forceinline__ void segment_aabb_b(const double bmin[3], const double bmax[3], const float a[3],
+                                               const float b[3], float& tmin, float& tmax) {
   float dir[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
   const float len = sqrtf(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
   dir[0] = dir[0] / len;
@@ -61,13 +61,76 @@ __device__ __forceinline__ void segment_aabb(const ExactGeo& g, const float a[3]
   tmax = __int_as_float(0x7f800000);
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const float t0 = (float)((g.bmin[d] - (double)a[d]) / (double)dir[d]);
-    const float t1 = (float)((g.bmax[d] - (double)a[d]) / (double)dir[d]);
+    const float t0 = (float)((bmin[d] - (double)a[d]) / (double)dir[d]);
+    const float t1 = (float)((bmax[d] - (double)a[d]) / (double)dir[d]);
     tmin = mx(tmin, mn(t0, t1));
     tmax = mn(tmax, mx(t0, t1));
   }
   if (tmin < 0.f) tmin = 1e-4f;
   if (tmax > len) tmax = len;
+}
+
+__device__ __forceinline__ void segment_aabb(const ExactGeo& g, const float a[3], const float b[3], float& tmin,
+                                             float& tmax) {
+  segment_aabb_b(g.bmin, g.bmax, a, b, tmin, tmax);
+}
+
+// GetEstimateUsingVerticesT of another brick's Phase-1 map at p
+// (TransmittanceMap.h:93-112, :200-229; TransmittanceFetcher2 :505-508).
+__device__ __forceinline__ float brick_map_opacity(const BrickRef& R, const float p[3]) {
+  int c[3];
+  float pc[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    float t = (p[d] - R.morig[d]) * R.minv[d];
+    if (t < 0.f) t = 0.f;
+    if (t >= (float)(R.pd[d] - 1)) t = (float)(R.pd[d] - 2);
+    c[d] = (int)t;
+    const float lo = R.morig[d] + R.msp[d] * (float)c[d];
+    const float hi = R.morig[d] + R.msp[d] * (float)(c[d] + 1);
+    pc[d] = (p[d] - lo) / (hi - lo);
+  }
+  const unsigned px = (unsigned)R.pd[0], pxy = (unsigned)R.pd[0] * (unsigned)R.pd[1];
+  const float* m = R.map + ((unsigned)c[2] * pxy + (unsigned)c[1] * px + (unsigned)c[0]);
+  float v[8] = {__ldg(m), __ldg(m + 1), __ldg(m + 1 + px), __ldg(m + px), __ldg(m + pxy), __ldg(m + pxy + 1),
+                __ldg(m + pxy + 1 + px), __ldg(m + pxy + px)};
+  return hex_interp(v, pc[0], pc[1], pc[2]);
+}
+
+// Cross-brick shadow prefix of one vertex ray (the reference's Phases 2-3,
+// LightedVolumeRenderer.cxx:968-1235, TransmittanceMap.h:387-453): every other
+// brick the segment light->vertex crosses (SegmentAABB hit, glancing hits
+// included) contributes its Phase-1 map opacity at the segment's exit point;
+// contributions are over-composited in increasing exit distance (HitSort;
+// ties by brick id). The over operator on opacity is a product of
+// transmittances, so no cross-brick exchange or sort of hit lists is needed.
+__device__ __forceinline__ float stitch_prefix(const BrickRef* __restrict__ refs, int nrefs, int self,
+                                               const float L[3], const float V[3], const float dir[3]) {
+  float ht[kMaxBricks], ho[kMaxBricks];
+  int hb[kMaxBricks];
+  int nh = 0;
+  for (int c = 0; c < nrefs; ++c) {
+    if (c == self) continue;
+    const BrickRef& R = refs[c];
+    float tmin, tmax;
+    segment_aabb_b(R.bmin, R.bmax, L, V, tmin, tmax);
+    if (!(tmin <= tmax)) continue;
+    const float P[3] = {L[0] + dir[0] * tmax, L[1] + dir[1] * tmax, L[2] + dir[2] * tmax};
+    const float op = brick_map_opacity(R, P);
+    int j = nh++;
+    while (j > 0 && (tmax < ht[j - 1] || (tmax == ht[j - 1] && c < hb[j - 1]))) {
+      ht[j] = ht[j - 1];
+      ho[j] = ho[j - 1];
+      hb[j] = hb[j - 1];
+      --j;
+    }
+    ht[j] = tmax;
+    ho[j] = op;
+    hb[j] = c;
+  }
+  float o = 0.f;
+  for (int i = 0; i < nh; ++i) o = o + (1.f - o) * ho[i];
+  return o;
 }
 
 // Map vertex position (uniform point coordinates of the opacity map).

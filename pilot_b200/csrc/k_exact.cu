@@ -35,12 +35,17 @@ __device__ __forceinline__ void load_tables(float4* s_tab, const float4* __restr
 // ---------------------------------------------------------------------------
 // K1
 // ---------------------------------------------------------------------------
-template <typename QuadT>
+// STITCH: the multi-brick Phase 3 — the march starts from the cross-brick
+// prefix (stitch_prefix) instead of zero, as GenerateEstimator is re-run on
+// the prefix opacities (LightedVolumeRenderer.cxx:1241-1252).
+template <typename QuadT, bool STITCH>
 __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, const QuadT* __restrict__ quads,
                                                           const float4* __restrict__ tab,
                                                           const float4* __restrict__ tf,
                                                           float* __restrict__ map, int nvert,
-                                                          Counters* __restrict__ cnt) {
+                                                          Counters* __restrict__ cnt,
+                                                          const BrickRef* __restrict__ refs, int nrefs,
+                                                          int self) {
   extern __shared__ float4 s_dyn[];
   const int nfield = g.max_off[0];             // field-axis table entries only
   float4* s_tab = s_dyn;
@@ -104,7 +109,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
       pc[2] = div_rn_markstein(s[2] - e2.x, e2.z, e2.w);
       return true;
     };
-    float o = 0.f;
+    float o = STITCH ? stitch_prefix(refs, nrefs, self, L, V, dir) : 0.f;
     float va[8], pa[3], vb[8], pb[3];
     bool ok = gen(va, pa);
     while (ok) {
@@ -455,14 +460,54 @@ cudaError_t launch_build_quads(const float* field, float4* quads, const int n[3]
 }
 
 cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
-                                   float* map, Counters* cnt, cudaStream_t st) {
+                                   float* map, Counters* cnt, cudaStream_t st, const BrickRef* refs, int nrefs,
+                                   int self) {
   const int nvert = g.pd[0] * g.pd[1] * g.pd[2];
   const size_t smem = (size_t)g.max_off[0] * sizeof(float4) + (size_t)g.tf_n * sizeof(float);
   const int ntiles = (nvert + kThreads - 1) / kThreads;
   int grid = 0;
-  cudaError_t e = persistent_grid(k_light_march<float4>, smem, ntiles, grid);
-  if (e != cudaSuccess) return e;
-  k_light_march<float4><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, map, nvert, cnt);
+  cudaError_t e;
+  if (refs) {
+    e = persistent_grid(k_light_march<float4, true>, smem, ntiles, grid);
+    if (e != cudaSuccess) return e;
+    k_light_march<float4, true><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, map, nvert, cnt, refs, nrefs, self);
+  } else {
+    e = persistent_grid(k_light_march<float4, false>, smem, ntiles, grid);
+    if (e != cudaSuccess) return e;
+    k_light_march<float4, false><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, map, nvert, cnt, nullptr, 0, -1);
+  }
+  return cudaGetLastError();
+}
+
+// K6: sort-last composite of nb brick images in the given order
+// (MapperLightedVolume.cxx:284-297): a.rgb += b.rgb*(1-a.a), then a.a += b.a*(1-a.a).
+struct CompositeOrder {
+  int idx[kMaxBricks];
+};
+
+__global__ void k_composite(const float4* __restrict__ imgs, int nb, size_t npix, CompositeOrder order,
+                            float4* __restrict__ out) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += (size_t)gridDim.x * blockDim.x) {
+    float4 a = imgs[(size_t)order.idx[0] * npix + i];
+    for (int k = 1; k < nb; ++k) {
+      const float4 b = imgs[(size_t)order.idx[k] * npix + i];
+      a.x = a.x + b.x * (1.f - a.w);
+      a.y = a.y + b.y * (1.f - a.w);
+      a.z = a.z + b.z * (1.f - a.w);
+      a.w = a.w + b.w * (1.f - a.w);
+    }
+    out[i] = a;
+  }
+}
+
+cudaError_t launch_composite(const float4* imgs, int nb, size_t npix, const int* order, float4* out,
+                             cudaStream_t st) {
+  if (nb < 1 || nb > kMaxBricks) return cudaErrorInvalidValue;
+  CompositeOrder o;
+  for (int i = 0; i < kMaxBricks; ++i) o.idx[i] = i < nb ? order[i] : 0;
+  size_t blocks = (npix + 255) / 256;
+  const size_t cap = (size_t)num_sms() * 8;
+  k_composite<<<(unsigned)(blocks < cap ? blocks : cap), 256, 0, st>>>(imgs, nb, npix, o, out);
   return cudaGetLastError();
 }
 

@@ -10,7 +10,10 @@ namespace beams {
 cudaError_t launch_build_tables(const ExactGeo& g, float4* tab, cudaStream_t st);
 cudaError_t launch_build_quads(const float* field, float4* quads, const int n[3], cudaStream_t st);
 cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
-                                   float* map, Counters* cnt, cudaStream_t st);
+                                   float* map, Counters* cnt, cudaStream_t st, const BrickRef* refs = nullptr,
+                                   int nrefs = 0, int self = -1);
+cudaError_t launch_composite(const float4* imgs, int nb, size_t npix, const int* order, float4* out,
+                             cudaStream_t st);
 cudaError_t launch_view_march_f32(const ExactGeo& g, const float* field, const float4* quads, const float4* tab,
                                   const float4* tf, const float* map, float4* out, Counters* cnt, cudaStream_t st);
 cudaError_t launch_selftest_division(float org, float h, int ncells, int samples, unsigned long long* d_out,

@@ -21,6 +21,38 @@ struct Light {
   float intensity = 1.f;
 };
 
+// One block of a multi-block scene: its own field and derived buffers (the
+// reference holds one block per MPI rank; here all blocks share one GPU).
+struct Brick {
+  beams_volume vol{};
+  void* d_field_owned = nullptr;
+  size_t field_cap = 0;
+  const void* d_field = nullptr;
+  unsigned long long version = 0;
+  float4* d_quads = nullptr;
+  size_t quads_cap = 0;
+  unsigned long long quads_version = 0;
+  float4* d_tab = nullptr;
+  size_t tab_cap = 0;
+  unsigned long long tab_key[4] = {0, 0, 0, 0};
+  float* d_map_local = nullptr;
+  size_t local_cap = 0;
+  float* d_map_final = nullptr;
+  size_t final_cap = 0;
+  size_t map_count = 0;
+  void release() {
+    if (d_field_owned) cudaFree(d_field_owned);
+    if (d_quads) cudaFree(d_quads);
+    if (d_tab) cudaFree(d_tab);
+    if (d_map_local) cudaFree(d_map_local);
+    if (d_map_final) cudaFree(d_map_final);
+    d_field_owned = d_quads = nullptr;
+    d_quads = nullptr;
+    d_tab = nullptr;
+    d_map_local = d_map_final = nullptr;
+  }
+};
+
 struct MapKey {
   unsigned long long volume_version;
   unsigned long long tf_version;
@@ -83,6 +115,15 @@ struct beams_renderer {
   size_t tab_cap = 0;
   unsigned long long tab_key[4] = {0, 0, 0, 0};  // volume_version, map m[3] packed
 
+  // multi-block scene (beams_set_bricks)
+  std::vector<beams::Brick> bricks;
+  bool brick_mode = false;
+  beams::BrickRef* d_refs = nullptr;
+  size_t refs_cap = 0;
+  float4* d_brick_imgs = nullptr;
+  size_t brick_imgs_cap = 0;
+  unsigned long long brick_counter = 0;
+
   // image + counters + timing
   float4* d_rgba = nullptr;
   size_t rgba_cap = 0;
@@ -96,6 +137,9 @@ struct beams_renderer {
     if (d_quads) cudaFree(d_quads);
     if (d_tab) cudaFree(d_tab);
     if (d_rgba) cudaFree(d_rgba);
+    for (auto& b : bricks) b.release();
+    if (d_refs) cudaFree(d_refs);
+    if (d_brick_imgs) cudaFree(d_brick_imgs);
     if (d_cnt) cudaFree(d_cnt);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);

@@ -146,8 +146,12 @@ class Scene:
     octaves: int = 4
     base_freq: float = 4.0
 
+    brick_spacing: tuple | None = None
+
     @property
     def spacing(self):
+        if self.brick_spacing is not None:
+            return self.brick_spacing
         return tuple(1.0 / (d - 1) for d in self.dims)
 
     def field_numpy(self) -> np.ndarray:
@@ -252,3 +256,30 @@ def small(seed: int = 0, n: int = 24, image: int = 48, m: int = 12, kind: str = 
     return Scene(name=f"small_{kind}{n}", dims=(n, n, n), kind=kind, params=params, tf=tf_table(),
                  light_kind=light_kind, light=light, map_m=m, sample_distance=0.5 / (n - 1), cutoff=cutoff,
                  cam_pos=pos, cam_up=up, width=image, height=image, base_freq=2.0)
+
+
+def split_bricks(s: Scene, splits=(2, 2, 2)) -> list:
+    """Splits a scene's field into bricks, one dataset per brick as the reference's
+    ranks hold them: the cells of each axis are cut into `splits` contiguous runs
+    and neighbouring bricks share the point plane between them. Each brick keeps
+    the scene's camera, light, TF, map size and sample distance."""
+    from dataclasses import replace
+    field = s.field_numpy()
+    nx, ny, nz = s.dims
+    h = s.spacing
+    cuts = []
+    for n, k in zip((nx, ny, nz), splits):
+        cells = n - 1
+        edges = [round(i * cells / k) for i in range(k + 1)]
+        cuts.append([(edges[i], edges[i + 1]) for i in range(k)])  # cell ranges [a, b)
+    bricks = []
+    for (z0, z1) in cuts[2]:
+        for (y0, y1) in cuts[1]:
+            for (x0, x1) in cuts[0]:
+                sub = np.ascontiguousarray(field[z0:z1 + 1, y0:y1 + 1, x0:x1 + 1])
+                org = (s.origin[0] + x0 * h[0], s.origin[1] + y0 * h[1], s.origin[2] + z0 * h[2])
+                b = replace(s, name=f"{s.name}_brick{len(bricks)}", dims=(x1 - x0 + 1, y1 - y0 + 1, z1 - z0 + 1),
+                            kind="array", params=None, array=sub, origin=org)
+                b.brick_spacing = h
+                bricks.append(b)
+    return bricks

@@ -50,6 +50,13 @@ typedef enum beams_assoc { BEAMS_ASSOC_POINTS = 0, BEAMS_ASSOC_CELLS = 1 } beams
  * map build and lookup by a trained transmittance network. */
 typedef enum beams_form { BEAMS_FORM_EXACT = 0, BEAMS_FORM_PRECISION = 1, BEAMS_FORM_MLP = 2 } beams_form;
 
+/* Options of BEAMS_FORM_PRECISION: the dtype the field is stored and read in
+ * (BEAMS_BF16 or BEAMS_F16) when the volume is given in float32; a 16-bit
+ * volume is used as given. The map is binary16 transmittance exp(-tau). */
+typedef struct beams_precision_options {
+  int field_dtype;
+} beams_precision_options;
+
 /* A structured scalar volume on a uniform grid. The renderer builds the same
  * float32 rectilinear coordinate arrays the reference scenes build
  * (origin + i*spacing, beams/sources/Spheres.cxx:144-156). */

@@ -88,6 +88,8 @@ struct Geo {
   const float* field;
   int use_map;
   int slab_fp64;
+  int precision;
+  std::vector<T> tau;  // -ln(1 - a_i) per TF entry (precision form)
   // camera
   T cam_pos[3], cf[3], cr[3], cu[3], kx, cx, ky, cy;
   int width, height;
@@ -142,6 +144,17 @@ void build_geo(const oracle_scene* s, Geo<T>& g) {
   g.field = s->field;
   g.use_map = s->use_map;
   g.slab_fp64 = s->slab_fp64;
+  g.precision = s->precision;
+  g.tau.resize(s->tf_n);
+  {
+    float ma = 0.f;  // float32 max alpha, as the device derives it
+    for (int i = 0; i < s->tf_n; ++i) ma = (ma < s->tf[4 * i + 3]) ? s->tf[4 * i + 3] : ma;
+    for (int i = 0; i < s->tf_n; ++i) {
+      // a_i = alpha / max alpha in float, then -ln(1 - a_i) in double, stored as float.
+      const float a = (ma > 0.f) ? s->tf[4 * i + 3] / ma : 0.f;
+      g.tau[i] = (a >= 1.f) ? std::numeric_limits<T>::infinity() : (T)(float)(-std::log1p(-(double)a));
+    }
+  }
   // Pinhole camera set up in double; per-pixel arithmetic in T.
   double f[3], r[3], u[3];
   for (int d = 0; d < 3; ++d) f[d] = s->cam_look[d] - s->cam_pos[d];
@@ -266,6 +279,73 @@ T light_march_point(const Geo<T>& g, const T L[3], const T P[3], uint64_t& nsamp
   return o;
 }
 
+// Precision form of the light march: same samples as light_march_point, but
+// the opacity is accumulated as optical depth tau = sum -ln(1 - a_i) with Kahan
+// compensation, a_i = 1 cuts the ray (T = 0), and the result is the
+// transmittance exp(-tau) rounded to IEEE binary16 (returned as float).
+template <typename T>
+T light_march_point_tau(const Geo<T>& g, const T L[3], const T P[3], uint64_t& nsamples) {
+  T v[3] = {P[0] - L[0], P[1] - L[1], P[2] - L[2]};
+  const T rs = T(1) / std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  const T dir[3] = {v[0] * rs, v[1] * rs, v[2] * rs};
+  T tmin, tmax;
+  segment_aabb(L, P, g, tmin, tmax);
+  const T start[3] = {L[0] + tmin * dir[0], L[1] + tmin * dir[1], L[2] + tmin * dir[2]};
+  T sl[3] = {start[0], start[1], start[2]};
+  const T len2 = (tmax - tmin) * (tmax - tmin);
+  const int N1 = g.tf_n - 1;
+  float sum = 0.f, comp = 0.f;
+  bool cut = false;
+  int budget = (int)(g.extent_mag / g.step) + 8;
+  while (budget-- > 0) {
+    const T q[3] = {sl[0] - start[0], sl[1] - start[1], sl[2] - start[2]};
+    if (!(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] <= len2)) break;
+    for (int d = 0; d < 3; ++d) sl[d] = sl[d] + g.step * dir[d];
+    bool inside = true;
+    for (int d = 0; d < 3; ++d)
+      if (sl[d] < g.minp[d] || sl[d] > g.maxp[d]) inside = false;
+    if (!inside) break;
+    T pc[3];
+    int c[3];
+    for (int d = 0; d < 3; ++d) {
+      int lo = 0, hi = g.n[d] - 2;
+      const T val = sl[d];
+      while (lo <= hi) {
+        const int mid = (lo + hi) / 2;
+        if (val <= g.C[d][mid + 1]) hi = mid - 1;
+        else lo = mid + 1;
+      }
+      c[d] = lo;
+      pc[d] = (val - g.C[d][lo]) / (g.C[d][lo + 1] - g.C[d][lo]);
+    }
+    const int64_t nx = g.n[0], nxy = (int64_t)g.n[0] * g.n[1];
+    const int64_t i0 = (int64_t)c[2] * nxy + (int64_t)c[1] * nx + c[0];
+    T vals[8] = {field_at(g, i0), field_at(g, i0 + 1), field_at(g, i0 + 1 + nx), field_at(g, i0 + nx),
+                 field_at(g, i0 + nxy), field_at(g, i0 + nxy + 1), field_at(g, i0 + nxy + 1 + nx),
+                 field_at(g, i0 + nxy + nx)};
+    T scalar = hex_interp(vals, pc[0], pc[1], pc[2]);
+    scalar = (scalar - g.min_scalar) * g.inv_delta;
+    const T fi = scalar * (T)N1;
+    int idx;
+    if (fi > T(-1) && fi < (T)(N1 + 1)) idx = (int)(int64_t)fi;
+    else idx = (fi >= (T)(N1 + 1)) ? N1 : 0;
+    idx = idx < 0 ? 0 : (idx > N1 ? N1 : idx);
+    ++nsamples;
+    const float ti = (float)g.tau[idx];
+    if (std::isinf(ti)) {
+      cut = true;
+      break;
+    }
+    const float y = ti - comp;
+    const float t = sum + y;
+    comp = (t - sum) - y;
+    sum = t;
+    if (sum >= 18.f) break;  // exp(-18) < 2^-25 rounds to 0 in binary16 however tau grows
+  }
+  const float tr = cut ? 0.f : (float)std::exp(-(double)sum);
+  return (T)(float)(_Float16)tr;
+}
+
 template <typename T>
 inline void map_vertex(const Geo<T>& g, int64_t id, T V[3]) {
   const int64_t px = g.pd[0], pxy = (int64_t)g.pd[0] * g.pd[1];
@@ -284,11 +364,13 @@ inline void light_origin(const Geo<T>& g, const T V[3], T L[3]) {
   }
 }
 
+// Map value of one vertex: opacity (reference) or FP16 transmittance (precision form).
 template <typename T>
 T vertex_opacity(const Geo<T>& g, int64_t id, uint64_t& ns) {
   T V[3], L[3];
   map_vertex(g, id, V);
   light_origin(g, V, L);
+  if (g.precision) return light_march_point_tau(g, L, V, ns);
   return light_march_point(g, L, V, ns);
 }
 
@@ -299,7 +381,8 @@ inline T map_opacity_at(const Geo<T>& g, const T p[3], MapGet get);
 
 template <typename T, typename MapGet>
 inline void map_estimate(const Geo<T>& g, const T p[3], MapGet get, T est[3]) {
-  const T tr = T(1) - map_opacity_at(g, p, get);
+  // precision form: the map holds transmittance, interpolated directly
+  const T tr = g.precision ? map_opacity_at(g, p, get) : T(1) - map_opacity_at(g, p, get);
   for (int d = 0; d < 3; ++d) est[d] = tr * g.light_color[d];
 }
 

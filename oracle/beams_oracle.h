@@ -47,6 +47,11 @@ typedef struct oracle_scene {
   double fov_y_deg;
   int width;
   int height;
+  /* 0: the reference algorithm. 1: the precision form — optical depth
+   * tau = sum -ln(1 - a_i) accumulated in float with Kahan compensation (a_i = 1
+   * cuts the ray), the map stores transmittance T = exp(-tau) rounded to IEEE
+   * binary16, and the view march shades by the interpolated T. */
+  int precision;
 } oracle_scene;
 
 /* Light march over every map vertex ((M+1)^3, x fastest). */

@@ -24,7 +24,8 @@ class OracleScene(C.Structure):
                 ("light_intensity", C.c_float), ("map_m", C.c_int * 3), ("use_map", C.c_int),
                 ("sample_distance", C.c_float), ("alpha_cutoff", C.c_float), ("light_steps", C.c_float),
                 ("slab_fp64", C.c_int), ("cam_pos", C.c_double * 3), ("cam_look", C.c_double * 3),
-                ("cam_up", C.c_double * 3), ("fov_y_deg", C.c_double), ("width", C.c_int), ("height", C.c_int)]
+                ("cam_up", C.c_double * 3), ("fov_y_deg", C.c_double), ("width", C.c_int), ("height", C.c_int),
+                ("precision", C.c_int)]
 
 
 def lib():
@@ -64,7 +65,7 @@ def _p(a):
 class Oracle:
     """Oracle bound to one scene and one field array (z, y, x) float32."""
 
-    def __init__(self, scene, field: np.ndarray | None = None, threads: int = 0):
+    def __init__(self, scene, field: np.ndarray | None = None, threads: int = 0, precision: bool = False):
         self.scene = scene
         self.field = np.ascontiguousarray(scene.field_numpy() if field is None else field, np.float32)
         self.tf = np.ascontiguousarray(scene.tf, np.float32)
@@ -76,7 +77,7 @@ class Oracle:
             (C.c_double * 3)(*s.light), (C.c_float * 3)(*s.light_color), s.light_intensity,
             (C.c_int * 3)(s.map_m, s.map_m, s.map_m), int(s.use_map), s.sample_distance, s.cutoff,
             s.light_steps, int(s.slab_fp64), (C.c_double * 3)(*s.cam_pos), (C.c_double * 3)(*s.cam_look),
-            (C.c_double * 3)(*s.cam_up), s.fov_y_deg, s.width, s.height)
+            (C.c_double * 3)(*s.cam_up), s.fov_y_deg, s.width, s.height, int(precision))
 
     @property
     def map_shape(self):
@@ -181,6 +182,19 @@ def noise_field(dims, perm, octaves=4, base_freq=4.0, lacunarity=2.0, gain=0.5, 
     if lib().oracle_generate_noise(_p(out), nx, ny, nz, _p(perm), octaves, base_freq, lacunarity, gain, threads):
         raise RuntimeError("oracle noise generator rejected the arguments")
     return out
+
+
+def quantize(field: np.ndarray, dtype: str) -> np.ndarray:
+    """float32 values of a field rounded to bfloat16 or float16 (round to nearest even)."""
+    f = np.ascontiguousarray(field, np.float32)
+    if dtype == "f16":
+        return f.astype(np.float16).astype(np.float32)
+    if dtype == "bf16":
+        u = f.view(np.uint32).astype(np.uint64)
+        lsb = (u >> 16) & 1
+        r = ((u + 0x7FFF + lsb) >> 16) << 16
+        return r.astype(np.uint32).view(np.float32)
+    raise ValueError(dtype)
 
 
 def psnr(a: np.ndarray, b: np.ndarray) -> float:

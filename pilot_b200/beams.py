@@ -176,8 +176,10 @@ class Renderer:
                 arr = arr.astype(np.float32, copy=False)
             self._keep_host = arr
             ptr = arr.ctypes.data_as(C.c_void_p)
-        else:  # torch tensor
+        else:  # torch tensor (float32, bfloat16 or float16)
+            import torch
             on_device = 1 if data.is_cuda else 0
+            dtype = {torch.float32: F32, torch.bfloat16: BF16, torch.float16: F16}[data.dtype]
             if dims is None:
                 nz, ny, nx = data.shape
                 dims = (nx, ny, nz) if assoc == ASSOC_POINTS else (nx + 1, ny + 1, nz + 1)
@@ -254,7 +256,12 @@ class Renderer:
         c = (C.c_float * 4)(*rgba)
         self._check(self._L.beams_set_background(self._h, int(bool(on)), c))
 
-    def set_form(self, form: int, opts=None):
+    def set_form(self, form: int, field_dtype: int = BF16):
+        """FORM_EXACT, or FORM_PRECISION with the 16-bit field dtype (BF16 or F16)."""
+        opts = None
+        if form == FORM_PRECISION:
+            self._prec_opts = (C.c_int * 1)(int(field_dtype))
+            opts = C.cast(self._prec_opts, C.c_void_p)
         self._check(self._L.beams_set_form(self._h, int(form), opts))
 
     # -- render ---------------------------------------------------------------

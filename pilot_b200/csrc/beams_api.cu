@@ -5,6 +5,7 @@
 // (beams/rendering/LightedVolumeRenderer.cxx:910-1372): the map is built once
 // (the reference's Phase 3 re-runs Phase 1 from zero opacity when there is a
 // single block, :1210-1256, which yields the same map), then the view march.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -208,7 +209,7 @@ static beams_status prepare_layouts_for(beams_renderer* r, const ExactGeo& g, in
     const size_t nq = (size_t)(g.n[0] - 1) * (g.n[1] - 1) * g.n[2];
     beams_status s = ensure_buffer(r, (void**)d_quads, quads_cap, nq * sizeof(float4), "allocating quad field");
     if (s != BEAMS_OK) return s;
-    cudaError_t e = launch_build_quads((const float*)d_field, *d_quads, g.n, r->stream);
+    cudaError_t e = launch_build_quads(d_field, BEAMS_F32, *d_quads, BEAMS_F32, g.n, r->stream);
     if (e != cudaSuccess) return cuda_fail(r, e, "quad field build");
     ++launches;
     *quads_version = version;
@@ -216,8 +217,15 @@ static beams_status prepare_layouts_for(beams_renderer* r, const ExactGeo& g, in
   return BEAMS_OK;
 }
 
+// Element type of the quad field the current form reads: float32 quads in the
+// exact form, bfloat16/binary16 quads in the precision form.
+static int quad_dtype(const beams_renderer* r) {
+  if (r->form != BEAMS_FORM_PRECISION) return BEAMS_F32;
+  return (r->vol.dtype == BEAMS_BF16 || r->vol.dtype == BEAMS_F16) ? r->vol.dtype : r->prec_dtype;
+}
+
 // Builds the derived layouts the kernels read: cell tables (per frame geometry)
-// and, for point fields, the 4-corner quad copy of the field.
+// and, for point fields, the 4-corner quad copy of the field in the form's dtype.
 beams_status prepare_layouts(beams_renderer* r, const ExactGeo& g, int& launches) {
   const unsigned long long key[4] = {r->volume_version, (unsigned long long)r->map_m[0],
                                      (unsigned long long)r->map_m[1], (unsigned long long)r->map_m[2]};
@@ -230,15 +238,17 @@ beams_status prepare_layouts(beams_renderer* r, const ExactGeo& g, int& launches
     ++launches;
     std::memcpy(r->tab_key, key, sizeof(key));
   }
-  if (r->vol.assoc == BEAMS_ASSOC_POINTS && r->quads_version != r->volume_version) {
+  const int qd = quad_dtype(r);
+  const unsigned long long qkey = r->volume_version * 4ull + (unsigned long long)qd;
+  if (r->vol.assoc == BEAMS_ASSOC_POINTS && r->quads_version != qkey) {
     const size_t nq = (size_t)(g.n[0] - 1) * (g.n[1] - 1) * g.n[2];
-    beams_status s = ensure_buffer(r, (void**)&r->d_quads, &r->quads_cap, nq * sizeof(float4),
-                                   "allocating quad field");
+    const size_t qbytes = (qd == BEAMS_F32) ? sizeof(float4) : 8;
+    beams_status s = ensure_buffer(r, (void**)&r->d_quads, &r->quads_cap, nq * qbytes, "allocating quad field");
     if (s != BEAMS_OK) return s;
-    cudaError_t e = launch_build_quads((const float*)r->d_field, r->d_quads, g.n, r->stream);
+    cudaError_t e = launch_build_quads(r->d_field, r->vol.dtype, r->d_quads, qd, g.n, r->stream);
     if (e != cudaSuccess) return cuda_fail(r, e, "quad field build");
     ++launches;
-    r->quads_version = r->volume_version;
+    r->quads_version = qkey;
   }
   return BEAMS_OK;
 }
@@ -249,15 +259,21 @@ beams_status build_map(beams_renderer* r, const ExactGeo& g, int& launches, bool
   map_key(r, key);
   if (r->reuse_map && r->map_valid && std::memcmp(&key, &r->map_key, sizeof(key)) == 0) return BEAMS_OK;
   const size_t nvert = (size_t)g.pd[0] * g.pd[1] * g.pd[2];
-  beams_status s = ensure_buffer(r, (void**)&r->d_map, &r->map_cap, nvert * sizeof(float), "allocating map");
+  const bool prec = r->form == BEAMS_FORM_PRECISION;
+  beams_status s = ensure_buffer(r, (void**)&r->d_map, &r->map_cap, nvert * (prec ? 2 : sizeof(float)),
+                                 "allocating map");
   if (s != BEAMS_OK) return s;
   r->map_valid = false;
-  cudaError_t e = launch_light_march_f32(g, r->d_quads, r->d_tab, r->d_tf, r->d_map, r->d_cnt, r->stream);
+  cudaError_t e = prec ? launch_light_march_prec(g, quad_dtype(r), r->d_quads, r->d_tab, r->d_tf, r->d_tau,
+                                                 (__half*)r->d_map, r->d_cnt, r->stream)
+                       : launch_light_march_f32(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map, r->d_cnt,
+                                                r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "light_march launch");
   ++launches;
   r->map_key = key;
   r->map_valid = true;
   r->map_count = nvert;
+  r->map_is_half = prec;
   built = true;
   return BEAMS_OK;
 }
@@ -291,6 +307,8 @@ beams_status check_ready(beams_renderer* r) {
     return fail(r, BEAMS_ERR_STATE, "shadow map enabled but no light added");
   if (r->form == BEAMS_FORM_EXACT && r->vol.dtype != BEAMS_F32)
     return fail(r, BEAMS_ERR_UNSUPPORTED, "the exact form needs a float32 volume");
+  if (r->form == BEAMS_FORM_PRECISION && r->vol.assoc != BEAMS_ASSOC_POINTS)
+    return fail(r, BEAMS_ERR_UNSUPPORTED, "the precision form renders point fields");
   const double nq = (double)(r->vol.dims[0] - 1) * (r->vol.dims[1] - 1) * r->vol.dims[2];
   if (nq >= 4294967296.0) return fail(r, BEAMS_ERR_UNSUPPORTED, "volume too large for 32-bit cell indexing");
   const double nv = (double)(r->map_m[0] + 1) * (r->map_m[1] + 1) * (r->map_m[2] + 1);
@@ -535,6 +553,21 @@ beams_status beams_set_color_map(beams_renderer* r, const float* rgba, int n) {
   if (s != BEAMS_OK) return s;
   cudaError_t e = cudaMemcpyAsync(r->d_tf, r->tf.data(), sizeof(float) * 4 * n, cudaMemcpyHostToDevice, r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "copying colour map");
+  // -ln(1 - a_i) per entry for the precision form's optical depth, a_i = alpha /
+  // max alpha in float32 as the light march forms it; a_i = 1 -> +inf (a cut).
+  {
+    float ma = 0.f;
+    for (int i = 0; i < n; ++i) ma = (ma < rgba[4 * i + 3]) ? rgba[4 * i + 3] : ma;
+    r->tau.assign(n, 0.f);
+    for (int i = 0; i < n; ++i) {
+      const float a = (ma > 0.f) ? rgba[4 * i + 3] / ma : 0.f;
+      r->tau[i] = (a >= 1.f) ? INFINITY : (float)(-std::log1p(-(double)a));
+    }
+    s = ensure_buffer(r, (void**)&r->d_tau, &r->tau_cap, sizeof(float) * 1024, "allocating tau table");
+    if (s != BEAMS_OK) return s;
+    e = cudaMemcpyAsync(r->d_tau, r->tau.data(), sizeof(float) * n, cudaMemcpyHostToDevice, r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "copying tau table");
+  }
   r->tf_n = n;
   ++r->tf_version;
   return BEAMS_OK;
@@ -632,10 +665,20 @@ beams_status beams_set_background(beams_renderer* r, int enable, const float rgb
 
 beams_status beams_set_form(beams_renderer* r, int form, const void* opts) {
   if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
-  (void)opts;
-  if (form != BEAMS_FORM_EXACT) return fail(r, BEAMS_ERR_UNSUPPORTED, "form not available in this build");
-  r->form = form;
-  return BEAMS_OK;
+  if (form == BEAMS_FORM_EXACT) {
+    r->form = form;
+    return BEAMS_OK;
+  }
+  if (form == BEAMS_FORM_PRECISION) {
+    int dt = BEAMS_BF16;
+    if (opts) dt = ((const beams_precision_options*)opts)->field_dtype;
+    if (dt != BEAMS_BF16 && dt != BEAMS_F16)
+      return fail(r, BEAMS_ERR_INVALID_ARG, "precision form: field_dtype must be BEAMS_BF16 or BEAMS_F16");
+    r->form = form;
+    r->prec_dtype = dt;
+    return BEAMS_OK;
+  }
+  return fail(r, BEAMS_ERR_UNSUPPORTED, "form not available in this build");
 }
 
 beams_status beams_build_shadow_map(beams_renderer* r, beams_timings* t) {
@@ -681,6 +724,16 @@ beams_status beams_get_shadow_map(beams_renderer* r, float* dst, size_t count, i
   if (!r->map_valid) return fail(r, BEAMS_ERR_STATE, "no map has been built");
   if (!dst || count < r->map_count) return fail(r, BEAMS_ERR_INVALID_ARG, "destination too small for the map");
   cudaSetDevice(r->device);
+  if (r->map_is_half) {
+    // precision form: binary16 transmittance, widened to float on the host
+    if (dst_on_device) return fail(r, BEAMS_ERR_UNSUPPORTED, "precision-form maps are copied to the host only");
+    std::vector<__half> h(r->map_count);
+    cudaError_t e = cudaMemcpyAsync(h.data(), r->d_map, r->map_count * 2, cudaMemcpyDeviceToHost, r->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "copying map");
+    for (size_t i = 0; i < r->map_count; ++i) dst[i] = __half2float(h[i]);
+    return BEAMS_OK;
+  }
   cudaError_t e = cudaMemcpyAsync(dst, r->d_map, r->map_count * sizeof(float),
                                   dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, r->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(r->stream);
@@ -722,8 +775,12 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
     if (s != BEAMS_OK) return s;
     dst = r->d_rgba;
   }
-  e = launch_view_march_f32(g, (const float*)r->d_field, r->d_quads, r->d_tab, r->d_tf, need_map ? r->d_map : nullptr,
-                            dst, r->d_cnt, r->stream);
+  if (r->form == BEAMS_FORM_PRECISION && r->vol.assoc == BEAMS_ASSOC_POINTS)
+    e = launch_view_march_prec(g, quad_dtype(r), r->d_quads, r->d_tab, r->d_tf,
+                               need_map ? (const __half*)r->d_map : nullptr, dst, r->d_cnt, r->stream);
+  else
+    e = launch_view_march_f32(g, (const float*)r->d_field, (const float4*)r->d_quads, r->d_tab, r->d_tf,
+                              need_map ? r->d_map : nullptr, dst, r->d_cnt, r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "view_march launch");
   ++launches;
   cudaEventRecord(r->ev[2], r->stream);

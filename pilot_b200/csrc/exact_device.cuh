@@ -5,6 +5,8 @@
 // build, and the explicit fmaf() calls below are the only fused operations
 // (lcl's lerp uses std::fma). Division and sqrtf are IEEE (no fast-math).
 #pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -270,10 +272,17 @@ __device__ __forceinline__ bool inside_vol(const ExactGeo& g, const float p[3]) 
            p[2] < g.minp[2] || p[2] > g.maxp[2]);
 }
 
+template <typename MapT> __device__ __forceinline__ float ld_map(const MapT* p);
+template <> __device__ __forceinline__ float ld_map<float>(const float* p) { return __ldg(p); }
+template <> __device__ __forceinline__ float ld_map<__half>(const __half* p) { return __half2float(__ldg(p)); }
+
 // TransmittanceLocator::LocateCell + GetEstimateUsingVerticesT
-// (TransmittanceMap.h:93-112, :200-229): map opacity at p. MT = map cell tables.
-__device__ __forceinline__ float map_opacity_t(const ExactGeo& g, const float4* MT, const float* __restrict__ map,
-                                               const float p[3]) {
+// (TransmittanceMap.h:93-112, :200-229): the map value interpolated at p
+// (opacity in the exact form, transmittance in the precision form).
+// MT = map cell tables.
+template <typename MapT>
+__device__ __forceinline__ float map_interp_t(const ExactGeo& g, const float4* MT, const MapT* __restrict__ map,
+                                              const float p[3]) {
   int c[3];
   float pc[3];
 #pragma unroll
@@ -286,16 +295,16 @@ __device__ __forceinline__ float map_opacity_t(const ExactGeo& g, const float4* 
     pc[d] = div_rn_markstein(p[d] - e.x, e.z, e.w);
   }
   const unsigned px = (unsigned)g.pd[0], pxy = (unsigned)g.pd[0] * (unsigned)g.pd[1];
-  const float* m = map + ((unsigned)c[2] * pxy + (unsigned)c[1] * px + (unsigned)c[0]);
+  const MapT* m = map + ((unsigned)c[2] * pxy + (unsigned)c[1] * px + (unsigned)c[0]);
   float v[8];
-  v[0] = __ldg(m);
-  v[1] = __ldg(m + 1);
-  v[2] = __ldg(m + 1 + px);
-  v[3] = __ldg(m + px);
-  v[4] = __ldg(m + pxy);
-  v[5] = __ldg(m + pxy + 1);
-  v[6] = __ldg(m + pxy + 1 + px);
-  v[7] = __ldg(m + pxy + px);
+  v[0] = ld_map(m);
+  v[1] = ld_map(m + 1);
+  v[2] = ld_map(m + 1 + px);
+  v[3] = ld_map(m + px);
+  v[4] = ld_map(m + pxy);
+  v[5] = ld_map(m + pxy + 1);
+  v[6] = ld_map(m + pxy + 1 + px);
+  v[7] = ld_map(m + pxy + px);
   return hex_interp(v, pc[0], pc[1], pc[2]);
 }
 
@@ -303,6 +312,29 @@ __device__ __forceinline__ float map_opacity_t(const ExactGeo& g, const float4* 
 // f(x+1,y+1,z)} for x < nx-1, y < ny-1, so one cell is two 16-byte loads
 // (z and z+1). VTK corner order 0..7 = lo.x lo.y lo.w lo.z hi.x hi.y hi.w hi.z.
 template <typename Q> struct QuadLoad;
+// 16-bit quads (precision form): four binary16 or bfloat16 values in 8 bytes.
+struct __align__(8) QuadBF16 { unsigned short v[4]; };
+struct __align__(8) QuadF16 { unsigned short v[4]; };
+__device__ __forceinline__ float bf16_lo(unsigned u) { return __uint_as_float(u << 16); }
+__device__ __forceinline__ float bf16_hi(unsigned u) { return __uint_as_float(u & 0xffff0000u); }
+__device__ __forceinline__ float f16_lo(unsigned u) { return __half2float(__ushort_as_half((unsigned short)(u & 0xffffu))); }
+__device__ __forceinline__ float f16_hi(unsigned u) { return __half2float(__ushort_as_half((unsigned short)(u >> 16))); }
+template <> struct QuadLoad<QuadBF16> {
+  static __device__ __forceinline__ void cell(const QuadBF16* __restrict__ q, unsigned qi, unsigned qz, float v[8]) {
+    const uint2 a = __ldg((const uint2*)(q + qi));
+    const uint2 b = __ldg((const uint2*)(q + qi + qz));
+    v[0] = bf16_lo(a.x); v[1] = bf16_hi(a.x); v[2] = bf16_hi(a.y); v[3] = bf16_lo(a.y);
+    v[4] = bf16_lo(b.x); v[5] = bf16_hi(b.x); v[6] = bf16_hi(b.y); v[7] = bf16_lo(b.y);
+  }
+};
+template <> struct QuadLoad<QuadF16> {
+  static __device__ __forceinline__ void cell(const QuadF16* __restrict__ q, unsigned qi, unsigned qz, float v[8]) {
+    const uint2 a = __ldg((const uint2*)(q + qi));
+    const uint2 b = __ldg((const uint2*)(q + qi + qz));
+    v[0] = f16_lo(a.x); v[1] = f16_hi(a.x); v[2] = f16_hi(a.y); v[3] = f16_lo(a.y);
+    v[4] = f16_lo(b.x); v[5] = f16_hi(b.x); v[6] = f16_hi(b.y); v[7] = f16_lo(b.y);
+  }
+};
 template <> struct QuadLoad<float4> {
   static __device__ __forceinline__ void cell(const float4* __restrict__ q, unsigned qi, unsigned qz, float v[8]) {
     const float4 a = __ldg(q + qi);

@@ -35,14 +35,56 @@ __device__ __forceinline__ void load_tables(float4* s_tab, const float4* __restr
 // ---------------------------------------------------------------------------
 // K1
 // ---------------------------------------------------------------------------
+// Opacity accumulation of one light ray.
+// Exact form: o <- o + (1 - o) a (TransmittanceMap.h:329-330); o == 1 is a fixed point.
+// Precision form: optical depth tau += -ln(1 - a) in float with Kahan
+// compensation (the per-entry -ln(1 - a) comes from a table), a = 1 cuts the
+// ray, and the map stores the transmittance exp(-tau) as binary16.
+template <bool PREC> struct Accum;
+template <> struct Accum<false> {
+  float o;
+  __device__ __forceinline__ void init(float o0) { o = o0; }
+  __device__ __forceinline__ bool add(const float* s_a, const float*, int idx) {
+    o = o + (1.f - o) * s_a[idx];
+    return o == 1.f;
+  }
+  __device__ __forceinline__ void store(void* map, int id) const { ((float*)map)[id] = o; }
+};
+template <> struct Accum<true> {
+  float sum, comp;
+  bool cut;
+  __device__ __forceinline__ void init(float) {
+    sum = 0.f;
+    comp = 0.f;
+    cut = false;
+  }
+  __device__ __forceinline__ bool add(const float*, const float* s_tau, int idx) {
+    const float ti = s_tau[idx];
+    if (ti == __int_as_float(0x7f800000)) {
+      cut = true;
+      return true;
+    }
+    const float y = ti - comp;
+    const float t = sum + y;
+    comp = (t - sum) - y;
+    sum = t;
+    return sum >= 18.f;  // exp(-18) < 2^-25: the binary16 result is 0 from here on
+  }
+  __device__ __forceinline__ void store(void* map, int id) const {
+    const float tr = cut ? 0.f : (float)exp(-(double)sum);
+    ((__half*)map)[id] = __float2half_rn(tr);
+  }
+};
+
 // STITCH: the multi-brick Phase 3 — the march starts from the cross-brick
 // prefix (stitch_prefix) instead of zero, as GenerateEstimator is re-run on
 // the prefix opacities (LightedVolumeRenderer.cxx:1241-1252).
-template <typename QuadT, bool STITCH>
+template <typename QuadT, bool STITCH, bool PREC>
 __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, const QuadT* __restrict__ quads,
                                                           const float4* __restrict__ tab,
                                                           const float4* __restrict__ tf,
-                                                          float* __restrict__ map, int nvert,
+                                                          const float* __restrict__ tau,
+                                                          void* __restrict__ map, int nvert,
                                                           Counters* __restrict__ cnt,
                                                           const BrickRef* __restrict__ refs, int nrefs,
                                                           int self) {
@@ -50,9 +92,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
   const int nfield = g.max_off[0];             // field-axis table entries only
   float4* s_tab = s_dyn;
   float* s_a = (float*)(s_dyn + nfield);       // TF alpha / max alpha (TransmittanceMap.h:329)
+  float* s_tau = s_a + g.tf_n;                 // -ln(1 - a) (precision form)
   load_tables(s_tab, tab, nfield);
-  for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x)
+  for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) {
     s_a[i] = (g.max_alpha > 0.f) ? tf[i].w / g.max_alpha : 0.f;
+    if (PREC) s_tau[i] = tau[i];
+  }
   __syncthreads();
 
   const float4* T0 = s_tab + g.ax_off[0];
@@ -109,29 +154,31 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
       pc[2] = div_rn_markstein(s[2] - e2.x, e2.z, e2.w);
       return true;
     };
-    float o = STITCH ? stitch_prefix(refs, nrefs, self, L, V, dir) : 0.f;
+    Accum<PREC> acc;
+    acc.init(STITCH ? stitch_prefix(refs, nrefs, self, L, V, dir) : 0.f);
     float va[8], pa[3], vb[8], pb[3];
     bool ok = gen(va, pa);
     while (ok) {
       const bool okb = gen(vb, pb);
+      bool done;
       {
         float scalar = hex_interp(va, pa[0], pa[1], pa[2]);
         scalar = (scalar - g.min_scalar) * g.inv_delta;
-        o = o + (1.f - o) * s_a[tf_index_clamped(scalar * (float)n1, n1)];
+        done = acc.add(s_a, s_tau, tf_index_clamped(scalar * (float)n1, n1));
         ++ns;
       }
-      // o == 1 is a fixed point of o + (1-o)a: the remaining samples cannot change it.
-      if (o == 1.f || !okb) break;
+      // Stop when the accumulated value can no longer change (see Accum).
+      if (done || !okb) break;
       ok = gen(va, pa);
       {
         float scalar = hex_interp(vb, pb[0], pb[1], pb[2]);
         scalar = (scalar - g.min_scalar) * g.inv_delta;
-        o = o + (1.f - o) * s_a[tf_index_clamped(scalar * (float)n1, n1)];
+        done = acc.add(s_a, s_tau, tf_index_clamped(scalar * (float)n1, n1));
         ++ns;
       }
-      if (o == 1.f) break;
+      if (done) break;
     }
-    map[id] = o;
+    acc.store(map, id);
   }
   warp_add(&cnt->light_samples, ns);
 }
@@ -154,10 +201,10 @@ __device__ __forceinline__ int next_warp_tile(unsigned* counter) {
   return (int)__shfl_sync(0xffffffffu, t, 0);
 }
 
-template <typename QuadT, bool USE_MAP>
+template <typename QuadT, bool USE_MAP, typename MapT>
 __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT* __restrict__ quads,
                                                  const float4* s_tab, const float4* s_tf,
-                                                 const float* __restrict__ map, int x, int y, float4& color,
+                                                 const MapT* __restrict__ map, int x, int y, float4& color,
                                                  unsigned& lit, unsigned& hit) {
   color = make_float4(0.f, 0.f, 0.f, 0.f);
   float o[3], d[3], minD, maxD;
@@ -229,7 +276,9 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT*
       float sc0 = tfc.x, sc1 = tfc.y, sc2 = tfc.z;
       const float sa = tfc.w * (1.f - color.w);
       if (USE_MAP) {
-        const float tr = 1.f - map_opacity_t(g, s_tab, map, p);
+        // exact form: 1 - opacity (TransmittanceMap.h:195); precision form: stored transmittance
+        const float mv = map_interp_t<MapT>(g, s_tab, map, p);
+        const float tr = (sizeof(MapT) == 2) ? mv : 1.f - mv;
         sc0 = sc0 * (tr * g.light_color[0]);
         sc1 = sc1 * (tr * g.light_color[1]);
         sc2 = sc2 * (tr * g.light_color[2]);
@@ -254,11 +303,11 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT*
   }
 }
 
-template <typename QuadT, bool USE_MAP>
+template <typename QuadT, bool USE_MAP, typename MapT>
 __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const QuadT* __restrict__ quads,
                                                          const float4* __restrict__ tab,
                                                          const float4* __restrict__ tf,
-                                                         const float* __restrict__ map,
+                                                         const MapT* __restrict__ map,
                                                          float4* __restrict__ out,
                                                          Counters* __restrict__ cnt) {
   extern __shared__ float4 s_dyn[];
@@ -275,7 +324,7 @@ __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const
     tile_pixel(tiles_x, tile, x, y);
     if (x < g.width && y < g.height) {
       float4 color;
-      view_march_pixel<QuadT, USE_MAP>(g, quads, s_tab, s_tf, map, x, y, color, lit, hit);
+      view_march_pixel<QuadT, USE_MAP, MapT>(g, quads, s_tab, s_tf, map, x, y, color, lit, hit);
       out[(size_t)y * g.width + x] = color;
     }
   }
@@ -406,15 +455,45 @@ __global__ void k_build_tables(const ExactGeo g, float4* __restrict__ tab) {
   tab[i] = make_float4(lo, hi, w, 1.f / w);
 }
 
-__global__ void k_build_quads(const float* __restrict__ f, float4* __restrict__ q, int nx, int ny, int nz) {
+// Quad element conversion: input element -> stored quad element.
+struct CvtF32 { static __device__ __forceinline__ float get(const float* p) { return __ldg(p); } };
+struct CvtU16 {
+  static __device__ __forceinline__ unsigned short get(const unsigned short* p) { return __ldg(p); }
+};
+struct CvtF32toBF16 {
+  static __device__ __forceinline__ unsigned short get(const float* p) {
+    return __bfloat16_as_ushort(__float2bfloat16_rn(__ldg(p)));
+  }
+};
+struct CvtF32toF16 {
+  static __device__ __forceinline__ unsigned short get(const float* p) {
+    return __half_as_ushort(__float2half_rn(__ldg(p)));
+  }
+};
+template <typename In, typename Cvt> struct QuadOut;
+template <> struct QuadOut<float, CvtF32> {
+  using T = float4;
+  static __device__ __forceinline__ T make(const float* b, int nx) {
+    return make_float4(__ldg(b), __ldg(b + 1), __ldg(b + nx), __ldg(b + nx + 1));
+  }
+};
+template <typename In, typename Cvt> struct QuadOut16 {
+  static __device__ __forceinline__ uint2 make(const In* b, int nx) {
+    const unsigned v0 = Cvt::get(b), v1 = Cvt::get(b + 1), v2 = Cvt::get(b + nx), v3 = Cvt::get(b + nx + 1);
+    return make_uint2(v0 | (v1 << 16), v2 | (v3 << 16));
+  }
+};
+
+template <typename In, typename OutT, typename Maker>
+__global__ void k_build_quads(const In* __restrict__ f, OutT* __restrict__ q, int nx, int ny, int nz) {
   const unsigned qx = nx - 1, qxy = (unsigned)(nx - 1) * (ny - 1);
   const size_t total = (size_t)qxy * nz;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const unsigned z = (unsigned)(i / qxy);
     const unsigned r = (unsigned)(i - (size_t)z * qxy);
     const unsigned y = r / qx, x = r - y * qx;
-    const float* b = f + ((size_t)z * ny + y) * nx + x;
-    q[i] = make_float4(__ldg(b), __ldg(b + 1), __ldg(b + nx), __ldg(b + nx + 1));
+    const In* b = f + ((size_t)z * ny + y) * nx + x;
+    q[i] = Maker::make(b, nx);
   }
 }
 
@@ -451,32 +530,58 @@ cudaError_t launch_build_tables(const ExactGeo& g, float4* tab, cudaStream_t st)
   return cudaGetLastError();
 }
 
-cudaError_t launch_build_quads(const float* field, float4* quads, const int n[3], cudaStream_t st) {
+// in_dtype: dtype of the field (BEAMS_F32/BF16/F16); quad_dtype: stored quads.
+cudaError_t launch_build_quads(const void* field, int in_dtype, void* quads, int quad_dtype, const int n[3],
+                               cudaStream_t st) {
   const size_t total = (size_t)(n[0] - 1) * (n[1] - 1) * n[2];
   size_t blocks = (total + 255) / 256;
   const size_t cap = (size_t)num_sms() * 16;
-  k_build_quads<<<(unsigned)(blocks < cap ? blocks : cap), 256, 0, st>>>(field, quads, n[0], n[1], n[2]);
+  const unsigned grid = (unsigned)(blocks < cap ? blocks : cap);
+  if (quad_dtype == 0 && in_dtype == 0) {
+    k_build_quads<float, float4, QuadOut<float, CvtF32>><<<grid, 256, 0, st>>>((const float*)field, (float4*)quads,
+                                                                               n[0], n[1], n[2]);
+  } else if (quad_dtype == 1 && in_dtype == 0) {
+    k_build_quads<float, uint2, QuadOut16<float, CvtF32toBF16>><<<grid, 256, 0, st>>>(
+        (const float*)field, (uint2*)quads, n[0], n[1], n[2]);
+  } else if (quad_dtype == 2 && in_dtype == 0) {
+    k_build_quads<float, uint2, QuadOut16<float, CvtF32toF16>><<<grid, 256, 0, st>>>(
+        (const float*)field, (uint2*)quads, n[0], n[1], n[2]);
+  } else if (quad_dtype == in_dtype && in_dtype != 0) {
+    k_build_quads<unsigned short, uint2, QuadOut16<unsigned short, CvtU16>><<<grid, 256, 0, st>>>(
+        (const unsigned short*)field, (uint2*)quads, n[0], n[1], n[2]);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template <typename QuadT, bool STITCH, bool PREC>
+static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4* tab, const float4* tf,
+                             const float* tau, void* map, Counters* cnt, cudaStream_t st, const BrickRef* refs,
+                             int nrefs, int self) {
+  const int nvert = g.pd[0] * g.pd[1] * g.pd[2];
+  const size_t smem = (size_t)g.max_off[0] * sizeof(float4) + 2 * (size_t)g.tf_n * sizeof(float);
+  const int ntiles = (nvert + kThreads - 1) / kThreads;
+  int grid = 0;
+  cudaError_t e = persistent_grid(k_light_march<QuadT, STITCH, PREC>, smem, ntiles, grid);
+  if (e != cudaSuccess) return e;
+  k_light_march<QuadT, STITCH, PREC><<<grid, kThreads, smem, st>>>(g, (const QuadT*)quads, tab, tf, tau, map,
+                                                                   nvert, cnt, refs, nrefs, self);
   return cudaGetLastError();
 }
 
 cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    float* map, Counters* cnt, cudaStream_t st, const BrickRef* refs, int nrefs,
                                    int self) {
-  const int nvert = g.pd[0] * g.pd[1] * g.pd[2];
-  const size_t smem = (size_t)g.max_off[0] * sizeof(float4) + (size_t)g.tf_n * sizeof(float);
-  const int ntiles = (nvert + kThreads - 1) / kThreads;
-  int grid = 0;
-  cudaError_t e;
-  if (refs) {
-    e = persistent_grid(k_light_march<float4, true>, smem, ntiles, grid);
-    if (e != cudaSuccess) return e;
-    k_light_march<float4, true><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, map, nvert, cnt, refs, nrefs, self);
-  } else {
-    e = persistent_grid(k_light_march<float4, false>, smem, ntiles, grid);
-    if (e != cudaSuccess) return e;
-    k_light_march<float4, false><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, map, nvert, cnt, nullptr, 0, -1);
-  }
-  return cudaGetLastError();
+  if (refs) return launch_k1<float4, true, false>(g, quads, tab, tf, nullptr, map, cnt, st, refs, nrefs, self);
+  return launch_k1<float4, false, false>(g, quads, tab, tf, nullptr, map, cnt, st, nullptr, 0, -1);
+}
+
+cudaError_t launch_light_march_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,
+                                    const float4* tf, const float* tau, __half* map, Counters* cnt, cudaStream_t st) {
+  if (quad_dtype == 1)
+    return launch_k1<QuadBF16, false, true>(g, quads, tab, tf, tau, map, cnt, st, nullptr, 0, -1);
+  return launch_k1<QuadF16, false, true>(g, quads, tab, tf, tau, map, cnt, st, nullptr, 0, -1);
 }
 
 // K6: sort-last composite of nb brick images in the given order
@@ -522,15 +627,36 @@ cudaError_t launch_view_march_f32(const ExactGeo& g, const float* field, const f
     if (e != cudaSuccess) return e;
     k_view_march_cells<float><<<grid, kThreads, smem, st>>>(g, field, tab, tf, out, cnt);
   } else if (g.use_map) {
-    e = persistent_grid(k_view_march<float4, true>, smem, ntiles, grid);
+    e = persistent_grid(k_view_march<float4, true, float>, smem, ntiles, grid);
     if (e != cudaSuccess) return e;
-    k_view_march<float4, true><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, map, out, cnt);
+    k_view_march<float4, true, float><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, map, out, cnt);
   } else {
-    e = persistent_grid(k_view_march<float4, false>, smem, ntiles, grid);
+    e = persistent_grid(k_view_march<float4, false, float>, smem, ntiles, grid);
     if (e != cudaSuccess) return e;
-    k_view_march<float4, false><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, nullptr, out, cnt);
+    k_view_march<float4, false, float><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, nullptr, out, cnt);
   }
   return cudaGetLastError();
+}
+
+template <typename QuadT, bool USE_MAP>
+static cudaError_t launch_k2_prec(const ExactGeo& g, const void* quads, const float4* tab, const float4* tf,
+                                  const __half* map, float4* out, Counters* cnt, cudaStream_t st) {
+  const size_t smem = ((size_t)g.ntab + (size_t)g.tf_n) * sizeof(float4);
+  const int ntiles = (((g.width + 7) >> 3) * ((g.height + 3) >> 2) + 7) / 8;
+  int grid = 0;
+  cudaError_t e = persistent_grid(k_view_march<QuadT, USE_MAP, __half>, smem, ntiles, grid);
+  if (e != cudaSuccess) return e;
+  k_view_march<QuadT, USE_MAP, __half><<<grid, kThreads, smem, st>>>(g, (const QuadT*)quads, tab, tf, map, out, cnt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_view_march_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,
+                                   const float4* tf, const __half* map, float4* out, Counters* cnt, cudaStream_t st) {
+  if (quad_dtype == 1)
+    return g.use_map ? launch_k2_prec<QuadBF16, true>(g, quads, tab, tf, map, out, cnt, st)
+                     : launch_k2_prec<QuadBF16, false>(g, quads, tab, tf, map, out, cnt, st);
+  return g.use_map ? launch_k2_prec<QuadF16, true>(g, quads, tab, tf, map, out, cnt, st)
+                   : launch_k2_prec<QuadF16, false>(g, quads, tab, tf, map, out, cnt, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -1,5 +1,6 @@
 // kernels.h — launch wrappers shared between the kernel files and the C-ABI layer.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -8,7 +9,12 @@
 namespace beams {
 
 cudaError_t launch_build_tables(const ExactGeo& g, float4* tab, cudaStream_t st);
-cudaError_t launch_build_quads(const float* field, float4* quads, const int n[3], cudaStream_t st);
+cudaError_t launch_build_quads(const void* field, int in_dtype, void* quads, int quad_dtype, const int n[3],
+                               cudaStream_t st);
+cudaError_t launch_light_march_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,
+                                    const float4* tf, const float* tau, __half* map, Counters* cnt, cudaStream_t st);
+cudaError_t launch_view_march_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,
+                                   const float4* tf, const __half* map, float4* out, Counters* cnt, cudaStream_t st);
 cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    float* map, Counters* cnt, cudaStream_t st, const BrickRef* refs = nullptr,
                                    int nrefs = 0, int self = -1);

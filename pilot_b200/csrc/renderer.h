@@ -106,11 +106,18 @@ struct beams_renderer {
   size_t map_count = 0;
   bool map_valid = false;
   beams::MapKey map_key{};
+  bool map_is_half = false;  // precision form: binary16 transmittance
+
+  // precision form
+  int prec_dtype = BEAMS_BF16;
+  std::vector<float> tau;     // -ln(1 - a_i) per TF entry
+  float* d_tau = nullptr;
+  size_t tau_cap = 0;
 
   // derived layouts: 4-corner quads of the field, per-axis cell tables
-  float4* d_quads = nullptr;
+  void* d_quads = nullptr;                // float4 (exact) or 8-byte 16-bit quads (precision)
   size_t quads_cap = 0;
-  unsigned long long quads_version = 0;  // volume_version the quads were built from
+  unsigned long long quads_version = 0;  // volume_version * 4 + quad dtype the quads were built from
   float4* d_tab = nullptr;
   size_t tab_cap = 0;
   unsigned long long tab_key[4] = {0, 0, 0, 0};  // volume_version, map m[3] packed
@@ -136,6 +143,7 @@ struct beams_renderer {
     if (d_map) cudaFree(d_map);
     if (d_quads) cudaFree(d_quads);
     if (d_tab) cudaFree(d_tab);
+    if (d_tau) cudaFree(d_tau);
     if (d_rgba) cudaFree(d_rgba);
     for (auto& b : bricks) b.release();
     if (d_refs) cudaFree(d_refs);

@@ -171,6 +171,48 @@ beams_status beams_set_bricks(beams_renderer* r, const beams_volume* bricks, int
 beams_status beams_get_brick_map(beams_renderer* r, int brick, int stage, float* dst, size_t count,
                                  int dst_on_device);
 
+/* ---- learned form ------------------------------------------------------------ */
+/* No reference counterpart: a transmittance network (encoded position and light
+ * direction -> 4 x 64 ReLU -> sigmoid) that replaces the map build and lookup
+ * in BEAMS_FORM_MLP. Trained on the device on samples of the exact light march. */
+typedef struct beams_mlp_options {
+  int samples_log2;      /* training samples 2^k (default 24) */
+  int n_lights;          /* light directions on a Fibonacci sphere (default 32) */
+  int epochs;            /* default 4 */
+  int batch;             /* rows per step (default 16384) */
+  float lr;              /* Adam learning rate, cosine-decayed (default 2e-3) */
+  unsigned seed;
+  float fallback_tol;    /* render: |MLP - exact| on the probe set that sends a tile to the exact map (0.01) */
+  float probe_fraction;  /* render: fraction of pixels probed (0.01) */
+  int knot;              /* render: MLP evaluated every `knot` lit samples, linear in between (1 = every sample) */
+} beams_mlp_options;
+
+typedef struct beams_mlp_report {
+  float datagen_ms;
+  float train_ms;
+  float holdout_rmse;   /* trained network on held-out samples */
+  float initial_rmse;   /* the initial network on the same samples */
+  float unlit_rmse;     /* the method without a shadow model: T = 1 */
+  float mean_rmse;      /* the best constant T */
+  int steps;
+  int samples;
+} beams_mlp_report;
+
+/* Trains the network on the current volume and colour map. */
+beams_status beams_mlp_train(beams_renderer* r, const beams_mlp_options* opts, beams_mlp_report* report);
+int beams_mlp_param_count(void);
+beams_status beams_mlp_get_params(beams_renderer* r, float* dst, int n);
+beams_status beams_mlp_set_params(beams_renderer* r, const float* src, int n);
+/* The training kernels' loss (mean squared error) and gradient for features
+ * (n x 112 floats, rounded to bfloat16) and targets; T gets the predictions. */
+beams_status beams_mlp_loss_grad(beams_renderer* r, const float* features, const float* target, int n,
+                                 float* loss, float* grad, float* T);
+/* The network's input encoding of n world positions under n light features. */
+beams_status beams_mlp_encode(beams_renderer* r, const float* pos, const float* lfeat, int n, float* out);
+/* Versioned checkpoint of parameters and Adam moments (FNV-1a checksummed). */
+beams_status beams_mlp_save(beams_renderer* r, const char* path);
+beams_status beams_mlp_load(beams_renderer* r, const char* path);
+
 /* ---- render --------------------------------------------------------------- */
 /* Replaces MapperLightedVolume::RenderCells (MapperLightedVolume.cxx:114-193):
  * map build (Phase 1/3) + view march (Phase 4) + copy-out (Phase 5).

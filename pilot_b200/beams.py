@@ -27,6 +27,26 @@ ASSOC_POINTS, ASSOC_CELLS = 0, 1
 FORM_EXACT, FORM_PRECISION, FORM_MLP = 0, 1, 2
 
 
+class MlpOptions(C.Structure):
+    _fields_ = [("samples_log2", C.c_int), ("n_lights", C.c_int), ("epochs", C.c_int), ("batch", C.c_int),
+                ("lr", C.c_float), ("seed", C.c_uint), ("fallback_tol", C.c_float), ("probe_fraction", C.c_float),
+                ("knot", C.c_int)]
+
+
+class MlpReport(C.Structure):
+    _fields_ = [("datagen_ms", C.c_float), ("train_ms", C.c_float), ("holdout_rmse", C.c_float),
+                ("initial_rmse", C.c_float), ("unlit_rmse", C.c_float), ("mean_rmse", C.c_float),
+                ("steps", C.c_int), ("samples", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def mlp_options(samples_log2=24, n_lights=32, epochs=4, batch=16384, lr=2e-3, seed=1, fallback_tol=0.01,
+                probe_fraction=0.01, knot=4):
+    return MlpOptions(samples_log2, n_lights, epochs, batch, lr, seed, fallback_tol, probe_fraction, knot)
+
+
 class BeamsError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
@@ -92,6 +112,14 @@ def lib():
         "beams_selftest_division": ([C.c_float, C.c_float, C.c_int, C.c_int, C.POINTER(C.c_ulonglong),
                                      C.POINTER(C.c_ulonglong)], C.c_int),
         "beams_set_bricks": ([P, P, C.c_int], C.c_int),
+        "beams_mlp_train": ([P, C.POINTER(MlpOptions), C.POINTER(MlpReport)], C.c_int),
+        "beams_mlp_param_count": ([], C.c_int),
+        "beams_mlp_get_params": ([P, P, C.c_int], C.c_int),
+        "beams_mlp_set_params": ([P, P, C.c_int], C.c_int),
+        "beams_mlp_loss_grad": ([P, P, P, C.c_int, C.POINTER(C.c_float), P, P], C.c_int),
+        "beams_mlp_encode": ([P, P, P, C.c_int, P], C.c_int),
+        "beams_mlp_save": ([P, C.c_char_p], C.c_int),
+        "beams_mlp_load": ([P, C.c_char_p], C.c_int),
         "beams_get_brick_map": ([P, C.c_int, C.c_int, P, C.c_size_t, C.c_int], C.c_int),
         "beams_generate_noise": ([P, P, P, C.c_int, C.c_float, C.c_float, C.c_float, P], C.c_int),
     }
@@ -215,6 +243,45 @@ class Renderer:
         m = np.empty(count, np.float32)
         self._check(self._L.beams_get_brick_map(self._h, brick, stage, _ptr(m), m.size, 0))
         return m
+
+    # -- learned form ---------------------------------------------------------
+    def mlp_train(self, opts: MlpOptions | None = None):
+        rep = MlpReport()
+        self._check(self._L.beams_mlp_train(self._h, C.byref(opts) if opts is not None else None, C.byref(rep)))
+        return rep.as_dict()
+
+    def mlp_params(self):
+        n = self._L.beams_mlp_param_count()
+        out = np.empty(n, np.float32)
+        self._check(self._L.beams_mlp_get_params(self._h, _ptr(out), n))
+        return out
+
+    def mlp_set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self._check(self._L.beams_mlp_set_params(self._h, _ptr(p), p.size))
+
+    def mlp_loss_grad(self, features, target):
+        f = np.ascontiguousarray(features, np.float32)
+        t = np.ascontiguousarray(target, np.float32)
+        n = t.size
+        g = np.empty(self._L.beams_mlp_param_count(), np.float32)
+        T = np.empty(n, np.float32)
+        loss = C.c_float()
+        self._check(self._L.beams_mlp_loss_grad(self._h, _ptr(f), _ptr(t), n, C.byref(loss), _ptr(g), _ptr(T)))
+        return loss.value, g, T
+
+    def mlp_encode(self, pos, lfeat):
+        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        lf = np.ascontiguousarray(lfeat, np.float32).reshape(-1, 3)
+        out = np.empty((pos.shape[0], 112), np.float32)
+        self._check(self._L.beams_mlp_encode(self._h, _ptr(pos), _ptr(lf), pos.shape[0], _ptr(out)))
+        return out
+
+    def mlp_save(self, path):
+        self._check(self._L.beams_mlp_save(self._h, str(path).encode()))
+
+    def mlp_load(self, path):
+        self._check(self._L.beams_mlp_load(self._h, str(path).encode()))
 
     def set_color_map(self, rgba):
         t = np.ascontiguousarray(rgba, dtype=np.float32).reshape(-1, 4)

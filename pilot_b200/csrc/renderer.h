@@ -14,6 +14,8 @@
 
 namespace beams {
 
+struct MlpState;  // learned form (mlp_api.cu)
+
 struct Light {
   int kind = 0;  // 0 point, 1 directional
   double v[3] = {0, 0, 0};
@@ -131,13 +133,17 @@ struct beams_renderer {
   size_t brick_imgs_cap = 0;
   unsigned long long brick_counter = 0;
 
+  // learned form: parameters, optimiser state, inference weights
+  beams::MlpState* mlp = nullptr;
+
   // image + counters + timing
   float4* d_rgba = nullptr;
   size_t rgba_cap = 0;
   beams::Counters* d_cnt = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
-  ~beams_renderer() {
+  ~beams_renderer();
+  void release_buffers() {
     if (d_field_owned) cudaFree(d_field_owned);
     if (d_tf) cudaFree(d_tf);
     if (d_map) cudaFree(d_map);
@@ -155,7 +161,13 @@ struct beams_renderer {
 };
 
 namespace beams {
+void mlp_release(beams_renderer* r);
 beams_status fail(beams_renderer* r, beams_status s, const std::string& msg);
 beams_status cuda_fail(beams_renderer* r, cudaError_t e, const char* what);
 beams_status ensure_buffer(beams_renderer* r, void** buf, size_t* cap, size_t bytes, const char* what);
 }  // namespace beams
+
+inline beams_renderer::~beams_renderer() {
+  beams::mlp_release(this);
+  release_buffers();
+}

@@ -473,8 +473,13 @@ inline bool inside_vol(const Geo<T>& g, const T p[3]) {
   return true;
 }
 
-template <typename T, typename MapGet>
-void march_pixel(const Geo<T>& g, int x, int y, MapGet get, T color[4], uint64_t& lit) {
+struct NoRecord {
+  template <typename T> void operator()(const T*, const T*, T) const {}
+};
+
+// rec(p, tf_rgba, sa) is called at every composited sample, before shading.
+template <typename T, typename MapGet, typename Rec = NoRecord>
+void march_pixel(const Geo<T>& g, int x, int y, MapGet get, T color[4], uint64_t& lit, Rec rec = Rec()) {
   color[0] = color[1] = color[2] = color[3] = T(0);
   T o[3], d[3], minD, maxD;
   if (!ray_setup(g, x, y, o, d, minD, maxD)) return;  // minDistance == -1
@@ -561,6 +566,7 @@ void march_pixel(const Geo<T>& g, int x, int y, MapGet get, T color[4], uint64_t
       const int idx = (int)(int64_t)fi;
       T sc[4] = {g.tf[4 * idx], g.tf[4 * idx + 1], g.tf[4 * idx + 2], g.tf[4 * idx + 3]};
       sc[3] *= (T(1) - color[3]);
+      rec(p, sc, sc[3]);
       if (g.use_map) {
         T est[3];
         map_estimate(g, p, get, est);
@@ -953,6 +959,40 @@ int oracle_view_march_lazy_f64(const oracle_scene* s, int x0, int y0, int w, int
   }
   if (lit_out) *lit_out = lit;
   return 0;
+}
+
+// Lit samples of the pixel window in march order: for each sample its position
+// (xyz), TF rgb and premultiplied alpha (7 floats); counts[i] per pixel. Stops
+// at cap samples in total (returns 2 if the cap was hit). The shading is not
+// applied, so any transmittance model can be composited from these records.
+int oracle_record_samples_f32(const oracle_scene* s, int x0, int y0, int w, int h, float* rec, int64_t cap,
+                              int* counts) {
+  if (!valid(s) || !rec || !counts) return 1;
+  Geo<float> g;
+  build_geo(s, g);
+  g.use_map = 0;
+  int64_t n = 0;
+  bool full = false;
+  for (int yy = 0; yy < h; ++yy)
+    for (int xx = 0; xx < w; ++xx) {
+      float c[4];
+      uint64_t l = 0;
+      int cnt = 0;
+      auto r = [&](const float* p, const float* sc, float sa) {
+        if (n >= cap) {
+          full = true;
+          return;
+        }
+        float* d = rec + 7 * n;
+        d[0] = p[0]; d[1] = p[1]; d[2] = p[2];
+        d[3] = sc[0]; d[4] = sc[1]; d[5] = sc[2]; d[6] = sa;
+        ++n;
+        ++cnt;
+      };
+      march_pixel(g, x0 + xx, y0 + yy, [](int64_t) { return 0.f; }, c, l, r);
+      counts[yy * w + xx] = cnt;
+    }
+  return full ? 2 : 0;
 }
 
 int oracle_ray_setup_f32(const oracle_scene* s, int x, int y, float out[8]) {

@@ -76,6 +76,10 @@ int oracle_view_march_f64(const oracle_scene* s, const double* map, int x0, int 
 int oracle_view_march_lazy_f64(const oracle_scene* s, int x0, int y0, int w, int h, int stride,
                                double* rgba_out, int threads, uint64_t* lit_samples);
 
+/* Lit samples of a pixel window in march order (x, y, z, r, g, b, sa per sample). */
+int oracle_record_samples_f32(const oracle_scene* s, int x0, int y0, int w, int h, float* rec, int64_t cap,
+                              int* counts);
+
 /* Per-pixel slab test (t_enter, t_exit; miss -> t_enter = -1). */
 int oracle_ray_setup_f32(const oracle_scene* s, int x, int y, float out[8]);
 

@@ -49,6 +49,7 @@ def lib():
             "oracle_generate_noise": [P, C.c_int, C.c_int, C.c_int, P, C.c_int, C.c_float, C.c_float,
                                       C.c_float, C.c_int],
             "oracle_render_bricks_f32": [P, C.c_int, P, P, P, P, C.c_int, u64p],
+            "oracle_record_samples_f32": [S, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int64, P],
             "oracle_render_bricks_f64": [P, C.c_int, P, P, P, P, C.c_int, u64p],
         }.items():
             f = getattr(L, name)
@@ -134,6 +135,19 @@ class Oracle:
                                             C.byref(lit)):
             raise RuntimeError("oracle lazy view march rejected the scene")
         return out, lit.value
+
+    def record_samples(self, window=None, cap=1 << 24):
+        """Lit samples per pixel in march order: (records (n,7), counts (h,w))."""
+        s = self.scene
+        x0, y0, w, h = window if window is not None else (0, 0, s.width, s.height)
+        rec = np.zeros((cap, 7), np.float32)
+        counts = np.zeros((h, w), np.int32)
+        rc = lib().oracle_record_samples_f32(C.byref(self.cs), x0, y0, w, h, _p(rec), cap, _p(counts))
+        if rc == 1:
+            raise RuntimeError("oracle sample recorder rejected the scene")
+        if rc == 2:
+            raise RuntimeError("sample cap reached")
+        return rec[:counts.sum()], counts
 
     def ray_setup(self, x: int, y: int):
         out = np.zeros(8, np.float32)

@@ -323,12 +323,17 @@ class Renderer:
         c = (C.c_float * 4)(*rgba)
         self._check(self._L.beams_set_background(self._h, int(bool(on)), c))
 
-    def set_form(self, form: int, field_dtype: int = BF16):
-        """FORM_EXACT, or FORM_PRECISION with the 16-bit field dtype (BF16 or F16)."""
+    def set_form(self, form: int, field_dtype=BF16):
+        """FORM_EXACT; FORM_PRECISION with the 16-bit field dtype (BF16 or F16);
+        FORM_MLP with an MlpOptions (its knot, probe_fraction and fallback_tol
+        are read; None takes the defaults)."""
         opts = None
         if form == FORM_PRECISION:
             self._prec_opts = (C.c_int * 1)(int(field_dtype))
             opts = C.cast(self._prec_opts, C.c_void_p)
+        elif form == FORM_MLP and isinstance(field_dtype, MlpOptions):
+            self._mlp_render_opts = field_dtype
+            opts = C.cast(C.pointer(self._mlp_render_opts), C.c_void_p)
         self._check(self._L.beams_set_form(self._h, int(form), opts))
 
     # -- render ---------------------------------------------------------------

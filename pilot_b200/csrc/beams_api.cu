@@ -289,6 +289,10 @@ static beams_status check_sizes(beams_renderer* r, const beams_volume& v) {
   return BEAMS_OK;
 }
 
+beams_status mlp_set_render_options(beams_renderer* r, const beams_mlp_options* o);
+beams_status mlp_render_view(beams_renderer* r, const ExactGeo& g, float4* out, int& launches);
+bool mlp_ready(const beams_renderer* r);
+
 beams_status check_ready(beams_renderer* r) {
   if (r->brick_mode) {
     if (r->bricks.empty()) return fail(r, BEAMS_ERR_STATE, "no bricks set (beams_set_bricks)");
@@ -309,6 +313,11 @@ beams_status check_ready(beams_renderer* r) {
     return fail(r, BEAMS_ERR_UNSUPPORTED, "the exact form needs a float32 volume");
   if (r->form == BEAMS_FORM_PRECISION && r->vol.assoc != BEAMS_ASSOC_POINTS)
     return fail(r, BEAMS_ERR_UNSUPPORTED, "the precision form renders point fields");
+  if (r->form == BEAMS_FORM_MLP) {
+    if (r->vol.dtype != BEAMS_F32 || r->vol.assoc != BEAMS_ASSOC_POINTS)
+      return fail(r, BEAMS_ERR_UNSUPPORTED, "the MLP form renders float32 point fields");
+    if (!r->use_map) return fail(r, BEAMS_ERR_STATE, "the MLP form shades: enable the shadow map");
+  }
   const double nq = (double)(r->vol.dims[0] - 1) * (r->vol.dims[1] - 1) * r->vol.dims[2];
   if (nq >= 4294967296.0) return fail(r, BEAMS_ERR_UNSUPPORTED, "volume too large for 32-bit cell indexing");
   const double nv = (double)(r->map_m[0] + 1) * (r->map_m[1] + 1) * (r->map_m[2] + 1);
@@ -669,6 +678,12 @@ beams_status beams_set_form(beams_renderer* r, int form, const void* opts) {
     r->form = form;
     return BEAMS_OK;
   }
+  if (form == BEAMS_FORM_MLP) {
+    beams_status s = mlp_set_render_options(r, (const beams_mlp_options*)opts);
+    if (s != BEAMS_OK) return s;
+    r->form = form;
+    return BEAMS_OK;
+  }
   if (form == BEAMS_FORM_PRECISION) {
     int dt = BEAMS_BF16;
     if (opts) dt = ((const beams_precision_options*)opts)->field_dtype;
@@ -761,7 +776,8 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
   if (r->brick_mode) return render_bricks_frame(r, cam, rgba_out, out_on_device, t, launches);
   s = prepare_layouts(r, g, launches);
   if (s != BEAMS_OK) return s;
-  const bool need_map = r->use_map && r->vol.assoc == BEAMS_ASSOC_POINTS;
+  const bool use_mlp = r->form == BEAMS_FORM_MLP;
+  const bool need_map = r->use_map && r->vol.assoc == BEAMS_ASSOC_POINTS && !use_mlp;
   if (need_map) {
     s = build_map(r, g, launches, built);
     if (s != BEAMS_OK) return s;
@@ -775,7 +791,12 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
     if (s != BEAMS_OK) return s;
     dst = r->d_rgba;
   }
-  if (r->form == BEAMS_FORM_PRECISION && r->vol.assoc == BEAMS_ASSOC_POINTS)
+  if (use_mlp) {
+    s = mlp_render_view(r, g, dst, launches);
+    if (s != BEAMS_OK) return s;
+    --launches;  // counted below with the other view marches
+    e = cudaSuccess;
+  } else if (r->form == BEAMS_FORM_PRECISION && r->vol.assoc == BEAMS_ASSOC_POINTS)
     e = launch_view_march_prec(g, quad_dtype(r), r->d_quads, r->d_tab, r->d_tf,
                                need_map ? (const __half*)r->d_map : nullptr, dst, r->d_cnt, r->stream);
   else

@@ -18,6 +18,8 @@ cudaError_t launch_view_march_prec(const ExactGeo& g, int quad_dtype, const void
 cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    float* map, Counters* cnt, cudaStream_t st, const BrickRef* refs = nullptr,
                                    int nrefs = 0, int self = -1);
+size_t mlp_packed_bytes();
+cudaError_t launch_pack_weights(const float* P, uint2* W, float* aux, cudaStream_t st);
 cudaError_t launch_composite(const float4* imgs, int nb, size_t npix, const int* order, float4* out,
                              cudaStream_t st);
 cudaError_t launch_view_march_f32(const ExactGeo& g, const float* field, const float4* quads, const float4* tab,

@@ -36,8 +36,10 @@ struct MlpState {
   float4* lights = nullptr;  // training light positions (xyz)
   float4* lfeat = nullptr;   // their direction features
   int nlights = 0;
+  void* packed = nullptr;    // inference weights: B fragments + biases
+  beams_mlp_options render_opts{};
   ~MlpState() {
-    for (void* p : {(void*)P, (void*)G, (void*)m, (void*)v, ws_mem, (void*)lights, (void*)lfeat})
+    for (void* p : {(void*)P, (void*)G, (void*)m, (void*)v, ws_mem, (void*)lights, (void*)lfeat, packed})
       if (p) cudaFree(p);
   }
 };
@@ -125,6 +127,53 @@ static void init_params(std::vector<float>& h, unsigned seed) {
   fill(oW4, kHid, kHid * kHid, 1.f);
   fill(oW5, kHid, kHid, 0.5f);
   h[oB5] = 2.f;  // sigmoid(2) = 0.88: most of the volume is lit
+}
+
+cudaError_t launch_view_march_mlp(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
+                                  const uint2* W, const float* aux, const Encoding& enc, const float lf[3], int knot,
+                                  float4* out, Counters* cnt, cudaStream_t st);
+
+bool mlp_ready(const beams_renderer* r) { return r->mlp && r->mlp->ready; }
+
+beams_status mlp_set_render_options(beams_renderer* r, const beams_mlp_options* o) {
+  MlpState* st = mlp_state(r);
+  beams_mlp_options d;
+  std::memset(&d, 0, sizeof(d));
+  d.fallback_tol = 0.01f;
+  d.probe_fraction = 0.01f;
+  d.knot = 4;
+  if (o) {
+    if (o->knot < 1 || o->knot > 8) return fail(r, BEAMS_ERR_INVALID_ARG, "mlp form: knot must be in [1, 8]");
+    if (!(o->probe_fraction >= 0.f && o->probe_fraction <= 1.f) || !(o->fallback_tol >= 0.f))
+      return fail(r, BEAMS_ERR_INVALID_ARG, "mlp form: bad probe fraction or tolerance");
+    d.knot = o->knot;
+    d.fallback_tol = o->fallback_tol;
+    d.probe_fraction = o->probe_fraction;
+  }
+  st->render_opts = d;
+  return BEAMS_OK;
+}
+
+// The view march shaded by the network (no map is built).
+beams_status mlp_render_view(beams_renderer* r, const ExactGeo& g, float4* out, int& launches) {
+  MlpState* st = r->mlp;
+  if (!st || !st->ready) return fail(r, BEAMS_ERR_STATE, "mlp form: no trained or loaded network");
+  if (!st->packed) {
+    cudaError_t e = cudaMalloc(&st->packed, mlp_packed_bytes());
+    if (e != cudaSuccess) return cuda_fail(r, e, "allocating packed MLP weights");
+  }
+  uint2* W = (uint2*)st->packed;
+  float* aux = (float*)((char*)st->packed + (7 * 8 * 32 + 3 * 4 * 8 * 32) * sizeof(uint2));
+  cudaError_t e = launch_pack_weights(st->P, W, aux, r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "packing MLP weights");
+  ++launches;
+  float lf[3];
+  mlp_light_feature(r, g, lf);
+  e = launch_view_march_mlp(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, W, aux, mlp_encoding(g), lf,
+                            st->render_opts.knot, out, r->d_cnt, r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "mlp view march launch");
+  ++launches;
+  return BEAMS_OK;
 }
 
 }  // namespace beams

@@ -44,28 +44,51 @@ __device__ __forceinline__ float freq(int k) { return exp2f((float)(7 * k) / 15.
 
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
+// sin(pi x), cos(pi x): x is reduced to r = x - 2 rint(x/2) in [-1, 1] (exact in
+// float), then the hardware sine and cosine take pi r (|pi r| <= pi, where
+// their absolute error is about 2^-21); the features are rounded to bfloat16.
+__device__ __forceinline__ void sincospi_fast(float x, float* s, float* c) {
+  const float r = x - 2.f * rintf(0.5f * x);
+  __sincosf(3.14159265358979f * r, s, c);
+}
+
+// The (even) feature pair starting at column c of the encoding.
+__device__ __forceinline__ void feature_pair(const float u[3], const float l[3], int c, float& a, float& b) {
+  if (c >= 6 && c < kUsed) {
+    const int q = c - 6, ax = q >> 5, k = (q & 31) >> 1;
+    sincospi_fast(freq(k) * u[ax], &a, &b);
+  } else if (c == 0) {
+    a = u[0] * 2.f - 1.f;
+    b = u[1] * 2.f - 1.f;
+  } else if (c == 2) {
+    a = u[2] * 2.f - 1.f;
+    b = l[0];
+  } else if (c == 4) {
+    a = l[1];
+    b = l[2];
+  } else {
+    a = 0.f;
+    b = 0.f;
+  }
+}
+
 // Writes the kIn features of position p (world space) under light feature l.
+__device__ __forceinline__ void normalised(const Encoding& e, const float p[3], float u[3]) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) u[a] = (p[a] - e.bmin[a]) * e.inv_ext[a];
+}
+
 template <typename Out>
 __device__ __forceinline__ void encode(const Encoding& e, const float p[3], const float l[3], Out&& out) {
   float u[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    u[a] = (p[a] - e.bmin[a]) * e.inv_ext[a];
-    out(a, u[a] * 2.f - 1.f);
-    out(3 + a, l[a]);
+  normalised(e, p, u);
+#pragma unroll 1
+  for (int c = 0; c < kIn; c += 2) {
+    float a, b;
+    feature_pair(u, l, c, a, b);
+    out(c, a);
+    out(c + 1, b);
   }
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-#pragma unroll 4
-    for (int k = 0; k < kFreq; ++k) {
-      float s, c;
-      sincospif(freq(k) * u[a], &s, &c);
-      out(6 + a * 2 * kFreq + 2 * k, s);
-      out(6 + a * 2 * kFreq + 2 * k + 1, c);
-    }
-  }
-#pragma unroll
-  for (int i = kUsed; i < kIn; ++i) out(i, 0.f);
 }
 
 }  // namespace mlp

@@ -1,0 +1,106 @@
+"""Learned form, render side: the fused tensor-core view march against the
+float64 network applied to the oracle's lit samples, knot interpolation, and
+the trained network's gain over rendering without a shadow model."""
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as M
+from oracle.oracle import Oracle, psnr
+from pilot_b200 import beams as B
+from pilot_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def light_feature(s):
+    c = np.array([0.5 * (0 + (s.dims[i] - 1) * s.spacing[i]) for i in range(3)])
+    v = np.array(s.light, np.float64) - c if s.light_kind == 0 else -np.array(s.light, np.float64)
+    return v / np.linalg.norm(v)
+
+
+def oracle_mlp_image(s, P):
+    """The float64 network shading the oracle's lit samples, composited in order."""
+    o = Oracle(s)
+    rec, cnt = o.record_samples()
+    hi = np.array([(s.dims[i] - 1) * s.spacing[i] for i in range(3)])
+    X = M.encode(rec[:, :3], np.repeat(light_feature(s)[None, :], rec.shape[0], 0), (0, 0, 0), hi)
+    _, _, T = M.forward_backward(P, M.bf16(X), np.zeros(rec.shape[0]))
+    lc = np.float32(s.light_intensity) * np.array(s.light_color, np.float32)
+    img = np.zeros((s.height, s.width, 4), np.float32)
+    k = 0
+    for yy in range(s.height):
+        for xx in range(s.width):
+            c = np.zeros(4, np.float32)
+            for _ in range(cnt[yy, xx]):
+                r = rec[k]
+                t = np.float32(T[k])
+                for ch in range(3):
+                    c[ch] = c[ch] + np.float32(min(max(r[3 + ch] * (t * lc[ch]), 0.0), 1.0)) * r[6]
+                c[3] = r[6] + c[3]
+                k += 1
+            img[yy, xx] = c
+    return img
+
+
+def mlp_render(s, P=None, knot=1, r=None):
+    if r is None:
+        r = B.Renderer(0)
+        r.set_volume(s.field_numpy(), origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+        s.configure(r)
+    if P is not None:
+        r.mlp_set_params(P)
+    r.set_form(B.FORM_MLP, B.mlp_options(knot=knot))
+    img, t = r.render(s.camera())
+    return img, t, r
+
+
+def smooth_params(seed=7):
+    rng = np.random.default_rng(seed)
+    P = rng.normal(0, 0.08, M.N_PARAMS).astype(np.float32)
+    P[M.OFF["B5"][0]] = 0.5
+    return P
+
+
+def test_mlp_render_matches_float64_network(cuda_device):
+    s = scenes.small(61, n=32, image=40, m=8, kind="blobs")
+    P = smooth_params()
+    img, t, _ = mlp_render(s, P, knot=1)
+    ref = oracle_mlp_image(s, P)
+    err = np.abs(img - ref)
+    print(f"mlp render vs float64 network: max {err.max():.2e} mean {err.mean():.2e}; "
+          f"evals {t['mlp_samples']} lit {t['lit_samples']}")
+    assert t["map_vertices"] == 0 and t["mlp_samples"] == t["lit_samples"]
+    assert err.max() < 1e-2 and err.mean() < 1e-3
+    # alpha does not depend on the shading: identical to the exact path's
+    with B.Renderer(0) as q:
+        q.set_volume(s.field_numpy(), origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+        s.configure(q)
+        exact, _ = q.render(s.camera())
+    assert np.array_equal(img[..., 3], exact[..., 3])
+
+
+def test_mlp_knot_interpolation_close_to_every_sample(cuda_device):
+    s = scenes.small(62, n=40, image=64, m=8, kind="noise")
+    P = smooth_params(8)
+    i1, t1, r = mlp_render(s, P, knot=1)
+    i4, t4, _ = mlp_render(s, None, knot=4, r=r)
+    p = psnr(i1, i4)
+    print(f"knot 4 vs knot 1: PSNR {p:.1f} dB, evaluations {t4['mlp_samples']} vs {t1['mlp_samples']}")
+    assert t4["mlp_samples"] < 0.4 * t1["mlp_samples"] and p > 40
+
+
+def test_trained_mlp_render_beats_no_shadow_model(cuda_device):
+    s = scenes.small(63, n=48, image=64, m=24, kind="blobs", light_kind=0)
+    r = B.Renderer(0)
+    r.set_volume(s.field_numpy(), origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+    s.configure(r)
+    rep = r.mlp_train(B.mlp_options(samples_log2=18, epochs=8, batch=2048, lr=3e-3))
+    img, t, _ = mlp_render(s, None, knot=2, r=r)
+    o = Oracle(s)
+    ref64, _ = o.view_march(o.light_march(fp64=True)[0], fp64=True)
+    s2 = scenes.small(63, n=48, image=64, m=24, kind="blobs", light_kind=0)
+    s2.use_map = False
+    unlit, _ = Oracle(s2).view_march(None)
+    p_mlp, p_unlit = psnr(img, ref64), psnr(unlit, ref64)
+    print(f"trained MLP (holdout rmse {rep['holdout_rmse']:.3f}): PSNR {p_mlp:.1f} dB vs unshadowed {p_unlit:.1f} dB")
+    assert p_mlp > p_unlit + 3

@@ -185,6 +185,10 @@ typedef struct beams_mlp_options {
   float fallback_tol;    /* render: |MLP - exact| on the probe set that sends a tile to the exact map (0.01) */
   float probe_fraction;  /* render: fraction of pixels probed (0.01) */
   int knot;              /* render: MLP evaluated every `knot` lit samples, linear in between (1 = every sample) */
+  int scene_light;       /* train: 1 = the renderer's current light is training light 0 (a directional light
+                            stands in as a point at 1e4 x the diagonal); the rest on the Fibonacci sphere */
+  float focus;           /* train: fraction of positions drawn where the colour map's alpha is non-zero
+                            (rejection sampling, 16 tries); the rest uniform in the volume. 0 = all uniform */
 } beams_mlp_options;
 
 typedef struct beams_mlp_report {
@@ -207,6 +211,12 @@ beams_status beams_mlp_set_params(beams_renderer* r, const float* src, int n);
  * (n x 112 floats, rounded to bfloat16) and targets; T gets the predictions. */
 beams_status beams_mlp_loss_grad(beams_renderer* r, const float* features, const float* target, int n,
                                  float* loss, float* grad, float* T);
+/* Per-probe max |dRGBA| between the network's pixel and the pixel composited
+ * with the exact light march's transmittance, for the last BEAMS_FORM_MLP frame
+ * (row-major over the probe grid: probe (i, j) is pixel (i*P + P/2, j*P + P/2),
+ * P = round(1/sqrt(probe_fraction))); +inf marks a probe past the sample cap.
+ * n must be the probe count; for tests and tools. */
+beams_status beams_mlp_probe_errors(beams_renderer* r, float* dst, int n);
 /* The network's input encoding of n world positions under n light features. */
 beams_status beams_mlp_encode(beams_renderer* r, const float* pos, const float* lfeat, int n, float* out);
 /* Versioned checkpoint of parameters and Adam moments (FNV-1a checksummed). */

@@ -874,6 +874,29 @@ extern "C" int oracle_generate_noise(float* out, int nx, int ny, int nz, const u
   return 0;
 }
 
+template <typename T>
+static int light_march_points(const oracle_scene* s, const T* pts, int64_t n, const T* light_pos, T* out,
+                              int threads) {
+  if (!valid(s) || !pts || !out) return 1;
+  Geo<T> g;
+  build_geo(s, g);
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads(threads))
+  for (int64_t i = 0; i < n; ++i) {
+    const T P[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
+    T L[3];
+    if (light_pos) {
+      L[0] = light_pos[3 * i];
+      L[1] = light_pos[3 * i + 1];
+      L[2] = light_pos[3 * i + 2];
+    } else {
+      light_origin(g, P, L);
+    }
+    uint64_t ns = 0;
+    out[i] = light_march_point(g, L, P, ns);
+  }
+  return 0;
+}
+
 extern "C" {
 
 int oracle_light_march_f32(const oracle_scene* s, float* out, int threads, uint64_t* samples) {
@@ -893,24 +916,11 @@ int oracle_light_march_ids_f64(const oracle_scene* s, const int64_t* ids, int64_
 
 int oracle_light_march_points_f64(const oracle_scene* s, const double* pts, int64_t n,
                                   const double* light_pos, double* out, int threads) {
-  if (!valid(s) || !pts || !out) return 1;
-  Geo<double> g;
-  build_geo(s, g);
-#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads(threads))
-  for (int64_t i = 0; i < n; ++i) {
-    const double P[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
-    double L[3];
-    if (light_pos) {
-      L[0] = light_pos[3 * i];
-      L[1] = light_pos[3 * i + 1];
-      L[2] = light_pos[3 * i + 2];
-    } else {
-      light_origin(g, P, L);
-    }
-    uint64_t ns = 0;
-    out[i] = light_march_point(g, L, P, ns);
-  }
-  return 0;
+  return light_march_points<double>(s, pts, n, light_pos, out, threads);
+}
+int oracle_light_march_points_f32(const oracle_scene* s, const float* pts, int64_t n, const float* light_pos,
+                                  float* out, int threads) {
+  return light_march_points<float>(s, pts, n, light_pos, out, threads);
 }
 
 int oracle_view_march_f32(const oracle_scene* s, const float* map, int x0, int y0, int w, int h,

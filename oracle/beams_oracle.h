@@ -65,6 +65,8 @@ int oracle_light_march_ids_f64(const oracle_scene* s, const int64_t* ids, int64_
 /* Transmittance 1 - o at arbitrary points (march from the light to each point). */
 int oracle_light_march_points_f64(const oracle_scene* s, const double* pts, int64_t n,
                                   const double* light_pos, double* opacity_out, int threads);
+int oracle_light_march_points_f32(const oracle_scene* s, const float* pts, int64_t n, const float* light_pos,
+                                  float* out, int threads);
 
 /* View march over the pixel window [x0,x0+w) x [y0,y0+h); rgba_out is w*h*4.
  * map may be NULL when use_map == 0. lazy != 0: ignore map and compute the map

@@ -41,6 +41,7 @@ def lib():
             "oracle_light_march_ids_f32": [S, P, C.c_int64, P, C.c_int, u64p],
             "oracle_light_march_ids_f64": [S, P, C.c_int64, P, C.c_int, u64p],
             "oracle_light_march_points_f64": [S, P, C.c_int64, P, P, C.c_int],
+            "oracle_light_march_points_f32": [S, P, C.c_int64, P, P, C.c_int],
             "oracle_view_march_f32": [S, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
             "oracle_view_march_f64": [S, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
             "oracle_view_march_lazy_f64": [S, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
@@ -102,12 +103,14 @@ class Oracle:
             raise RuntimeError("oracle light march rejected the scene")
         return out, ns.value
 
-    def point_opacity(self, pts: np.ndarray, light_pos: np.ndarray | None = None):
-        pts = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
-        out = np.empty(pts.shape[0], np.float64)
-        lp = None if light_pos is None else np.ascontiguousarray(light_pos, np.float64).reshape(-1, 3)
-        if lib().oracle_light_march_points_f64(C.byref(self.cs), _p(pts), pts.shape[0],
-                                               None if lp is None else _p(lp), _p(out), self.threads):
+    def point_opacity(self, pts: np.ndarray, light_pos: np.ndarray | None = None, fp64: bool = True):
+        """Light-march opacity from the light (or light_pos per point) to each point."""
+        dt = np.float64 if fp64 else np.float32
+        pts = np.ascontiguousarray(pts, dt).reshape(-1, 3)
+        out = np.empty(pts.shape[0], dt)
+        lp = None if light_pos is None else np.ascontiguousarray(light_pos, dt).reshape(-1, 3)
+        fn = lib().oracle_light_march_points_f64 if fp64 else lib().oracle_light_march_points_f32
+        if fn(C.byref(self.cs), _p(pts), pts.shape[0], None if lp is None else _p(lp), _p(out), self.threads):
             raise RuntimeError("oracle point march rejected the scene")
         return out
 

@@ -30,7 +30,7 @@ FORM_EXACT, FORM_PRECISION, FORM_MLP = 0, 1, 2
 class MlpOptions(C.Structure):
     _fields_ = [("samples_log2", C.c_int), ("n_lights", C.c_int), ("epochs", C.c_int), ("batch", C.c_int),
                 ("lr", C.c_float), ("seed", C.c_uint), ("fallback_tol", C.c_float), ("probe_fraction", C.c_float),
-                ("knot", C.c_int)]
+                ("knot", C.c_int), ("scene_light", C.c_int), ("focus", C.c_float)]
 
 
 class MlpReport(C.Structure):
@@ -43,8 +43,9 @@ class MlpReport(C.Structure):
 
 
 def mlp_options(samples_log2=24, n_lights=32, epochs=4, batch=16384, lr=2e-3, seed=1, fallback_tol=0.01,
-                probe_fraction=0.01, knot=4):
-    return MlpOptions(samples_log2, n_lights, epochs, batch, lr, seed, fallback_tol, probe_fraction, knot)
+                probe_fraction=0.01, knot=4, scene_light=0, focus=0.875):
+    return MlpOptions(samples_log2, n_lights, epochs, batch, lr, seed, fallback_tol, probe_fraction, knot,
+                      scene_light, focus)
 
 
 class BeamsError(RuntimeError):
@@ -118,6 +119,7 @@ def lib():
         "beams_mlp_set_params": ([P, P, C.c_int], C.c_int),
         "beams_mlp_loss_grad": ([P, P, P, C.c_int, C.POINTER(C.c_float), P, P], C.c_int),
         "beams_mlp_encode": ([P, P, P, C.c_int, P], C.c_int),
+        "beams_mlp_probe_errors": ([P, P, C.c_int], C.c_int),
         "beams_mlp_save": ([P, C.c_char_p], C.c_int),
         "beams_mlp_load": ([P, C.c_char_p], C.c_int),
         "beams_get_brick_map": ([P, C.c_int, C.c_int, P, C.c_size_t, C.c_int], C.c_int),
@@ -275,6 +277,11 @@ class Renderer:
         lf = np.ascontiguousarray(lfeat, np.float32).reshape(-1, 3)
         out = np.empty((pos.shape[0], 112), np.float32)
         self._check(self._L.beams_mlp_encode(self._h, _ptr(pos), _ptr(lf), pos.shape[0], _ptr(out)))
+        return out
+
+    def mlp_probe_errors(self, n):
+        out = np.empty(n, np.float32)
+        self._check(self._L.beams_mlp_probe_errors(self._h, _ptr(out), int(n)))
         return out
 
     def mlp_save(self, path):

@@ -490,12 +490,12 @@ beams_status beams_create(beams_renderer** out, int device, void* stream) {
       return cuda_fail(nullptr, e, "cudaEventCreate");
     }
   }
-  e = cudaMalloc((void**)&r->d_cnt, sizeof(Counters));
+  e = cudaMalloc((void**)&r->d_cnt, 2 * sizeof(Counters));  // [1]: the learned form's fallback pass
   if (e != cudaSuccess) {
     delete r;
     return cuda_fail(nullptr, e, "allocating counters");
   }
-  e = cudaMemset(r->d_cnt, 0, sizeof(Counters));
+  e = cudaMemset(r->d_cnt, 0, 2 * sizeof(Counters));
   if (e != cudaSuccess) {
     delete r;
     return cuda_fail(nullptr, e, "clearing counters");
@@ -769,7 +769,7 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
   s = make_geo_vol(r, r->brick_mode ? r->bricks[0].vol : r->vol, cam, g);
   if (s != BEAMS_OK) return s;
   int launches = 0;
-  cudaError_t e = cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), r->stream);
+  cudaError_t e = cudaMemsetAsync(r->d_cnt, 0, 2 * sizeof(Counters), r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "clearing counters");
   cudaEventRecord(r->ev[0], r->stream);
   bool built = false;
@@ -826,7 +826,9 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
     t->lit_samples = c.lit_samples;
     t->rays_hit = c.rays_hit;
     t->mlp_samples = c.mlp_samples;
-    t->map_vertices = built ? (int)r->map_count : 0;
+    t->fallback_tiles = (int)c.fallback_tiles;
+    if (use_mlp && c.fallback_tiles) built = true;  // the fallback's gated map build ran
+    t->map_vertices = built ? (int)((size_t)g.pd[0] * g.pd[1] * g.pd[2]) : 0;
     t->kernel_launches = launches;
   } else if (!out_on_device) {
     // The caller reads rgba_out on return.

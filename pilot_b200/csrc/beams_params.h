@@ -55,6 +55,8 @@ struct BrickRef {
 };
 
 constexpr int kMaxBricks = 32;
+// Learned form: pixel tile that falls back to the exact map as a unit.
+constexpr int kFallbackTile = 32;
 
 // Counters written by the kernels (one atomic per warp).
 struct Counters {

@@ -344,6 +344,45 @@ template <> struct QuadLoad<float4> {
   }
 };
 
+// The light march of TransmittanceMap.h:279-332 from L to an arbitrary point P
+// (K1 runs it to map vertices): opacity accumulated over the same sample
+// sequence. T0..T2: field cell tables; s_a: TF alpha / max alpha.
+__device__ __forceinline__ float point_opacity(const ExactGeo& g, const float4* __restrict__ quads, const float4* T0,
+                                               const float4* T1, const float4* T2, const float* s_a, const float L[3],
+                                               const float P[3]) {
+  const float v[3] = {P[0] - L[0], P[1] - L[1], P[2] - L[2]};
+  const float rs = 1.f / sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  const float dir[3] = {v[0] * rs, v[1] * rs, v[2] * rs};
+  float tmin, tmax;
+  segment_aabb(g, L, P, tmin, tmax);
+  const float st[3] = {L[0] + tmin * dir[0], L[1] + tmin * dir[1], L[2] + tmin * dir[2]};
+  float s[3] = {st[0], st[1], st[2]};
+  const float len2 = (tmax - tmin) * (tmax - tmin);
+  const int n1 = g.tf_n - 1;
+  const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
+  float o = 0.f;
+  for (int b = g.light_budget; b > 0; --b) {
+    const float q0 = s[0] - st[0], q1 = s[1] - st[1], q2 = s[2] - st[2];
+    if (!(q0 * q0 + q1 * q1 + q2 * q2 <= len2)) break;
+    s[0] = s[0] + g.step * dir[0];
+    s[1] = s[1] + g.step * dir[1];
+    s[2] = s[2] + g.step * dir[2];
+    if (!inside_vol(g, s)) break;
+    float4 e0, e1, e2;
+    const int c0 = find_cell_bsearch_t(T0, g.n[0] - 2, g.org[0], g.invh[0], s[0], e0);
+    const int c1 = find_cell_bsearch_t(T1, g.n[1] - 2, g.org[1], g.invh[1], s[1], e1);
+    const int c2 = find_cell_bsearch_t(T2, g.n[2] - 2, g.org[2], g.invh[2], s[2], e2);
+    float vals[8];
+    QuadLoad<float4>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qz, vals);
+    float scalar = hex_interp(vals, div_rn_markstein(s[0] - e0.x, e0.z, e0.w), div_rn_markstein(s[1] - e1.x, e1.z, e1.w),
+                              div_rn_markstein(s[2] - e2.x, e2.z, e2.w));
+    scalar = (scalar - g.min_scalar) * g.inv_delta;
+    o = o + (1.f - o) * s_a[tf_index_clamped(scalar * (float)n1, n1)];
+    if (o == 1.f) break;
+  }
+  return o;
+}
+
 // Warp-aggregated counter increment (one atomic per warp). Must be reached by
 // all 32 lanes of the warp (kernels keep out-of-range lanes alive with v = 0);
 // blocks are one-dimensional.

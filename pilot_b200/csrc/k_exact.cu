@@ -21,6 +21,7 @@
 
 #include "exact_device.cuh"
 #include "kernels.h"
+#include "view_march.cuh"
 
 namespace beams {
 
@@ -87,7 +88,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
                                                           void* __restrict__ map, int nvert,
                                                           Counters* __restrict__ cnt,
                                                           const BrickRef* __restrict__ refs, int nrefs,
-                                                          int self) {
+                                                          int self, const unsigned* __restrict__ gate) {
+  // gate: the learned form's fallback builds the map only when a tile failed its probes
+  if (gate && *gate == 0u) return;
   extern __shared__ float4 s_dyn[];
   const int nfield = g.max_off[0];             // field-axis table entries only
   float4* s_tab = s_dyn;
@@ -186,130 +189,15 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
 // ---------------------------------------------------------------------------
 // K2 (point field)
 // ---------------------------------------------------------------------------
-// 8x4-pixel warp tiles; tiles_x = ceil(width / 8).
-__device__ __forceinline__ void tile_pixel(int tiles_x, int tile, int& x, int& y) {
-  const int lane = threadIdx.x & 31;
-  const int bx = tile % tiles_x, by = tile / tiles_x;
-  x = (bx << 3) + (lane & 7);
-  y = (by << 2) + (lane >> 3);
-}
-
-// Next warp tile from the frame's counter (one atomic per warp tile).
-__device__ __forceinline__ int next_warp_tile(unsigned* counter) {
-  unsigned t = 0;
-  if ((threadIdx.x & 31) == 0) t = atomicAdd(counter, 1u);
-  return (int)__shfl_sync(0xffffffffu, t, 0);
-}
-
-template <typename QuadT, bool USE_MAP, typename MapT>
-__device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT* __restrict__ quads,
-                                                 const float4* s_tab, const float4* s_tf,
-                                                 const MapT* __restrict__ map, int x, int y, float4& color,
-                                                 unsigned& lit, unsigned& hit) {
-  color = make_float4(0.f, 0.f, 0.f, 0.f);
-  float o[3], d[3], minD, maxD;
-  if (!ray_setup(g, x, y, o, d, minD, maxD)) return;
-  hit += 1;
-  const float qd = (maxD - minD) / g.sd;
-  long long budget = (qd < 1e9f) ? (long long)qd + 16 : 1000000000ll;
-  float dist = minD + g.mesh_eps;
-  float p[3] = {o[0] + dist * d[0], o[1] + dist * d[1], o[2] + dist * d[2]};
-  while (!inside_vol(g, p) && dist < maxD && budget-- > 0) {
-    dist += g.sd;
-    p[0] = o[0] + dist * d[0];
-    p[1] = o[1] + dist * d[1];
-    p[2] = o[2] + dist * d[2];
-  }
-  const float sdx = g.sd * d[0], sdy = g.sd * d[1], sdz = g.sd * d[2];
-  const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
-  float bl[3] = {0.f, 0.f, 0.f};
-  bool newCell = true;
-  float tx = 0.f, ty = 0.f, tz = 0.f;
-  float s0 = 0.f, s1m0 = 0.f, s2m3 = 0.f, s3 = 0.f, s4 = 0.f, s5m4 = 0.f, s6m7 = 0.f, s7 = 0.f;
-  int c[3] = {0, 0, 0};
-  float inv[3] = {0.f, 0.f, 0.f};
-  const int n1 = g.tf_n - 1;
-  while (inside_vol(g, p) && dist < maxD && budget-- > 0) {
-    const float mint = mn(tx, mn(ty, tz));
-    const float maxt = mx(tx, mx(ty, tz));
-    if (maxt > 1.f || mint < 0.f) newCell = true;
-    if (newCell) {
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const float4* T = s_tab + g.ax_off[k];
-        float4 e;
-        if (p[k] == g.maxp[k]) {
-          c[k] = g.n[k] - 2;  // the reference leaves invSpacing[k] unchanged here
-          e = T[c[k]];
-        } else {
-          c[k] = find_cell_walk_t(T, g.n[k] - 2, g.org[k], g.invh[k], p[k], e);
-          inv[k] = e.w;  // 1.f / (coord(c+1) - coord(c)), IEEE
-        }
-        bl[k] = e.x;
-      }
-      float v[8];
-      QuadLoad<QuadT>::cell(quads, (unsigned)c[2] * qz + (unsigned)c[1] * qx + (unsigned)c[0], qz, v);
-      s0 = v[0];
-      s3 = v[3];
-      s4 = v[4];
-      s7 = v[7];
-      s6m7 = v[6] - v[7];
-      s5m4 = v[5] - v[4];
-      s1m0 = v[1] - v[0];
-      s2m3 = v[2] - v[3];
-      tx = (p[0] - bl[0]) * inv[0];
-      ty = (p[1] - bl[1]) * inv[1];
-      tz = (p[2] - bl[2]) * inv[2];
-      newCell = false;
-    }
-    const float l76 = s7 + tx * s6m7;
-    const float l45 = s4 + tx * s5m4;
-    const float top = l45 + ty * (l76 - l45);
-    const float l01 = s0 + tx * s1m0;
-    const float l32 = s3 + tx * s2m3;
-    const float bot = l01 + ty * (l32 - l01);
-    float fs = bot + tz * (top - bot);
-    fs = (fs - g.min_scalar) * g.inv_delta;
-    const float fi = fs * (float)n1;
-    if (fi > -1.f && fi < (float)(n1 + 1)) {
-      const float4 tfc = s_tf[(int)fi];
-      float sc0 = tfc.x, sc1 = tfc.y, sc2 = tfc.z;
-      const float sa = tfc.w * (1.f - color.w);
-      if (USE_MAP) {
-        // exact form: 1 - opacity (TransmittanceMap.h:195); precision form: stored transmittance
-        const float mv = map_interp_t<MapT>(g, s_tab, map, p);
-        const float tr = (sizeof(MapT) == 2) ? mv : 1.f - mv;
-        sc0 = sc0 * (tr * g.light_color[0]);
-        sc1 = sc1 * (tr * g.light_color[1]);
-        sc2 = sc2 * (tr * g.light_color[2]);
-      }
-      sc0 = clamp01(sc0);
-      sc1 = clamp01(sc1);
-      sc2 = clamp01(sc2);
-      color.x = color.x + sc0 * sa;
-      color.y = color.y + sc1 * sa;
-      color.z = color.z + sc2 * sa;
-      color.w = sa + color.w;
-      ++lit;
-    }
-    dist += g.sd;
-    p[0] = p[0] + sdx;
-    p[1] = p[1] + sdy;
-    p[2] = p[2] + sdz;
-    tx = (p[0] - bl[0]) * inv[0];
-    ty = (p[1] - bl[1]) * inv[1];
-    tz = (p[2] - bl[2]) * inv[2];
-    if (color.w >= g.cutoff) break;
-  }
-}
-
-template <typename QuadT, bool USE_MAP, typename MapT>
+template <typename QuadT, bool USE_MAP, typename MapT, bool LIST = false>
 __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const QuadT* __restrict__ quads,
                                                          const float4* __restrict__ tab,
                                                          const float4* __restrict__ tf,
                                                          const MapT* __restrict__ map,
                                                          float4* __restrict__ out,
-                                                         Counters* __restrict__ cnt) {
+                                                         Counters* __restrict__ cnt,
+                                                         const unsigned* __restrict__ flist = nullptr,
+                                                         const unsigned* __restrict__ fcount = nullptr) {
   extern __shared__ float4 s_dyn[];
   float4* s_tab = s_dyn;
   float4* s_tf = s_dyn + g.ntab;
@@ -317,11 +205,19 @@ __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const
   for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) s_tf[i] = tf[i];
   __syncthreads();
   const int tiles_x = (g.width + 7) >> 3;
-  const int ntiles = tiles_x * ((g.height + 3) >> 2);
+  // flist: only the listed kFallbackTile^2 tiles (32 warp tiles each) are marched
+  const int ntiles = LIST ? (int)(*fcount) * 32 : tiles_x * ((g.height + 3) >> 2);
+  const int ftx = (g.width + kFallbackTile - 1) / kFallbackTile;
   unsigned lit = 0, hit = 0;
   for (int tile = next_warp_tile(&cnt->tiles_view); tile < ntiles; tile = next_warp_tile(&cnt->tiles_view)) {
     int x, y;
-    tile_pixel(tiles_x, tile, x, y);
+    if (LIST) {
+      const int f = (int)flist[tile >> 5], sub = tile & 31, lane = threadIdx.x & 31;
+      x = (f % ftx) * kFallbackTile + ((sub & 3) << 3) + (lane & 7);
+      y = (f / ftx) * kFallbackTile + ((sub >> 2) << 2) + (lane >> 3);
+    } else {
+      tile_pixel(tiles_x, tile, x, y);
+    }
     if (x < g.width && y < g.height) {
       float4 color;
       view_march_pixel<QuadT, USE_MAP, MapT>(g, quads, s_tab, s_tf, map, x, y, color, lit, hit);
@@ -558,7 +454,7 @@ cudaError_t launch_build_quads(const void* field, int in_dtype, void* quads, int
 template <typename QuadT, bool STITCH, bool PREC>
 static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4* tab, const float4* tf,
                              const float* tau, void* map, Counters* cnt, cudaStream_t st, const BrickRef* refs,
-                             int nrefs, int self) {
+                             int nrefs, int self, const unsigned* gate = nullptr) {
   const int nvert = g.pd[0] * g.pd[1] * g.pd[2];
   const size_t smem = (size_t)g.max_off[0] * sizeof(float4) + 2 * (size_t)g.tf_n * sizeof(float);
   const int ntiles = (nvert + kThreads - 1) / kThreads;
@@ -566,15 +462,15 @@ static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4*
   cudaError_t e = persistent_grid(k_light_march<QuadT, STITCH, PREC>, smem, ntiles, grid);
   if (e != cudaSuccess) return e;
   k_light_march<QuadT, STITCH, PREC><<<grid, kThreads, smem, st>>>(g, (const QuadT*)quads, tab, tf, tau, map,
-                                                                   nvert, cnt, refs, nrefs, self);
+                                                                   nvert, cnt, refs, nrefs, self, gate);
   return cudaGetLastError();
 }
 
 cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    float* map, Counters* cnt, cudaStream_t st, const BrickRef* refs, int nrefs,
-                                   int self) {
-  if (refs) return launch_k1<float4, true, false>(g, quads, tab, tf, nullptr, map, cnt, st, refs, nrefs, self);
-  return launch_k1<float4, false, false>(g, quads, tab, tf, nullptr, map, cnt, st, nullptr, 0, -1);
+                                   int self, const unsigned* gate) {
+  if (refs) return launch_k1<float4, true, false>(g, quads, tab, tf, nullptr, map, cnt, st, refs, nrefs, self, gate);
+  return launch_k1<float4, false, false>(g, quads, tab, tf, nullptr, map, cnt, st, nullptr, 0, -1, gate);
 }
 
 cudaError_t launch_light_march_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,
@@ -635,6 +531,19 @@ cudaError_t launch_view_march_f32(const ExactGeo& g, const float* field, const f
     if (e != cudaSuccess) return e;
     k_view_march<float4, false, float><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, nullptr, out, cnt);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_view_march_tiles(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
+                                    const float* map, float4* out, Counters* cnt, const unsigned* flist,
+                                    const unsigned* fcount, cudaStream_t st) {
+  const size_t smem = ((size_t)g.ntab + (size_t)g.tf_n) * sizeof(float4);
+  const int ntiles = (((g.width + 7) >> 3) * ((g.height + 3) >> 2) + 7) / 8;  // upper bound
+  int grid = 0;
+  cudaError_t e = persistent_grid(k_view_march<float4, true, float, true>, smem, ntiles, grid);
+  if (e != cudaSuccess) return e;
+  k_view_march<float4, true, float, true><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, map, out, cnt, flist,
+                                                                        fcount);
   return cudaGetLastError();
 }
 

@@ -1,0 +1,200 @@
+// k_mlp_probe.cu — the learned form's per-tile check against the exact light march.
+//
+// A regular 1-in-P x 1-in-P grid of probe pixels (P = round(1/sqrt(fraction)),
+// offset P/2) is re-marched after the network has shaded the frame:
+//   1. k_probe_record: each probe pixel's view march (the K2 body, no map)
+//      records its compositing samples (sa > 0): position, TF colour and
+//      premultiplied alpha, up to kProbeCap per pixel;
+//   2. k_probe_transmittance: one thread per recorded sample runs the exact
+//      light march (TransmittanceMap.h:279-332) from the light to that point;
+//   3. k_probe_compare: each probe pixel composites its samples with the exact
+//      transmittance (the shading of Sampler::operator(),
+//      LightedVolumeRenderer.cxx:456-475) and compares with the network's
+//      pixel; a kFallbackTile^2 tile whose max |dRGBA| exceeds the tolerance
+//      (or that holds no probe, or a probe past the cap) joins the fallback
+//      list.
+// The host then launches K1 gated on the list being non-empty and K2 over the
+// listed tiles, so a failing tile is exactly the exact form's pixels.
+// Compiled with -fmad=false like every kernel file.
+#include <cuda_runtime.h>
+
+#include "exact_device.cuh"
+#include "kernels.h"
+#include "view_march.cuh"
+
+namespace beams {
+
+namespace {
+
+constexpr int kThreadsP = 256;
+
+struct ProbeGrid {
+  int P, h, nqx, nqy;  // stride, offset, probes per row / column
+};
+
+__host__ __device__ inline int probes_along(int n, int P, int h) { return n > h ? (n - h - 1) / P + 1 : 0; }
+
+// Records compositing samples (sa > 0) of one pixel: {x, y, z, T} and {r, g, b, sa}.
+struct SampleRecorder {
+  float4* rec;
+  int n, cap;
+  __device__ __forceinline__ void operator()(const float* p, const float4& tfc, float sa) {
+    if (!(sa > 0.f)) return;
+    if (n < cap) {
+      rec[2 * n] = make_float4(p[0], p[1], p[2], 1.f);
+      rec[2 * n + 1] = make_float4(tfc.x, tfc.y, tfc.z, sa);
+    }
+    ++n;
+  }
+};
+
+__global__ void __launch_bounds__(kThreadsP) k_probe_record(const ExactGeo g, const float4* __restrict__ quads,
+                                                            const float4* __restrict__ tab,
+                                                            const float4* __restrict__ tf, ProbeGrid pg, int cap,
+                                                            float4* __restrict__ rec, int* __restrict__ count) {
+  extern __shared__ float4 s_dyn[];
+  float4* s_tab = s_dyn;
+  float4* s_tf = s_dyn + g.ntab;
+  for (int i = threadIdx.x; i < g.ntab; i += blockDim.x) s_tab[i] = tab[i];
+  for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) s_tf[i] = tf[i];
+  __syncthreads();
+  const int nprobe = pg.nqx * pg.nqy;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nprobe; q += gridDim.x * blockDim.x) {
+    const int x = (q % pg.nqx) * pg.P + pg.h, y = (q / pg.nqx) * pg.P + pg.h;
+    SampleRecorder r{rec + (size_t)q * cap * 2, 0, cap};
+    float4 color;
+    unsigned lit = 0, hit = 0;
+    view_march_pixel<float4, false, float, SampleRecorder>(g, quads, s_tab, s_tf, nullptr, x, y, color, lit, hit,
+                                                           &r);
+    count[q] = r.n;
+  }
+}
+
+__global__ void __launch_bounds__(kThreadsP) k_probe_transmittance(const ExactGeo g, const float4* __restrict__ quads,
+                                                                   const float4* __restrict__ tab,
+                                                                   const float4* __restrict__ tf, int nprobe,
+                                                                   int cap, float4* __restrict__ rec,
+                                                                   const int* __restrict__ count) {
+  extern __shared__ float4 s_dyn[];
+  const int nfield = g.max_off[0];
+  float4* s_tab = s_dyn;
+  float* s_a = (float*)(s_dyn + nfield);
+  for (int i = threadIdx.x; i < nfield; i += blockDim.x) s_tab[i] = tab[i];
+  for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) s_a[i] = (g.max_alpha > 0.f) ? tf[i].w / g.max_alpha : 0.f;
+  __syncthreads();
+  const size_t total = (size_t)nprobe * cap;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int q = (int)(i / cap), k = (int)(i - (size_t)q * cap);
+    if (k >= count[q]) continue;
+    float4* slot = rec + 2 * i;
+    const float4 pw = *slot;
+    const float P[3] = {pw.x, pw.y, pw.z};
+    float L[3];
+    light_origin(g, P, L);
+    const float o = point_opacity(g, quads, s_tab + g.ax_off[0], s_tab + g.ax_off[1], s_tab + g.ax_off[2], s_a, L, P);
+    slot->w = 1.f - o;
+  }
+}
+
+__global__ void k_probe_compare(const ExactGeo g, ProbeGrid pg, int cap, const float4* __restrict__ rec,
+                                const int* __restrict__ count, const float4* __restrict__ img, float tol,
+                                unsigned* __restrict__ flags, unsigned* __restrict__ flist,
+                                unsigned* __restrict__ fcount, float* __restrict__ probe_err,
+                                Counters* __restrict__ cnt) {
+  const int nprobe = pg.nqx * pg.nqy;
+  const int ftx = (g.width + kFallbackTile - 1) / kFallbackTile;
+  const int fty = (g.height + kFallbackTile - 1) / kFallbackTile;
+  const int ntiles = ftx * fty;
+  const int n = nprobe > ntiles ? nprobe : ntiles;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int flag_tile = -1;
+    if (i < nprobe) {
+      const int x = (i % pg.nqx) * pg.P + pg.h, y = (i / pg.nqx) * pg.P + pg.h;
+      const int m = count[i];
+      float err = __int_as_float(0x7f800000);
+      if (m <= cap) {
+        const float4* r = rec + (size_t)i * cap * 2;
+        float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int k = 0; k < m; ++k) {
+          const float4 pw = r[2 * k], tc = r[2 * k + 1];
+          const float tr = pw.w;
+          const float s0 = clamp01(tc.x * (tr * g.light_color[0]));
+          const float s1 = clamp01(tc.y * (tr * g.light_color[1]));
+          const float s2 = clamp01(tc.z * (tr * g.light_color[2]));
+          c.x = c.x + s0 * tc.w;
+          c.y = c.y + s1 * tc.w;
+          c.z = c.z + s2 * tc.w;
+          c.w = tc.w + c.w;
+        }
+        const float4 v = img[(size_t)y * g.width + x];
+        err = fmaxf(fmaxf(fabsf(v.x - c.x), fabsf(v.y - c.y)), fmaxf(fabsf(v.z - c.z), fabsf(v.w - c.w)));
+        if (v.x != v.x || v.y != v.y || v.z != v.z || v.w != v.w) err = __int_as_float(0x7f800000);
+      }
+      if (probe_err) probe_err[i] = err;
+      if (!(err <= tol)) flag_tile = (y / kFallbackTile) * ftx + x / kFallbackTile;
+    }
+    if (flag_tile < 0 && i < ntiles) {
+      // a tile that holds no probe pixel cannot be checked: it always falls back
+      const int tx = i % ftx, ty = i / ftx;
+      const int x0 = tx * kFallbackTile, x1 = min(x0 + kFallbackTile, g.width);
+      const int y0 = ty * kFallbackTile, y1 = min(y0 + kFallbackTile, g.height);
+      // first probe column/row at or after x0 / y0
+      const int kx = x0 <= pg.h ? 0 : (x0 - pg.h + pg.P - 1) / pg.P;
+      const int ky = y0 <= pg.h ? 0 : (y0 - pg.h + pg.P - 1) / pg.P;
+      const bool has = kx < pg.nqx && kx * pg.P + pg.h < x1 && ky < pg.nqy && ky * pg.P + pg.h < y1;
+      if (!has) flag_tile = i;
+    }
+    if (flag_tile >= 0 && atomicExch(&flags[flag_tile], 1u) == 0u) {
+      flist[atomicAdd(fcount, 1u)] = (unsigned)flag_tile;
+      atomicAdd(&cnt->fallback_tiles, 1ull);
+    }
+  }
+}
+
+int grid_for(size_t n, int threads, int cap_blocks) {
+  size_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > (size_t)cap_blocks) b = cap_blocks;
+  return (int)b;
+}
+
+}  // namespace
+
+ProbeLayout probe_layout(int width, int height, float fraction) {
+  ProbeLayout L{};
+  if (!(fraction > 0.f)) return L;
+  int P = (int)lrintf(1.f / sqrtf(fminf(fraction, 1.f)));
+  if (P < 1) P = 1;
+  L.stride = P;
+  L.offset = P / 2;
+  L.nqx = probes_along(width, P, L.offset);
+  L.nqy = probes_along(height, P, L.offset);
+  L.nprobe = L.nqx * L.nqy;
+  L.ntiles = ((width + kFallbackTile - 1) / kFallbackTile) * ((height + kFallbackTile - 1) / kFallbackTile);
+  L.cap = kProbeCap;
+  return L;
+}
+
+cudaError_t launch_mlp_probe(const ExactGeo& g, const ProbeLayout& L, const float4* quads, const float4* tab,
+                             const float4* tf, const float4* img, float tol, float4* rec, int* count, unsigned* flags,
+                             unsigned* flist, unsigned* fcount, float* probe_err, Counters* cnt, cudaStream_t st) {
+  if (L.nprobe < 0 || L.cap < 1) return cudaErrorInvalidValue;
+  const ProbeGrid pg{L.stride, L.offset, L.nqx, L.nqy};
+  cudaError_t e;
+  if (L.nprobe > 0) {
+    const size_t smem1 = ((size_t)g.ntab + (size_t)g.tf_n) * sizeof(float4);
+    e = cudaFuncSetAttribute(k_probe_record, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1);
+    if (e != cudaSuccess) return e;
+    k_probe_record<<<grid_for(L.nprobe, 64, 148 * 8), 64, smem1, st>>>(g, quads, tab, tf, pg, L.cap, rec, count);
+    const size_t smem2 = (size_t)g.max_off[0] * sizeof(float4) + (size_t)g.tf_n * sizeof(float);
+    e = cudaFuncSetAttribute(k_probe_transmittance, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
+    if (e != cudaSuccess) return e;
+    k_probe_transmittance<<<148 * 8, kThreadsP, smem2, st>>>(g, quads, tab, tf, L.nprobe, L.cap, rec, count);
+  }
+  const int n = L.nprobe > L.ntiles ? L.nprobe : L.ntiles;
+  k_probe_compare<<<grid_for(n, 128, 148 * 8), 128, 0, st>>>(g, pg, L.cap, rec, count, img, tol, flags, flist, fcount,
+                                                             probe_err, cnt);
+  return cudaGetLastError();
+}
+
+}  // namespace beams

@@ -33,53 +33,36 @@ __device__ __forceinline__ unsigned hash32(unsigned x) {
   return x;
 }
 __device__ __forceinline__ float uniform01(unsigned seed, unsigned i, unsigned k) {
-  return (float)(hash32(seed ^ hash32(i * 3u + k + 0x9e3779b9u)) >> 8) * (1.f / 16777216.f);
+  return (float)(hash32(seed ^ hash32(hash32(i) + k * 0x9e3779b9u)) >> 8) * (1.f / 16777216.f);
 }
 
 // ---- data: exact transmittance at random points ---------------------------------
-// Light march from L to P over the quad field and shared-memory cell tables,
-// the same sample sequence as k_light_march (exact form).
-__device__ float exact_opacity_to(const ExactGeo& g, const float4* __restrict__ quads, const float4* T0,
-                                  const float4* T1, const float4* T2, const float* s_a, const float L[3],
-                                  const float P[3]) {
-  const float v[3] = {P[0] - L[0], P[1] - L[1], P[2] - L[2]};
-  const float rs = 1.f / sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-  const float dir[3] = {v[0] * rs, v[1] * rs, v[2] * rs};
-  float tmin, tmax;
-  segment_aabb(g, L, P, tmin, tmax);
-  const float st[3] = {L[0] + tmin * dir[0], L[1] + tmin * dir[1], L[2] + tmin * dir[2]};
-  float s[3] = {st[0], st[1], st[2]};
-  const float len2 = (tmax - tmin) * (tmax - tmin);
-  const int n1 = g.tf_n - 1;
+// Normalised colour-map alpha of the field at P (one light-march sample).
+__device__ float alpha_at(const ExactGeo& g, const float4* __restrict__ quads, const float4* T0, const float4* T1,
+                          const float4* T2, const float* s_a, const float P[3]) {
   const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
-  float o = 0.f;
-  for (int b = g.light_budget; b > 0; --b) {
-    const float q0 = s[0] - st[0], q1 = s[1] - st[1], q2 = s[2] - st[2];
-    if (!(q0 * q0 + q1 * q1 + q2 * q2 <= len2)) break;
-    s[0] = s[0] + g.step * dir[0];
-    s[1] = s[1] + g.step * dir[1];
-    s[2] = s[2] + g.step * dir[2];
-    if (!inside_vol(g, s)) break;
-    float4 e0, e1, e2;
-    const int c0 = find_cell_bsearch_t(T0, g.n[0] - 2, g.org[0], g.invh[0], s[0], e0);
-    const int c1 = find_cell_bsearch_t(T1, g.n[1] - 2, g.org[1], g.invh[1], s[1], e1);
-    const int c2 = find_cell_bsearch_t(T2, g.n[2] - 2, g.org[2], g.invh[2], s[2], e2);
-    float vals[8];
-    QuadLoad<float4>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qz, vals);
-    float scalar = hex_interp(vals, div_rn_markstein(s[0] - e0.x, e0.z, e0.w), div_rn_markstein(s[1] - e1.x, e1.z, e1.w),
-                              div_rn_markstein(s[2] - e2.x, e2.z, e2.w));
-    scalar = (scalar - g.min_scalar) * g.inv_delta;
-    o = o + (1.f - o) * s_a[tf_index_clamped(scalar * (float)n1, n1)];
-    if (o == 1.f) break;
-  }
-  return o;
+  float4 e0, e1, e2;
+  const int c0 = find_cell_bsearch_t(T0, g.n[0] - 2, g.org[0], g.invh[0], P[0], e0);
+  const int c1 = find_cell_bsearch_t(T1, g.n[1] - 2, g.org[1], g.invh[1], P[1], e1);
+  const int c2 = find_cell_bsearch_t(T2, g.n[2] - 2, g.org[2], g.invh[2], P[2], e2);
+  float vals[8];
+  QuadLoad<float4>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qz, vals);
+  float scalar = hex_interp(vals, div_rn_markstein(P[0] - e0.x, e0.z, e0.w), div_rn_markstein(P[1] - e1.x, e1.z, e1.w),
+                            div_rn_markstein(P[2] - e2.x, e2.z, e2.w));
+  scalar = (scalar - g.min_scalar) * g.inv_delta;
+  const int n1 = g.tf_n - 1;
+  return s_a[tf_index_clamped(scalar * (float)n1, n1)];
 }
 
-// sample i: position (world) in xyz, light index in w; target transmittance
+// sample i: position (world) in xyz, light index in w; target transmittance.
+// A fraction `focus` of the positions is rejection-sampled (16 tries) where the
+// colour map's alpha is non-zero: the shading only reads T where samples
+// composite, so the network's capacity goes there.
 __global__ void __launch_bounds__(256) k_gen_data(const ExactGeo g, const float4* __restrict__ quads,
                                                   const float4* __restrict__ tab, const float4* __restrict__ tf,
                                                   const float4* __restrict__ lights, int nlights, unsigned seed,
-                                                  float4* __restrict__ samples, float* __restrict__ target, int n) {
+                                                  float focus, float4* __restrict__ samples,
+                                                  float* __restrict__ target, int n) {
   extern __shared__ float4 s_dyn[];
   float4* s_tab = s_dyn;
   float* s_a = (float*)(s_dyn + g.max_off[0]);
@@ -89,12 +72,19 @@ __global__ void __launch_bounds__(256) k_gen_data(const ExactGeo g, const float4
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int li = (int)(hash32(seed + 7919u * (unsigned)i) % (unsigned)nlights);
     float P[3];
+    const int tries = (uniform01(seed, (unsigned)i, 3u) < focus) ? 16 : 1;
+    for (int t = 0; t < tries; ++t) {
+      const unsigned k = 4u + 3u * (unsigned)t;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) P[a] = g.minp[a] + uniform01(seed, (unsigned)i, (unsigned)a) * (g.maxp[a] - g.minp[a]);
+      for (int a = 0; a < 3; ++a)
+        P[a] = g.minp[a] + uniform01(seed, (unsigned)i, k + (unsigned)a) * (g.maxp[a] - g.minp[a]);
+      if (tries == 1 || alpha_at(g, quads, s_tab + g.ax_off[0], s_tab + g.ax_off[1], s_tab + g.ax_off[2], s_a, P) > 0.f)
+        break;
+    }
     const float4 Lw = lights[li];
     const float L[3] = {Lw.x, Lw.y, Lw.z};
-    const float o = exact_opacity_to(g, quads, s_tab + g.ax_off[0], s_tab + g.ax_off[1], s_tab + g.ax_off[2], s_a,
-                                     L, P);
+    const float o = point_opacity(g, quads, s_tab + g.ax_off[0], s_tab + g.ax_off[1], s_tab + g.ax_off[2], s_a,
+                                  L, P);
     samples[i] = make_float4(P[0], P[1], P[2], (float)li);
     target[i] = 1.f - o;
   }
@@ -297,12 +287,12 @@ static unsigned grid_cap(size_t n, int per) {
 }
 
 cudaError_t mlp_gen_data(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
-                         const float4* lights, int nlights, unsigned seed, float4* samples, float* target, int n,
-                         cudaStream_t st) {
+                         const float4* lights, int nlights, unsigned seed, float focus, float4* samples,
+                         float* target, int n, cudaStream_t st) {
   const size_t smem = (size_t)g.max_off[0] * sizeof(float4) + (size_t)g.tf_n * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(k_gen_data, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  k_gen_data<<<148 * 8, 256, smem, st>>>(g, quads, tab, tf, lights, nlights, seed, samples, target, n);
+  k_gen_data<<<148 * 8, 256, smem, st>>>(g, quads, tab, tf, lights, nlights, seed, focus, samples, target, n);
   return cudaGetLastError();
 }
 

@@ -17,8 +17,21 @@ cudaError_t launch_view_march_prec(const ExactGeo& g, int quad_dtype, const void
                                    const float4* tf, const __half* map, float4* out, Counters* cnt, cudaStream_t st);
 cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    float* map, Counters* cnt, cudaStream_t st, const BrickRef* refs = nullptr,
-                                   int nrefs = 0, int self = -1);
+                                   int nrefs = 0, int self = -1, const unsigned* gate = nullptr);
+// K2 over a device list of kFallbackTile^2 pixel tiles (count in *fcount), with the map.
+cudaError_t launch_view_march_tiles(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
+                                    const float* map, float4* out, Counters* cnt, const unsigned* flist,
+                                    const unsigned* fcount, cudaStream_t st);
 size_t mlp_packed_bytes();
+// Learned form probe (k_mlp_probe.cu): probe grid and fallback tiles of one frame.
+constexpr int kProbeCap = 512;  // compositing samples recorded per probe pixel
+struct ProbeLayout {
+  int stride, offset, nqx, nqy, nprobe, ntiles, cap;
+};
+ProbeLayout probe_layout(int width, int height, float fraction);
+cudaError_t launch_mlp_probe(const ExactGeo& g, const ProbeLayout& L, const float4* quads, const float4* tab,
+                             const float4* tf, const float4* img, float tol, float4* rec, int* count, unsigned* flags,
+                             unsigned* flist, unsigned* fcount, float* probe_err, Counters* cnt, cudaStream_t st);
 cudaError_t launch_pack_weights(const float* P, uint2* W, float* aux, cudaStream_t st);
 cudaError_t launch_composite(const float4* imgs, int nb, size_t npix, const int* order, float4* out,
                              cudaStream_t st);

@@ -19,6 +19,7 @@ namespace beams {
 using namespace mlp;
 
 beams_status make_geo(beams_renderer* r, const beams_camera* cam, ExactGeo& g);
+beams_status ensure_buffer(beams_renderer* r, void** buf, size_t* cap, size_t bytes, const char* what);
 beams_status prepare_layouts(beams_renderer* r, const ExactGeo& g, int& launches);
 beams_status check_ready(beams_renderer* r);
 
@@ -37,9 +38,14 @@ struct MlpState {
   float4* lfeat = nullptr;   // their direction features
   int nlights = 0;
   void* packed = nullptr;    // inference weights: B fragments + biases
+  void* probe_mem = nullptr; // probe records, counts, tile flags, fallback list
+  size_t probe_bytes = 0;
+  float* probe_err = nullptr;  // per-probe max |dRGBA| of the last frame (tests)
+  int probe_err_n = 0;
   beams_mlp_options render_opts{};
   ~MlpState() {
-    for (void* p : {(void*)P, (void*)G, (void*)m, (void*)v, ws_mem, (void*)lights, (void*)lfeat, packed})
+    for (void* p : {(void*)P, (void*)G, (void*)m, (void*)v, ws_mem, (void*)lights, (void*)lfeat, packed, probe_mem,
+                    (void*)probe_err})
       if (p) cudaFree(p);
   }
 };
@@ -154,6 +160,57 @@ beams_status mlp_set_render_options(beams_renderer* r, const beams_mlp_options* 
   return BEAMS_OK;
 }
 
+// Probe pixels against the exact light march, then the exact map path over the
+// tiles that failed: K1 gated on a non-empty list, K2 over the listed tiles.
+// Nothing here waits on the host.
+static beams_status mlp_probe_and_fallback(beams_renderer* r, const ExactGeo& g, float4* out, int& launches) {
+  MlpState* st = r->mlp;
+  const beams_mlp_options& o = st->render_opts;
+  const ProbeLayout L = probe_layout(g.width, g.height, o.probe_fraction);
+  if (L.stride == 0) return BEAMS_OK;  // probe fraction 0: the network's image stands
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t b_rec = al((size_t)L.nprobe * L.cap * 2 * sizeof(float4));
+  const size_t b_cnt = al((size_t)L.nprobe * sizeof(int) + 4);
+  const size_t b_flags = al(((size_t)L.ntiles + 1) * sizeof(unsigned));
+  const size_t b_list = al((size_t)L.ntiles * sizeof(unsigned) + 4);
+  beams_status s = ensure_buffer(r, &st->probe_mem, &st->probe_bytes, b_rec + b_cnt + b_flags + b_list,
+                                 "allocating the probe buffers");
+  if (s != BEAMS_OK) return s;
+  char* base = (char*)st->probe_mem;
+  float4* rec = (float4*)base;
+  int* count = (int*)(base + b_rec);
+  unsigned* flags = (unsigned*)(base + b_rec + b_cnt);
+  unsigned* fcount = flags + L.ntiles;
+  unsigned* flist = (unsigned*)(base + b_rec + b_cnt + b_flags);
+  if (st->probe_err_n < L.nprobe) {
+    if (st->probe_err) cudaFree(st->probe_err);
+    st->probe_err = nullptr;
+    st->probe_err_n = 0;
+    cudaError_t e = cudaMalloc((void**)&st->probe_err, (size_t)std::max(L.nprobe, 1) * sizeof(float));
+    if (e != cudaSuccess) return cuda_fail(r, e, "allocating probe errors");
+    st->probe_err_n = std::max(L.nprobe, 1);
+  }
+  cudaError_t e = cudaMemsetAsync(flags, 0, ((size_t)L.ntiles + 1) * sizeof(unsigned), r->stream);
+  if (e == cudaSuccess)
+    e = launch_mlp_probe(g, L, (const float4*)r->d_quads, r->d_tab, r->d_tf, out, o.fallback_tol, rec, count, flags,
+                         flist, fcount, st->probe_err, r->d_cnt, r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "mlp probe launch");
+  launches += L.nprobe > 0 ? 3 : 1;
+  const size_t nvert = (size_t)g.pd[0] * g.pd[1] * g.pd[2];
+  s = ensure_buffer(r, (void**)&r->d_map, &r->map_cap, nvert * sizeof(float), "allocating map");
+  if (s != BEAMS_OK) return s;
+  r->map_valid = false;  // whether the gated build ran is known on the device only
+  r->map_is_half = false;
+  e = launch_light_march_f32(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map, r->d_cnt, r->stream, nullptr,
+                             0, -1, fcount);
+  if (e == cudaSuccess)
+    e = launch_view_march_tiles(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map, out, r->d_cnt + 1, flist,
+                                fcount, r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "mlp fallback launch");
+  launches += 2;
+  return BEAMS_OK;
+}
+
 // The view march shaded by the network (no map is built).
 beams_status mlp_render_view(beams_renderer* r, const ExactGeo& g, float4* out, int& launches) {
   MlpState* st = r->mlp;
@@ -173,7 +230,7 @@ beams_status mlp_render_view(beams_renderer* r, const ExactGeo& g, float4* out, 
                             st->render_opts.knot, out, r->d_cnt, r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "mlp view march launch");
   ++launches;
-  return BEAMS_OK;
+  return mlp_probe_and_fallback(r, g, out, launches);
 }
 
 }  // namespace beams
@@ -181,6 +238,18 @@ beams_status mlp_render_view(beams_renderer* r, const ExactGeo& g, float4* out, 
 using namespace beams;
 
 extern "C" {
+
+beams_status beams_mlp_probe_errors(beams_renderer* r, float* dst, int n) {
+  if (!r || !dst) return fail(r, BEAMS_ERR_INVALID_ARG, "mlp_probe_errors: NULL argument");
+  MlpState* st = r->mlp;
+  if (!st || !st->probe_err || n < 1 || n > st->probe_err_n)
+    return fail(r, BEAMS_ERR_STATE, "mlp_probe_errors: no probed frame of that size");
+  cudaSetDevice(r->device);
+  cudaError_t e = cudaStreamSynchronize(r->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(dst, st->probe_err, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(r, e, "mlp_probe_errors");
+  return BEAMS_OK;
+}
 
 beams_status beams_mlp_train(beams_renderer* r, const beams_mlp_options* opt, beams_mlp_report* rep) {
   if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
@@ -192,9 +261,10 @@ beams_status beams_mlp_train(beams_renderer* r, const beams_mlp_options* opt, be
   o.batch = 16384;
   o.lr = 2e-3f;
   o.seed = 1;
+  o.focus = 0.875f;
   if (opt) o = *opt;
   if (o.samples_log2 < 10 || o.samples_log2 > 26 || o.n_lights < 1 || o.n_lights > kMaxLights || o.epochs < 1 ||
-      o.batch < 256 || o.batch > (1 << 20) || !(o.lr > 0.f))
+      o.batch < 256 || o.batch > (1 << 20) || !(o.lr > 0.f) || !(o.focus >= 0.f && o.focus <= 1.f))
     return fail(r, BEAMS_ERR_INVALID_ARG, "mlp_train: options out of range");
   const int saved_form = r->form;
   r->form = BEAMS_FORM_EXACT;  // data come from the exact light march
@@ -224,12 +294,27 @@ beams_status beams_mlp_train(beams_renderer* r, const beams_mlp_options* opt, be
                        0.5 * ((double)g.minp[2] + g.maxp[2])};
   const double R = 2.0 * (double)g.extent_mag;
   const double ga = M_PI * (3.0 - std::sqrt(5.0));
-  for (int j = 0; j < o.n_lights; ++j) {
-    const double z = 1.0 - (2.0 * j + 1.0) / o.n_lights;
+  const int j0 = (o.scene_light && !r->lights.empty()) ? 1 : 0;
+  const int nfib = o.n_lights - j0;
+  for (int j = 0; j < nfib; ++j) {
+    const double z = nfib > 0 ? 1.0 - (2.0 * j + 1.0) / nfib : 0.0;
     const double rr = std::sqrt(std::max(0.0, 1.0 - z * z));
     const double d[3] = {rr * std::cos(ga * j), rr * std::sin(ga * j), z};
-    lp[j] = make_float4((float)(c[0] + R * d[0]), (float)(c[1] + R * d[1]), (float)(c[2] + R * d[2]), 0.f);
-    lf[j] = make_float4((float)d[0], (float)d[1], (float)d[2], 0.f);
+    lp[j0 + j] = make_float4((float)(c[0] + R * d[0]), (float)(c[1] + R * d[1]), (float)(c[2] + R * d[2]), 0.f);
+    lf[j0 + j] = make_float4((float)d[0], (float)d[1], (float)d[2], 0.f);
+  }
+  if (j0) {
+    // the renderer's light: its own position (a directional light as a far point)
+    const Light& L = r->lights[0];
+    float f[3];
+    mlp_light_feature(r, g, f);
+    const double far = 1e4 * (double)g.extent_mag;
+    for (int d = 0; d < 3; ++d) {
+      const double p = (L.kind == 0) ? L.v[d] : c[d] + far * (double)f[d];
+      (&lp[0].x)[d] = (float)p;
+      (&lf[0].x)[d] = f[d];
+    }
+    lp[0].w = lf[0].w = 0.f;
   }
   cudaError_t e = cudaSuccess;
   if (!st->lights) e = cudaMalloc((void**)&st->lights, kMaxLights * sizeof(float4));
@@ -257,7 +342,7 @@ beams_status beams_mlp_train(beams_renderer* r, const beams_mlp_options* opt, be
     return cuda_fail(r, e, "mlp_train: allocating the training set");
   }
   cudaEventRecord(t0, r->stream);
-  e = mlp_gen_data(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, st->lights, o.n_lights, o.seed, d_samples,
+  e = mlp_gen_data(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, st->lights, o.n_lights, o.seed, o.focus, d_samples,
                    d_target, n, r->stream);
   const Encoding enc = mlp_encoding(g);
   if (e == cudaSuccess) e = mlp_features(d_samples, st->lfeat, enc, d_X, n, r->stream);

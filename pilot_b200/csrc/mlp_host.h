@@ -19,8 +19,8 @@ struct TrainWS {
 };
 
 cudaError_t mlp_gen_data(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
-                         const float4* lights, int nlights, unsigned seed, float4* samples, float* target, int n,
-                         cudaStream_t st);
+                         const float4* lights, int nlights, unsigned seed, float focus, float4* samples,
+                         float* target, int n, cudaStream_t st);
 cudaError_t mlp_features(const float4* samples, const float4* lfeat, const mlp::Encoding& enc, __nv_bfloat16* X,
                          int n, cudaStream_t st);
 cudaError_t mlp_fwd_bwd(const float* P, float* G, const __nv_bfloat16* X, const float* target, int n,

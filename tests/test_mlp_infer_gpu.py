@@ -42,14 +42,14 @@ def oracle_mlp_image(s, P):
     return img
 
 
-def mlp_render(s, P=None, knot=1, r=None):
+def mlp_render(s, P=None, knot=1, r=None, probe_fraction=0.0):
     if r is None:
         r = B.Renderer(0)
         r.set_volume(s.field_numpy(), origin=s.origin, spacing=s.spacing, value_range=s.value_range)
         s.configure(r)
     if P is not None:
         r.mlp_set_params(P)
-    r.set_form(B.FORM_MLP, B.mlp_options(knot=knot))
+    r.set_form(B.FORM_MLP, B.mlp_options(knot=knot, probe_fraction=probe_fraction))
     img, t = r.render(s.camera())
     return img, t, r
 
@@ -104,3 +104,117 @@ def test_trained_mlp_render_beats_no_shadow_model(cuda_device):
     p_mlp, p_unlit = psnr(img, ref64), psnr(unlit, ref64)
     print(f"trained MLP (holdout rmse {rep['holdout_rmse']:.3f}): PSNR {p_mlp:.1f} dB vs unshadowed {p_unlit:.1f} dB")
     assert p_mlp > p_unlit + 3
+
+
+# ---- per-tile fallback to the exact map -------------------------------------------
+TILE = 32
+
+
+def _renderer(s):
+    r = B.Renderer(0)
+    r.set_volume(s.field_numpy(), origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+    s.configure(r)
+    return r
+
+
+def _tile_max(err, h, w):
+    ty, tx = -(-h // TILE), -(-w // TILE)
+    out = np.full((ty, tx), -np.inf)
+    for y in range(h):
+        for x in range(w):
+            out[y // TILE, x // TILE] = max(out[y // TILE, x // TILE], err[y, x])
+    return out
+
+
+def _probe_errors_cpu(s, mlp_img):
+    """Every pixel composited with the exact light march's transmittance (float32
+    oracle), against the network's image: max |dRGBA| per pixel."""
+    o = Oracle(s)
+    rec, cnt = o.record_samples()
+    T = (np.float32(1) - o.point_opacity(rec[:, :3], fp64=False)).astype(np.float32)
+    lc = np.float32(s.light_intensity) * np.array(s.light_color, np.float32)
+    err = np.zeros((s.height, s.width), np.float32)
+    k = 0
+    for y in range(s.height):
+        for x in range(s.width):
+            c = np.zeros(4, np.float32)
+            for _ in range(cnt[y, x]):
+                r = rec[k]
+                for ch in range(3):
+                    c[ch] = c[ch] + np.float32(min(max(r[3 + ch] * (T[k] * lc[ch]), 0.0), 1.0)) * r[6]
+                c[3] = r[6] + c[3]
+                k += 1
+            err[y, x] = np.abs(mlp_img[y, x] - c).max()
+    return err
+
+
+def _check_tiles(img, mlp_img, exact_img, flagged):
+    h, w = img.shape[:2]
+    for ty in range(flagged.shape[0]):
+        for tx in range(flagged.shape[1]):
+            sl = (slice(ty * TILE, min(h, (ty + 1) * TILE)), slice(tx * TILE, min(w, (tx + 1) * TILE)))
+            want = exact_img if flagged[ty, tx] else mlp_img
+            assert np.array_equal(img[sl], want[sl]), (ty, tx, bool(flagged[ty, tx]))
+
+
+def test_mlp_fallback_every_pixel_probed(cuda_device):
+    """probe_fraction 1: the device's probe errors equal the oracle's exact
+    transmittance composite, and exactly the tiles above the tolerance carry
+    the exact form's pixels."""
+    s = scenes.small(64, n=32, image=72, m=8, kind="blobs")
+    r = _renderer(s)
+    exact_img, _ = r.render(s.camera())
+    r.mlp_set_params(smooth_params(9))
+    r.set_form(B.FORM_MLP, B.mlp_options(knot=2, probe_fraction=0.0))
+    mlp_img, _ = r.render(s.camera())
+    cpu_err = _probe_errors_cpu(s, mlp_img)
+    tiles = _tile_max(cpu_err, s.height, s.width)
+    tol = float(np.median(tiles))
+    r.set_form(B.FORM_MLP, B.mlp_options(knot=2, probe_fraction=1.0, fallback_tol=tol))
+    img, t = r.render(s.camera())
+    gpu_err = r.mlp_probe_errors(s.width * s.height).reshape(s.height, s.width)
+    assert np.array_equal(gpu_err, cpu_err), np.abs(gpu_err - cpu_err).max()
+    flagged = tiles > tol
+    print(f"tol {tol:.4f}: {flagged.sum()} of {flagged.size} tiles fall back")
+    assert 0 < flagged.sum() < flagged.size and t["fallback_tiles"] == flagged.sum()
+    assert t["map_vertices"] == (s.map_m + 1) ** 3
+    _check_tiles(img, mlp_img, exact_img, flagged)
+    # a tolerance above every error keeps the network's image and builds no map
+    r.set_form(B.FORM_MLP, B.mlp_options(knot=2, probe_fraction=1.0, fallback_tol=1e30))
+    img2, t2 = r.render(s.camera())
+    assert t2["fallback_tiles"] == 0 and t2["map_vertices"] == 0 and t2["light_samples"] == 0
+    assert np.array_equal(img2, mlp_img)
+    # tolerance 0 with a network far from the map: every tile with a visible probe falls back
+    r.set_form(B.FORM_MLP, B.mlp_options(knot=2, probe_fraction=1.0, fallback_tol=0.0))
+    img3, t3 = r.render(s.camera())
+    _check_tiles(img3, mlp_img, exact_img, tiles > 0)
+
+
+def test_mlp_fallback_one_percent_probes(cuda_device):
+    s = scenes.small(65, n=40, image=96, m=10, kind="noise")
+    r = _renderer(s)
+    exact_img, _ = r.render(s.camera())
+    r.mlp_set_params(smooth_params(10))
+    r.set_form(B.FORM_MLP, B.mlp_options(knot=4, probe_fraction=0.0))
+    mlp_img, _ = r.render(s.camera())
+    r.set_form(B.FORM_MLP, B.mlp_options(knot=4, probe_fraction=0.01, fallback_tol=0.05))
+    img, t = r.render(s.camera())
+    P = 10
+    n = len(range(P // 2, s.width, P))
+    err = r.mlp_probe_errors(n * n).reshape(n, n)
+    cpu = _probe_errors_cpu(s, mlp_img)[P // 2::P, P // 2::P]
+    assert np.array_equal(err, cpu)
+    tiles = np.full((3, 3), -np.inf)
+    for j in range(n):
+        for i in range(n):
+            y, x = j * P + P // 2, i * P + P // 2
+            tiles[y // TILE, x // TILE] = max(tiles[y // TILE, x // TILE], err[j, i])
+    assert t["fallback_tiles"] == (tiles > 0.05).sum()
+    _check_tiles(img, mlp_img, exact_img, tiles > 0.05)
+    tol = float(np.median(tiles))
+    r.set_form(B.FORM_MLP, B.mlp_options(knot=4, probe_fraction=0.01, fallback_tol=tol))
+    img, t = r.render(s.camera())
+    flagged = tiles > tol
+    print(f"1% probes, tol {tol:.3f}: {flagged.sum()} of 9 tiles fall back; probe errors max {err.max():.3f}")
+    assert 0 < flagged.sum() < 9 and t["fallback_tiles"] == flagged.sum()
+    _check_tiles(img, mlp_img, exact_img, flagged)

@@ -8,6 +8,8 @@ field already resident in HBM. Synthetic seeded input; the 512 MiB field is
 larger than L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --form precision [--field-dtype bf16|f16]   # config 2, 1024^3, 2048^2, M = 512
+  python bench.py --form mlp [--knot 4] [--mlp-scene-light]    # learned form on the config 1 field
 
 N > 1 runs N independent replicas (the path does not shard across GPUs: there
 is no exchange step), launched by torch.distributed.run; value is the total over
@@ -143,7 +145,7 @@ def dist_setup():
 
 def build_scene(config: int):
     from pilot_b200 import scenes
-    return scenes.config1() if config == 1 else scenes.config0()
+    return {0: scenes.config0, 1: scenes.config1, 2: scenes.config2}[config]()
 
 
 def workload_desc(s, config: int):
@@ -260,6 +262,7 @@ def run_ours(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda") if args.config != 1 else None
 
     r.render(cam, out=out, timings=True)                  # builds the cell tables and quad field
+    tuning = r.autotune(cam)                              # launch choices only; results are identical
     _, t0 = r.render(cam, out=out, timings=True)          # counts for one frame (deterministic)
     lit_frame, light_frame = t0["lit_samples"], t0["light_samples"]
     launches_per_frame = t0["kernel_launches"]
@@ -368,11 +371,197 @@ def run_ours(args):
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded 4-octave gradient noise, generated on the device)",
-                "config": dict(workload_desc(s, args.config), parallelism=f"replicas x{world}"),
+                "config": dict(workload_desc(s, args.config), parallelism=f"replicas x{world}", tuning=tuning),
                 "ms_per_frame": max_ms / args.steps, "map_build_ms": k1_ms, "view_march_ms": k2_ms,
                 "lit_samples_per_frame": lit_frame, "light_samples_per_frame": light_frame,
                 "gpu_launches": launches_per_frame * args.steps,
                 "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": sampler.summary()}
+        print(json.dumps(line), flush=True)
+    r.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# the other forms: --form precision (config 2) and --form mlp (config 1 field)
+# ---------------------------------------------------------------------------
+MLP_FLOP_PER_EVAL = 2 * (112 * 64 + 3 * 64 * 64 + 64)  # 39,040 FLOP per network evaluation
+
+
+def measured_tensor_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("bf16_tflops", 1590.0)), "measured (burst)"
+    return 1590.0, "fallback"
+
+
+def time_frames(frame, steps, warmup, stream, world, local):
+    """W untimed frames, then K frames between device events; max over ranks."""
+    import torch
+    import torch.distributed as dist
+    for _ in range(warmup):
+        frame()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    with sampler:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            frame()
+        b.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t = torch.tensor([a.elapsed_time(b)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item()), sampler.summary()
+
+
+def fp64_crops(s, field, images, crop, stride, ncrops, threads):
+    """PSNR / max |d| of each image against the FP64 oracle (lazy map) on ncrops
+    crop x crop windows, every stride-th pixel."""
+    from oracle.oracle import Oracle, psnr
+    o = Oracle(s, field=field, threads=threads)
+    rng = np.random.default_rng(7)
+    res = {k: [] for k in images}
+    t0 = time.perf_counter()
+    for c in range(ncrops):
+        x0 = int(rng.integers(0, s.width - crop + 1)) if c else (s.width - crop) // 2
+        y0 = int(rng.integers(0, s.height - crop + 1)) if c else (s.height - crop) // 2
+        ref, _ = o.view_march_lazy_f64((x0, y0, crop, crop), stride=stride)
+        for k, img in images.items():
+            sub = img[y0:y0 + crop:stride, x0:x0 + crop:stride]
+            res[k].append((psnr(sub, ref), float(np.abs(sub - ref).max()), float(np.abs(sub - ref).mean())))
+    out = {k: {"psnr_db": float(np.mean([v[0] for v in r])), "max_abs": max(v[1] for v in r),
+               "mean_abs": float(np.mean([v[2] for v in r]))} for k, r in res.items()}
+    out["crops"] = f"{ncrops} crops of {crop}x{crop}, every {stride}th pixel, FP64 oracle with lazy map"
+    out["oracle_s"] = time.perf_counter() - t0
+    return out
+
+
+def run_form(args):
+    import torch
+    import torch.distributed as dist
+
+    from oracle.oracle import psnr
+    from pilot_b200 import beams as B
+    from pilot_b200 import scenes
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    stream = torch.cuda.current_stream()
+    cfg = args.config
+    s = scenes.config2() if cfg == 2 else build_scene(cfg)
+    fd = s.field_device()
+    r = B.Renderer(local, stream=stream.cuda_stream)
+    r.set_volume(fd, origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+    s.configure(r)
+    cam = s.camera()
+    out = torch.empty((s.height, s.width, 4), dtype=torch.float32, device="cuda")
+    threads = os.cpu_count() or 1
+
+    # the exact form in the same run: the speed and quality reference of the form
+    r.set_form(B.FORM_EXACT)
+    r.render(cam, out=out, timings=False)
+    exact_tuning = r.autotune(cam)
+    _, te = r.render(cam, out=out, timings=True)
+    exact_img = out.cpu().numpy()
+    lit_frame = te["lit_samples"]
+    exact_ms, _ = time_frames(lambda: r.render(cam, out=out, timings=False), max(3, args.steps // 4), 2, stream,
+                              world, local)
+    exact_ms /= max(3, args.steps // 4)
+    extra, roofline = {}, None
+    if args.form == "precision":
+        dt = B.F16 if args.field_dtype == "f16" else B.BF16
+        r.set_form(B.FORM_PRECISION, dt)
+        r.render(cam, out=out, timings=False)
+        extra["tuning"] = r.autotune(cam)
+        _, tp = r.render(cam, out=out, timings=True)
+        img = out.cpu().numpy()
+        launches = tp["kernel_launches"]
+        frame = lambda: r.render(cam, out=out, timings=False)  # noqa: E731  map build + view march
+        total_ms, clocks = time_frames(frame, args.steps, args.warmup, stream, world, local)
+        _, tk = r.render(cam, out=out, timings=True)
+        nvert = (s.map_m + 1) ** 3
+        kb = tk["light_samples"] * 16 + nvert * 2  # bf16/f16 quads: 8 corners x 2 B; binary16 map
+        roofline = {"bound": "hbm", "kernel": "k_light_march (precision)", "unit": "GB/s",
+                    "achieved": kb / (tk["map_build_ms"] / 1e3) / 1e9, "traffic": None,
+                    "bytes_model": "light sample 16 B (8 16-bit corners) + 2 B/vertex",
+                    "k_light_march_ms": tk["map_build_ms"], "k_view_march_ms": tk["view_march_ms"]}
+        dtype = args.field_dtype
+        extra["precision"] = {"field_dtype": dtype, "exact_f32_ms_per_frame": exact_ms, "exact_tuning": exact_tuning,
+                              "speedup_vs_exact_f32": exact_ms / (total_ms / args.steps),
+                              "psnr_vs_exact_f32_full_frame": psnr(img, exact_img)}
+        if not args.no_quality and rank == 0:
+            extra["precision"]["vs_fp64"] = fp64_crops(s, fd.cpu().numpy(), {"precision": img, "exact_f32": exact_img},
+                                                       args.crop, args.crop_stride, args.crops, threads)
+    else:  # mlp
+        rep = r.mlp_train(B.mlp_options(samples_log2=args.mlp_samples_log2, n_lights=args.mlp_lights,
+                                        epochs=args.mlp_epochs, scene_light=int(args.mlp_scene_light)))
+        opts = dict(knot=args.knot, probe_fraction=args.probe_fraction, fallback_tol=args.fallback_tol)
+        # the network alone (no probes): its kernel time for the tensor roofline and its image
+        r.set_form(B.FORM_MLP, B.mlp_options(**dict(opts, probe_fraction=0.0)))
+        r.render(cam, out=out, timings=True)
+        _, tn = r.render(cam, out=out, timings=True)
+        net_img = out.cpu().numpy()
+        r.set_form(B.FORM_MLP, B.mlp_options(**opts))
+        _, tm = r.render(cam, out=out, timings=True)
+        img = out.cpu().numpy()
+        launches = tm["kernel_launches"]
+        frame = lambda: r.render(cam, out=out, timings=False)  # noqa: E731  network + probes + fallback
+        total_ms, clocks = time_frames(frame, args.steps, args.warmup, stream, world, local)
+        tpeak, tsrc = measured_tensor_peak()
+        flops = tn["mlp_samples"] * MLP_FLOP_PER_EVAL
+        ach = flops / (tn["view_march_ms"] / 1e3) / 1e12
+        roofline = {"bound": "tensor", "kernel": "k_view_march_mlp", "achieved": ach, "peak": tpeak,
+                    "unit": "TFLOP/s", "frac": ach / tpeak, "peak_source": tsrc, "traffic": None,
+                    "flops_model": f"{MLP_FLOP_PER_EVAL} FLOP per network evaluation",
+                    "evaluations": tn["mlp_samples"], "kernel_ms": tn["view_march_ms"]}
+        dtype = "bf16"
+        ntiles = -(-s.width // 32) * -(-s.height // 32)
+        extra["learned"] = {"train": {k: rep[k] for k in ("datagen_ms", "train_ms", "holdout_rmse", "unlit_rmse",
+                                                           "mean_rmse", "steps", "samples")},
+                            "lights": args.mlp_lights, "scene_light": bool(args.mlp_scene_light),
+                            "knot": args.knot, "probe_fraction": args.probe_fraction,
+                            "fallback_tol": args.fallback_tol,
+                            "fallback_tiles": tm["fallback_tiles"], "tiles": ntiles,
+                            "network_evaluations": tm["mlp_samples"],
+                            "exact_ms_per_frame": exact_ms,
+                            "speedup_vs_exact": exact_ms / (total_ms / args.steps),
+                            "network_only_ms": tn["total_ms"],
+                            "psnr_vs_exact_map_full_frame": psnr(img, exact_img),
+                            "network_only_psnr_vs_exact_map": psnr(net_img, exact_img)}
+        if not args.no_quality and rank == 0:
+            extra["learned"]["vs_fp64"] = fp64_crops(s, fd.cpu().numpy(), {"learned_form": img, "network_only": net_img,
+                                                                            "exact": exact_img},
+                                                     args.crop, args.crop_stride, args.crops, threads)
+    if roofline.get("peak") is None:
+        peak, src = measured_peaks()
+        roofline.update(peak=peak, frac=roofline["achieved"] / peak, peak_source=src)
+    value = world * args.steps * lit_frame / (total_ms / 1e3)
+    if rank == 0:
+        wl = workload_desc(s, cfg) if cfg != 2 else {
+            "workload": f"config2: {s.dims[0]}^3 64 blobs + 10% noise, {s.width}x{s.height} image, M={s.map_m} "
+                        f"binary16 map, view step 0.25 voxel, alpha cut {s.cutoff}, point light",
+            "field": list(s.dims), "image": [s.width, s.height], "map_cells": s.map_m,
+            "l2": "inputs larger than L2 (2 GiB 16-bit field); no flush"}
+        wl = dict(wl, form=args.form, parallelism=f"replicas x{world}")
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+                "data": "synthetic (seeded fields generated on the device)", "config": wl,
+                "lit_samples_per_frame": lit_frame, "gpu_launches": launches * args.steps,
+                "roofline": roofline, "clocks": clocks, **extra}
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:
@@ -386,14 +575,31 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=1, choices=[0, 1])
+    ap.add_argument("--config", type=int, default=None, choices=[0, 1, 2])
+    ap.add_argument("--form", default="exact", choices=["exact", "precision", "mlp"])
+    ap.add_argument("--field-dtype", default="bf16", choices=["bf16", "f16"], help="precision form")
+    ap.add_argument("--knot", type=int, default=4, help="mlp form: network every knot lit samples")
+    ap.add_argument("--probe-fraction", type=float, default=0.01)
+    ap.add_argument("--fallback-tol", type=float, default=0.01)
+    ap.add_argument("--mlp-lights", type=int, default=32)
+    ap.add_argument("--mlp-scene-light", action="store_true")
+    ap.add_argument("--mlp-samples-log2", type=int, default=24)
+    ap.add_argument("--mlp-epochs", type=int, default=4)
+    ap.add_argument("--no-quality", action="store_true", help="skip the FP64 oracle crops")
+    ap.add_argument("--crops", type=int, default=3)
+    ap.add_argument("--crop", type=int, default=128)
+    ap.add_argument("--crop-stride", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work for cpu_baseline")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up frames
+    if args.config is None:
+        args.config = 2 if args.form == "precision" else 1
     if args.impl == "reference":
         return run_reference(args)
+    if args.form != "exact":
+        return run_form(args)
     return run_ours(args)
 
 

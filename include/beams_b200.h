@@ -150,6 +150,26 @@ beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable);
 /* Replaces MapperLightedVolume::SetCompositeBackground (MapperLightedVolume.cxx:321-324):
  * blend rgb over an opaque background colour after compositing. Off by default. */
 beams_status beams_set_background(beams_renderer* r, int enable, const float rgba[4]);
+/* Launch tuning (no reference counterpart; results do not depend on it).
+ * light_brick: the order in which the map build takes its vertices: 0 = rows
+ * (x fastest), or cubic bricks of 8 (default), 16, 32 or 64 vertices per edge.
+ * no_empty_skip: 1 turns off the map build's skipping of 8^3-cell macro-cells
+ * whose values all map to colour-map alpha 0 (such samples change nothing).
+ * no_view_skip: the same for the view march (skipped samples still count as lit). */
+typedef struct beams_tuning {
+  int light_brick;
+  int no_empty_skip;
+  int no_view_skip;
+  int reserved;
+} beams_tuning;
+beams_status beams_set_tuning(beams_renderer* r, const beams_tuning* t);
+beams_status beams_get_tuning(beams_renderer* r, beams_tuning* t);
+/* Times the map build under every vertex order x empty-skip choice on the
+ * current volume, colour map, light and form and, given a camera, the view
+ * march with and without its skip; keeps the fastest (results are identical
+ * under all of them) and reports it. Synchronises. */
+beams_status beams_autotune(beams_renderer* r, const beams_camera* cam, beams_tuning* best, float* best_map_ms,
+                            float* best_view_ms);
 /* Selects the render form (beams_form). opts: NULL, or for BEAMS_FORM_MLP a
  * const beams_mlp_options*. */
 beams_status beams_set_form(beams_renderer* r, int form, const void* opts);

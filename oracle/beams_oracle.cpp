@@ -281,8 +281,9 @@ T light_march_point(const Geo<T>& g, const T L[3], const T P[3], uint64_t& nsamp
 
 // Precision form of the light march: same samples as light_march_point, but
 // the opacity is accumulated as optical depth tau = sum -ln(1 - a_i) with Kahan
-// compensation, a_i = 1 cuts the ray (T = 0), and the result is the
-// transmittance exp(-tau) rounded to IEEE binary16 (returned as float).
+// compensation over the non-zero terms (a sample of alpha 0 adds nothing, not
+// even its compensation step), a_i = 1 cuts the ray (T = 0), and the result is
+// the transmittance exp(-tau) rounded to IEEE binary16 (returned as float).
 template <typename T>
 T light_march_point_tau(const Geo<T>& g, const T L[3], const T P[3], uint64_t& nsamples) {
   T v[3] = {P[0] - L[0], P[1] - L[1], P[2] - L[2]};
@@ -336,6 +337,7 @@ T light_march_point_tau(const Geo<T>& g, const T L[3], const T P[3], uint64_t& n
       cut = true;
       break;
     }
+    if (ti == 0.f) continue;
     const float y = ti - comp;
     const float t = sum + y;
     comp = (t - sum) - y;

@@ -48,6 +48,11 @@ def mlp_options(samples_log2=24, n_lights=32, epochs=4, batch=16384, lr=2e-3, se
                       scene_light, focus)
 
 
+class Tuning(C.Structure):
+    _fields_ = [("light_brick", C.c_int), ("no_empty_skip", C.c_int), ("no_view_skip", C.c_int),
+                ("reserved", C.c_int)]
+
+
 class BeamsError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
@@ -120,6 +125,10 @@ def lib():
         "beams_mlp_loss_grad": ([P, P, P, C.c_int, C.POINTER(C.c_float), P, P], C.c_int),
         "beams_mlp_encode": ([P, P, P, C.c_int, P], C.c_int),
         "beams_mlp_probe_errors": ([P, P, C.c_int], C.c_int),
+        "beams_set_tuning": ([P, C.POINTER(Tuning)], C.c_int),
+        "beams_get_tuning": ([P, C.POINTER(Tuning)], C.c_int),
+        "beams_autotune": ([P, C.POINTER(Camera), C.POINTER(Tuning), C.POINTER(C.c_float), C.POINTER(C.c_float)],
+                           C.c_int),
         "beams_mlp_save": ([P, C.c_char_p], C.c_int),
         "beams_mlp_load": ([P, C.c_char_p], C.c_int),
         "beams_get_brick_map": ([P, C.c_int, C.c_int, P, C.c_size_t, C.c_int], C.c_int),
@@ -329,6 +338,24 @@ class Renderer:
     def set_background(self, on: bool, rgba=(1, 1, 1, 1)):
         c = (C.c_float * 4)(*rgba)
         self._check(self._L.beams_set_background(self._h, int(bool(on)), c))
+
+    def set_tuning(self, light_brick: int = 8, empty_skip: bool = True, view_skip: bool = True):
+        t = Tuning(int(light_brick), 0 if empty_skip else 1, 0 if view_skip else 1)
+        self._check(self._L.beams_set_tuning(self._h, C.byref(t)))
+
+    def get_tuning(self):
+        t = Tuning()
+        self._check(self._L.beams_get_tuning(self._h, C.byref(t)))
+        return {"light_brick": t.light_brick, "empty_skip": not t.no_empty_skip, "view_skip": not t.no_view_skip}
+
+    def autotune(self, cam=None):
+        """Picks the fastest tuning for the current scene (the view march too when a
+        camera is given); returns it with the map-build and view-march times."""
+        t, ms, vms = Tuning(), C.c_float(), C.c_float()
+        self._check(self._L.beams_autotune(self._h, C.byref(cam) if cam is not None else None, C.byref(t),
+                                           C.byref(ms), C.byref(vms)))
+        return {"light_brick": t.light_brick, "empty_skip": not t.no_empty_skip, "view_skip": not t.no_view_skip,
+                "map_ms": ms.value, "view_ms": vms.value}
 
     def set_form(self, form: int, field_dtype=BF16):
         """FORM_EXACT; FORM_PRECISION with the 16-bit field dtype (BF16 or F16);

@@ -103,6 +103,8 @@ beams_status make_geo_vol(beams_renderer* r, const beams_volume& v, const beams_
   g.step = g.extent_mag / r->light_steps;
   g.cutoff = r->cutoff;
   g.light_budget = (int)(g.extent_mag / g.step) + 8;
+  g.light_brick_log2 = r->light_brick_log2;
+  occupancy_dims(g.n, g.occ_n);
   g.dir_dist = 2.f * g.extent_mag;
   if (!r->lights.empty()) {
     const Light& L = r->lights[0];
@@ -253,6 +255,22 @@ beams_status prepare_layouts(beams_renderer* r, const ExactGeo& g, int& launches
   return BEAMS_OK;
 }
 
+// Occupancy of the current quads under the current colour map (rebuilt when either changes).
+beams_status prepare_occupancy(beams_renderer* r, const ExactGeo& g, int& launches) {
+  const int qd = quad_dtype(r);
+  const unsigned long long key[2] = {r->volume_version * 4ull + (unsigned long long)qd, r->tf_version};
+  if (key[0] == r->occ_key[0] && key[1] == r->occ_key[1]) return BEAMS_OK;
+  const size_t nm = (size_t)g.occ_n[0] * g.occ_n[1] * g.occ_n[2];
+  beams_status s = ensure_buffer(r, (void**)&r->d_occ, &r->occ_cap, nm, "allocating occupancy grid");
+  if (s != BEAMS_OK) return s;
+  cudaError_t e = launch_build_occupancy(g, qd, r->d_quads, r->d_tf, r->d_occ, r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "occupancy build");
+  ++launches;
+  r->occ_key[0] = key[0];
+  r->occ_key[1] = key[1];
+  return BEAMS_OK;
+}
+
 beams_status build_map(beams_renderer* r, const ExactGeo& g, int& launches, bool& built) {
   built = false;
   MapKey key;
@@ -264,10 +282,16 @@ beams_status build_map(beams_renderer* r, const ExactGeo& g, int& launches, bool
                                  "allocating map");
   if (s != BEAMS_OK) return s;
   r->map_valid = false;
+  const unsigned char* occ = nullptr;
+  if (r->empty_skip) {
+    s = prepare_occupancy(r, g, launches);
+    if (s != BEAMS_OK) return s;
+    occ = r->d_occ;
+  }
   cudaError_t e = prec ? launch_light_march_prec(g, quad_dtype(r), r->d_quads, r->d_tab, r->d_tf, r->d_tau,
-                                                 (__half*)r->d_map, r->d_cnt, r->stream)
+                                                 (__half*)r->d_map, r->d_cnt, r->stream, occ)
                        : launch_light_march_f32(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map, r->d_cnt,
-                                                r->stream);
+                                                r->stream, nullptr, 0, -1, nullptr, occ);
   if (e != cudaSuccess) return cuda_fail(r, e, "light_march launch");
   ++launches;
   r->map_key = key;
@@ -658,6 +682,32 @@ beams_status beams_set_slab_fp64(beams_renderer* r, int enable) {
   return BEAMS_OK;
 }
 
+beams_status beams_set_tuning(beams_renderer* r, const beams_tuning* t) {
+  if (!r || !t) return fail(r, BEAMS_ERR_INVALID_ARG, "set_tuning: NULL argument");
+  int lb = 0;
+  switch (t->light_brick) {
+    case 0: lb = 0; break;
+    case 8: lb = 3; break;
+    case 16: lb = 4; break;
+    case 32: lb = 5; break;
+    case 64: lb = 6; break;
+    default: return fail(r, BEAMS_ERR_INVALID_ARG, "set_tuning: light_brick must be 0, 8, 16, 32 or 64");
+  }
+  r->light_brick_log2 = lb;
+  r->empty_skip = t->no_empty_skip ? 0 : 1;
+  r->view_skip = t->no_view_skip ? 0 : 1;
+  return BEAMS_OK;
+}
+
+beams_status beams_get_tuning(beams_renderer* r, beams_tuning* t) {
+  if (!r || !t) return fail(r, BEAMS_ERR_INVALID_ARG, "get_tuning: NULL argument");
+  std::memset(t, 0, sizeof(*t));
+  t->light_brick = r->light_brick_log2 ? 1 << r->light_brick_log2 : 0;
+  t->no_empty_skip = r->empty_skip ? 0 : 1;
+  t->no_view_skip = r->view_skip ? 0 : 1;
+  return BEAMS_OK;
+}
+
 beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable) {
   if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
   r->reuse_map = enable != 0;
@@ -734,6 +784,113 @@ beams_status beams_build_shadow_map(beams_renderer* r, beams_timings* t) {
   return BEAMS_OK;
 }
 
+beams_status beams_autotune(beams_renderer* r, const beams_camera* cam, beams_tuning* best, float* best_map_ms,
+                            float* best_view_ms) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  beams_status s = check_ready(r);
+  if (s != BEAMS_OK) return s;
+  if (r->lights.empty()) return fail(r, BEAMS_ERR_STATE, "no light added");
+  if (r->brick_mode || r->vol.assoc != BEAMS_ASSOC_POINTS || r->form == BEAMS_FORM_MLP)
+    return fail(r, BEAMS_ERR_UNSUPPORTED, "autotune: single point volume in the exact or precision form");
+  cudaSetDevice(r->device);
+  ExactGeo g;
+  s = make_geo(r, nullptr, g);
+  if (s != BEAMS_OK) return s;
+  int launches = 0;
+  s = prepare_layouts(r, g, launches);
+  if (s != BEAMS_OK) return s;
+  const int keep_lb = r->light_brick_log2, keep_skip = r->empty_skip;
+  const bool keep_reuse = r->reuse_map;
+  r->reuse_map = false;
+  int best_lb = keep_lb, best_skip = keep_skip;
+  float best_t = 3.4e38f;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  for (int lb : {0, 3, 4, 5, 6}) {
+    for (int skip : {0, 1}) {
+      r->light_brick_log2 = lb;
+      r->empty_skip = skip;
+      s = make_geo(r, nullptr, g);
+      bool built = false;
+      if (s == BEAMS_OK) s = build_map(r, g, launches, built);  // warm-up (and the occupancy grid)
+      float tmin = 3.4e38f;
+      for (int rep = 0; rep < 2 && s == BEAMS_OK; ++rep) {
+        cudaEventRecord(a, r->stream);
+        s = build_map(r, g, launches, built);
+        cudaEventRecord(b, r->stream);
+        cudaError_t e = cudaEventSynchronize(b);
+        if (e != cudaSuccess) s = cuda_fail(r, e, "autotune");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        tmin = std::min(tmin, ms);
+      }
+      if (s != BEAMS_OK) break;
+      if (tmin < best_t) {
+        best_t = tmin;
+        best_lb = lb;
+        best_skip = skip;
+      }
+    }
+    if (s != BEAMS_OK) break;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  r->reuse_map = keep_reuse;
+  r->map_valid = false;
+  if (s != BEAMS_OK) {
+    r->light_brick_log2 = keep_lb;
+    r->empty_skip = keep_skip;
+    return s;
+  }
+  r->light_brick_log2 = best_lb;
+  r->empty_skip = best_skip;
+  float best_v = 0.f;
+  if (cam) {
+    // the view march with and without its skip, on the map just chosen
+    const int keep_view = r->view_skip;
+    const bool keep_reuse2 = r->reuse_map;
+    r->reuse_map = true;  // the first render of each choice builds the map; the timed ones reuse it
+    float tv[2] = {3.4e38f, 3.4e38f};
+    float4* img = nullptr;
+    s = validate_camera(r, cam);
+    if (s == BEAMS_OK) {
+      const size_t npix = (size_t)cam->width * cam->height;
+      s = ensure_buffer(r, (void**)&r->d_rgba, &r->rgba_cap, npix * sizeof(float4), "allocating image");
+      img = r->d_rgba;
+    }
+    for (int vs = 0; vs < 2 && s == BEAMS_OK; ++vs) {
+      r->view_skip = vs;
+      for (int rep = 0; rep < 3 && s == BEAMS_OK; ++rep) {
+        cudaEvent_t a2, b2;
+        cudaEventCreate(&a2);
+        cudaEventCreate(&b2);
+        cudaEventRecord(a2, r->stream);
+        s = beams_render(r, cam, (float*)img, 1, nullptr);
+        cudaEventRecord(b2, r->stream);
+        cudaError_t e = cudaEventSynchronize(b2);
+        if (e != cudaSuccess && s == BEAMS_OK) s = cuda_fail(r, e, "autotune");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a2, b2);
+        cudaEventDestroy(a2);
+        cudaEventDestroy(b2);
+        if (rep > 0) tv[vs] = std::min(tv[vs], ms);
+      }
+    }
+    r->reuse_map = keep_reuse2;
+    if (s != BEAMS_OK) {
+      r->view_skip = keep_view;
+      return s;
+    }
+    r->view_skip = tv[1] < tv[0] ? 1 : 0;
+    best_v = std::min(tv[0], tv[1]);
+  }
+  if (best) beams_get_tuning(r, best);
+  if (best_map_ms) *best_map_ms = best_t;
+  if (best_view_ms) *best_view_ms = best_v;
+  return BEAMS_OK;
+}
+
 beams_status beams_get_shadow_map(beams_renderer* r, float* dst, size_t count, int dst_on_device) {
   if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
   if (!r->map_valid) return fail(r, BEAMS_ERR_STATE, "no map has been built");
@@ -796,12 +953,20 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
     if (s != BEAMS_OK) return s;
     --launches;  // counted below with the other view marches
     e = cudaSuccess;
-  } else if (r->form == BEAMS_FORM_PRECISION && r->vol.assoc == BEAMS_ASSOC_POINTS)
-    e = launch_view_march_prec(g, quad_dtype(r), r->d_quads, r->d_tab, r->d_tf,
-                               need_map ? (const __half*)r->d_map : nullptr, dst, r->d_cnt, r->stream);
-  else
-    e = launch_view_march_f32(g, (const float*)r->d_field, (const float4*)r->d_quads, r->d_tab, r->d_tf,
-                              need_map ? r->d_map : nullptr, dst, r->d_cnt, r->stream);
+  } else {
+    const unsigned char* occ = nullptr;
+    if (r->view_skip && r->vol.assoc == BEAMS_ASSOC_POINTS) {
+      s = prepare_occupancy(r, g, launches);
+      if (s != BEAMS_OK) return s;
+      occ = r->d_occ;
+    }
+    if (r->form == BEAMS_FORM_PRECISION && r->vol.assoc == BEAMS_ASSOC_POINTS)
+      e = launch_view_march_prec(g, quad_dtype(r), r->d_quads, r->d_tab, r->d_tf,
+                                 need_map ? (const __half*)r->d_map : nullptr, dst, r->d_cnt, r->stream, occ);
+    else
+      e = launch_view_march_f32(g, (const float*)r->d_field, (const float4*)r->d_quads, r->d_tab, r->d_tf,
+                                need_map ? r->d_map : nullptr, dst, r->d_cnt, r->stream, occ);
+  }
   if (e != cudaSuccess) return cuda_fail(r, e, "view_march launch");
   ++launches;
   cudaEventRecord(r->ev[2], r->stream);

@@ -43,7 +43,15 @@ struct ExactGeo {
   int ax_off[3];   // offset of field axis d in the table
   int max_off[3];  // offset of map axis d in the table
   int ntab;        // total table entries
+  // K1 vertex order: 0 = x-fastest rows of the vertex grid; b > 0 = cubic
+  // bricks of 2^b vertices per edge in brick order (rays in flight stay in a
+  // narrow cone towards the light, so the field they read stays in L2).
+  int light_brick_log2;
+  // Occupancy of 8^3-cell macro-cells (empty-space skipping): counts per axis.
+  int occ_n[3];
 };
+
+constexpr int kMacroLog2 = 3;  // macro-cell edge = 8 field cells
 
 // What the stitch kernel needs of every other brick (multi-block scenes): its
 // bounds (for SegmentAABB) and its Phase-1 map with that map's geometry.

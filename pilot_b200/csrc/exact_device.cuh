@@ -344,6 +344,19 @@ template <> struct QuadLoad<float4> {
   }
 };
 
+// Whether the macro-cell holding p may hold a non-zero TF alpha. The macro
+// index comes from the approximate cell (p - org) / h; the occupancy of macro
+// m covers cells [8m - 1, 8m + 8], so a cell search off by one stays covered.
+__device__ __forceinline__ bool occupied(const ExactGeo& g, const unsigned char* __restrict__ occ, const float p[3]) {
+  int m[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float f = fminf(fmaxf((p[d] - g.org[d]) * g.invh[d], 0.f), (float)(g.n[d] - 2));
+    m[d] = (int)f >> kMacroLog2;
+  }
+  return __ldg(occ + ((size_t)m[2] * g.occ_n[1] + m[1]) * g.occ_n[0] + m[0]) != 0;
+}
+
 // The light march of TransmittanceMap.h:279-332 from L to an arbitrary point P
 // (K1 runs it to map vertices): opacity accumulated over the same sample
 // sequence. T0..T2: field cell tables; s_a: TF alpha / max alpha.

@@ -19,6 +19,8 @@
 // Compiled with -fmad=false (see exact_device.cuh).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "exact_device.cuh"
 #include "kernels.h"
 #include "view_march.cuh"
@@ -39,8 +41,10 @@ __device__ __forceinline__ void load_tables(float4* s_tab, const float4* __restr
 // Opacity accumulation of one light ray.
 // Exact form: o <- o + (1 - o) a (TransmittanceMap.h:329-330); o == 1 is a fixed point.
 // Precision form: optical depth tau += -ln(1 - a) in float with Kahan
-// compensation (the per-entry -ln(1 - a) comes from a table), a = 1 cuts the
-// ray, and the map stores the transmittance exp(-tau) as binary16.
+// compensation over the non-zero terms (the per-entry -ln(1 - a) comes from a
+// table), a = 1 cuts the ray, and the map stores the transmittance exp(-tau) as
+// binary16. In both forms a sample of alpha 0 leaves the state unchanged, which
+// is what lets the march skip empty macro-cells.
 template <bool PREC> struct Accum;
 template <> struct Accum<false> {
   float o;
@@ -65,6 +69,7 @@ template <> struct Accum<true> {
       cut = true;
       return true;
     }
+    if (ti == 0.f) return false;  // alpha 0 adds nothing (no compensation step either)
     const float y = ti - comp;
     const float t = sum + y;
     comp = (t - sum) - y;
@@ -80,7 +85,7 @@ template <> struct Accum<true> {
 // STITCH: the multi-brick Phase 3 — the march starts from the cross-brick
 // prefix (stitch_prefix) instead of zero, as GenerateEstimator is re-run on
 // the prefix opacities (LightedVolumeRenderer.cxx:1241-1252).
-template <typename QuadT, bool STITCH, bool PREC>
+template <typename QuadT, bool STITCH, bool PREC, bool SKIP>
 __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, const QuadT* __restrict__ quads,
                                                           const float4* __restrict__ tab,
                                                           const float4* __restrict__ tf,
@@ -88,7 +93,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
                                                           void* __restrict__ map, int nvert,
                                                           Counters* __restrict__ cnt,
                                                           const BrickRef* __restrict__ refs, int nrefs,
-                                                          int self, const unsigned* __restrict__ gate) {
+                                                          int self, const unsigned* __restrict__ gate,
+                                                          const unsigned char* __restrict__ occ) {
   // gate: the learned form's fallback builds the map only when a tile failed its probes
   if (gate && *gate == 0u) return;
   extern __shared__ float4 s_dyn[];
@@ -114,14 +120,45 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const int ntiles = (nvert + 31) >> 5;
+  // Brick counts per axis live in shared memory and are re-read per tile, so
+  // they occupy no registers across the march (the march is register-bound).
+  __shared__ int s_nb[2];
+  if (threadIdx.x == 0) {
+    const int b0 = g.light_brick_log2;
+    s_nb[0] = (g.pd[0] + (1 << b0) - 1) >> b0;
+    s_nb[1] = (g.pd[1] + (1 << b0) - 1) >> b0;
+  }
+  __syncthreads();
+  const int ntiles = [&] {
+    const int b0 = g.light_brick_log2;
+    const int nbz = (g.pd[2] + (1 << b0) - 1) >> b0;
+    return b0 ? (s_nb[0] * s_nb[1] * nbz) << (3 * b0 - 5) : (nvert + 31) >> 5;
+  }();
   unsigned ns = 0;
 
   for (int tile = warp; tile < ntiles; tile += nwarps) {
-    const int id = (tile << 5) + lane;
-    if (id >= nvert) continue;
+    int id;
     float V[3], L[3];
-    map_vertex(g, id, V);
+    const int bl = g.light_brick_log2;
+    if (bl) {
+      const int nbx = *(volatile int*)&s_nb[0], nby = *(volatile int*)&s_nb[1];
+      // tile -> brick, lane -> vertex of the brick (x fastest inside the brick)
+      const int bi = tile >> (3 * bl - 5);
+      const int li = ((tile & ((1 << (3 * bl - 5)) - 1)) << 5) + lane;
+      const int m = (1 << bl) - 1;
+      const int bx = bi % nbx, byz = bi / nbx;
+      const int x = (bx << bl) + (li & m), y = ((byz % nby) << bl) + ((li >> bl) & m);
+      const int z = ((byz / nby) << bl) + (li >> (2 * bl));
+      if (x >= g.pd[0] || y >= g.pd[1] || z >= g.pd[2]) continue;
+      id = (z * g.pd[1] + y) * g.pd[0] + x;
+      V[0] = vtx_coord(g, 0, x);
+      V[1] = vtx_coord(g, 1, y);
+      V[2] = vtx_coord(g, 2, z);
+    } else {
+      id = (tile << 5) + lane;
+      if (id >= nvert) continue;
+      map_vertex(g, id, V);
+    }
     light_origin(g, V, L);
     const float v[3] = {V[0] - L[0], V[1] - L[1], V[2] - L[2]};
     const float rs = 1.f / sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
@@ -137,49 +174,92 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
     // two samples are in flight per ray). The break conditions are evaluated
     // in the reference's order for every sample; only o == 1 ends the march
     // early, after which the prefetched sample is discarded.
+    // Empty macro-cells (occ == 0: every value there has TF alpha 0) are
+    // stepped over without a field fetch: such a sample leaves the state
+    // unchanged (Accum), so only its position update and break checks run. sk
+    // counts the samples skipped before the one returned; they are counted as
+    // marched once that sample is composited (or the ray ends on its own).
     int b = g.light_budget;
-    auto gen = [&](float v8[8], float pc[3]) -> bool {
-      if (b-- <= 0) return false;
-      const float q0 = s[0] - st[0], q1 = s[1] - st[1], q2 = s[2] - st[2];
-      if (!(q0 * q0 + q1 * q1 + q2 * q2 <= len2)) return false;
-      s[0] = s[0] + sdx;
-      s[1] = s[1] + sdy;
-      s[2] = s[2] + sdz;
-      if (!inside_vol(g, s)) return false;
-      float4 e0, e1, e2;
-      const int c0 = find_cell_bsearch_t(T0, cm0, g.org[0], g.invh[0], s[0], e0);
-      const int c1 = find_cell_bsearch_t(T1, cm1, g.org[1], g.invh[1], s[1], e1);
-      const int c2 = find_cell_bsearch_t(T2, cm2, g.org[2], g.invh[2], s[2], e2);
-      QuadLoad<QuadT>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qz, v8);
-      // pcoords = (p - min) / (max - min) (RectilinearMeshOracle.h:189-192)
-      pc[0] = div_rn_markstein(s[0] - e0.x, e0.z, e0.w);
-      pc[1] = div_rn_markstein(s[1] - e1.x, e1.z, e1.w);
-      pc[2] = div_rn_markstein(s[2] - e2.x, e2.z, e2.w);
-      return true;
+    auto gen = [&](float v8[8], float pc[3], unsigned& sk) -> bool {
+      sk = 0;
+      for (;;) {
+        if (b-- <= 0) return false;
+        const float q0 = s[0] - st[0], q1 = s[1] - st[1], q2 = s[2] - st[2];
+        if (!(q0 * q0 + q1 * q1 + q2 * q2 <= len2)) return false;
+        s[0] = s[0] + sdx;
+        s[1] = s[1] + sdy;
+        s[2] = s[2] + sdz;
+        if (!inside_vol(g, s)) return false;
+        if (SKIP && !occupied(g, occ, s)) {
+          ++sk;
+          continue;
+        }
+        float4 e0, e1, e2;
+        const int c0 = find_cell_bsearch_t(T0, cm0, g.org[0], g.invh[0], s[0], e0);
+        const int c1 = find_cell_bsearch_t(T1, cm1, g.org[1], g.invh[1], s[1], e1);
+        const int c2 = find_cell_bsearch_t(T2, cm2, g.org[2], g.invh[2], s[2], e2);
+        QuadLoad<QuadT>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qz, v8);
+        // pcoords = (p - min) / (max - min) (RectilinearMeshOracle.h:189-192)
+        pc[0] = div_rn_markstein(s[0] - e0.x, e0.z, e0.w);
+        pc[1] = div_rn_markstein(s[1] - e1.x, e1.z, e1.w);
+        pc[2] = div_rn_markstein(s[2] - e2.x, e2.z, e2.w);
+        return true;
+      }
     };
     Accum<PREC> acc;
     acc.init(STITCH ? stitch_prefix(refs, nrefs, self, L, V, dir) : 0.f);
     float va[8], pa[3], vb[8], pb[3];
-    bool ok = gen(va, pa);
+    unsigned ska, skb;
+    if constexpr (!SKIP) {
+      bool ok = gen(va, pa, ska);
+      while (ok) {
+        const bool okb = gen(vb, pb, skb);
+        bool done;
+        {
+          float scalar = hex_interp(va, pa[0], pa[1], pa[2]);
+          scalar = (scalar - g.min_scalar) * g.inv_delta;
+          done = acc.add(s_a, s_tau, tf_index_clamped(scalar * (float)n1, n1));
+          ++ns;
+        }
+        if (done || !okb) break;
+        ok = gen(va, pa, ska);
+        {
+          float scalar = hex_interp(vb, pb[0], pb[1], pb[2]);
+          scalar = (scalar - g.min_scalar) * g.inv_delta;
+          done = acc.add(s_a, s_tau, tf_index_clamped(scalar * (float)n1, n1));
+          ++ns;
+        }
+        if (done) break;
+      }
+      acc.store(map, id);
+      continue;
+    }
+    bool ok = gen(va, pa, ska);
+    if (!ok) ns += ska;
     while (ok) {
-      const bool okb = gen(vb, pb);
+      const bool okb = gen(vb, pb, skb);
       bool done;
       {
         float scalar = hex_interp(va, pa[0], pa[1], pa[2]);
         scalar = (scalar - g.min_scalar) * g.inv_delta;
         done = acc.add(s_a, s_tau, tf_index_clamped(scalar * (float)n1, n1));
-        ++ns;
+        ns += 1 + ska;
       }
       // Stop when the accumulated value can no longer change (see Accum).
-      if (done || !okb) break;
-      ok = gen(va, pa);
+      if (done) break;
+      if (!okb) {
+        ns += skb;
+        break;
+      }
+      ok = gen(va, pa, ska);
       {
         float scalar = hex_interp(vb, pb[0], pb[1], pb[2]);
         scalar = (scalar - g.min_scalar) * g.inv_delta;
         done = acc.add(s_a, s_tau, tf_index_clamped(scalar * (float)n1, n1));
-        ++ns;
+        ns += 1 + skb;
       }
       if (done) break;
+      if (!ok) ns += ska;
     }
     acc.store(map, id);
   }
@@ -189,7 +269,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
 // ---------------------------------------------------------------------------
 // K2 (point field)
 // ---------------------------------------------------------------------------
-template <typename QuadT, bool USE_MAP, typename MapT, bool LIST = false>
+template <typename QuadT, bool USE_MAP, typename MapT, bool LIST = false, bool SKIP = false>
 __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const QuadT* __restrict__ quads,
                                                          const float4* __restrict__ tab,
                                                          const float4* __restrict__ tf,
@@ -197,7 +277,8 @@ __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const
                                                          float4* __restrict__ out,
                                                          Counters* __restrict__ cnt,
                                                          const unsigned* __restrict__ flist = nullptr,
-                                                         const unsigned* __restrict__ fcount = nullptr) {
+                                                         const unsigned* __restrict__ fcount = nullptr,
+                                                         const unsigned char* __restrict__ occ = nullptr) {
   extern __shared__ float4 s_dyn[];
   float4* s_tab = s_dyn;
   float4* s_tf = s_dyn + g.ntab;
@@ -220,7 +301,8 @@ __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const
     }
     if (x < g.width && y < g.height) {
       float4 color;
-      view_march_pixel<QuadT, USE_MAP, MapT>(g, quads, s_tab, s_tf, map, x, y, color, lit, hit);
+      view_march_pixel<QuadT, USE_MAP, MapT, NoRecord, SKIP>(g, quads, s_tab, s_tf, map, x, y, color, lit, hit,
+                                                              nullptr, occ);
       out[(size_t)y * g.width + x] = color;
     }
   }
@@ -454,30 +536,124 @@ cudaError_t launch_build_quads(const void* field, int in_dtype, void* quads, int
 template <typename QuadT, bool STITCH, bool PREC>
 static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4* tab, const float4* tf,
                              const float* tau, void* map, Counters* cnt, cudaStream_t st, const BrickRef* refs,
-                             int nrefs, int self, const unsigned* gate = nullptr) {
+                             int nrefs, int self, const unsigned* gate = nullptr,
+                             const unsigned char* occ = nullptr) {
   const int nvert = g.pd[0] * g.pd[1] * g.pd[2];
   const size_t smem = (size_t)g.max_off[0] * sizeof(float4) + 2 * (size_t)g.tf_n * sizeof(float);
   const int ntiles = (nvert + kThreads - 1) / kThreads;
   int grid = 0;
-  cudaError_t e = persistent_grid(k_light_march<QuadT, STITCH, PREC>, smem, ntiles, grid);
-  if (e != cudaSuccess) return e;
-  k_light_march<QuadT, STITCH, PREC><<<grid, kThreads, smem, st>>>(g, (const QuadT*)quads, tab, tf, tau, map,
-                                                                   nvert, cnt, refs, nrefs, self, gate);
+  cudaError_t e;
+  if (occ) {
+    e = persistent_grid(k_light_march<QuadT, STITCH, PREC, true>, smem, ntiles, grid);
+    if (e != cudaSuccess) return e;
+    k_light_march<QuadT, STITCH, PREC, true><<<grid, kThreads, smem, st>>>(g, (const QuadT*)quads, tab, tf, tau, map,
+                                                                           nvert, cnt, refs, nrefs, self, gate, occ);
+  } else {
+    e = persistent_grid(k_light_march<QuadT, STITCH, PREC, false>, smem, ntiles, grid);
+    if (e != cudaSuccess) return e;
+    k_light_march<QuadT, STITCH, PREC, false><<<grid, kThreads, smem, st>>>(g, (const QuadT*)quads, tab, tf, tau,
+                                                                            map, nvert, cnt, refs, nrefs, self, gate,
+                                                                            nullptr);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    float* map, Counters* cnt, cudaStream_t st, const BrickRef* refs, int nrefs,
-                                   int self, const unsigned* gate) {
-  if (refs) return launch_k1<float4, true, false>(g, quads, tab, tf, nullptr, map, cnt, st, refs, nrefs, self, gate);
-  return launch_k1<float4, false, false>(g, quads, tab, tf, nullptr, map, cnt, st, nullptr, 0, -1, gate);
+                                   int self, const unsigned* gate, const unsigned char* occ) {
+  if (refs)
+    return launch_k1<float4, true, false>(g, quads, tab, tf, nullptr, map, cnt, st, refs, nrefs, self, gate, occ);
+  return launch_k1<float4, false, false>(g, quads, tab, tf, nullptr, map, cnt, st, nullptr, 0, -1, gate, occ);
 }
 
 cudaError_t launch_light_march_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,
-                                    const float4* tf, const float* tau, __half* map, Counters* cnt, cudaStream_t st) {
+                                    const float4* tf, const float* tau, __half* map, Counters* cnt, cudaStream_t st,
+                                    const unsigned char* occ) {
   if (quad_dtype == 1)
-    return launch_k1<QuadBF16, false, true>(g, quads, tab, tf, tau, map, cnt, st, nullptr, 0, -1);
-  return launch_k1<QuadF16, false, true>(g, quads, tab, tf, tau, map, cnt, st, nullptr, 0, -1);
+    return launch_k1<QuadBF16, false, true>(g, quads, tab, tf, tau, map, cnt, st, nullptr, 0, -1, nullptr, occ);
+  return launch_k1<QuadF16, false, true>(g, quads, tab, tf, tau, map, cnt, st, nullptr, 0, -1, nullptr, occ);
+}
+
+// Occupancy of the 8^3-cell macro-cells: 0 when every value the trilinear
+// interpolation can produce inside cells [8m - 1, 8m + 8] (per axis) maps to a
+// TF entry of alpha 0 that lies inside the TF's index range (so a skipped view
+// sample still counts as lit). The corner min / max are widened by a relative
+// margin (the interpolation can overshoot its corners by a few ulps) and the TF
+// index range by 0.01 on each side; a NaN corner makes the macro-cell occupied,
+// and so does touching a volume max face (the view march's max-face rule keeps
+// the previous cell's reciprocal there, so those samples are never skipped).
+template <typename QuadT>
+__global__ void k_build_occupancy(const ExactGeo g, const QuadT* __restrict__ quads, const float4* __restrict__ tf,
+                                  unsigned char* __restrict__ occ) {
+  const int lane = threadIdx.x & 31;
+  const int nm = g.occ_n[0] * g.occ_n[1] * g.occ_n[2];
+  const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nm; w += (gridDim.x * blockDim.x) >> 5) {
+    const int m0 = w % g.occ_n[0], m1 = (w / g.occ_n[0]) % g.occ_n[1], m2 = w / (g.occ_n[0] * g.occ_n[1]);
+    int lo[3], ext[3];
+    const int mm[3] = {m0, m1, m2};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = max((mm[d] << kMacroLog2) - 1, 0);
+      const int hi = min((mm[d] << kMacroLog2) + (1 << kMacroLog2), g.n[d] - 2);
+      ext[d] = hi - lo[d] + 1;
+    }
+    const int count = ext[0] * ext[1] * ext[2];
+    float vmin = __int_as_float(0x7f800000), vmax = -vmin;
+    bool nan = false;
+    for (int i = lane; i < count; i += 32) {
+      const int x = lo[0] + i % ext[0], y = lo[1] + (i / ext[0]) % ext[1], z = lo[2] + i / (ext[0] * ext[1]);
+      float v[8];
+      QuadLoad<QuadT>::cell(quads, (unsigned)z * qz + (unsigned)y * qx + (unsigned)x, qz, v);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        nan |= (v[k] != v[k]);
+        vmin = fminf(vmin, v[k]);
+        vmax = fmaxf(vmax, v[k]);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      vmin = fminf(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+      vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+    }
+    nan = __any_sync(0xffffffffu, nan);
+    if (lane == 0) {
+      bool empty = !nan;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) empty &= (lo[d] + ext[d] - 1 < g.n[d] - 2);  // max face
+      if (empty) {
+        const double n1 = g.tf_n - 1;
+        const double pad = 1e-5 * fmax(fabs((double)vmin), fabs((double)vmax)) + 1e-30;
+        const double f0 = ((double)vmin - pad - g.min_scalar) * g.inv_delta * n1;
+        const double f1 = ((double)vmax + pad - g.min_scalar) * g.inv_delta * n1;
+        double a = fmin(f0, f1) - 0.01, b = fmax(f0, f1) + 0.01;
+        empty = a > -1.0 && b < n1 + 1.0;  // every sample passes the view march's range test
+        a = fmin(fmax(a, 0.0), n1);
+        b = fmin(fmax(b, 0.0), n1);
+        if (g.max_alpha > 0.f)
+          for (int i = (int)a; i <= (int)b && empty; ++i) empty = (tf[i].w == 0.f);
+      }
+      occ[w] = empty ? 0 : 1;
+    }
+  }
+}
+
+void occupancy_dims(const int n[3], int occ_n[3]) {
+  for (int d = 0; d < 3; ++d) occ_n[d] = ((n[d] - 1) + (1 << kMacroLog2) - 1) >> kMacroLog2;
+}
+
+cudaError_t launch_build_occupancy(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tf,
+                                   unsigned char* occ, cudaStream_t st) {
+  const int nm = g.occ_n[0] * g.occ_n[1] * g.occ_n[2];
+  const int blocks = (int)std::min<long long>(((long long)nm * 32 + 255) / 256, 148 * 64);
+  if (quad_dtype == 1)
+    k_build_occupancy<QuadBF16><<<blocks, 256, 0, st>>>(g, (const QuadBF16*)quads, tf, occ);
+  else if (quad_dtype == 2)
+    k_build_occupancy<QuadF16><<<blocks, 256, 0, st>>>(g, (const QuadF16*)quads, tf, occ);
+  else
+    k_build_occupancy<float4><<<blocks, 256, 0, st>>>(g, (const float4*)quads, tf, occ);
+  return cudaGetLastError();
 }
 
 // K6: sort-last composite of nb brick images in the given order
@@ -512,8 +688,29 @@ cudaError_t launch_composite(const float4* imgs, int nb, size_t npix, const int*
   return cudaGetLastError();
 }
 
+template <typename QuadT, bool USE_MAP, typename MapT>
+static cudaError_t launch_k2(const ExactGeo& g, const QuadT* quads, const float4* tab, const float4* tf,
+                             const MapT* map, float4* out, Counters* cnt, const unsigned char* occ, cudaStream_t st) {
+  const size_t smem = ((size_t)g.ntab + (size_t)g.tf_n) * sizeof(float4);
+  const int ntiles = (((g.width + 7) >> 3) * ((g.height + 3) >> 2) + 7) / 8;  // 8 warp tiles per block
+  int grid = 0;
+  cudaError_t e;
+  if (occ) {
+    e = persistent_grid(k_view_march<QuadT, USE_MAP, MapT, false, true>, smem, ntiles, grid);
+    if (e != cudaSuccess) return e;
+    k_view_march<QuadT, USE_MAP, MapT, false, true><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, map, out, cnt,
+                                                                                  nullptr, nullptr, occ);
+  } else {
+    e = persistent_grid(k_view_march<QuadT, USE_MAP, MapT>, smem, ntiles, grid);
+    if (e != cudaSuccess) return e;
+    k_view_march<QuadT, USE_MAP, MapT><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, map, out, cnt);
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_view_march_f32(const ExactGeo& g, const float* field, const float4* quads, const float4* tab,
-                                  const float4* tf, const float* map, float4* out, Counters* cnt, cudaStream_t st) {
+                                  const float4* tf, const float* map, float4* out, Counters* cnt, cudaStream_t st,
+                                  const unsigned char* occ) {
   const size_t smem = ((size_t)g.ntab + (size_t)g.tf_n) * sizeof(float4);
   const int ntiles = (((g.width + 7) >> 3) * ((g.height + 3) >> 2) + 7) / 8;  // 8 warp tiles per block
   int grid = 0;
@@ -523,13 +720,9 @@ cudaError_t launch_view_march_f32(const ExactGeo& g, const float* field, const f
     if (e != cudaSuccess) return e;
     k_view_march_cells<float><<<grid, kThreads, smem, st>>>(g, field, tab, tf, out, cnt);
   } else if (g.use_map) {
-    e = persistent_grid(k_view_march<float4, true, float>, smem, ntiles, grid);
-    if (e != cudaSuccess) return e;
-    k_view_march<float4, true, float><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, map, out, cnt);
+    return launch_k2<float4, true, float>(g, quads, tab, tf, map, out, cnt, occ, st);
   } else {
-    e = persistent_grid(k_view_march<float4, false, float>, smem, ntiles, grid);
-    if (e != cudaSuccess) return e;
-    k_view_march<float4, false, float><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, nullptr, out, cnt);
+    return launch_k2<float4, false, float>(g, quads, tab, tf, (const float*)nullptr, out, cnt, occ, st);
   }
   return cudaGetLastError();
 }
@@ -547,25 +740,14 @@ cudaError_t launch_view_march_tiles(const ExactGeo& g, const float4* quads, cons
   return cudaGetLastError();
 }
 
-template <typename QuadT, bool USE_MAP>
-static cudaError_t launch_k2_prec(const ExactGeo& g, const void* quads, const float4* tab, const float4* tf,
-                                  const __half* map, float4* out, Counters* cnt, cudaStream_t st) {
-  const size_t smem = ((size_t)g.ntab + (size_t)g.tf_n) * sizeof(float4);
-  const int ntiles = (((g.width + 7) >> 3) * ((g.height + 3) >> 2) + 7) / 8;
-  int grid = 0;
-  cudaError_t e = persistent_grid(k_view_march<QuadT, USE_MAP, __half>, smem, ntiles, grid);
-  if (e != cudaSuccess) return e;
-  k_view_march<QuadT, USE_MAP, __half><<<grid, kThreads, smem, st>>>(g, (const QuadT*)quads, tab, tf, map, out, cnt);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_view_march_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,
-                                   const float4* tf, const __half* map, float4* out, Counters* cnt, cudaStream_t st) {
+                                   const float4* tf, const __half* map, float4* out, Counters* cnt, cudaStream_t st,
+                                   const unsigned char* occ) {
   if (quad_dtype == 1)
-    return g.use_map ? launch_k2_prec<QuadBF16, true>(g, quads, tab, tf, map, out, cnt, st)
-                     : launch_k2_prec<QuadBF16, false>(g, quads, tab, tf, map, out, cnt, st);
-  return g.use_map ? launch_k2_prec<QuadF16, true>(g, quads, tab, tf, map, out, cnt, st)
-                   : launch_k2_prec<QuadF16, false>(g, quads, tab, tf, map, out, cnt, st);
+    return g.use_map ? launch_k2<QuadBF16, true, __half>(g, (const QuadBF16*)quads, tab, tf, map, out, cnt, occ, st)
+                     : launch_k2<QuadBF16, false, __half>(g, (const QuadBF16*)quads, tab, tf, map, out, cnt, occ, st);
+  return g.use_map ? launch_k2<QuadF16, true, __half>(g, (const QuadF16*)quads, tab, tf, map, out, cnt, occ, st)
+                   : launch_k2<QuadF16, false, __half>(g, (const QuadF16*)quads, tab, tf, map, out, cnt, occ, st);
 }
 
 // ---------------------------------------------------------------------------

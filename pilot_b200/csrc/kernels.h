@@ -12,12 +12,19 @@ cudaError_t launch_build_tables(const ExactGeo& g, float4* tab, cudaStream_t st)
 cudaError_t launch_build_quads(const void* field, int in_dtype, void* quads, int quad_dtype, const int n[3],
                                cudaStream_t st);
 cudaError_t launch_light_march_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,
-                                    const float4* tf, const float* tau, __half* map, Counters* cnt, cudaStream_t st);
+                                    const float4* tf, const float* tau, __half* map, Counters* cnt, cudaStream_t st,
+                                    const unsigned char* occ = nullptr);
 cudaError_t launch_view_march_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,
-                                   const float4* tf, const __half* map, float4* out, Counters* cnt, cudaStream_t st);
+                                   const float4* tf, const __half* map, float4* out, Counters* cnt, cudaStream_t st,
+                                   const unsigned char* occ = nullptr);
 cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    float* map, Counters* cnt, cudaStream_t st, const BrickRef* refs = nullptr,
-                                   int nrefs = 0, int self = -1, const unsigned* gate = nullptr);
+                                   int nrefs = 0, int self = -1, const unsigned* gate = nullptr,
+                                   const unsigned char* occ = nullptr);
+// Empty-space occupancy of 8^3-cell macro-cells for the light march's skip.
+void occupancy_dims(const int n[3], int occ_n[3]);
+cudaError_t launch_build_occupancy(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tf,
+                                   unsigned char* occ, cudaStream_t st);
 // K2 over a device list of kFallbackTile^2 pixel tiles (count in *fcount), with the map.
 cudaError_t launch_view_march_tiles(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                     const float* map, float4* out, Counters* cnt, const unsigned* flist,
@@ -36,7 +43,8 @@ cudaError_t launch_pack_weights(const float* P, uint2* W, float* aux, cudaStream
 cudaError_t launch_composite(const float4* imgs, int nb, size_t npix, const int* order, float4* out,
                              cudaStream_t st);
 cudaError_t launch_view_march_f32(const ExactGeo& g, const float* field, const float4* quads, const float4* tab,
-                                  const float4* tf, const float* map, float4* out, Counters* cnt, cudaStream_t st);
+                                  const float4* tf, const float* map, float4* out, Counters* cnt, cudaStream_t st,
+                                  const unsigned char* occ = nullptr);
 cudaError_t launch_selftest_division(float org, float h, int ncells, int samples, unsigned long long* d_out,
                                      cudaStream_t st);
 

@@ -97,6 +97,7 @@ struct beams_renderer {
   float cutoff = 1.f;
   float light_steps = 128.f;
   int slab_fp64 = 1;
+  int light_brick_log2 = 3;  // beams_set_tuning (8^3-vertex bricks)
   bool reuse_map = false;
   bool bg = false;
   float bg_rgba[4] = {1.f, 1.f, 1.f, 1.f};
@@ -123,6 +124,12 @@ struct beams_renderer {
   float4* d_tab = nullptr;
   size_t tab_cap = 0;
   unsigned long long tab_key[4] = {0, 0, 0, 0};  // volume_version, map m[3] packed
+  // empty-space occupancy of 8^3-cell macro-cells (light-march skip)
+  unsigned char* d_occ = nullptr;
+  size_t occ_cap = 0;
+  unsigned long long occ_key[2] = {~0ull, ~0ull};  // quads key, tf_version
+  int empty_skip = 1;  // map build skips empty macro-cells
+  int view_skip = 1;   // view march skips empty macro-cells
 
   // multi-block scene (beams_set_bricks)
   std::vector<beams::Brick> bricks;
@@ -149,6 +156,7 @@ struct beams_renderer {
     if (d_map) cudaFree(d_map);
     if (d_quads) cudaFree(d_quads);
     if (d_tab) cudaFree(d_tab);
+    if (d_occ) cudaFree(d_occ);
     if (d_tau) cudaFree(d_tau);
     if (d_rgba) cudaFree(d_rgba);
     for (auto& b : bricks) b.release();

@@ -28,11 +28,15 @@ struct NoRecord {
   __device__ __forceinline__ void operator()(const float*, const float4&, float) {}
 };
 
-template <typename QuadT, bool USE_MAP, typename MapT, typename Rec = NoRecord>
+// SKIP: samples in macro-cells whose occupancy is 0 (every value there maps to
+// an in-range TF entry of alpha 0) only advance and count as lit: their
+// premultiplied alpha is 0, so they change neither colour nor alpha.
+template <typename QuadT, bool USE_MAP, typename MapT, typename Rec = NoRecord, bool SKIP = false>
 __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT* __restrict__ quads,
                                                  const float4* s_tab, const float4* s_tf,
                                                  const MapT* __restrict__ map, int x, int y, float4& color,
-                                                 unsigned& lit, unsigned& hit, Rec* rec = nullptr) {
+                                                 unsigned& lit, unsigned& hit, Rec* rec = nullptr,
+                                                 const unsigned char* __restrict__ occ = nullptr) {
   color = make_float4(0.f, 0.f, 0.f, 0.f);
   float o[3], d[3], minD, maxD;
   if (!ray_setup(g, x, y, o, d, minD, maxD)) return;
@@ -57,6 +61,17 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT*
   float inv[3] = {0.f, 0.f, 0.f};
   const int n1 = g.tf_n - 1;
   while (inside_vol(g, p) && dist < maxD && budget-- > 0) {
+    if (SKIP && !occupied(g, occ, p)) {
+      ++lit;
+      dist += g.sd;
+      p[0] = p[0] + sdx;
+      p[1] = p[1] + sdy;
+      p[2] = p[2] + sdz;
+      tx = (p[0] - bl[0]) * inv[0];
+      ty = (p[1] - bl[1]) * inv[1];
+      tz = (p[2] - bl[2]) * inv[2];
+      continue;  // colour unchanged, so the cutoff test cannot newly pass
+    }
     const float mint = mn(tx, mn(ty, tz));
     const float maxt = mx(tx, mx(ty, tz));
     if (maxt > 1.f || mint < 0.f) newCell = true;

@@ -10,6 +10,8 @@ synthetic fields, so every scene here is generated from a seed:
 * ``config1``: 512^3 float32 4-octave gradient noise (lacunarity 2, gain 0.5)
   remapped to [0,1]; 1024x1024 image; point light at 2x the domain diagonal
   along a seeded direction; map M = 256; step 0.5 voxel; alpha cut 0.99.
+* ``config2``: 1024^3 sum of 64 blobs plus 10% gradient noise, normalised;
+  2048x2048 image; M = 512; step 0.25 voxel (the precision form's workload).
 
 The domain is the unit cube, spacing 1/(N-1). The transfer function is a
 256-entry table: alpha piecewise-linear through (0.2, 0), (0.4, 0.05),
@@ -147,6 +149,7 @@ class Scene:
     base_freq: float = 4.0
 
     brick_spacing: tuple | None = None
+    noise_amp: float = 0.1
 
     @property
     def spacing(self):
@@ -161,6 +164,10 @@ class Scene:
             self.array = blobs_numpy(self.dims, self.params)
         elif self.kind == "noise":
             self.array = noise_numpy(self.dims, self.params, self.octaves, self.base_freq)
+        elif self.kind == "blobnoise":
+            b = blobs_numpy(self.dims, self.params[0])
+            nz = noise_numpy(self.dims, self.params[1], self.octaves, self.base_freq)
+            self.array = _normalise(b + np.float32(self.noise_amp) * nz)
         else:
             raise ValueError(self.kind)
         return self.array
@@ -185,6 +192,20 @@ class Scene:
             p = np.ascontiguousarray(self.params, np.uint8)
             st = L.beams_generate_noise(C.c_void_p(t.data_ptr()), n, p.ctypes.data_as(C.c_void_p),
                                         self.octaves, self.base_freq, 2.0, 0.5, stream)
+        elif self.kind == "blobnoise":
+            p = np.ascontiguousarray(self.params[0], np.float32)
+            st = L.beams_generate_blobs(C.c_void_p(t.data_ptr()), n, p.ctypes.data_as(C.c_void_p),
+                                        p.shape[0], 1, stream)
+            if st == 0:
+                nz = torch.empty_like(t)
+                q = np.ascontiguousarray(self.params[1], np.uint8)
+                st = L.beams_generate_noise(C.c_void_p(nz.data_ptr()), n, q.ctypes.data_as(C.c_void_p),
+                                            self.octaves, self.base_freq, 2.0, 0.5, stream)
+                if st == 0:
+                    t.add_(nz, alpha=self.noise_amp)
+                    del nz
+                    lo, hi = t.min(), t.max()
+                    t.sub_(lo).mul_(1.0 / (hi - lo)).clamp_(0, 1)
         else:
             return torch.from_numpy(self.field_numpy()).cuda()
         if st != 0:
@@ -239,6 +260,21 @@ def config1(seed: int = 1, n: int = 512, image: int = 1024, m: int = 256, cutoff
     return Scene(name=f"noise{n}_img{image}_M{m}", dims=(n, n, n), kind="noise", params=perm, tf=tf_table(),
                  light_kind=0, light=lpos, map_m=m, sample_distance=0.5 / (n - 1), cutoff=cutoff,
                  cam_pos=pos, cam_up=up, width=image, height=image)
+
+
+def config2(seed: int = 2, n: int = 1024, image: int = 2048, m: int = 512, cutoff: float = 0.99) -> Scene:
+    """The precision form's workload: 64 Gaussian blobs plus 10% gradient noise,
+    normalised to [0,1]; 2048^2 image; M = 512 map; view step 0.25 voxel; point
+    light at 2x the diagonal."""
+    rng = np.random.default_rng(seed)
+    params = blob_params(rng, 64)
+    perm = rng.permutation(256).astype(np.uint8)
+    pos, up = _unit_sphere_camera(rng)
+    ldir = random_unit(rng)
+    lpos = tuple(float(x) for x in (np.array([0.5, 0.5, 0.5]) + 2.0 * np.sqrt(3.0) * ldir))
+    return Scene(name=f"blobnoise{n}_img{image}_M{m}", dims=(n, n, n), kind="blobnoise", params=(params, perm),
+                 tf=tf_table(), light_kind=0, light=lpos, map_m=m, sample_distance=0.25 / (n - 1), cutoff=cutoff,
+                 cam_pos=pos, cam_up=up, width=image, height=image, base_freq=8.0)
 
 
 def small(seed: int = 0, n: int = 24, image: int = 48, m: int = 12, kind: str = "blobs", light_kind: int = 0,

@@ -205,3 +205,33 @@ def test_mapper_mirror(cuda_device):
     assert s.cutoff == 1.0  # the mapper keeps the reference's alpha >= 1 break
     ref, _ = Oracle(s).view_march(None)
     assert np.max(np.abs(img - ref)) <= TOL
+
+
+@pytest.mark.parametrize("kind", ["blobs", "noise"])
+def test_vertex_order_and_empty_skip_change_nothing(cuda_device, kind):
+    """The map build's vertex order (rows or bricks) and its skipping of empty
+    macro-cells are launch choices: map, image and sample counts stay identical."""
+    s = scenes.small(71, n=40, image=48, m=20, kind=kind, light_kind=0)
+    r = B.Renderer(0)
+    r.set_volume(s.field_numpy(), origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+    s.configure(r)
+    ref = None
+    for lb in (0, 8, 16, 32, 64):
+        for skip in (False, True):
+            r.set_tuning(light_brick=lb, empty_skip=skip, view_skip=skip)
+            assert r.get_tuning() == {"light_brick": lb, "empty_skip": skip, "view_skip": skip}
+            img, t = r.render(s.camera())
+            m = r.get_shadow_map((s.map_m + 1) ** 3)
+            cur = (m, img, t["light_samples"], t["lit_samples"])
+            if ref is None:
+                ref = cur
+                om, _ = Oracle(s).light_march()
+                assert np.array_equal(m, om.ravel())
+            assert np.array_equal(cur[0], ref[0]) and np.array_equal(cur[1], ref[1]), (lb, skip)
+            assert cur[2:] == ref[2:], (lb, skip, cur[2:], ref[2:])
+    with pytest.raises(B.BeamsError):
+        r.set_tuning(light_brick=12)
+    best = r.autotune(s.camera())
+    assert best["light_brick"] in (0, 8, 16, 32, 64) and best["map_ms"] > 0 and best["view_ms"] > 0
+    img, _ = r.render(s.camera())
+    assert np.array_equal(img, ref[1])

@@ -10,6 +10,8 @@ larger than L2, so no flush is needed between steps.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
   python bench.py --form precision [--field-dtype bf16|f16]   # config 2, 1024^3, 2048^2, M = 512
   python bench.py --form mlp [--knot 4] [--mlp-scene-light]    # learned form on the config 1 field
+  python bench.py --form batch [--requests 64]                 # config 3: batched requests, one launch
+  python bench.py --form bricks                                # config 3: 2x2x2 bricks of the 512^3 field
 
 N > 1 runs N independent replicas (the path does not shard across GPUs: there
 is no exchange step), launched by torch.distributed.run; value is the total over
@@ -569,6 +571,190 @@ def run_form(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# --form batch: 64 serving requests in one persistent launch (config 3)
+# --form bricks: the 512^3 noise field as 2x2x2 bricks, stitched and composited
+# ---------------------------------------------------------------------------
+BATCH_SIZES = (64, 128, 256, 384)
+BATCH_IMAGES = (256, 512, 1024)
+
+
+def batch_volumes(seed=3):
+    """Eight resident volumes: {64, 128, 256, 384}^3 x {blobs, noise}, generated on the device."""
+    from pilot_b200 import scenes
+    vols = []
+    for i, n in enumerate(BATCH_SIZES):
+        for kind in ("blobs", "noise"):
+            sc = scenes.small(seed + 10 * i + (kind == "noise"), n=n, kind=kind)
+            sc.base_freq = 4.0
+            vols.append((sc, sc.field_device()))
+    return vols
+
+
+def batch_requests(B, vols, rng, nreq, outs):
+    reqs = []
+    for i in range(nreq):
+        sc, _ = vols[i % len(vols)]
+        n = sc.dims[0]
+        w = outs[i].shape[1]
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        cam = B.Renderer.camera(tuple(0.5 + d), (0.5, 0.5, 0.5), (0, 1, 0) if abs(d[1]) < 0.9 else (1, 0, 0),
+                                30.0, w, w)
+        ld = rng.normal(size=3)
+        ld /= np.linalg.norm(ld)
+        light = tuple(0.5 + 2.0 * np.sqrt(3.0) * ld)
+        reqs.append(B.Renderer.request(i % len(vols), cam, light, map_cells=n // 2, sample_distance=0.5 / (n - 1),
+                                       termination_alpha=0.99, out=outs[i]))
+    return reqs
+
+
+def run_batch(args):
+    import torch
+
+    from pilot_b200 import beams as B
+    from pilot_b200 import scenes
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    vols = batch_volumes()
+    rng = np.random.default_rng(11)
+    nreq = args.requests
+    sizes = [int(rng.choice(BATCH_IMAGES)) for _ in range(nreq)]
+    outs = [torch.empty((w, w, 4), device="cuda") for w in sizes]
+    r = B.Renderer(local, stream=stream.cuda_stream)
+    r.set_color_map(scenes.tf_table())
+    r.batch_set_volumes([(f, sc.origin, sc.spacing, sc.value_range) for sc, f in vols])
+    reqs = batch_requests(B, vols, rng, nreq, outs)
+    tuning = r.batch_autotune(reqs)
+    for _ in range(args.warmup):
+        r.render_batch(batch_requests(B, vols, rng, nreq, outs), timings=False)
+    torch.cuda.synchronize()
+    lit = 0
+    sampler = ClockSampler(local)
+    with sampler:
+        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):  # new cameras and lights every step; the graph is replayed
+            _, t = r.render_batch(batch_requests(B, vols, rng, nreq, outs), timings=True)
+            lit += t["lit_samples"]
+        z.record(stream)
+        torch.cuda.synchronize()
+    total_ms = a.elapsed_time(z)
+    # the same requests one render at a time through the single-request API
+    singles = []
+    for sc, f in vols:
+        q = B.Renderer(local, stream=stream.cuda_stream)
+        q.set_volume(f, origin=sc.origin, spacing=sc.spacing, value_range=sc.value_range)
+        q.set_color_map(scenes.tf_table())
+        q.set_termination_alpha(0.99)
+        q.set_sample_distance(0.5 / (sc.dims[0] - 1))
+        q.set_shadow_map_size(sc.dims[0] // 2)
+        singles.append(q)
+    seq_reqs = batch_requests(B, vols, rng, nreq, outs)
+
+    def sequential():
+        for (rq, o) in seq_reqs:
+            q = singles[rq.volume]
+            q.clear_lights()
+            q.add_point_light(tuple(rq.light), (1, 1, 1), 1.0)
+            q.render(rq.camera, out=o, timings=False)
+    sequential()
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(max(1, args.steps // 4)):
+        sequential()
+    z.record(stream)
+    torch.cuda.synchronize()
+    seq_ms = a.elapsed_time(z) / max(1, args.steps // 4)
+    # end to end: images to pinned host memory
+    host = [torch.empty((w, w, 4)).pin_memory() for w in sizes]
+    r.render_batch(batch_requests(B, vols, rng, nreq, host), timings=False)
+    t0 = time.perf_counter()
+    ne = max(3, min(args.steps, 10))
+    lit_e = 0
+    for _ in range(ne):
+        _, t = r.render_batch(batch_requests(B, vols, rng, nreq, host), timings=True)
+        lit_e += t["lit_samples"]
+    e2e_s = time.perf_counter() - t0
+    value = lit / (total_ms / 1e3)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded blob and noise volumes generated on the device)",
+            "config": {"workload": f"config3: {nreq} requests per step over 8 resident volumes "
+                                   f"{{64,128,256,384}}^3 x {{blobs, noise}}, images {{256,512,1024}}^2, M = N/2, "
+                                   f"view step 0.5 voxel, alpha cut 0.99, new random camera and point light per "
+                                   f"request every step; one persistent launch replayed from a CUDA graph",
+                       "form": "batch", "tuning": tuning, "parallelism": "1 GPU",
+                       "l2": "volumes and maps total well above L2; no flush"},
+            "requests_per_s": nreq * args.steps / (total_ms / 1e3),
+            "sequential_ms_per_batch": seq_ms, "speedup_vs_sequential": seq_ms / (total_ms / args.steps),
+            "gpu_launches": args.steps,
+            "e2e": {"value": lit_e / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(sum(w * w * 16 for w in sizes)),
+                    "note": "wall clock per batch: host request set-up, graph replay, images to pinned host memory"},
+            "clocks": sampler.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_bricks(args):
+    import torch
+
+    from oracle.oracle import psnr
+    from pilot_b200 import beams as B
+    from pilot_b200 import scenes
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    s = scenes.config1()
+    fd = s.field_device()
+    cam = s.camera()
+    out = torch.empty((s.height, s.width, 4), device="cuda")
+    r = B.Renderer(local, stream=stream.cuda_stream)
+    r.set_volume(fd, origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+    s.configure(r)
+    r.render(cam, out=out, timings=False)
+    r.autotune(cam)
+    whole_ms, _ = time_frames(lambda: r.render(cam, out=out, timings=False), 10, 3, stream, 1, local)
+    whole_ms /= 10
+    whole = out.cpu().numpy()
+    # 2x2x2 bricks; neighbours share their face plane (the reference's blocks)
+    nx = s.dims[0]
+    cells = nx - 1
+    edges = [round(i * cells / 2) for i in range(3)]
+    h = s.spacing
+    bricks = []
+    for z0, z1 in zip(edges[:-1], edges[1:]):
+        for y0, y1 in zip(edges[:-1], edges[1:]):
+            for x0, x1 in zip(edges[:-1], edges[1:]):
+                sub = fd[z0:z1 + 1, y0:y1 + 1, x0:x1 + 1].contiguous()
+                org = (s.origin[0] + x0 * h[0], s.origin[1] + y0 * h[1], s.origin[2] + z0 * h[2])
+                bricks.append((sub, org, h, s.value_range))
+    del fd
+    r.set_bricks(bricks)
+    s.configure(r)
+    r.set_shadow_map_size(s.map_m // 2)  # each brick's map keeps the whole field's vertex spacing
+    _, tb = r.render(cam, out=out, timings=True)
+    img = out.cpu().numpy()
+    frame = lambda: r.render(cam, out=out, timings=False)  # noqa: E731
+    total_ms, clocks = time_frames(frame, args.steps, args.warmup, stream, 1, local)
+    value = tb["lit_samples"] * args.steps / (total_ms / 1e3)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded 4-octave gradient noise generated on the device)",
+            "config": {"workload": "config3 bricks: the 512^3 noise field as 2x2x2 bricks of 256-257 points per axis, "
+                                   "1024^2 image, per-brick M = 128; Phase 1 local maps, cross-brick stitch, "
+                                   "per-brick view march, depth-ordered composite",
+                       "form": "bricks", "parallelism": "1 GPU, 8 bricks", "l2": "inputs larger than L2; no flush"},
+            "lit_samples_per_frame": tb["lit_samples"], "gpu_launches": tb["kernel_launches"] * args.steps,
+            "phases_ms": {"maps_and_stitch": tb["map_build_ms"], "view_marches": tb["view_march_ms"],
+                          "composite": tb["composite_ms"]},
+            "undivided_ms_per_frame": whole_ms, "psnr_vs_undivided": psnr(img, whole), "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -576,7 +762,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=None, choices=[0, 1, 2])
-    ap.add_argument("--form", default="exact", choices=["exact", "precision", "mlp"])
+    ap.add_argument("--form", default="exact", choices=["exact", "precision", "mlp", "batch", "bricks"])
+    ap.add_argument("--requests", type=int, default=64, help="batch form: requests per step")
     ap.add_argument("--field-dtype", default="bf16", choices=["bf16", "f16"], help="precision form")
     ap.add_argument("--knot", type=int, default=4, help="mlp form: network every knot lit samples")
     ap.add_argument("--probe-fraction", type=float, default=0.01)
@@ -598,6 +785,10 @@ def main():
         args.config = 2 if args.form == "precision" else 1
     if args.impl == "reference":
         return run_reference(args)
+    if args.form == "batch":
+        return run_batch(args)
+    if args.form == "bricks":
+        return run_bricks(args)
     if args.form != "exact":
         return run_form(args)
     return run_ours(args)

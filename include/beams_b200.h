@@ -191,6 +191,48 @@ beams_status beams_set_bricks(beams_renderer* r, const beams_volume* bricks, int
 beams_status beams_get_brick_map(beams_renderer* r, int brick, int stage, float* dst, size_t count,
                                  int dst_on_device);
 
+/* ---- batched form (serving) ---------------------------------------------------- */
+/* No reference counterpart: the reference renders one camera per RenderCells call
+ * (MapperLightedVolume.cxx:114-193). Here volumes stay resident and a batch of
+ * requests, each with its own volume, camera, light, map size and sample
+ * distance, runs as ONE persistent kernel launch (map builds first, view tiles
+ * after, a view tile waiting with a bounded wait for its request's map),
+ * captured once into a CUDA graph and replayed while the batch's shapes stay
+ * the same. The colour map is the renderer's. Results equal beams_render's
+ * exact form for the same settings. */
+beams_status beams_batch_set_volumes(beams_renderer* r, const beams_volume* vols, int n);  /* float32 points */
+typedef struct beams_request {
+  int volume;               /* index into the beams_batch_set_volumes list */
+  beams_camera camera;
+  int light_kind;           /* 0 point (light = position), 1 directional (light = travel direction) */
+  double light[3];
+  float light_color[3];
+  float light_intensity;
+  int map_cells;            /* M: the map has (M+1)^3 vertices */
+  float sample_distance;    /* <= 0: |extent| / 200 */
+  float termination_alpha;  /* (0, 1]; 1 is the reference's */
+  float* rgba_out;          /* width * height RGBA */
+  int out_on_device;
+} beams_request;
+typedef struct beams_batch_options {
+  int tile_w, tile_h;       /* view work item in pixels (default 32 x 32): tile_w a multiple of 8, tile_h of 4,
+                               at most 16384 pixels; warps take its 8 x 4 sub-tiles */
+  int light_brick;          /* map-build vertex order: 0 rows, 8/16/32/64 bricks */
+  int use_graph;            /* 1: capture once, replay (default) */
+  int no_skip;              /* 1: no empty-space skipping (default 0: both marches skip empty macro-cells) */
+  int reserved;
+} beams_batch_options;
+beams_status beams_set_batch_options(beams_renderer* r, const beams_batch_options* o);
+/* Timings: total_ms = the batch (launch to last image copied), view_march_ms = the
+ * persistent kernel and its staging copies, lit_samples and rays_hit summed. */
+beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, int n, beams_timings* t);
+/* Tunes the batch options on these requests by coordinate descent over the
+ * empty-space skip, the vertex order {rows, 8, 16, 32, 64 bricks} and the view
+ * tile {16x16, 32x8, 8x32, 32x32, 64x32, 64x64}; keeps the fastest (images are identical
+ * under all of them) and reports it. */
+beams_status beams_batch_autotune(beams_renderer* r, const beams_request* reqs, int n, beams_batch_options* best,
+                                  float* best_ms);
+
 /* ---- learned form ------------------------------------------------------------ */
 /* No reference counterpart: a transmittance network (encoded position and light
  * direction -> 4 x 64 ReLU -> sigmoid) that replaces the map build and lookup

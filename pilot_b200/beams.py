@@ -70,6 +70,18 @@ class Camera(C.Structure):
                 ("fov_y_deg", C.c_double), ("width", C.c_int), ("height", C.c_int)]
 
 
+class Request(C.Structure):
+    _fields_ = [("volume", C.c_int), ("camera", Camera), ("light_kind", C.c_int), ("light", C.c_double * 3),
+                ("light_color", C.c_float * 3), ("light_intensity", C.c_float), ("map_cells", C.c_int),
+                ("sample_distance", C.c_float), ("termination_alpha", C.c_float), ("rgba_out", C.c_void_p),
+                ("out_on_device", C.c_int)]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("tile_w", C.c_int), ("tile_h", C.c_int), ("light_brick", C.c_int), ("use_graph", C.c_int),
+                ("no_skip", C.c_int), ("reserved", C.c_int)]
+
+
 class Timings(C.Structure):
     _fields_ = [("map_build_ms", C.c_float), ("view_march_ms", C.c_float), ("composite_ms", C.c_float),
                 ("total_ms", C.c_float), ("light_samples", C.c_ulonglong), ("lit_samples", C.c_ulonglong),
@@ -127,6 +139,10 @@ def lib():
         "beams_mlp_probe_errors": ([P, P, C.c_int], C.c_int),
         "beams_set_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "beams_get_tuning": ([P, C.POINTER(Tuning)], C.c_int),
+        "beams_batch_set_volumes": ([P, P, C.c_int], C.c_int),
+        "beams_set_batch_options": ([P, C.POINTER(BatchOptions)], C.c_int),
+        "beams_render_batch": ([P, P, C.c_int, C.POINTER(Timings)], C.c_int),
+        "beams_batch_autotune": ([P, P, C.c_int, C.POINTER(BatchOptions), C.POINTER(C.c_float)], C.c_int),
         "beams_autotune": ([P, C.POINTER(Camera), C.POINTER(Tuning), C.POINTER(C.c_float), C.POINTER(C.c_float)],
                            C.c_int),
         "beams_mlp_save": ([P, C.c_char_p], C.c_int),
@@ -231,6 +247,54 @@ class Renderer:
         v = Volume(ptr, dtype, (C.c_int * 3)(*dims), _d3(origin), _d3(spacing),
                    (C.c_double * 2)(*value_range), assoc, on_device)
         self._check(self._L.beams_set_volume(self._h, C.byref(v)))
+
+    # -- batched form -----------------------------------------------------------
+    def batch_set_volumes(self, volumes):
+        """volumes: list of (array (z,y,x) float32 numpy or torch CUDA tensor, origin, spacing, value_range)."""
+        vols = (Volume * len(volumes))()
+        self._keep_batch = []
+        for i, (data, origin, spacing, vrange) in enumerate(volumes):
+            if isinstance(data, np.ndarray):
+                arr = np.ascontiguousarray(data, np.float32)
+                self._keep_batch.append(arr)
+                ptr, on_dev = arr.ctypes.data_as(C.c_void_p), 0
+                nz, ny, nx = arr.shape
+            else:
+                self._keep_batch.append(data)
+                ptr, on_dev = C.c_void_p(data.data_ptr()), 1
+                nz, ny, nx = data.shape
+            vols[i] = Volume(ptr, F32, (C.c_int * 3)(nx, ny, nz), _d3(origin), _d3(spacing),
+                             (C.c_double * 2)(*vrange), ASSOC_POINTS, on_dev)
+        self._check(self._L.beams_batch_set_volumes(self._h, vols, len(volumes)))
+
+    def set_batch_options(self, tile_w=32, tile_h=32, light_brick=8, use_graph=True, skip=True):
+        o = BatchOptions(int(tile_w), int(tile_h), int(light_brick), int(bool(use_graph)), int(not skip))
+        self._check(self._L.beams_set_batch_options(self._h, C.byref(o)))
+
+    @staticmethod
+    def request(volume, camera, light, light_kind=0, light_color=(1, 1, 1), light_intensity=1.0, map_cells=16,
+                sample_distance=-1.0, termination_alpha=1.0, out=None):
+        """One batch request; out: numpy (H,W,4) float32 or torch CUDA tensor (allocated if None)."""
+        if out is None:
+            out = np.zeros((camera.height, camera.width, 4), np.float32)
+        on_dev = 0 if isinstance(out, np.ndarray) else int(out.is_cuda)
+        rq = Request(int(volume), camera, int(light_kind), _d3(light), _f3(light_color), float(light_intensity),
+                     int(map_cells), float(sample_distance), float(termination_alpha), _ptr(out), on_dev)
+        return rq, out
+
+    def batch_autotune(self, reqs):
+        arr = (Request * len(reqs))(*[r for r, _ in reqs])
+        o, ms = BatchOptions(), C.c_float()
+        self._check(self._L.beams_batch_autotune(self._h, arr, len(reqs), C.byref(o), C.byref(ms)))
+        return {"tile_w": o.tile_w, "tile_h": o.tile_h, "light_brick": o.light_brick, "skip": not o.no_skip,
+                "batch_ms": ms.value}
+
+    def render_batch(self, reqs, timings=True):
+        """reqs: list of (Request, out) from Renderer.request; returns the outputs and timings."""
+        arr = (Request * len(reqs))(*[r for r, _ in reqs])
+        t = Timings() if timings else None
+        self._check(self._L.beams_render_batch(self._h, arr, len(reqs), C.byref(t) if t is not None else None))
+        return [o for _, o in reqs], (t.as_dict() if t is not None else None)
 
     def set_bricks(self, bricks):
         """bricks: list of (array (z,y,x) float32 numpy or torch CUDA tensor, origin, spacing, value_range)."""

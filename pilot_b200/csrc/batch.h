@@ -1,0 +1,56 @@
+// batch.h — device-side layout of a batch of render requests (k_batch.cu,
+// batch_api.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "beams_params.h"
+
+namespace beams {
+
+constexpr int kMaxRequests = 256;
+constexpr int kBatchThreads = 256;
+constexpr int kBatchChunk = 2048;  // vertex slots per map-build work item (64 warp tiles)
+
+// What the persistent kernel needs of one request besides its ExactGeo.
+struct BatchDesc {
+  const float4* quads;        // the request volume's 4-corner quad field (float32)
+  const unsigned char* occ;   // its macro-cell occupancy (empty-space skipping), or null
+  float* map;                 // (M+1)^3 opacities, 256-byte aligned, private to the request
+  float4* out;                // width * height RGBA
+  int nvert;
+  int tiles_x;                // view tiles per image row
+};
+
+// Work items, in queue order: the map-build items of request 0, then for
+// r = 1..n-1 the map-build items of r followed by the view items of r-1, and
+// last the view items of n-1. A view item of r waits for r's map items, which
+// all precede it in the queue; r's map is then one request old, so it is
+// still in L2 when its view tiles read it. Segment k covers items
+// [seg_off[k], seg_off[k+1]) of request seg_req[k] & 0xffff, phase 2 (view)
+// when bit 16 is set. Lives in device memory (uploaded when the batch's shapes change).
+struct BatchPlan {
+  int n;
+  int nseg;
+  int total;
+  int tile_w, tile_h;     // view tile: a multiple of 8 x 4 warp tiles
+  int brick_log2;         // map-build vertex order inside a request (0 = rows)
+  int skip;               // 1: both marches skip empty macro-cells (every desc has occ)
+  int pad;
+  int seg_off[2 * kMaxRequests + 1];
+  int seg_req[2 * kMaxRequests];
+  int k1_items[kMaxRequests];  // map-build items per request (what a view item waits for)
+};
+
+// Zeroed before every launch.
+struct BatchQueue {
+  unsigned next;
+  unsigned error;         // 1: a view item gave up waiting for its map (bounded wait)
+  unsigned done1[kMaxRequests];
+};
+
+// Dynamic shared memory and persistent grid of the batch kernel (call outside graph capture).
+cudaError_t batch_launch_config(int tf_n, size_t max_ntab, int total_items, size_t& smem, int& grid);
+cudaError_t launch_batch(const ExactGeo* geos, const BatchDesc* descs, const BatchPlan* plan, int skip,
+                         const float4* tf, size_t smem, int grid, BatchQueue* q, Counters* cnt, cudaStream_t st);
+
+}  // namespace beams

@@ -159,6 +159,25 @@ __device__ __forceinline__ void light_origin(const ExactGeo& g, const float V[3]
   }
 }
 
+// Entry i of the cell tables: {lo, hi, hi - lo, RN(1 / (hi - lo))} of field
+// cell i (axes in order) or, past max_off[0], of map cell i - max_off[0].
+__device__ __forceinline__ float4 table_entry(const ExactGeo& g, int i) {
+  float lo, hi;
+  if (i < g.max_off[0]) {
+    const int d = (i >= g.ax_off[2]) ? 2 : (i >= g.ax_off[1] ? 1 : 0);
+    const int c = i - g.ax_off[d];
+    lo = coord(g, d, c);
+    hi = coord(g, d, c + 1);
+  } else {
+    const int d = (i >= g.max_off[2]) ? 2 : (i >= g.max_off[1] ? 1 : 0);
+    const int c = i - g.max_off[d];
+    lo = vtx_coord(g, d, c);
+    hi = vtx_coord(g, d, c + 1);
+  }
+  const float w = hi - lo;
+  return make_float4(lo, hi, w, 1.f / w);
+}
+
 // Correctly rounded division x / w given r = RN(1/w), after Markstein's
 // theorem (P. Markstein, "Computation of elementary functions on the IBM
 // RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990): with r the

@@ -1,0 +1,213 @@
+// k_batch.cu — many render requests in one persistent launch.
+//
+// The reference renders one camera per RenderCells call
+// (beams/rendering/MapperLightedVolume.cxx:114-193), each a map build followed
+// by a view march. Here a batch of requests (each its own volume, camera,
+// light and map size) is one grid of persistent blocks pulling work items from
+// a global queue: first every request's map-build items (256 vertices each),
+// then every view item (a tile of pixels). A view item of request r waits,
+// with a bounded wait, until all of r's map items have completed, so view work
+// of early requests overlaps the map builds of later ones and the grid never
+// drains between the two stages. Queue order guarantees progress: every item a
+// view item waits on was dequeued earlier by a running block that waits on
+// nothing.
+//
+// Per item a block keeps the request's geometry and cell tables in shared
+// memory (recomputed there when the request changes, so no table buffers or
+// table launches exist). Results equal the single-request kernels': the light
+// march per vertex is point_opacity (the K1 sample sequence) and the view march
+// is view_march_pixel. Compiled with -fmad=false like every kernel file.
+#include <cuda_runtime.h>
+
+#include "batch.h"
+#include "exact_device.cuh"
+#include "light_march.cuh"
+#include "view_march.cuh"
+
+namespace beams {
+
+namespace {
+
+constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 2 GHz: a view item's wait for its map
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ int find_request(const int* off, int n, int item) {
+  int lo = 0, hi = n - 1;  // largest k with off[k] <= item
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <bool SKIP>
+__global__ void __launch_bounds__(kBatchThreads, 3) k_batch(const ExactGeo* __restrict__ geos,
+                                                            const BatchDesc* __restrict__ descs,
+                                                            const BatchPlan* __restrict__ pl,
+                                                            const float4* __restrict__ tf,
+                                                            BatchQueue* __restrict__ q, Counters* __restrict__ cnt) {
+  __shared__ ExactGeo sg;
+  __shared__ BatchDesc sd;
+  __shared__ int s_item, s_req, s_phase, s_skip;
+  __shared__ unsigned s_sub;
+  extern __shared__ float4 s_dyn[];
+  const int tid = threadIdx.x, lane = tid & 31;
+  // shared TF (one colour map for the batch) and its normalised alpha
+  const int tf_n = geos[0].tf_n;
+  float4* s_tf = s_dyn;
+  float* s_a = (float*)(s_tf + tf_n);
+  float4* s_tab = (float4*)(s_a + ((tf_n + 3) & ~3));
+  const float max_alpha = geos[0].max_alpha;
+  for (int i = tid; i < tf_n; i += blockDim.x) {
+    const float4 c = tf[i];
+    s_tf[i] = c;
+    s_a[i] = (max_alpha > 0.f) ? c.w / max_alpha : 0.f;
+  }
+  if (tid == 0) s_req = -1;
+  __syncthreads();
+  const BatchPlan& plan = *pl;
+  unsigned lit = 0, hit = 0;
+  for (;;) {
+    if (tid == 0) {
+      s_item = (int)atomicAdd(&q->next, 1u);
+      s_sub = 0u;
+    }
+    __syncthreads();
+    const int item = s_item;
+    if (item >= plan.total) break;
+    const int seg = find_request(plan.seg_off, plan.nseg, item);
+    const int phase = (plan.seg_req[seg] >> 16) ? 2 : 1;
+    const int req = plan.seg_req[seg] & 0xffff;
+    const int li = item - plan.seg_off[seg];  // item index inside the request's phase
+    if (req != s_req || phase != s_phase) {
+      __syncthreads();  // every thread has read s_req / s_phase
+      const int* src = (const int*)(geos + req);
+      for (int i = tid; i < (int)(sizeof(ExactGeo) / 4); i += blockDim.x) ((int*)&sg)[i] = src[i];
+      if (tid < (int)(sizeof(BatchDesc) / 4)) ((int*)&sd)[tid] = ((const int*)(descs + req))[tid];
+      __syncthreads();
+      const int ntab = phase == 1 ? sg.max_off[0] : sg.ntab;
+      for (int i = tid; i < ntab; i += blockDim.x) s_tab[i] = table_entry(sg, i);
+      if (tid == 0) {
+        s_req = req;
+        s_phase = phase;
+      }
+      __syncthreads();
+    }
+    if (phase == 1) {
+      // a chunk of kBatchChunk vertex slots; warps take 32-slot tiles from the block's counter
+      const int bl = plan.brick_log2;
+      const int base = li * kBatchChunk;
+      for (;;) {
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(&s_sub, 1u);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= (unsigned)(kBatchChunk / 32)) break;
+        const int slot = base + (int)(t << 5) + lane;
+        int id = -1, x = 0, y = 0, z = 0;
+        if (bl) {
+          const int nbx = (sg.pd[0] + (1 << bl) - 1) >> bl, nby = (sg.pd[1] + (1 << bl) - 1) >> bl;
+          const int bi = slot >> (3 * bl), li = slot & ((1 << (3 * bl)) - 1), m = (1 << bl) - 1;
+          x = ((bi % nbx) << bl) + (li & m);
+          y = (((bi / nbx) % nby) << bl) + ((li >> bl) & m);
+          z = ((bi / (nbx * nby)) << bl) + (li >> (2 * bl));
+          if (x < sg.pd[0] && y < sg.pd[1] && z < sg.pd[2]) id = (z * sg.pd[1] + y) * sg.pd[0] + x;
+        } else if (slot < sd.nvert) {
+          id = slot;
+          x = id % sg.pd[0];
+          y = (id / sg.pd[0]) % sg.pd[1];
+          z = id / (sg.pd[0] * sg.pd[1]);
+        }
+        if (id >= 0) {
+          const float V[3] = {vtx_coord(sg, 0, x), vtx_coord(sg, 1, y), vtx_coord(sg, 2, z)};
+          float L[3];
+          light_origin(sg, V, L);
+          Accum<false> acc;
+          unsigned ns = 0;
+          march_vertex<float4, false, SKIP>(sg, sd.quads, s_tab + sg.ax_off[0], s_tab + sg.ax_off[1],
+                                            s_tab + sg.ax_off[2], s_a, nullptr, sd.occ, V, L,
+                                            [](const float*) { return 0.f; }, acc, ns);
+          acc.store(sd.map, id);
+        }
+      }
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) atomicAdd(&q->done1[req], 1u);
+    } else {
+      if (tid == 0) {
+        const unsigned need = (unsigned)plan.k1_items[req];
+        const long long t0 = clock64();
+        int skip = 0;
+        while (ld_acquire(&q->done1[req]) < need) {
+          if (clock64() - t0 > kWaitCycles) {
+            atomicOr(&q->error, 1u);
+            skip = 1;
+            break;
+          }
+          __nanosleep(200);
+        }
+        __threadfence();
+        s_skip = skip;
+      }
+      __syncthreads();
+      if (s_skip) continue;  // the host reports the timeout; this item's pixels stay unwritten
+      // a tile_w x tile_h tile; warps take 8x4 sub-tiles from the block's counter
+      const int tx0 = (li % sd.tiles_x) * plan.tile_w, ty0 = (li / sd.tiles_x) * plan.tile_h;
+      const int sx = plan.tile_w >> 3, nsub = sx * (plan.tile_h >> 2);
+      for (;;) {
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(&s_sub, 1u);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= (unsigned)nsub) break;
+        const int x = tx0 + (((int)t % sx) << 3) + (lane & 7), y = ty0 + (((int)t / sx) << 2) + (lane >> 3);
+        if (x < sg.width && y < sg.height) {
+          float4 color;
+          view_march_pixel<float4, true, float, NoRecord, SKIP>(sg, sd.quads, s_tab, s_tf, sd.map, x, y, color, lit,
+                                                                hit, nullptr, sd.occ);
+          sd.out[(size_t)y * sg.width + x] = color;
+        }
+      }
+      __syncthreads();  // every warp is done with this tile before s_sub is reset
+    }
+  }
+  warp_add(&cnt->lit_samples, lit);
+  warp_add(&cnt->rays_hit, hit);
+}
+
+}  // namespace
+
+cudaError_t batch_launch_config(int tf_n, size_t max_ntab, int total_items, size_t& smem, int& grid) {
+  smem = (size_t)tf_n * sizeof(float4) + (size_t)((tf_n + 3) & ~3) * sizeof(float) + max_ntab * sizeof(float4);
+  cudaError_t e = cudaFuncSetAttribute(k_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0, per_sm2 = 0, dev = 0, sms = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<false>, kBatchThreads, smem);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_batch<true>, kBatchThreads, smem);
+  if (e != cudaSuccess) return e;
+  per_sm = per_sm < per_sm2 ? per_sm : per_sm2;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  grid = sms * per_sm;
+  if (grid > total_items) grid = total_items;
+  if (grid < 1) grid = 1;
+  return cudaSuccess;
+}
+
+cudaError_t launch_batch(const ExactGeo* geos, const BatchDesc* descs, const BatchPlan* plan, int skip,
+                         const float4* tf, size_t smem, int grid, BatchQueue* q, Counters* cnt, cudaStream_t st) {
+  if (skip)
+    k_batch<true><<<grid, kBatchThreads, smem, st>>>(geos, descs, plan, tf, q, cnt);
+  else
+    k_batch<false><<<grid, kBatchThreads, smem, st>>>(geos, descs, plan, tf, q, cnt);
+  return cudaGetLastError();
+}
+
+}  // namespace beams

@@ -1,0 +1,170 @@
+// light_march.cuh — one light ray of the map build: the march of
+// TransmittanceMapGenerator::operator() (beams/rendering/TransmittanceMap.h:279-332)
+// from the light towards a map vertex, software-pipelined two samples deep.
+// Shared by K1 (k_exact.cu) and the batched kernel (k_batch.cu).
+// Compiled with -fmad=false (see exact_device.cuh).
+#pragma once
+#include <cuda_fp16.h>
+
+#include "exact_device.cuh"
+
+namespace beams {
+
+// Opacity accumulation of one light ray.
+// Exact form: o <- o + (1 - o) a (TransmittanceMap.h:329-330); o == 1 is a fixed point.
+// Precision form: optical depth tau += -ln(1 - a) in float with Kahan
+// compensation over the non-zero terms (the per-entry -ln(1 - a) comes from a
+// table), a = 1 cuts the ray, and the map stores the transmittance exp(-tau) as
+// binary16. In both forms a sample of alpha 0 leaves the state unchanged, which
+// is what lets the march skip empty macro-cells.
+template <bool PREC> struct Accum;
+template <> struct Accum<false> {
+  float o;
+  __device__ __forceinline__ void init(float o0) { o = o0; }
+  __device__ __forceinline__ bool add(const float* s_a, const float*, int idx) {
+    o = o + (1.f - o) * s_a[idx];
+    return o == 1.f;
+  }
+  __device__ __forceinline__ void store(void* map, int id) const { ((float*)map)[id] = o; }
+};
+template <> struct Accum<true> {
+  float sum, comp;
+  bool cut;
+  __device__ __forceinline__ void init(float) {
+    sum = 0.f;
+    comp = 0.f;
+    cut = false;
+  }
+  __device__ __forceinline__ bool add(const float*, const float* s_tau, int idx) {
+    const float ti = s_tau[idx];
+    if (ti == __int_as_float(0x7f800000)) {
+      cut = true;
+      return true;
+    }
+    if (ti == 0.f) return false;  // alpha 0 adds nothing (no compensation step either)
+    const float y = ti - comp;
+    const float t = sum + y;
+    comp = (t - sum) - y;
+    sum = t;
+    return sum >= 18.f;  // exp(-18) < 2^-25: the binary16 result is 0 from here on
+  }
+  __device__ __forceinline__ void store(void* map, int id) const {
+    const float tr = cut ? 0.f : (float)exp(-(double)sum);
+    ((__half*)map)[id] = __float2half_rn(tr);
+  }
+};
+
+// March from L towards vertex V. prefix(dir) gives the starting opacity (0,
+// or the cross-brick prefix of the multi-brick Phase 3). ns counts the samples
+// marched. With SKIP, occ is the macro-cell occupancy (see occupied()).
+template <typename QuadT, bool PREC, bool SKIP, typename Prefix>
+__device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __restrict__ quads, const float4* T0,
+                                             const float4* T1, const float4* T2, const float* s_a,
+                                             const float* s_tau, const unsigned char* __restrict__ occ,
+                                             const float V[3], const float L[3], Prefix prefix, Accum<PREC>& acc,
+                                             unsigned& ns) {
+  const int cm0 = g.n[0] - 2, cm1 = g.n[1] - 2, cm2 = g.n[2] - 2;
+  const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
+  const int n1 = g.tf_n - 1;
+  const float v[3] = {V[0] - L[0], V[1] - L[1], V[2] - L[2]};
+  const float rs = 1.f / sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  const float dir[3] = {v[0] * rs, v[1] * rs, v[2] * rs};
+  float tmin, tmax;
+  segment_aabb(g, L, V, tmin, tmax);
+  const float st[3] = {L[0] + tmin * dir[0], L[1] + tmin * dir[1], L[2] + tmin * dir[2]};
+  float s[3] = {st[0], st[1], st[2]};
+  const float len2 = (tmax - tmin) * (tmax - tmin);
+  const float sdx = g.step * dir[0], sdy = g.step * dir[1], sdz = g.step * dir[2];
+  // The sample positions do not depend on the opacity, so sample k+1 is
+  // located and its loads issued before sample k is composited (the loads of
+  // two samples are in flight per ray). The break conditions are evaluated
+  // in the reference's order for every sample; only o == 1 ends the march
+  // early, after which the prefetched sample is discarded.
+  // Empty macro-cells (occ == 0: every value there has TF alpha 0) are
+  // stepped over without a field fetch: such a sample leaves the state
+  // unchanged (Accum), so only its position update and break checks run. sk
+  // counts the samples skipped before the one returned; they are counted as
+  // marched once that sample is composited (or the ray ends on its own).
+  int b = g.light_budget;
+  auto gen = [&](float v8[8], float pc[3], unsigned& sk) -> bool {
+    sk = 0;
+    for (;;) {
+      if (b-- <= 0) return false;
+      const float q0 = s[0] - st[0], q1 = s[1] - st[1], q2 = s[2] - st[2];
+      if (!(q0 * q0 + q1 * q1 + q2 * q2 <= len2)) return false;
+      s[0] = s[0] + sdx;
+      s[1] = s[1] + sdy;
+      s[2] = s[2] + sdz;
+      if (!inside_vol(g, s)) return false;
+      if (SKIP && !occupied(g, occ, s)) {
+        ++sk;
+        continue;
+      }
+      float4 e0, e1, e2;
+      const int c0 = find_cell_bsearch_t(T0, cm0, g.org[0], g.invh[0], s[0], e0);
+      const int c1 = find_cell_bsearch_t(T1, cm1, g.org[1], g.invh[1], s[1], e1);
+      const int c2 = find_cell_bsearch_t(T2, cm2, g.org[2], g.invh[2], s[2], e2);
+      QuadLoad<QuadT>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qz, v8);
+      // pcoords = (p - min) / (max - min) (RectilinearMeshOracle.h:189-192)
+      pc[0] = div_rn_markstein(s[0] - e0.x, e0.z, e0.w);
+      pc[1] = div_rn_markstein(s[1] - e1.x, e1.z, e1.w);
+      pc[2] = div_rn_markstein(s[2] - e2.x, e2.z, e2.w);
+      return true;
+    }
+  };
+  acc.init(prefix(dir));
+  float va[8], pa[3], vb[8], pb[3];
+  unsigned ska, skb;
+  if constexpr (!SKIP) {
+    bool ok = gen(va, pa, ska);
+    while (ok) {
+      const bool okb = gen(vb, pb, skb);
+      bool done;
+      {
+        float scalar = hex_interp(va, pa[0], pa[1], pa[2]);
+        scalar = (scalar - g.min_scalar) * g.inv_delta;
+        done = acc.add(s_a, s_tau, tf_index_clamped(scalar * (float)n1, n1));
+        ++ns;
+      }
+      if (done || !okb) break;
+      ok = gen(va, pa, ska);
+      {
+        float scalar = hex_interp(vb, pb[0], pb[1], pb[2]);
+        scalar = (scalar - g.min_scalar) * g.inv_delta;
+        done = acc.add(s_a, s_tau, tf_index_clamped(scalar * (float)n1, n1));
+        ++ns;
+      }
+      if (done) break;
+    }
+    return;
+  }
+  bool ok = gen(va, pa, ska);
+  if (!ok) ns += ska;
+  while (ok) {
+    const bool okb = gen(vb, pb, skb);
+    bool done;
+    {
+      float scalar = hex_interp(va, pa[0], pa[1], pa[2]);
+      scalar = (scalar - g.min_scalar) * g.inv_delta;
+      done = acc.add(s_a, s_tau, tf_index_clamped(scalar * (float)n1, n1));
+      ns += 1 + ska;
+    }
+    // Stop when the accumulated value can no longer change (see Accum).
+    if (done) break;
+    if (!okb) {
+      ns += skb;
+      break;
+    }
+    ok = gen(va, pa, ska);
+    {
+      float scalar = hex_interp(vb, pb[0], pb[1], pb[2]);
+      scalar = (scalar - g.min_scalar) * g.inv_delta;
+      done = acc.add(s_a, s_tau, tf_index_clamped(scalar * (float)n1, n1));
+      ns += 1 + skb;
+    }
+    if (done) break;
+    if (!ok) ns += ska;
+  }
+}
+
+}  // namespace beams

@@ -14,7 +14,8 @@
 
 namespace beams {
 
-struct MlpState;  // learned form (mlp_api.cu)
+struct MlpState;    // learned form (mlp_api.cu)
+struct BatchState;  // batched form (batch_api.cu)
 
 struct Light {
   int kind = 0;  // 0 point, 1 directional
@@ -142,6 +143,7 @@ struct beams_renderer {
 
   // learned form: parameters, optimiser state, inference weights
   beams::MlpState* mlp = nullptr;
+  beams::BatchState* batch = nullptr;
 
   // image + counters + timing
   float4* d_rgba = nullptr;
@@ -170,6 +172,7 @@ struct beams_renderer {
 
 namespace beams {
 void mlp_release(beams_renderer* r);
+void batch_release(beams_renderer* r);
 beams_status fail(beams_renderer* r, beams_status s, const std::string& msg);
 beams_status cuda_fail(beams_renderer* r, cudaError_t e, const char* what);
 beams_status ensure_buffer(beams_renderer* r, void** buf, size_t* cap, size_t bytes, const char* what);
@@ -177,5 +180,6 @@ beams_status ensure_buffer(beams_renderer* r, void** buf, size_t* cap, size_t by
 
 inline beams_renderer::~beams_renderer() {
   beams::mlp_release(this);
+  beams::batch_release(this);
   release_buffers();
 }

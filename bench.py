@@ -264,7 +264,11 @@ def run_ours(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda") if args.config != 1 else None
 
     r.render(cam, out=out, timings=True)                  # builds the cell tables and quad field
-    tuning = r.autotune(cam)                              # launch choices only; results are identical
+    if args.no_autotune:  # the tuning the autotuner picks for this workload, fixed
+        r.set_tuning(light_brick=8, empty_skip=False, view_skip=False)
+        tuning = dict(r.get_tuning(), autotuned=False)
+    else:
+        tuning = r.autotune(cam)                          # launch choices only; results are identical
     _, t0 = r.render(cam, out=out, timings=True)          # counts for one frame (deterministic)
     lit_frame, light_frame = t0["lit_samples"], t0["light_samples"]
     launches_per_frame = t0["kernel_launches"]
@@ -777,6 +781,7 @@ def main():
     ap.add_argument("--crop", type=int, default=128)
     ap.add_argument("--crop-stride", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="fixed tuning (for launch lists under ncu)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work for cpu_baseline")
     args = ap.parse_args()

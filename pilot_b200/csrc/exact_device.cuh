@@ -178,6 +178,14 @@ __device__ __forceinline__ float4 table_entry(const ExactGeo& g, int i) {
   return make_float4(lo, hi, w, 1.f / w);
 }
 
+// (int)x for x in [0, 2^23), computed on the FMA pipe instead of the
+// conversion unit: 2^23 + x rounded toward zero has the integer part of x in
+// its mantissa (its exponent is fixed in [2^23, 2^24)). Callers clamp first, so
+// NaN has become 0 before it arrives here.
+__device__ __forceinline__ int trunc_small(float x) {
+  return __float_as_int(__fadd_rz(x, 8388608.f)) - 0x4B000000;
+}
+
 // Correctly rounded division x / w given r = RN(1/w), after Markstein's
 // theorem (P. Markstein, "Computation of elementary functions on the IBM
 // RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990): with r the
@@ -205,7 +213,7 @@ __device__ __forceinline__ float div_rn_markstein(float x, float w, float r) {
 // inside the volume val <= coord(cmax+1), so one test per side suffices.
 __device__ __forceinline__ int find_cell_bsearch_t(const float4* T, int cmax, float org, float invh,
                                                    float val, float4& e) {
-  int c = (int)fminf(fmaxf((val - org) * invh, 0.f), (float)cmax);
+  int c = trunc_small(fminf(fmaxf((val - org) * invh, 0.f), (float)cmax));
   e = T[c];
   if (val <= e.x || val > e.y) {
     while (c > 0 && val <= e.x) e = T[--c];
@@ -218,7 +226,7 @@ __device__ __forceinline__ int find_cell_bsearch_t(const float4* T, int cmax, fl
 // walks to the unique cell with coord(c) <= p < coord(c+1).
 __device__ __forceinline__ int find_cell_walk_t(const float4* T, int cmax, float org, float invh, float p,
                                                 float4& e) {
-  int c = (int)fminf(fmaxf((p - org) * invh, 0.f), (float)cmax);
+  int c = trunc_small(fminf(fmaxf((p - org) * invh, 0.f), (float)cmax));
   e = T[c];
   if (p < e.x || p >= e.y) {
     while (c > 0 && p < e.x) e = T[--c];
@@ -231,7 +239,7 @@ __device__ __forceinline__ int find_cell_walk_t(const float4* T, int cmax, float
 // [0, n1]; saturating, NaN -> 0. Clamping in float first gives the same index:
 // (-1, 0) truncates to 0 either way and [n1, n1+1) to n1.
 __device__ __forceinline__ int tf_index_clamped(float fi, int n1) {
-  return (int)fminf(fmaxf(fi, 0.f), (float)n1);
+  return trunc_small(fminf(fmaxf(fi, 0.f), (float)n1));
 }
 
 // Pinhole camera ray through pixel centre (x, y).
@@ -306,10 +314,10 @@ __device__ __forceinline__ float map_interp_t(const ExactGeo& g, const float4* M
   float pc[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    float t = (p[d] - g.morig[d]) * g.minv[d];
-    if (t < 0.f) t = 0.f;
-    if (t >= (float)(g.pd[d] - 1)) t = (float)(g.pd[d] - 2);
-    c[d] = (int)t;
+    // the reference clamps t to [0, pd-2] when t >= pd-1 and truncates; the
+    // cell is the same as truncating min(max(t, 0), pd-2)
+    const float t = (p[d] - g.morig[d]) * g.minv[d];
+    c[d] = trunc_small(fminf(fmaxf(t, 0.f), (float)(g.pd[d] - 2)));
     const float4 e = MT[g.max_off[d] + c[d]];
     pc[d] = div_rn_markstein(p[d] - e.x, e.z, e.w);
   }
@@ -371,7 +379,7 @@ __device__ __forceinline__ bool occupied(const ExactGeo& g, const unsigned char*
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const float f = fminf(fmaxf((p[d] - g.org[d]) * g.invh[d], 0.f), (float)(g.n[d] - 2));
-    m[d] = (int)f >> kMacroLog2;
+    m[d] = trunc_small(f) >> kMacroLog2;
   }
   return __ldg(occ + ((size_t)m[2] * g.occ_n[1] + m[1]) * g.occ_n[0] + m[0]) != 0;
 }

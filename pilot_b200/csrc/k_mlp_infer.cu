@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
         fs = (fs - g.min_scalar) * g.inv_delta;
         const float fi = fs * (float)n1;
         if (fi > -1.f && fi < (float)(n1 + 1)) {
-          const float4 tfc = s_tf[(int)fi];
+          const float4 tfc = s_tf[trunc_small(fmaxf(fi, 0.f))];  // (int)fi: fi in (-1, n1 + 1)
           const float sa = tfc.w * (1.f - color.w);
           buf[nb] = make_float4(tfc.x, tfc.y, tfc.z, sa);
           kp[0] = p[0];

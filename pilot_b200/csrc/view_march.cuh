@@ -114,7 +114,7 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT*
     fs = (fs - g.min_scalar) * g.inv_delta;
     const float fi = fs * (float)n1;
     if (fi > -1.f && fi < (float)(n1 + 1)) {
-      const float4 tfc = s_tf[(int)fi];
+      const float4 tfc = s_tf[trunc_small(fmaxf(fi, 0.f))];  // (int)fi: fi in (-1, n1 + 1)
       float sc0 = tfc.x, sc1 = tfc.y, sc2 = tfc.z;
       const float sa = tfc.w * (1.f - color.w);
       if (rec) (*rec)(p, tfc, sa);

@@ -1,0 +1,85 @@
+"""Fixed small cases for profiling one kernel at a time (ncu -k <kernel>).
+
+    python -m pilot_b200.profile_cases --case light_march      # K1, 512^3 noise, M = 256
+    python -m pilot_b200.profile_cases --case view_march       # K2, 512^3 noise, 1024^2, map cached
+    python -m pilot_b200.profile_cases --case mlp_view         # learned-form view march, 1024^2
+    python -m pilot_b200.profile_cases --case batch            # 16-request persistent batch
+    python -m pilot_b200.profile_cases --case precision_light  # precision-form K1, bf16 640^3
+
+Each case sets up its scene, runs the target kernel --reps times and exits 0;
+device memory stays within a few GB. The tuning is fixed (8^3 vertex bricks,
+skipping as stated per case) so that the launch sequence is the same every run.
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+
+
+def main(argv=None) -> int:
+    import numpy as np
+    import torch
+
+    from . import beams as B
+    from . import scenes
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", required=True,
+                    choices=["light_march", "view_march", "mlp_view", "batch", "precision_light"])
+    ap.add_argument("--reps", type=int, default=3)
+    a = ap.parse_args(argv)
+    torch.cuda.set_device(0)
+    if a.case in ("light_march", "view_march", "mlp_view"):
+        s = scenes.config1()
+        fd = s.field_device()
+        r = B.Renderer(0)
+        r.set_volume(fd, origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+        s.configure(r)
+        r.set_tuning(light_brick=8, empty_skip=False, view_skip=False)
+        cam = s.camera()
+        out = torch.empty((s.height, s.width, 4), device="cuda")
+        if a.case == "light_march":
+            for _ in range(a.reps):
+                r.build_shadow_map(timings=False)
+        elif a.case == "view_march":
+            r.build_shadow_map(timings=False)
+            r.set_reuse_shadow_map(True)
+            for _ in range(a.reps):
+                r.render(cam, out=out, timings=False)
+        else:
+            r.mlp_train(B.mlp_options(samples_log2=18, epochs=1, batch=16384))
+            r.set_form(B.FORM_MLP, B.mlp_options(knot=4, probe_fraction=0.0))
+            for _ in range(a.reps):
+                r.render(cam, out=out, timings=False)
+    elif a.case == "precision_light":
+        s = scenes.config2(n=640, image=1024, m=320)
+        fd = s.field_device()
+        r = B.Renderer(0)
+        r.set_volume(fd, origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+        s.configure(r)
+        r.set_form(B.FORM_PRECISION, B.BF16)
+        r.set_tuning(light_brick=8, empty_skip=True, view_skip=True)
+        for _ in range(a.reps):
+            r.build_shadow_map(timings=False)
+    else:  # batch
+        sys.path.insert(0, str(__import__("pathlib").Path(__file__).resolve().parent.parent))
+        import bench
+        vols = bench.batch_volumes()
+        rng = np.random.default_rng(11)
+        n = 16
+        sizes = [int(rng.choice(bench.BATCH_IMAGES)) for _ in range(n)]
+        outs = [torch.empty((w, w, 4), device="cuda") for w in sizes]
+        r = B.Renderer(0)
+        r.set_color_map(scenes.tf_table())
+        r.batch_set_volumes([(f, sc.origin, sc.spacing, sc.value_range) for sc, f in vols])
+        r.set_batch_options(tile_w=32, tile_h=32, light_brick=8, skip=True)
+        reqs = bench.batch_requests(B, vols, rng, n, outs)
+        for _ in range(a.reps):
+            r.render_batch(reqs, timings=False)
+    torch.cuda.synchronize()
+    print(f"profile case {a.case}: ok")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -345,6 +345,102 @@ beams_status beams_generate_noise(float* dev_out, const int n[3], const unsigned
                                   int octaves, float base_freq, float lacunarity, float gain,
                                   void* cuda_stream);
 
+/* Sphere / ellipsoid field of the reference's sources::Spheres
+ * (beams/sources/Spheres.cxx:19-96, :172-199): at each point of the grid
+ * origin + spacing * i (float32, the rectilinear coordinates it builds), the
+ * mean over the ellipsoids containing the point of lerp(min, max, d), d the
+ * ellipsoid distance sqrt(sum((c - p)^2 / r^2)) <= 1, else default_value; with
+ * a floor (floor_height >= 0 is not required: has_floor != 0) points below
+ * origin.y + floor_height take floor_value. ellipsoids: n x {cx, cy, cz, rx, ry,
+ * rz, min, max}. */
+beams_status beams_generate_spheres(float* dev_out, const int n[3], const double origin[3],
+                                    const double spacing[3], const float* ellipsoids, int n_ellipsoids,
+                                    float default_value, int has_floor, float floor_height, float floor_value,
+                                    void* cuda_stream);
+
+/* ---- configuration (stage TOML) -------------------------------------------- */
+/* The reference reads `<base-dir>/stage.toml` (pilot/staging/Stage.cxx:25-49):
+ * [dataset_providers.<name>] with `type` and `cell_dims` (an integer or
+ * [x, y, z], SubdividedSpheresDescriptor.cxx:22-44); its render knobs lived in
+ * the (now commented) JSON presets of beams/Config.cxx:140-247. This reader
+ * takes that file plus tables named after those preset keys:
+ *   [render]            width, height, sample_distance, termination_alpha,
+ *                       form = "exact" | "precision" | "mlp", field_dtype = "bf16" | "f16",
+ *                       composite_background, background = [r, g, b, a]
+ *   [shadow_map]        enabled, size = N | [x, y, z] | size_ratio = f, num_steps
+ *   [camera]            azimuth, elevation, fov_y (an orbit around the bounds), or
+ *                       position / look_at / up
+ *   [[light]]           type = "point" | "directional", position, color, intensity
+ *   [transfer_function] preset = "cool to warm" | "ramp", points, alphas, range, size
+ *   [form]              knot, probe_fraction, fallback_tol, samples_log2, lights
+ * Providers: "subdivided_spheres" (the reference's scene: one sphere of radius
+ * 0.45 at the centre, value 1, default 0.1, SubdividedSpheresScene.cxx),
+ * "spheres" (that scene's centre sphere, radius 0.1, and floor), "blobs" and
+ * "noise" (seeded, `seed`). Parsed by a TOML-subset reader (tables, arrays of
+ * tables, strings, numbers, booleans, arrays; comments); unknown keys are
+ * errors. No reference counterpart for the reader itself (the reference uses
+ * toml++, which is absent here). */
+#define BEAMS_MAX_CONFIG_LIGHTS 8
+#define BEAMS_MAX_TF_POINTS 64
+typedef struct beams_config_light {
+  int kind;                 /* 0 point, 1 directional */
+  double position[3];       /* point: position; directional: travel direction */
+  float color[3];
+  float intensity;
+} beams_config_light;
+
+typedef struct beams_scene_desc {
+  char provider_name[64];
+  char provider_type[32];
+  int cell_dims[3];         /* the field has cell_dims + 1 points per axis on [0,1]^3 */
+  unsigned seed;
+  int octaves;
+  float base_freq;
+  int width, height;
+  float sample_distance;
+  float termination_alpha;
+  int form;
+  int field_dtype;
+  int composite_background;
+  float background[4];
+  int shadow_enabled;
+  int shadow_size[3];       /* 0: from shadow_size_ratio x cell_dims (OpacityMapOptions::CalculateSize) */
+  float shadow_size_ratio;
+  float light_steps;        /* num_steps */
+  int camera_explicit;
+  float azimuth, elevation, fov_y_deg;
+  double position[3], look_at[3], up[3];
+  int n_lights;
+  beams_config_light lights[BEAMS_MAX_CONFIG_LIGHTS];
+  char tf_preset[32];
+  int tf_points;
+  double tf_x[BEAMS_MAX_TF_POINTS];
+  float tf_alpha[BEAMS_MAX_TF_POINTS];
+  float tf_range[2];
+  int tf_size;
+  int mlp_knot;
+  float mlp_probe_fraction, mlp_fallback_tol;
+  int mlp_samples_log2, mlp_lights;
+} beams_scene_desc;
+
+/* Parses TOML text / a TOML file into *out (defaults for absent keys). On a
+ * syntax or schema error returns BEAMS_ERR_CONFIG and writes "line N: ..." to err. */
+beams_status beams_parse_config_toml(const char* text, beams_scene_desc* out, char* err, int errlen);
+beams_status beams_load_config_toml(const char* path, beams_scene_desc* out, char* err, int errlen);
+/* Scene::Ready + SceneFactory for a parsed description: generates the dataset
+ * on the device (owned by the renderer), sets the colour map (preset RGB,
+ * piecewise-linear alpha through the points over `range`), map size, light steps,
+ * the first light (the reference uses Locations[0] only), sample distance,
+ * termination alpha, background and form (the learned form trains here when no
+ * network is loaded), and returns the camera. */
+beams_status beams_apply_scene(beams_renderer* r, const beams_scene_desc* d, beams_camera* camera_out);
+/* The colour table beams_apply_scene sets (d->tf_size RGBA entries into rgba; n = tf_size). */
+beams_status beams_scene_color_table(const beams_scene_desc* d, float* rgba, int n);
+/* The light orbit of the reference's Beams::Run (Beams.cxx:239-288): frame k
+ * puts a point light at (0.5, 0.5, 0.5) + 0.5 (cos k*5deg, sin k*5deg, 0),
+ * keeping the first configured light's colour and intensity. */
+beams_status beams_orbit_light(beams_renderer* r, const beams_scene_desc* d, int frame);
+
 #ifdef __cplusplus
 }
 #endif

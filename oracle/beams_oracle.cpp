@@ -1022,6 +1022,35 @@ int oracle_ray_setup_f32(const oracle_scene* s, int x, int y, float out[8]) {
   return 0;
 }
 
+// SphereFieldGenerator::operator() (beams/sources/Spheres.cxx:36-91), float32,
+// with vtkm::Lerp(a, b, t) taken as a + t * (b - a) (VTK-m not vendored here).
+int oracle_generate_spheres(float* out, int nx, int ny, int nz, const float origin[3], const float spacing[3],
+                            const float* e, int ne, float def, int has_floor, float floor_y, float floor_v) {
+  if (!out || nx < 1 || ny < 1 || nz < 1 || ne < 0 || (ne > 0 && !e)) return 1;
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const float p[3] = {origin[0] + spacing[0] * (float)x, origin[1] + spacing[1] * (float)y,
+                            origin[2] + spacing[2] * (float)z};
+        float sum = 0.f, cnt = 0.f;
+        for (int k = 0; k < ne; ++k) {
+          const float* s = e + 8 * k;
+          const float d0 = s[0] - p[0], d1 = s[1] - p[1], d2 = s[2] - p[2];
+          float a = ((d0 * d0) / (s[3] * s[3])) + ((d1 * d1) / (s[4] * s[4]));
+          a = a + ((d2 * d2) / (s[5] * s[5]));
+          a = std::sqrt(a);
+          if (a <= 1.f) {
+            sum = sum + (s[6] + a * (s[7] - s[6]));
+            cnt = cnt + 1.f;
+          }
+        }
+        float v = cnt > 0.f ? sum / cnt : def;
+        if (has_floor && p[1] < floor_y) v = floor_v;
+        out[((size_t)z * ny + y) * nx + x] = v;
+      }
+  return 0;
+}
+
 int oracle_composite_f32(const float* images, int nimages, int npix, const int* order, float* out) {
   if (!images || !order || !out || nimages < 1 || npix < 0) return 1;
   const float* first = images + (int64_t)order[0] * npix * 4;

@@ -98,6 +98,11 @@ int oracle_render_bricks_f64(const oracle_scene* scenes, int nbricks, double* ma
 int oracle_generate_noise(float* out, int nx, int ny, int nz, const unsigned char* perm, int octaves,
                           float f0, float lac, float gain, int threads);
 
+/* The sphere / ellipsoid field of sources::Spheres (beams/sources/Spheres.cxx:36-91)
+ * on the float32 grid origin + spacing * i: e = n x {cx, cy, cz, rx, ry, rz, min, max}. */
+int oracle_generate_spheres(float* out, int nx, int ny, int nz, const float origin[3], const float spacing[3],
+                            const float* e, int ne, float def, int has_floor, float floor_y, float floor_v);
+
 /* Sort-last "over" of B premultiplied RGBA images in the given order
  * (MapperLightedVolume.cxx:284-297). */
 int oracle_composite_f32(const float* images, int nimages, int npix, const int* order,

@@ -50,6 +50,8 @@ def lib():
             "oracle_generate_noise": [P, C.c_int, C.c_int, C.c_int, P, C.c_int, C.c_float, C.c_float,
                                       C.c_float, C.c_int],
             "oracle_render_bricks_f32": [P, C.c_int, P, P, P, P, C.c_int, u64p],
+            "oracle_generate_spheres": [P, C.c_int, C.c_int, C.c_int, P, P, P, C.c_int, C.c_float, C.c_int,
+                                        C.c_float, C.c_float],
             "oracle_record_samples_f32": [S, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int64, P],
             "oracle_render_bricks_f64": [P, C.c_int, P, P, P, P, C.c_int, u64p],
         }.items():
@@ -198,6 +200,21 @@ def noise_field(dims, perm, octaves=4, base_freq=4.0, lacunarity=2.0, gain=0.5, 
     perm = np.ascontiguousarray(perm, np.uint8)
     if lib().oracle_generate_noise(_p(out), nx, ny, nz, _p(perm), octaves, base_freq, lacunarity, gain, threads):
         raise RuntimeError("oracle noise generator rejected the arguments")
+    return out
+
+
+def spheres_field(dims, origin, spacing, ellipsoids, default=0.1, floor=None):
+    """sources::Spheres field (float32, (z, y, x)); floor = (height, value) or None."""
+    nx, ny, nz = dims
+    out = np.zeros((nz, ny, nx), np.float32)
+    e = np.ascontiguousarray(ellipsoids, np.float32).reshape(-1, 8)
+    org = np.asarray(origin, np.float32)
+    sp = np.asarray(spacing, np.float32)
+    fy, fv = (0.0, 0.0) if floor is None else floor
+    floor_y = float(np.float32(org[1]) + np.float32(fy))
+    if lib().oracle_generate_spheres(_p(out), nx, ny, nz, _p(org), _p(sp), _p(e), e.shape[0], float(default),
+                                     int(floor is not None), floor_y, float(fv)):
+        raise RuntimeError("oracle spheres generator rejected the arguments")
     return out
 
 

@@ -82,6 +82,53 @@ class BatchOptions(C.Structure):
                 ("no_skip", C.c_int), ("reserved", C.c_int)]
 
 
+class ConfigLight(C.Structure):
+    _fields_ = [("kind", C.c_int), ("position", C.c_double * 3), ("color", C.c_float * 3),
+                ("intensity", C.c_float)]
+
+
+class SceneDesc(C.Structure):
+    """beams_scene_desc: a parsed stage TOML (see beams_parse_config_toml)."""
+    _fields_ = [("provider_name", C.c_char * 64), ("provider_type", C.c_char * 32), ("cell_dims", C.c_int * 3),
+                ("seed", C.c_uint), ("octaves", C.c_int), ("base_freq", C.c_float),
+                ("width", C.c_int), ("height", C.c_int), ("sample_distance", C.c_float),
+                ("termination_alpha", C.c_float), ("form", C.c_int), ("field_dtype", C.c_int),
+                ("composite_background", C.c_int), ("background", C.c_float * 4),
+                ("shadow_enabled", C.c_int), ("shadow_size", C.c_int * 3), ("shadow_size_ratio", C.c_float),
+                ("light_steps", C.c_float), ("camera_explicit", C.c_int), ("azimuth", C.c_float),
+                ("elevation", C.c_float), ("fov_y_deg", C.c_float), ("position", C.c_double * 3),
+                ("look_at", C.c_double * 3), ("up", C.c_double * 3), ("n_lights", C.c_int),
+                ("lights", ConfigLight * 8), ("tf_preset", C.c_char * 32), ("tf_points", C.c_int),
+                ("tf_x", C.c_double * 64), ("tf_alpha", C.c_float * 64), ("tf_range", C.c_float * 2),
+                ("tf_size", C.c_int), ("mlp_knot", C.c_int), ("mlp_probe_fraction", C.c_float),
+                ("mlp_fallback_tol", C.c_float), ("mlp_samples_log2", C.c_int), ("mlp_lights", C.c_int)]
+
+
+def parse_config(text: str) -> SceneDesc:
+    """Parses stage TOML text; raises BeamsError with "line N: ..." on errors."""
+    d, err = SceneDesc(), C.create_string_buffer(512)
+    st = lib().beams_parse_config_toml(text.encode(), C.byref(d), err, 512)
+    if st != BEAMS_OK:
+        raise BeamsError(st, err.value.decode())
+    return d
+
+
+def load_config(path) -> SceneDesc:
+    d, err = SceneDesc(), C.create_string_buffer(512)
+    st = lib().beams_load_config_toml(str(path).encode(), C.byref(d), err, 512)
+    if st != BEAMS_OK:
+        raise BeamsError(st, err.value.decode())
+    return d
+
+
+def scene_color_table(d: SceneDesc) -> np.ndarray:
+    out = np.zeros((d.tf_size, 4), np.float32)
+    st = lib().beams_scene_color_table(C.byref(d), _ptr(out), d.tf_size)
+    if st != BEAMS_OK:
+        raise BeamsError(st, "scene_color_table")
+    return out
+
+
 class Timings(C.Structure):
     _fields_ = [("map_build_ms", C.c_float), ("view_march_ms", C.c_float), ("composite_ms", C.c_float),
                 ("total_ms", C.c_float), ("light_samples", C.c_ulonglong), ("lit_samples", C.c_ulonglong),
@@ -143,6 +190,12 @@ def lib():
         "beams_set_batch_options": ([P, C.POINTER(BatchOptions)], C.c_int),
         "beams_render_batch": ([P, P, C.c_int, C.POINTER(Timings)], C.c_int),
         "beams_batch_autotune": ([P, P, C.c_int, C.POINTER(BatchOptions), C.POINTER(C.c_float)], C.c_int),
+        "beams_parse_config_toml": ([P, P, P, C.c_int], C.c_int),
+        "beams_load_config_toml": ([P, P, P, C.c_int], C.c_int),
+        "beams_apply_scene": ([P, P, C.POINTER(Camera)], C.c_int),
+        "beams_orbit_light": ([P, P, C.c_int], C.c_int),
+        "beams_scene_color_table": ([P, P, C.c_int], C.c_int),
+        "beams_generate_spheres": ([P, P, P, P, P, C.c_int, C.c_float, C.c_int, C.c_float, C.c_float, P], C.c_int),
         "beams_autotune": ([P, C.POINTER(Camera), C.POINTER(Tuning), C.POINTER(C.c_float), C.POINTER(C.c_float)],
                            C.c_int),
         "beams_mlp_save": ([P, C.c_char_p], C.c_int),
@@ -247,6 +300,17 @@ class Renderer:
         v = Volume(ptr, dtype, (C.c_int * 3)(*dims), _d3(origin), _d3(spacing),
                    (C.c_double * 2)(*value_range), assoc, on_device)
         self._check(self._L.beams_set_volume(self._h, C.byref(v)))
+
+    # -- configuration ----------------------------------------------------------
+    def apply_scene(self, desc: SceneDesc) -> Camera:
+        """Generates the described dataset on the device and configures the renderer; returns the camera."""
+        cam = Camera()
+        self._check(self._L.beams_apply_scene(self._h, C.byref(desc), C.byref(cam)))
+        self._scene_desc = desc
+        return cam
+
+    def orbit_light(self, desc: SceneDesc, frame: int):
+        self._check(self._L.beams_orbit_light(self._h, C.byref(desc), int(frame)))
 
     # -- batched form -----------------------------------------------------------
     def batch_set_volumes(self, volumes):

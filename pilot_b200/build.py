@@ -63,6 +63,13 @@ def build(verbose: bool = False, force: bool = False, extra_flags=None) -> Path:
         objs = list(ex.map(compile_one, sources))
     if force or not _newer(LIB, objs):
         _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs], verbose)
+    # the driver executable (host C++ over the C ABI)
+    drv = PKG / "driver" / "beams_run.cpp"
+    exe = PKG / "bin" / "beams_run"
+    if drv.exists() and (force or not _newer(exe, [drv, LIB, *headers])):
+        exe.parent.mkdir(exist_ok=True)
+        _run([os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-I", PKG.parent / "include", drv, "-o", exe,
+              "-L", LIB.parent, "-lbeams_b200", "-Wl,-rpath,$ORIGIN/../lib"], verbose)
     return LIB
 
 

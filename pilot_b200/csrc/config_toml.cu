@@ -475,7 +475,7 @@ struct Schema {
       } else if (t == "form") {
         if (k == "knot") {
           d.mlp_knot = (int)integer();
-          if (d.mlp_knot < 1 || d.mlp_knot > 8) bad("'knot' must be in [1, 8]");
+          if (d.mlp_knot < 1 || d.mlp_knot > 32) bad("'knot' must be in [1, 32]");
         } else if (k == "probe_fraction") {
           d.mlp_probe_fraction = (float)num();
         } else if (k == "fallback_tol") {

@@ -182,7 +182,7 @@ __device__ __forceinline__ float mlp_eval_warp(const Encoding& enc, const float 
 
 using namespace mlp;
 
-constexpr int kKnotMax = 8;
+constexpr int kKnotMax = 32;  // lit samples between two network evaluations, at most
 
 __device__ __forceinline__ int next_warp_tile_mlp(unsigned* counter) {
   unsigned t = 0;
@@ -198,13 +198,17 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
                                                            const uint2* __restrict__ Wp,
                                                            const float* __restrict__ aux, Encoding enc,
                                                            float lf0, float lf1, float lf2, int knot,
-                                                           float4* __restrict__ out, Counters* __restrict__ cnt) {
+                                                           float4* __restrict__ out, Counters* __restrict__ cnt,
+                                                           MlpProbe probe) {
   extern __shared__ float4 s_dyn[];
   const int nfield = g.max_off[0];
   float4* s_tab = s_dyn;
   float4* s_tf = s_dyn + nfield;
   uint2* sW = reinterpret_cast<uint2*>(s_tf + g.tf_n);
   float* sAux = reinterpret_cast<float*>(sW + kPacked);
+  // per warp, the TF indices of the round's pending lit samples: [warp][j][lane]
+  unsigned short* s_idx = reinterpret_cast<unsigned short*>(sAux + ((kAux + 3) & ~3)) +
+                          (threadIdx.x >> 5) * (kKnotMax * 32) + (threadIdx.x & 31);
   for (int i = threadIdx.x; i < nfield; i += blockDim.x) s_tab[i] = tab[i];
   for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) s_tf[i] = tf[i];
   for (int i = threadIdx.x; i < kPacked; i += blockDim.x) sW[i] = Wp[i];
@@ -219,6 +223,11 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
   for (int tile = next_warp_tile_mlp(&cnt->tiles_view); tile < ntiles; tile = next_warp_tile_mlp(&cnt->tiles_view)) {
     const int lane = threadIdx.x & 31;
     const int x = (tile % tiles_x) * 8 + (lane & 7), y = (tile / tiles_x) * 4 + (lane >> 3);
+    // a probe pixel records its compositing samples for the exact-march check
+    const bool is_probe = probe.P > 0 && x < g.width && y < g.height && x % probe.P == probe.h &&
+                          y % probe.P == probe.h && x / probe.P < probe.nqx && y / probe.P < probe.nqy;
+    float4* prec = is_probe ? probe.rec + (size_t)((y / probe.P) * probe.nqx + x / probe.P) * probe.cap * 2 : nullptr;
+    int pn = 0;
     float4 color = make_float4(0.f, 0.f, 0.f, 0.f);
     float o[3] = {0.f, 0.f, 0.f}, d[3] = {0.f, 0.f, 1.f}, minD = 0.f, maxD = -1.f;
     bool done = true;
@@ -245,7 +254,11 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
     bool have_prev = false;
     // march state lives across rounds; each round gathers up to `need` lit samples
     while (__any_sync(0xffffffffu, !done)) {
-      float4 buf[kKnotMax];
+      // The round's lit samples are kept as their TF indices only (16 bits in
+      // shared memory); compositing replays the alpha recurrence from the
+      // round's starting alpha, which gives back each sample's premultiplied
+      // alpha bit for bit.
+      const float cw0 = color.w;
       int nb = 0;
       float kp[3] = {p[0], p[1], p[2]};
       const int need = have_prev ? knot : 1;
@@ -297,9 +310,17 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
         fs = (fs - g.min_scalar) * g.inv_delta;
         const float fi = fs * (float)n1;
         if (fi > -1.f && fi < (float)(n1 + 1)) {
-          const float4 tfc = s_tf[trunc_small(fmaxf(fi, 0.f))];  // (int)fi: fi in (-1, n1 + 1)
+          const int ti = trunc_small(fmaxf(fi, 0.f));  // (int)fi: fi in (-1, n1 + 1)
+          const float4 tfc = s_tf[ti];
           const float sa = tfc.w * (1.f - color.w);
-          buf[nb] = make_float4(tfc.x, tfc.y, tfc.z, sa);
+          s_idx[nb * 32] = (unsigned short)ti;
+          if (is_probe && sa > 0.f) {
+            if (pn < probe.cap) {
+              prec[2 * pn] = make_float4(p[0], p[1], p[2], 1.f);
+              prec[2 * pn + 1] = make_float4(tfc.x, tfc.y, tfc.z, sa);
+            }
+            ++pn;
+          }
           kp[0] = p[0];
           kp[1] = p[1];
           kp[2] = p[2];
@@ -320,23 +341,25 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
       if (nb > 0) {
         ++evals;
         const float inv_nb = 1.f / (float)nb;
-#pragma unroll
-        for (int j = 0; j < kKnotMax; ++j) {
-          if (j >= nb) break;
+        float cw = cw0;
+        for (int j = 0; j < nb; ++j) {
           const float T = have_prev ? Tprev + (Tk - Tprev) * ((float)(j + 1) * inv_nb) : Tk;
-          const float4 b = buf[j];
+          const float4 b = s_tf[s_idx[j * 32]];
+          const float sa = b.w * (1.f - cw);
+          cw = sa + cw;
           const float sc0 = clamp01(b.x * (T * g.light_color[0]));
           const float sc1 = clamp01(b.y * (T * g.light_color[1]));
           const float sc2 = clamp01(b.z * (T * g.light_color[2]));
-          color.x = color.x + sc0 * b.w;
-          color.y = color.y + sc1 * b.w;
-          color.z = color.z + sc2 * b.w;
+          color.x = color.x + sc0 * sa;
+          color.y = color.y + sc1 * sa;
+          color.z = color.z + sc2 * sa;
         }
         Tprev = Tk;
         have_prev = true;
       }
     }
     if (x < g.width && y < g.height) out[(size_t)y * g.width + x] = color;
+    if (is_probe) probe.count[(y / probe.P) * probe.nqx + x / probe.P] = pn;
   }
   warp_add(&cnt->lit_samples, lit);
   warp_add(&cnt->rays_hit, hit);
@@ -352,10 +375,11 @@ size_t mlp_packed_bytes() { return (size_t)kPacked * sizeof(uint2) + (size_t)kAu
 
 cudaError_t launch_view_march_mlp(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                   const uint2* W, const float* aux, const Encoding& enc, const float lf[3], int knot,
-                                  float4* out, Counters* cnt, cudaStream_t st) {
+                                  float4* out, Counters* cnt, const MlpProbe& probe, cudaStream_t st) {
   if (knot < 1 || knot > kKnotMax) return cudaErrorInvalidValue;
   const size_t smem = (size_t)g.max_off[0] * sizeof(float4) + (size_t)g.tf_n * sizeof(float4) +
-                      (size_t)kPacked * sizeof(uint2) + (size_t)kAux * sizeof(float);
+                      (size_t)kPacked * sizeof(uint2) + (size_t)((kAux + 3) & ~3) * sizeof(float) +
+                      (size_t)8 * kKnotMax * 32 * sizeof(unsigned short);
   cudaError_t e = cudaFuncSetAttribute(k_view_march_mlp<float4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -370,7 +394,7 @@ cudaError_t launch_view_march_mlp(const ExactGeo& g, const float4* quads, const 
   const int need = (ntiles + 7) / 8;
   if (grid > need) grid = need;
   k_view_march_mlp<float4><<<grid, 256, smem, st>>>(g, quads, tab, tf, W, aux, enc, lf[0], lf[1], lf[2], knot, out,
-                                                    cnt);
+                                                    cnt, probe);
   return cudaGetLastError();
 }
 

@@ -177,7 +177,8 @@ ProbeLayout probe_layout(int width, int height, float fraction) {
 
 cudaError_t launch_mlp_probe(const ExactGeo& g, const ProbeLayout& L, const float4* quads, const float4* tab,
                              const float4* tf, const float4* img, float tol, float4* rec, int* count, unsigned* flags,
-                             unsigned* flist, unsigned* fcount, float* probe_err, Counters* cnt, cudaStream_t st) {
+                             unsigned* flist, unsigned* fcount, float* probe_err, Counters* cnt, cudaStream_t st,
+                             bool recorded) {
   if (L.nprobe < 0 || L.cap < 1) return cudaErrorInvalidValue;
   const ProbeGrid pg{L.stride, L.offset, L.nqx, L.nqy};
   cudaError_t e;
@@ -185,7 +186,8 @@ cudaError_t launch_mlp_probe(const ExactGeo& g, const ProbeLayout& L, const floa
     const size_t smem1 = ((size_t)g.ntab + (size_t)g.tf_n) * sizeof(float4);
     e = cudaFuncSetAttribute(k_probe_record, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1);
     if (e != cudaSuccess) return e;
-    k_probe_record<<<grid_for(L.nprobe, 64, 148 * 8), 64, smem1, st>>>(g, quads, tab, tf, pg, L.cap, rec, count);
+    if (!recorded)
+      k_probe_record<<<grid_for(L.nprobe, 64, 148 * 8), 64, smem1, st>>>(g, quads, tab, tf, pg, L.cap, rec, count);
     const size_t smem2 = (size_t)g.max_off[0] * sizeof(float4) + (size_t)g.tf_n * sizeof(float);
     e = cudaFuncSetAttribute(k_probe_transmittance, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
     if (e != cudaSuccess) return e;

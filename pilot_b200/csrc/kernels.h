@@ -35,10 +35,19 @@ constexpr int kProbeCap = 512;  // compositing samples recorded per probe pixel
 struct ProbeLayout {
   int stride, offset, nqx, nqy, nprobe, ntiles, cap;
 };
+// What the network's view march records for the probe pixels (P = 0: none):
+// per probe its compositing samples {x, y, z, 1}, {r, g, b, sa} and their count.
+struct MlpProbe {
+  int P, h, nqx, nqy, cap;
+  float4* rec;
+  int* count;
+};
 ProbeLayout probe_layout(int width, int height, float fraction);
+// recorded: the network's view march already recorded the probe samples (no probe march).
 cudaError_t launch_mlp_probe(const ExactGeo& g, const ProbeLayout& L, const float4* quads, const float4* tab,
                              const float4* tf, const float4* img, float tol, float4* rec, int* count, unsigned* flags,
-                             unsigned* flist, unsigned* fcount, float* probe_err, Counters* cnt, cudaStream_t st);
+                             unsigned* flist, unsigned* fcount, float* probe_err, Counters* cnt, cudaStream_t st,
+                             bool recorded = false);
 cudaError_t launch_pack_weights(const float* P, uint2* W, float* aux, cudaStream_t st);
 cudaError_t launch_composite(const float4* imgs, int nb, size_t npix, const int* order, float4* out,
                              cudaStream_t st);

@@ -137,7 +137,7 @@ static void init_params(std::vector<float>& h, unsigned seed) {
 
 cudaError_t launch_view_march_mlp(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                   const uint2* W, const float* aux, const Encoding& enc, const float lf[3], int knot,
-                                  float4* out, Counters* cnt, cudaStream_t st);
+                                  float4* out, Counters* cnt, const MlpProbe& probe, cudaStream_t st);
 
 bool mlp_ready(const beams_renderer* r) { return r->mlp && r->mlp->ready; }
 
@@ -149,7 +149,7 @@ beams_status mlp_set_render_options(beams_renderer* r, const beams_mlp_options* 
   d.probe_fraction = 0.01f;
   d.knot = 4;
   if (o) {
-    if (o->knot < 1 || o->knot > 8) return fail(r, BEAMS_ERR_INVALID_ARG, "mlp form: knot must be in [1, 8]");
+    if (o->knot < 1 || o->knot > 32) return fail(r, BEAMS_ERR_INVALID_ARG, "mlp form: knot must be in [1, 32]");
     if (!(o->probe_fraction >= 0.f && o->probe_fraction <= 1.f) || !(o->fallback_tol >= 0.f))
       return fail(r, BEAMS_ERR_INVALID_ARG, "mlp form: bad probe fraction or tolerance");
     d.knot = o->knot;
@@ -160,14 +160,21 @@ beams_status mlp_set_render_options(beams_renderer* r, const beams_mlp_options* 
   return BEAMS_OK;
 }
 
-// Probe pixels against the exact light march, then the exact map path over the
-// tiles that failed: K1 gated on a non-empty list, K2 over the listed tiles.
-// Nothing here waits on the host.
-static beams_status mlp_probe_and_fallback(beams_renderer* r, const ExactGeo& g, float4* out, int& launches) {
+struct ProbeBuffers {
+  ProbeLayout L{};
+  float4* rec = nullptr;
+  int* count = nullptr;
+  unsigned* flags = nullptr;
+  unsigned* fcount = nullptr;
+  unsigned* flist = nullptr;
+};
+
+// Lays out this frame's probe buffers (none when the probe fraction is 0).
+static beams_status probe_buffers(beams_renderer* r, const ExactGeo& g, ProbeBuffers& pb) {
   MlpState* st = r->mlp;
-  const beams_mlp_options& o = st->render_opts;
-  const ProbeLayout L = probe_layout(g.width, g.height, o.probe_fraction);
-  if (L.stride == 0) return BEAMS_OK;  // probe fraction 0: the network's image stands
+  pb.L = probe_layout(g.width, g.height, st->render_opts.probe_fraction);
+  const ProbeLayout& L = pb.L;
+  if (L.stride == 0) return BEAMS_OK;
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t b_rec = al((size_t)L.nprobe * L.cap * 2 * sizeof(float4));
   const size_t b_cnt = al((size_t)L.nprobe * sizeof(int) + 4);
@@ -177,11 +184,11 @@ static beams_status mlp_probe_and_fallback(beams_renderer* r, const ExactGeo& g,
                                  "allocating the probe buffers");
   if (s != BEAMS_OK) return s;
   char* base = (char*)st->probe_mem;
-  float4* rec = (float4*)base;
-  int* count = (int*)(base + b_rec);
-  unsigned* flags = (unsigned*)(base + b_rec + b_cnt);
-  unsigned* fcount = flags + L.ntiles;
-  unsigned* flist = (unsigned*)(base + b_rec + b_cnt + b_flags);
+  pb.rec = (float4*)base;
+  pb.count = (int*)(base + b_rec);
+  pb.flags = (unsigned*)(base + b_rec + b_cnt);
+  pb.fcount = pb.flags + L.ntiles;
+  pb.flist = (unsigned*)(base + b_rec + b_cnt + b_flags);
   if (st->probe_err_n < L.nprobe) {
     if (st->probe_err) cudaFree(st->probe_err);
     st->probe_err = nullptr;
@@ -190,22 +197,34 @@ static beams_status mlp_probe_and_fallback(beams_renderer* r, const ExactGeo& g,
     if (e != cudaSuccess) return cuda_fail(r, e, "allocating probe errors");
     st->probe_err_n = std::max(L.nprobe, 1);
   }
-  cudaError_t e = cudaMemsetAsync(flags, 0, ((size_t)L.ntiles + 1) * sizeof(unsigned), r->stream);
+  return BEAMS_OK;
+}
+
+// Probe pixels against the exact light march, then the exact map path over the
+// tiles that failed: K1 gated on a non-empty list, K2 over the listed tiles.
+// The network's view march has already recorded the probe pixels' samples.
+// Nothing here waits on the host.
+static beams_status mlp_probe_and_fallback(beams_renderer* r, const ExactGeo& g, const ProbeBuffers& pb, float4* out,
+                                           int& launches) {
+  MlpState* st = r->mlp;
+  const ProbeLayout& L = pb.L;
+  if (L.stride == 0) return BEAMS_OK;  // probe fraction 0: the network's image stands
+  cudaError_t e = cudaMemsetAsync(pb.flags, 0, ((size_t)L.ntiles + 1) * sizeof(unsigned), r->stream);
   if (e == cudaSuccess)
-    e = launch_mlp_probe(g, L, (const float4*)r->d_quads, r->d_tab, r->d_tf, out, o.fallback_tol, rec, count, flags,
-                         flist, fcount, st->probe_err, r->d_cnt, r->stream);
+    e = launch_mlp_probe(g, L, (const float4*)r->d_quads, r->d_tab, r->d_tf, out, st->render_opts.fallback_tol, pb.rec,
+                         pb.count, pb.flags, pb.flist, pb.fcount, st->probe_err, r->d_cnt, r->stream, true);
   if (e != cudaSuccess) return cuda_fail(r, e, "mlp probe launch");
-  launches += L.nprobe > 0 ? 3 : 1;
+  launches += L.nprobe > 0 ? 2 : 1;
   const size_t nvert = (size_t)g.pd[0] * g.pd[1] * g.pd[2];
-  s = ensure_buffer(r, (void**)&r->d_map, &r->map_cap, nvert * sizeof(float), "allocating map");
+  beams_status s = ensure_buffer(r, (void**)&r->d_map, &r->map_cap, nvert * sizeof(float), "allocating map");
   if (s != BEAMS_OK) return s;
   r->map_valid = false;  // whether the gated build ran is known on the device only
   r->map_is_half = false;
   e = launch_light_march_f32(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map, r->d_cnt, r->stream, nullptr,
-                             0, -1, fcount);
+                             0, -1, pb.fcount);
   if (e == cudaSuccess)
-    e = launch_view_march_tiles(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map, out, r->d_cnt + 1, flist,
-                                fcount, r->stream);
+    e = launch_view_march_tiles(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map, out, r->d_cnt + 1,
+                                pb.flist, pb.fcount, r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "mlp fallback launch");
   launches += 2;
   return BEAMS_OK;
@@ -226,11 +245,17 @@ beams_status mlp_render_view(beams_renderer* r, const ExactGeo& g, float4* out, 
   ++launches;
   float lf[3];
   mlp_light_feature(r, g, lf);
+  ProbeBuffers pb;
+  beams_status s = probe_buffers(r, g, pb);
+  if (s != BEAMS_OK) return s;
+  MlpProbe probe{0, 0, 0, 0, 0, nullptr, nullptr};
+  if (pb.L.stride > 0 && pb.L.nprobe > 0)
+    probe = MlpProbe{pb.L.stride, pb.L.offset, pb.L.nqx, pb.L.nqy, pb.L.cap, pb.rec, pb.count};
   e = launch_view_march_mlp(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, W, aux, mlp_encoding(g), lf,
-                            st->render_opts.knot, out, r->d_cnt, r->stream);
+                            st->render_opts.knot, out, r->d_cnt, probe, r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "mlp view march launch");
   ++launches;
-  return mlp_probe_and_fallback(r, g, out, launches);
+  return mlp_probe_and_fallback(r, g, pb, out, launches);
 }
 
 }  // namespace beams

@@ -138,6 +138,22 @@ class ClockSampler:
                 "reasons": sorted(self.reasons - {"gpu_idle"}), "samples": len(self.samples)}
 
 
+def max_over_ranks(ms: float, world: int, device: str = "cuda") -> float:
+    """The slowest rank's time (all ranks take part; world == 1 returns ms)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world: int, steps: int, units_per_step: float, max_ms: float) -> float:
+    """Whole-job throughput of N independent replicas: all units over the slowest rank's time."""
+    return world * steps * units_per_step / (max_ms / 1e3)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -308,11 +324,8 @@ def run_ours(args):
         total_ms = sum(e[0].elapsed_time(e[2]) for e in evs)
     k1_ms = sum(e[0].elapsed_time(e[1]) for e in evs) / args.steps
     k2_ms = sum(e[1].elapsed_time(e[2]) for e in evs) / args.steps
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = world * args.steps * lit_frame / (max_ms / 1e3)
+    max_ms = max_over_ranks(total_ms, world)
+    value = replica_value(world, args.steps, lit_frame, max_ms)
 
     # roofline of the dominant kernel
     peak, peak_kind = measured_peaks()
@@ -353,13 +366,11 @@ def run_ours(args):
             r.render(cam, out=host_out, timings=False)
         e1.record(stream)
         torch.cuda.synchronize()
-        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * ne * lit_frame / (float(te.item()) / 1e3), "unit": UNIT,
+        te_ms = max_over_ranks(e0.elapsed_time(e1), world)
+        e2e = {"value": replica_value(world, ne, lit_frame, te_ms), "unit": UNIT,
                "h2d_bytes_per_step": int(host_field.numel() * 4 + s.tf.nbytes),
                "d2h_bytes_per_step": int(host_out.numel() * 4),
-               "ms_per_step": float(te.item()) / ne,
+               "ms_per_step": te_ms / ne,
                "path": "beams_set_volume(pinned host field) + beams_render(pinned host image) per step"}
         r.set_reuse_shadow_map(True)
 
@@ -424,10 +435,7 @@ def time_frames(frame, steps, warmup, stream, world, local):
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    t = torch.tensor([a.elapsed_time(b)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item()), sampler.summary()
+    return max_over_ranks(a.elapsed_time(b), world), sampler.summary()
 
 
 def fp64_crops(s, field, images, crop, stride, ncrops, threads):

@@ -95,6 +95,7 @@ typedef struct beams_timings {
   int map_vertices;                  /* (M+1)^3 of the map built this frame, 0 if reused */
   int fallback_tiles;                /* MLP form: tiles that used the exact map */
   int kernel_launches;               /* kernels this call launched */
+  unsigned long long mlp_rows;       /* learned form: network rows computed, idle lanes included */
 } beams_timings;
 
 typedef struct beams_renderer beams_renderer;
@@ -279,6 +280,11 @@ beams_status beams_mlp_loss_grad(beams_renderer* r, const float* features, const
  * P = round(1/sqrt(probe_fraction))); +inf marks a probe past the sample cap.
  * n must be the probe count; for tests and tools. */
 beams_status beams_mlp_probe_errors(beams_renderer* r, float* dst, int n);
+/* The network's forward pass on the tcgen05 tensor cores for n rows of
+ * features (n x 112 floats, rounded to bfloat16): T receives the predictions.
+ * For tests and tools (the training loop and the dense render path call the
+ * same kernel directly). */
+beams_status beams_mlp_forward_tc(beams_renderer* r, const float* features, int n, float* T);
 /* The network's input encoding of n world positions under n light features. */
 beams_status beams_mlp_encode(beams_renderer* r, const float* pos, const float* lfeat, int n, float* out);
 /* Versioned checkpoint of parameters and Adam moments (FNV-1a checksummed). */

@@ -133,7 +133,7 @@ class Timings(C.Structure):
     _fields_ = [("map_build_ms", C.c_float), ("view_march_ms", C.c_float), ("composite_ms", C.c_float),
                 ("total_ms", C.c_float), ("light_samples", C.c_ulonglong), ("lit_samples", C.c_ulonglong),
                 ("rays_hit", C.c_ulonglong), ("mlp_samples", C.c_ulonglong), ("map_vertices", C.c_int),
-                ("fallback_tiles", C.c_int), ("kernel_launches", C.c_int)]
+                ("fallback_tiles", C.c_int), ("kernel_launches", C.c_int), ("mlp_rows", C.c_ulonglong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -184,6 +184,7 @@ def lib():
         "beams_mlp_loss_grad": ([P, P, P, C.c_int, C.POINTER(C.c_float), P, P], C.c_int),
         "beams_mlp_encode": ([P, P, P, C.c_int, P], C.c_int),
         "beams_mlp_probe_errors": ([P, P, C.c_int], C.c_int),
+        "beams_mlp_forward_tc": ([P, P, C.c_int, P], C.c_int),
         "beams_set_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "beams_get_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "beams_batch_set_volumes": ([P, P, C.c_int], C.c_int),
@@ -415,6 +416,13 @@ class Renderer:
         out = np.empty((pos.shape[0], 112), np.float32)
         self._check(self._L.beams_mlp_encode(self._h, _ptr(pos), _ptr(lf), pos.shape[0], _ptr(out)))
         return out
+
+    def mlp_forward_tc(self, features):
+        """The tcgen05 forward pass on (n, 112) features; returns T (n,)."""
+        X = np.ascontiguousarray(features, np.float32).reshape(-1, 112)
+        T = np.empty(X.shape[0], np.float32)
+        self._check(self._L.beams_mlp_forward_tc(self._h, _ptr(X), X.shape[0], _ptr(T)))
+        return T
 
     def mlp_probe_errors(self, n):
         out = np.empty(n, np.float32)

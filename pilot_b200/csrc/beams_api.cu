@@ -991,6 +991,7 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
     t->lit_samples = c.lit_samples;
     t->rays_hit = c.rays_hit;
     t->mlp_samples = c.mlp_samples;
+    t->mlp_rows = c.mlp_rows;
     t->fallback_tiles = (int)c.fallback_tiles;
     if (use_mlp && c.fallback_tiles) built = true;  // the fallback's gated map build ran
     t->map_vertices = built ? (int)((size_t)g.pd[0] * g.pd[1] * g.pd[2]) : 0;

@@ -76,7 +76,7 @@ struct Counters {
   unsigned long long errors;
   unsigned int tiles_light;   // persistent-block work counters (zeroed per frame)
   unsigned int tiles_view;
-  unsigned long long pad;
+  unsigned long long mlp_rows;  // network rows computed (idle lanes included)
 };
 
 }  // namespace beams

@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
   const int ntiles = tiles_x * ((g.height + 3) >> 2);
   const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
   const int n1 = g.tf_n - 1;
-  unsigned lit = 0, hit = 0, evals = 0;
+  unsigned lit = 0, hit = 0, evals = 0, rows = 0;
   for (int tile = next_warp_tile_mlp(&cnt->tiles_view); tile < ntiles; tile = next_warp_tile_mlp(&cnt->tiles_view)) {
     const int lane = threadIdx.x & 31;
     const int x = (tile % tiles_x) * 8 + (lane & 7), y = (tile / tiles_x) * 4 + (lane >> 3);
@@ -338,6 +338,7 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
         if (color.w >= g.cutoff) done = true;
       }
       const float Tk = mlp_eval_warp(enc, kp, lf, sW, sAux);
+      rows += 32;
       if (nb > 0) {
         ++evals;
         const float inv_nb = 1.f / (float)nb;
@@ -364,6 +365,7 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
   warp_add(&cnt->lit_samples, lit);
   warp_add(&cnt->rays_hit, hit);
   warp_add(&cnt->mlp_samples, evals);
+  if ((threadIdx.x & 31) == 0 && rows) atomicAdd(&cnt->mlp_rows, (unsigned long long)rows);
 }
 
 cudaError_t launch_pack_weights(const float* P, uint2* W, float* aux, cudaStream_t st) {

@@ -264,6 +264,35 @@ using namespace beams;
 
 extern "C" {
 
+beams_status beams_mlp_forward_tc(beams_renderer* r, const float* features, int n, float* T) {
+  if (!r || !features || !T || n < 1 || n > (1 << 24)) return fail(r, BEAMS_ERR_INVALID_ARG, "mlp_forward_tc: bad arguments");
+  MlpState* st = r->mlp;
+  if (!st || !st->P) return fail(r, BEAMS_ERR_STATE, "mlp_forward_tc: no network");
+  cudaSetDevice(r->device);
+  std::vector<__nv_bfloat16> hx((size_t)n * kIn);
+  for (size_t i = 0; i < hx.size(); ++i) hx[i] = __float2bfloat16_rn(features[i]);
+  __nv_bfloat16* dx = nullptr;
+  float* dt = nullptr;
+  unsigned* derr = nullptr;
+  cudaError_t e = cudaMalloc((void**)&dx, hx.size() * sizeof(__nv_bfloat16));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&dt, (size_t)n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&derr, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemsetAsync(derr, 0, sizeof(unsigned), r->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dx, hx.data(), hx.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice, r->stream);
+  if (e == cudaSuccess) e = mlp_forward_tc_features(dx, n, st->P, nullptr, dt, derr, r->stream);
+  unsigned herr = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(T, dt, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, r->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, derr, sizeof(unsigned), cudaMemcpyDeviceToHost, r->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(r->stream);
+  cudaFree(dx);
+  cudaFree(dt);
+  cudaFree(derr);
+  if (e != cudaSuccess) return cuda_fail(r, e, "mlp_forward_tc");
+  if (herr) return fail(r, BEAMS_ERR_TIMEOUT, "mlp_forward_tc: a tensor-core wait timed out");
+  return BEAMS_OK;
+}
+
 beams_status beams_mlp_probe_errors(beams_renderer* r, float* dst, int n) {
   if (!r || !dst) return fail(r, BEAMS_ERR_INVALID_ARG, "mlp_probe_errors: NULL argument");
   MlpState* st = r->mlp;

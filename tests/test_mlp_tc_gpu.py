@@ -1,0 +1,38 @@
+"""The network's forward pass on the tcgen05 tensor cores (TMEM accumulators,
+shared-memory operands) against the CUDA-core forward and the float64 oracle."""
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as M
+from pilot_b200 import beams as B
+from pilot_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _features(r, n, seed):
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(0, 1, (n, 3)).astype(np.float32)
+    lf = rng.normal(size=(n, 3))
+    lf = (lf / np.linalg.norm(lf, axis=1, keepdims=True)).astype(np.float32)
+    return r.mlp_encode(pos, lf)
+
+
+@pytest.mark.parametrize("n", [1, 1000, 300_001])
+def test_tcgen05_forward_matches_cuda_core_forward(cuda_device, n):
+    s = scenes.small(81, n=24, image=16, m=8)
+    with B.Renderer(0) as r:
+        r.set_volume(s.field_numpy(), origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+        s.configure(r)
+        rng = np.random.default_rng(3)
+        P = rng.normal(0, 0.1, M.N_PARAMS).astype(np.float32)
+        r.mlp_set_params(P)
+        X = _features(r, n, 5)
+        T_tc = r.mlp_forward_tc(X)
+        _, _, T_cc = r.mlp_loss_grad(X, np.zeros(n, np.float32))
+        d = np.abs(T_tc - T_cc)
+        print(f"n={n}: tcgen05 vs CUDA cores max {d.max():.2e} mean {d.mean():.2e}")
+        assert np.all(np.isfinite(T_tc)) and d.max() < 2e-3 and d.mean() < 1e-4
+        if n <= 1000:
+            _, _, T64 = M.forward_backward(P, M.bf16(X), np.zeros(n))
+            assert np.abs(T_tc - T64).max() < 5e-3

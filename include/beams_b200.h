@@ -285,6 +285,9 @@ beams_status beams_mlp_probe_errors(beams_renderer* r, float* dst, int n);
  * For tests and tools (the training loop and the dense render path call the
  * same kernel directly). */
 beams_status beams_mlp_forward_tc(beams_renderer* r, const float* features, int n, float* T);
+/* 1 (default): training and beams_mlp_loss_grad run the hidden layers on the
+ * tcgen05 tensor cores; 0: on the CUDA cores (the reference path for tests). */
+beams_status beams_mlp_set_tensor_cores(beams_renderer* r, int enable);
 /* The network's input encoding of n world positions under n light features. */
 beams_status beams_mlp_encode(beams_renderer* r, const float* pos, const float* lfeat, int n, float* out);
 /* Versioned checkpoint of parameters and Adam moments (FNV-1a checksummed). */

@@ -309,10 +309,16 @@ cudaError_t mlp_fwd_bwd(const float* P, float* G, const __nv_bfloat16* X, const 
   const unsigned rb = (unsigned)((n + 63) / 64);
   const int Ks[4] = {kIn, kHid, kHid, kHid};
   const int oW[4] = {oW1, oW2, oW3, oW4}, oB[4] = {oB1, oB2, oB3, oB4};
-  const __nv_bfloat16* in = X;
-  for (int l = 0; l < 4; ++l) {
-    k_linear_fwd<<<rf, 256, 0, st>>>(in, P + oW[l], P + oB[l], w.H[l], n, Ks[l]);
-    in = w.H[l];
+  if (w.err) {
+    // the four hidden layers on the tcgen05 tensor cores (k_mlp_tc.cu)
+    cudaError_t e = mlp_forward_tc_features(X, n, P, w.H, nullptr, w.err, st);
+    if (e != cudaSuccess) return e;
+  } else {
+    const __nv_bfloat16* in = X;
+    for (int l = 0; l < 4; ++l) {
+      k_linear_fwd<<<rf, 256, 0, st>>>(in, P + oW[l], P + oB[l], w.H[l], n, Ks[l]);
+      in = w.H[l];
+    }
   }
   k_head<<<grid_cap(n, 256), 256, 0, st>>>(w.H[3], P, target, w.T, G ? w.dB : nullptr, G ? w.dz : nullptr, w.loss, n,
                                            1.f / (float)n);

@@ -43,6 +43,8 @@ struct MlpState {
   float* probe_err = nullptr;  // per-probe max |dRGBA| of the last frame (tests)
   int probe_err_n = 0;
   beams_mlp_options render_opts{};
+  bool use_tc = true;            // training forward on the tcgen05 tensor cores
+  unsigned* err_slot = nullptr;  // their timeout flag in the workspace
   ~MlpState() {
     for (void* p : {(void*)P, (void*)G, (void*)m, (void*)v, ws_mem, (void*)lights, (void*)lfeat, packed, probe_mem,
                     (void*)probe_err})
@@ -114,6 +116,10 @@ static beams_status ensure_ws(beams_renderer* r, MlpState* s, int rows) {
   s->ws.T = (float*)p;
   p += (size_t)rows * 4;
   s->ws.loss = (float*)p;
+  s->err_slot = (unsigned*)(p + 64);
+  s->ws.err = s->use_tc ? s->err_slot : nullptr;  // the forward runs on the tcgen05 tensor cores
+  e = cudaMemsetAsync(s->err_slot, 0, sizeof(unsigned), r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "clearing the MLP workspace");
   s->ws_rows = rows;
   return BEAMS_OK;
 }
@@ -263,6 +269,14 @@ beams_status mlp_render_view(beams_renderer* r, const ExactGeo& g, float4* out, 
 using namespace beams;
 
 extern "C" {
+
+beams_status beams_mlp_set_tensor_cores(beams_renderer* r, int enable) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  MlpState* st = mlp_state(r);
+  st->use_tc = enable != 0;
+  st->ws.err = (st->use_tc && st->err_slot) ? st->err_slot : nullptr;
+  return BEAMS_OK;
+}
 
 beams_status beams_mlp_forward_tc(beams_renderer* r, const float* features, int n, float* T) {
   if (!r || !features || !T || n < 1 || n > (1 << 24)) return fail(r, BEAMS_ERR_INVALID_ARG, "mlp_forward_tc: bad arguments");
@@ -454,7 +468,19 @@ beams_status beams_mlp_train(beams_renderer* r, const beams_mlp_options* opt, be
   if (e == cudaSuccess)
     e = mlp_fwd_bwd(st->P, nullptr, d_X + (size_t)ntrain * kIn, d_target + ntrain, holdout, st->ws, r->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&hl, st->ws.loss, sizeof(float), cudaMemcpyDeviceToHost, r->stream);
+  unsigned tc_err = 0;
+  if (e == cudaSuccess && st->ws.err)
+    e = cudaMemcpyAsync(&tc_err, st->ws.err, sizeof(unsigned), cudaMemcpyDeviceToHost, r->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(r->stream);
+  if (e == cudaSuccess && tc_err) {
+    cudaFree(d_samples);
+    cudaFree(d_target);
+    cudaFree(d_X);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    cudaEventDestroy(t2);
+    return fail(r, BEAMS_ERR_TIMEOUT, "mlp_train: a tensor-core wait timed out");
+  }
   if (rep && e == cudaSuccess) {
     std::memset(rep, 0, sizeof(*rep));
     cudaEventElapsedTime(&rep->datagen_ms, t0, t1);

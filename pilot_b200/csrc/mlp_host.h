@@ -16,6 +16,7 @@ struct TrainWS {
   float* dz;            // rows
   float* T;             // rows
   float* loss;          // 1
+  unsigned* err;        // tensor-core wait timeouts; null: the forward runs on the CUDA cores
 };
 
 cudaError_t mlp_gen_data(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,

@@ -29,7 +29,11 @@ def test_tcgen05_forward_matches_cuda_core_forward(cuda_device, n):
         r.mlp_set_params(P)
         X = _features(r, n, 5)
         T_tc = r.mlp_forward_tc(X)
+        r.mlp_set_tensor_cores(False)  # the CUDA-core forward as the reference
         _, _, T_cc = r.mlp_loss_grad(X, np.zeros(n, np.float32))
+        r.mlp_set_tensor_cores(True)
+        _, _, T_tr = r.mlp_loss_grad(X, np.zeros(n, np.float32))  # training's forward: tcgen05
+        assert np.array_equal(T_tr, T_tc)
         d = np.abs(T_tc - T_cc)
         print(f"n={n}: tcgen05 vs CUDA cores max {d.max():.2e} mean {d.mean():.2e}")
         assert np.all(np.isfinite(T_tc)) and d.max() < 2e-3 and d.mean() < 1e-4

@@ -543,6 +543,14 @@ def run_form(args):
                     "evaluations": tn["mlp_samples"], "kernel_ms": tn["view_march_ms"]}
         dtype = "bf16"
         ntiles = -(-s.width // 32) * -(-s.height // 32)
+        # the tcgen05 forward kernel on 2^22 device-resident rows (training's forward pass)
+        nrow = 1 << 22
+        X = torch.empty((nrow, 112), device="cuda").uniform_(-1, 1).to(torch.bfloat16)
+        Tt = torch.empty(nrow, device="cuda")
+        tc_ms, _ = time_frames(lambda: r.mlp_forward_tc_device(X, Tt), 10, 3, stream, world, local)
+        tc_ms /= 10
+        tc_tflops = nrow * MLP_FLOP_PER_EVAL / (tc_ms / 1e3) / 1e12
+        del X, Tt
         extra["learned"] = {"train": {k: rep[k] for k in ("datagen_ms", "train_ms", "holdout_rmse", "unlit_rmse",
                                                            "mean_rmse", "steps", "samples")},
                             "lights": args.mlp_lights, "scene_light": bool(args.mlp_scene_light),
@@ -553,6 +561,9 @@ def run_form(args):
                             "exact_ms_per_frame": exact_ms,
                             "speedup_vs_exact": exact_ms / (total_ms / args.steps),
                             "network_only_ms": tn["total_ms"],
+                            "tcgen05_forward": {"rows": nrow, "ms": tc_ms, "tflops": tc_tflops,
+                                                "frac_of_bf16_peak": tc_tflops / tpeak,
+                                                "note": "dense forward kernel (TMEM accumulators), training's forward"},
                             "psnr_vs_exact_map_full_frame": psnr(img, exact_img),
                             "network_only_psnr_vs_exact_map": psnr(net_img, exact_img)}
         if not args.no_quality and rank == 0:

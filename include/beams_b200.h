@@ -285,6 +285,9 @@ beams_status beams_mlp_probe_errors(beams_renderer* r, float* dst, int n);
  * For tests and tools (the training loop and the dense render path call the
  * same kernel directly). */
 beams_status beams_mlp_forward_tc(beams_renderer* r, const float* features, int n, float* T);
+/* The same on device memory: features_bf16 = n x 112 bfloat16 rows, T = n floats;
+ * asynchronous on the renderer's stream, allocates nothing once a network exists. */
+beams_status beams_mlp_forward_tc_device(beams_renderer* r, const void* features_bf16, int n, float* T);
 /* 1 (default): training and beams_mlp_loss_grad run the hidden layers on the
  * tcgen05 tensor cores; 0: on the CUDA cores (the reference path for tests). */
 beams_status beams_mlp_set_tensor_cores(beams_renderer* r, int enable);

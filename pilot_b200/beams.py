@@ -186,6 +186,7 @@ def lib():
         "beams_mlp_probe_errors": ([P, P, C.c_int], C.c_int),
         "beams_mlp_forward_tc": ([P, P, C.c_int, P], C.c_int),
         "beams_mlp_set_tensor_cores": ([P, C.c_int], C.c_int),
+        "beams_mlp_forward_tc_device": ([P, P, C.c_int, P], C.c_int),
         "beams_set_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "beams_get_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "beams_batch_set_volumes": ([P, P, C.c_int], C.c_int),
@@ -424,6 +425,10 @@ class Renderer:
         T = np.empty(X.shape[0], np.float32)
         self._check(self._L.beams_mlp_forward_tc(self._h, _ptr(X), X.shape[0], _ptr(T)))
         return T
+
+    def mlp_forward_tc_device(self, features_bf16, T):
+        """tcgen05 forward on torch CUDA tensors: features (n, 112) bfloat16, T (n,) float32."""
+        self._check(self._L.beams_mlp_forward_tc_device(self._h, _ptr(features_bf16), int(T.numel()), _ptr(T)))
 
     def mlp_set_tensor_cores(self, enable: bool):
         self._check(self._L.beams_mlp_set_tensor_cores(self._h, int(bool(enable))))

@@ -270,6 +270,21 @@ using namespace beams;
 
 extern "C" {
 
+beams_status beams_mlp_forward_tc_device(beams_renderer* r, const void* features_bf16, int n, float* T) {
+  if (!r || !features_bf16 || !T || n < 1) return fail(r, BEAMS_ERR_INVALID_ARG, "mlp_forward_tc_device: bad arguments");
+  MlpState* st = r->mlp;
+  if (!st || !st->P) return fail(r, BEAMS_ERR_STATE, "mlp_forward_tc_device: no network");
+  if (!st->err_slot) {
+    beams_status s = ensure_ws(r, st, 256);
+    if (s != BEAMS_OK) return s;
+  }
+  cudaSetDevice(r->device);
+  cudaError_t e = mlp_forward_tc_features((const __nv_bfloat16*)features_bf16, n, st->P, nullptr, T, st->err_slot,
+                                          r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "mlp_forward_tc_device");
+  return BEAMS_OK;
+}
+
 beams_status beams_mlp_set_tensor_cores(beams_renderer* r, int enable) {
   if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
   MlpState* st = mlp_state(r);

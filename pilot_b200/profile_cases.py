@@ -3,6 +3,7 @@
     python -m pilot_b200.profile_cases --case light_march      # K1, 512^3 noise, M = 256
     python -m pilot_b200.profile_cases --case view_march       # K2, 512^3 noise, 1024^2, map cached
     python -m pilot_b200.profile_cases --case mlp_view         # learned-form view march, 1024^2
+    python -m pilot_b200.profile_cases --case mlp_tc           # tcgen05 forward, 2^21 rows
     python -m pilot_b200.profile_cases --case batch            # 16-request persistent batch
     python -m pilot_b200.profile_cases --case precision_light  # precision-form K1, bf16 640^3
 
@@ -25,7 +26,7 @@ def main(argv=None) -> int:
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", required=True,
-                    choices=["light_march", "view_march", "mlp_view", "batch", "precision_light"])
+                    choices=["light_march", "view_march", "mlp_view", "mlp_tc", "batch", "precision_light"])
     ap.add_argument("--reps", type=int, default=3)
     a = ap.parse_args(argv)
     torch.cuda.set_device(0)
@@ -51,6 +52,19 @@ def main(argv=None) -> int:
             r.set_form(B.FORM_MLP, B.mlp_options(knot=4, probe_fraction=0.0))
             for _ in range(a.reps):
                 r.render(cam, out=out, timings=False)
+    elif a.case == "mlp_tc":
+        # the tcgen05 forward on 2^21 rows of device-resident features
+        s = scenes.small(5, n=32, image=16, m=8)
+        r = B.Renderer(0)
+        r.set_volume(s.field_numpy(), origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+        s.configure(r)
+        rng = np.random.default_rng(1)
+        r.mlp_set_params(rng.normal(0, 0.1, B.lib().beams_mlp_param_count()).astype(np.float32))
+        n = 1 << 21
+        X = torch.empty((n, 112), device="cuda").uniform_(-1, 1).to(torch.bfloat16)
+        T = torch.empty(n, device="cuda")
+        for _ in range(a.reps):
+            r.mlp_forward_tc_device(X, T)
     elif a.case == "precision_light":
         s = scenes.config2(n=640, image=1024, m=320)
         fd = s.field_device()

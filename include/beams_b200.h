@@ -221,7 +221,8 @@ typedef struct beams_batch_options {
   int light_brick;          /* map-build vertex order: 0 rows, 8/16/32/64 bricks */
   int use_graph;            /* 1: capture once, replay (default) */
   int no_skip;              /* 1: no empty-space skipping (default 0: both marches skip empty macro-cells) */
-  int reserved;
+  int reserved;             /* 0; 0x7e57 makes the map items withhold their completion (tests of the bounded
+                               wait: the call then returns BEAMS_ERR_TIMEOUT after about 2 s) */
 } beams_batch_options;
 beams_status beams_set_batch_options(beams_renderer* r, const beams_batch_options* o);
 /* Timings: total_ms = the batch (launch to last image copied), view_march_ms = the
@@ -338,6 +339,9 @@ beams_status beams_render_noalloc(const beams_volume* vol, const float* tf_rgba_
                                   const beams_camera* cam, float* rgba_out_device, void* cuda_stream);
 
 /* ---- diagnostics ------------------------------------------------------------ */
+/* Fault injection for tests (no reference counterpart): the nth following device
+ * buffer allocation of any renderer fails with BEAMS_ERR_OOM (0 disarms). */
+beams_status beams_test_fail_allocation(int nth);
 /* Checks, on the device, the kernels' correctly rounded division (Markstein's
  * correction on a tabulated reciprocal) against IEEE division for every cell
  * width of the counting coordinates origin + i*spacing (ncells cells) and

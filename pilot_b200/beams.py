@@ -188,6 +188,7 @@ def lib():
         "beams_mlp_set_tensor_cores": ([P, C.c_int], C.c_int),
         "beams_mlp_forward_tc_device": ([P, P, C.c_int, P], C.c_int),
         "beams_set_tuning": ([P, C.POINTER(Tuning)], C.c_int),
+        "beams_test_fail_allocation": ([C.c_int], C.c_int),
         "beams_get_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "beams_batch_set_volumes": ([P, P, C.c_int], C.c_int),
         "beams_set_batch_options": ([P, C.POINTER(BatchOptions)], C.c_int),
@@ -334,8 +335,9 @@ class Renderer:
                              (C.c_double * 2)(*vrange), ASSOC_POINTS, on_dev)
         self._check(self._L.beams_batch_set_volumes(self._h, vols, len(volumes)))
 
-    def set_batch_options(self, tile_w=32, tile_h=32, light_brick=8, use_graph=True, skip=True):
-        o = BatchOptions(int(tile_w), int(tile_h), int(light_brick), int(bool(use_graph)), int(not skip))
+    def set_batch_options(self, tile_w=32, tile_h=32, light_brick=8, use_graph=True, skip=True, _withhold=False):
+        o = BatchOptions(int(tile_w), int(tile_h), int(light_brick), int(bool(use_graph)), int(not skip),
+                         0x7E57 if _withhold else 0)
         self._check(self._L.beams_set_batch_options(self._h, C.byref(o)))
 
     @staticmethod

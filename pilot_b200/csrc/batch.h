@@ -35,7 +35,7 @@ struct BatchPlan {
   int tile_w, tile_h;     // view tile: a multiple of 8 x 4 warp tiles
   int brick_log2;         // map-build vertex order inside a request (0 = rows)
   int skip;               // 1: both marches skip empty macro-cells (every desc has occ)
-  int pad;
+  int test_withhold;      // tests: map items never publish, so view items time out
   int seg_off[2 * kMaxRequests + 1];
   int seg_req[2 * kMaxRequests];
   int k1_items[kMaxRequests];  // map-build items per request (what a view item waits for)

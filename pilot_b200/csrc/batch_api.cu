@@ -266,6 +266,7 @@ beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, in
     P.tile_h = b->opts.tile_h;
     P.brick_log2 = bl;
     P.skip = skip;
+    P.test_withhold = b->opts.reserved == 0x7e57 ? 1 : 0;
     b->max_ntab = 0;
     std::vector<int> k2(n);
     for (int i = 0; i < n; ++i) {

@@ -8,6 +8,8 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -42,6 +44,10 @@ beams_status cuda_fail(beams_renderer* r, cudaError_t e, const char* what) {
   return fail(r, e == cudaErrorMemoryAllocation ? BEAMS_ERR_OOM : BEAMS_ERR_CUDA, m);
 }
 
+// Allocation-failure injection for tests (beams_test_fail_allocation): the
+// n-th following buffer allocation reports out-of-memory instead of allocating.
+static std::atomic<int> g_fail_alloc_in{0};
+
 beams_status ensure_buffer(beams_renderer* r, void** buf, size_t* cap, size_t bytes, const char* what) {
   if (*cap >= bytes && *buf) return BEAMS_OK;
   if (*buf) {
@@ -49,6 +55,10 @@ beams_status ensure_buffer(beams_renderer* r, void** buf, size_t* cap, size_t by
     *buf = nullptr;
     *cap = 0;
   }
+  int pending = g_fail_alloc_in.load();
+  while (pending > 0 && !g_fail_alloc_in.compare_exchange_weak(pending, pending - 1)) {
+  }
+  if (pending == 1) return fail(r, BEAMS_ERR_OOM, std::string(what) + ": out of device memory (injected)");
   cudaError_t e = cudaMalloc(buf, bytes);
   if (e != cudaSuccess) {
     *buf = nullptr;
@@ -679,6 +689,12 @@ beams_status beams_set_light_steps(beams_renderer* r, float steps) {
 beams_status beams_set_slab_fp64(beams_renderer* r, int enable) {
   if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
   r->slab_fp64 = enable != 0;
+  return BEAMS_OK;
+}
+
+beams_status beams_test_fail_allocation(int nth) {
+  if (nth < 0) return BEAMS_ERR_INVALID_ARG;
+  g_fail_alloc_in.store(nth);
   return BEAMS_OK;
 }
 

@@ -137,14 +137,15 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch(const ExactGeo* __re
       }
       __threadfence();
       __syncthreads();
-      if (tid == 0) atomicAdd(&q->done1[req], 1u);
+      if (tid == 0 && !plan.test_withhold) atomicAdd(&q->done1[req], 1u);
     } else {
       if (tid == 0) {
         const unsigned need = (unsigned)plan.k1_items[req];
         const long long t0 = clock64();
         int skip = 0;
         while (ld_acquire(&q->done1[req]) < need) {
-          if (clock64() - t0 > kWaitCycles) {
+          // give up after the budget, or at once when another block already has
+          if (clock64() - t0 > kWaitCycles || ld_acquire(&q->error)) {
             atomicOr(&q->error, 1u);
             skip = 1;
             break;

@@ -151,6 +151,14 @@ beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable);
 /* Replaces MapperLightedVolume::SetCompositeBackground (MapperLightedVolume.cxx:321-324):
  * blend rgb over an opaque background colour after compositing. Off by default. */
 beams_status beams_set_background(beams_renderer* r, int enable, const float rgba[4]);
+/* The multi-light extension (the reference's notes.txt:4 "use multiple lights";
+ * its renderer uses Locations[0] only, TransmittanceMap.h:591-592, which stays the
+ * default): with enable != 0 and more than one light, the exact form builds one
+ * map per light and the view march shades by sum_l (1 - opacity_l) * color_l *
+ * intensity_l (light order) in place of the single term. Up to 8 lights; exact
+ * form, single point volume. beams_get_shadow_map returns the maps one after the
+ * other. */
+beams_status beams_set_multi_light(beams_renderer* r, int enable);
 /* Launch tuning (no reference counterpart; results do not depend on it).
  * light_brick: the order in which the map build takes its vertices: 0 = rows
  * (x fastest), or cubic bricks of 8 (default), 16, 32 or 64 vertices per edge.

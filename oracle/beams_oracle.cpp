@@ -80,6 +80,12 @@ struct Geo {
   int pd[3];                    // map point dims M+1
   T morig[3], msp[3], minv[3];  // CreateDataSetForOpacityMap, TransmittanceMap.h:550-563
   T light_color[3];             // Color * Intensity, LightedVolumeRenderer.cxx:840
+  // multi-light extension (off in the reference, which shades with Locations[0]
+  // only, LightedVolumeRenderer.cxx:836-840): n_lights maps of map_nv vertices
+  // stacked in light order, light l shaded with lcols[3l..3l+2]
+  int n_lights = 1;
+  int64_t map_nv = 0;
+  std::vector<T> lcols;
   T extent_mag;                 // BoundsMagnitude, Math.h:13-21
   T sd, mesh_eps, step, cutoff;
   int light_kind;
@@ -383,6 +389,19 @@ inline T map_opacity_at(const Geo<T>& g, const T p[3], MapGet get);
 
 template <typename T, typename MapGet>
 inline void map_estimate(const Geo<T>& g, const T p[3], MapGet get, T est[3]) {
+  if (g.n_lights > 1) {
+    // sum over the lights of (1 - opacity_l) * colour_l, accumulated in light order
+    for (int l = 0; l < g.n_lights; ++l) {
+      const int64_t off = (int64_t)l * g.map_nv;
+      auto gl = [&get, off](int64_t i) -> T { return get(i + off); };
+      const T tr = T(1) - map_opacity_at(g, p, gl);
+      for (int d = 0; d < 3; ++d) {
+        const T t = tr * g.lcols[3 * l + d];
+        est[d] = (l == 0) ? t : est[d] + t;
+      }
+    }
+    return;
+  }
   // precision form: the map holds transmittance, interpolated directly
   const T tr = g.precision ? map_opacity_at(g, p, get) : T(1) - map_opacity_at(g, p, get);
   for (int d = 0; d < 3; ++d) est[d] = tr * g.light_color[d];
@@ -649,12 +668,18 @@ int light_march_ids(const oracle_scene* s, const int64_t* ids, int64_t n, T* out
 
 template <typename T>
 int view_march(const oracle_scene* s, const T* map, int x0, int y0, int w, int h, T* rgba,
-               int threads, uint64_t* lit_out) {
+               int threads, uint64_t* lit_out, int n_lights = 1, const float* lcols = nullptr) {
   if (!valid(s) || !rgba) return 1;
   if (s->use_map && !map) return 1;
   if (x0 < 0 || y0 < 0 || x0 + w > s->width || y0 + h > s->height) return 1;
   Geo<T> g;
   build_geo(s, g);
+  if (n_lights > 1) {
+    if (!lcols || !s->use_map || s->precision) return 1;
+    g.n_lights = n_lights;
+    g.map_nv = (int64_t)g.pd[0] * g.pd[1] * g.pd[2];
+    g.lcols.assign(lcols, lcols + 3 * (size_t)n_lights);
+  }
   uint64_t lit = 0;
   auto get = [map](int64_t i) -> T { return map[i]; };
   const int64_t npx = (int64_t)w * h;
@@ -932,6 +957,14 @@ int oracle_view_march_f32(const oracle_scene* s, const float* map, int x0, int y
 int oracle_view_march_f64(const oracle_scene* s, const double* map, int x0, int y0, int w, int h,
                           double* rgba, int threads, uint64_t* lit) {
   return view_march<double>(s, map, x0, y0, w, h, rgba, threads, lit);
+}
+
+// Multi-light extension: maps holds n_lights exact-form maps stacked in light
+// order; light_colors holds colour * intensity per light (float32, n_lights x 3).
+int oracle_view_march_multi_f32(const oracle_scene* s, const float* maps, int n_lights, const float* light_colors,
+                                int x0, int y0, int w, int h, float* rgba, int threads, uint64_t* lit) {
+  if (n_lights < 1) return 1;
+  return view_march<float>(s, maps, x0, y0, w, h, rgba, threads, lit, n_lights, light_colors);
 }
 
 // FP64 view march whose map vertices are computed on first use (memoised), for

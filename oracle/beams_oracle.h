@@ -75,6 +75,10 @@ int oracle_view_march_f32(const oracle_scene* s, const float* map, int x0, int y
                           float* rgba_out, int threads, uint64_t* lit_samples);
 int oracle_view_march_f64(const oracle_scene* s, const double* map, int x0, int y0, int w, int h,
                           double* rgba_out, int threads, uint64_t* lit_samples);
+/* Multi-light extension: n_lights exact-form maps stacked in light order, shaded
+ * with sum_l (1 - opacity_l) * light_colors[l] (colour * intensity, float32). */
+int oracle_view_march_multi_f32(const oracle_scene* s, const float* maps, int n_lights, const float* light_colors,
+                                int x0, int y0, int w, int h, float* rgba_out, int threads, uint64_t* lit_samples);
 int oracle_view_march_lazy_f64(const oracle_scene* s, int x0, int y0, int w, int h, int stride,
                                double* rgba_out, int threads, uint64_t* lit_samples);
 

@@ -45,6 +45,8 @@ def lib():
             "oracle_view_march_f32": [S, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
             "oracle_view_march_f64": [S, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
             "oracle_view_march_lazy_f64": [S, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
+            "oracle_view_march_multi_f32": [S, P, C.c_int, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int,
+                                            u64p],
             "oracle_ray_setup_f32": [S, C.c_int, C.c_int, P],
             "oracle_composite_f32": [P, C.c_int, C.c_int, P, P],
             "oracle_generate_noise": [P, C.c_int, C.c_int, C.c_int, P, C.c_int, C.c_float, C.c_float,
@@ -129,6 +131,22 @@ class Oracle:
         if fn(C.byref(self.cs), None if mp is None else _p(mp), x0, y0, w, h, _p(out), self.threads,
               C.byref(lit)):
             raise RuntimeError("oracle view march rejected the scene")
+        return out, lit.value
+
+    def view_march_multi(self, maps, light_colors, window=None):
+        """Multi-light extension: maps is (n_lights, map vertices) exact-form
+        opacity, light_colors (n_lights, 3) colour * intensity in float32."""
+        s = self.scene
+        x0, y0, w, h = window if window is not None else (0, 0, s.width, s.height)
+        mp = np.ascontiguousarray(maps, np.float32)
+        lc = np.ascontiguousarray(light_colors, np.float32).reshape(-1, 3)
+        if mp.shape[0] != lc.shape[0]:
+            raise ValueError("one map per light colour")
+        out = np.zeros((h, w, 4), np.float32)
+        lit = C.c_uint64()
+        if lib().oracle_view_march_multi_f32(C.byref(self.cs), _p(mp), lc.shape[0], _p(lc), x0, y0, w, h, _p(out),
+                                             self.threads, C.byref(lit)):
+            raise RuntimeError("oracle multi-light view march rejected the scene")
         return out, lit.value
 
     def view_march_lazy_f64(self, window, stride: int = 1):

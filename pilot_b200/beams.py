@@ -188,6 +188,7 @@ def lib():
         "beams_mlp_set_tensor_cores": ([P, C.c_int], C.c_int),
         "beams_mlp_forward_tc_device": ([P, P, C.c_int, P], C.c_int),
         "beams_set_tuning": ([P, C.POINTER(Tuning)], C.c_int),
+        "beams_set_multi_light": ([P, C.c_int], C.c_int),
         "beams_test_fail_allocation": ([C.c_int], C.c_int),
         "beams_get_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "beams_batch_set_volumes": ([P, P, C.c_int], C.c_int),
@@ -485,6 +486,9 @@ class Renderer:
     def set_background(self, on: bool, rgba=(1, 1, 1, 1)):
         c = (C.c_float * 4)(*rgba)
         self._check(self._L.beams_set_background(self._h, int(bool(on)), c))
+
+    def set_multi_light(self, enable: bool):
+        self._check(self._L.beams_set_multi_light(self._h, int(bool(enable))))
 
     def set_tuning(self, light_brick: int = 8, empty_skip: bool = True, view_skip: bool = True):
         t = Tuning(int(light_brick), 0 if empty_skip else 1, 0 if view_skip else 1)

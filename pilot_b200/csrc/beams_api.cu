@@ -72,6 +72,18 @@ static bool finite3(const double* v) {
   return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]);
 }
 
+// Light l's part of the kernel parameters (Color * Intensity, LightedVolumeRenderer.cxx:840).
+static void geo_set_light(ExactGeo& g, const Light& L) {
+  g.light_kind = L.kind;
+  for (int d = 0; d < 3; ++d) g.light_color[d] = L.color[d] * L.intensity;
+  if (L.kind == 0) {
+    for (int d = 0; d < 3; ++d) g.light[d] = (float)L.v[d];
+  } else {
+    const double len = std::sqrt(L.v[0] * L.v[0] + L.v[1] * L.v[1] + L.v[2] * L.v[2]);
+    for (int d = 0; d < 3; ++d) g.light[d] = (float)(L.v[d] / len);
+  }
+}
+
 // Derives the kernel parameters exactly as the reference derives them
 // (float32 arithmetic; see the cited lines in beams_params.h).
 beams_status make_geo_vol(beams_renderer* r, const beams_volume& v, const beams_camera* cam, ExactGeo& g) {
@@ -116,16 +128,13 @@ beams_status make_geo_vol(beams_renderer* r, const beams_volume& v, const beams_
   g.light_brick_log2 = r->light_brick_log2;
   occupancy_dims(g.n, g.occ_n);
   g.dir_dist = 2.f * g.extent_mag;
-  if (!r->lights.empty()) {
-    const Light& L = r->lights[0];
-    g.light_kind = L.kind;
-    for (int d = 0; d < 3; ++d) g.light_color[d] = L.color[d] * L.intensity;
-    if (L.kind == 0) {
-      for (int d = 0; d < 3; ++d) g.light[d] = (float)L.v[d];
-    } else {
-      const double len = std::sqrt(L.v[0] * L.v[0] + L.v[1] * L.v[1] + L.v[2] * L.v[2]);
-      for (int d = 0; d < 3; ++d) g.light[d] = (float)(L.v[d] / len);
-    }
+  if (!r->lights.empty()) geo_set_light(g, r->lights[0]);
+  g.n_lights = 1;
+  for (int d = 0; d < 3; ++d) g.light_colors[0][d] = g.light_color[d];
+  if (r->multi_light && r->lights.size() > 1) {
+    g.n_lights = (int)r->lights.size();
+    for (int l = 0; l < g.n_lights; ++l)
+      for (int d = 0; d < 3; ++d) g.light_colors[l][d] = r->lights[l].color[d] * r->lights[l].intensity;
   }
   int off = 0;
   for (int d = 0; d < 3; ++d) {
@@ -199,6 +208,11 @@ static void map_key(const beams_renderer* r, MapKey& k) {
   if (!r->lights.empty()) {
     k.light_kind = r->lights[0].kind;
     for (int d = 0; d < 3; ++d) k.light[d] = r->lights[0].v[d];
+  }
+  k.n_lights = (r->multi_light && r->lights.size() > 1) ? (int)r->lights.size() : 1;
+  for (int l = 1; l < k.n_lights && l < kMaxMultiLights; ++l) {
+    k.extra_kind[l] = r->lights[l].kind;
+    for (int d = 0; d < 3; ++d) k.extra[l][d] = r->lights[l].v[d];
   }
 }
 
@@ -288,7 +302,8 @@ beams_status build_map(beams_renderer* r, const ExactGeo& g, int& launches, bool
   if (r->reuse_map && r->map_valid && std::memcmp(&key, &r->map_key, sizeof(key)) == 0) return BEAMS_OK;
   const size_t nvert = (size_t)g.pd[0] * g.pd[1] * g.pd[2];
   const bool prec = r->form == BEAMS_FORM_PRECISION;
-  beams_status s = ensure_buffer(r, (void**)&r->d_map, &r->map_cap, nvert * (prec ? 2 : sizeof(float)),
+  const int nl = g.n_lights > 1 ? g.n_lights : 1;  // the multi-light extension: one map per light
+  beams_status s = ensure_buffer(r, (void**)&r->d_map, &r->map_cap, nl * nvert * (prec ? 2 : sizeof(float)),
                                  "allocating map");
   if (s != BEAMS_OK) return s;
   r->map_valid = false;
@@ -304,9 +319,17 @@ beams_status build_map(beams_renderer* r, const ExactGeo& g, int& launches, bool
                                                 r->stream, nullptr, 0, -1, nullptr, occ);
   if (e != cudaSuccess) return cuda_fail(r, e, "light_march launch");
   ++launches;
+  for (int l = 1; l < nl; ++l) {
+    ExactGeo gl = g;
+    geo_set_light(gl, r->lights[l]);
+    e = launch_light_march_f32(gl, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map + (size_t)l * nvert,
+                               r->d_cnt, r->stream, nullptr, 0, -1, nullptr, occ);
+    if (e != cudaSuccess) return cuda_fail(r, e, "light_march launch");
+    ++launches;
+  }
   r->map_key = key;
   r->map_valid = true;
-  r->map_count = nvert;
+  r->map_count = nl * nvert;
   r->map_is_half = prec;
   built = true;
   return BEAMS_OK;
@@ -328,6 +351,12 @@ beams_status mlp_render_view(beams_renderer* r, const ExactGeo& g, float4* out, 
 bool mlp_ready(const beams_renderer* r);
 
 beams_status check_ready(beams_renderer* r) {
+  if (r->multi_light && r->lights.size() > 1) {
+    if (r->brick_mode || r->form != BEAMS_FORM_EXACT || (r->has_volume && r->vol.assoc != BEAMS_ASSOC_POINTS))
+      return fail(r, BEAMS_ERR_UNSUPPORTED, "several lights render in the exact form of a point volume only");
+    if ((int)r->lights.size() > kMaxMultiLights)
+      return fail(r, BEAMS_ERR_UNSUPPORTED, "at most 8 lights in the multi-light extension");
+  }
   if (r->brick_mode) {
     if (r->bricks.empty()) return fail(r, BEAMS_ERR_STATE, "no bricks set (beams_set_bricks)");
     if (r->tf_n < 1) return fail(r, BEAMS_ERR_STATE, "no colour map set (beams_set_color_map)");
@@ -689,6 +718,12 @@ beams_status beams_set_light_steps(beams_renderer* r, float steps) {
 beams_status beams_set_slab_fp64(beams_renderer* r, int enable) {
   if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
   r->slab_fp64 = enable != 0;
+  return BEAMS_OK;
+}
+
+beams_status beams_set_multi_light(beams_renderer* r, int enable) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  r->multi_light = enable != 0;
   return BEAMS_OK;
 }
 

@@ -49,7 +49,13 @@ struct ExactGeo {
   int light_brick_log2;
   // Occupancy of 8^3-cell macro-cells (empty-space skipping): counts per axis.
   int occ_n[3];
+  // The multi-light extension: n_lights maps, map l at map + l * (M+1)^3, the
+  // view march shading by sum_l T_l * light_colors[l] (n_lights <= 1: light 0 only).
+  int n_lights;
+  float light_colors[8][3];
 };
+
+constexpr int kMaxMultiLights = 8;
 
 constexpr int kMacroLog2 = 3;  // macro-cell edge = 8 field cells
 

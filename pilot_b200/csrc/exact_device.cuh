@@ -335,6 +335,35 @@ __device__ __forceinline__ float map_interp_t(const ExactGeo& g, const float4* M
   return hex_interp(v, pc[0], pc[1], pc[2]);
 }
 
+// The multi-light shading term at p: sum over the maps of (1 - opacity_l) *
+// light_colors[l], in light order. The cell and parametric coordinates are the
+// same for every map (one map grid), so they are located once.
+__device__ __forceinline__ void map_light_sum(const ExactGeo& g, const float4* MT, const float* __restrict__ map,
+                                              const float p[3], float est[3]) {
+  int c[3];
+  float pc[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float t = (p[d] - g.morig[d]) * g.minv[d];
+    c[d] = trunc_small(fminf(fmaxf(t, 0.f), (float)(g.pd[d] - 2)));
+    const float4 e = MT[g.max_off[d] + c[d]];
+    pc[d] = div_rn_markstein(p[d] - e.x, e.z, e.w);
+  }
+  const unsigned px = (unsigned)g.pd[0], pxy = (unsigned)g.pd[0] * (unsigned)g.pd[1];
+  const size_t nv = (size_t)pxy * (unsigned)g.pd[2];
+  const float* m = map + ((unsigned)c[2] * pxy + (unsigned)c[1] * px + (unsigned)c[0]);
+  for (int l = 0; l < g.n_lights; ++l, m += nv) {
+    const float v[8] = {__ldg(m), __ldg(m + 1), __ldg(m + 1 + px), __ldg(m + px),
+                        __ldg(m + pxy), __ldg(m + pxy + 1), __ldg(m + pxy + 1 + px), __ldg(m + pxy + px)};
+    const float tr = 1.f - hex_interp(v, pc[0], pc[1], pc[2]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float t = tr * g.light_colors[l][d];
+      est[d] = (l == 0) ? t : est[d] + t;
+    }
+  }
+}
+
 // Quad layout of a point field: Q[z][y][x] = {f(x,y,z), f(x+1,y,z), f(x,y+1,z),
 // f(x+1,y+1,z)} for x < nx-1, y < ny-1, so one cell is two 16-byte loads
 // (z and z+1). VTK corner order 0..7 = lo.x lo.y lo.w lo.z hi.x hi.y hi.w hi.z.

@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
 // ---------------------------------------------------------------------------
 // K2 (point field)
 // ---------------------------------------------------------------------------
-template <typename QuadT, bool USE_MAP, typename MapT, bool LIST = false, bool SKIP = false>
+template <typename QuadT, bool USE_MAP, typename MapT, bool LIST = false, bool SKIP = false, bool MULTI = false>
 __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const QuadT* __restrict__ quads,
                                                          const float4* __restrict__ tab,
                                                          const float4* __restrict__ tf,
@@ -163,8 +163,8 @@ __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const
     }
     if (x < g.width && y < g.height) {
       float4 color;
-      view_march_pixel<QuadT, USE_MAP, MapT, NoRecord, SKIP>(g, quads, s_tab, s_tf, map, x, y, color, lit, hit,
-                                                              nullptr, occ);
+      view_march_pixel<QuadT, USE_MAP, MapT, NoRecord, SKIP, MULTI>(g, quads, s_tab, s_tf, map, x, y, color, lit,
+                                                                     hit, nullptr, occ);
       out[(size_t)y * g.width + x] = color;
     }
   }
@@ -568,6 +568,12 @@ cudaError_t launch_view_march_f32(const ExactGeo& g, const float* field, const f
     e = persistent_grid(k_view_march_cells<float>, smem, ntiles, grid);
     if (e != cudaSuccess) return e;
     k_view_march_cells<float><<<grid, kThreads, smem, st>>>(g, field, tab, tf, out, cnt);
+  } else if (g.use_map && g.n_lights > 1) {
+    // the multi-light extension (empty-space skipping is not combined with it)
+    e = persistent_grid(k_view_march<float4, true, float, false, false, true>, smem, ntiles, grid);
+    if (e != cudaSuccess) return e;
+    k_view_march<float4, true, float, false, false, true><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, map, out,
+                                                                                        cnt);
   } else if (g.use_map) {
     return launch_k2<float4, true, float>(g, quads, tab, tf, map, out, cnt, occ, st);
   } else {

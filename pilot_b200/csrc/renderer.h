@@ -64,6 +64,9 @@ struct MapKey {
   int form;
   int light_kind;
   double light[3];
+  int n_lights;          // the multi-light extension: lights 1.. below
+  int extra_kind[8];
+  double extra[8][3];
 };
 
 }  // namespace beams
@@ -131,6 +134,7 @@ struct beams_renderer {
   unsigned long long occ_key[2] = {~0ull, ~0ull};  // quads key, tf_version
   int empty_skip = 1;  // map build skips empty macro-cells
   int view_skip = 1;   // view march skips empty macro-cells
+  int multi_light = 0; // beams_set_multi_light: shade by every light (one map each)
 
   // multi-block scene (beams_set_bricks)
   std::vector<beams::Brick> bricks;

@@ -31,7 +31,7 @@ struct NoRecord {
 // SKIP: samples in macro-cells whose occupancy is 0 (every value there maps to
 // an in-range TF entry of alpha 0) only advance and count as lit: their
 // premultiplied alpha is 0, so they change neither colour nor alpha.
-template <typename QuadT, bool USE_MAP, typename MapT, typename Rec = NoRecord, bool SKIP = false>
+template <typename QuadT, bool USE_MAP, typename MapT, typename Rec = NoRecord, bool SKIP = false, bool MULTI = false>
 __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT* __restrict__ quads,
                                                  const float4* s_tab, const float4* s_tf,
                                                  const MapT* __restrict__ map, int x, int y, float4& color,
@@ -118,7 +118,13 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT*
       float sc0 = tfc.x, sc1 = tfc.y, sc2 = tfc.z;
       const float sa = tfc.w * (1.f - color.w);
       if (rec) (*rec)(p, tfc, sa);
-      if (USE_MAP) {
+      if (USE_MAP && MULTI) {
+        float est[3];
+        map_light_sum(g, s_tab, (const float*)map, p, est);
+        sc0 = sc0 * est[0];
+        sc1 = sc1 * est[1];
+        sc2 = sc2 * est[2];
+      } else if (USE_MAP) {
         // exact form: 1 - opacity (TransmittanceMap.h:195); precision form: stored transmittance
         const float mv = map_interp_t<MapT>(g, s_tab, map, p);
         const float tr = (sizeof(MapT) == 2) ? mv : 1.f - mv;

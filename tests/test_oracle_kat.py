@@ -159,3 +159,38 @@ def test_oracle_rejects_bad_scene():
     s.light_steps = 0
     with pytest.raises(RuntimeError):
         Oracle(s).light_march()
+
+
+def _light_color(s):
+    return np.float32(s.light_color) * np.float32(s.light_intensity)
+
+
+def test_multi_light_with_dark_second_light_equals_single_light():
+    """Multi-light extension: a second light of colour 0 adds exact zeros, so the
+    image equals the first-light-only image bit for bit."""
+    s = scenes.small(6, n=24, image=32, m=12)
+    o = Oracle(s)
+    m0, _ = o.light_march()
+    single, lit1 = o.view_march(m0)
+    lc = np.stack([_light_color(s), np.zeros(3, np.float32)])
+    multi, lit2 = o.view_march_multi(np.stack([m0, np.ones_like(m0)]), lc)
+    assert np.array_equal(single, multi) and lit1 == lit2
+
+
+def test_multi_light_two_half_lights_equal_one_full_light():
+    """Halving a light's intensity scales every term by 2^-1 exactly, so two
+    identical half-intensity lights sum to the full-intensity shading bit for bit."""
+    s = scenes.small(7, n=24, image=32, m=12, light_kind=1)
+    o = Oracle(s)
+    m0, _ = o.light_march()
+    single, _ = o.view_march(m0)
+    half = _light_color(s) * np.float32(0.5)
+    multi, _ = o.view_march_multi(np.stack([m0, m0]), np.stack([half, half]))
+    assert np.array_equal(single, multi)
+
+
+def test_multi_light_oracle_rejects_mismatched_inputs():
+    s = scenes.small(0, n=16, image=8, m=4)
+    m0, _ = Oracle(s).light_march()
+    with pytest.raises(ValueError):
+        Oracle(s).view_march_multi(np.stack([m0, m0]), np.ones((3, 3), np.float32))

@@ -21,11 +21,13 @@ struct BatchDesc {
   int tiles_x;                // view tiles per image row
 };
 
-// Work items, in queue order: the map-build items of request 0, then for
-// r = 1..n-1 the map-build items of r followed by the view items of r-1, and
-// last the view items of n-1. A view item of r waits for r's map items, which
+// Work items, in queue order over the request order o (requests grouped by
+// volume, most work first): the map-build items of o0, then for k = 1..n-1
+// the map-build items of o_k followed by the view items of o_{k-1}, and last
+// the view items of o_{n-1}. A view item of r waits for r's map items, which
 // all precede it in the queue; r's map is then one request old, so it is
-// still in L2 when its view tiles read it. Segment k covers items
+// still in L2 when its view tiles read it, and the map build beside them
+// reads the same volume. Segment k covers items
 // [seg_off[k], seg_off[k+1]) of request seg_req[k] & 0xffff, phase 2 (view)
 // when bit 16 is set. Lives in device memory (uploaded when the batch's shapes change).
 struct BatchPlan {

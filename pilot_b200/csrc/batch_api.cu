@@ -283,7 +283,22 @@ beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, in
       k2[i] = tx * ty;
       b->max_ntab = std::max(b->max_ntab, (size_t)g.ntab);
     }
-    // queue: K1(0), then K1(r) and K2(r-1) for r = 1..n-1, then K2(n-1)
+    // Queue order o[0..n-1]: requests grouped by volume, so that the map build
+    // of o[k] and the view march of o[k-1] that runs beside it read the same
+    // field through L2; groups with the most work first, so the small requests
+    // fill the tail of the launch. Then K1(o0), K1(o_k) and K2(o_{k-1}) for
+    // k = 1..n-1, K2(o_{n-1}).
+    std::vector<int> o(n);
+    std::vector<double> vwork(b->vols.size(), 0.0);
+    for (int i = 0; i < n; ++i) {
+      o[i] = i;
+      vwork[reqs[i].volume] += (double)P.k1_items[i] + (double)k2[i];
+    }
+    std::stable_sort(o.begin(), o.end(), [&](int a, int c) {
+      const int va = reqs[a].volume, vc = reqs[c].volume;
+      if (va != vc) return vwork[va] != vwork[vc] ? vwork[va] > vwork[vc] : va < vc;
+      return false;
+    });
     int items = 0;
     auto seg = [&](int req, int phase, int count) {
       P.seg_off[P.nseg] = items;
@@ -291,11 +306,11 @@ beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, in
       ++P.nseg;
       items += count;
     };
-    for (int i = 0; i < n; ++i) {
-      seg(i, 1, P.k1_items[i]);
-      if (i > 0) seg(i - 1, 2, k2[i - 1]);
+    for (int k = 0; k < n; ++k) {
+      seg(o[k], 1, P.k1_items[o[k]]);
+      if (k > 0) seg(o[k - 1], 2, k2[o[k - 1]]);
     }
-    seg(n - 1, 2, k2[n - 1]);
+    seg(o[n - 1], 2, k2[o[n - 1]]);
     P.seg_off[P.nseg] = items;
     P.total = items;
     s = ensure_buffer(r, &b->arena, &b->arena_cap, std::max(off, (size_t)256), "allocating batch arena");

@@ -148,9 +148,33 @@ beams_status beams_set_slab_fp64(beams_renderer* r, int enable);
 /* Keep the last map when its inputs (volume, colour map, light, map size) did not
  * change. Off by default: the reference rebuilds the map every frame. */
 beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable);
-/* Replaces MapperLightedVolume::SetCompositeBackground (MapperLightedVolume.cxx:321-324):
- * blend rgb over an opaque background colour after compositing. Off by default. */
+/* Replaces MapperLightedVolume::SetCompositeBackground (MapperLightedVolume.cxx:321-324)
+ * and the Canvas::BlendBackground call it enables (:185-188): after the image is
+ * complete (composite included), the premultiplied image is placed over the
+ * background colour (Porter-Duff over: a = bg.a (1 - C.a), C.rgb += bg.rgb a,
+ * C.a += a; pixels with C.a >= 1 unchanged), on the device. Off by default. */
 beams_status beams_set_background(beams_renderer* r, int enable, const float rgba[4]);
+
+/* Canvas depth clipping. Replaces the canvas depth buffer that
+ * RayOperations::MapCanvasToRays turns into each camera ray's MaxDistance before
+ * the slab test narrows it (MapperLightedVolume.cxx:151-152,
+ * LightedVolumeRenderer.cxx:644-718). depth holds width x height floats in the
+ * image's pixel order (row y at y * width, row 0 at the bottom):
+ *   BEAMS_DEPTH_RAY_DISTANCE  the limit itself, a distance along the normalised
+ *                             ray from the camera (NaN or +inf: no limit);
+ *   BEAMS_DEPTH_WINDOW        OpenGL window depth in [0, 1] under the camera's
+ *                             perspective with near_plane / far_plane, unprojected
+ *                             at the pixel centre (1 = far plane; NaN reads as 1).
+ * Every render whose camera has this width and height is clipped (others fail
+ * with BEAMS_ERR_INVALID_ARG) until the buffer is cleared with depth = NULL.
+ * The buffer is copied; on_device says where depth lives. */
+#define BEAMS_DEPTH_RAY_DISTANCE 0
+#define BEAMS_DEPTH_WINDOW 1
+beams_status beams_set_depth_buffer(beams_renderer* r, const float* depth, int width, int height, int kind,
+                                    double near_plane, double far_plane, int on_device);
+/* The per-pixel ray limits the current depth buffer gives for camera cam
+ * (width x height floats). Synchronises. */
+beams_status beams_get_ray_limits(beams_renderer* r, const beams_camera* cam, float* dst, int dst_on_device);
 /* The multi-light extension (the reference's notes.txt:4 "use multiple lights";
  * its renderer uses Locations[0] only, TransmittanceMap.h:591-592, which stays the
  * default): with enable != 0 and more than one light, the exact form builds one

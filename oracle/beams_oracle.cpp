@@ -86,6 +86,7 @@ struct Geo {
   int n_lights = 1;
   int64_t map_nv = 0;
   std::vector<T> lcols;
+  const float* ray_max = nullptr;  // canvas depth clipping, per pixel (width * height)
   T extent_mag;                 // BoundsMagnitude, Math.h:13-21
   T sd, mesh_eps, step, cutoff;
   int light_kind;
@@ -151,6 +152,7 @@ void build_geo(const oracle_scene* s, Geo<T>& g) {
   g.use_map = s->use_map;
   g.slab_fp64 = s->slab_fp64;
   g.precision = s->precision;
+  g.ray_max = s->ray_max;
   g.tau.resize(s->tf_n);
   {
     float ma = 0.f;  // float32 max alpha, as the device derives it
@@ -471,17 +473,19 @@ bool slab(const S o[3], const S d[3], const double bmin[3], const double bmax[3]
 template <typename T>
 bool ray_setup(const Geo<T>& g, int x, int y, T o[3], T d[3], T& minD, T& maxD) {
   camera_ray(g, x, y, o, d);
+  // MaxDistance enters as the pixel's canvas limit (+inf without a depth buffer)
+  const float lim = g.ray_max ? g.ray_max[(int64_t)y * g.width + x] : std::numeric_limits<float>::infinity();
   if (sizeof(T) == 4 && g.slab_fp64) {
     double od[3] = {(double)o[0], (double)o[1], (double)o[2]};
     double dd[3] = {(double)d[0], (double)d[1], (double)d[2]};
-    double lo = 0.0, hi = std::numeric_limits<double>::infinity();
+    double lo = 0.0, hi = (double)lim;
     const bool hit = slab(od, dd, g.bmin, g.bmax, lo, hi);
     minD = (T)lo;
     maxD = (T)hi;
     return hit;
   }
   minD = T(0);
-  maxD = std::numeric_limits<T>::infinity();
+  maxD = (T)lim;
   return slab(o, d, g.bmin, g.bmax, minD, maxD);
 }
 
@@ -957,6 +961,26 @@ int oracle_view_march_f32(const oracle_scene* s, const float* map, int x0, int y
 int oracle_view_march_f64(const oracle_scene* s, const double* map, int x0, int y0, int w, int h,
                           double* rgba, int threads, uint64_t* lit) {
   return view_march<double>(s, map, x0, y0, w, h, rgba, threads, lit);
+}
+
+int oracle_window_depth_to_distance(const oracle_scene* s, const float* depth, double near_plane,
+                                    double far_plane, double* out) {
+  if (!valid(s) || !depth || !out || !(near_plane > 0.0) || !(far_plane > near_plane)) return 1;
+  Geo<double> g;
+  build_geo(s, g);
+  for (int y = 0; y < g.height; ++y)
+    for (int x = 0; x < g.width; ++x) {
+      const int64_t i = (int64_t)y * g.width + x;
+      double dw = (double)depth[i];
+      dw = (dw == dw) ? std::min(std::max(dw, 0.0), 1.0) : 1.0;
+      const double z = 2.0 * dw - 1.0;
+      const double t = 2.0 * far_plane * near_plane / ((far_plane + near_plane) - z * (far_plane - near_plane));
+      const double sx = ((double)x + 0.5) * g.kx - g.cx, sy = ((double)y + 0.5) * g.ky - g.cy;
+      double v[3];
+      for (int k = 0; k < 3; ++k) v[k] = (g.cf[k] + sx * g.cr[k]) + sy * g.cu[k];
+      out[i] = t * std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    }
+  return 0;
 }
 
 // Multi-light extension: maps holds n_lights exact-form maps stacked in light

@@ -52,6 +52,10 @@ typedef struct oracle_scene {
    * cuts the ray), the map stores transmittance T = exp(-tau) rounded to IEEE
    * binary16, and the view march shades by the interpolated T. */
   int precision;
+  /* Canvas depth clipping: width x height per-pixel limits on the camera ray's
+   * distance (row y at y * width), the slab test's initial MaxDistance; NULL:
+   * no limit (MapperLightedVolume.cxx:151-152, LightedVolumeRenderer.cxx:644-718). */
+  const float* ray_max;
 } oracle_scene;
 
 /* Light march over every map vertex ((M+1)^3, x fastest). */
@@ -75,6 +79,12 @@ int oracle_view_march_f32(const oracle_scene* s, const float* map, int x0, int y
                           float* rgba_out, int threads, uint64_t* lit_samples);
 int oracle_view_march_f64(const oracle_scene* s, const double* map, int x0, int y0, int w, int h,
                           double* rgba_out, int threads, uint64_t* lit_samples);
+/* Per-pixel ray limits of a window-depth buffer (OpenGL depth in [0, 1] under
+ * the camera's perspective with near/far planes, unprojected at the pixel
+ * centre: t = 2fn / ((f + n) - (2d - 1)(f - n)) times the length of the
+ * un-normalised camera ray), in double. */
+int oracle_window_depth_to_distance(const oracle_scene* s, const float* depth, double near_plane,
+                                    double far_plane, double* out);
 /* Multi-light extension: n_lights exact-form maps stacked in light order, shaded
  * with sum_l (1 - opacity_l) * light_colors[l] (colour * intensity, float32). */
 int oracle_view_march_multi_f32(const oracle_scene* s, const float* maps, int n_lights, const float* light_colors,

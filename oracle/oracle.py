@@ -25,7 +25,7 @@ class OracleScene(C.Structure):
                 ("sample_distance", C.c_float), ("alpha_cutoff", C.c_float), ("light_steps", C.c_float),
                 ("slab_fp64", C.c_int), ("cam_pos", C.c_double * 3), ("cam_look", C.c_double * 3),
                 ("cam_up", C.c_double * 3), ("fov_y_deg", C.c_double), ("width", C.c_int), ("height", C.c_int),
-                ("precision", C.c_int)]
+                ("precision", C.c_int), ("ray_max", C.c_void_p)]
 
 
 def lib():
@@ -45,6 +45,7 @@ def lib():
             "oracle_view_march_f32": [S, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
             "oracle_view_march_f64": [S, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
             "oracle_view_march_lazy_f64": [S, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
+            "oracle_window_depth_to_distance": [S, P, C.c_double, C.c_double, P],
             "oracle_view_march_multi_f32": [S, P, C.c_int, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int,
                                             u64p],
             "oracle_ray_setup_f32": [S, C.c_int, C.c_int, P],
@@ -84,6 +85,19 @@ class Oracle:
             (C.c_int * 3)(s.map_m, s.map_m, s.map_m), int(s.use_map), s.sample_distance, s.cutoff,
             s.light_steps, int(s.slab_fp64), (C.c_double * 3)(*s.cam_pos), (C.c_double * 3)(*s.cam_look),
             (C.c_double * 3)(*s.cam_up), s.fov_y_deg, s.width, s.height, int(precision))
+
+    def set_ray_limits(self, limits):
+        """Canvas depth clipping: (height, width) float32 per-pixel ray limits, or None."""
+        self._ray_max = None if limits is None else np.ascontiguousarray(limits, np.float32)
+        self.cs.ray_max = None if limits is None else self._ray_max.ctypes.data
+
+    def window_depth_to_distance(self, depth, near, far):
+        """Per-pixel ray limits (float64) of an OpenGL window-depth buffer under this camera."""
+        d = np.ascontiguousarray(depth, np.float32)
+        out = np.empty(d.shape, np.float64)
+        if lib().oracle_window_depth_to_distance(C.byref(self.cs), _p(d), float(near), float(far), _p(out)):
+            raise RuntimeError("oracle depth conversion rejected its input")
+        return out
 
     @property
     def map_shape(self):
@@ -178,10 +192,13 @@ class Oracle:
         return out
 
 
-def render_bricks(bricks, fp64: bool = False, threads: int = 0):
-    """Multi-block render of a list of brick scenes (scenes.split_bricks).
+def render_bricks(bricks, fp64: bool = False, threads: int = 0, ray_limits=None):
+    """Multi-block render of a list of brick scenes (scenes.split_bricks), with
+    optional per-pixel ray limits (canvas depth clipping) shared by all bricks.
     Returns (rgba, brick_images, local_maps, final_maps, lit)."""
     orcs = [Oracle(b, threads=threads) for b in bricks]
+    for o in orcs:
+        o.set_ray_limits(ray_limits)
     arr = (OracleScene * len(bricks))(*[o.cs for o in orcs])
     dt = np.float64 if fp64 else np.float32
     W, H = bricks[0].width, bricks[0].height
@@ -252,3 +269,17 @@ def quantize(field: np.ndarray, dtype: str) -> np.ndarray:
 def psnr(a: np.ndarray, b: np.ndarray) -> float:
     mse = float(np.mean((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2))
     return float("inf") if mse == 0 else 10.0 * np.log10(1.0 / mse)
+
+
+def blend_background(img, bg):
+    """Porter-Duff "over" of a premultiplied float32 RGBA image over the colour bg
+    (a = bg.a (1 - C.a), C.rgb += bg.rgb a, C.a += a; pixels with C.a >= 1 kept),
+    in float32 with one rounding per operation."""
+    out = np.array(img, np.float32, copy=True)
+    b = np.asarray(bg, np.float32)
+    m = out[..., 3] < np.float32(1)
+    a = b[3] * (np.float32(1) - out[..., 3])
+    for k in range(3):
+        out[..., k] = np.where(m, out[..., k] + b[k] * a, out[..., k])
+    out[..., 3] = np.where(m, a + out[..., 3], out[..., 3])
+    return out

@@ -25,6 +25,7 @@ STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "UNSUPPORTED", 3: "CUDA", 4: "OOM"
 F32, BF16, F16 = 0, 1, 2
 ASSOC_POINTS, ASSOC_CELLS = 0, 1
 FORM_EXACT, FORM_PRECISION, FORM_MLP = 0, 1, 2
+DEPTH_RAY_DISTANCE, DEPTH_WINDOW = 0, 1
 
 
 class MlpOptions(C.Structure):
@@ -189,6 +190,8 @@ def lib():
         "beams_mlp_forward_tc_device": ([P, P, C.c_int, P], C.c_int),
         "beams_set_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "beams_set_multi_light": ([P, C.c_int], C.c_int),
+        "beams_set_depth_buffer": ([P, P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int], C.c_int),
+        "beams_get_ray_limits": ([P, C.POINTER(Camera), P, C.c_int], C.c_int),
         "beams_test_fail_allocation": ([C.c_int], C.c_int),
         "beams_get_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "beams_batch_set_volumes": ([P, P, C.c_int], C.c_int),
@@ -486,6 +489,26 @@ class Renderer:
     def set_background(self, on: bool, rgba=(1, 1, 1, 1)):
         c = (C.c_float * 4)(*rgba)
         self._check(self._L.beams_set_background(self._h, int(bool(on)), c))
+
+    def set_depth_buffer(self, depth, kind=0, near=0.0, far=0.0):
+        """Canvas depth clipping: depth (H, W) float32 numpy or torch CUDA tensor,
+        kind DEPTH_RAY_DISTANCE or DEPTH_WINDOW (with near/far); None clears."""
+        if depth is None:
+            self._check(self._L.beams_set_depth_buffer(self._h, None, 0, 0, 0, 0.0, 0.0, 0))
+            return
+        if isinstance(depth, np.ndarray):
+            depth = np.ascontiguousarray(depth, np.float32)
+            on_dev = 0
+        else:
+            on_dev = int(depth.is_cuda)
+        h, w = depth.shape
+        self._check(self._L.beams_set_depth_buffer(self._h, _ptr(depth), int(w), int(h), int(kind), float(near),
+                                                   float(far), on_dev))
+
+    def get_ray_limits(self, cam):
+        out = np.empty((cam.height, cam.width), np.float32)
+        self._check(self._L.beams_get_ray_limits(self._h, C.byref(cam), _ptr(out), 0))
+        return out
 
     def set_multi_light(self, enable: bool):
         self._check(self._L.beams_set_multi_light(self._h, int(bool(enable))))

@@ -445,6 +445,9 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
     }
   }
   cudaEventRecord(r->ev[1], r->stream);
+  s = prepare_ray_limits(r, G[0], launches);  // one camera: the same limits for every brick
+  if (s != BEAMS_OK) return s;
+  for (int b = 1; b < nb; ++b) G[b].ray_max = G[0].ray_max;
   for (int b = 0; b < nb; ++b) {
     Brick& B = r->bricks[b];
     e = cudaMemsetAsync(&r->d_cnt->tiles_view, 0, sizeof(unsigned), r->stream);
@@ -488,6 +491,8 @@ beams_status render_bricks_frame(beams_renderer* r, const beams_camera* cam, flo
     dst = r->d_rgba;
   }
   s = render_bricks(r, cam, dst, launches);
+  if (s != BEAMS_OK) return s;
+  s = blend_background(r, dst, npix, launches);
   if (s != BEAMS_OK) return s;
   cudaError_t e;
   if (!direct) {
@@ -999,6 +1004,8 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
     if (s != BEAMS_OK) return s;
     dst = r->d_rgba;
   }
+  s = prepare_ray_limits(r, g, launches);
+  if (s != BEAMS_OK) return s;
   if (use_mlp) {
     s = mlp_render_view(r, g, dst, launches);
     if (s != BEAMS_OK) return s;
@@ -1021,6 +1028,8 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
   if (e != cudaSuccess) return cuda_fail(r, e, "view_march launch");
   ++launches;
   cudaEventRecord(r->ev[2], r->stream);
+  s = blend_background(r, dst, npix, launches);
+  if (s != BEAMS_OK) return s;
   if (!direct) {
     e = cudaMemcpyAsync(rgba_out, dst, npix * sizeof(float4),
                         out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, r->stream);

@@ -53,6 +53,11 @@ struct ExactGeo {
   // view march shading by sum_l T_l * light_colors[l] (n_lights <= 1: light 0 only).
   int n_lights;
   float light_colors[8][3];
+  // Canvas depth clipping: per-pixel limit on each camera ray's distance
+  // (width * height floats, row y at y * width), the MaxDistance that
+  // MapCanvasToRays hands the slab test (MapperLightedVolume.cxx:151-152).
+  // Null: no limit.
+  const float* ray_max;
 };
 
 constexpr int kMaxMultiLights = 8;

@@ -277,20 +277,23 @@ __device__ __forceinline__ bool slab_t(const S o[3], const S d[3], const double 
   return !(maxD < minD);
 }
 
+// The ray enters with MinDistance 0 and MaxDistance +inf, or the canvas depth
+// limit of its pixel when one is set; the slab test narrows both.
 __device__ __forceinline__ bool ray_setup(const ExactGeo& g, int x, int y, float o[3], float d[3],
                                           float& minD, float& maxD) {
   camera_ray(g, x, y, o, d);
+  const float lim = g.ray_max ? __ldg(g.ray_max + (size_t)y * g.width + x) : __int_as_float(0x7f800000);
   if (g.slab_fp64) {
     const double od[3] = {(double)o[0], (double)o[1], (double)o[2]};
     const double dd[3] = {(double)d[0], (double)d[1], (double)d[2]};
-    double lo = 0.0, hi = __longlong_as_double(0x7ff0000000000000ull);
+    double lo = 0.0, hi = (double)lim;
     const bool hit = slab_t<double>(od, dd, g.bmin, g.bmax, lo, hi);
     minD = (float)lo;
     maxD = (float)hi;
     return hit;
   }
   minD = 0.f;
-  maxD = __int_as_float(0x7f800000);
+  maxD = lim;
   return slab_t<float>(o, d, g.bmin, g.bmax, minD, maxD);
 }
 

@@ -105,6 +105,14 @@ struct beams_renderer {
   bool reuse_map = false;
   bool bg = false;
   float bg_rgba[4] = {1.f, 1.f, 1.f, 1.f};
+  // canvas depth buffer (beams_set_depth_buffer) and the per-pixel ray limits derived from it
+  bool depth_set = false;
+  int depth_w = 0, depth_h = 0, depth_kind = 0;
+  double depth_near = 0.0, depth_far = 0.0;
+  float* d_depth = nullptr;
+  size_t depth_cap = 0;
+  float* d_raymax = nullptr;
+  size_t raymax_cap = 0;
   int form = BEAMS_FORM_EXACT;
 
   // transmittance map
@@ -165,6 +173,8 @@ struct beams_renderer {
     if (d_occ) cudaFree(d_occ);
     if (d_tau) cudaFree(d_tau);
     if (d_rgba) cudaFree(d_rgba);
+    if (d_depth) cudaFree(d_depth);
+    if (d_raymax) cudaFree(d_raymax);
     for (auto& b : bricks) b.release();
     if (d_refs) cudaFree(d_refs);
     if (d_brick_imgs) cudaFree(d_brick_imgs);
@@ -180,6 +190,8 @@ void batch_release(beams_renderer* r);
 beams_status fail(beams_renderer* r, beams_status s, const std::string& msg);
 beams_status cuda_fail(beams_renderer* r, cudaError_t e, const char* what);
 beams_status ensure_buffer(beams_renderer* r, void** buf, size_t* cap, size_t bytes, const char* what);
+beams_status prepare_ray_limits(beams_renderer* r, ExactGeo& g, int& launches);
+beams_status blend_background(beams_renderer* r, float4* img, size_t npix, int& launches);
 }  // namespace beams
 
 inline beams_renderer::~beams_renderer() {

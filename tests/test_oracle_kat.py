@@ -194,3 +194,63 @@ def test_multi_light_oracle_rejects_mismatched_inputs():
     m0, _ = Oracle(s).light_march()
     with pytest.raises(ValueError):
         Oracle(s).view_march_multi(np.stack([m0, m0]), np.ones((3, 3), np.float32))
+
+
+def _camera_ray_lengths(s):
+    """|forward + sx right + sy up| per pixel centre, from the camera alone (float64)."""
+    p, l, u = (np.asarray(v, np.float64) for v in (s.cam_pos, s.cam_look, s.cam_up))
+    f = (l - p) / np.linalg.norm(l - p)
+    r = np.cross(f, u)
+    r /= np.linalg.norm(r)
+    up = np.cross(r, f)
+    th = np.tan(np.radians(s.fov_y_deg) / 2)
+    aspect = s.width / s.height
+    sx = ((np.arange(s.width) + 0.5) * (2 * th * aspect / s.width) - th * aspect)[None, :]
+    sy = ((np.arange(s.height) + 0.5) * (2 * th / s.height) - th)[:, None]
+    v = f[None, None, :] + sx[..., None] * r[None, None, :] + sy[..., None] * up[None, None, :]
+    return np.linalg.norm(v, axis=-1)
+
+
+def test_window_depth_of_a_view_plane_unprojects_to_its_distance():
+    """A plane at view depth t0 has window depth ((f+n) - 2fn/t0)/(f-n) mapped to
+    [0, 1]; unprojected, each pixel's limit is t0 times its ray's length."""
+    s = scenes.small(0, n=16, image=24, m=4)
+    n, f, t0 = 0.1, 10.0, 1.3
+    z = ((f + n) - 2 * f * n / t0) / (f - n)
+    depth = np.full((s.height, s.width), (z + 1) / 2, np.float32)
+    got = Oracle(s).window_depth_to_distance(depth, n, f)
+    want = t0 * _camera_ray_lengths(s)
+    assert np.max(np.abs(got - want) / want) < 1e-5  # depth was rounded to float32
+    # d = 1 is the far plane, d = 0 the near plane, NaN reads as 1
+    depth[0, 0], depth[0, 1], depth[0, 2] = 1.0, 0.0, np.nan
+    got = Oracle(s).window_depth_to_distance(depth, n, f)
+    L = _camera_ray_lengths(s)[0]
+    assert np.allclose(got[0, :3], [f * L[0], n * L[1], f * L[2]], rtol=1e-12)
+
+
+def test_ray_limits_clip_the_view_march():
+    s = scenes.small(2, n=24, image=32, m=8)
+    o = Oracle(s)
+    m, _ = o.light_march()
+    full, lit_full = o.view_march(m)
+    o.set_ray_limits(np.full((s.height, s.width), np.inf, np.float32))
+    same, lit_same = o.view_march(m)
+    assert np.array_equal(full, same) and lit_full == lit_same
+    o.set_ray_limits(np.zeros((s.height, s.width), np.float32))  # every ray ends at the camera
+    none, lit_none = o.view_march(m)
+    assert not none.any() and lit_none == 0
+    # a limit half-way through the volume composites a prefix of each ray's samples
+    cam_to_centre = np.linalg.norm(np.asarray(s.cam_pos) - 0.5)
+    o.set_ray_limits(np.full((s.height, s.width), cam_to_centre, np.float32))
+    half, lit_half = o.view_march(m)
+    assert 0 < lit_half < lit_full
+    assert np.all(half[..., 3] <= full[..., 3] + 1e-6)
+
+
+def test_background_blend_is_over():
+    from oracle.oracle import blend_background
+    img = np.array([[[0, 0, 0, 0], [0.2, 0.1, 0.0, 0.5], [0.3, 0.3, 0.3, 1.0]]], np.float32)
+    out = blend_background(img, (1.0, 0.5, 0.25, 0.8))
+    assert np.allclose(out[0, 0], [0.8, 0.4, 0.2, 0.8])
+    assert np.allclose(out[0, 1], [0.2 + 0.4, 0.1 + 0.2, 0.1, 0.5 + 0.4])
+    assert np.array_equal(out[0, 2], img[0, 2])

@@ -73,6 +73,17 @@ class MapperLightedVolume {
   void SetCompositeBackground(bool on, std::array<float, 4> rgba = {1, 1, 1, 1}) {
     check(beams_set_background(r_, on ? 1 : 0, rgba.data()), r_);
   }
+  // The canvas depth buffer MapCanvasToRays reads (MapperLightedVolume.cxx:151-152):
+  // OpenGL window depth in [0, 1] with the camera's near/far planes, row 0 at the
+  // bottom; an empty vector removes it.
+  void SetCanvasDepth(const std::vector<float>& depth, int width, int height, double near_plane, double far_plane) {
+    if (depth.empty()) {
+      check(beams_set_depth_buffer(r_, nullptr, 0, 0, 0, 0.0, 0.0, 0), r_);
+      return;
+    }
+    if (depth.size() != (size_t)width * height) throw Error(BEAMS_ERR_INVALID_ARG, "depth buffer size");
+    check(beams_set_depth_buffer(r_, depth.data(), width, height, BEAMS_DEPTH_WINDOW, near_plane, far_plane, 0), r_);
+  }
   void SetDensityScale(float s) { density_scale_ = s; }  // stored, never read (as in the reference)
   // SetActiveColorTable: the colour table already sampled to RGBA entries.
   void SetActiveColorTable(const std::vector<float>& rgba) {

@@ -333,10 +333,22 @@ beams_status beams_mlp_load(beams_renderer* r, const char* path);
 /* ---- render --------------------------------------------------------------- */
 /* Replaces MapperLightedVolume::RenderCells (MapperLightedVolume.cxx:114-193):
  * map build (Phase 1/3) + view march (Phase 4) + copy-out (Phase 5).
- * rgba_out holds width*height*4 floats, premultiplied RGBA, on the host unless
- * out_on_device. t may be NULL (then nothing synchronises). */
+ * rgba_out holds width*height*4 floats, premultiplied RGBA. out_on_device:
+ *   BEAMS_OUT_HOST        host memory; the call returns once the image is there;
+ *   BEAMS_OUT_DEVICE      device memory; the call returns once the work is queued;
+ *   BEAMS_OUT_HOST_ASYNC  pinned host memory; the copy is queued on the renderer's
+ *                         stream and the call returns at once: read the image
+ *                         after beams_synchronize (lets a caller upload the next
+ *                         volume while this frame renders).
+ * t may be NULL; a non-NULL t synchronises. */
+#define BEAMS_OUT_HOST 0
+#define BEAMS_OUT_DEVICE 1
+#define BEAMS_OUT_HOST_ASYNC 2
 beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgba_out,
                           int out_on_device, beams_timings* t);
+/* Waits for everything queued on the renderer's stream; reports an asynchronous
+ * CUDA error of that work. */
+beams_status beams_synchronize(beams_renderer* r);
 
 /* Map access for tests and tools: copies the current (M+1)^3 float32 map
  * (x fastest) to dst (host or device). Returns BEAMS_ERR_STATE before a build. */

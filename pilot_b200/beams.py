@@ -26,6 +26,7 @@ F32, BF16, F16 = 0, 1, 2
 ASSOC_POINTS, ASSOC_CELLS = 0, 1
 FORM_EXACT, FORM_PRECISION, FORM_MLP = 0, 1, 2
 DEPTH_RAY_DISTANCE, DEPTH_WINDOW = 0, 1
+OUT_HOST, OUT_DEVICE, OUT_HOST_ASYNC = 0, 1, 2
 
 
 class MlpOptions(C.Structure):
@@ -192,6 +193,7 @@ def lib():
         "beams_set_multi_light": ([P, C.c_int], C.c_int),
         "beams_set_depth_buffer": ([P, P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int], C.c_int),
         "beams_get_ray_limits": ([P, C.POINTER(Camera), P, C.c_int], C.c_int),
+        "beams_synchronize": ([P], C.c_int),
         "beams_test_fail_allocation": ([C.c_int], C.c_int),
         "beams_get_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "beams_batch_set_volumes": ([P, P, C.c_int], C.c_int),
@@ -549,15 +551,24 @@ class Renderer:
     def camera(position, look_at, up, fov_y_deg, width, height) -> Camera:
         return Camera(_d3(position), _d3(look_at), _d3(up), float(fov_y_deg), int(width), int(height))
 
-    def render(self, cam: Camera, out=None, timings=True):
-        """Renders into out (numpy (H,W,4) float32 host array or torch CUDA tensor)."""
+    def render(self, cam: Camera, out=None, timings=True, host_async=False):
+        """Renders into out (numpy (H,W,4) float32 host array or torch tensor, CUDA
+        or host). host_async with a pinned host tensor queues the copy and returns
+        at once (OUT_HOST_ASYNC): call synchronize() before reading out."""
         if out is None:
             out = np.zeros((cam.height, cam.width, 4), np.float32)
-        on_dev = 0 if isinstance(out, np.ndarray) else int(out.is_cuda)
+        on_dev = OUT_HOST if isinstance(out, np.ndarray) else (OUT_DEVICE if out.is_cuda else OUT_HOST)
+        if host_async:
+            if on_dev != OUT_HOST or isinstance(out, np.ndarray) or not out.is_pinned():
+                raise ValueError("host_async needs a pinned host torch tensor")
+            on_dev = OUT_HOST_ASYNC
         t = Timings() if timings else None
         self._check(self._L.beams_render(self._h, C.byref(cam), _ptr(out), on_dev,
                                          C.byref(t) if t is not None else None))
         return out, (t.as_dict() if t is not None else None)
+
+    def synchronize(self):
+        self._check(self._L.beams_synchronize(self._h))
 
     def build_shadow_map(self, timings=True):
         """Phase 1 only. With timings=False nothing synchronises."""

@@ -483,7 +483,7 @@ beams_status render_bricks_frame(beams_renderer* r, const beams_camera* cam, flo
                                  beams_timings* t, int& launches) {
   const size_t npix = (size_t)cam->width * cam->height;
   float4* dst = (float4*)rgba_out;
-  const bool direct = out_on_device && (((uintptr_t)rgba_out & 15) == 0);
+  const bool direct = out_on_device == BEAMS_OUT_DEVICE && (((uintptr_t)rgba_out & 15) == 0);
   beams_status s;
   if (!direct) {
     s = ensure_buffer(r, (void**)&r->d_rgba, &r->rgba_cap, npix * sizeof(float4), "allocating image");
@@ -497,7 +497,8 @@ beams_status render_bricks_frame(beams_renderer* r, const beams_camera* cam, flo
   cudaError_t e;
   if (!direct) {
     e = cudaMemcpyAsync(rgba_out, dst, npix * sizeof(float4),
-                        out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, r->stream);
+                        out_on_device == BEAMS_OUT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                        r->stream);
     if (e != cudaSuccess) return cuda_fail(r, e, "copying image out");
   }
   cudaEventRecord(r->ev[3], r->stream);
@@ -519,7 +520,7 @@ beams_status render_bricks_frame(beams_renderer* r, const beams_camera* cam, flo
     for (auto& b : r->bricks) nv += r->use_map ? b.map_count : 0;
     t->map_vertices = (int)nv;
     t->kernel_launches = launches;
-  } else if (!out_on_device) {
+  } else if (out_on_device == BEAMS_OUT_HOST) {
     e = cudaStreamSynchronize(r->stream);
     if (e != cudaSuccess) return cuda_fail(r, e, "render");
   }
@@ -975,6 +976,8 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
   beams_status s = validate_camera(r, cam);
   if (s != BEAMS_OK) return s;
   if (!rgba_out) return fail(r, BEAMS_ERR_INVALID_ARG, "rgba_out is NULL");
+  if (out_on_device < BEAMS_OUT_HOST || out_on_device > BEAMS_OUT_HOST_ASYNC)
+    return fail(r, BEAMS_ERR_INVALID_ARG, "out_on_device must be BEAMS_OUT_HOST, _DEVICE or _HOST_ASYNC");
   s = check_ready(r);
   if (s != BEAMS_OK) return s;
   cudaSetDevice(r->device);
@@ -998,7 +1001,7 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
   cudaEventRecord(r->ev[1], r->stream);
   const size_t npix = (size_t)cam->width * cam->height;
   float4* dst = (float4*)rgba_out;
-  const bool direct = out_on_device && (((uintptr_t)rgba_out & 15) == 0);
+  const bool direct = out_on_device == BEAMS_OUT_DEVICE && (((uintptr_t)rgba_out & 15) == 0);
   if (!direct) {
     s = ensure_buffer(r, (void**)&r->d_rgba, &r->rgba_cap, npix * sizeof(float4), "allocating image");
     if (s != BEAMS_OK) return s;
@@ -1032,7 +1035,8 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
   if (s != BEAMS_OK) return s;
   if (!direct) {
     e = cudaMemcpyAsync(rgba_out, dst, npix * sizeof(float4),
-                        out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, r->stream);
+                        out_on_device == BEAMS_OUT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                        r->stream);
     if (e != cudaSuccess) return cuda_fail(r, e, "copying image out");
   }
   cudaEventRecord(r->ev[3], r->stream);
@@ -1056,11 +1060,19 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
     if (use_mlp && c.fallback_tiles) built = true;  // the fallback's gated map build ran
     t->map_vertices = built ? (int)((size_t)g.pd[0] * g.pd[1] * g.pd[2]) : 0;
     t->kernel_launches = launches;
-  } else if (!out_on_device) {
+  } else if (out_on_device == BEAMS_OUT_HOST) {
     // The caller reads rgba_out on return.
     e = cudaStreamSynchronize(r->stream);
     if (e != cudaSuccess) return cuda_fail(r, e, "render");
   }
+  return BEAMS_OK;
+}
+
+beams_status beams_synchronize(beams_renderer* r) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  cudaSetDevice(r->device);
+  const cudaError_t e = cudaStreamSynchronize(r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "synchronize");
   return BEAMS_OK;
 }
 

@@ -235,3 +235,33 @@ def test_vertex_order_and_empty_skip_change_nothing(cuda_device, kind):
     assert best["light_brick"] in (0, 8, 16, 32, 64) and best["map_ms"] > 0 and best["view_ms"] > 0
     img, _ = r.render(s.camera())
     assert np.array_equal(img, ref[1])
+
+
+def test_async_host_output_and_double_buffered_renderers(cuda_device):
+    """BEAMS_OUT_HOST_ASYNC: the image lands in pinned host memory after
+    beams_synchronize; two renderers on two streams, uploading the field from
+    pinned memory in turn, give the synchronous image every step."""
+    import torch
+    s = scenes.small(8, n=40, image=64, m=16)
+    ref, _, _, _ = gpu_render(s)
+    field = torch.from_numpy(s.field_numpy()).pin_memory()
+    rs = []
+    for _ in range(2):
+        r = B.Renderer(0, stream=torch.cuda.Stream().cuda_stream)
+        r.set_volume(field.numpy(), origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+        s.configure(r)
+        rs.append(r)
+    outs = [torch.full((s.height, s.width, 4), -1.0).pin_memory() for _ in rs]
+    for i in range(6):
+        q = rs[i % 2]
+        if i >= 2:
+            q.synchronize()
+            assert np.array_equal(outs[i % 2].numpy(), ref)
+        q.set_volume(field, dims=s.dims, origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+        q.render(s.camera(), out=outs[i % 2], timings=False, host_async=True)
+    for q in rs:
+        q.synchronize()
+    for o in outs:
+        assert np.array_equal(o.numpy(), ref)
+    with pytest.raises(ValueError):
+        rs[0].render(s.camera(), out=np.zeros((s.height, s.width, 4), np.float32), host_async=True)

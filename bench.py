@@ -345,6 +345,13 @@ def run_ours(args):
                 "k_light_march_ms": k1_ms, "k_view_march_ms": k2_ms,
                 "k_light_march_GBps": k1_bytes / (k1_ms / 1e3) / 1e9,
                 "k_view_march_GBps": k2_bytes / (k2_ms / 1e3) / 1e9}
+    # compulsory footprint: every byte the launch must touch once (the 4-corner
+    # quad field it reads, 16 B per cell, and the map it writes; for the view
+    # march the quads, the map and the image)
+    ncell = (s.dims[0] - 1) * (s.dims[1] - 1) * s.dims[2]
+    unique = ncell * 16 + nvert * 4 if kname == "k_light_march" else ncell * 16 + nvert * 4 + npix * 16
+    roofline["compulsory_bytes_per_launch"] = unique
+    roofline["compulsory_frac"] = unique / (kms / 1e3) / 1e9 / peak
 
     # end to end through the C ABI with host buffers: every step uploads the
     # field from pinned host memory (beams_set_volume) and renders into pinned

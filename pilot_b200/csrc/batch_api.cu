@@ -457,7 +457,7 @@ beams_status beams_batch_autotune(beams_renderer* r, const beams_request* reqs, 
           cand.push_back(o);
         }
     } else {
-      static const int tiles[][2] = {{16, 16}, {32, 8}, {8, 32}, {32, 32}, {64, 32}, {64, 64}};
+      static const int tiles[][2] = {{8, 8}, {16, 16}, {32, 8}, {8, 32}, {32, 32}, {64, 32}, {64, 64}};
       for (const auto& tw : tiles)
         if (tw[0] != bo.tile_w || tw[1] != bo.tile_h) {
           o.tile_w = tw[0];

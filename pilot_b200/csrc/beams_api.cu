@@ -82,12 +82,33 @@ static void geo_set_light(ExactGeo& g, const Light& L) {
     const double len = std::sqrt(L.v[0] * L.v[0] + L.v[1] * L.v[1] + L.v[2] * L.v[2]);
     for (int d = 0; d < 3; ++d) g.light[d] = (float)(L.v[d] / len);
   }
+  // the map build's brick order follows the light's travel direction at the
+  // volume centre, in map-vertex units (see ExactGeo::bo_axis)
+  double e[3];
+  for (int d = 0; d < 3; ++d) {
+    const double c = 0.5 * (g.bmin[d] + g.bmax[d]);
+    const double t = (L.kind == 0) ? c - L.v[d] : L.v[d];
+    e[d] = (g.msp[d] > 0.f) ? t / (double)g.msp[d] : 0.0;
+  }
+  int w = 2;
+  for (int d = 0; d < 3; ++d)
+    if (std::fabs(e[d]) > std::fabs(e[w])) w = d;
+  const int u = (w == 0) ? 1 : 0, v = (w == 2) ? 1 : 2;
+  g.bo_axis[0] = w;
+  g.bo_axis[1] = u;
+  g.bo_axis[2] = v;
+  const bool ok = std::fabs(e[w]) > 0.0 && std::isfinite(e[w]);
+  g.bo_shear[0] = ok ? (int)std::lround(65536.0 * e[u] / e[w]) : 0;
+  g.bo_shear[1] = ok ? (int)std::lround(65536.0 * e[v] / e[w]) : 0;
 }
 
 // Derives the kernel parameters exactly as the reference derives them
 // (float32 arithmetic; see the cited lines in beams_params.h).
 beams_status make_geo_vol(beams_renderer* r, const beams_volume& v, const beams_camera* cam, ExactGeo& g) {
   std::memset(&g, 0, sizeof(g));
+  g.bo_axis[0] = 2;  // z-pencils until a light sets the order
+  g.bo_axis[1] = 0;
+  g.bo_axis[2] = 1;
   for (int d = 0; d < 3; ++d) {
     g.n[d] = v.dims[d];
     g.org[d] = (float)v.origin[d];

@@ -47,6 +47,15 @@ struct ExactGeo {
   // bricks of 2^b vertices per edge in brick order (rays in flight stay in a
   // narrow cone towards the light, so the field they read stays in L2).
   int light_brick_log2;
+  // Brick order that follows the light: bricks are visited in pencils along
+  // bo_axis[0] (the axis the light travels most along, in map-vertex units),
+  // the two other brick coordinates (bo_axis[1], bo_axis[2]) sheared by
+  // floor(w * bo_shear / 65536) modulo their brick counts, so that a pencil
+  // tracks the light rays through the brick grid; pencils in raster order.
+  // The bricks in flight then sit in a few adjacent pencils and their light
+  // rays cross one narrow region of the field. Any order gives the same map.
+  int bo_axis[3];
+  int bo_shear[2];
   // Occupancy of 8^3-cell macro-cells (empty-space skipping): counts per axis.
   int occ_n[3];
   // The multi-light extension: n_lights maps, map l at map + l * (M+1)^3, the

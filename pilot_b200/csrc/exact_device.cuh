@@ -367,6 +367,36 @@ __device__ __forceinline__ void map_light_sum(const ExactGeo& g, const float4* M
   }
 }
 
+// Shared-memory form of the light-aligned brick order for bricks of 2^bl
+// vertices per edge: {nb_w, nb_u, nb_v, axis_w, axis_u, axis_v, shear_u, shear_v}.
+__device__ __forceinline__ void brick_order_setup(const ExactGeo& g, int bl, int* s_bo) {
+  int nb[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) nb[d] = (g.pd[d] + (1 << bl) - 1) >> bl;
+  for (int k = 0; k < 3; ++k) {
+    s_bo[k] = nb[g.bo_axis[k]];
+    s_bo[3 + k] = g.bo_axis[k];
+  }
+  s_bo[6] = g.bo_shear[0];
+  s_bo[7] = g.bo_shear[1];
+}
+
+// Brick bi of that order -> brick coordinates. Read through volatile loads so
+// the parameters stay in shared memory rather than in registers.
+__device__ __forceinline__ void pencil_brick(int bi, const int* s_bo, int& bx, int& by, int& bz) {
+  const volatile int* q = s_bo;
+  const int nw = q[0], nu = q[1], nv = q[2];
+  const int w = bi % nw, pe = bi / nw;
+  int u = (pe % nu + ((w * q[6]) >> 16)) % nu;
+  int v = (pe / nu + ((w * q[7]) >> 16)) % nv;
+  u += (u < 0) ? nu : 0;
+  v += (v < 0) ? nv : 0;
+  const int aw = q[3], au = q[4];
+  bx = aw == 0 ? w : (au == 0 ? u : v);
+  by = aw == 1 ? w : (au == 1 ? u : v);
+  bz = aw == 2 ? w : (au == 2 ? u : v);
+}
+
 // Quad layout of a point field: Q[z][y][x] = {f(x,y,z), f(x+1,y,z), f(x,y+1,z),
 // f(x+1,y+1,z)} for x < nx-1, y < ny-1, so one cell is two 16-byte loads
 // (z and z+1). VTK corner order 0..7 = lo.x lo.y lo.w lo.z hi.x hi.y hi.w hi.z.

@@ -56,6 +56,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch(const ExactGeo* __re
   __shared__ BatchDesc sd;
   __shared__ int s_item, s_req, s_phase, s_skip;
   __shared__ unsigned s_sub;
+  __shared__ int s_bo[8];  // the request's light-aligned brick order
   extern __shared__ float4 s_dyn[];
   const int tid = threadIdx.x, lane = tid & 31;
   // shared TF (one colour map for the batch) and its normalised alpha
@@ -93,6 +94,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch(const ExactGeo* __re
       __syncthreads();
       const int ntab = phase == 1 ? sg.max_off[0] : sg.ntab;
       for (int i = tid; i < ntab; i += blockDim.x) s_tab[i] = table_entry(sg, i);
+      if (tid == 0 && plan.brick_log2) brick_order_setup(sg, plan.brick_log2, s_bo);
       if (tid == 0) {
         s_req = req;
         s_phase = phase;
@@ -111,11 +113,12 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch(const ExactGeo* __re
         const int slot = base + (int)(t << 5) + lane;
         int id = -1, x = 0, y = 0, z = 0;
         if (bl) {
-          const int nbx = (sg.pd[0] + (1 << bl) - 1) >> bl, nby = (sg.pd[1] + (1 << bl) - 1) >> bl;
           const int bi = slot >> (3 * bl), li = slot & ((1 << (3 * bl)) - 1), m = (1 << bl) - 1;
-          x = ((bi % nbx) << bl) + (li & m);
-          y = (((bi / nbx) % nby) << bl) + ((li >> bl) & m);
-          z = ((bi / (nbx * nby)) << bl) + (li >> (2 * bl));
+          int bx, by, bz;
+          pencil_brick(bi, s_bo, bx, by, bz);
+          x = (bx << bl) + (li & m);
+          y = (by << bl) + ((li >> bl) & m);
+          z = (bz << bl) + (li >> (2 * bl));
           if (x < sg.pd[0] && y < sg.pd[1] && z < sg.pd[2]) id = (z * sg.pd[1] + y) * sg.pd[0] + x;
         } else if (slot < sd.nvert) {
           id = slot;

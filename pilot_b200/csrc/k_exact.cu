@@ -77,19 +77,15 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  // Brick counts per axis live in shared memory and are re-read per tile, so
-  // they occupy no registers across the march (the march is register-bound).
-  __shared__ int s_nb[2];
-  if (threadIdx.x == 0) {
-    const int b0 = g.light_brick_log2;
-    s_nb[0] = (g.pd[0] + (1 << b0) - 1) >> b0;
-    s_nb[1] = (g.pd[1] + (1 << b0) - 1) >> b0;
-  }
+  // The brick order's parameters live in shared memory and are re-read per
+  // tile, so they occupy no registers across the march (the march is
+  // register-bound).
+  __shared__ int s_bo[8];
+  if (threadIdx.x == 0) brick_order_setup(g, g.light_brick_log2, s_bo);
   __syncthreads();
   const int ntiles = [&] {
     const int b0 = g.light_brick_log2;
-    const int nbz = (g.pd[2] + (1 << b0) - 1) >> b0;
-    return b0 ? (s_nb[0] * s_nb[1] * nbz) << (3 * b0 - 5) : (nvert + 31) >> 5;
+    return b0 ? (s_bo[0] * s_bo[1] * s_bo[2]) << (3 * b0 - 5) : (nvert + 31) >> 5;
   }();
   unsigned ns = 0;
 
@@ -98,14 +94,14 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
     float V[3], L[3];
     const int bl = g.light_brick_log2;
     if (bl) {
-      const int nbx = *(volatile int*)&s_nb[0], nby = *(volatile int*)&s_nb[1];
-      // tile -> brick, lane -> vertex of the brick (x fastest inside the brick)
+      // tile -> brick (light-aligned order), lane -> vertex of the brick (x fastest inside the brick)
       const int bi = tile >> (3 * bl - 5);
       const int li = ((tile & ((1 << (3 * bl - 5)) - 1)) << 5) + lane;
       const int m = (1 << bl) - 1;
-      const int bx = bi % nbx, byz = bi / nbx;
-      const int x = (bx << bl) + (li & m), y = ((byz % nby) << bl) + ((li >> bl) & m);
-      const int z = ((byz / nby) << bl) + (li >> (2 * bl));
+      int bx, by, bz;
+      pencil_brick(bi, s_bo, bx, by, bz);
+      const int x = (bx << bl) + (li & m), y = (by << bl) + ((li >> bl) & m);
+      const int z = (bz << bl) + (li >> (2 * bl));
       if (x >= g.pd[0] || y >= g.pd[1] || z >= g.pd[2]) continue;
       id = (z * g.pd[1] + y) * g.pd[0] + x;
       V[0] = vtx_coord(g, 0, x);

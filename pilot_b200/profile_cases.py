@@ -6,6 +6,7 @@
     python -m pilot_b200.profile_cases --case mlp_tc           # tcgen05 forward, 2^21 rows
     python -m pilot_b200.profile_cases --case batch            # 16-request persistent batch
     python -m pilot_b200.profile_cases --case precision_light  # precision-form K1, bf16 640^3
+    python -m pilot_b200.profile_cases --case bricks           # 512^3 noise as 2x2x2 bricks: K1, K5, K2, K6
 
 Each case sets up its scene, runs the target kernel --reps times and exits 0;
 device memory stays within a few GB. The tuning is fixed (8^3 vertex bricks,
@@ -26,7 +27,8 @@ def main(argv=None) -> int:
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", required=True,
-                    choices=["light_march", "view_march", "mlp_view", "mlp_tc", "batch", "precision_light"])
+                    choices=["light_march", "view_march", "mlp_view", "mlp_tc", "batch", "precision_light",
+                             "bricks"])
     ap.add_argument("--reps", type=int, default=3)
     a = ap.parse_args(argv)
     torch.cuda.set_device(0)
@@ -75,6 +77,27 @@ def main(argv=None) -> int:
         r.set_tuning(light_brick=8, empty_skip=True, view_skip=True)
         for _ in range(a.reps):
             r.build_shadow_map(timings=False)
+    elif a.case == "bricks":
+        s = scenes.config1()
+        fd = s.field_device()
+        cells = s.dims[0] - 1
+        edges = [round(i * cells / 2) for i in range(3)]
+        h = s.spacing
+        bricks = []  # 2x2x2; neighbours share their face plane
+        for z0, z1 in zip(edges[:-1], edges[1:]):
+            for y0, y1 in zip(edges[:-1], edges[1:]):
+                for x0, x1 in zip(edges[:-1], edges[1:]):
+                    org = (s.origin[0] + x0 * h[0], s.origin[1] + y0 * h[1], s.origin[2] + z0 * h[2])
+                    bricks.append((fd[z0:z1 + 1, y0:y1 + 1, x0:x1 + 1].contiguous(), org, h, s.value_range))
+        del fd
+        r = B.Renderer(0)
+        r.set_bricks(bricks)
+        s.configure(r)
+        r.set_shadow_map_size(s.map_m // 2)
+        cam = s.camera()
+        out = torch.empty((s.height, s.width, 4), device="cuda")
+        for _ in range(a.reps):
+            r.render(cam, out=out, timings=False)
     else:  # batch
         sys.path.insert(0, str(__import__("pathlib").Path(__file__).resolve().parent.parent))
         import bench

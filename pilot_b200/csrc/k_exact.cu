@@ -72,11 +72,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
   const int cm0 = g.n[0] - 2, cm1 = g.n[1] - 2, cm2 = g.n[2] - 2;
   const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
   const int n1 = g.tf_n - 1;
-  // Warps take 32-vertex tiles round-robin: no block barriers inside the march,
-  // and the tiles in flight sweep the vertex array in order.
+  // Warps take 32-vertex tiles from a launch-wide counter: no block barriers
+  // inside the march, and the tiles in flight sweep the vertex order as one
+  // compact window.
   const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
   // The brick order's parameters live in shared memory and are re-read per
   // tile, so they occupy no registers across the march (the march is
   // register-bound).
@@ -89,7 +88,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
   }();
   unsigned ns = 0;
 
-  for (int tile = warp; tile < ntiles; tile += nwarps) {
+  for (int tile = next_warp_tile(&cnt->tiles_light); tile < ntiles; tile = next_warp_tile(&cnt->tiles_light)) {
     int id;
     float V[3], L[3];
     const int bl = g.light_brick_log2;
@@ -387,7 +386,10 @@ static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4*
   const size_t smem = (size_t)g.max_off[0] * sizeof(float4) + 2 * (size_t)g.tf_n * sizeof(float);
   const int ntiles = (nvert + kThreads - 1) / kThreads;
   int grid = 0;
-  cudaError_t e;
+  // warps take tiles from a launch-wide counter, so the tiles in flight stay a
+  // compact window of the brick order however unevenly the rays run
+  cudaError_t e = cudaMemsetAsync(&cnt->tiles_light, 0, sizeof(unsigned), st);
+  if (e != cudaSuccess) return e;
   if (occ) {
     e = persistent_grid(k_light_march<QuadT, STITCH, PREC, true>, smem, ntiles, grid);
     if (e != cudaSuccess) return e;

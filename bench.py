@@ -717,6 +717,39 @@ def run_batch(args):
     z.record(stream)
     torch.cuda.synchronize()
     seq_ms = a.elapsed_time(z) / max(1, args.steps // 4)
+    # The same comparison for small requests only (the 64^3 and 128^3 volumes,
+    # 256^2 images), where one request alone cannot fill the GPU.
+    small_outs = [torch.empty((256, 256, 4), device="cuda") for _ in range(nreq)]
+
+    def small_requests():
+        rq = batch_requests(B, vols, rng, nreq, small_outs)
+        for q, _ in rq:
+            q.volume = q.volume % 4
+            n = vols[q.volume][0].dims[0]
+            q.map_cells = n // 2
+            q.sample_distance = 0.5 / (n - 1)
+        return rq
+    small_tuning = r.batch_autotune(small_requests())
+    small_reqs = small_requests()
+    for _ in range(3):
+        r.render_batch(small_reqs, timings=False)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(args.steps):
+        r.render_batch(small_reqs, timings=False)
+    z.record(stream)
+    torch.cuda.synchronize()
+    small_ms = a.elapsed_time(z) / args.steps
+    seq_reqs = small_reqs
+    sequential()
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(max(1, args.steps // 4)):
+        sequential()
+    z.record(stream)
+    torch.cuda.synchronize()
+    small_seq_ms = a.elapsed_time(z) / max(1, args.steps // 4)
+    r.set_batch_options(**{k: tuning[k] for k in ("tile_w", "tile_h", "light_brick", "skip")})
     # end to end: images to pinned host memory
     host = [torch.empty((w, w, 4)).pin_memory() for w in sizes]
     r.render_batch(batch_requests(B, vols, rng, nreq, host), timings=False)
@@ -739,6 +772,9 @@ def run_batch(args):
                        "l2": "volumes and maps total well above L2; no flush"},
             "requests_per_s": nreq * args.steps / (total_ms / 1e3),
             "sequential_ms_per_batch": seq_ms, "speedup_vs_sequential": seq_ms / (total_ms / args.steps),
+            "small_requests": {"workload": f"{nreq} requests over the 64^3 and 128^3 volumes, 256^2 images",
+                               "batch_ms": small_ms, "sequential_ms": small_seq_ms,
+                               "speedup_vs_sequential": small_seq_ms / small_ms, "tuning": small_tuning},
             "gpu_launches": args.steps,
             "e2e": {"value": lit_e / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(sum(w * w * 16 for w in sizes)),

@@ -28,7 +28,6 @@
 
 namespace beams {
 
-constexpr int kMaxTF = 1024;
 constexpr int kThreads = 256;
 
 // Loads the cell tables (and nothing else) into shared memory.
@@ -69,9 +68,6 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
   const float4* T0 = s_tab + g.ax_off[0];
   const float4* T1 = s_tab + g.ax_off[1];
   const float4* T2 = s_tab + g.ax_off[2];
-  const int cm0 = g.n[0] - 2, cm1 = g.n[1] - 2, cm2 = g.n[2] - 2;
-  const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
-  const int n1 = g.tf_n - 1;
   // Warps take 32-vertex tiles from a launch-wide counter: no block barriers
   // inside the march, and the tiles in flight sweep the vertex order as one
   // compact window.

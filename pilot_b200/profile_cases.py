@@ -3,6 +3,7 @@
     python -m pilot_b200.profile_cases --case light_march      # K1, 512^3 noise, M = 256
     python -m pilot_b200.profile_cases --case view_march       # K2, 512^3 noise, 1024^2, map cached
     python -m pilot_b200.profile_cases --case mlp_view         # learned-form view march, 1024^2
+    python -m pilot_b200.profile_cases --case mlp_frame        # learned form frame: scene-light network, 1% probes
     python -m pilot_b200.profile_cases --case mlp_tc           # tcgen05 forward, 2^21 rows
     python -m pilot_b200.profile_cases --case batch            # 16-request persistent batch
     python -m pilot_b200.profile_cases --case precision_light  # precision-form K1, bf16 640^3
@@ -27,12 +28,12 @@ def main(argv=None) -> int:
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", required=True,
-                    choices=["light_march", "view_march", "mlp_view", "mlp_tc", "batch", "precision_light",
-                             "bricks"])
+                    choices=["light_march", "view_march", "mlp_view", "mlp_frame", "mlp_tc", "batch",
+                             "precision_light", "bricks"])
     ap.add_argument("--reps", type=int, default=3)
     a = ap.parse_args(argv)
     torch.cuda.set_device(0)
-    if a.case in ("light_march", "view_march", "mlp_view"):
+    if a.case in ("light_march", "view_march", "mlp_view", "mlp_frame"):
         s = scenes.config1()
         fd = s.field_device()
         r = B.Renderer(0)
@@ -47,6 +48,12 @@ def main(argv=None) -> int:
         elif a.case == "view_march":
             r.build_shadow_map(timings=False)
             r.set_reuse_shadow_map(True)
+            for _ in range(a.reps):
+                r.render(cam, out=out, timings=False)
+        elif a.case == "mlp_frame":
+            # the learned form as benchmarked: network trained for the scene's light, knot 32, 1% probes
+            r.mlp_train(B.mlp_options(n_lights=1, scene_light=1))
+            r.set_form(B.FORM_MLP, B.mlp_options(knot=32, probe_fraction=0.01))
             for _ in range(a.reps):
                 r.render(cam, out=out, timings=False)
         else:

@@ -7,6 +7,7 @@
     python -m pilot_b200.profile_cases --case mlp_tc           # tcgen05 forward, 2^21 rows
     python -m pilot_b200.profile_cases --case batch            # 16-request persistent batch
     python -m pilot_b200.profile_cases --case precision_light  # precision-form K1, bf16 640^3
+    python -m pilot_b200.profile_cases --case precision_view   # precision-form K2, bf16 640^3, 1024^2, map cached
     python -m pilot_b200.profile_cases --case bricks           # 512^3 noise as 2x2x2 bricks: K1, K5, K2, K6
 
 Each case sets up its scene, runs the target kernel --reps times and exits 0;
@@ -29,7 +30,7 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", required=True,
                     choices=["light_march", "view_march", "mlp_view", "mlp_frame", "mlp_tc", "batch",
-                             "precision_light", "bricks"])
+                             "precision_light", "precision_view", "bricks"])
     ap.add_argument("--reps", type=int, default=3)
     a = ap.parse_args(argv)
     torch.cuda.set_device(0)
@@ -74,7 +75,7 @@ def main(argv=None) -> int:
         T = torch.empty(n, device="cuda")
         for _ in range(a.reps):
             r.mlp_forward_tc_device(X, T)
-    elif a.case == "precision_light":
+    elif a.case in ("precision_light", "precision_view"):
         s = scenes.config2(n=640, image=1024, m=320)
         fd = s.field_device()
         r = B.Renderer(0)
@@ -82,8 +83,15 @@ def main(argv=None) -> int:
         s.configure(r)
         r.set_form(B.FORM_PRECISION, B.BF16)
         r.set_tuning(light_brick=8, empty_skip=True, view_skip=True)
-        for _ in range(a.reps):
+        if a.case == "precision_light":
+            for _ in range(a.reps):
+                r.build_shadow_map(timings=False)
+        else:
             r.build_shadow_map(timings=False)
+            r.set_reuse_shadow_map(True)
+            out = torch.empty((s.height, s.width, 4), device="cuda")
+            for _ in range(a.reps):
+                r.render(s.camera(), out=out, timings=False)
     elif a.case == "bricks":
         s = scenes.config1()
         fd = s.field_device()

@@ -265,3 +265,28 @@ def test_async_host_output_and_double_buffered_renderers(cuda_device):
         assert np.array_equal(o.numpy(), ref)
     with pytest.raises(ValueError):
         rs[0].render(s.camera(), out=np.zeros((s.height, s.width, 4), np.float32), host_async=True)
+
+
+@pytest.mark.parametrize("offset,scale", [((1000.0, -500.0, 250.0), 1.0), ((3.0, 2.0, -1.0), 40.0),
+                                          ((-20000.0, 0.0, 7.0), 0.5)])
+def test_far_and_scaled_volumes_bit_exact(cuda_device, offset, scale):
+    """Volumes far from the origin or at other scales: the float32 rounding of
+    the sample positions grows with the coordinates, so this exercises the
+    light march's bound on the steps that cannot fail its distance test (the
+    map must still equal the oracle's bit for bit)."""
+    s = scenes.small(12, n=32, image=48, m=12, kind="noise")
+    off = np.asarray(offset)
+    sp = scale / (s.dims[0] - 1)
+    s.origin = tuple(float(v) for v in off)
+    s.brick_spacing = (sp, sp, sp)
+    s.light = tuple(float(v) for v in off + scale * (np.asarray(s.light)))
+    s.cam_pos = tuple(float(v) for v in off + scale * np.asarray(s.cam_pos))
+    s.cam_look = tuple(float(v) for v in off + scale * np.asarray(s.cam_look))
+    s.sample_distance = 0.5 * sp
+    img, m, t, _ = gpu_render(s)
+    o = Oracle(s)
+    om, _ = o.light_march()
+    assert np.array_equal(m, om), f"map mismatch: max {np.max(np.abs(m - om))}"
+    oimg, olit = o.view_march(om)
+    assert np.max(np.abs(img - oimg)) <= TOL
+    assert t["lit_samples"] == olit

@@ -148,6 +148,18 @@ beams_status beams_set_slab_fp64(beams_renderer* r, int enable);
 /* Keep the last map when its inputs (volume, colour map, light, map size) did not
  * change. Off by default: the reference rebuilds the map every frame. */
 beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable);
+/* Explicit rectilinear coordinates for the current point volume (after
+ * beams_set_volume): x, y, z hold dims[0], dims[1], dims[2] strictly increasing
+ * float32 coordinates, the arrays of the ArrayHandleCartesianProduct coordinate
+ * system that RenderCells receives (MapperLightedVolume.cxx:114-119) and that the
+ * reference's RectilinearLocator and RectilinearMeshOracle search
+ * (LightedVolumeRenderer.cxx:45-186, RectilinearMeshOracle.h:140-176). The
+ * volume's origin/spacing are then ignored; the map grid spans the coordinates'
+ * bounds. All three NULL return to uniform spacing; beams_set_volume also does.
+ * Exact and precision forms of a single volume with one light; empty-space
+ * skipping is off for such a volume. */
+beams_status beams_set_volume_coordinates(beams_renderer* r, const float* x, const float* y, const float* z);
+
 /* Replaces MapperLightedVolume::SetCompositeBackground (MapperLightedVolume.cxx:321-324)
  * and the Canvas::BlendBackground call it enables (:185-188): after the image is
  * complete (composite included), the premultiplied image is placed over the

@@ -108,7 +108,7 @@ void build_geo(const oracle_scene* s, Geo<T>& g) {
     g.n[d] = s->dims[d];
     g.C[d].resize(s->dims[d]);
     const T o = (T)s->origin[d], h = (T)s->spacing[d];
-    for (int i = 0; i < s->dims[d]; ++i) g.C[d][i] = o + h * (T)i;
+    for (int i = 0; i < s->dims[d]; ++i) g.C[d][i] = s->coords[d] ? (T)s->coords[d][i] : o + h * (T)i;
     g.minp[d] = g.C[d][0];
     g.maxp[d] = g.C[d][s->dims[d] - 1];
     g.bmin[d] = (double)g.C[d][0];

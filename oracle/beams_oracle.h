@@ -56,6 +56,9 @@ typedef struct oracle_scene {
    * distance (row y at y * width), the slab test's initial MaxDistance; NULL:
    * no limit (MapperLightedVolume.cxx:151-152, LightedVolumeRenderer.cxx:644-718). */
   const float* ray_max;
+  /* Explicit rectilinear coordinates: dims[d] float32 values per axis (the
+   * reference's ArrayHandleCartesianProduct); NULL: origin + spacing * i. */
+  const float* coords[3];
 } oracle_scene;
 
 /* Light march over every map vertex ((M+1)^3, x fastest). */

@@ -25,7 +25,7 @@ class OracleScene(C.Structure):
                 ("sample_distance", C.c_float), ("alpha_cutoff", C.c_float), ("light_steps", C.c_float),
                 ("slab_fp64", C.c_int), ("cam_pos", C.c_double * 3), ("cam_look", C.c_double * 3),
                 ("cam_up", C.c_double * 3), ("fov_y_deg", C.c_double), ("width", C.c_int), ("height", C.c_int),
-                ("precision", C.c_int), ("ray_max", C.c_void_p)]
+                ("precision", C.c_int), ("ray_max", C.c_void_p), ("coords", C.c_void_p * 3)]
 
 
 def lib():
@@ -85,6 +85,11 @@ class Oracle:
             (C.c_int * 3)(s.map_m, s.map_m, s.map_m), int(s.use_map), s.sample_distance, s.cutoff,
             s.light_steps, int(s.slab_fp64), (C.c_double * 3)(*s.cam_pos), (C.c_double * 3)(*s.cam_look),
             (C.c_double * 3)(*s.cam_up), s.fov_y_deg, s.width, s.height, int(precision))
+        coords = getattr(scene, "coords", None)
+        if coords is not None:
+            self._coords = [np.ascontiguousarray(c, np.float32) for c in coords]
+            for d in range(3):
+                self.cs.coords[d] = self._coords[d].ctypes.data
 
     def set_ray_limits(self, limits):
         """Canvas depth clipping: (height, width) float32 per-pixel ray limits, or None."""

@@ -194,6 +194,7 @@ def lib():
         "beams_set_depth_buffer": ([P, P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int], C.c_int),
         "beams_get_ray_limits": ([P, C.POINTER(Camera), P, C.c_int], C.c_int),
         "beams_synchronize": ([P], C.c_int),
+        "beams_set_volume_coordinates": ([P, P, P, P], C.c_int),
         "beams_test_fail_allocation": ([C.c_int], C.c_int),
         "beams_get_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "beams_batch_set_volumes": ([P, P, C.c_int], C.c_int),
@@ -491,6 +492,15 @@ class Renderer:
     def set_background(self, on: bool, rgba=(1, 1, 1, 1)):
         c = (C.c_float * 4)(*rgba)
         self._check(self._L.beams_set_background(self._h, int(bool(on)), c))
+
+    def set_volume_coordinates(self, x=None, y=None, z=None):
+        """Explicit rectilinear coordinates of the current point volume (float32,
+        strictly increasing, dims[d] values per axis); no arguments: uniform again."""
+        if x is None and y is None and z is None:
+            self._check(self._L.beams_set_volume_coordinates(self._h, None, None, None))
+            return
+        self._coords = [np.ascontiguousarray(a, np.float32) for a in (x, y, z)]
+        self._check(self._L.beams_set_volume_coordinates(self._h, *[_ptr(a) for a in self._coords]))
 
     def set_depth_buffer(self, depth, kind=0, near=0.0, far=0.0):
         """Canvas depth clipping: depth (H, W) float32 numpy or torch CUDA tensor,

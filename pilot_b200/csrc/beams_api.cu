@@ -109,13 +109,25 @@ beams_status make_geo_vol(beams_renderer* r, const beams_volume& v, const beams_
   g.bo_axis[0] = 2;  // z-pencils until a light sets the order
   g.bo_axis[1] = 0;
   g.bo_axis[2] = 1;
+  // the renderer's own volume may carry explicit rectilinear coordinates
+  const bool rect = r->rect && &v == &r->vol;
+  g.rect = rect ? 1 : 0;
   for (int d = 0; d < 3; ++d) {
     g.n[d] = v.dims[d];
-    g.org[d] = (float)v.origin[d];
-    g.h[d] = (float)v.spacing[d];
+    if (rect) {
+      // MinPoint / MaxPoint are the first and last coordinates
+      // (LightedVolumeRenderer.cxx:77-87); the uniform fields keep the average spacing
+      g.minp[d] = r->coords[d].front();
+      g.maxp[d] = r->coords[d].back();
+      g.org[d] = g.minp[d];
+      g.h[d] = (g.maxp[d] - g.minp[d]) / (float)(v.dims[d] - 1);
+    } else {
+      g.org[d] = (float)v.origin[d];
+      g.h[d] = (float)v.spacing[d];
+      g.minp[d] = g.org[d] + g.h[d] * 0.f;
+      g.maxp[d] = g.org[d] + g.h[d] * (float)(v.dims[d] - 1);
+    }
     g.invh[d] = 1.f / g.h[d];
-    g.minp[d] = g.org[d] + g.h[d] * 0.f;
-    g.maxp[d] = g.org[d] + g.h[d] * (float)(v.dims[d] - 1);
     g.bmin[d] = (double)g.minp[d];
     g.bmax[d] = (double)g.maxp[d];
   }
@@ -283,6 +295,18 @@ beams_status prepare_layouts(beams_renderer* r, const ExactGeo& g, int& launches
     cudaError_t e = launch_build_tables(g, r->d_tab, r->stream);
     if (e != cudaSuccess) return cuda_fail(r, e, "cell table build");
     ++launches;
+    if (g.rect) {
+      // explicit coordinates: the field axes' entries {lo, hi, hi - lo, RN(1 / (hi - lo))}
+      std::vector<float4> fe((size_t)g.max_off[0]);
+      for (int d = 0; d < 3; ++d)
+        for (int c = 0; c + 1 < g.n[d]; ++c) {
+          const float lo = r->coords[d][c], hi = r->coords[d][c + 1], w = hi - lo;
+          fe[(size_t)g.ax_off[d] + c] = make_float4(lo, hi, w, 1.f / w);
+        }
+      e = cudaMemcpyAsync(r->d_tab, fe.data(), fe.size() * sizeof(float4), cudaMemcpyHostToDevice, r->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(r->stream);
+      if (e != cudaSuccess) return cuda_fail(r, e, "coordinate table upload");
+    }
     std::memcpy(r->tab_key, key, sizeof(key));
   }
   const int qd = quad_dtype(r);
@@ -329,7 +353,7 @@ beams_status build_map(beams_renderer* r, const ExactGeo& g, int& launches, bool
   if (s != BEAMS_OK) return s;
   r->map_valid = false;
   const unsigned char* occ = nullptr;
-  if (r->empty_skip) {
+  if (r->empty_skip && !g.rect) {  // the occupancy grid indexes uniform macro-cells
     s = prepare_occupancy(r, g, launches);
     if (s != BEAMS_OK) return s;
     occ = r->d_occ;
@@ -372,6 +396,11 @@ beams_status mlp_render_view(beams_renderer* r, const ExactGeo& g, float4* out, 
 bool mlp_ready(const beams_renderer* r);
 
 beams_status check_ready(beams_renderer* r) {
+  if (r->rect && (r->brick_mode || r->form == BEAMS_FORM_MLP || r->vol.assoc != BEAMS_ASSOC_POINTS ||
+                  (r->multi_light && r->lights.size() > 1)))
+    return fail(r, BEAMS_ERR_UNSUPPORTED,
+                "explicit volume coordinates render in the exact and precision forms of a single point volume "
+                "with one light");
   if (r->multi_light && r->lights.size() > 1) {
     if (r->brick_mode || r->form != BEAMS_FORM_EXACT || (r->has_volume && r->vol.assoc != BEAMS_ASSOC_POINTS))
       return fail(r, BEAMS_ERR_UNSUPPORTED, "several lights render in the exact form of a point volume only");
@@ -637,7 +666,31 @@ beams_status beams_set_volume(beams_renderer* r, const beams_volume* v) {
   r->field_bytes = bytes;
   r->has_volume = true;
   r->brick_mode = false;
+  r->rect = false;  // a new volume is uniform until beams_set_volume_coordinates
   ++r->volume_version;
+  return BEAMS_OK;
+}
+
+beams_status beams_set_volume_coordinates(beams_renderer* r, const float* x, const float* y, const float* z) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  if (!x && !y && !z) {
+    if (r->rect) ++r->volume_version;
+    r->rect = false;
+    return BEAMS_OK;
+  }
+  if (!x || !y || !z) return fail(r, BEAMS_ERR_INVALID_ARG, "volume coordinates: give all three axes or none");
+  if (!r->has_volume || r->vol.assoc != BEAMS_ASSOC_POINTS)
+    return fail(r, BEAMS_ERR_STATE, "volume coordinates: set a point volume first (beams_set_volume)");
+  const float* a[3] = {x, y, z};
+  for (int d = 0; d < 3; ++d) {
+    const int n = r->vol.dims[d];
+    for (int i = 0; i < n; ++i)
+      if (!std::isfinite(a[d][i]) || (i > 0 && !(a[d][i] > a[d][i - 1])))
+        return fail(r, BEAMS_ERR_INVALID_ARG, "volume coordinates must be finite and strictly increasing");
+  }
+  for (int d = 0; d < 3; ++d) r->coords[d].assign(a[d], a[d] + r->vol.dims[d]);
+  r->rect = true;
+  ++r->volume_version;  // new cell tables, occupancy and map
   return BEAMS_OK;
 }
 
@@ -1037,7 +1090,7 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
     e = cudaSuccess;
   } else {
     const unsigned char* occ = nullptr;
-    if (r->view_skip && r->vol.assoc == BEAMS_ASSOC_POINTS) {
+    if (r->view_skip && r->vol.assoc == BEAMS_ASSOC_POINTS && !g.rect) {
       s = prepare_occupancy(r, g, launches);
       if (s != BEAMS_OK) return s;
       occ = r->d_occ;

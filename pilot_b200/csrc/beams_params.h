@@ -62,6 +62,11 @@ struct ExactGeo {
   // view march shading by sum_l T_l * light_colors[l] (n_lights <= 1: light 0 only).
   int n_lights;
   float light_colors[8][3];
+  // Explicit rectilinear coordinates (beams_set_volume_coordinates): the field
+  // axes' cell tables hold the given coordinates and cells are found by
+  // search instead of from the uniform spacing; org/h/invh then only describe
+  // the average spacing. 0: coord(d, i) = org[d] + h[d] * float(i).
+  int rect;
   // Canvas depth clipping: per-pixel limit on each camera ray's distance
   // (width * height floats, row y at y * width), the MaxDistance that
   // MapCanvasToRays hands the slab test (MapperLightedVolume.cxx:151-152).

@@ -222,6 +222,33 @@ __device__ __forceinline__ int find_cell_bsearch_t(const float4* T, int cmax, fl
   return c;
 }
 
+// Searches for explicit (non-uniform) rectilinear coordinates, where no seed
+// from a uniform spacing is close: the light march's binary search
+// (RectilinearMeshOracle.h:154-176, smallest c with val <= coord(c+1)) and the
+// view march's cell lookup (the unique c with coord(c) <= p < coord(c+1) that
+// RectilinearLocator::LocateCell walks to, LightedVolumeRenderer.cxx:119-165),
+// both over the shared-memory cell table.
+__device__ __forceinline__ int find_cell_bsearch_rect(const float4* T, int cmax, float val, float4& e) {
+  int lo = 0, hi = cmax;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (val <= T[mid].y) hi = mid;
+    else lo = mid + 1;
+  }
+  e = T[lo];
+  return lo;
+}
+__device__ __forceinline__ int find_cell_walk_rect(const float4* T, int cmax, float p, float4& e) {
+  int lo = 0, hi = cmax;  // largest c with coord(c) <= p
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (T[mid].x <= p) lo = mid;
+    else hi = mid - 1;
+  }
+  e = T[lo];
+  return lo;
+}
+
 // View-march cell search: RectilinearLocator::LocateCell (LightedVolumeRenderer.cxx:119-165)
 // walks to the unique cell with coord(c) <= p < coord(c+1).
 __device__ __forceinline__ int find_cell_walk_t(const float4* T, int cmax, float org, float invh, float p,

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "exact_device.cuh"
 #include "kernels.h"
@@ -41,7 +42,7 @@ __device__ __forceinline__ void load_tables(float4* s_tab, const float4* __restr
 // STITCH: the multi-brick Phase 3 — the march starts from the cross-brick
 // prefix (stitch_prefix) instead of zero, as GenerateEstimator is re-run on
 // the prefix opacities (LightedVolumeRenderer.cxx:1241-1252).
-template <typename QuadT, bool STITCH, bool PREC, bool SKIP>
+template <typename QuadT, bool STITCH, bool PREC, bool SKIP, bool RECT = false>
 __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, const QuadT* __restrict__ quads,
                                                           const float4* __restrict__ tab,
                                                           const float4* __restrict__ tf,
@@ -109,7 +110,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
     }
     light_origin(g, V, L);
     Accum<PREC> acc;
-    march_vertex<QuadT, PREC, SKIP>(g, quads, T0, T1, T2, s_a, s_tau, occ, V, L,
+    march_vertex<QuadT, PREC, SKIP, RECT>(g, quads, T0, T1, T2, s_a, s_tau, occ, V, L,
                                     [&](const float dir[3]) {
                                       return STITCH ? stitch_prefix(refs, nrefs, self, L, V, dir) : 0.f;
                                     },
@@ -122,7 +123,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
 // ---------------------------------------------------------------------------
 // K2 (point field)
 // ---------------------------------------------------------------------------
-template <typename QuadT, bool USE_MAP, typename MapT, bool LIST = false, bool SKIP = false, bool MULTI = false>
+template <typename QuadT, bool USE_MAP, typename MapT, bool LIST = false, bool SKIP = false, bool MULTI = false,
+          bool RECT = false>
 __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const QuadT* __restrict__ quads,
                                                          const float4* __restrict__ tab,
                                                          const float4* __restrict__ tf,
@@ -154,7 +156,8 @@ __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const
     }
     if (x < g.width && y < g.height) {
       float4 color;
-      view_march_pixel<QuadT, USE_MAP, MapT, NoRecord, SKIP, MULTI>(g, quads, s_tab, s_tf, map, x, y, color, lit,
+      view_march_pixel<QuadT, USE_MAP, MapT, NoRecord, SKIP, MULTI, RECT>(g, quads, s_tab, s_tf, map, x, y, color,
+                                                                           lit,
                                                                      hit, nullptr, occ);
       out[(size_t)y * g.width + x] = color;
     }
@@ -386,6 +389,20 @@ static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4*
   // compact window of the brick order however unevenly the rays run
   cudaError_t e = cudaMemsetAsync(&cnt->tiles_light, 0, sizeof(unsigned), st);
   if (e != cudaSuccess) return e;
+  if (g.rect && !PREC) {
+    // explicit rectilinear coordinates, exact form: binary-search cell location, no
+    // empty-space skipping (the precision form keeps the seeded walk, correct for
+    // any increasing coordinates)
+    if constexpr (!STITCH && !PREC && std::is_same<QuadT, float4>::value) {
+      e = persistent_grid(k_light_march<float4, false, false, false, true>, smem, ntiles, grid);
+      if (e != cudaSuccess) return e;
+      k_light_march<float4, false, false, false, true><<<grid, kThreads, smem, st>>>(
+          g, (const float4*)quads, tab, tf, tau, map, nvert, cnt, refs, nrefs, self, gate, nullptr);
+      return cudaGetLastError();
+    } else {
+      return cudaErrorInvalidValue;
+    }
+  }
   if (occ) {
     e = persistent_grid(k_light_march<QuadT, STITCH, PREC, true>, smem, ntiles, grid);
     if (e != cudaSuccess) return e;
@@ -562,6 +579,20 @@ cudaError_t launch_view_march_f32(const ExactGeo& g, const float* field, const f
     e = persistent_grid(k_view_march_cells<float>, smem, ntiles, grid);
     if (e != cudaSuccess) return e;
     k_view_march_cells<float><<<grid, kThreads, smem, st>>>(g, field, tab, tf, out, cnt);
+  } else if (g.rect) {
+    // explicit rectilinear coordinates (single light, no empty-space skipping)
+    if (g.n_lights > 1) return cudaErrorInvalidValue;
+    if (g.use_map) {
+      e = persistent_grid(k_view_march<float4, true, float, false, false, false, true>, smem, ntiles, grid);
+      if (e != cudaSuccess) return e;
+      k_view_march<float4, true, float, false, false, false, true><<<grid, kThreads, smem, st>>>(g, quads, tab, tf,
+                                                                                                map, out, cnt);
+    } else {
+      e = persistent_grid(k_view_march<float4, false, float, false, false, false, true>, smem, ntiles, grid);
+      if (e != cudaSuccess) return e;
+      k_view_march<float4, false, float, false, false, false, true><<<grid, kThreads, smem, st>>>(
+          g, quads, tab, tf, (const float*)nullptr, out, cnt);
+    }
   } else if (g.use_map && g.n_lights > 1) {
     // the multi-light extension (empty-space skipping is not combined with it)
     e = persistent_grid(k_view_march<float4, true, float, false, false, true>, smem, ntiles, grid);

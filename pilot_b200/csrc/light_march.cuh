@@ -57,7 +57,7 @@ template <> struct Accum<true> {
 // March from L towards vertex V. prefix(dir) gives the starting opacity (0,
 // or the cross-brick prefix of the multi-brick Phase 3). ns counts the samples
 // marched. With SKIP, occ is the macro-cell occupancy (see occupied()).
-template <typename QuadT, bool PREC, bool SKIP, typename Prefix>
+template <typename QuadT, bool PREC, bool SKIP, bool RECT = false, typename Prefix>
 __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __restrict__ quads, const float4* T0,
                                              const float4* T1, const float4* T2, const float* s_a,
                                              const float* s_tau, const unsigned char* __restrict__ occ,
@@ -121,9 +121,16 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
         continue;
       }
       float4 e0, e1, e2;
-      const int c0 = find_cell_bsearch_t(T0, cm0, g.org[0], g.invh[0], s[0], e0);
-      const int c1 = find_cell_bsearch_t(T1, cm1, g.org[1], g.invh[1], s[1], e1);
-      const int c2 = find_cell_bsearch_t(T2, cm2, g.org[2], g.invh[2], s[2], e2);
+      int c0, c1, c2;
+      if constexpr (RECT) {
+        c0 = find_cell_bsearch_rect(T0, cm0, s[0], e0);
+        c1 = find_cell_bsearch_rect(T1, cm1, s[1], e1);
+        c2 = find_cell_bsearch_rect(T2, cm2, s[2], e2);
+      } else {
+        c0 = find_cell_bsearch_t(T0, cm0, g.org[0], g.invh[0], s[0], e0);
+        c1 = find_cell_bsearch_t(T1, cm1, g.org[1], g.invh[1], s[1], e1);
+        c2 = find_cell_bsearch_t(T2, cm2, g.org[2], g.invh[2], s[2], e2);
+      }
       QuadLoad<QuadT>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qz, v8);
       // pcoords = (p - min) / (max - min) (RectilinearMeshOracle.h:189-192)
       pc[0] = div_rn_markstein(s[0] - e0.x, e0.z, e0.w);

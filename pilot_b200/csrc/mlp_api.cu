@@ -356,9 +356,9 @@ beams_status beams_mlp_train(beams_renderer* r, const beams_mlp_options* opt, be
     r->form = saved_form;
     return s;
   }
-  if (r->brick_mode || r->vol.assoc != BEAMS_ASSOC_POINTS) {
+  if (r->brick_mode || r->vol.assoc != BEAMS_ASSOC_POINTS || r->rect) {
     r->form = saved_form;
-    return fail(r, BEAMS_ERR_UNSUPPORTED, "mlp_train: needs a single float32 point volume");
+    return fail(r, BEAMS_ERR_UNSUPPORTED, "mlp_train: needs a single float32 point volume with uniform spacing");
   }
   cudaSetDevice(r->device);
   ExactGeo g;

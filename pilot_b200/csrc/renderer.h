@@ -105,6 +105,9 @@ struct beams_renderer {
   bool reuse_map = false;
   bool bg = false;
   float bg_rgba[4] = {1.f, 1.f, 1.f, 1.f};
+  // explicit rectilinear coordinates of the volume's point axes (beams_set_volume_coordinates)
+  bool rect = false;
+  std::vector<float> coords[3];
   // canvas depth buffer (beams_set_depth_buffer) and the per-pixel ray limits derived from it
   bool depth_set = false;
   int depth_w = 0, depth_h = 0, depth_kind = 0;

@@ -31,7 +31,8 @@ struct NoRecord {
 // SKIP: samples in macro-cells whose occupancy is 0 (every value there maps to
 // an in-range TF entry of alpha 0) only advance and count as lit: their
 // premultiplied alpha is 0, so they change neither colour nor alpha.
-template <typename QuadT, bool USE_MAP, typename MapT, typename Rec = NoRecord, bool SKIP = false, bool MULTI = false>
+template <typename QuadT, bool USE_MAP, typename MapT, typename Rec = NoRecord, bool SKIP = false, bool MULTI = false,
+          bool RECT = false>
 __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT* __restrict__ quads,
                                                  const float4* s_tab, const float4* s_tf,
                                                  const MapT* __restrict__ map, int x, int y, float4& color,
@@ -84,7 +85,8 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT*
           c[k] = g.n[k] - 2;  // the reference leaves invSpacing[k] unchanged here
           e = T[c[k]];
         } else {
-          c[k] = find_cell_walk_t(T, g.n[k] - 2, g.org[k], g.invh[k], p[k], e);
+          if constexpr (RECT) c[k] = find_cell_walk_rect(T, g.n[k] - 2, p[k], e);
+          else c[k] = find_cell_walk_t(T, g.n[k] - 2, g.org[k], g.invh[k], p[k], e);
           inv[k] = e.w;  // 1.f / (coord(c+1) - coord(c)), IEEE
         }
         bl[k] = e.x;

@@ -254,3 +254,27 @@ def test_background_blend_is_over():
     assert np.allclose(out[0, 0], [0.8, 0.4, 0.2, 0.8])
     assert np.allclose(out[0, 1], [0.2 + 0.4, 0.1 + 0.2, 0.1, 0.5 + 0.4])
     assert np.array_equal(out[0, 2], img[0, 2])
+
+
+def test_explicit_uniform_coordinates_equal_generated_ones():
+    """Explicit coordinates equal to the generated float32 origin + spacing * i
+    give the same map and image as the generated (counting) coordinates."""
+    s = scenes.small(9, n=24, image=32, m=10)
+    base_m, _ = Oracle(s).light_march()
+    base_i, base_lit = Oracle(s).view_march(base_m)
+    h = np.float32(s.spacing[0])
+    c = np.float32(s.origin[0]) + h * np.arange(s.dims[0], dtype=np.float32)
+    s.coords = (c, c.copy(), c.copy())
+    m, _ = Oracle(s).light_march()
+    i, lit = Oracle(s).view_march(m)
+    assert np.array_equal(m, base_m) and np.array_equal(i, base_i) and lit == base_lit
+
+
+def test_stretched_coordinates_move_the_samples():
+    s = scenes.small(9, n=24, image=32, m=10)
+    base_m, _ = Oracle(s).light_march()
+    t = np.linspace(0, 1, s.dims[0])
+    s.coords = tuple(np.float32(t ** p) for p in (1.4, 1.0, 0.8))
+    m, _ = Oracle(s).light_march()
+    assert not np.array_equal(m, base_m)
+    assert np.all((m >= 0) & (m <= 1))

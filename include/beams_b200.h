@@ -148,6 +148,27 @@ beams_status beams_set_slab_fp64(beams_renderer* r, int enable);
 /* Keep the last map when its inputs (volume, colour map, light, map size) did not
  * change. Off by default: the reference rebuilds the map every frame. */
 beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable);
+/* ---- legacy VTK files ---------------------------------------------------------
+ * Replaces the reference's dataset read (pilot/io/DataSetUtils.cxx:13-42, VTK-m's
+ * legacy reader) for structured volumes: DATASET STRUCTURED_POINTS or
+ * RECTILINEAR_GRID, ASCII or BINARY, with POINT_DATA or CELL_DATA and one
+ * one-component SCALARS array of any numeric type, read as float32 (x fastest).
+ * coords[d] is NULL for STRUCTURED_POINTS; for RECTILINEAR_GRID it holds the
+ * dims[d] axis coordinates (then origin/spacing give the first value and the
+ * average spacing). Host memory, freed by beams_vtk_free. Host code only. */
+typedef struct beams_vtk_field {
+  int dims[3];        /* point dimensions */
+  int assoc;          /* beams_assoc */
+  double origin[3];
+  double spacing[3];
+  float* coords[3];
+  float* data;
+  double range[2];    /* min / max of the scalars */
+  char name[64];
+} beams_vtk_field;
+beams_status beams_vtk_read(const char* path, beams_vtk_field* out);
+void beams_vtk_free(beams_vtk_field* f);
+
 /* Explicit rectilinear coordinates for the current point volume (after
  * beams_set_volume): x, y, z hold dims[0], dims[1], dims[2] strictly increasing
  * float32 coordinates, the arrays of the ArrayHandleCartesianProduct coordinate
@@ -493,6 +514,8 @@ typedef struct beams_scene_desc {
   int mlp_knot;
   float mlp_probe_fraction, mlp_fallback_tol;
   int mlp_samples_log2, mlp_lights;
+  char file_name[256];      /* provider type "vtk_file": the legacy VTK volume (relative paths
+                               are taken from the stage file's directory by beams_load_config_toml) */
 } beams_scene_desc;
 
 /* Parses TOML text / a TOML file into *out (defaults for absent keys). On a

@@ -103,7 +103,8 @@ class SceneDesc(C.Structure):
                 ("lights", ConfigLight * 8), ("tf_preset", C.c_char * 32), ("tf_points", C.c_int),
                 ("tf_x", C.c_double * 64), ("tf_alpha", C.c_float * 64), ("tf_range", C.c_float * 2),
                 ("tf_size", C.c_int), ("mlp_knot", C.c_int), ("mlp_probe_fraction", C.c_float),
-                ("mlp_fallback_tol", C.c_float), ("mlp_samples_log2", C.c_int), ("mlp_lights", C.c_int)]
+                ("mlp_fallback_tol", C.c_float), ("mlp_samples_log2", C.c_int), ("mlp_lights", C.c_int),
+                ("file_name", C.c_char * 256)]
 
 
 def parse_config(text: str) -> SceneDesc:
@@ -139,6 +140,12 @@ class Timings(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class VtkField(C.Structure):
+    _fields_ = [("dims", C.c_int * 3), ("assoc", C.c_int), ("origin", C.c_double * 3), ("spacing", C.c_double * 3),
+                ("coords", C.POINTER(C.c_float) * 3), ("data", C.POINTER(C.c_float)), ("range", C.c_double * 2),
+                ("name", C.c_char * 64)]
 
 
 _lib = None
@@ -195,6 +202,8 @@ def lib():
         "beams_get_ray_limits": ([P, C.POINTER(Camera), P, C.c_int], C.c_int),
         "beams_synchronize": ([P], C.c_int),
         "beams_set_volume_coordinates": ([P, P, P, P], C.c_int),
+        "beams_vtk_read": ([C.c_char_p, C.POINTER(VtkField)], C.c_int),
+        "beams_vtk_free": ([C.POINTER(VtkField)], None),
         "beams_test_fail_allocation": ([C.c_int], C.c_int),
         "beams_get_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "beams_batch_set_volumes": ([P, P, C.c_int], C.c_int),
@@ -590,6 +599,30 @@ class Renderer:
         m = np.empty(count, np.float32)
         self._check(self._L.beams_get_shadow_map(self._h, _ptr(m), m.size, 0))
         return m
+
+
+def vtk_read(path):
+    """Reads a legacy VTK structured volume (beams_vtk_read): a dict with dims
+    (point dims, x y z), assoc, origin, spacing, coords (three arrays for a
+    rectilinear grid, else None), data (float32, shape z, y, x of points or
+    cells), range and name."""
+    L = lib()
+    f = VtkField()
+    st = L.beams_vtk_read(str(path).encode(), C.byref(f))
+    if st != BEAMS_OK:
+        raise BeamsError(st, L.beams_last_error(None).decode())
+    try:
+        nx, ny, nz = f.dims
+        shape = (nz, ny, nx) if f.assoc == ASSOC_POINTS else (nz - 1, ny - 1, nx - 1)
+        n = int(np.prod(shape))
+        data = np.ctypeslib.as_array(f.data, shape=(n,)).copy().reshape(shape)
+        coords = None
+        if f.coords[0]:
+            coords = [np.ctypeslib.as_array(f.coords[d], shape=(f.dims[d],)).copy() for d in range(3)]
+        return {"dims": tuple(f.dims), "assoc": f.assoc, "origin": tuple(f.origin), "spacing": tuple(f.spacing),
+                "coords": coords, "data": data, "range": tuple(f.range), "name": f.name.decode()}
+    finally:
+        L.beams_vtk_free(C.byref(f))
 
 
 def selftest_division(origin: float, spacing: float, ncells: int, samples: int):

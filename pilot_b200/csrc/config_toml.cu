@@ -345,11 +345,15 @@ struct Schema {
         std::snprintf(d.provider_name, sizeof(d.provider_name), "%s", name.c_str());
         if (k == "type") {
           const std::string v = str();
-          if (v != "subdivided_spheres" && v != "spheres" && v != "blobs" && v != "noise")
+          if (v != "subdivided_spheres" && v != "spheres" && v != "blobs" && v != "noise" && v != "vtk_file")
             bad("unknown dataset provider type '" + v + "'");
           std::snprintf(d.provider_type, sizeof(d.provider_type), "%s", v.c_str());
         } else if (k == "cell_dims") {
           int3(d.cell_dims, 1, 4095);
+        } else if (k == "file_name") {
+          const std::string v = str();
+          if (v.empty() || v.size() >= sizeof(d.file_name)) bad("'file_name' must be 1..255 characters");
+          std::snprintf(d.file_name, sizeof(d.file_name), "%s", v.c_str());
         } else if (k == "seed") {
           d.seed = (unsigned)integer();
         } else if (k == "octaves") {
@@ -542,7 +546,21 @@ beams_status beams_load_config_toml(const char* path, beams_scene_desc* out, cha
   }
   std::stringstream ss;
   ss << f.rdbuf();
-  return beams_parse_config_toml(ss.str().c_str(), out, err, errlen);
+  beams_status st = beams_parse_config_toml(ss.str().c_str(), out, err, errlen);
+  if (st == BEAMS_OK && out->file_name[0] && out->file_name[0] != '/') {
+    // a relative dataset file is relative to the stage file's directory
+    const std::string p(path);
+    const size_t slash = p.find_last_of('/');
+    if (slash != std::string::npos) {
+      const std::string full = p.substr(0, slash + 1) + out->file_name;
+      if (full.size() >= sizeof(out->file_name)) {
+        if (err && errlen > 0) std::snprintf(err, (size_t)errlen, "dataset file path too long");
+        return BEAMS_ERR_CONFIG;
+      }
+      std::snprintf(out->file_name, sizeof(out->file_name), "%s", full.c_str());
+    }
+  }
+  return st;
 }
 
 }  // extern "C"

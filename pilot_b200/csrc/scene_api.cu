@@ -208,11 +208,45 @@ beams_status beams_generate_spheres(float* dev_out, const int n[3], const double
   return BEAMS_OK;
 }
 
-beams_status beams_apply_scene(beams_renderer* r, const beams_scene_desc* d, beams_camera* camera_out) {
-  if (!r || !d) return fail(r, BEAMS_ERR_INVALID_ARG, "apply_scene: NULL argument");
-  cudaSetDevice(r->device);
+// The "vtk_file" provider: a legacy VTK volume from disk (the reference's
+// FileDescriptor scenes, read through pilot/io/DataSetUtils.cxx:13-42).
+static beams_status load_vtk_scene(beams_renderer* r, const beams_scene_desc* d, int cells[3], double org[3],
+                                   double hi[3]) {
+  if (!d->file_name[0]) return fail(r, BEAMS_ERR_CONFIG, "apply_scene: vtk_file provider without file_name");
+  beams_vtk_field f;
+  beams_status s = beams_vtk_read(d->file_name, &f);
+  if (s != BEAMS_OK) return fail(r, s, std::string("apply_scene: ") + beams_last_error(nullptr));
+  beams_volume v;
+  std::memset(&v, 0, sizeof(v));
+  v.data = f.data;
+  v.dtype = BEAMS_F32;
+  v.assoc = f.assoc;
+  v.on_device = 0;
+  for (int k = 0; k < 3; ++k) {
+    v.dims[k] = f.dims[k];
+    v.origin[k] = f.origin[k];
+    v.spacing[k] = f.spacing[k];
+    cells[k] = f.dims[k] - 1;
+  }
+  v.range[0] = f.range[0];
+  v.range[1] = f.range[1];
+  s = beams_set_volume(r, &v);
+  if (s == BEAMS_OK) s = cudaStreamSynchronize(r->stream) == cudaSuccess ? BEAMS_OK : BEAMS_ERR_CUDA;
+  if (s == BEAMS_OK && f.coords[0]) s = beams_set_volume_coordinates(r, f.coords[0], f.coords[1], f.coords[2]);
+  for (int k = 0; k < 3; ++k) {
+    org[k] = f.coords[k] ? (double)f.coords[k][0] : (double)(float)f.origin[k];
+    hi[k] = f.coords[k] ? (double)f.coords[k][f.dims[k] - 1]
+                        : (double)((float)f.origin[k] + (float)f.spacing[k] * (float)(f.dims[k] - 1));
+  }
+  beams_vtk_free(&f);
+  return s;
+}
+
+// The generated providers (SceneFactory / DataSetFactory): the field on
+// [0,1]^3 with cell_dims + 1 points per axis, generated on the device.
+static beams_status generate_scene(beams_renderer* r, const beams_scene_desc* d, double org[3], double hi[3]) {
   int pts[3];
-  double org[3] = {0, 0, 0}, sp[3], hi[3];
+  double sp[3];
   for (int k = 0; k < 3; ++k) {
     pts[k] = d->cell_dims[k] + 1;
     if (d->cell_dims[k] < 1) return fail(r, BEAMS_ERR_CONFIG, "apply_scene: cell_dims must be positive");
@@ -285,6 +319,22 @@ beams_status beams_apply_scene(beams_renderer* r, const beams_scene_desc* d, bea
   v.on_device = 1;
   s = beams_set_volume(r, &v);
   if (s != BEAMS_OK) return s;
+  return BEAMS_OK;
+}
+
+beams_status beams_apply_scene(beams_renderer* r, const beams_scene_desc* d, beams_camera* camera_out) {
+  if (!r || !d) return fail(r, BEAMS_ERR_INVALID_ARG, "apply_scene: NULL argument");
+  cudaSetDevice(r->device);
+  int cells[3];
+  double org[3] = {0, 0, 0}, hi[3];
+  beams_status s;
+  if (std::string(d->provider_type) == "vtk_file") {
+    s = load_vtk_scene(r, d, cells, org, hi);
+  } else {
+    s = generate_scene(r, d, org, hi);
+    for (int k = 0; k < 3; ++k) cells[k] = d->cell_dims[k];
+  }
+  if (s != BEAMS_OK) return s;
   std::vector<float> tf;
   build_table(*d, tf);
   s = beams_set_color_map(r, tf.data(), d->tf_size);
@@ -292,7 +342,7 @@ beams_status beams_apply_scene(beams_renderer* r, const beams_scene_desc* d, bea
   int m[3];
   for (int k = 0; k < 3; ++k) {
     if (d->shadow_size[k] > 0) m[k] = d->shadow_size[k];
-    else if (d->shadow_size_ratio > 0.f) m[k] = std::max(1, (int)((float)d->cell_dims[k] * d->shadow_size_ratio));
+    else if (d->shadow_size_ratio > 0.f) m[k] = std::max(1, (int)((float)cells[k] * d->shadow_size_ratio));
     else m[k] = 16;  // LightedVolumeRenderer.cxx:752-759
   }
   s = beams_set_shadow_map_size(r, m[0], m[1], m[2]);

@@ -104,3 +104,14 @@ def test_cool_to_warm_table_and_alpha_points():
     assert np.allclose(t[:, 3], np.clip((v - 0.2) / 0.6, 0, 1), atol=1e-6)
     r = B.scene_color_table(B.parse_config('[transfer_function]\npreset = "ramp"\n'))
     assert np.allclose(r[0, :3], [0.23, 0.30, 0.75], atol=1e-6)
+
+
+def test_vtk_file_provider_path_resolution(tmp_path):
+    (tmp_path / "stage.toml").write_text('[dataset_providers.v]\ntype = "vtk_file"\nfile_name = "data/v.vtk"\n')
+    d = B.load_config(tmp_path / "stage.toml")
+    assert d.provider_type.decode() == "vtk_file"
+    assert d.file_name.decode() == str(tmp_path / "data" / "v.vtk")
+    d2 = B.parse_config('[dataset_providers.v]\ntype = "vtk_file"\nfile_name = "/abs/v.vtk"\n')
+    assert d2.file_name.decode() == "/abs/v.vtk"
+    with pytest.raises(B.BeamsError):
+        B.parse_config('[dataset_providers.v]\ntype = "vtk_file"\nfile_name = ""\n')

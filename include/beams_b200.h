@@ -295,10 +295,18 @@ beams_status beams_set_batch_options(beams_renderer* r, const beams_batch_option
 beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, int n, beams_timings* t);
 /* Tunes the batch options on these requests by coordinate descent over the
  * empty-space skip, the vertex order {rows, 8, 16, 32, 64 bricks} and the view
- * tile {16x16, 32x8, 8x32, 32x32, 64x32, 64x64}; keeps the fastest (images are identical
+ * tile {8x8, 16x16, 32x8, 8x32, 32x32, 64x32, 64x64}; keeps the fastest (images are identical
  * under all of them) and reports it. */
 beams_status beams_batch_autotune(beams_renderer* r, const beams_request* reqs, int n, beams_batch_options* best,
                                   float* best_ms);
+/* The autotuner's results cache: beams_batch_autotune keeps its result per batch
+ * shape (each request's volume dimensions, map size and image size; cameras and
+ * lights may differ) and returns it without timing when the same shape comes
+ * again. A serving process saves the cache to a text file and loads it at
+ * start-up (after beams_batch_set_volumes) to skip the tuning runs. */
+beams_status beams_batch_tuning_save(beams_renderer* r, const char* path);
+beams_status beams_batch_tuning_load(beams_renderer* r, const char* path);
+beams_status beams_batch_tuning_clear(beams_renderer* r);
 
 /* ---- learned form ------------------------------------------------------------ */
 /* No reference counterpart: a transmittance network (encoded position and light

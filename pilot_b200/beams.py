@@ -201,6 +201,9 @@ def lib():
         "beams_set_depth_buffer": ([P, P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int], C.c_int),
         "beams_get_ray_limits": ([P, C.POINTER(Camera), P, C.c_int], C.c_int),
         "beams_synchronize": ([P], C.c_int),
+        "beams_batch_tuning_save": ([P, C.c_char_p], C.c_int),
+        "beams_batch_tuning_load": ([P, C.c_char_p], C.c_int),
+        "beams_batch_tuning_clear": ([P], C.c_int),
         "beams_set_volume_coordinates": ([P, P, P, P], C.c_int),
         "beams_vtk_read": ([C.c_char_p, C.POINTER(VtkField)], C.c_int),
         "beams_vtk_free": ([C.POINTER(VtkField)], None),
@@ -373,6 +376,15 @@ class Renderer:
         self._check(self._L.beams_batch_autotune(self._h, arr, len(reqs), C.byref(o), C.byref(ms)))
         return {"tile_w": o.tile_w, "tile_h": o.tile_h, "light_brick": o.light_brick, "skip": not o.no_skip,
                 "batch_ms": ms.value}
+
+    def batch_tuning_save(self, path):
+        self._check(self._L.beams_batch_tuning_save(self._h, str(path).encode()))
+
+    def batch_tuning_load(self, path):
+        self._check(self._L.beams_batch_tuning_load(self._h, str(path).encode()))
+
+    def batch_tuning_clear(self):
+        self._check(self._L.beams_batch_tuning_clear(self._h))
 
     def render_batch(self, reqs, timings=True):
         """reqs: list of (Request, out) from Renderer.request; returns the outputs and timings."""

@@ -4,7 +4,12 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <string>
 #include <vector>
 
 #include "../../include/beams_b200.h"
@@ -31,9 +36,16 @@ struct BatchVolume {
   }
 };
 
+struct BatchTuned {
+  beams_batch_options opts;
+  float ms;
+};
+
 struct BatchState {
   std::vector<BatchVolume*> vols;
   beams_batch_options opts{32, 32, 8, 1, 0, 0};
+  // autotuner results per batch shape (tuning_key), kept for later calls and files
+  std::map<std::string, BatchTuned> tuned;
   // per-signature device state
   std::vector<long long> sig;
   void* arena = nullptr;
@@ -413,11 +425,39 @@ beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, in
   return BEAMS_OK;
 }
 
+// The shape of a batch as the autotuner sees it: per request the volume's point
+// dims, the map size and the image size (cameras and lights vary freely).
+static bool tuning_key(const BatchState* b, const beams_request* reqs, int n, std::string& key) {
+  std::ostringstream k;
+  k << n;
+  for (int i = 0; i < n; ++i) {
+    const beams_request& q = reqs[i];
+    if (q.volume < 0 || q.volume >= (int)b->vols.size()) return false;
+    const beams_volume& v = b->vols[q.volume]->vol;
+    k << ';' << v.dims[0] << ',' << v.dims[1] << ',' << v.dims[2] << ',' << q.map_cells << ','
+      << q.camera.width << ',' << q.camera.height;
+  }
+  key = k.str();
+  return true;
+}
+
 beams_status beams_batch_autotune(beams_renderer* r, const beams_request* reqs, int n, beams_batch_options* best,
                                   float* best_ms) {
   if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
   BatchState* b = r->batch;
   if (!b) return fail(r, BEAMS_ERR_STATE, "batch_autotune: no batch volumes set");
+  if (!reqs || n < 1) return fail(r, BEAMS_ERR_INVALID_ARG, "batch_autotune: no requests");
+  std::string key;
+  const bool keyed = tuning_key(b, reqs, n, key);
+  if (keyed) {
+    const auto it = b->tuned.find(key);
+    if (it != b->tuned.end()) {  // tuned before: keep that result
+      beams_status s = beams_set_batch_options(r, &it->second.opts);
+      if (s == BEAMS_OK && best) *best = it->second.opts;
+      if (s == BEAMS_OK && best_ms) *best_ms = it->second.ms;
+      return s;
+    }
+  }
   const beams_batch_options keep = b->opts;
   cudaEvent_t a, z;
   cudaEventCreate(&a);
@@ -482,9 +522,60 @@ beams_status beams_batch_autotune(beams_renderer* r, const beams_request* reqs, 
     return s;
   }
   s = beams_set_batch_options(r, &bo);
+  if (s == BEAMS_OK && keyed) b->tuned[key] = BatchTuned{bo, bt};
   if (best) *best = bo;
   if (best_ms) *best_ms = bt;
   return s;
+}
+
+beams_status beams_batch_tuning_clear(beams_renderer* r) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  if (r->batch) r->batch->tuned.clear();
+  return BEAMS_OK;
+}
+
+// Text file: a header line, then one line per batch shape:
+// <key> <tile_w> <tile_h> <light_brick> <no_skip> <ms>
+beams_status beams_batch_tuning_save(beams_renderer* r, const char* path) {
+  if (!r || !path) return fail(r, BEAMS_ERR_INVALID_ARG, "batch_tuning_save: NULL argument");
+  std::ofstream f(path);
+  if (!f) return fail(r, BEAMS_ERR_INVALID_ARG, std::string("batch_tuning_save: cannot write ") + path);
+  f << "beams-batch-tuning 1\n";
+  if (r->batch)
+    for (const auto& e : r->batch->tuned)
+      f << e.first << ' ' << e.second.opts.tile_w << ' ' << e.second.opts.tile_h << ' '
+        << e.second.opts.light_brick << ' ' << e.second.opts.no_skip << ' ' << e.second.ms << '\n';
+  if (!f) return fail(r, BEAMS_ERR_INVALID_ARG, std::string("batch_tuning_save: write failed: ") + path);
+  return BEAMS_OK;
+}
+
+beams_status beams_batch_tuning_load(beams_renderer* r, const char* path) {
+  if (!r || !path) return fail(r, BEAMS_ERR_INVALID_ARG, "batch_tuning_load: NULL argument");
+  if (!r->batch) return fail(r, BEAMS_ERR_STATE, "batch_tuning_load: no batch volumes set");
+  std::ifstream f(path);
+  if (!f) return fail(r, BEAMS_ERR_INVALID_ARG, std::string("batch_tuning_load: cannot read ") + path);
+  std::string line;
+  if (!std::getline(f, line) || line != "beams-batch-tuning 1")
+    return fail(r, BEAMS_ERR_CONFIG, "batch_tuning_load: not a batch tuning file");
+  std::map<std::string, BatchTuned> got;
+  int ln = 1;
+  while (std::getline(f, line)) {
+    ++ln;
+    if (line.empty()) continue;
+    std::istringstream is(line);
+    std::string key;
+    BatchTuned t{};
+    t.opts = r->batch->opts;
+    if (!(is >> key >> t.opts.tile_w >> t.opts.tile_h >> t.opts.light_brick >> t.opts.no_skip >> t.ms) ||
+        t.opts.tile_w < 8 || t.opts.tile_w % 8 || t.opts.tile_h < 4 || t.opts.tile_h % 4 ||
+        t.opts.tile_w * t.opts.tile_h > 16384 || log2_brick(t.opts.light_brick) < 0 ||
+        (t.opts.no_skip != 0 && t.opts.no_skip != 1))
+      return fail(r, BEAMS_ERR_CONFIG, "batch_tuning_load: bad entry on line " + std::to_string(ln));
+    t.opts.reserved = 0;
+    got[key] = t;
+  }
+  for (auto& e : got) r->batch->tuned[e.first] = e.second;
+  return BEAMS_OK;
 }
 
 }  // extern "C"

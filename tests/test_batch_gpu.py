@@ -121,3 +121,41 @@ def test_batch_autotune_keeps_images(cuda_device):
         for o, spec in zip(outs, specs):
             ref, _ = _single(vols[spec["volume"]], tf, spec)
             assert np.array_equal(_as_np(o), ref)
+
+
+def test_batch_tuning_cache_and_file(cuda_device, tmp_path):
+    """The autotuner keeps its result per batch shape: the same shape with new
+    cameras and lights is answered from the cache (no timing runs), and a saved
+    cache file lets another renderer skip tuning too."""
+    import time
+    vols = _volumes()
+    tf = scenes.tf_table()
+    rng = np.random.default_rng(12)
+    with B.Renderer(0) as r:
+        r.set_color_map(tf)
+        r.batch_set_volumes([(s.field_numpy(), s.origin, s.spacing, s.value_range) for s in vols])
+        reqs, _ = _requests(vols, rng, device_out=False)
+        t0 = time.perf_counter()
+        first = r.batch_autotune(reqs)
+        t_tune = time.perf_counter() - t0
+        reqs2, _ = _requests(vols, rng, device_out=False)  # same shapes, new cameras and lights
+        t0 = time.perf_counter()
+        again = r.batch_autotune(reqs2)
+        t_hit = time.perf_counter() - t0
+        assert again == first and t_hit < t_tune / 5
+        path = tmp_path / "tuning.txt"
+        r.batch_tuning_save(path)
+        r.batch_tuning_clear()
+    with B.Renderer(0) as q:
+        q.set_color_map(tf)
+        q.batch_set_volumes([(s.field_numpy(), s.origin, s.spacing, s.value_range) for s in vols])
+        q.batch_tuning_load(path)
+        t0 = time.perf_counter()
+        loaded = q.batch_autotune(reqs2)
+        assert time.perf_counter() - t0 < t_tune / 5
+        assert {k: loaded[k] for k in ("tile_w", "tile_h", "light_brick", "skip")} == \
+               {k: first[k] for k in ("tile_w", "tile_h", "light_brick", "skip")}
+        bad = tmp_path / "bad.txt"
+        bad.write_text("beams-batch-tuning 1\nkey 7 4 8 0 1.0\n")
+        with pytest.raises(B.BeamsError):
+            q.batch_tuning_load(bad)

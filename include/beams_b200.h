@@ -321,7 +321,7 @@ typedef struct beams_mlp_options {
   unsigned seed;
   float fallback_tol;    /* render: |MLP - exact| on the probe set that sends a tile to the exact map (0.01) */
   float probe_fraction;  /* render: fraction of pixels probed (0.01) */
-  int knot;              /* render: MLP evaluated every `knot` lit samples, linear in between (1 = every sample) */
+  int knot;              /* render: MLP evaluated every `knot` lit samples (1..64), linear in between (1 = every sample) */
   int scene_light;       /* train: 1 = the renderer's current light is training light 0 (a directional light
                             stands in as a point at 1e4 x the diagonal); the rest on the Fibonacci sphere */
   float focus;           /* train: fraction of positions drawn where the colour map's alpha is non-zero

@@ -479,7 +479,7 @@ struct Schema {
       } else if (t == "form") {
         if (k == "knot") {
           d.mlp_knot = (int)integer();
-          if (d.mlp_knot < 1 || d.mlp_knot > 32) bad("'knot' must be in [1, 32]");
+          if (d.mlp_knot < 1 || d.mlp_knot > 64) bad("'knot' must be in [1, 64]");
         } else if (k == "probe_fraction") {
           d.mlp_probe_fraction = (float)num();
         } else if (k == "fallback_tol") {

@@ -182,7 +182,7 @@ __device__ __forceinline__ float mlp_eval_warp(const Encoding& enc, const float 
 
 using namespace mlp;
 
-constexpr int kKnotMax = 32;  // lit samples between two network evaluations, at most
+constexpr int kKnotMax = 64;  // lit samples between two network evaluations, at most
 
 __device__ __forceinline__ int next_warp_tile_mlp(unsigned* counter) {
   unsigned t = 0;

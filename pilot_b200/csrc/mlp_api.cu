@@ -155,7 +155,7 @@ beams_status mlp_set_render_options(beams_renderer* r, const beams_mlp_options* 
   d.probe_fraction = 0.01f;
   d.knot = 4;
   if (o) {
-    if (o->knot < 1 || o->knot > 32) return fail(r, BEAMS_ERR_INVALID_ARG, "mlp form: knot must be in [1, 32]");
+    if (o->knot < 1 || o->knot > 64) return fail(r, BEAMS_ERR_INVALID_ARG, "mlp form: knot must be in [1, 64]");
     if (!(o->probe_fraction >= 0.f && o->probe_fraction <= 1.f) || !(o->fallback_tol >= 0.f))
       return fail(r, BEAMS_ERR_INVALID_ARG, "mlp form: bad probe fraction or tolerance");
     d.knot = o->knot;

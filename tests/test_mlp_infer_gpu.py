@@ -87,7 +87,7 @@ def test_mlp_knot_interpolation_close_to_every_sample(cuda_device):
     p = psnr(i1, i4)
     print(f"knot 4 vs knot 1: PSNR {p:.1f} dB, evaluations {t4['mlp_samples']} vs {t1['mlp_samples']}")
     assert t4["mlp_samples"] < 0.4 * t1["mlp_samples"] and p > 40
-    for k in (16, 32):
+    for k in (16, 32, 64):
         ik, tk, _ = mlp_render(s, None, knot=k, r=r)
         pk = psnr(i1, ik)
         print(f"knot {k} vs knot 1: PSNR {pk:.1f} dB, evaluations {tk['mlp_samples']}")

@@ -4,19 +4,19 @@
 // (beams/rendering/MapperLightedVolume.cxx:114-193), each a map build followed
 // by a view march. Here a batch of requests (each its own volume, camera,
 // light and map size) is one grid of persistent blocks pulling work items from
-// a global queue: first every request's map-build items (256 vertices each),
-// then every view item (a tile of pixels). A view item of request r waits,
-// with a bounded wait, until all of r's map items have completed, so view work
-// of early requests overlaps the map builds of later ones and the grid never
-// drains between the two stages. Queue order guarantees progress: every item a
-// view item waits on was dequeued earlier by a running block that waits on
-// nothing.
+// a global queue (batch.h): map-build items (kBatchChunk vertex slots of the
+// light-aligned brick order each) and view items (a tile of pixels), with the
+// map items of one request beside the view items of the one before it. A view
+// item of request r waits, with a bounded wait, until all of r's map items have
+// completed, so the grid never drains between the two stages. Queue order
+// guarantees progress: every item a view item waits on was dequeued earlier by
+// a running block that waits on nothing.
 //
 // Per item a block keeps the request's geometry and cell tables in shared
 // memory (recomputed there when the request changes, so no table buffers or
 // table launches exist). Results equal the single-request kernels': the light
-// march per vertex is point_opacity (the K1 sample sequence) and the view march
-// is view_march_pixel. Compiled with -fmad=false like every kernel file.
+// march per vertex is march_vertex (the K1 march) and the view march is
+// view_march_pixel. Compiled with -fmad=false like every kernel file.
 #include <cuda_runtime.h>
 
 #include "batch.h"

@@ -290,3 +290,22 @@ def test_far_and_scaled_volumes_bit_exact(cuda_device, offset, scale):
     oimg, olit = o.view_march(om)
     assert np.max(np.abs(img - oimg)) <= TOL
     assert t["lit_samples"] == olit
+
+
+@pytest.mark.parametrize("light_kind", [0, 1])
+def test_non_cubic_volume_odd_image(cuda_device, light_kind):
+    """Different point counts per axis (so different spacings and brick counts
+    per axis of the light-aligned order) and an image whose sides are not
+    multiples of the 8x4 warp tile."""
+    import dataclasses
+    s = scenes.small(14, n=24, image=32, m=11, kind="noise", light_kind=light_kind)
+    s = dataclasses.replace(s, dims=(33, 21, 40), width=37, height=29, array=None)
+    img, m, t, _ = gpu_render(s)
+    o = Oracle(s)
+    om, _ = o.light_march()
+    assert np.array_equal(m, om), f"map mismatch: max {np.max(np.abs(m - om))}"
+    oimg, olit = o.view_march(om)
+    assert img.shape == (29, 37, 4)
+    assert np.max(np.abs(img - oimg)) <= TOL
+    assert np.mean(np.all(img == oimg, axis=-1)) > 0.999
+    assert t["lit_samples"] == olit

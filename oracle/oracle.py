@@ -82,7 +82,7 @@ class Oracle:
             _p(self.field), (C.c_int * 3)(*s.dims), (C.c_double * 3)(*s.origin), (C.c_double * 3)(*s.spacing),
             (C.c_double * 2)(*s.value_range), _p(self.tf), self.tf.shape[0], s.light_kind,
             (C.c_double * 3)(*s.light), (C.c_float * 3)(*s.light_color), s.light_intensity,
-            (C.c_int * 3)(s.map_m, s.map_m, s.map_m), int(s.use_map), s.sample_distance, s.cutoff,
+            (C.c_int * 3)(*self._map_cells(s.map_m)), int(s.use_map), s.sample_distance, s.cutoff,
             s.light_steps, int(s.slab_fp64), (C.c_double * 3)(*s.cam_pos), (C.c_double * 3)(*s.cam_look),
             (C.c_double * 3)(*s.cam_up), s.fov_y_deg, s.width, s.height, int(precision))
         coords = getattr(scene, "coords", None)
@@ -104,10 +104,15 @@ class Oracle:
             raise RuntimeError("oracle depth conversion rejected its input")
         return out
 
+    @staticmethod
+    def _map_cells(m):
+        """Map cells per axis (x, y, z): one integer for a cubic map, or three."""
+        return tuple(int(v) for v in m) if isinstance(m, (tuple, list)) else (int(m),) * 3
+
     @property
     def map_shape(self):
-        m = self.scene.map_m + 1
-        return (m, m, m)
+        mx, my, mz = self._map_cells(self.scene.map_m)
+        return (mz + 1, my + 1, mx + 1)
 
     def light_march(self, fp64: bool = False):
         out = np.empty(self.map_shape, np.float64 if fp64 else np.float32)

@@ -215,7 +215,10 @@ class Scene:
     def configure(self, r) -> None:
         """Applies every setting except the volume to a Renderer."""
         r.set_color_map(self.tf)
-        r.set_shadow_map_size(self.map_m)
+        if isinstance(self.map_m, (tuple, list)):
+            r.set_shadow_map_size(*self.map_m)
+        else:
+            r.set_shadow_map_size(self.map_m)
         r.set_use_shadow_map(self.use_map)
         r.clear_lights()
         if self.light_kind == 0:

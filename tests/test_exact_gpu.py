@@ -309,3 +309,25 @@ def test_non_cubic_volume_odd_image(cuda_device, light_kind):
     assert np.max(np.abs(img - oimg)) <= TOL
     assert np.mean(np.all(img == oimg, axis=-1)) > 0.999
     assert t["lit_samples"] == olit
+
+
+def test_non_cubic_map(cuda_device):
+    """A map with a different cell count per axis (beams_set_shadow_map_size(mx,
+    my, mz)) over a non-cubic volume: vertex bricks, pencils and map tables all
+    differ per axis."""
+    import dataclasses
+    s = scenes.small(15, n=24, image=40, m=8, kind="blobs")
+    s = dataclasses.replace(s, dims=(30, 26, 35), map_m=(11, 7, 14), array=None)
+    r = B.Renderer(0)
+    r.set_volume(s.field_numpy(), origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+    s.configure(r)
+    img, t = r.render(s.camera())
+    m = r.get_shadow_map(12 * 8 * 15).reshape(15, 8, 12)
+    o = Oracle(s)
+    om, _ = o.light_march()
+    assert om.shape == (15, 8, 12)
+    assert np.array_equal(m, om), f"map mismatch: max {np.max(np.abs(m - om))}"
+    oimg, olit = o.view_march(om)
+    assert np.max(np.abs(img - oimg)) <= TOL
+    assert np.mean(np.all(img == oimg, axis=-1)) > 0.999
+    assert t["lit_samples"] == olit

@@ -49,14 +49,16 @@ __device__ __forceinline__ void mma16816(float c[4], const unsigned a[4], const 
 
 // B fragments of W_l (row-major [in][64]) for every (k-tile, n-tile, lane):
 // lane (g = lane/4, t = lane%4) holds rows 16kt+2t, +1 and 16kt+2t+8, +9 of
-// column 8nt+g, bfloat16 pairs (low half = lower row).
+// column 8nt+g, bfloat16 pairs (low half = lower row). The fragments of
+// n-tiles 2j and 2j+1 sit side by side for each lane, so one 16-byte load
+// fetches both: uint2 index ((kt*4 + j)*32 + lane)*2 + (nt & 1) in the layer.
 __global__ void k_pack_weights(const float* __restrict__ P, uint2* __restrict__ W, float* __restrict__ aux) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < kPacked) {
     int l = 0;
     while (l < 3 && i >= off_l(l + 1)) ++l;
     const int rel = i - off_l(l);
-    const int lane = rel & 31, nt = (rel >> 5) & 7, kt = rel >> 8;
+    const int lane = (rel >> 1) & 31, nt = 2 * ((rel >> 6) & 3) + (rel & 1), kt = rel >> 8;
     const int g = lane >> 2, t = lane & 3;
     const int woff = (l == 0) ? oW1 : (l == 1 ? oW2 : (l == 2 ? oW3 : oW4));
     const int col = 8 * nt + g, r0 = 16 * kt + 2 * t;
@@ -94,7 +96,8 @@ __device__ __forceinline__ void to_a(const float C[8][4], const float* bias, int
 // T for the calling lane's row (lane = row of the warp's 32-row batch); every
 // lane of the warp must call it. kp: this lane's knot position; lf: light feature.
 __device__ __forceinline__ float mlp_eval_warp(const Encoding& enc, const float kp[3], const float lf[3],
-                                               const uint2* __restrict__ sW, const float* __restrict__ sAux) {
+                                               const uint2* __restrict__ sW, const float* __restrict__ sAux,
+                                               const float* __restrict__ s_freq) {
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   float mine = 0.f;
 #pragma unroll 1
@@ -117,14 +120,18 @@ __device__ __forceinline__ float mlp_eval_warp(const Encoding& enc, const float 
     for (int kt = 0; kt < 7; ++kt) {
       const int c0 = 16 * kt + 2 * t, c1 = c0 + 8;
       float x0, x1, y0, y1, z0, z1, w0, w1;
-      feature_pair(ua, lf, c0, x0, x1);
-      feature_pair(ub, lf, c0, y0, y1);
-      feature_pair(ua, lf, c1, z0, z1);
-      feature_pair(ub, lf, c1, w0, w1);
+      feature_pair(ua, lf, c0, x0, x1, s_freq);
+      feature_pair(ub, lf, c0, y0, y1, s_freq);
+      feature_pair(ua, lf, c1, z0, z1, s_freq);
+      feature_pair(ub, lf, c1, w0, w1, s_freq);
       const unsigned a[4] = {pack_bf16(x0, x1), pack_bf16(y0, y1), pack_bf16(z0, z1), pack_bf16(w0, w1)};
-      const uint2* wb = sW + off_l(0) + kt * 256 + lane;
+      const uint4* wb = reinterpret_cast<const uint4*>(sW + off_l(0) + kt * 256) + lane;
 #pragma unroll
-      for (int n = 0; n < 8; ++n) mma16816(C[n], a, wb[n * 32]);
+      for (int j = 0; j < 4; ++j) {
+        const uint4 w = wb[j * 32];
+        mma16816(C[2 * j], a, make_uint2(w.x, w.y));
+        mma16816(C[2 * j + 1], a, make_uint2(w.z, w.w));
+      }
     }
     unsigned A[4][4];
     to_a(C, sAux, t, A);
@@ -135,9 +142,13 @@ __device__ __forceinline__ float mlp_eval_warp(const Encoding& enc, const float 
       for (int n = 0; n < 8; ++n) C[n][0] = C[n][1] = C[n][2] = C[n][3] = 0.f;
 #pragma unroll
       for (int kt = 0; kt < 4; ++kt) {
-        const uint2* wb = sW + off_l(l) + kt * 256 + lane;
+        const uint4* wb = reinterpret_cast<const uint4*>(sW + off_l(l) + kt * 256) + lane;
 #pragma unroll
-        for (int n = 0; n < 8; ++n) mma16816(C[n], A[kt], wb[n * 32]);
+        for (int j = 0; j < 4; ++j) {
+          const uint4 w = wb[j * 32];
+          mma16816(C[2 * j], A[kt], make_uint2(w.x, w.y));
+          mma16816(C[2 * j + 1], A[kt], make_uint2(w.z, w.w));
+        }
       }
       to_a(C, sAux + l * kHid, t, A);
     }
@@ -213,6 +224,8 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
   for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) s_tf[i] = tf[i];
   for (int i = threadIdx.x; i < kPacked; i += blockDim.x) sW[i] = Wp[i];
   for (int i = threadIdx.x; i < kAux; i += blockDim.x) sAux[i] = aux[i];
+  __shared__ float s_freq[kFreq];  // the encoding's frequencies, once per block
+  if (threadIdx.x < kFreq) s_freq[threadIdx.x] = freq(threadIdx.x);
   __syncthreads();
   const float lf[3] = {lf0, lf1, lf2};
   const int tiles_x = (g.width + 7) >> 3;
@@ -337,7 +350,7 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
         tz = (p[2] - bl[2]) * inv[2];
         if (color.w >= g.cutoff) done = true;
       }
-      const float Tk = mlp_eval_warp(enc, kp, lf, sW, sAux);
+      const float Tk = mlp_eval_warp(enc, kp, lf, sW, sAux, s_freq);
       rows += 32;
       if (nb > 0) {
         ++evals;

@@ -52,11 +52,14 @@ __device__ __forceinline__ void sincospi_fast(float x, float* s, float* c) {
   __sincosf(3.14159265358979f * r, s, c);
 }
 
-// The (even) feature pair starting at column c of the encoding.
-__device__ __forceinline__ void feature_pair(const float u[3], const float l[3], int c, float& a, float& b) {
+// The (even) feature pair starting at column c of the encoding; fk[k] holds
+// freq(k) (a table filled once per block by the same function, so the
+// features are identical to computing it here).
+__device__ __forceinline__ void feature_pair(const float u[3], const float l[3], int c, float& a, float& b,
+                                             const float* fk = nullptr) {
   if (c >= 6 && c < kUsed) {
     const int q = c - 6, ax = q >> 5, k = (q & 31) >> 1;
-    sincospi_fast(freq(k) * u[ax], &a, &b);
+    sincospi_fast((fk ? fk[k] : freq(k)) * u[ax], &a, &b);
   } else if (c == 0) {
     a = u[0] * 2.f - 1.f;
     b = u[1] * 2.f - 1.f;

@@ -120,10 +120,17 @@ __device__ __forceinline__ float mlp_eval_warp(const Encoding& enc, const float 
     for (int kt = 0; kt < 7; ++kt) {
       const int c0 = 16 * kt + 2 * t, c1 = c0 + 8;
       float x0, x1, y0, y1, z0, z1, w0, w1;
-      feature_pair(ua, lf, c0, x0, x1, s_freq);
-      feature_pair(ub, lf, c0, y0, y1, s_freq);
-      feature_pair(ua, lf, c1, z0, z1, s_freq);
-      feature_pair(ub, lf, c1, w0, w1, s_freq);
+      if (kt >= 1 && kt <= 5) {  // columns 16..95: sin/cos features only
+        sincos_pair(ua, c0, s_freq, x0, x1);
+        sincos_pair(ub, c0, s_freq, y0, y1);
+        sincos_pair(ua, c1, s_freq, z0, z1);
+        sincos_pair(ub, c1, s_freq, w0, w1);
+      } else {
+        feature_pair(ua, lf, c0, x0, x1, s_freq);
+        feature_pair(ub, lf, c0, y0, y1, s_freq);
+        feature_pair(ua, lf, c1, z0, z1, s_freq);
+        feature_pair(ub, lf, c1, w0, w1, s_freq);
+      }
       const unsigned a[4] = {pack_bf16(x0, x1), pack_bf16(y0, y1), pack_bf16(z0, z1), pack_bf16(w0, w1)};
       const uint4* wb = reinterpret_cast<const uint4*>(sW + off_l(0) + kt * 256) + lane;
 #pragma unroll

@@ -52,6 +52,12 @@ __device__ __forceinline__ void sincospi_fast(float x, float* s, float* c) {
   __sincosf(3.14159265358979f * r, s, c);
 }
 
+// A sin/cos feature pair, c in [6, kUsed): the branch of feature_pair below.
+__device__ __forceinline__ void sincos_pair(const float u[3], int c, const float* fk, float& a, float& b) {
+  const int q = c - 6, ax = q >> 5, k = (q & 31) >> 1;
+  sincospi_fast(fk[k] * u[ax], &a, &b);
+}
+
 // The (even) feature pair starting at column c of the encoding; fk[k] holds
 // freq(k) (a table filled once per block by the same function, so the
 // features are identical to computing it here).

@@ -123,3 +123,30 @@ def test_bricks_with_depth_limits_and_background(cuda_device):
     img, _ = r.render(bricks[0].camera())
     orgba, _, _, _, _ = render_bricks(bricks, ray_limits=np.where(np.isnan(lim), np.inf, lim))
     check(img, blend_background(orgba, bg))
+
+
+def test_depth_limits_in_the_precision_and_learned_forms(cuda_device):
+    """The limits apply in every single-volume form: the alpha channel never
+    depends on the shading, so under the same limits the precision form's
+    alpha matches the oracle's precision mode and the learned form's alpha
+    equals the exact form's bit for bit, with equal lit-sample counts."""
+    from oracle.oracle import quantize
+    s = scenes.small(9, n=40, image=64, m=16, kind="noise")
+    lim = limits(s, 9)
+    r = renderer(s)
+    r.set_depth_buffer(lim, B.DEPTH_RAY_DISTANCE)
+    exact, te = r.render(s.camera())
+    r.set_form(B.FORM_PRECISION, B.BF16)
+    prec, tp = r.render(s.camera())
+    m = r.get_shadow_map((s.map_m + 1) ** 3)
+    o = Oracle(s, field=quantize(s.field_numpy(), "bf16"), precision=True)
+    o.set_ray_limits(np.where(np.isnan(lim), np.inf, lim))
+    oimg, olit = o.view_march(m.reshape((s.map_m + 1,) * 3))
+    check(prec, oimg)
+    assert tp["lit_samples"] == olit
+    r.set_form(B.FORM_EXACT)
+    r.mlp_train(B.mlp_options(samples_log2=14, n_lights=1, scene_light=1, epochs=1))
+    r.set_form(B.FORM_MLP, B.mlp_options(knot=4, probe_fraction=0.0))
+    learned, tl = r.render(s.camera())
+    assert np.array_equal(learned[..., 3], exact[..., 3])
+    assert tl["lit_samples"] == te["lit_samples"]

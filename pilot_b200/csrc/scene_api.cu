@@ -231,7 +231,10 @@ static beams_status load_vtk_scene(beams_renderer* r, const beams_scene_desc* d,
   v.range[0] = f.range[0];
   v.range[1] = f.range[1];
   s = beams_set_volume(r, &v);
-  if (s == BEAMS_OK) s = cudaStreamSynchronize(r->stream) == cudaSuccess ? BEAMS_OK : BEAMS_ERR_CUDA;
+  if (s == BEAMS_OK) {
+    const cudaError_t e = cudaStreamSynchronize(r->stream);  // the host copy is freed below
+    if (e != cudaSuccess) s = cuda_fail(r, e, "apply_scene: volume upload");
+  }
   if (s == BEAMS_OK && f.coords[0]) s = beams_set_volume_coordinates(r, f.coords[0], f.coords[1], f.coords[2]);
   for (int k = 0; k < 3; ++k) {
     org[k] = f.coords[k] ? (double)f.coords[k][0] : (double)(float)f.origin[k];

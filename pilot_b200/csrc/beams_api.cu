@@ -211,8 +211,56 @@ beams_status make_geo_vol(beams_renderer* r, const beams_volume& v, const beams_
     g.cy = (float)th;
     g.width = cam->width;
     g.height = cam->height;
+    g.win[0] = 0;
+    g.win[1] = 0;
+    g.win[2] = cam->width;
+    g.win[3] = cam->height;
   }
   return BEAMS_OK;
+}
+
+// The pixels whose rays can meet the box [bmin, bmax]: the bounding rectangle
+// of its corners projected through the pinhole camera (the projection of a box
+// in front of the camera is the convex hull of its corners'), widened by two
+// pixels, which is far more than the rounding of a ray's direction. A corner at
+// or behind the camera plane gives the whole image. Returns false when the
+// window is empty.
+static bool brick_window(const ExactGeo& g, int win[4]) {
+  win[0] = 0;
+  win[1] = 0;
+  win[2] = g.width;
+  win[3] = g.height;
+  double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+  for (int k = 0; k < 8; ++k) {
+    const double c[3] = {(k & 1) ? g.bmax[0] : g.bmin[0], (k & 2) ? g.bmax[1] : g.bmin[1],
+                         (k & 4) ? g.bmax[2] : g.bmin[2]};
+    double v[3], zf = 0, xr = 0, yu = 0;
+    for (int d = 0; d < 3; ++d) v[d] = c[d] - (double)g.cam_pos[d];
+    for (int d = 0; d < 3; ++d) {
+      zf += v[d] * g.cf[d];
+      xr += v[d] * g.cr[d];
+      yu += v[d] * g.cu[d];
+    }
+    if (!(zf > 1e-6 * (std::fabs(xr) + std::fabs(yu) + 1e-30))) return true;  // whole image
+    // pixel x of direction cf + sx cr + sy cu: (x + 0.5) kx - cx = sx
+    const double px = (xr / zf + g.cx) / g.kx - 0.5, py = (yu / zf + g.cy) / g.ky - 0.5;
+    xmin = std::min(xmin, px);
+    xmax = std::max(xmax, px);
+    ymin = std::min(ymin, py);
+    ymax = std::max(ymax, py);
+  }
+  const double x0 = std::max(0.0, std::floor(xmin) - 2.0), y0 = std::max(0.0, std::floor(ymin) - 2.0);
+  const double x1 = std::min((double)g.width, std::ceil(xmax) + 3.0);
+  const double y1 = std::min((double)g.height, std::ceil(ymax) + 3.0);
+  if (!(x1 > x0 && y1 > y0)) {
+    win[2] = win[3] = 0;
+    return false;
+  }
+  win[0] = (int)x0;
+  win[1] = (int)y0;
+  win[2] = (int)(x1 - x0);
+  win[3] = (int)(y1 - y0);
+  return true;
 }
 
 beams_status make_geo(beams_renderer* r, const beams_camera* cam, ExactGeo& g) {
@@ -500,11 +548,18 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
   for (int b = 1; b < nb; ++b) G[b].ray_max = G[0].ray_max;
   for (int b = 0; b < nb; ++b) {
     Brick& B = r->bricks[b];
+    float4* img = r->d_brick_imgs + (size_t)b * npix;
+    // only the pixels whose rays can reach this brick are marched; the rest stay transparent
+    const bool any = brick_window(G[b], G[b].win);
+    if (!any || (size_t)G[b].win[2] * G[b].win[3] < npix) {
+      e = cudaMemsetAsync(img, 0, npix * sizeof(float4), r->stream);
+      if (e != cudaSuccess) return cuda_fail(r, e, "clearing brick image");
+      if (!any) continue;
+    }
     e = cudaMemsetAsync(&r->d_cnt->tiles_view, 0, sizeof(unsigned), r->stream);
     if (e != cudaSuccess) return cuda_fail(r, e, "clearing tile counter");
     e = launch_view_march_f32(G[b], (const float*)B.d_field, B.d_quads, B.d_tab, r->d_tf,
-                              r->use_map ? B.d_map_final : nullptr, r->d_brick_imgs + (size_t)b * npix, r->d_cnt,
-                              r->stream);
+                              r->use_map ? B.d_map_final : nullptr, img, r->d_cnt, r->stream);
     if (e != cudaSuccess) return cuda_fail(r, e, "brick view march");
     ++launches;
   }

@@ -67,6 +67,10 @@ struct ExactGeo {
   // search instead of from the uniform spacing; org/h/invh then only describe
   // the average spacing. 0: coord(d, i) = org[d] + h[d] * float(i).
   int rect;
+  // Pixel window {x0, y0, w, h} the (non-listed) view march covers; the whole
+  // image unless a brick's projection is known to lie inside a smaller one
+  // (every pixel outside it misses the volume).
+  int win[4];
   // Canvas depth clipping: per-pixel limit on each camera ray's distance
   // (width * height floats, row y at y * width), the MaxDistance that
   // MapCanvasToRays hands the slab test (MapperLightedVolume.cxx:151-152).

@@ -140,9 +140,10 @@ __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const
   load_tables(s_tab, tab, g.ntab);
   for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) s_tf[i] = tf[i];
   __syncthreads();
-  const int tiles_x = (g.width + 7) >> 3;
+  // the pixel window (the whole image except for bricks, see ExactGeo::win)
+  const int tiles_x = (g.win[2] + 7) >> 3;
   // flist: only the listed kFallbackTile^2 tiles (32 warp tiles each) are marched
-  const int ntiles = LIST ? (int)(*fcount) * 32 : tiles_x * ((g.height + 3) >> 2);
+  const int ntiles = LIST ? (int)(*fcount) * 32 : tiles_x * ((g.win[3] + 3) >> 2);
   const int ftx = (g.width + kFallbackTile - 1) / kFallbackTile;
   unsigned lit = 0, hit = 0;
   for (int tile = next_warp_tile(&cnt->tiles_view); tile < ntiles; tile = next_warp_tile(&cnt->tiles_view)) {
@@ -153,6 +154,9 @@ __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const
       y = (f / ftx) * kFallbackTile + ((sub >> 2) << 2) + (lane >> 3);
     } else {
       tile_pixel(tiles_x, tile, x, y);
+      // outside the window's own extent: pushed past the image so the test below skips it
+      x = (x < g.win[2]) ? x + g.win[0] : g.width;
+      y = (y < g.win[3]) ? y + g.win[1] : g.height;
     }
     if (x < g.width && y < g.height) {
       float4 color;
@@ -552,7 +556,7 @@ template <typename QuadT, bool USE_MAP, typename MapT>
 static cudaError_t launch_k2(const ExactGeo& g, const QuadT* quads, const float4* tab, const float4* tf,
                              const MapT* map, float4* out, Counters* cnt, const unsigned char* occ, cudaStream_t st) {
   const size_t smem = ((size_t)g.ntab + (size_t)g.tf_n) * sizeof(float4);
-  const int ntiles = (((g.width + 7) >> 3) * ((g.height + 3) >> 2) + 7) / 8;  // 8 warp tiles per block
+  const int ntiles = (((g.win[2] + 7) >> 3) * ((g.win[3] + 3) >> 2) + 7) / 8;  // 8 warp tiles per block
   int grid = 0;
   cudaError_t e;
   if (occ) {

@@ -749,7 +749,7 @@ def run_batch(args):
     z.record(stream)
     torch.cuda.synchronize()
     small_seq_ms = a.elapsed_time(z) / max(1, args.steps // 4)
-    r.set_batch_options(**{k: tuning[k] for k in ("tile_w", "tile_h", "light_brick", "skip")})
+    r.set_batch_options(**{k: tuning[k] for k in ("tile_w", "tile_h", "light_brick", "skip", "split")})
     # end to end: images to pinned host memory
     host = [torch.empty((w, w, 4)).pin_memory() for w in sizes]
     r.render_batch(batch_requests(B, vols, rng, nreq, host), timings=False)

@@ -286,6 +286,9 @@ typedef struct beams_batch_options {
   int light_brick;          /* map-build vertex order: 0 rows, 8/16/32/64 bricks */
   int use_graph;            /* 1: capture once, replay (default) */
   int no_skip;              /* 1: no empty-space skipping (default 0: both marches skip empty macro-cells) */
+  int split;                /* 1: two launches, every request's map build and then every view march, each
+                               kernel at its own occupancy; 0: one launch whose view tiles wait for their map
+                               (default) */
   int reserved;             /* 0; 0x7e57 makes the map items withhold their completion (tests of the bounded
                                wait: the call then returns BEAMS_ERR_TIMEOUT after about 2 s) */
 } beams_batch_options;
@@ -294,7 +297,7 @@ beams_status beams_set_batch_options(beams_renderer* r, const beams_batch_option
  * persistent kernel and its staging copies, lit_samples and rays_hit summed. */
 beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, int n, beams_timings* t);
 /* Tunes the batch options on these requests by coordinate descent over the
- * empty-space skip, the vertex order {rows, 8, 16, 32, 64 bricks} and the view
+ * empty-space skip, one or two launches, the vertex order {rows, 8, 16, 32, 64 bricks} and the view
  * tile {8x8, 16x16, 32x8, 8x32, 32x32, 64x32, 64x64}; keeps the fastest (images are identical
  * under all of them) and reports it. */
 beams_status beams_batch_autotune(beams_renderer* r, const beams_request* reqs, int n, beams_batch_options* best,

@@ -81,7 +81,7 @@ class Request(C.Structure):
 
 class BatchOptions(C.Structure):
     _fields_ = [("tile_w", C.c_int), ("tile_h", C.c_int), ("light_brick", C.c_int), ("use_graph", C.c_int),
-                ("no_skip", C.c_int), ("reserved", C.c_int)]
+                ("no_skip", C.c_int), ("split", C.c_int), ("reserved", C.c_int)]
 
 
 class ConfigLight(C.Structure):
@@ -354,9 +354,11 @@ class Renderer:
                              (C.c_double * 2)(*vrange), ASSOC_POINTS, on_dev)
         self._check(self._L.beams_batch_set_volumes(self._h, vols, len(volumes)))
 
-    def set_batch_options(self, tile_w=32, tile_h=32, light_brick=8, use_graph=True, skip=True, _withhold=False):
+    def set_batch_options(self, tile_w=32, tile_h=32, light_brick=8, use_graph=True, skip=True, split=False,
+                          _withhold=False):
+        """split: every map build, then every view march, as two launches (no waits between them)."""
         o = BatchOptions(int(tile_w), int(tile_h), int(light_brick), int(bool(use_graph)), int(not skip),
-                         0x7E57 if _withhold else 0)
+                         int(bool(split)), 0x7E57 if _withhold else 0)
         self._check(self._L.beams_set_batch_options(self._h, C.byref(o)))
 
     @staticmethod
@@ -375,7 +377,7 @@ class Renderer:
         o, ms = BatchOptions(), C.c_float()
         self._check(self._L.beams_batch_autotune(self._h, arr, len(reqs), C.byref(o), C.byref(ms)))
         return {"tile_w": o.tile_w, "tile_h": o.tile_h, "light_brick": o.light_brick, "skip": not o.no_skip,
-                "batch_ms": ms.value}
+                "split": bool(o.split), "batch_ms": ms.value}
 
     def batch_tuning_save(self, path):
         self._check(self._L.beams_batch_tuning_save(self._h, str(path).encode()))

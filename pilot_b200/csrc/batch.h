@@ -30,10 +30,14 @@ struct BatchDesc {
 // reads the same volume. Segment k covers items
 // [seg_off[k], seg_off[k+1]) of request seg_req[k] & 0xffff, phase 2 (view)
 // when bit 16 is set. Lives in device memory (uploaded when the batch's shapes change).
+// Split plans (two launches) order all map items first, o0..o_{n-1}, then all
+// view items in the same order; k1_total counts the map items.
 struct BatchPlan {
   int n;
   int nseg;
   int total;
+  int k1_total;           // split plans: map items [0, k1_total), view items [k1_total, total)
+  int split;              // 1: two launches (map items, then view items)
   int tile_w, tile_h;     // view tile: a multiple of 8 x 4 warp tiles
   int brick_log2;         // map-build vertex order inside a request (0 = rows)
   int skip;               // 1: both marches skip empty macro-cells (every desc has occ)
@@ -48,11 +52,15 @@ struct BatchQueue {
   unsigned next;
   unsigned error;         // 1: a view item gave up waiting for its map (bounded wait)
   unsigned done1[kMaxRequests];
+  unsigned next_view;     // split plans: the view launch's counter
 };
 
-// Dynamic shared memory and persistent grid of the batch kernel (call outside graph capture).
-cudaError_t batch_launch_config(int tf_n, size_t max_ntab, int total_items, size_t& smem, int& grid);
-cudaError_t launch_batch(const ExactGeo* geos, const BatchDesc* descs, const BatchPlan* plan, int skip,
-                         const float4* tf, size_t smem, int grid, BatchQueue* q, Counters* cnt, cudaStream_t st);
+// Dynamic shared memory and persistent grid(s) of the batch kernel(s) (call
+// outside graph capture): grid[0] for the fused or map launch, grid[1] for the
+// split plan's view launch.
+cudaError_t batch_launch_config(int tf_n, size_t max_ntab, const BatchPlan& plan, size_t& smem, int grid[2]);
+cudaError_t launch_batch(const ExactGeo* geos, const BatchDesc* descs, const BatchPlan* plan, int skip, int split,
+                         const float4* tf, size_t smem, const int grid[2], BatchQueue* q, Counters* cnt,
+                         cudaStream_t st);
 
 }  // namespace beams

@@ -43,7 +43,7 @@ struct BatchTuned {
 
 struct BatchState {
   std::vector<BatchVolume*> vols;
-  beams_batch_options opts{32, 32, 8, 1, 0, 0};
+  beams_batch_options opts{32, 32, 8, 1, 0, 0, 0};
   // autotuner results per batch shape (tuning_key), kept for later calls and files
   std::map<std::string, BatchTuned> tuned;
   // per-signature device state
@@ -54,7 +54,7 @@ struct BatchState {
   BatchPlan plan{};
   size_t max_ntab = 0;
   size_t smem = 0;
-  int grid = 0;
+  int grid[2] = {0, 0};
   ExactGeo* h_geos = nullptr;  // pinned staging, copied by the graph's first node
   BatchDesc* h_descs = nullptr;
   ExactGeo* d_geos = nullptr;
@@ -175,6 +175,7 @@ beams_status beams_set_batch_options(beams_renderer* r, const beams_batch_option
     return fail(r, BEAMS_ERR_INVALID_ARG, "batch options: tile_w a multiple of 8, tile_h of 4, at most 16384 pixels");
   if (log2_brick(o->light_brick) < 0)
     return fail(r, BEAMS_ERR_INVALID_ARG, "batch options: light_brick must be 0, 8, 16, 32 or 64");
+  if (o->split != 0 && o->split != 1) return fail(r, BEAMS_ERR_INVALID_ARG, "batch options: split must be 0 or 1");
   BatchState* b = batch_state(r);
   b->opts = *o;
   b->drop_graph();
@@ -202,6 +203,7 @@ beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, in
   sig.push_back(b->opts.tile_w);
   sig.push_back(b->opts.tile_h);
   sig.push_back(bl);
+  sig.push_back(b->opts.split);
   beams_status s = BEAMS_OK;
   for (int i = 0; i < n && s == BEAMS_OK; ++i) {
     const beams_request& q = reqs[i];
@@ -278,7 +280,8 @@ beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, in
     P.tile_h = b->opts.tile_h;
     P.brick_log2 = bl;
     P.skip = skip;
-    P.test_withhold = b->opts.reserved == 0x7e57 ? 1 : 0;
+    P.split = b->opts.split;
+    P.test_withhold = (b->opts.reserved == 0x7e57 && !P.split) ? 1 : 0;
     b->max_ntab = 0;
     std::vector<int> k2(n);
     for (int i = 0; i < n; ++i) {
@@ -299,7 +302,7 @@ beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, in
     // of o[k] and the view march of o[k-1] that runs beside it read the same
     // field through L2; groups with the most work first, so the small requests
     // fill the tail of the launch. Then K1(o0), K1(o_k) and K2(o_{k-1}) for
-    // k = 1..n-1, K2(o_{n-1}).
+    // k = 1..n-1, K2(o_{n-1}); split plans K1(o0..o_{n-1}), K2(o0..o_{n-1}).
     std::vector<int> o(n);
     std::vector<double> vwork(b->vols.size(), 0.0);
     for (int i = 0; i < n; ++i) {
@@ -318,16 +321,22 @@ beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, in
       ++P.nseg;
       items += count;
     };
-    for (int k = 0; k < n; ++k) {
-      seg(o[k], 1, P.k1_items[o[k]]);
-      if (k > 0) seg(o[k - 1], 2, k2[o[k - 1]]);
+    if (P.split) {
+      for (int k = 0; k < n; ++k) seg(o[k], 1, P.k1_items[o[k]]);
+      P.k1_total = items;
+      for (int k = 0; k < n; ++k) seg(o[k], 2, k2[o[k]]);
+    } else {
+      for (int k = 0; k < n; ++k) {
+        seg(o[k], 1, P.k1_items[o[k]]);
+        if (k > 0) seg(o[k - 1], 2, k2[o[k - 1]]);
+      }
+      seg(o[n - 1], 2, k2[o[n - 1]]);
     }
-    seg(o[n - 1], 2, k2[o[n - 1]]);
     P.seg_off[P.nseg] = items;
     P.total = items;
     s = ensure_buffer(r, &b->arena, &b->arena_cap, std::max(off, (size_t)256), "allocating batch arena");
     if (s != BEAMS_OK) return s;
-    e = batch_launch_config(r->tf_n, b->max_ntab, P.total, b->smem, b->grid);
+    e = batch_launch_config(r->tf_n, b->max_ntab, P, b->smem, b->grid);
     if (e != cudaSuccess) return cuda_fail(r, e, "render_batch: launch configuration");
     if (!b->h_geos) {
       e = cudaMallocHost((void**)&b->h_geos, kMaxRequests * sizeof(ExactGeo));
@@ -362,8 +371,8 @@ beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, in
     if (x == cudaSuccess) x = cudaMemsetAsync(b->d_q, 0, sizeof(BatchQueue), sq);
     if (x == cudaSuccess) x = cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), sq);
     if (x == cudaSuccess)
-      x = launch_batch(b->d_geos, b->d_descs, b->d_plan, b->plan.skip, r->d_tf, b->smem, b->grid, b->d_q, r->d_cnt,
-                       sq);
+      x = launch_batch(b->d_geos, b->d_descs, b->d_plan, b->plan.skip, b->plan.split, r->d_tf, b->smem, b->grid,
+                       b->d_q, r->d_cnt, sq);
     return x;
   };
   cudaEventRecord(r->ev[0], r->stream);
@@ -419,7 +428,7 @@ beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, in
       long long nv = 0;
       for (int i = 0; i < n; ++i) nv += (long long)geos[i].pd[0] * geos[i].pd[1] * geos[i].pd[2];
       t->map_vertices = (int)std::min<long long>(nv, 2147483647ll);
-      t->kernel_launches = 1;
+      t->kernel_launches = b->plan.split ? 2 : 1;
     }
   }
   return BEAMS_OK;
@@ -480,17 +489,21 @@ beams_status beams_batch_autotune(beams_renderer* r, const beams_request* reqs, 
     ms_out = tmin;
     return st;
   };
-  // coordinate descent: skip, then the vertex order, then the view tile
+  // coordinate descent: skip, one or two launches, the vertex order, the view tile
   beams_batch_options bo = keep;
+  bo.reserved = 0;
   float bt = 3.4e38f;
   s = time_opts(bo, bt);
-  for (int stage = 0; stage < 3 && s == BEAMS_OK; ++stage) {
+  for (int stage = 0; stage < 4 && s == BEAMS_OK; ++stage) {
     std::vector<beams_batch_options> cand;
     beams_batch_options o = bo;
     if (stage == 0) {
       o.no_skip = !bo.no_skip;
       cand.push_back(o);
     } else if (stage == 1) {
+      o.split = !bo.split;
+      cand.push_back(o);
+    } else if (stage == 2) {
       for (int br : {0, 8, 16, 32, 64})
         if (br != bo.light_brick) {
           o.light_brick = br;
@@ -535,16 +548,18 @@ beams_status beams_batch_tuning_clear(beams_renderer* r) {
 }
 
 // Text file: a header line, then one line per batch shape:
-// <key> <tile_w> <tile_h> <light_brick> <no_skip> <ms>
+// <key> <tile_w> <tile_h> <light_brick> <no_skip> <split> <ms>
+// (files of format 1, written before the split option, lack <split>: read as 0)
 beams_status beams_batch_tuning_save(beams_renderer* r, const char* path) {
   if (!r || !path) return fail(r, BEAMS_ERR_INVALID_ARG, "batch_tuning_save: NULL argument");
   std::ofstream f(path);
   if (!f) return fail(r, BEAMS_ERR_INVALID_ARG, std::string("batch_tuning_save: cannot write ") + path);
-  f << "beams-batch-tuning 1\n";
+  f << "beams-batch-tuning 2\n";
   if (r->batch)
     for (const auto& e : r->batch->tuned)
       f << e.first << ' ' << e.second.opts.tile_w << ' ' << e.second.opts.tile_h << ' '
-        << e.second.opts.light_brick << ' ' << e.second.opts.no_skip << ' ' << e.second.ms << '\n';
+        << e.second.opts.light_brick << ' ' << e.second.opts.no_skip << ' ' << e.second.opts.split << ' '
+        << e.second.ms << '\n';
   if (!f) return fail(r, BEAMS_ERR_INVALID_ARG, std::string("batch_tuning_save: write failed: ") + path);
   return BEAMS_OK;
 }
@@ -555,8 +570,9 @@ beams_status beams_batch_tuning_load(beams_renderer* r, const char* path) {
   std::ifstream f(path);
   if (!f) return fail(r, BEAMS_ERR_INVALID_ARG, std::string("batch_tuning_load: cannot read ") + path);
   std::string line;
-  if (!std::getline(f, line) || line != "beams-batch-tuning 1")
+  if (!std::getline(f, line) || (line != "beams-batch-tuning 1" && line != "beams-batch-tuning 2"))
     return fail(r, BEAMS_ERR_CONFIG, "batch_tuning_load: not a batch tuning file");
+  const bool v1 = line == "beams-batch-tuning 1";
   std::map<std::string, BatchTuned> got;
   int ln = 1;
   while (std::getline(f, line)) {
@@ -566,10 +582,12 @@ beams_status beams_batch_tuning_load(beams_renderer* r, const char* path) {
     std::string key;
     BatchTuned t{};
     t.opts = r->batch->opts;
-    if (!(is >> key >> t.opts.tile_w >> t.opts.tile_h >> t.opts.light_brick >> t.opts.no_skip >> t.ms) ||
+    t.opts.split = 0;
+    if (!(is >> key >> t.opts.tile_w >> t.opts.tile_h >> t.opts.light_brick >> t.opts.no_skip) ||
+        (!v1 && !(is >> t.opts.split)) || !(is >> t.ms) ||
         t.opts.tile_w < 8 || t.opts.tile_w % 8 || t.opts.tile_h < 4 || t.opts.tile_h % 4 ||
         t.opts.tile_w * t.opts.tile_h > 16384 || log2_brick(t.opts.light_brick) < 0 ||
-        (t.opts.no_skip != 0 && t.opts.no_skip != 1))
+        (t.opts.no_skip != 0 && t.opts.no_skip != 1) || (t.opts.split != 0 && t.opts.split != 1))
       return fail(r, BEAMS_ERR_CONFIG, "batch_tuning_load: bad entry on line " + std::to_string(ln));
     t.opts.reserved = 0;
     got[key] = t;

@@ -12,6 +12,13 @@
 // guarantees progress: every item a view item waits on was dequeued earlier by
 // a running block that waits on nothing.
 //
+// The split variant runs the same items as two persistent launches, all map
+// items and then all view items (MODE 1 and 2; stream order replaces the
+// waits). The fused kernel holds the registers of both marches (80, three
+// blocks per SM); each split kernel holds only its own march's and runs four
+// blocks per SM, which pays when the requests are large enough to fill the GPU
+// on their own.
+//
 // Per item a block keeps the request's geometry and cell tables in shared
 // memory (recomputed there when the request changes, so no table buffers or
 // table launches exist). Results equal the single-request kernels': the light
@@ -46,8 +53,9 @@ __device__ __forceinline__ int find_request(const int* off, int n, int item) {
   return lo;
 }
 
-template <bool SKIP>
-__global__ void __launch_bounds__(kBatchThreads, 3) k_batch(const ExactGeo* __restrict__ geos,
+// MODE 0: map and view items in one launch; 1: map items only; 2: view items only.
+template <bool SKIP, int MODE>
+__global__ void __launch_bounds__(kBatchThreads, MODE == 0 ? 3 : 4) k_batch(const ExactGeo* __restrict__ geos,
                                                             const BatchDesc* __restrict__ descs,
                                                             const BatchPlan* __restrict__ pl,
                                                             const float4* __restrict__ tf,
@@ -76,14 +84,14 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch(const ExactGeo* __re
   unsigned lit = 0, hit = 0;
   for (;;) {
     if (tid == 0) {
-      s_item = (int)atomicAdd(&q->next, 1u);
+      s_item = MODE == 2 ? plan.k1_total + (int)atomicAdd(&q->next_view, 1u) : (int)atomicAdd(&q->next, 1u);
       s_sub = 0u;
     }
     __syncthreads();
     const int item = s_item;
-    if (item >= plan.total) break;
+    if (item >= (MODE == 1 ? plan.k1_total : plan.total)) break;
     const int seg = find_request(plan.seg_off, plan.nseg, item);
-    const int phase = (plan.seg_req[seg] >> 16) ? 2 : 1;
+    const int phase = MODE == 1 ? 1 : MODE == 2 ? 2 : ((plan.seg_req[seg] >> 16) ? 2 : 1);
     const int req = plan.seg_req[seg] & 0xffff;
     const int li = item - plan.seg_off[seg];  // item index inside the request's phase
     if (req != s_req || phase != s_phase) {
@@ -138,11 +146,15 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch(const ExactGeo* __re
           acc.store(sd.map, id);
         }
       }
-      __threadfence();
-      __syncthreads();
-      if (tid == 0 && !plan.test_withhold) atomicAdd(&q->done1[req], 1u);
+      if (MODE == 0) {
+        __threadfence();
+        __syncthreads();
+        if (tid == 0 && !plan.test_withhold) atomicAdd(&q->done1[req], 1u);
+      } else {
+        __syncthreads();  // every warp is done with this chunk before s_sub is reset
+      }
     } else {
-      if (tid == 0) {
+      if (MODE == 0 && tid == 0) {
         const unsigned need = (unsigned)plan.k1_items[req];
         const long long t0 = clock64();
         int skip = 0;
@@ -159,7 +171,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch(const ExactGeo* __re
         s_skip = skip;
       }
       __syncthreads();
-      if (s_skip) continue;  // the host reports the timeout; this item's pixels stay unwritten
+      if (MODE == 0 && s_skip) continue;  // the host reports the timeout; this item's pixels stay unwritten
       // a tile_w x tile_h tile; warps take 8x4 sub-tiles from the block's counter
       const int tx0 = (li % sd.tiles_x) * plan.tile_w, ty0 = (li / sd.tiles_x) * plan.tile_h;
       const int sx = plan.tile_w >> 3, nsub = sx * (plan.tile_h >> 2);
@@ -185,14 +197,15 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch(const ExactGeo* __re
 
 }  // namespace
 
-cudaError_t batch_launch_config(int tf_n, size_t max_ntab, int total_items, size_t& smem, int& grid) {
-  smem = (size_t)tf_n * sizeof(float4) + (size_t)((tf_n + 3) & ~3) * sizeof(float) + max_ntab * sizeof(float4);
-  cudaError_t e = cudaFuncSetAttribute(k_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+template <int MODE>
+cudaError_t mode_grid(size_t smem, int items, int& grid) {
+  cudaError_t e = cudaFuncSetAttribute(k_batch<false, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_batch<true, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0, per_sm2 = 0, dev = 0, sms = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<false>, kBatchThreads, smem);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_batch<true>, kBatchThreads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<false, MODE>, kBatchThreads, smem);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_batch<true, MODE>, kBatchThreads, smem);
   if (e != cudaSuccess) return e;
   per_sm = per_sm < per_sm2 ? per_sm : per_sm2;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
@@ -200,17 +213,40 @@ cudaError_t batch_launch_config(int tf_n, size_t max_ntab, int total_items, size
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
   grid = sms * per_sm;
-  if (grid > total_items) grid = total_items;
+  if (grid > items) grid = items;
   if (grid < 1) grid = 1;
   return cudaSuccess;
 }
 
-cudaError_t launch_batch(const ExactGeo* geos, const BatchDesc* descs, const BatchPlan* plan, int skip,
-                         const float4* tf, size_t smem, int grid, BatchQueue* q, Counters* cnt, cudaStream_t st) {
+cudaError_t batch_launch_config(int tf_n, size_t max_ntab, const BatchPlan& plan, size_t& smem, int grid[2]) {
+  smem = (size_t)tf_n * sizeof(float4) + (size_t)((tf_n + 3) & ~3) * sizeof(float) + max_ntab * sizeof(float4);
+  grid[1] = 0;
+  if (!plan.split) return mode_grid<0>(smem, plan.total, grid[0]);
+  cudaError_t e = mode_grid<1>(smem, plan.k1_total, grid[0]);
+  if (e == cudaSuccess) e = mode_grid<2>(smem, plan.total - plan.k1_total, grid[1]);
+  return e;
+}
+
+template <int MODE>
+void launch_mode(const ExactGeo* geos, const BatchDesc* descs, const BatchPlan* plan, int skip, const float4* tf,
+                 size_t smem, int grid, BatchQueue* q, Counters* cnt, cudaStream_t st) {
   if (skip)
-    k_batch<true><<<grid, kBatchThreads, smem, st>>>(geos, descs, plan, tf, q, cnt);
+    k_batch<true, MODE><<<grid, kBatchThreads, smem, st>>>(geos, descs, plan, tf, q, cnt);
   else
-    k_batch<false><<<grid, kBatchThreads, smem, st>>>(geos, descs, plan, tf, q, cnt);
+    k_batch<false, MODE><<<grid, kBatchThreads, smem, st>>>(geos, descs, plan, tf, q, cnt);
+}
+
+cudaError_t launch_batch(const ExactGeo* geos, const BatchDesc* descs, const BatchPlan* plan, int skip, int split,
+                         const float4* tf, size_t smem, const int grid[2], BatchQueue* q, Counters* cnt,
+                         cudaStream_t st) {
+  if (!split) {
+    launch_mode<0>(geos, descs, plan, skip, tf, smem, grid[0], q, cnt, st);
+    return cudaGetLastError();
+  }
+  launch_mode<1>(geos, descs, plan, skip, tf, smem, grid[0], q, cnt, st);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  launch_mode<2>(geos, descs, plan, skip, tf, smem, grid[1], q, cnt, st);
   return cudaGetLastError();
 }
 

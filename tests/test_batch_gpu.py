@@ -1,6 +1,7 @@
 """Batched form: many requests (own volume, camera, light, map size) in one
-persistent launch replayed from a CUDA graph; every image equals the
-single-request exact render bit for bit."""
+persistent launch replayed from a CUDA graph (or, split, one launch of map
+builds and one of view marches); every image equals the single-request exact
+render bit for bit."""
 import numpy as np
 import pytest
 import torch
@@ -67,7 +68,9 @@ def _as_np(o):
                                   dict(tile_w=32, tile_h=8, light_brick=0, use_graph=True, skip=False),
                                   dict(tile_w=8, tile_h=32, light_brick=16, use_graph=False),
                                   dict(tile_w=32, tile_h=32, light_brick=64, use_graph=True, skip=False),
-                                  dict(tile_w=64, tile_h=64, light_brick=32, use_graph=True)])
+                                  dict(tile_w=64, tile_h=64, light_brick=32, use_graph=True),
+                                  dict(tile_w=32, tile_h=32, light_brick=8, use_graph=True, split=True),
+                                  dict(tile_w=16, tile_h=8, light_brick=0, use_graph=False, skip=False, split=True)])
 def test_batch_equals_single_renders(cuda_device, opts):
     vols = _volumes()
     tf = scenes.tf_table()
@@ -84,7 +87,7 @@ def test_batch_equals_single_renders(cuda_device, opts):
                 ref, ts = _single(vols[spec["volume"]], tf, spec)
                 assert np.array_equal(_as_np(o), ref), (call, spec["volume"], opts)
                 lit += ts["lit_samples"]
-            assert t["lit_samples"] == lit and t["kernel_launches"] == 1
+            assert t["lit_samples"] == lit and t["kernel_launches"] == (2 if opts.get("split") else 1)
 
 
 def test_batch_rejects_bad_requests(cuda_device):
@@ -153,9 +156,20 @@ def test_batch_tuning_cache_and_file(cuda_device, tmp_path):
         t0 = time.perf_counter()
         loaded = q.batch_autotune(reqs2)
         assert time.perf_counter() - t0 < t_tune / 5
-        assert {k: loaded[k] for k in ("tile_w", "tile_h", "light_brick", "skip")} == \
-               {k: first[k] for k in ("tile_w", "tile_h", "light_brick", "skip")}
+        keys = ("tile_w", "tile_h", "light_brick", "skip", "split")
+        assert {k: loaded[k] for k in keys} == {k: first[k] for k in keys}
         bad = tmp_path / "bad.txt"
-        bad.write_text("beams-batch-tuning 1\nkey 7 4 8 0 1.0\n")
+        bad.write_text("beams-batch-tuning 2\nkey 7 4 8 0 0 1.0\n")
         with pytest.raises(B.BeamsError):
             q.batch_tuning_load(bad)
+        bad.write_text("beams-batch-tuning 2\nkey 8 4 8 0 2 1.0\n")
+        with pytest.raises(B.BeamsError):
+            q.batch_tuning_load(bad)
+        # a format-1 file (no split column) still loads, as one launch
+        old = tmp_path / "v1.txt"
+        key = path.read_text().splitlines()[1].split()[0]
+        old.write_text(f"beams-batch-tuning 1\n{key} 16 8 0 1 2.5\n")
+        q.batch_tuning_clear()
+        q.batch_tuning_load(old)
+        got = q.batch_autotune(reqs2)
+        assert (got["tile_w"], got["tile_h"], got["light_brick"], got["skip"], got["split"]) == (16, 8, 0, False, False)

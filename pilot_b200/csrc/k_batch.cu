@@ -122,12 +122,14 @@ __global__ void __launch_bounds__(kBatchThreads, MODE == 0 ? 3 : 4) k_batch(cons
         int id = -1, x = 0, y = 0, z = 0;
         if (bl) {
           const int bi = slot >> (3 * bl), li = slot & ((1 << (3 * bl)) - 1), m = (1 << bl) - 1;
+          // slots past the last brick (the request's last item is padded to a whole item) do nothing
+          const int nb = ((const volatile int*)s_bo)[0] * ((const volatile int*)s_bo)[1] * ((const volatile int*)s_bo)[2];
           int bx, by, bz;
           pencil_brick(bi, s_bo, bx, by, bz);
           x = (bx << bl) + (li & m);
           y = (by << bl) + ((li >> bl) & m);
           z = (bz << bl) + (li >> (2 * bl));
-          if (x < sg.pd[0] && y < sg.pd[1] && z < sg.pd[2]) id = (z * sg.pd[1] + y) * sg.pd[0] + x;
+          if (bi < nb && x < sg.pd[0] && y < sg.pd[1] && z < sg.pd[2]) id = (z * sg.pd[1] + y) * sg.pd[0] + x;
         } else if (slot < sd.nvert) {
           id = slot;
           x = id % sg.pd[0];

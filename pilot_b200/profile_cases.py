@@ -32,6 +32,7 @@ def main(argv=None) -> int:
                     choices=["light_march", "view_march", "mlp_view", "mlp_frame", "mlp_tc", "batch",
                              "precision_light", "precision_view", "bricks"])
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--split", action="store_true", help="batch: map-build launch, then view launch")
     a = ap.parse_args(argv)
     torch.cuda.set_device(0)
     if a.case in ("light_march", "view_march", "mlp_view", "mlp_frame"):
@@ -124,7 +125,7 @@ def main(argv=None) -> int:
         r = B.Renderer(0)
         r.set_color_map(scenes.tf_table())
         r.batch_set_volumes([(f, sc.origin, sc.spacing, sc.value_range) for sc, f in vols])
-        r.set_batch_options(tile_w=32, tile_h=32, light_brick=8, skip=True)
+        r.set_batch_options(tile_w=32, tile_h=32, light_brick=8, skip=True, split=a.split)
         reqs = bench.batch_requests(B, vols, rng, n, outs)
         for _ in range(a.reps):
             r.render_batch(reqs, timings=False)

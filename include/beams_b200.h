@@ -262,7 +262,8 @@ beams_status beams_get_brick_map(beams_renderer* r, int brick, int stage, float*
  * (MapperLightedVolume.cxx:114-193). Here volumes stay resident and a batch of
  * requests, each with its own volume, camera, light, map size and sample
  * distance, runs as ONE persistent kernel launch (map builds first, view tiles
- * after, a view tile waiting with a bounded wait for its request's map),
+ * after, a view tile waiting with a bounded wait for its request's map), or
+ * split into a map-build launch and a view launch (beams_batch_options.split),
  * captured once into a CUDA graph and replayed while the batch's shapes stay
  * the same. The colour map is the renderer's. Results equal beams_render's
  * exact form for the same settings. */
@@ -290,11 +291,13 @@ typedef struct beams_batch_options {
                                kernel at its own occupancy; 0: one launch whose view tiles wait for their map
                                (default) */
   int reserved;             /* 0; 0x7e57 makes the map items withhold their completion (tests of the bounded
-                               wait: the call then returns BEAMS_ERR_TIMEOUT after about 2 s) */
+                               wait of the one-launch plan: the call then returns BEAMS_ERR_TIMEOUT after
+                               about 2 s) */
 } beams_batch_options;
 beams_status beams_set_batch_options(beams_renderer* r, const beams_batch_options* o);
 /* Timings: total_ms = the batch (launch to last image copied), view_march_ms = the
- * persistent kernel and its staging copies, lit_samples and rays_hit summed. */
+ * persistent kernel(s) and their staging copies, lit_samples and rays_hit summed,
+ * kernel_launches 1 or 2 (split). */
 beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, int n, beams_timings* t);
 /* Tunes the batch options on these requests by coordinate descent over the
  * empty-space skip, one or two launches, the vertex order {rows, 8, 16, 32, 64 bricks} and the view

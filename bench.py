@@ -695,6 +695,20 @@ def run_batch(args):
         z.record(stream)
         torch.cuda.synchronize()
     total_ms = a.elapsed_time(z)
+    # the other launch plan (one fused launch, or split) with the same options, for comparison
+    tuned_opts = {k: tuning[k] for k in ("tile_w", "tile_h", "light_brick", "skip", "split")}
+    r.set_batch_options(**dict(tuned_opts, split=not tuning["split"]))
+    other_reqs = batch_requests(B, vols, rng, nreq, outs)
+    for _ in range(3):
+        r.render_batch(other_reqs, timings=False)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(args.steps):
+        r.render_batch(other_reqs, timings=False)
+    z.record(stream)
+    torch.cuda.synchronize()
+    other_plan = {"split": not tuning["split"], "ms_per_batch": a.elapsed_time(z) / args.steps}
+    r.set_batch_options(**tuned_opts)
     # the same requests one render at a time through the single-request API
     singles = []
     for sc, f in vols:
@@ -753,7 +767,7 @@ def run_batch(args):
     z.record(stream)
     torch.cuda.synchronize()
     small_seq_ms = a.elapsed_time(z) / max(1, args.steps // 4)
-    r.set_batch_options(**{k: tuning[k] for k in ("tile_w", "tile_h", "light_brick", "skip", "split")})
+    r.set_batch_options(**tuned_opts)
     # end to end: images to pinned host memory
     host = [torch.empty((w, w, 4)).pin_memory() for w in sizes]
     r.render_batch(batch_requests(B, vols, rng, nreq, host), timings=False)
@@ -777,6 +791,7 @@ def run_batch(args):
                        "l2": "volumes and maps total well above L2; no flush"},
             "requests_per_s": nreq * args.steps / (total_ms / 1e3),
             "sequential_ms_per_batch": seq_ms, "speedup_vs_sequential": seq_ms / (total_ms / args.steps),
+            "other_launch_plan": other_plan,
             "small_requests": {"workload": f"{nreq} requests over the 64^3 and 128^3 volumes, 256^2 images",
                                "batch_ms": small_ms, "sequential_ms": small_seq_ms,
                                "speedup_vs_sequential": small_seq_ms / small_ms, "tuning": small_tuning},

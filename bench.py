@@ -841,6 +841,7 @@ def run_bricks(args):
     r.set_bricks(bricks)
     s.configure(r)
     r.set_shadow_map_size(s.map_m // 2)  # each brick's map keeps the whole field's vertex spacing
+    r.render(cam, out=out, timings=False)  # first frame: brick quads, tables and buffers
     _, tb = r.render(cam, out=out, timings=True)
     img = out.cpu().numpy()
     frame = lambda: r.render(cam, out=out, timings=False)  # noqa: E731

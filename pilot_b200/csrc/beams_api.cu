@@ -489,8 +489,44 @@ beams_status check_ready(beams_renderer* r) {
   return BEAMS_OK;
 }
 
+// Side streams, events and per-brick counters of the per-brick launches (created on first use).
+static beams_status brick_lanes_ready(beams_renderer* r) {
+  cudaError_t e = cudaSuccess;
+  if (!r->brick_fork) e = cudaEventCreateWithFlags(&r->brick_fork, cudaEventDisableTiming);
+  for (int l = 0; l < beams_renderer::kBrickLanes && e == cudaSuccess; ++l) {
+    if (!r->brick_lane[l]) e = cudaStreamCreateWithFlags(&r->brick_lane[l], cudaStreamNonBlocking);
+    if (e == cudaSuccess && !r->brick_join[l]) e = cudaEventCreateWithFlags(&r->brick_join[l], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess && !r->d_brick_cnt) e = cudaMalloc((void**)&r->d_brick_cnt, kMaxBricks * sizeof(Counters));
+  if (e != cudaSuccess) return cuda_fail(r, e, "creating brick streams");
+  return BEAMS_OK;
+}
+
+// The fork of work onto the lanes: every lane waits for what r->stream has queued so far.
+static beams_status brick_lanes_fork(beams_renderer* r) {
+  cudaError_t e = cudaEventRecord(r->brick_fork, r->stream);
+  for (int l = 0; l < beams_renderer::kBrickLanes && e == cudaSuccess; ++l)
+    e = cudaStreamWaitEvent(r->brick_lane[l], r->brick_fork, 0);
+  if (e != cudaSuccess) return cuda_fail(r, e, "forking brick streams");
+  return BEAMS_OK;
+}
+
+// r->stream waits for everything queued on the lanes (called on error paths too).
+static cudaError_t brick_lanes_join(beams_renderer* r) {
+  cudaError_t first = cudaSuccess;
+  for (int l = 0; l < beams_renderer::kBrickLanes; ++l) {
+    cudaError_t e = cudaEventRecord(r->brick_join[l], r->brick_lane[l]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(r->stream, r->brick_join[l], 0);
+    if (e != cudaSuccess && first == cudaSuccess) first = e;
+  }
+  return first;
+}
+
 // One frame of a multi-block scene: Phase 1 local maps, Phases 2-3 stitched
 // maps, Phase 4 per-brick view marches, Phase 5 depth-ordered composite.
+// Within a phase the bricks' launches are independent and run on the lanes;
+// the phases are joined on r->stream (Phase 3 reads every Phase-1 map, Phase 5
+// every brick image).
 beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* out, int& launches) {
   const int nb = (int)r->bricks.size();
   std::vector<ExactGeo> G(nb);
@@ -507,6 +543,15 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
                                  "allocating brick images");
   if (s != BEAMS_OK) return s;
   cudaError_t e;
+  s = brick_lanes_ready(r);
+  if (s != BEAMS_OK) return s;
+  e = cudaMemsetAsync(r->d_brick_cnt, 0, nb * sizeof(Counters), r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "clearing brick counters");
+  auto lane = [&](int b) { return r->brick_lane[b % beams_renderer::kBrickLanes]; };
+  auto lane_fail = [&](cudaError_t err, const char* what) {
+    brick_lanes_join(r);
+    return cuda_fail(r, err, what);
+  };
   if (r->use_map) {
     std::vector<BrickRef> refs(nb);
     for (int b = 0; b < nb; ++b) {
@@ -516,9 +561,6 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
       if (s == BEAMS_OK) s = ensure_buffer(r, (void**)&B.d_map_final, &B.final_cap, nv * sizeof(float), "allocating brick map");
       if (s != BEAMS_OK) return s;
       B.map_count = nv;
-      e = launch_light_march_f32(G[b], B.d_quads, B.d_tab, r->d_tf, B.d_map_local, r->d_cnt, r->stream);
-      if (e != cudaSuccess) return cuda_fail(r, e, "brick light march");
-      ++launches;
       BrickRef& R = refs[b];
       for (int d = 0; d < 3; ++d) {
         R.bmin[d] = G[b].bmin[d];
@@ -534,35 +576,54 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
     if (s != BEAMS_OK) return s;
     e = cudaMemcpyAsync(r->d_refs, refs.data(), nb * sizeof(BrickRef), cudaMemcpyHostToDevice, r->stream);
     if (e != cudaSuccess) return cuda_fail(r, e, "copying brick table");
+    // Phase 1: local maps
+    s = brick_lanes_fork(r);
+    if (s != BEAMS_OK) return s;
     for (int b = 0; b < nb; ++b) {
       Brick& B = r->bricks[b];
-      e = launch_light_march_f32(G[b], B.d_quads, B.d_tab, r->d_tf, B.d_map_final, r->d_cnt, r->stream, r->d_refs,
-                                 nb, b);
-      if (e != cudaSuccess) return cuda_fail(r, e, "brick stitch march");
+      e = launch_light_march_f32(G[b], B.d_quads, B.d_tab, r->d_tf, B.d_map_local, r->d_brick_cnt + b, lane(b));
+      if (e != cudaSuccess) return lane_fail(e, "brick light march");
       ++launches;
     }
+    e = brick_lanes_join(r);
+    if (e != cudaSuccess) return cuda_fail(r, e, "joining brick streams");
+    // Phases 2-3: stitched maps (each reads every brick's Phase-1 map)
+    s = brick_lanes_fork(r);
+    if (s != BEAMS_OK) return s;
+    for (int b = 0; b < nb; ++b) {
+      Brick& B = r->bricks[b];
+      e = launch_light_march_f32(G[b], B.d_quads, B.d_tab, r->d_tf, B.d_map_final, r->d_brick_cnt + b, lane(b),
+                                 r->d_refs, nb, b);
+      if (e != cudaSuccess) return lane_fail(e, "brick stitch march");
+      ++launches;
+    }
+    e = brick_lanes_join(r);
+    if (e != cudaSuccess) return cuda_fail(r, e, "joining brick streams");
   }
   cudaEventRecord(r->ev[1], r->stream);
   s = prepare_ray_limits(r, G[0], launches);  // one camera: the same limits for every brick
   if (s != BEAMS_OK) return s;
   for (int b = 1; b < nb; ++b) G[b].ray_max = G[0].ray_max;
+  // Phase 4: view marches
+  s = brick_lanes_fork(r);
+  if (s != BEAMS_OK) return s;
   for (int b = 0; b < nb; ++b) {
     Brick& B = r->bricks[b];
     float4* img = r->d_brick_imgs + (size_t)b * npix;
     // only the pixels whose rays can reach this brick are marched; the rest stay transparent
     const bool any = brick_window(G[b], G[b].win);
     if (!any || (size_t)G[b].win[2] * G[b].win[3] < npix) {
-      e = cudaMemsetAsync(img, 0, npix * sizeof(float4), r->stream);
-      if (e != cudaSuccess) return cuda_fail(r, e, "clearing brick image");
+      e = cudaMemsetAsync(img, 0, npix * sizeof(float4), lane(b));
+      if (e != cudaSuccess) return lane_fail(e, "clearing brick image");
       if (!any) continue;
     }
-    e = cudaMemsetAsync(&r->d_cnt->tiles_view, 0, sizeof(unsigned), r->stream);
-    if (e != cudaSuccess) return cuda_fail(r, e, "clearing tile counter");
     e = launch_view_march_f32(G[b], (const float*)B.d_field, B.d_quads, B.d_tab, r->d_tf,
-                              r->use_map ? B.d_map_final : nullptr, img, r->d_cnt, r->stream);
-    if (e != cudaSuccess) return cuda_fail(r, e, "brick view march");
+                              r->use_map ? B.d_map_final : nullptr, img, r->d_brick_cnt + b, lane(b));
+    if (e != cudaSuccess) return lane_fail(e, "brick view march");
     ++launches;
   }
+  e = brick_lanes_join(r);
+  if (e != cudaSuccess) return cuda_fail(r, e, "joining brick streams");
   cudaEventRecord(r->ev[2], r->stream);
   // Depth order: |camera - block centre| in float (MapperLightedVolume.cxx:221-241).
   std::vector<std::pair<float, int>> order;
@@ -611,16 +672,21 @@ beams_status render_bricks_frame(beams_renderer* r, const beams_camera* cam, flo
     std::memset(t, 0, sizeof(*t));
     e = cudaStreamSynchronize(r->stream);
     if (e != cudaSuccess) return cuda_fail(r, e, "render");
-    Counters c;
-    e = cudaMemcpy(&c, r->d_cnt, sizeof(c), cudaMemcpyDeviceToHost);
+    // the frame's counters plus every brick's (the per-brick launches count into their own)
+    std::vector<Counters> c(1 + r->bricks.size());
+    e = cudaMemcpy(c.data(), r->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(c.data() + 1, r->d_brick_cnt, r->bricks.size() * sizeof(Counters), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(r, e, "reading counters");
     cudaEventElapsedTime(&t->map_build_ms, r->ev[0], r->ev[1]);
     cudaEventElapsedTime(&t->view_march_ms, r->ev[1], r->ev[2]);
     cudaEventElapsedTime(&t->composite_ms, r->ev[2], r->ev[3]);
     cudaEventElapsedTime(&t->total_ms, r->ev[0], r->ev[3]);
-    t->light_samples = c.light_samples;
-    t->lit_samples = c.lit_samples;
-    t->rays_hit = c.rays_hit;
+    for (const Counters& k : c) {
+      t->light_samples += k.light_samples;
+      t->lit_samples += k.lit_samples;
+      t->rays_hit += k.rays_hit;
+    }
     size_t nv = 0;
     for (auto& b : r->bricks) nv += r->use_map ? b.map_count : 0;
     t->map_vertices = (int)nv;

@@ -155,6 +155,14 @@ struct beams_renderer {
   float4* d_brick_imgs = nullptr;
   size_t brick_imgs_cap = 0;
   unsigned long long brick_counter = 0;
+  // Per-brick launches run on kBrickLanes side streams (fork/join by events),
+  // so one brick's launch fills the SMs that the previous one's tail leaves
+  // idle; each brick has its own work counters (d_brick_cnt[b]).
+  static constexpr int kBrickLanes = 4;
+  cudaStream_t brick_lane[kBrickLanes] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t brick_fork = nullptr;
+  cudaEvent_t brick_join[kBrickLanes] = {nullptr, nullptr, nullptr, nullptr};
+  beams::Counters* d_brick_cnt = nullptr;  // kMaxBricks entries
 
   // learned form: parameters, optimiser state, inference weights
   beams::MlpState* mlp = nullptr;
@@ -181,6 +189,12 @@ struct beams_renderer {
     for (auto& b : bricks) b.release();
     if (d_refs) cudaFree(d_refs);
     if (d_brick_imgs) cudaFree(d_brick_imgs);
+    if (d_brick_cnt) cudaFree(d_brick_cnt);
+    for (auto& s : brick_lane)
+      if (s) cudaStreamDestroy(s);
+    for (auto& e : brick_join)
+      if (e) cudaEventDestroy(e);
+    if (brick_fork) cudaEventDestroy(brick_fork);
     if (d_cnt) cudaFree(d_cnt);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);

@@ -49,3 +49,34 @@ def test_null_arguments_are_rejected_without_a_device():
     assert L.beams_destroy(None) == 0
     n = (C.c_int * 3)(1, 1, 1)
     assert L.beams_generate_blobs(None, n, None, 0, 1, None) == 1
+
+
+# The ctypes mirrors of the header's structs, by C name.
+MIRRORS = {"beams_mlp_options": "MlpOptions", "beams_mlp_report": "MlpReport", "beams_tuning": "Tuning",
+           "beams_volume": "Volume", "beams_camera": "Camera", "beams_request": "Request",
+           "beams_batch_options": "BatchOptions", "beams_config_light": "ConfigLight",
+           "beams_scene_desc": "SceneDesc", "beams_timings": "Timings", "beams_vtk_field": "VtkField"}
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """Every struct the Python binding mirrors has the header's size and field
+    offsets (a C program built with the host compiler prints them)."""
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "beams_b200.h"', "int main(void) {"]
+    for cname, pyname in MIRRORS.items():
+        lines.append(f'  printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for field, _ in getattr(B, pyname)._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for ln in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        cname, key, val = ln.split()
+        got[(cname, key)] = int(val)
+    for cname, pyname in MIRRORS.items():
+        cls = getattr(B, pyname)
+        assert got[(cname, "sizeof")] == C.sizeof(cls), cname
+        for field, _ in cls._fields_:
+            assert got[(cname, field)] == getattr(cls, field).offset, (cname, field)

@@ -1287,6 +1287,7 @@ beams_status beams_set_bricks(beams_renderer* r, const beams_volume* bricks, int
       return fail(r, BEAMS_ERR_INVALID_ARG, "bricks: range must be finite");
   }
   cudaSetDevice(r->device);
+  cudaStreamSynchronize(r->stream);  // the previous frame's brick work (lanes join into r->stream) is done
   for (auto& b : r->bricks) b.release();
   r->bricks.assign(nbricks, Brick());
   for (int b = 0; b < nbricks; ++b) {

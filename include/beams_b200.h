@@ -14,7 +14,9 @@
  *  - Caller-owned inputs are copied unless the struct says on_device=1, in which
  *    case the device pointer is borrowed until the next set_* call or destroy.
  *  - One renderer per host thread. All GPU work is ordered on the stream given
- *    to beams_create (NULL = the legacy default stream).
+ *    to beams_create (NULL = the legacy default stream); multi-brick frames
+ *    fork their per-brick launches onto the renderer's own side streams and
+ *    join them back onto it before the call returns.
  *  - Pixel (x, y) is stored at rgba[4*(y*width + x)], y = 0 is the bottom row.
  */
 #ifndef BEAMS_B200_H

@@ -171,16 +171,16 @@ typedef struct beams_vtk_field {
 beams_status beams_vtk_read(const char* path, beams_vtk_field* out);
 void beams_vtk_free(beams_vtk_field* f);
 
-/* Explicit rectilinear coordinates for the current point volume (after
- * beams_set_volume): x, y, z hold dims[0], dims[1], dims[2] strictly increasing
+/* Explicit rectilinear coordinates for the current volume, point or cell field
+ * (after beams_set_volume): x, y, z hold dims[0], dims[1], dims[2] strictly increasing
  * float32 coordinates, the arrays of the ArrayHandleCartesianProduct coordinate
  * system that RenderCells receives (MapperLightedVolume.cxx:114-119) and that the
  * reference's RectilinearLocator and RectilinearMeshOracle search
  * (LightedVolumeRenderer.cxx:45-186, RectilinearMeshOracle.h:140-176). The
  * volume's origin/spacing are then ignored; the map grid spans the coordinates'
  * bounds. All three NULL return to uniform spacing; beams_set_volume also does.
- * Exact and precision forms of a single volume with one light; empty-space
- * skipping is off for such a volume. */
+ * Exact and precision forms of a single volume with one light (a cell field:
+ * the exact form's unlit march); empty-space skipping is off for such a volume. */
 beams_status beams_set_volume_coordinates(beams_renderer* r, const float* x, const float* y, const float* z);
 
 /* Replaces MapperLightedVolume::SetCompositeBackground (MapperLightedVolume.cxx:321-324)
@@ -419,9 +419,13 @@ beams_status beams_build_shadow_map(beams_renderer* r, beams_timings* t);
  * (map_cells+1)^3 transmittance map, lives in one static device array sized for
  * map_cells <= BEAMS_NOALLOC_MAX_MAP_CELLS (129^3 floats, 8.6 MB), which every
  * device that loads the library holds until exit; larger map_cells is rejected
- * with BEAMS_ERR_INVALID_ARG. The first call on each device looks up that
- * array's device address (cudaGetSymbolAddress), so make the first call on a
- * device outside any stream capture. All calls share the one array: calls that
+ * with BEAMS_ERR_INVALID_ARG. Every call looks up that array's device address
+ * in the current context (cudaGetSymbolAddress). With lazy module loading
+ * (CUDA_MODULE_LOADING=LAZY, the CUDA default) the first call on a device is
+ * what loads the module, and so where the 8.6 MB and the kernels' code are
+ * taken: make that first call (a warm-up frame) before the host framework claims
+ * its memory, and outside any stream capture. The volume data must be 4-byte
+ * aligned. All calls share the one array: calls that
  * overlap on the GPU (other streams, other threads) race and corrupt each
  * other's maps; serialise them. Each call rewrites every map entry it reads, so
  * no clearing is needed between calls. Errors: beams_last_error(NULL). */

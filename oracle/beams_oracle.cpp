@@ -30,8 +30,8 @@
 //    step absorbed by float rounding cannot spin forever.
 //  * A transfer function whose alphas are all 0 gives a light-march opacity of
 //    0 instead of 0/0 (TransmittanceMap.h:329 divides by the max alpha).
-//  * The TF index of the light march saturates for |value| >= 2^63 instead of
-//    taking x86's indefinite-integer value.
+//  * The TF index of the light march and of the cell-field march saturates for
+//    |value| >= 2^63 instead of taking x86's indefinite-integer value.
 
 #include "beams_oracle.h"
 
@@ -502,6 +502,42 @@ struct NoRecord {
   template <typename T> void operator()(const T*, const T*, T) const {}
 };
 
+// RectilinearLocator::LocateCell (LightedVolumeRenderer.cxx:108-156): per axis,
+// a point on the max face takes the last cell and keeps the previous inverse
+// spacing; otherwise the cell is walked from the previous one until
+// min <= p < max, and invSpacing = 1 / (max - min).
+template <typename T>
+inline void locate_cell_walk(const Geo<T>& g, const T p[3], int c[3], T inv[3]) {
+  for (int k = 0; k < 3; ++k) {
+    if (p[k] == g.maxp[k]) {
+      c[k] = g.n[k] - 2;
+      continue;
+    }
+    const std::vector<T>& C = g.C[k];
+    bool found = false;
+    T minVal = C[c[k]];
+    const int dirn = (p[k] - minVal >= T(0)) ? 1 : -1;
+    T maxVal = C[c[k] + 1];
+    while (!found) {
+      if (p[k] >= minVal && p[k] < maxVal) {
+        found = true;
+        continue;
+      }
+      c[k] += dirn;
+      const int nid = dirn == 1 ? c[k] + 1 : c[k];
+      const T next = C[nid];
+      if (dirn == 1) {
+        minVal = maxVal;
+        maxVal = next;
+      } else {
+        maxVal = minVal;
+        minVal = next;
+      }
+    }
+    inv[k] = T(1) / (maxVal - minVal);
+  }
+}
+
 // rec(p, tf_rgba, sa) is called at every composited sample, before shading.
 template <typename T, typename MapGet, typename Rec = NoRecord>
 void march_pixel(const Geo<T>& g, int x, int y, MapGet get, T color[4], uint64_t& lit, Rec rec = Rec()) {
@@ -529,34 +565,7 @@ void march_pixel(const Geo<T>& g, int x, int y, MapGet get, T color[4], uint64_t
     const T maxt = mx(tx, mx(ty, tz));
     if (maxt > T(1) || mint < T(0)) newCell = true;
     if (newCell) {
-      for (int k = 0; k < 3; ++k) {
-        if (p[k] == g.maxp[k]) {
-          c[k] = g.n[k] - 2;
-          continue;
-        }
-        const std::vector<T>& C = g.C[k];
-        bool found = false;
-        T minVal = C[c[k]];
-        const int dirn = (p[k] - minVal >= T(0)) ? 1 : -1;
-        T maxVal = C[c[k] + 1];
-        while (!found) {
-          if (p[k] >= minVal && p[k] < maxVal) {
-            found = true;
-            continue;
-          }
-          c[k] += dirn;
-          const int nid = dirn == 1 ? c[k] + 1 : c[k];
-          const T next = C[nid];
-          if (dirn == 1) {
-            minVal = maxVal;
-            maxVal = next;
-          } else {
-            maxVal = minVal;
-            minVal = next;
-          }
-        }
-        inv[k] = T(1) / (maxVal - minVal);
-      }
+      locate_cell_walk(g, p, c, inv);
       const int64_t i0 = (int64_t)c[2] * nxy + (int64_t)c[1] * nx + c[0];
       bl[0] = g.C[0][c[0]];
       bl[1] = g.C[1][c[1]];
@@ -617,6 +626,74 @@ void march_pixel(const Geo<T>& g, int x, int y, MapGet get, T color[4], uint64_t
   }
 }
 
+// SamplerCellAssoc::operator() (LightedVolumeRenderer.cxx:540-641): the unlit
+// march of a cell-centred field ((n-1)^3 values, x fastest, cell id
+// (c2 (ny-1) + c1) (nx-1) + c0, :252-255). The TF index of the cell value is
+// truncated and clamped to [0, n-1] (:603-608); the colour is fetched once per
+// cell, the cell is kept while tx, ty, tz stay in [0, 1] (starting from 2, so
+// the first sample locates, :581-583), each sample composites
+// a = A (1 - C.a), C.rgb += rgb a, C.a += a (:617-621), then the ray advances
+// and breaks on C.a >= cutoff before tx/ty/tz are updated (:624-631); the
+// result is clamped to 1 per channel (:632-635). Every composite is counted.
+template <typename T>
+void march_pixel_cells(const Geo<T>& g, int x, int y, T color[4], uint64_t& lit) {
+  color[0] = color[1] = color[2] = color[3] = T(0);
+  T o[3], d[3], minD, maxD;
+  if (!ray_setup(g, x, y, o, d, minD, maxD)) return;  // minDistance == -1
+  const T q = (maxD - minD) / g.sd;
+  int64_t budget = (q < (T)1e9) ? (int64_t)q + 16 : (int64_t)1000000000;
+  T dist = minD + g.mesh_eps;
+  T p[3] = {o[0] + dist * d[0], o[1] + dist * d[1], o[2] + dist * d[2]};
+  while (!inside_vol(g, p) && dist < maxD && budget-- > 0) {
+    dist += g.sd;
+    for (int k = 0; k < 3; ++k) p[k] = o[k] + dist * d[k];
+  }
+  bool newCell = true;
+  T tx = T(2), ty = T(2), tz = T(2);
+  T sc[4] = {0, 0, 0, 0};
+  T bl[3] = {0, 0, 0};
+  T inv[3] = {0, 0, 0};
+  int c[3] = {0, 0, 0};
+  const int N1 = g.tf_n - 1;
+  const int64_t cx = g.n[0] - 1, cxy = (int64_t)(g.n[0] - 1) * (g.n[1] - 1);
+  while (inside_vol(g, p) && dist < maxD && budget-- > 0) {
+    const T mint = mn(tx, mn(ty, tz));
+    const T maxt = mx(tx, mx(ty, tz));
+    if (maxt > T(1) || mint < T(0)) newCell = true;
+    if (newCell) {
+      locate_cell_walk(g, p, c, inv);
+      const int64_t cid = (int64_t)c[2] * cxy + (int64_t)c[1] * cx + c[0];
+      const T s0 = (T)g.field[cid];
+      const T ns = (s0 - g.min_scalar) * g.inv_delta;
+      const T fi = ns * (T)N1;
+      int idx;  // static_cast<vtkm::Id>, saturating (see the file header), then the clamp
+      if (fi > T(-1) && fi < (T)(N1 + 1)) idx = (int)(int64_t)fi;
+      else idx = (fi >= (T)(N1 + 1)) ? N1 : 0;
+      if (idx < 0) idx = 0;
+      if (idx > N1) idx = N1;
+      for (int k = 0; k < 4; ++k) sc[k] = g.tf[4 * idx + k];
+      for (int k = 0; k < 3; ++k) bl[k] = g.C[k][c[k]];  // GetMinPoint
+      tx = (p[0] - bl[0]) * inv[0];
+      ty = (p[1] - bl[1]) * inv[1];
+      tz = (p[2] - bl[2]) * inv[2];
+      newCell = false;
+    }
+    const T alpha = sc[3] * (T(1) - color[3]);
+    color[0] = color[0] + sc[0] * alpha;
+    color[1] = color[1] + sc[1] * alpha;
+    color[2] = color[2] + sc[2] * alpha;
+    color[3] = alpha + color[3];
+    ++lit;
+    dist += g.sd;
+    for (int k = 0; k < 3; ++k) p[k] = p[k] + g.sd * d[k];
+    if (color[3] >= g.cutoff) break;
+    tx = (p[0] - bl[0]) * inv[0];
+    ty = (p[1] - bl[1]) * inv[1];
+    tz = (p[2] - bl[2]) * inv[2];
+  }
+  for (int k = 0; k < 4; ++k) color[k] = mn(color[k], T(1));
+}
+
 int nthreads(int t) {
 #ifdef _OPENMP
   return t > 0 ? t : omp_get_max_threads();
@@ -667,6 +744,28 @@ int light_march_ids(const oracle_scene* s, const int64_t* ids, int64_t n, T* out
     total += ns;
   }
   if (samples) *samples = total;
+  return 0;
+}
+
+template <typename T>
+int view_march_cells(const oracle_scene* s, int x0, int y0, int w, int h, T* rgba, int threads,
+                     uint64_t* lit_out) {
+  if (!valid(s) || !rgba) return 1;
+  if (x0 < 0 || y0 < 0 || x0 + w > s->width || y0 + h > s->height) return 1;
+  Geo<T> g;
+  build_geo(s, g);
+  uint64_t lit = 0;
+  const int64_t npx = (int64_t)w * h;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads(threads)) reduction(+ : lit)
+  for (int64_t i = 0; i < npx; ++i) {
+    const int yy = (int)(i / w), xx = (int)(i - (int64_t)yy * w);
+    T c[4];
+    uint64_t l = 0;
+    march_pixel_cells(g, x0 + xx, y0 + yy, c, l);
+    lit += l;
+    for (int k = 0; k < 4; ++k) rgba[4 * i + k] = c[k];
+  }
+  if (lit_out) *lit_out = lit;
   return 0;
 }
 
@@ -963,6 +1062,14 @@ int oracle_view_march_f64(const oracle_scene* s, const double* map, int x0, int 
   return view_march<double>(s, map, x0, y0, w, h, rgba, threads, lit);
 }
 
+int oracle_view_march_cells_f32(const oracle_scene* s, int x0, int y0, int w, int h, float* rgba_out, int threads,
+                                uint64_t* lit_samples) {
+  return view_march_cells(s, x0, y0, w, h, rgba_out, threads, lit_samples);
+}
+int oracle_view_march_cells_f64(const oracle_scene* s, int x0, int y0, int w, int h, double* rgba_out, int threads,
+                                uint64_t* lit_samples) {
+  return view_march_cells(s, x0, y0, w, h, rgba_out, threads, lit_samples);
+}
 int oracle_window_depth_to_distance(const oracle_scene* s, const float* depth, double near_plane,
                                     double far_plane, double* out) {
   if (!valid(s) || !depth || !out || !(near_plane > 0.0) || !(far_plane > near_plane)) return 1;

@@ -82,6 +82,12 @@ int oracle_view_march_f32(const oracle_scene* s, const float* map, int x0, int y
                           float* rgba_out, int threads, uint64_t* lit_samples);
 int oracle_view_march_f64(const oracle_scene* s, const double* map, int x0, int y0, int w, int h,
                           double* rgba_out, int threads, uint64_t* lit_samples);
+/* Cell-associated field (SamplerCellAssoc): s->field holds (dims-1)^3 cell
+ * values, x fastest; unlit, use_map is ignored. rgba_out is w*h*4. */
+int oracle_view_march_cells_f32(const oracle_scene* s, int x0, int y0, int w, int h, float* rgba_out, int threads,
+                                uint64_t* lit_samples);
+int oracle_view_march_cells_f64(const oracle_scene* s, int x0, int y0, int w, int h, double* rgba_out, int threads,
+                                uint64_t* lit_samples);
 /* Per-pixel ray limits of a window-depth buffer (OpenGL depth in [0, 1] under
  * the camera's perspective with near/far planes, unprojected at the pixel
  * centre: t = 2fn / ((f + n) - (2d - 1)(f - n)) times the length of the

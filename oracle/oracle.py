@@ -44,6 +44,8 @@ def lib():
             "oracle_light_march_points_f32": [S, P, C.c_int64, P, P, C.c_int],
             "oracle_view_march_f32": [S, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
             "oracle_view_march_f64": [S, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
+            "oracle_view_march_cells_f32": [S, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
+            "oracle_view_march_cells_f64": [S, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
             "oracle_view_march_lazy_f64": [S, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, u64p],
             "oracle_window_depth_to_distance": [S, P, C.c_double, C.c_double, P],
             "oracle_view_march_multi_f32": [S, P, C.c_int, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int,
@@ -155,6 +157,21 @@ class Oracle:
         if fn(C.byref(self.cs), None if mp is None else _p(mp), x0, y0, w, h, _p(out), self.threads,
               C.byref(lit)):
             raise RuntimeError("oracle view march rejected the scene")
+        return out, lit.value
+
+    def view_march_cells(self, window=None, fp64: bool = False):
+        """Unlit march of a cell-centred field (SamplerCellAssoc): build the Oracle
+        with field = the (nz-1, ny-1, nx-1) cell values and the scene's point dims."""
+        s = self.scene
+        x0, y0, w, h = window if window is not None else (0, 0, s.width, s.height)
+        if self.field.size != (s.dims[0] - 1) * (s.dims[1] - 1) * (s.dims[2] - 1):
+            raise ValueError("view_march_cells needs the (dims - 1)^3 cell values as the field")
+        dt = np.float64 if fp64 else np.float32
+        out = np.zeros((h, w, 4), dt)
+        lit = C.c_uint64()
+        fn = lib().oracle_view_march_cells_f64 if fp64 else lib().oracle_view_march_cells_f32
+        if fn(C.byref(self.cs), x0, y0, w, h, _p(out), self.threads, C.byref(lit)):
+            raise RuntimeError("oracle cell-field march rejected the scene")
         return out, lit.value
 
     def view_march_multi(self, maps, light_colors, window=None):

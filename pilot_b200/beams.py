@@ -517,7 +517,7 @@ class Renderer:
         self._check(self._L.beams_set_background(self._h, int(bool(on)), c))
 
     def set_volume_coordinates(self, x=None, y=None, z=None):
-        """Explicit rectilinear coordinates of the current point volume (float32,
+        """Explicit rectilinear coordinates of the current volume (float32,
         strictly increasing, dims[d] values per axis); no arguments: uniform again."""
         if x is None and y is None and z is None:
             self._check(self._L.beams_set_volume_coordinates(self._h, None, None, None))

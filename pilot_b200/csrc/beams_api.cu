@@ -444,10 +444,9 @@ beams_status mlp_render_view(beams_renderer* r, const ExactGeo& g, float4* out, 
 bool mlp_ready(const beams_renderer* r);
 
 beams_status check_ready(beams_renderer* r) {
-  if (r->rect && (r->brick_mode || r->form == BEAMS_FORM_MLP || r->vol.assoc != BEAMS_ASSOC_POINTS ||
-                  (r->multi_light && r->lights.size() > 1)))
+  if (r->rect && (r->brick_mode || r->form == BEAMS_FORM_MLP || (r->multi_light && r->lights.size() > 1)))
     return fail(r, BEAMS_ERR_UNSUPPORTED,
-                "explicit volume coordinates render in the exact and precision forms of a single point volume "
+                "explicit volume coordinates render in the exact and precision forms of a single volume "
                 "with one light");
   if (r->multi_light && r->lights.size() > 1) {
     if (r->brick_mode || r->form != BEAMS_FORM_EXACT || (r->has_volume && r->vol.assoc != BEAMS_ASSOC_POINTS))
@@ -800,8 +799,7 @@ beams_status beams_set_volume_coordinates(beams_renderer* r, const float* x, con
     return BEAMS_OK;
   }
   if (!x || !y || !z) return fail(r, BEAMS_ERR_INVALID_ARG, "volume coordinates: give all three axes or none");
-  if (!r->has_volume || r->vol.assoc != BEAMS_ASSOC_POINTS)
-    return fail(r, BEAMS_ERR_STATE, "volume coordinates: set a point volume first (beams_set_volume)");
+  if (!r->has_volume) return fail(r, BEAMS_ERR_STATE, "volume coordinates: set a volume first (beams_set_volume)");
   const float* a[3] = {x, y, z};
   for (int d = 0; d < 3; ++d) {
     const int n = r->vol.dims[d];

@@ -18,7 +18,6 @@
 
 #include <cmath>
 #include <cstring>
-#include <mutex>
 
 #include "../../include/beams_b200.h"
 #include "exact_device.cuh"
@@ -31,7 +30,6 @@ constexpr int kMaxMapCells = BEAMS_NOALLOC_MAX_MAP_CELLS;
 constexpr size_t kMaxMapVertices = (size_t)(kMaxMapCells + 1) * (kMaxMapCells + 1) * (kMaxMapCells + 1);
 constexpr size_t kScratchFloats = (kMaxMapVertices + 63) / 64 * 64;
 constexpr int kMaxTFn = 1024;
-constexpr int kMaxDevices = 64;
 
 // The scratch: one frame's (M+1)^3 map, M <= BEAMS_NOALLOC_MAX_MAP_CELLS
 // (129^3 floats, 8.6 MB). Every device that loads this library holds it until
@@ -39,25 +37,18 @@ constexpr int kMaxDevices = 64;
 // kernels get the device address from cudaGetSymbolAddress.
 static __device__ __align__(256) float g_noalloc_map[kScratchFloats];
 
-std::mutex g_mu;
-void* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of the scratch on the current device, looked up once per
-// device (the first call on a device does this, so it must not be the first
-// CUDA call inside a stream capture).
+// Device address of the scratch in the current context, looked up on every
+// call: it is cheap once the module is loaded, and it stays right when the
+// context changes under this library (a cudaDeviceReset, or a host that runs
+// the call under its own driver-API context on the device). With lazy module
+// loading (CUDA_MODULE_LOADING=LAZY, the default) the first lookup on a device
+// loads this file's module and so reserves the array; that first call must not
+// run inside a stream capture.
 cudaError_t scratch_address(float** out) {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_map);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_map);
-    if (e != cudaSuccess) return e;
-    g_scratch_addr[dev] = p;
-  }
-  *out = (float*)g_scratch_addr[dev];
+  *out = (float*)p;
   return cudaSuccess;
 }
 
@@ -76,6 +67,12 @@ __device__ void stage_tf(const float4* __restrict__ tf, int n, float4* s_tf, flo
   __syncthreads();
   const float m = *s_max;
   for (int i = threadIdx.x; i < n; i += blockDim.x) s_a[i] = (m > 0.f) ? s_tf[i].w / m : 0.f;
+  __syncthreads();
+}
+
+// The view march reads the TF colours only (no alpha / max alpha pass).
+__device__ void stage_tf_colors(const float4* __restrict__ tf, int n, float4* s_tf) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s_tf[i] = tf[i];
   __syncthreads();
 }
 
@@ -183,9 +180,7 @@ __global__ void __launch_bounds__(256) k_noalloc_view_march(const ExactGeo g, co
                                                             const float* __restrict__ map,
                                                             float4* __restrict__ out) {
   __shared__ float4 s_tf[kMaxTFn];
-  __shared__ float s_a[kMaxTFn];
-  __shared__ float s_max;
-  stage_tf(tf, g.tf_n, s_tf, s_a, &s_max);
+  stage_tf_colors(tf, g.tf_n, s_tf);
   const int tiles_x = (g.width + 15) >> 4;
   const int x = (blockIdx.x % tiles_x) * 16 + (threadIdx.x & 15);
   const int y = (blockIdx.x / tiles_x) * 16 + (threadIdx.x >> 4);
@@ -309,6 +304,10 @@ extern "C" beams_status beams_render_noalloc(const beams_volume* vol, const floa
     return nf(BEAMS_ERR_INVALID_ARG, "render_noalloc: bad camera");
   if (((uintptr_t)rgba_out_device & 15) != 0 || ((uintptr_t)tf_rgba_device & 15) != 0)
     return nf(BEAMS_ERR_INVALID_ARG, "render_noalloc: output and colour map must be 16-byte aligned");
+  if (((uintptr_t)vol->data & 3) != 0)
+    return nf(BEAMS_ERR_INVALID_ARG, "render_noalloc: the volume data must be 4-byte aligned");
+  if (!std::isfinite(light_color[0]) || !std::isfinite(light_color[1]) || !std::isfinite(light_color[2]))
+    return nf(BEAMS_ERR_INVALID_ARG, "render_noalloc: non-finite light colour");
 
   // Parameters, derived in the reference's float32 order (as beams_render does).
   ExactGeo g;

@@ -76,17 +76,13 @@ def test_slab_fp32_reference_mode(cuda_device):
     assert np.mean(np.all(img == oimg, axis=-1)) > 0.999
 
 
-def test_no_shadow_map_and_cell_field(cuda_device):
+def test_no_shadow_map(cuda_device):
+    """Unlit point field (use_map off); cell fields are in test_cells_gpu.py."""
     s = scenes.small(5, n=32, image=64, m=8)
     s.use_map = False
     img, _, t, r = gpu_render(s)
     oimg, lit = Oracle(s).view_march(None)
     assert np.max(np.abs(img - oimg)) <= TOL and t["map_vertices"] == 0 and t["lit_samples"] == lit
-    # Cell-associated field: SamplerCellAssoc (unlit, nearest cell value).
-    cells = s.field_numpy()[:-1, :-1, :-1].copy()
-    r.set_volume(cells, dims=s.dims, origin=s.origin, spacing=s.spacing, value_range=(0, 1), assoc=B.ASSOC_CELLS)
-    img2, t2 = r.render(s.camera())
-    assert t2["lit_samples"] > 0 and np.all(img2 <= 1.0) and img2[..., 3].max() > 0
 
 
 def test_config0_parity(cuda_device):

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 import torch
 
-from oracle.oracle import Oracle, spheres_field
+from oracle.oracle import Oracle, noise_field, spheres_field
 from pilot_b200 import beams as B
 from pilot_b200 import scenes
 
@@ -52,6 +52,22 @@ def test_spheres_field_matches_oracle(cuda_device):
     assert st == 0
     ref = spheres_field(dims, org, sp, ell, default=0.1, floor=(-0.01, 0.7))
     assert np.array_equal(t.cpu().numpy(), ref)
+
+
+def test_device_noise_equals_oracle_noise_config1(cuda_device):
+    """The benchmark's 512^3 gradient-noise field (the config-1 seed): the device
+    generator (beams_generate_noise, what the GPU arm renders) and the oracle's
+    CPU generator (what the reference arm renders) give the same float32 field
+    bit for bit, the [0, 1] normalisation included."""
+    s = scenes.config1()
+    fd = s.field_device()
+    torch.cuda.synchronize()
+    dev = fd.cpu().numpy()
+    del fd
+    ref = noise_field(s.dims, s.params, s.octaves, s.base_freq)
+    assert dev.shape == ref.shape
+    assert np.array_equal(dev, ref), f"{int(np.sum(dev != ref))} of {dev.size} values differ"
+    assert dev.min() == 0.0 and dev.max() == 1.0
 
 
 def _oracle_scene(d, cam, field, light, intensity):

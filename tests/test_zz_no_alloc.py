@@ -32,16 +32,17 @@ def _fn():
     return f
 
 
-def _render_noalloc(s, field_dev, tf_dev, out_dev):
+def _render_noalloc(s, field_dev, tf_dev, out_dev, data_offset=0, tf_n=None, light_color=None):
     import torch
     nz, ny, nx = field_dev.shape
-    vol = B.Volume(C.c_void_p(field_dev.data_ptr()), B.F32, (C.c_int * 3)(nx, ny, nz),
+    vol = B.Volume(C.c_void_p(field_dev.data_ptr() + data_offset), B.F32, (C.c_int * 3)(nx, ny, nz),
                    (C.c_double * 3)(*s.origin), (C.c_double * 3)(*s.spacing),
                    (C.c_double * 2)(*s.value_range), B.ASSOC_POINTS, 1)
     cam = s.camera()
     light = (C.c_double * 3)(*s.light)
-    color = (C.c_float * 3)(*s.light_color)
-    st = _fn()(C.byref(vol), C.c_void_p(tf_dev.data_ptr()), tf_dev.shape[0], light, color, s.light_intensity,
+    color = (C.c_float * 3)(*(s.light_color if light_color is None else light_color))
+    n = tf_dev.shape[0] if tf_n is None else tf_n
+    st = _fn()(C.byref(vol), C.c_void_p(tf_dev.data_ptr()), n, light, color, s.light_intensity,
                s.map_m, s.sample_distance, s.cutoff, C.byref(cam), C.c_void_p(out_dev.data_ptr()),
                C.c_void_p(torch.cuda.current_stream().cuda_stream))
     return st
@@ -92,3 +93,15 @@ def test_noalloc_rejects_maps_beyond_the_static_scratch(cuda_device):
     st = _render_noalloc(s, fd, tf, out)
     assert st == 1  # BEAMS_ERR_INVALID_ARG
     assert b"128" in B.lib().beams_last_error(None)
+    # Arguments the call checks on the host before it launches anything: a
+    # field pointer that is not 4-byte aligned, a non-finite light colour, and a
+    # colour map size outside [1, 1024].
+    ok = scenes.small(24, n=16, image=8, m=8)
+    fd = torch.from_numpy(ok.field_numpy()).cuda()
+    assert _render_noalloc(ok, fd, tf, out, data_offset=2) == 1
+    assert b"aligned" in B.lib().beams_last_error(None)
+    assert _render_noalloc(ok, fd, tf, out, light_color=(1.0, float("nan"), 1.0)) == 1
+    assert _render_noalloc(ok, fd, tf, out, tf_n=0) == 1
+    assert _render_noalloc(ok, fd, tf, out, tf_n=1025) == 1
+    assert _render_noalloc(ok, fd, tf, out) == 0
+    torch.cuda.synchronize()

@@ -12,6 +12,7 @@ larger than L2, so no flush is needed between steps.
   python bench.py --form mlp [--knot 4] [--mlp-scene-light]    # learned form on the config 1 field
   python bench.py --form batch [--requests 64]                 # config 3: batched requests, one launch
   python bench.py --form bricks                                # config 3: 2x2x2 bricks of the 512^3 field
+  python bench.py --profile-case light_march [--reps 3]        # one fixed small case per kernel, for ncu
 
 N > 1 runs N independent replicas (the path does not shard across GPUs: there
 is no exchange step), launched by torch.distributed.run; value is the total over
@@ -24,8 +25,14 @@ The line carries:
               uploads the field from pinned host memory and reads the image back,
   roofline    the dominant kernel's algorithmic bytes / its CUDA-event time,
               against the measured HBM copy bandwidth,
-  cpu_baseline the CPU oracle (the reference algorithm, OpenMP) on a bounded
-              sample of the same frame, extrapolated to a full frame.
+  cpu_baseline the CPU oracle (the reference algorithm, OpenMP) on one whole
+              frame when a sample says it fits the budget (the sample's
+              extrapolation and its error beside it), else on the sample,
+  learned     the metric's second half: the learned form on the same frame,
+              with config 4's network (32 training lights) and with a network
+              trained for the rendered light; frames/s against the exact frame,
+              PSNR against the FP64 oracle on crops, fallback tiles, tensor
+              roofline (training is not timed).
 """
 from __future__ import annotations
 
@@ -183,42 +190,65 @@ def workload_desc(s, config: int):
 def cpu_sample_frame(scene, field, map_values, budget_s: float, threads: int, rng_seed: int = 0):
     """Times the oracle on a bounded sample of one frame and extrapolates.
 
-    Light march: a random subset of map vertices. View march: every S-th image
-    row (full width), shading by map_values (the shading only scales colour, so
-    the work does not depend on the map's values). Returns per-frame estimates."""
+    Light march: whole z-slabs of map vertices, evenly spread over z and each
+    marched in the map's raster order (as a full build runs them). View march:
+    evenly spread whole image rows, shading by map_values (the shading only
+    scales colour, so the work does not depend on the map's values). Returns
+    per-frame estimates."""
     from oracle.oracle import Oracle
     o = Oracle(scene, field=field, threads=threads)
     pd = scene.map_m + 1
+    slab = pd * pd
     nvert = pd ** 3
-    rng = np.random.default_rng(rng_seed)
-    # calibrate on a small pilot, then size the sample to the budget
-    pilot = rng.choice(nvert, min(nvert, 4096), replace=False)
+    # calibrate on one slab and one row, then size the sample to the budget
+    mid = pd // 2
     t0 = time.perf_counter()
-    o.light_march_ids(pilot)
-    per_vertex = (time.perf_counter() - t0) / pilot.size
+    o.light_march_ids(np.arange(mid * slab, (mid + 1) * slab, dtype=np.int64))
+    per_slab = time.perf_counter() - t0
     t0 = time.perf_counter()
     row = scene.height // 2
     o.view_march(map_values, window=(0, row, scene.width, 1))
     per_row = time.perf_counter() - t0
-    nv = int(min(nvert, max(4096, 0.6 * budget_s / max(per_vertex, 1e-9))))
+    nslabs = int(min(pd, max(1, 0.6 * budget_s / max(per_slab, 1e-9))))
     nrows = int(min(scene.height, max(1, 0.4 * budget_s / max(per_row, 1e-9))))
-    ids = rng.choice(nvert, nv, replace=False)
+    off = np.random.default_rng(rng_seed).random()
+    zs = np.unique(np.minimum(pd - 1, ((np.arange(nslabs) + off) * pd / nslabs).astype(np.int64)))
+    ids = np.concatenate([np.arange(z * slab, (z + 1) * slab, dtype=np.int64) for z in zs])
     t0 = time.perf_counter()
-    _, light_samples = o.light_march_ids(ids)
+    _, light_samples = o.light_march_ids(ids)  # one call: the slabs in raster order
     t_light = time.perf_counter() - t0
-    rows = np.linspace(0, scene.height - 1, nrows).round().astype(int)
+    # the rows as 8 evenly spread bands of whole rows, one call per band
+    nb = min(8, nrows)
+    bh = max(1, nrows // nb)
+    y0s = np.unique(np.linspace(0, scene.height - bh, nb).round().astype(int))
     t0 = time.perf_counter()
     lit = 0
-    for y in rows:
-        _, l = o.view_march(map_values, window=(0, int(y), scene.width, 1))
+    for y in y0s:
+        _, l = o.view_march(map_values, window=(0, int(y), scene.width, bh))
         lit += l
     t_view = time.perf_counter() - t0
-    frame_s = t_light * nvert / nv + t_view * scene.height / nrows
+    nrows = y0s.size * bh
+    frame_s = t_light * nvert / ids.size + t_view * scene.height / nrows
     lit_frame = lit * scene.height / nrows
     return {"frame_s": frame_s, "lit_per_frame": lit_frame, "value": lit_frame / frame_s,
-            "sample": f"{nv} of {nvert} map vertices (random) + {nrows} of {scene.height} image rows; "
-                      f"timed {t_light + t_view:.1f} s, extrapolated to one frame",
+            "sample": f"{zs.size} of {pd} whole z-slabs of map vertices (raster order, evenly spread) + "
+                      f"{y0s.size} bands of {bh} of {scene.height} image rows; timed {t_light + t_view:.1f} s, "
+                      f"extrapolated to one frame",
             "t_light_s": t_light, "t_view_s": t_view, "light_samples_sampled": light_samples}
+
+
+def cpu_full_frame(scene, field, threads: int):
+    """One whole frame on the oracle: the light march over every map vertex,
+    then the view march over every pixel shading by that map."""
+    from oracle.oracle import Oracle
+    o = Oracle(scene, field=field, threads=threads)
+    t0 = time.perf_counter()
+    m, light_samples = o.light_march()
+    t1 = time.perf_counter()
+    _, lit = o.view_march(m)
+    t2 = time.perf_counter()
+    return {"frame_s": t2 - t0, "light_s": t1 - t0, "view_s": t2 - t1, "lit_per_frame": lit,
+            "light_samples": light_samples, "value": lit / (t2 - t0), "map": m}
 
 
 def run_reference(args):
@@ -233,6 +263,8 @@ def run_reference(args):
     else:
         field = s.field_numpy()
     zero_map = np.zeros((s.map_m + 1,) * 3, np.float32)
+    # one whole frame first (untimed): the yardstick of the per-step extrapolation
+    full = cpu_full_frame(s, field, threads) if not args.no_full_frame else None
     per_step = max(1.0, min(10.0, 150.0 / max(1, args.steps + args.warmup)))
     results = []
     for i in range(args.warmup + args.steps):
@@ -242,6 +274,13 @@ def run_reference(args):
     frame_s = float(np.mean([r["frame_s"] for r in results]))
     lit = float(np.mean([r["lit_per_frame"] for r in results]))
     value = lit / frame_s
+    check = None
+    if full is not None:
+        check = {"full_frame_s": full["frame_s"], "full_frame_light_s": full["light_s"],
+                 "full_frame_view_s": full["view_s"], "full_frame_value": full["value"],
+                 "extrapolated_frame_s": frame_s,
+                 "extrapolation_error": frame_s / full["frame_s"] - 1.0,
+                 "lit_error": lit / full["lit_per_frame"] - 1.0}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": frame_s * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -250,7 +289,8 @@ def run_reference(args):
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": results[-1]["sample"] + "; the reference cannot be built here (VTK-m, "
                                        "MPI absent), so its algorithm runs as the project's C++ restatement"},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "full_frame_check": check}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -409,6 +449,42 @@ def run_ours(args):
         c = cpu_sample_frame(s, field, gpu_map, args.cpu_budget, threads)
         cpu = {"value": c["value"], "unit": UNIT, "cores": threads, "kind": "port", "sample": c["sample"],
                "ms_per_frame": c["frame_s"] * 1e3}
+        # a whole frame when the sample says it fits the budget: it replaces the
+        # extrapolation, which is kept beside it with its error
+        if not args.no_full_frame and c["frame_s"] <= 4.0 * args.cpu_budget:
+            f = cpu_full_frame(s, field, threads)
+            cpu = {"value": f["value"], "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"one whole frame: light march over all {nvert} map vertices, view march over all "
+                             f"{npix} pixels ({f['frame_s']:.1f} s)",
+                   "ms_per_frame": f["frame_s"] * 1e3, "light_ms": f["light_s"] * 1e3, "view_ms": f["view_s"] * 1e3,
+                   "map_equals_gpu": bool(np.array_equal(f["map"], gpu_map)),
+                   "extrapolated_from_sample": {"ms_per_frame": c["frame_s"] * 1e3, "sample": c["sample"],
+                                                "error": c["frame_s"] / f["frame_s"] - 1.0}}
+
+    # the metric's second half: the learned form on the same field, camera and
+    # light, against this run's exact frame (config 4's network as specified,
+    # trained over 32 light directions, and a network trained for the rendered
+    # light); training runs before each record's timed frames
+    learned = None
+    if not args.no_learned:
+        r.set_reuse_shadow_map(False)
+        r.render(cam, out=out, timings=False)
+        exact_img = out.cpu().numpy()
+        field_host = None
+        if rank == 0 and not args.no_quality:
+            field_host = field if cpu is not None else fd.cpu().numpy()
+        learned = {}
+        for name, lights, scene_light in (("lights32", 32, False), ("scene_light", 1, True)):
+            rec, _, _, _, _ = learned_record(
+                B, r, s, cam, out, exact_img, max_ms / args.steps, stream, world, local, lights=lights,
+                scene_light=scene_light, knot=args.learned_knot, probe_fraction=args.probe_fraction,
+                fallback_tol=args.fallback_tol, samples_log2=args.mlp_samples_log2, epochs=args.mlp_epochs,
+                steps=max(10, min(args.steps, 50)), warmup=3, field_host=field_host, crops=args.crops,
+                crop=args.crop, crop_stride=args.crop_stride, threads=os.cpu_count() or 1)
+            rec["network"] = ("config 4 as specified: 2^24 samples over 32 light directions uniform on the sphere"
+                              if lights == 32 else "2^24 samples for the rendered light only (fixed light, any camera)")
+            learned[name] = rec
+        r.set_form(B.FORM_EXACT)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -421,7 +497,8 @@ def run_ours(args):
                                          "note": "the frame's view march, rendering with the frame's map reused"},
                 "lit_samples_per_frame": lit_frame, "light_samples_per_frame": light_frame,
                 "gpu_launches": launches_per_frame * args.steps,
-                "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": sampler.summary()}
+                "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": sampler.summary(),
+                "learned": learned}
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:
@@ -489,6 +566,55 @@ def fp64_crops(s, field, images, crop, stride, ncrops, threads):
     return out
 
 
+def learned_record(B, r, s, cam, out, exact_img, exact_ms, stream, world, local, *, lights, scene_light, knot,
+                   probe_fraction, fallback_tol, samples_log2, epochs, steps, warmup, field_host=None, crops=3,
+                   crop=128, crop_stride=1, threads=1):
+    """Trains the learned form's network (untimed), then times its frames (network
+    view march + probe check + fallback) and reports speed against the exact
+    frame, fallback tiles, the tensor roofline of the fused network march and the
+    image error against the exact-map image and (field_host given) the FP64
+    oracle. Leaves the renderer in the learned form."""
+    from oracle.oracle import psnr
+    rep = r.mlp_train(B.mlp_options(samples_log2=samples_log2, n_lights=lights, epochs=epochs,
+                                    scene_light=int(scene_light)))
+    opts = dict(knot=knot, probe_fraction=probe_fraction, fallback_tol=fallback_tol)
+    # the network alone (no probes): its kernel time for the tensor roofline and its image
+    r.set_form(B.FORM_MLP, B.mlp_options(**dict(opts, probe_fraction=0.0)))
+    r.render(cam, out=out, timings=True)
+    _, tn = r.render(cam, out=out, timings=True)
+    net_img = out.cpu().numpy()
+    r.set_form(B.FORM_MLP, B.mlp_options(**opts))
+    _, tm = r.render(cam, out=out, timings=True)
+    img = out.cpu().numpy()
+    frame = lambda: r.render(cam, out=out, timings=False)  # noqa: E731  network + probes + fallback
+    total_ms, clocks = time_frames(frame, steps, warmup, stream, world, local)
+    tpeak, tsrc = measured_tensor_peak()
+    flops = tn["mlp_samples"] * MLP_FLOP_PER_EVAL
+    ach = flops / (tn["view_march_ms"] / 1e3) / 1e12
+    ntiles = -(-s.width // 32) * -(-s.height // 32)
+    ms = total_ms / steps
+    rec = {"train": {k: rep[k] for k in ("datagen_ms", "train_ms", "holdout_rmse", "unlit_rmse", "mean_rmse", "steps",
+                                         "samples")},
+           "train_note": "training (data generation by the exact light march + Adam) runs before the timed frames",
+           "lights": lights, "scene_light": bool(scene_light), "knot": knot, "probe_fraction": probe_fraction,
+           "fallback_tol": fallback_tol, "fallback_tiles": tm["fallback_tiles"], "tiles": ntiles,
+           "network_evaluations": tm["mlp_samples"], "ms_per_frame": ms, "frames_per_s": 1e3 / ms,
+           "exact_ms_per_frame": exact_ms, "exact_frames_per_s": 1e3 / exact_ms,
+           "speedup_vs_exact": exact_ms / ms, "network_only_ms": tn["total_ms"],
+           "roofline": {"bound": "tensor", "kernel": "k_view_march_mlp", "achieved": ach, "peak": tpeak,
+                        "unit": "TFLOP/s", "frac": ach / tpeak, "peak_source": tsrc,
+                        "flops_model": f"{MLP_FLOP_PER_EVAL} FLOP per network evaluation",
+                        "evaluations": tn["mlp_samples"], "kernel_ms": tn["view_march_ms"]},
+           "psnr_vs_exact_map_full_frame": psnr(img, exact_img),
+           "network_only_psnr_vs_exact_map": psnr(net_img, exact_img), "clocks": clocks,
+           "launches_per_frame": tm["kernel_launches"]}
+    if field_host is not None:
+        rec["vs_fp64"] = fp64_crops(s, field_host, {"learned_form": img, "network_only": net_img,
+                                                    "exact": exact_img}, crop, crop_stride, crops, threads)
+        rec["target_met"] = bool(rec["speedup_vs_exact"] >= 3.0 and rec["vs_fp64"]["learned_form"]["psnr_db"] >= 45.0)
+    return rec, total_ms, clocks, tm, tn
+
+
 def run_form(args):
     import torch
     import torch.distributed as dist
@@ -549,29 +675,17 @@ def run_form(args):
             extra["precision"]["vs_fp64"] = fp64_crops(s, fd.cpu().numpy(), {"precision": img, "exact_f32": exact_img},
                                                        args.crop, args.crop_stride, args.crops, threads)
     else:  # mlp
-        rep = r.mlp_train(B.mlp_options(samples_log2=args.mlp_samples_log2, n_lights=args.mlp_lights,
-                                        epochs=args.mlp_epochs, scene_light=int(args.mlp_scene_light)))
-        opts = dict(knot=args.knot, probe_fraction=args.probe_fraction, fallback_tol=args.fallback_tol)
-        # the network alone (no probes): its kernel time for the tensor roofline and its image
-        r.set_form(B.FORM_MLP, B.mlp_options(**dict(opts, probe_fraction=0.0)))
-        r.render(cam, out=out, timings=True)
-        _, tn = r.render(cam, out=out, timings=True)
-        net_img = out.cpu().numpy()
-        r.set_form(B.FORM_MLP, B.mlp_options(**opts))
-        _, tm = r.render(cam, out=out, timings=True)
-        img = out.cpu().numpy()
+        rec, total_ms, clocks, tm, tn = learned_record(
+            B, r, s, cam, out, exact_img, exact_ms, stream, world, local, lights=args.mlp_lights,
+            scene_light=args.mlp_scene_light, knot=args.knot, probe_fraction=args.probe_fraction,
+            fallback_tol=args.fallback_tol, samples_log2=args.mlp_samples_log2, epochs=args.mlp_epochs,
+            steps=args.steps, warmup=args.warmup,
+            field_host=None if (args.no_quality or rank != 0) else fd.cpu().numpy(), crops=args.crops,
+            crop=args.crop, crop_stride=args.crop_stride, threads=threads)
         launches = tm["kernel_launches"]
-        frame = lambda: r.render(cam, out=out, timings=False)  # noqa: E731  network + probes + fallback
-        total_ms, clocks = time_frames(frame, args.steps, args.warmup, stream, world, local)
-        tpeak, tsrc = measured_tensor_peak()
-        flops = tn["mlp_samples"] * MLP_FLOP_PER_EVAL
-        ach = flops / (tn["view_march_ms"] / 1e3) / 1e12
-        roofline = {"bound": "tensor", "kernel": "k_view_march_mlp", "achieved": ach, "peak": tpeak,
-                    "unit": "TFLOP/s", "frac": ach / tpeak, "peak_source": tsrc, "traffic": None,
-                    "flops_model": f"{MLP_FLOP_PER_EVAL} FLOP per network evaluation",
-                    "evaluations": tn["mlp_samples"], "kernel_ms": tn["view_march_ms"]}
+        roofline = dict(rec["roofline"], traffic=None)
         dtype = "bf16"
-        ntiles = -(-s.width // 32) * -(-s.height // 32)
+        tpeak = roofline["peak"]
         # the tcgen05 forward kernel on 2^22 device-resident rows (training's forward pass)
         nrow = 1 << 22
         X = torch.empty((nrow, 112), device="cuda").uniform_(-1, 1).to(torch.bfloat16)
@@ -580,25 +694,10 @@ def run_form(args):
         tc_ms /= 10
         tc_tflops = nrow * MLP_FLOP_PER_EVAL / (tc_ms / 1e3) / 1e12
         del X, Tt
-        extra["learned"] = {"train": {k: rep[k] for k in ("datagen_ms", "train_ms", "holdout_rmse", "unlit_rmse",
-                                                           "mean_rmse", "steps", "samples")},
-                            "lights": args.mlp_lights, "scene_light": bool(args.mlp_scene_light),
-                            "knot": args.knot, "probe_fraction": args.probe_fraction,
-                            "fallback_tol": args.fallback_tol,
-                            "fallback_tiles": tm["fallback_tiles"], "tiles": ntiles,
-                            "network_evaluations": tm["mlp_samples"],
-                            "exact_ms_per_frame": exact_ms,
-                            "speedup_vs_exact": exact_ms / (total_ms / args.steps),
-                            "network_only_ms": tn["total_ms"],
-                            "tcgen05_forward": {"rows": nrow, "ms": tc_ms, "tflops": tc_tflops,
-                                                "frac_of_bf16_peak": tc_tflops / tpeak,
-                                                "note": "dense forward kernel (TMEM accumulators), training's forward"},
-                            "psnr_vs_exact_map_full_frame": psnr(img, exact_img),
-                            "network_only_psnr_vs_exact_map": psnr(net_img, exact_img)}
-        if not args.no_quality and rank == 0:
-            extra["learned"]["vs_fp64"] = fp64_crops(s, fd.cpu().numpy(), {"learned_form": img, "network_only": net_img,
-                                                                            "exact": exact_img},
-                                                     args.crop, args.crop_stride, args.crops, threads)
+        rec["tcgen05_forward"] = {"rows": nrow, "ms": tc_ms, "tflops": tc_tflops,
+                                  "frac_of_bf16_peak": tc_tflops / tpeak,
+                                  "note": "dense forward kernel (TMEM accumulators), training's forward"}
+        extra["learned"] = rec
     if roofline.get("peak") is None:
         peak, src = measured_peaks()
         roofline.update(peak=peak, frac=roofline["achieved"] / peak, peak_source=src)
@@ -862,6 +961,130 @@ def run_bricks(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# --profile-case: fixed small cases for profiling one kernel at a time (ncu -k):
+#   light_march      K1, 512^3 noise, M = 256
+#   view_march       K2, 512^3 noise, 1024^2, map cached
+#   mlp_view         learned-form view march, 1024^2
+#   mlp_frame        learned form frame: scene-light network, 1% probes
+#   mlp_tc           tcgen05 forward, 2^21 rows
+#   batch            16-request persistent batch (--split: map-build launch, then view launch)
+#   precision_light  precision-form K1, bf16 640^3
+#   precision_view   precision-form K2, bf16 640^3, 1024^2, map cached
+#   bricks           512^3 noise as 2x2x2 bricks: K1, K5, K2, K6
+# Each case sets up its scene, runs the target kernel --reps times and exits 0;
+# device memory stays within a few GB. The tuning is fixed (8^3 vertex bricks,
+# skipping as stated per case) so that the launch sequence is the same every run.
+# ---------------------------------------------------------------------------
+PROFILE_CASES = ["light_march", "view_march", "mlp_view", "mlp_frame", "mlp_tc", "batch", "precision_light",
+                 "precision_view", "bricks"]
+
+
+def run_profile_case(a):
+    import numpy as np
+    import torch
+
+    from pilot_b200 import beams as B
+    from pilot_b200 import scenes
+
+    torch.cuda.set_device(0)
+    if a.profile_case in ("light_march", "view_march", "mlp_view", "mlp_frame"):
+        s = scenes.config1()
+        fd = s.field_device()
+        r = B.Renderer(0)
+        r.set_volume(fd, origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+        s.configure(r)
+        r.set_tuning(light_brick=8, empty_skip=False, view_skip=False)
+        cam = s.camera()
+        out = torch.empty((s.height, s.width, 4), device="cuda")
+        if a.profile_case == "light_march":
+            for _ in range(a.reps):
+                r.build_shadow_map(timings=False)
+        elif a.profile_case == "view_march":
+            r.build_shadow_map(timings=False)
+            r.set_reuse_shadow_map(True)
+            for _ in range(a.reps):
+                r.render(cam, out=out, timings=False)
+        elif a.profile_case == "mlp_frame":
+            # the learned form as benchmarked: network trained for the scene's light, knot 32, 1% probes
+            r.mlp_train(B.mlp_options(n_lights=1, scene_light=1))
+            r.set_form(B.FORM_MLP, B.mlp_options(knot=32, probe_fraction=0.01))
+            for _ in range(a.reps):
+                r.render(cam, out=out, timings=False)
+        else:
+            r.mlp_train(B.mlp_options(samples_log2=18, epochs=1, batch=16384))
+            r.set_form(B.FORM_MLP, B.mlp_options(knot=4, probe_fraction=0.0))
+            for _ in range(a.reps):
+                r.render(cam, out=out, timings=False)
+    elif a.profile_case == "mlp_tc":
+        # the tcgen05 forward on 2^21 rows of device-resident features
+        s = scenes.small(5, n=32, image=16, m=8)
+        r = B.Renderer(0)
+        r.set_volume(s.field_numpy(), origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+        s.configure(r)
+        rng = np.random.default_rng(1)
+        r.mlp_set_params(rng.normal(0, 0.1, B.lib().beams_mlp_param_count()).astype(np.float32))
+        n = 1 << 21
+        X = torch.empty((n, 112), device="cuda").uniform_(-1, 1).to(torch.bfloat16)
+        T = torch.empty(n, device="cuda")
+        for _ in range(a.reps):
+            r.mlp_forward_tc_device(X, T)
+    elif a.profile_case in ("precision_light", "precision_view"):
+        s = scenes.config2(n=640, image=1024, m=320)
+        fd = s.field_device()
+        r = B.Renderer(0)
+        r.set_volume(fd, origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+        s.configure(r)
+        r.set_form(B.FORM_PRECISION, B.BF16)
+        r.set_tuning(light_brick=8, empty_skip=True, view_skip=True)
+        if a.profile_case == "precision_light":
+            for _ in range(a.reps):
+                r.build_shadow_map(timings=False)
+        else:
+            r.build_shadow_map(timings=False)
+            r.set_reuse_shadow_map(True)
+            out = torch.empty((s.height, s.width, 4), device="cuda")
+            for _ in range(a.reps):
+                r.render(s.camera(), out=out, timings=False)
+    elif a.profile_case == "bricks":
+        s = scenes.config1()
+        fd = s.field_device()
+        cells = s.dims[0] - 1
+        edges = [round(i * cells / 2) for i in range(3)]
+        h = s.spacing
+        bricks = []  # 2x2x2; neighbours share their face plane
+        for z0, z1 in zip(edges[:-1], edges[1:]):
+            for y0, y1 in zip(edges[:-1], edges[1:]):
+                for x0, x1 in zip(edges[:-1], edges[1:]):
+                    org = (s.origin[0] + x0 * h[0], s.origin[1] + y0 * h[1], s.origin[2] + z0 * h[2])
+                    bricks.append((fd[z0:z1 + 1, y0:y1 + 1, x0:x1 + 1].contiguous(), org, h, s.value_range))
+        del fd
+        r = B.Renderer(0)
+        r.set_bricks(bricks)
+        s.configure(r)
+        r.set_shadow_map_size(s.map_m // 2)
+        cam = s.camera()
+        out = torch.empty((s.height, s.width, 4), device="cuda")
+        for _ in range(a.reps):
+            r.render(cam, out=out, timings=False)
+    else:  # batch
+        vols = batch_volumes()
+        rng = np.random.default_rng(11)
+        n = 16
+        sizes = [int(rng.choice(BATCH_IMAGES)) for _ in range(n)]
+        outs = [torch.empty((w, w, 4), device="cuda") for w in sizes]
+        r = B.Renderer(0)
+        r.set_color_map(scenes.tf_table())
+        r.batch_set_volumes([(f, sc.origin, sc.spacing, sc.value_range) for sc, f in vols])
+        r.set_batch_options(tile_w=32, tile_h=32, light_brick=8, skip=True, split=a.split)
+        reqs = batch_requests(B, vols, rng, n, outs)
+        for _ in range(a.reps):
+            r.render_batch(reqs, timings=False)
+    torch.cuda.synchronize()
+    print(f"profile case {a.profile_case}: ok")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -884,10 +1107,20 @@ def main():
     ap.add_argument("--crop", type=int, default=128)
     ap.add_argument("--crop-stride", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="default line: skip the learned-form records")
+    ap.add_argument("--learned-knot", type=int, default=32, help="default line: knot of the learned-form records")
     ap.add_argument("--no-autotune", action="store_true", help="fixed tuning (for launch lists under ncu)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work for cpu_baseline")
+    ap.add_argument("--no-full-frame", action="store_true",
+                    help="CPU legs: skip the whole-frame oracle run that checks the sample's extrapolation")
+    ap.add_argument("--profile-case", default=None, choices=PROFILE_CASES,
+                    help="run one fixed small case for a kernel profile (see PROFILE_CASES) and exit")
+    ap.add_argument("--reps", type=int, default=3, help="--profile-case: repetitions of the target kernel")
+    ap.add_argument("--split", action="store_true", help="--profile-case batch: split launch plan")
     args = ap.parse_args()
+    if args.profile_case:
+        return run_profile_case(args)
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up frames
     if args.config is None:
         args.config = 2 if args.form == "precision" else 1

@@ -608,6 +608,30 @@ def learned_record(B, r, s, cam, out, exact_img, exact_ms, stream, world, local,
            "psnr_vs_exact_map_full_frame": psnr(img, exact_img),
            "network_only_psnr_vs_exact_map": psnr(net_img, exact_img), "clocks": clocks,
            "launches_per_frame": tm["kernel_launches"]}
+    # per-tile probe errors of the last frame: max |dRGBA| over each 32x32 tile's
+    # probes against the exact light march (the fallback decision), as a histogram
+    if probe_fraction > 0:
+        P = max(1, int(round(1.0 / np.sqrt(min(probe_fraction, 1.0)))))
+        off = P // 2
+        nqx = (s.width - off - 1) // P + 1 if s.width > off else 0
+        nqy = (s.height - off - 1) // P + 1 if s.height > off else 0
+        if nqx * nqy > 0:
+            perr = r.mlp_probe_errors(nqx * nqy).reshape(nqy, nqx)
+            tx, ty = -(-s.width // 32), -(-s.height // 32)
+            tmax = np.full((ty, tx), np.inf)
+            seen = np.zeros((ty, tx), bool)
+            for j in range(nqy):
+                for i in range(nqx):
+                    y, x = j * P + off, i * P + off
+                    t0 = tmax[y // 32, x // 32]
+                    tmax[y // 32, x // 32] = perr[j, i] if not seen[y // 32, x // 32] else max(t0, perr[j, i])
+                    seen[y // 32, x // 32] = True
+            edges = [0.0, 1e-3, 3e-3, 1e-2, 3e-2, 1e-1, 3e-1, np.inf]
+            hist, _ = np.histogram(np.where(np.isfinite(tmax), tmax, 1e30), bins=edges)
+            rec["tile_probe_error_histogram"] = {"edges": [str(e) for e in edges], "tiles": hist.tolist(),
+                                                 "median": float(np.median(tmax)),
+                                                 "note": "per 32x32 tile: max |dRGBA| of its probe pixels against "
+                                                         "the exact light march; above fallback_tol falls back"}
     if field_host is not None:
         rec["vs_fp64"] = fp64_crops(s, field_host, {"learned_form": img, "network_only": net_img,
                                                     "exact": exact_img}, crop, crop_stride, crops, threads)

@@ -1250,8 +1250,8 @@ beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgb
     t->mlp_samples = c.mlp_samples;
     t->mlp_rows = c.mlp_rows;
     t->fallback_tiles = (int)c.fallback_tiles;
-    if (use_mlp && c.fallback_tiles) built = true;  // the fallback's gated map build ran
-    t->map_vertices = built ? (int)((size_t)g.pd[0] * g.pd[1] * g.pd[2]) : 0;
+    // the learned form's fallback builds only the vertices its failing tiles read
+    t->map_vertices = use_mlp ? (int)c.map_vertices : (built ? (int)((size_t)g.pd[0] * g.pd[1] * g.pd[2]) : 0);
     t->kernel_launches = launches;
   } else if (out_on_device == BEAMS_OUT_HOST) {
     // The caller reads rgba_out on return.

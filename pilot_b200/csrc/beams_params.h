@@ -106,6 +106,7 @@ struct Counters {
   unsigned int tiles_light;   // persistent-block work counters (zeroed per frame)
   unsigned int tiles_view;
   unsigned long long mlp_rows;  // network rows computed (idle lanes included)
+  unsigned long long map_vertices;  // vertices a masked (lazy) light march built
 };
 
 }  // namespace beams

@@ -42,8 +42,17 @@ __device__ __forceinline__ void load_tables(float4* s_tab, const float4* __restr
 // STITCH: the multi-brick Phase 3 — the march starts from the cross-brick
 // prefix (stitch_prefix) instead of zero, as GenerateEstimator is re-run on
 // the prefix opacities (LightedVolumeRenderer.cxx:1241-1252).
+// Blocks per SM: 6 (40 registers) for the plain exact march, which then issues
+// one sample at a time (config 1: 2.70 ms against 2.78 ms at 4 blocks); the
+// skipping, precision, stitching and rectilinear marches keep 4 (at 6 they
+// spill: the 640^3 precision build went 6.4 -> 9.5 ms).
+template <bool STITCH, bool PREC, bool SKIP, bool RECT>
+constexpr int k1_blocks_per_sm() {
+  return (STITCH || PREC || SKIP || RECT) ? 4 : 6;
+}
+
 template <typename QuadT, bool STITCH, bool PREC, bool SKIP, bool RECT = false>
-__global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, const QuadT* __restrict__ quads,
+__global__ void __launch_bounds__(kThreads, k1_blocks_per_sm<STITCH, PREC, SKIP, RECT>()) k_light_march(const ExactGeo g, const QuadT* __restrict__ quads,
                                                           const float4* __restrict__ tab,
                                                           const float4* __restrict__ tf,
                                                           const float* __restrict__ tau,
@@ -51,8 +60,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
                                                           Counters* __restrict__ cnt,
                                                           const BrickRef* __restrict__ refs, int nrefs,
                                                           int self, const unsigned* __restrict__ gate,
-                                                          const unsigned char* __restrict__ occ) {
-  // gate: the learned form's fallback builds the map only when a tile failed its probes
+                                                          const unsigned char* __restrict__ occ,
+                                                          const unsigned char* __restrict__ vmask) {
+  // gate: the learned form's fallback builds the map only when a tile failed its
+  // probes, and (vmask) only the vertices the failing tiles' view rays read
   if (gate && *gate == 0u) return;
   extern __shared__ float4 s_dyn[];
   const int nfield = g.max_off[0];             // field-axis table entries only
@@ -83,7 +94,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
     const int b0 = g.light_brick_log2;
     return b0 ? (s_bo[0] * s_bo[1] * s_bo[2]) << (3 * b0 - 5) : (nvert + 31) >> 5;
   }();
-  unsigned ns = 0;
+  unsigned ns = 0, built = 0;
 
   for (int tile = next_warp_tile(&cnt->tiles_light); tile < ntiles; tile = next_warp_tile(&cnt->tiles_light)) {
     int id;
@@ -108,6 +119,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
       if (id >= nvert) continue;
       map_vertex(g, id, V);
     }
+    if (vmask && !vmask[id]) continue;
+    ++built;
     light_origin(g, V, L);
     Accum<PREC> acc;
     march_vertex<QuadT, PREC, SKIP, RECT>(g, quads, T0, T1, T2, s_a, s_tau, occ, V, L,
@@ -118,6 +131,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_light_march(const ExactGeo g, c
     acc.store(map, id);
   }
   warp_add(&cnt->light_samples, ns);
+  if (vmask) warp_add(&cnt->map_vertices, built);
 }
 
 // ---------------------------------------------------------------------------
@@ -384,7 +398,7 @@ template <typename QuadT, bool STITCH, bool PREC>
 static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4* tab, const float4* tf,
                              const float* tau, void* map, Counters* cnt, cudaStream_t st, const BrickRef* refs,
                              int nrefs, int self, const unsigned* gate = nullptr,
-                             const unsigned char* occ = nullptr) {
+                             const unsigned char* occ = nullptr, const unsigned char* vmask = nullptr) {
   const int nvert = g.pd[0] * g.pd[1] * g.pd[2];
   const size_t smem = (size_t)g.max_off[0] * sizeof(float4) + 2 * (size_t)g.tf_n * sizeof(float);
   const int ntiles = (nvert + kThreads - 1) / kThreads;
@@ -401,7 +415,7 @@ static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4*
       e = persistent_grid(k_light_march<float4, false, false, false, true>, smem, ntiles, grid);
       if (e != cudaSuccess) return e;
       k_light_march<float4, false, false, false, true><<<grid, kThreads, smem, st>>>(
-          g, (const float4*)quads, tab, tf, tau, map, nvert, cnt, refs, nrefs, self, gate, nullptr);
+          g, (const float4*)quads, tab, tf, tau, map, nvert, cnt, refs, nrefs, self, gate, nullptr, vmask);
       return cudaGetLastError();
     } else {
       return cudaErrorInvalidValue;
@@ -411,23 +425,26 @@ static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4*
     e = persistent_grid(k_light_march<QuadT, STITCH, PREC, true>, smem, ntiles, grid);
     if (e != cudaSuccess) return e;
     k_light_march<QuadT, STITCH, PREC, true><<<grid, kThreads, smem, st>>>(g, (const QuadT*)quads, tab, tf, tau, map,
-                                                                           nvert, cnt, refs, nrefs, self, gate, occ);
+                                                                           nvert, cnt, refs, nrefs, self, gate, occ,
+                                                                           vmask);
   } else {
     e = persistent_grid(k_light_march<QuadT, STITCH, PREC, false>, smem, ntiles, grid);
     if (e != cudaSuccess) return e;
     k_light_march<QuadT, STITCH, PREC, false><<<grid, kThreads, smem, st>>>(g, (const QuadT*)quads, tab, tf, tau,
                                                                             map, nvert, cnt, refs, nrefs, self, gate,
-                                                                            nullptr);
+                                                                            nullptr, vmask);
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    float* map, Counters* cnt, cudaStream_t st, const BrickRef* refs, int nrefs,
-                                   int self, const unsigned* gate, const unsigned char* occ) {
+                                   int self, const unsigned* gate, const unsigned char* occ,
+                                   const unsigned char* vmask) {
   if (refs)
-    return launch_k1<float4, true, false>(g, quads, tab, tf, nullptr, map, cnt, st, refs, nrefs, self, gate, occ);
-  return launch_k1<float4, false, false>(g, quads, tab, tf, nullptr, map, cnt, st, nullptr, 0, -1, gate, occ);
+    return launch_k1<float4, true, false>(g, quads, tab, tf, nullptr, map, cnt, st, refs, nrefs, self, gate, occ,
+                                          vmask);
+  return launch_k1<float4, false, false>(g, quads, tab, tf, nullptr, map, cnt, st, nullptr, 0, -1, gate, occ, vmask);
 }
 
 cudaError_t launch_light_march_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,

@@ -1,28 +1,47 @@
-// k_mlp_tc.cu — the transmittance network's forward pass on the 5th-generation
-// tensor cores (tcgen05): a dense GEMM chain over 128-row tiles.
+// k_mlp_tc.cu — the transmittance network on the 5th-generation tensor cores
+// (tcgen05): a dense forward pass, and the training step (forward, loss,
+// backward, gradient accumulation) fused into one kernel.
 //
-// One CTA of 128 threads owns a 128 x 64 float32 accumulator in tensor memory
-// (TMEM, 64 columns allocated once per CTA). Per tile:
-//   1. each thread writes its row's 112 bfloat16 features into shared memory in
-//      the canonical K-major no-swizzle layout (8-row x 16-byte core matrices);
-//   2. one thread issues the layer's tcgen05.mma (M = 128, N = 64, K = 16 per
-//      instruction, A and B from shared memory, D in TMEM) and commits them to
-//      an mbarrier; everyone waits on it (bounded);
-//   3. each warp reads its 32 TMEM lanes (= its 32 rows) with tcgen05.ld, adds
-//      the bias, applies ReLU, rounds to bfloat16 and writes the row back to
-//      shared memory as the next layer's A (and, for training, to global memory);
-//   4. after the 4th hidden layer the head (64-wide dot product, sigmoid) runs
-//      on the CUDA cores.
-// The weights stay in shared memory (bfloat16, the same layout, as B = W^T:
-// K-major N x K) for all tiles. Numerics as the CUDA-core kernels: bfloat16
-// operands, float32 accumulation (in the tensor core's order).
+// Operand layout in shared memory ("chunked"): an R-row x K-column bfloat16
+// matrix is stored as K/8 chunks; chunk j holds columns 8j..8j+7 of every row,
+// row r at j*R*16 + r*16 (16 bytes per row). One buffer serves three ways:
+//  * K-major operand (rows = M or N, reduction over the columns): core
+//    matrices are 8 rows x 16 bytes; the leading byte offset (next 8 columns,
+//    the K direction) is R*16, the stride byte offset (next 8 rows) is 128, and
+//    each 16-wide K slice starts 2*R*16 bytes further;
+//  * MN-major operand (rows = K, columns = M or N): the same core matrices
+//    read transposed; the stride byte offset (next 8 columns, the MN
+//    direction) is R*16, the leading byte offset (next 8 rows, the K
+//    direction) is 128, and each 16-row K slice starts 256 bytes further.
+// Both are the SWIZZLE_NONE canonical layouts of the tcgen05 shared-memory
+// descriptor (version 1). A TMA tiled load of a box {8 columns, 128 rows}
+// lands exactly as one chunk, so input tiles arrive in place.
 //
-// Shared-memory layout of an R-row, K-column bfloat16 operand (R = 128 for A,
-// 64 for B): K is cut into 16-wide slices; slice s occupies R * 32 bytes at
-// s * R * 32; inside it, element (r, k) sits at (r / 8) * 256 + ((k % 16) / 8)
-// * 128 + (r % 8) * 16 + (k % 8) * 2. The descriptor of slice s: start =
-// base + s * R * 32, leading byte offset 128 (the two 8-wide K halves), stride
-// byte offset 256 (consecutive 8-row groups), layout SWIZZLE_NONE, version 1.
+// Forward (k_mlp_fwd_tc, 256 threads, two CTAs per SM): 128-row tiles of
+// precomputed features are loaded by TMA into a double buffer (the next tile's
+// load runs under the current tile's layers); one thread issues each layer's
+// tcgen05.mma (M 128, N 64, K 16 per instruction, float32 accumulator in TMEM)
+// and commits to an mbarrier; eight warps read the accumulator back with
+// tcgen05.ld (warp w: TMEM lanes 32(w%4).. = its rows, columns 32(w/4)..),
+// add the bias, apply ReLU, round to bfloat16 and write the next layer's
+// operand over the input tile, which the first layer has finished reading.
+//
+// Training (k_mlp_train_tc, 256 threads, one CTA per SM): per tile the forward
+// keeps every layer's activations in shared memory, the head computes T, the
+// loss and dz = scale 2 (T - t) T (1 - T), and the backward runs on the tensor
+// cores: per layer l, the weight gradient G_W_l += in_l^T dY_l (MN-major A and
+// B: M = the layer's inputs padded to 128, N 64, K = the tile's 128 rows) into
+// a TMEM accumulator that lives across all the CTA's tiles, and the data
+// gradient dY_{l-1} = (dY_l W_l^T) * (in_l > 0) (K-major A, MN-major B).
+// Bias and head gradients are column sums on the CUDA cores. At the end the
+// accumulators are added to the float32 gradient vector.
+//
+// Numerics as the CUDA-core kernels of k_mlp_train.cu: bfloat16 weights and
+// activations at every product, float32 accumulation; the backward rounds dY
+// to bfloat16 where it enters a product. Every mbarrier wait is bounded: a
+// uniform timeout decision (BEAMS_ERR_TIMEOUT on the host), TMEM freed and
+// copies in flight waited for on every path.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -36,48 +55,50 @@ namespace beams {
 namespace mlp {
 namespace {
 
-constexpr int kTile = 128;                          // rows per tile (tcgen05 M)
-constexpr int kTcThreads = 128;                     // one thread per row
-constexpr int kA_bytes = kTile * kIn * 2;           // 28672
-constexpr int kB1_bytes = kHid * kIn * 2;           // 14336
-constexpr int kBh_bytes = kHid * kHid * 2;          // 8192
-constexpr int kOffB1 = kA_bytes;
-constexpr int kOffB2 = kOffB1 + kB1_bytes;
-constexpr int kOffAux = kOffB2 + 3 * kBh_bytes;     // 67584: biases (4 x 64), w5 (64), b5
-constexpr int kAuxFloats = 4 * kHid + kHid + 1;
-constexpr int kOffBar = ((kOffAux + kAuxFloats * 4 + 15) / 16) * 16;
-constexpr int kSmemTc = kOffBar + 16;
-constexpr unsigned kWaitLimit = 1u << 24;           // mbarrier polls before giving up
+constexpr int kTile = 128;                  // rows per tile (tcgen05 M)
+constexpr int kThreads = 256;               // eight warps: two per TMEM lane quarter
+constexpr unsigned kWaitLimit = 1u << 24;   // mbarrier polls before giving up
+constexpr int kXBytes = kTile * kIn * 2;    // 28672: one input tile
+constexpr int kHBytes = kTile * kHid * 2;   // 16384: one activation tile
+constexpr int kW1Bytes = kHid * kIn * 2;    // 14336
+constexpr int kWhBytes = kHid * kHid * 2;   // 8192
+constexpr int kWBytes = kW1Bytes + 3 * kWhBytes;  // 38912: all four weight matrices
 
-// Offset (bytes) of element (r, k) in an R-row operand.
-__host__ __device__ constexpr int op_off(int R, int r, int k) {
-  return (k >> 4) * R * 32 + (r >> 3) * 256 + ((k >> 3) & 1) * 128 + (r & 7) * 16 + (k & 7) * 2;
+// byte offset of element (r, k) of an R-row chunked operand
+__host__ __device__ constexpr int ch_off(int R, int r, int k) { return (k >> 3) * R * 16 + r * 16 + (k & 7) * 2; }
+
+// Instruction descriptor, kind::f16: D float32, A and B bfloat16, M x N, each
+// operand K-major (0) or MN-major (1).
+__host__ __device__ constexpr uint32_t idesc(int M, int N, int a_mn, int b_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+constexpr uint32_t kIdFwd = idesc(kTile, kHid, 0, 0);    // activations x W^T
+constexpr uint32_t kIdWgrad = idesc(kTile, kHid, 1, 1);  // in^T x dY
+constexpr uint32_t kIdDgrad = idesc(kTile, kHid, 0, 1);  // dY x W
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// The dynamic shared memory rounded up to a 1024-byte boundary (launches ask
+// for 1024 bytes more than the layout needs): TMA destinations and operand
+// descriptors then sit on known alignments.
+__device__ __forceinline__ unsigned char* aligned_smem(unsigned char* raw) {
+  const uint32_t a = smem_addr(raw);
+  return raw + (((a + 1023u) & ~1023u) - a);
 }
 
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
+// Shared-memory matrix descriptor, SWIZZLE_NONE, version 1 (tcgen05).
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+         ((uint64_t)1 << 46);
 }
 
-// Shared-memory matrix descriptor (no swizzle, K-major, LBO 128 B, SBO 256 B).
-__device__ __forceinline__ uint64_t op_desc(uint32_t addr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((addr & 0x3FFFFu) >> 4);          // start address, bits [0, 14)
-  d |= (uint64_t)(128u >> 4) << 16;                 // leading byte offset, bits [16, 30)
-  d |= (uint64_t)(256u >> 4) << 32;                 // stride byte offset, bits [32, 46)
-  d |= (uint64_t)1 << 46;                           // version 1 (tcgen05)
-  return d;                                         // base offset 0, lbo mode 0, SWIZZLE_NONE
-}
-
-// Instruction descriptor: D float32, A and B bfloat16, both K-major, N = 64, M = 128.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kHid >> 3) << 17) |
-                            ((uint32_t)(kTile >> 4) << 24);
-
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
-      "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      "l"(a), "l"(b), "r"(id), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
@@ -89,8 +110,12 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
 }
 
-// Waits for the phase to complete; false if the poll budget ran out.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, unsigned phase) {
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// Waits for the phase with the given parity to complete; false if the poll budget ran out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, unsigned parity) {
   for (unsigned i = 0; i < kWaitLimit; ++i) {
     uint32_t done;
     asm volatile(
@@ -98,11 +123,27 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, unsigned phase) {
         "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}\n"
         : "=r"(done)
-        : "r"(bar), "r"(phase)
+        : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
   }
   return false;
+}
+
+// TMA: box {8 columns, 128 rows} of the feature matrix at (col, row) into one chunk.
+__device__ __forceinline__ void tma_load_chunk(uint32_t dst, const CUtensorMap* map, int col, int row, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(map), "r"(col), "r"(row), "r"(bar)
+      : "memory");
+}
+
+// One input tile: 14 chunk loads completing on bar (expect_tx set first).
+__device__ __forceinline__ void tma_load_tile(uint32_t dst, const CUtensorMap* map, int row, uint32_t bar) {
+  mbar_expect_tx(bar, (uint32_t)kXBytes);
+#pragma unroll 1
+  for (int j = 0; j < kIn / 8; ++j) tma_load_chunk(dst + j * kTile * 16, map, j * 8, row, bar);
 }
 
 __device__ __forceinline__ void tmem_ld16(uint32_t addr, float v[16]) {
@@ -122,198 +163,504 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// Row input: precomputed features (training, tests) or positions to encode (rendering).
-struct RowsFromFeatures {
-  const __nv_bfloat16* X;  // n x 112
-  __device__ __forceinline__ void load(int row, unsigned char* A, int r) const {
-    const uint4* src = reinterpret_cast<const uint4*>(X + (size_t)row * kIn);
-#pragma unroll
-    for (int c = 0; c < kIn / 8; ++c) *reinterpret_cast<uint4*>(A + op_off(kTile, r, c * 8)) = src[c];
-  }
-};
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t cols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(slot)), "r"(cols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t base, uint32_t cols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(cols) : "memory");
+}
 
-struct RowsFromPositions {
-  const float4* pos;       // n x {x, y, z, -}
-  Encoding enc;
-  float lf[3];
-  __device__ __forceinline__ void load(int row, unsigned char* A, int r) const {
-    const float4 q = pos[row];
-    const float p[3] = {q.x, q.y, q.z};
-    float u[3];
-    normalised(enc, p, u);
-#pragma unroll 1
-    for (int c = 0; c < kIn; c += 8) {
-      uint32_t w[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        float a, b;
-        feature_pair(u, lf, c + 2 * j, a, b);
-        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-        w[j] = *reinterpret_cast<const uint32_t*>(&h);
-      }
-      *reinterpret_cast<uint4*>(A + op_off(kTile, r, c)) = make_uint4(w[0], w[1], w[2], w[3]);
-    }
-  }
-};
-
-template <typename Rows>
-__global__ void __launch_bounds__(kTcThreads) k_mlp_fwd_tc(Rows rows, int n, const float* __restrict__ P,
-                                                           __nv_bfloat16* __restrict__ H0,
-                                                           __nv_bfloat16* __restrict__ H1,
-                                                           __nv_bfloat16* __restrict__ H2,
-                                                           __nv_bfloat16* __restrict__ H3, float* __restrict__ T,
-                                                           unsigned* __restrict__ err) {
-  extern __shared__ __align__(1024) unsigned char sm[];
-  unsigned char* A = sm;
-  float* aux = reinterpret_cast<float*>(sm + kOffAux);
-  __shared__ uint32_t s_tmem;
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const uint32_t bar = smem_addr(sm + kOffBar);
-
-  // weights as B = W^T (N x K, K-major), bfloat16-rounded as every forward does
-  for (int i = tid; i < kIn * kHid; i += kTcThreads) {
-    const int k = i / kHid, nn = i - k * kHid;  // W1[k][n] at P[oW1 + k * 64 + n]
-    *reinterpret_cast<__nv_bfloat16*>(sm + kOffB1 + op_off(kHid, nn, k)) = __float2bfloat16_rn(P[oW1 + i]);
+// Stages the four weight matrices as bfloat16 B operands (W_l^T: N = 64
+// outputs as rows, chunked over the inputs) and the biases, bf16(w5), b5.
+__device__ void stage_weights(const float* __restrict__ P, unsigned char* W, float* aux) {
+  for (int i = threadIdx.x; i < kIn * kHid; i += blockDim.x) {
+    const int k = i / kHid, n = i - k * kHid;  // W1[k][n] at P[oW1 + k * 64 + n]
+    *reinterpret_cast<__nv_bfloat16*>(W + ch_off(kHid, n, k)) = __float2bfloat16_rn(P[oW1 + i]);
   }
   const int oW[3] = {oW2, oW3, oW4};
   for (int l = 0; l < 3; ++l)
-    for (int i = tid; i < kHid * kHid; i += kTcThreads) {
-      const int k = i / kHid, nn = i - k * kHid;
-      *reinterpret_cast<__nv_bfloat16*>(sm + kOffB2 + l * kBh_bytes + op_off(kHid, nn, k)) =
+    for (int i = threadIdx.x; i < kHid * kHid; i += blockDim.x) {
+      const int k = i / kHid, n = i - k * kHid;
+      *reinterpret_cast<__nv_bfloat16*>(W + kW1Bytes + l * kWhBytes + ch_off(kHid, n, k)) =
           __float2bfloat16_rn(P[oW[l] + i]);
     }
   const int oB[4] = {oB1, oB2, oB3, oB4};
-  for (int i = tid; i < 4 * kHid; i += kTcThreads) aux[i] = P[oB[i / kHid] + (i % kHid)];
-  for (int i = tid; i < kHid; i += kTcThreads) aux[4 * kHid + i] = bf16r(P[oW5 + i]);
+  for (int i = threadIdx.x; i < 4 * kHid; i += blockDim.x) aux[i] = P[oB[i / kHid] + (i % kHid)];
+  for (int i = threadIdx.x; i < kHid; i += blockDim.x) aux[4 * kHid + i] = bf16r(P[oW5 + i]);
+  if (threadIdx.x == 0) aux[5 * kHid] = P[oB5];
+}
+
+__device__ __forceinline__ uint32_t w_addr(uint32_t wbase, int l) {
+  return wbase + (l == 0 ? 0u : (uint32_t)(kW1Bytes + (l - 1) * kWhBytes));
+}
+
+// Layer l of the forward for one tile: A = the layer's input (chunked, 128
+// rows; 112 or 64 columns), B = W_l^T, D = the TMEM accumulator.
+__device__ __forceinline__ void issue_fwd(uint32_t d, uint32_t a, uint32_t wbase, int l) {
+  const int K = l == 0 ? kIn : kHid;
+  const uint32_t b = w_addr(wbase, l);
+  for (int s = 0; s < K / 16; ++s)
+    mma(d, sdesc(a + s * 2 * kTile * 16, kTile * 16, 128), sdesc(b + s * 2 * kHid * 16, kHid * 16, 128), kIdFwd,
+        s > 0 ? 1u : 0u);
+}
+
+// Epilogue of a hidden layer for the calling thread's row r and 32 columns
+// c0..c0+31: h = bf16(relu(acc + bias)), written as the chunked operand out.
+__device__ __forceinline__ void hidden_epilogue(uint32_t tmem_acc, const float* bias, int r, int c0, float h[32],
+                                                unsigned char* out) {
+  tmem_ld16(tmem_acc + c0, h);
+  tmem_ld16(tmem_acc + c0 + 16, h + 16);
+  tmem_wait_ld();
+#pragma unroll
+  for (int j = 0; j < 32; ++j) h[j] = bf16r(fmaxf(h[j] + bias[c0 + j], 0.f));
+  if (out) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      uint32_t w[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const __nv_bfloat162 b2 = __floats2bfloat162_rn(h[c * 8 + 2 * j], h[c * 8 + 2 * j + 1]);
+        w[j] = *reinterpret_cast<const uint32_t*>(&b2);
+      }
+      *reinterpret_cast<uint4*>(out + ch_off(kTile, r, c0 + c * 8)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  }
+}
+
+// Half of the head's dot product: sum over the thread's 32 columns of h * bf16(w5).
+__device__ __forceinline__ float head_partial(const float h[32], const float* w5, int c0) {
+  float p = 0.f;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) p = fmaf(h[j], w5[c0 + j], p);
+  return p;
+}
+
+// T from the two halves (the same expression in both kernels, so their T agree bit for bit).
+__device__ __forceinline__ float head_T(float b5, float p0, float p1) {
+  const float z = b5 + (p0 + p1);
+  return 1.f / (1.f + expf(-z));
+}
+
+// ---------------------------------------------------------------------------
+// dense forward
+// ---------------------------------------------------------------------------
+constexpr int kFwdOffW = 2 * kXBytes;                 // 57344
+constexpr int kFwdOffAux = kFwdOffW + kWBytes;        // 96256
+constexpr int kAuxFloats = 5 * kHid + 1 + 2 * kTile;  // biases, w5, b5, head halves
+constexpr int kFwdOffBar = ((kFwdOffAux + kAuxFloats * 4 + 15) / 16) * 16;
+constexpr int kFwdSmem = kFwdOffBar + 32;
+
+__global__ void __launch_bounds__(kThreads, 2) k_mlp_fwd_tc(const __grid_constant__ CUtensorMap xmap, int row0,
+                                                            int n, const float* __restrict__ P,
+                                                            float* __restrict__ T, unsigned* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  unsigned char* sm = aligned_smem(sm_raw);
+  float* aux = reinterpret_cast<float*>(sm + kFwdOffAux);
+  float* part = aux + 5 * kHid + 1;  // [2][kTile]
+  __shared__ uint32_t s_tmem;
+  const int tid = threadIdx.x, warp = tid >> 5, q = warp & 3, hf = warp >> 2;
+  const int r = q * 32 + (tid & 31), c0 = hf * 32;
+  const uint32_t xbase = smem_addr(sm), wbase = smem_addr(sm + kFwdOffW);
+  const uint32_t bar_load[2] = {smem_addr(sm + kFwdOffBar), smem_addr(sm + kFwdOffBar + 8)};
+  const uint32_t bar_mma = smem_addr(sm + kFwdOffBar + 16);
+  const int ntiles = (n + kTile - 1) / kTile;
+
+  stage_weights(P, sm + kFwdOffW, aux);
   if (tid == 0) {
-    aux[5 * kHid] = P[oB5];
-    mbar_init(bar, 1);
+    mbar_init(bar_load[0], 1);
+    mbar_init(bar_load[1], 1);
+    mbar_init(bar_mma, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
-                 "r"(64u)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
+  if (warp == 0) tmem_alloc(&s_tmem, 64u);
   fence_async_smem();  // the weights were written by ordinary stores
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
-  const uint32_t tmem_row = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's 32 lanes
-  unsigned phase = 0;
-  bool ok = true;
+  const uint32_t tmem_acc = tmem + ((uint32_t)(q * 32) << 16);
 
-  for (int tile = blockIdx.x; ok && tile * kTile < n; tile += gridDim.x) {
-    const int row = tile * kTile + tid;
-    if (row < n) {
-      rows.load(row, A, tid);
-    } else {
-#pragma unroll 1
-      for (int c = 0; c < kIn; c += 8) *reinterpret_cast<uint4*>(A + op_off(kTile, tid, c)) = make_uint4(0, 0, 0, 0);
+  int tile = blockIdx.x;
+  if (tid == 0 && tile < ntiles) tma_load_tile(xbase, &xmap, row0 + tile * kTile, bar_load[0]);
+  unsigned mphase = 0;
+  // loads issued and not yet waited for successfully, when leaving early:
+  // the current tile's (if its wait failed) and the next tile's prefetch
+  int it = 0;
+  bool cur_pending = false, next_pending = false;
+  bool ok = true;
+  for (; tile < ntiles; tile += gridDim.x, ++it) {
+    const int cur = it & 1;
+    const int next = tile + gridDim.x;
+    next_pending = next < ntiles;
+    if (next_pending && tid == 0)
+      tma_load_tile(xbase + (cur ^ 1) * kXBytes, &xmap, row0 + next * kTile, bar_load[cur ^ 1]);
+    ok = mbar_wait(bar_load[cur], (unsigned)(it >> 1) & 1u);
+    if (__syncthreads_or(!ok)) {
+      ok = false;
+      cur_pending = true;
+      break;
+    }
+    unsigned char* buf = sm + cur * kXBytes;
+    const uint32_t a = xbase + cur * kXBytes;
+    float h[32];
+    for (int l = 0; l < 4; ++l) {
+      if (tid == 0) {
+        tc_fence_after();
+        issue_fwd(tmem, a, wbase, l);
+        mma_commit(bar_mma);
+      }
+      ok = mbar_wait(bar_mma, mphase);
+      mphase ^= 1u;
+      if (__syncthreads_or(!ok)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      // layers 0-2 overwrite the tile's input (read only by layer 0) with their output
+      hidden_epilogue(tmem_acc, aux + l * kHid, r, c0, h, l < 3 ? buf : nullptr);
+      if (l == 3) part[hf * kTile + r] = head_partial(h, aux + 4 * kHid, c0);
+      fence_async_smem();
+      tc_fence_before();
+      __syncthreads();
+    }
+    if (!ok) break;
+    const int row = tile * kTile + r;
+    if (hf == 0 && row < n && T) T[row] = head_T(aux[5 * kHid], part[r], part[kTile + r]);
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1u);
+    // loads still in flight land in this CTA's shared memory: wait for them (bounded)
+    if (cur_pending) mbar_wait(bar_load[it & 1], (unsigned)(it >> 1) & 1u);
+    if (next_pending) mbar_wait(bar_load[(it + 1) & 1], (unsigned)((it + 1) >> 1) & 1u);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 64u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// fused training step
+// ---------------------------------------------------------------------------
+constexpr int kTrOffX = kWBytes;                       // 38912
+constexpr int kTrOffH = kTrOffX + kXBytes;             // 67584: H0..H3
+constexpr int kTrOffDY = kTrOffH + 4 * kHBytes;        // 133120
+constexpr int kTrOffAux = kTrOffDY + kHBytes;          // 149504
+constexpr int kTrAuxFloats = kAuxFloats + kTile;       // + dz per row
+constexpr int kTrOffBar = ((kTrOffAux + kTrAuxFloats * 4 + 15) / 16) * 16;
+constexpr int kTrSmem = kTrOffBar + 16;
+// TMEM columns: forward accumulator, data gradient, weight gradients of layers 0..3
+constexpr uint32_t kColFwd = 0, kColDg = 64, kColWg = 128;
+constexpr uint32_t kTrCols = 512;
+
+// The wgrad A operand (a layer's input, MN-major, M padded to 128) reads 16
+// column chunks = 32 KB from the buffer's start: X (14 chunks) runs into H0,
+// H0..H2 (8 chunks) into the next activation buffer. All inside the layout.
+static_assert(kTrOffX + 16 * kTile * 16 <= kTrOffDY, "wgrad A read of X stays inside shared memory");
+static_assert(kTrOffH + 2 * kHBytes + 16 * kTile * 16 <= kTrOffDY, "wgrad A read of H2 stays inside H3");
+
+__global__ void __launch_bounds__(kThreads, 1) k_mlp_train_tc(const __grid_constant__ CUtensorMap xmap, int row0,
+                                                              int n, const float* __restrict__ P,
+                                                              const float* __restrict__ target, float scale,
+                                                              float* __restrict__ G, float* __restrict__ T,
+                                                              float* __restrict__ loss, unsigned* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  unsigned char* sm = aligned_smem(sm_raw);
+  float* aux = reinterpret_cast<float*>(sm + kTrOffAux);
+  float* part = aux + 5 * kHid + 1;   // [2][kTile]
+  float* s_dz = part + 2 * kTile;     // [kTile]
+  __shared__ uint32_t s_tmem;
+  const int tid = threadIdx.x, warp = tid >> 5, q = warp & 3, hf = warp >> 2;
+  const int r = q * 32 + (tid & 31), c0 = hf * 32;
+  const uint32_t base = smem_addr(sm);
+  const uint32_t wbase = base, xaddr = base + kTrOffX, dyaddr = base + kTrOffDY;
+  const uint32_t bar_load = smem_addr(sm + kTrOffBar), bar_mma = bar_load + 8;
+  unsigned char* H[4] = {sm + kTrOffH, sm + kTrOffH + kHBytes, sm + kTrOffH + 2 * kHBytes, sm + kTrOffH + 3 * kHBytes};
+  unsigned char* DY = sm + kTrOffDY;
+  const int ntiles = (n + kTile - 1) / kTile;
+  const bool bwd = G != nullptr;
+
+  stage_weights(P, sm, aux);
+  if (tid == 0) {
+    mbar_init(bar_load, 1);
+    mbar_init(bar_mma, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) tmem_alloc(&s_tmem, kTrCols);
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  const uint32_t lanes = (uint32_t)(q * 32) << 16;
+
+  // per-thread partial sums: bias gradients of column cn over rows 32*(tid/64)..+31, head
+  const int cn = tid & (kHid - 1), rq = tid >> 6;
+  float gb[4] = {0.f, 0.f, 0.f, 0.f}, gw5 = 0.f, gb5 = 0.f, lsum = 0.f;
+  unsigned lphase = 0, mphase = 0;
+  int done_tiles = 0;
+  bool ok = true, load_pending = false;
+
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    if (tid == 0) tma_load_tile(xaddr, &xmap, row0 + tile * kTile, bar_load);
+    ok = mbar_wait(bar_load, lphase);
+    if (__syncthreads_or(!ok)) {
+      ok = false;
+      load_pending = true;
+      break;
+    }
+    lphase ^= 1u;
+    const int row = tile * kTile + r;
+    const bool valid = row < n;
+    float h[32];
+    // forward: layer l reads X or H[l-1], writes H[l]
+    for (int l = 0; l < 4 && ok; ++l) {
+      if (tid == 0) {
+        tc_fence_after();
+        issue_fwd(tmem + kColFwd, l == 0 ? xaddr : smem_addr(H[l - 1]), wbase, l);
+        mma_commit(bar_mma);
+      }
+      ok = mbar_wait(bar_mma, mphase);
+      mphase ^= 1u;
+      if (__syncthreads_or(!ok)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      hidden_epilogue(tmem + kColFwd + lanes, aux + l * kHid, r, c0, h, H[l]);
+      if (l == 3) part[hf * kTile + r] = head_partial(h, aux + 4 * kHid, c0);
+      fence_async_smem();
+      tc_fence_before();
+      __syncthreads();
+    }
+    if (!ok) break;
+    // head, loss, dz; then dY4 = dz * bf16(w5) * (h4 > 0) from the registers of layer 3
+    if (hf == 0) {
+      float dz = 0.f;
+      if (valid) {
+        const float t = head_T(aux[5 * kHid], part[r], part[kTile + r]);
+        if (T) T[row] = t;
+        if (target) {
+          const float d = t - target[row];
+          lsum += d * d;
+          dz = scale * 2.f * d * t * (1.f - t);
+        }
+      }
+      s_dz[r] = dz;
+    }
+    __syncthreads();
+    ++done_tiles;
+    if (!bwd) continue;
+    {
+      const float dz = s_dz[r];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int k = c * 8 + 2 * j;
+          const float a = h[k] > 0.f ? dz * aux[4 * kHid + c0 + k] : 0.f;
+          const float b = h[k + 1] > 0.f ? dz * aux[4 * kHid + c0 + k + 1] : 0.f;
+          const __nv_bfloat162 b2 = __floats2bfloat162_rn(a, b);
+          w[j] = *reinterpret_cast<const uint32_t*>(&b2);
+        }
+        *reinterpret_cast<uint4*>(DY + ch_off(kTile, r, c0 + c * 8)) = make_uint4(w[0], w[1], w[2], w[3]);
+      }
     }
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
-    for (int l = 0; l < 4; ++l) {
-      const int K = l == 0 ? kIn : kHid;
-      const uint32_t bbase = smem_addr(sm + (l == 0 ? kOffB1 : kOffB2 + (l - 1) * kBh_bytes));
+    // head gradients: G_w5[k] += sum_b dz[b] h4[b][k], G_b5 += sum_b dz[b]
+    for (int b = rq * 32; b < rq * 32 + 32; ++b)
+      gw5 = fmaf(s_dz[b], __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(H[3] + ch_off(kTile, b, cn))), gw5);
+    if (hf == 0) gb5 += s_dz[r];
+    // backward, layer l = 3..0: G_W_l += in_l^T dY_l; dY_{l-1} = (dY_l W_l^T) * (in_l > 0)
+    for (int l = 3; l >= 0 && ok; --l) {
+      const uint32_t in_addr = l == 0 ? xaddr : smem_addr(H[l - 1]);
       if (tid == 0) {
         tc_fence_after();
-        const uint32_t abase = smem_addr(A);
-        for (int s = 0; s < K / 16; ++s)
-          mma_bf16(tmem, op_desc(abase + s * kTile * 32), op_desc(bbase + s * kHid * 32), s > 0 ? 1u : 0u);
-        mma_commit(bar);
+        const uint32_t dwg = tmem + kColWg + 64u * (uint32_t)l;
+        for (int s = 0; s < kTile / 16; ++s)
+          mma(dwg, sdesc(in_addr + s * 256, 128, kTile * 16), sdesc(dyaddr + s * 256, 128, kTile * 16), kIdWgrad,
+              (done_tiles > 1 || s > 0) ? 1u : 0u);
+        if (l > 0) {
+          const uint32_t b = w_addr(wbase, l);
+          for (int s = 0; s < kHid / 16; ++s)
+            mma(tmem + kColDg, sdesc(dyaddr + s * 2 * kTile * 16, kTile * 16, 128),
+                sdesc(b + s * 256, 128, kHid * 16), kIdDgrad, s > 0 ? 1u : 0u);
+        }
+        mma_commit(bar_mma);
       }
-      const bool done = mbar_wait(bar, phase);
-      if (__syncthreads_or(!done)) {  // a uniform decision: every thread leaves together
+      // bias gradient of layer l: column sums of dY_l (read while the MMAs read it too)
+      {
+        float s = 0.f;
+        for (int b = rq * 32; b < rq * 32 + 32; ++b)
+          s += __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(DY + ch_off(kTile, b, cn)));
+        gb[l] += s;
+      }
+      ok = mbar_wait(bar_mma, mphase);
+      mphase ^= 1u;
+      if (__syncthreads_or(!ok)) {
         ok = false;
-        if (tid == 0) atomicExch(err, 1u);
         break;
       }
-      phase ^= 1u;
+      if (l == 0) break;
       tc_fence_after();
-      float h[kHid];
-#pragma unroll
-      for (int c = 0; c < kHid; c += 16) tmem_ld16(tmem_row + c, h + c);
+      float dx[32];
+      tmem_ld16(tmem + kColDg + lanes + c0, dx);
+      tmem_ld16(tmem + kColDg + lanes + c0 + 16, dx + 16);
       tmem_wait_ld();
-      const float* bias = aux + l * kHid;
+      const unsigned char* in = H[l - 1];
 #pragma unroll
-      for (int j = 0; j < kHid; ++j) h[j] = bf16r(fmaxf(h[j] + bias[j], 0.f));
-      __nv_bfloat16* Hout = l == 0 ? H0 : (l == 1 ? H1 : (l == 2 ? H2 : H3));
-      if (Hout && row < n) {
-        uint4* dst = reinterpret_cast<uint4*>(Hout + (size_t)row * kHid);
+      for (int c = 0; c < 4; ++c) {
+        const uint4 xv = *reinterpret_cast<const uint4*>(in + ch_off(kTile, r, c0 + c * 8));
+        const __nv_bfloat16* xb = reinterpret_cast<const __nv_bfloat16*>(&xv);
+        uint32_t w[4];
 #pragma unroll
-        for (int c = 0; c < kHid / 8; ++c) {
-          uint32_t w[4];
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const __nv_bfloat162 b2 = __floats2bfloat162_rn(h[c * 8 + 2 * j], h[c * 8 + 2 * j + 1]);
-            w[j] = *reinterpret_cast<const uint32_t*>(&b2);
-          }
-          dst[c] = make_uint4(w[0], w[1], w[2], w[3]);
+        for (int j = 0; j < 4; ++j) {
+          const int k = c * 8 + 2 * j;
+          const float a = __bfloat162float(xb[2 * j]) > 0.f ? dx[k] : 0.f;
+          const float b = __bfloat162float(xb[2 * j + 1]) > 0.f ? dx[k + 1] : 0.f;
+          const __nv_bfloat162 b2 = __floats2bfloat162_rn(a, b);
+          w[j] = *reinterpret_cast<const uint32_t*>(&b2);
         }
+        *reinterpret_cast<uint4*>(DY + ch_off(kTile, r, c0 + c * 8)) = make_uint4(w[0], w[1], w[2], w[3]);
       }
-      if (l < 3) {
-        // this row as the next layer's A (the MMAs that read A have completed)
-#pragma unroll
-        for (int c = 0; c < kHid / 8; ++c) {
-          uint32_t w[4];
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const __nv_bfloat162 b2 = __floats2bfloat162_rn(h[c * 8 + 2 * j], h[c * 8 + 2 * j + 1]);
-            w[j] = *reinterpret_cast<const uint32_t*>(&b2);
-          }
-          *reinterpret_cast<uint4*>(A + op_off(kTile, tid, c * 8)) = make_uint4(w[0], w[1], w[2], w[3]);
-        }
-        fence_async_smem();
-      } else if (T && row < n) {
-        float z = aux[5 * kHid];
-        for (int j = 0; j < kHid; ++j) z = fmaf(h[j], aux[4 * kHid + j], z);
-        T[row] = 1.f / (1.f + expf(-z));
-      }
+      fence_async_smem();
       tc_fence_before();
       __syncthreads();
     }
+    if (!ok) break;
   }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1u);
+    if (load_pending) mbar_wait(bar_load, lphase);  // the tile's load lands here: wait for it (bounded)
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  // flush: weight gradients from TMEM (row m of the layer-l accumulator = input m)
+  if (ok && bwd && done_tiles > 0) {
+    const int oW[4] = {oW1, oW2, oW3, oW4}, Ks[4] = {kIn, kHid, kHid, kHid}, oB[4] = {oB1, oB2, oB3, oB4};
+    for (int l = 0; l < 4; ++l) {
+      float v[32];
+      tmem_ld16(tmem + kColWg + 64u * (uint32_t)l + lanes + c0, v);
+      tmem_ld16(tmem + kColWg + 64u * (uint32_t)l + lanes + c0 + 16, v + 16);
+      tmem_wait_ld();
+      if (r < Ks[l]) {
+        float* g = G + oW[l] + r * kHid + c0;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) atomicAdd(g + j, v[j]);
+      }
+      atomicAdd(G + oB[l] + cn, gb[l]);
+    }
+    atomicAdd(G + oW5 + cn, gw5);
+  }
+  if (ok && done_tiles > 0) {
+    float a = lsum, b = gb5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if ((tid & 31) == 0) {
+      if (loss && target) atomicAdd(loss, a);
+      if (bwd) atomicAdd(G + oB5, b);
+    }
+  }
+  tc_fence_before();
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64u) : "memory");
+    tmem_dealloc(tmem, kTrCols);
   }
 }
 
-template <typename Rows>
-cudaError_t launch_fwd_tc(const Rows& rows, int n, const float* P, __nv_bfloat16* const H[4], float* T,
-                          unsigned* err, cudaStream_t st) {
-  if (n <= 0) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(k_mlp_fwd_tc<Rows>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemTc);
+// ---------------------------------------------------------------------------
+// host: tensor maps and launches
+// ---------------------------------------------------------------------------
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+cudaError_t encode_fn(EncodeTiled* fn) {
+  static EncodeTiled cached = nullptr;
+  if (!cached) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+    if (e != cudaSuccess) return e;
+    if (q != cudaDriverEntryPointSuccess || !p) return cudaErrorNotSupported;
+    cached = (EncodeTiled)p;
+  }
+  *fn = cached;
+  return cudaSuccess;
+}
+
+// Tensor map of an n x 112 bfloat16 feature matrix (rows 224 bytes apart), box
+// {8 columns, 128 rows}; rows past n read as zeros.
+cudaError_t feature_map(const __nv_bfloat16* X, int n, CUtensorMap* map) {
+  if (((uintptr_t)X & 15) != 0) return cudaErrorMisalignedAddress;
+  EncodeTiled fn;
+  cudaError_t e = encode_fn(&fn);
   if (e != cudaSuccess) return e;
-  int dev = 0, sms = 0, per_sm = 0;
+  const cuuint64_t dims[2] = {(cuuint64_t)kIn, (cuuint64_t)n};
+  const cuuint64_t strides[1] = {(cuuint64_t)kIn * 2};
+  const cuuint32_t box[2] = {8, (cuuint32_t)kTile};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)X, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+int sm_count() {
+  int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_fwd_tc<Rows>, kTcThreads, kSmemTc);
-  if (e != cudaSuccess) return e;
-  const int tiles = (n + kTile - 1) / kTile;
-  int grid = sms * (per_sm > 0 ? per_sm : 1);
-  if (grid > tiles) grid = tiles;
-  k_mlp_fwd_tc<Rows><<<grid, kTcThreads, kSmemTc, st>>>(rows, n, P, H ? H[0] : nullptr, H ? H[1] : nullptr,
-                                                        H ? H[2] : nullptr, H ? H[3] : nullptr, T, err);
-  return cudaGetLastError();
+  return sms > 0 ? sms : 1;
 }
 
 }  // namespace
 }  // namespace mlp
 
-cudaError_t mlp_forward_tc_features(const __nv_bfloat16* X, int n, const float* P, __nv_bfloat16* const H[4],
-                                    float* T, unsigned* err, cudaStream_t st) {
-  return mlp::launch_fwd_tc(mlp::RowsFromFeatures{X}, n, P, H, T, err, st);
+cudaError_t mlp_forward_tc_features(const __nv_bfloat16* X, int n, const float* P, float* T, unsigned* err,
+                                    cudaStream_t st) {
+  using namespace mlp;
+  if (n <= 0) return cudaSuccess;
+  CUtensorMap map;
+  cudaError_t e = feature_map(X, n, &map);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_mlp_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdSmem + 1024);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_fwd_tc, kThreads, kFwdSmem + 1024);
+  if (e != cudaSuccess) return e;
+  const int tiles = (n + kTile - 1) / kTile;
+  int grid = sm_count() * (per_sm > 0 ? per_sm : 1);
+  if (grid > tiles) grid = tiles;
+  k_mlp_fwd_tc<<<grid, kThreads, kFwdSmem + 1024, st>>>(map, 0, n, P, T, err);
+  return cudaGetLastError();
 }
 
-cudaError_t mlp_forward_tc_positions(const float4* pos, const mlp::Encoding& enc, const float lf[3], int n,
-                                     const float* P, float* T, unsigned* err, cudaStream_t st) {
-  mlp::RowsFromPositions rows{pos, enc, {lf[0], lf[1], lf[2]}};
-  return mlp::launch_fwd_tc(rows, n, P, nullptr, T, err, st);
+cudaError_t mlp_train_step_tc(const float* P, float* G, const __nv_bfloat16* X, const float* target, int n,
+                              float scale, float* T, float* loss, unsigned* err, cudaStream_t st) {
+  using namespace mlp;
+  if (n <= 0) return cudaSuccess;
+  CUtensorMap map;
+  cudaError_t e = feature_map(X, n, &map);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_mlp_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrSmem + 1024);
+  if (e != cudaSuccess) return e;
+  const int tiles = (n + kTile - 1) / kTile;
+  int grid = sm_count();
+  if (grid > tiles) grid = tiles;
+  k_mlp_train_tc<<<grid, kThreads, kTrSmem + 1024, st>>>(map, 0, n, P, target, scale, G, T, loss, err);
+  return cudaGetLastError();
 }
 
 }  // namespace beams

@@ -302,7 +302,8 @@ cudaError_t mlp_features(const float4* samples, const float4* lfeat, const Encod
   return cudaGetLastError();
 }
 
-// Forward (and, with G != null, backward) of n rows X (n x 112 bf16).
+// Forward (and, with G != null, backward) of n rows X (n x 112 bf16): on the
+// tensor cores when w.err is set, else on the CUDA cores (the reference path).
 cudaError_t mlp_fwd_bwd(const float* P, float* G, const __nv_bfloat16* X, const float* target, int n,
                         const TrainWS& w, cudaStream_t st) {
   const unsigned rf = (unsigned)((n + 31) / 32);
@@ -310,10 +311,10 @@ cudaError_t mlp_fwd_bwd(const float* P, float* G, const __nv_bfloat16* X, const 
   const int Ks[4] = {kIn, kHid, kHid, kHid};
   const int oW[4] = {oW1, oW2, oW3, oW4}, oB[4] = {oB1, oB2, oB3, oB4};
   if (w.err) {
-    // the four hidden layers on the tcgen05 tensor cores (k_mlp_tc.cu)
-    cudaError_t e = mlp_forward_tc_features(X, n, P, w.H, nullptr, w.err, st);
-    if (e != cudaSuccess) return e;
-  } else {
+    // forward, loss and backward fused on the tcgen05 tensor cores (k_mlp_tc.cu)
+    return mlp_train_step_tc(P, G, X, target, n, 1.f / (float)n, w.T, w.loss, w.err, st);
+  }
+  {
     const __nv_bfloat16* in = X;
     for (int l = 0; l < 4; ++l) {
       k_linear_fwd<<<rf, 256, 0, st>>>(in, P + oW[l], P + oB[l], w.H[l], n, Ks[l]);

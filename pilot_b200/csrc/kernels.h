@@ -20,12 +20,18 @@ cudaError_t launch_view_march_prec(const ExactGeo& g, int quad_dtype, const void
 cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    float* map, Counters* cnt, cudaStream_t st, const BrickRef* refs = nullptr,
                                    int nrefs = 0, int self = -1, const unsigned* gate = nullptr,
-                                   const unsigned char* occ = nullptr);
+                                   const unsigned char* occ = nullptr, const unsigned char* vmask = nullptr);
 // Empty-space occupancy of 8^3-cell macro-cells for the light march's skip.
 void occupancy_dims(const int n[3], int occ_n[3]);
 cudaError_t launch_build_occupancy(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tf,
                                    unsigned char* occ, cudaStream_t st);
 // K2 over a device list of kFallbackTile^2 pixel tiles (count in *fcount), with the map.
+// Learned form's lazy fallback (k_mlp_probe.cu): when the list of failing tiles
+// is non-empty, clears the vertex mask (nvert bytes, 16-byte multiple) and marks
+// the map vertices that the listed tiles' view rays read.
+cudaError_t launch_mark_fallback_vertices(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
+                                          const unsigned* flist, const unsigned* fcount, unsigned char* vmask,
+                                          size_t mask_bytes, cudaStream_t st);
 cudaError_t launch_view_march_tiles(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                     const float* map, float4* out, Counters* cnt, const unsigned* flist,
                                     const unsigned* fcount, cudaStream_t st);

@@ -1,7 +1,8 @@
 // light_march.cuh — one light ray of the map build: the march of
 // TransmittanceMapGenerator::operator() (beams/rendering/TransmittanceMap.h:279-332)
-// from the light towards a map vertex, software-pipelined two samples deep.
-// Shared by K1 (k_exact.cu) and the batched kernel (k_batch.cu).
+// from the light towards a map vertex (one sample at a time, or two deep in the
+// exact form's skipping march). Shared by K1 (k_exact.cu), the batched kernel
+// (k_batch.cu) and the learned form's probe check (k_mlp_probe.cu).
 // Compiled with -fmad=false (see exact_device.cuh).
 #pragma once
 #include <cuda_fp16.h>
@@ -57,7 +58,12 @@ template <> struct Accum<true> {
 // March from L towards vertex V. prefix(dir) gives the starting opacity (0,
 // or the cross-brick prefix of the multi-brick Phase 3). ns counts the samples
 // marched. With SKIP, occ is the macro-cell occupancy (see occupied()).
-template <typename QuadT, bool PREC, bool SKIP, bool RECT = false, typename Prefix>
+// PIPE: sample k+1 is located and its loads issued before sample k is
+// composited (two samples' loads in flight per ray). That pays only in the
+// exact form's skipping march; elsewhere the march issues one sample at a time,
+// which needs fewer registers and instructions (the config-1 map build went
+// 2.97 -> 2.78 ms at 4 blocks per SM, 2.70 ms at 6).
+template <typename QuadT, bool PREC, bool SKIP, bool RECT = false, bool PIPE = SKIP && !PREC, typename Prefix>
 __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __restrict__ quads, const float4* T0,
                                              const float4* T1, const float4* T2, const float* s_a,
                                              const float* s_tau, const unsigned char* __restrict__ occ,
@@ -75,11 +81,11 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
   float s[3] = {st[0], st[1], st[2]};
   const float len2 = (tmax - tmin) * (tmax - tmin);
   const float sdx = g.step * dir[0], sdy = g.step * dir[1], sdz = g.step * dir[2];
-  // The sample positions do not depend on the opacity, so sample k+1 is
-  // located and its loads issued before sample k is composited (the loads of
-  // two samples are in flight per ray). The break conditions are evaluated
-  // in the reference's order for every sample; only o == 1 ends the march
-  // early, after which the prefetched sample is discarded.
+  // The sample positions do not depend on the opacity, so with PIPE sample
+  // k+1 is located and its loads issued before sample k is composited. The
+  // break conditions are evaluated in the reference's order for every sample;
+  // only o == 1 ends the march early, after which a prefetched sample is
+  // discarded.
   // Empty macro-cells (occ == 0: every value there has TF alpha 0) are
   // stepped over without a field fetch: such a sample leaves the state
   // unchanged (Accum), so only its position update and break checks run. sk
@@ -140,31 +146,25 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
     }
   };
   acc.init(prefix(dir));
-  float va[8], pa[3], vb[8], pb[3];
-  unsigned ska, skb;
-  if constexpr (!SKIP) {
-    bool ok = gen(va, pa, ska);
-    while (ok) {
-      const bool okb = gen(vb, pb, skb);
-      bool done;
-      {
-        float scalar = hex_interp(va, pa[0], pa[1], pa[2]);
-        scalar = (scalar - g.min_scalar) * g.inv_delta;
-        done = acc.add(s_a, s_tau, tf_index_clamped(scalar * (float)n1, n1));
-        ++ns;
+  float va[8], pa[3];
+  unsigned ska;
+  if constexpr (!PIPE) {
+    for (;;) {
+      if (!gen(va, pa, ska)) {
+        ns += ska;  // skipped samples before the end of the ray
+        break;
       }
-      if (done || !okb) break;
-      ok = gen(va, pa, ska);
-      {
-        float scalar = hex_interp(vb, pb[0], pb[1], pb[2]);
-        scalar = (scalar - g.min_scalar) * g.inv_delta;
-        done = acc.add(s_a, s_tau, tf_index_clamped(scalar * (float)n1, n1));
-        ++ns;
-      }
-      if (done) break;
+      float scalar = hex_interp(va, pa[0], pa[1], pa[2]);
+      scalar = (scalar - g.min_scalar) * g.inv_delta;
+      ns += 1 + ska;
+      // Stop when the accumulated value can no longer change (see Accum).
+      if (acc.add(s_a, s_tau, tf_index_clamped(scalar * (float)n1, n1))) break;
     }
     return;
   }
+  static_assert(!PIPE || SKIP, "the two-sample pipeline is written for the skipping march");
+  float vb[8], pb[3];
+  unsigned skb;
   bool ok = gen(va, pa, ska);
   if (!ok) ns += ska;
   while (ok) {

@@ -42,12 +42,14 @@ struct MlpState {
   size_t probe_bytes = 0;
   float* probe_err = nullptr;  // per-probe max |dRGBA| of the last frame (tests)
   int probe_err_n = 0;
+  unsigned char* vmask = nullptr;  // lazy fallback: map vertices the failing tiles read
+  size_t vmask_bytes = 0;
   beams_mlp_options render_opts{};
   bool use_tc = true;            // training forward on the tcgen05 tensor cores
   unsigned* err_slot = nullptr;  // their timeout flag in the workspace
   ~MlpState() {
     for (void* p : {(void*)P, (void*)G, (void*)m, (void*)v, ws_mem, (void*)lights, (void*)lfeat, packed, probe_mem,
-                    (void*)probe_err})
+                    (void*)probe_err, (void*)vmask})
       if (p) cudaFree(p);
   }
 };
@@ -207,9 +209,10 @@ static beams_status probe_buffers(beams_renderer* r, const ExactGeo& g, ProbeBuf
 }
 
 // Probe pixels against the exact light march, then the exact map path over the
-// tiles that failed: K1 gated on a non-empty list, K2 over the listed tiles.
-// The network's view march has already recorded the probe pixels' samples.
-// Nothing here waits on the host.
+// tiles that failed, built lazily: the map vertices the listed tiles' view rays
+// read are marked, K1 marches only those (both gated on a non-empty list), K2
+// re-renders the listed tiles. The network's view march has already recorded
+// the probe pixels' samples. Nothing here waits on the host.
 static beams_status mlp_probe_and_fallback(beams_renderer* r, const ExactGeo& g, const ProbeBuffers& pb, float4* out,
                                            int& launches) {
   MlpState* st = r->mlp;
@@ -224,15 +227,21 @@ static beams_status mlp_probe_and_fallback(beams_renderer* r, const ExactGeo& g,
   const size_t nvert = (size_t)g.pd[0] * g.pd[1] * g.pd[2];
   beams_status s = ensure_buffer(r, (void**)&r->d_map, &r->map_cap, nvert * sizeof(float), "allocating map");
   if (s != BEAMS_OK) return s;
-  r->map_valid = false;  // whether the gated build ran is known on the device only
+  r->map_valid = false;  // a partial map, built (or not) on the device's decision
   r->map_is_half = false;
-  e = launch_light_march_f32(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map, r->d_cnt, r->stream, nullptr,
-                             0, -1, pb.fcount);
+  const size_t mask_bytes = (nvert + 15) & ~(size_t)15;
+  s = ensure_buffer(r, (void**)&st->vmask, &st->vmask_bytes, mask_bytes, "allocating the fallback vertex mask");
+  if (s != BEAMS_OK) return s;
+  e = launch_mark_fallback_vertices(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, pb.flist, pb.fcount, st->vmask,
+                                    mask_bytes, r->stream);
+  if (e == cudaSuccess)
+    e = launch_light_march_f32(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map, r->d_cnt, r->stream,
+                               nullptr, 0, -1, pb.fcount, nullptr, st->vmask);
   if (e == cudaSuccess)
     e = launch_view_march_tiles(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map, out, r->d_cnt + 1,
                                 pb.flist, pb.fcount, r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "mlp fallback launch");
-  launches += 2;
+  launches += 4;
   return BEAMS_OK;
 }
 
@@ -279,7 +288,7 @@ beams_status beams_mlp_forward_tc_device(beams_renderer* r, const void* features
     if (s != BEAMS_OK) return s;
   }
   cudaSetDevice(r->device);
-  cudaError_t e = mlp_forward_tc_features((const __nv_bfloat16*)features_bf16, n, st->P, nullptr, T, st->err_slot,
+  cudaError_t e = mlp_forward_tc_features((const __nv_bfloat16*)features_bf16, n, st->P, T, st->err_slot,
                                           r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "mlp_forward_tc_device");
   return BEAMS_OK;
@@ -309,7 +318,7 @@ beams_status beams_mlp_forward_tc(beams_renderer* r, const float* features, int 
   if (e == cudaSuccess) e = cudaMemsetAsync(derr, 0, sizeof(unsigned), r->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(dx, hx.data(), hx.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice, r->stream);
-  if (e == cudaSuccess) e = mlp_forward_tc_features(dx, n, st->P, nullptr, dt, derr, r->stream);
+  if (e == cudaSuccess) e = mlp_forward_tc_features(dx, n, st->P, dt, derr, r->stream);
   unsigned herr = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(T, dt, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, r->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, derr, sizeof(unsigned), cudaMemcpyDeviceToHost, r->stream);
@@ -466,14 +475,22 @@ beams_status beams_mlp_train(beams_renderer* r, const beams_mlp_options* opt, be
   const double mean_t = s1 / holdout;
   const int steps_per_epoch = std::max(1, ntrain / o.batch);
   const int total = steps_per_epoch * o.epochs;
-  for (int ep = 0; ep < o.epochs && e == cudaSuccess; ++ep) {
+  bool timed_out = false;
+  for (int ep = 0; ep < o.epochs && e == cudaSuccess && !timed_out; ++ep) {
     const int rot = (int)(((unsigned)ep * 2654435761u) % (unsigned)std::max(1, ntrain - o.batch));
-    for (int k = 0; k < steps_per_epoch && e == cudaSuccess; ++k) {
+    for (int k = 0; k < steps_per_epoch && e == cudaSuccess && !timed_out; ++k) {
       int off = (rot + k * o.batch) % std::max(1, ntrain - o.batch + 1);
       const float prog = (float)st->step / (float)total;
       const float lr = o.lr * (0.05f + 0.95f * 0.5f * (1.f + std::cos((float)M_PI * prog)));
       e = mlp_fwd_bwd(st->P, st->G, d_X + (size_t)off * kIn, d_target + off, o.batch, st->ws, r->stream);
       if (e == cudaSuccess) e = mlp_adam(st->P, st->G, st->m, st->v, lr, ++st->step, r->stream);
+      // a tensor-core wait that gave up ends the training early (checked every 256 steps)
+      if (e == cudaSuccess && st->ws.err && (st->step & 255) == 0) {
+        unsigned f = 0;
+        e = cudaMemcpyAsync(&f, st->ws.err, sizeof(unsigned), cudaMemcpyDeviceToHost, r->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(r->stream);
+        timed_out = f != 0;
+      }
     }
   }
   cudaEventRecord(t2, r->stream);

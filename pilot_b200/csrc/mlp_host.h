@@ -26,12 +26,16 @@ cudaError_t mlp_features(const float4* samples, const float4* lfeat, const mlp::
                          int n, cudaStream_t st);
 cudaError_t mlp_fwd_bwd(const float* P, float* G, const __nv_bfloat16* X, const float* target, int n,
                         const TrainWS& w, cudaStream_t st);
-// Forward pass on the tcgen05 tensor cores (k_mlp_tc.cu): rows of features
-// (H[l] receive the hidden activations when non-null) or positions to encode.
-cudaError_t mlp_forward_tc_features(const __nv_bfloat16* X, int n, const float* P, __nv_bfloat16* const H[4],
-                                    float* T, unsigned* err, cudaStream_t st);
-cudaError_t mlp_forward_tc_positions(const float4* pos, const mlp::Encoding& enc, const float lf[3], int n,
-                                     const float* P, float* T, unsigned* err, cudaStream_t st);
+// Forward pass on the tcgen05 tensor cores (k_mlp_tc.cu) of n rows of
+// features (16-byte aligned): T per row.
+cudaError_t mlp_forward_tc_features(const __nv_bfloat16* X, int n, const float* P, float* T, unsigned* err,
+                                    cudaStream_t st);
+// One training step on the tcgen05 tensor cores (k_mlp_tc.cu): forward, loss
+// (sum of squared errors added to *loss when target is given), and with G
+// non-null the backward, adding scale-weighted gradients to G; T per row when
+// non-null.
+cudaError_t mlp_train_step_tc(const float* P, float* G, const __nv_bfloat16* X, const float* target, int n,
+                              float scale, float* T, float* loss, unsigned* err, cudaStream_t st);
 cudaError_t mlp_adam(float* P, float* G, float* m, float* v, float lr, int t, cudaStream_t st);
 
 }  // namespace beams

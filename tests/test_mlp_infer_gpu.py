@@ -182,7 +182,8 @@ def test_mlp_fallback_every_pixel_probed(cuda_device):
     flagged = tiles > tol
     print(f"tol {tol:.4f}: {flagged.sum()} of {flagged.size} tiles fall back")
     assert 0 < flagged.sum() < flagged.size and t["fallback_tiles"] == flagged.sum()
-    assert t["map_vertices"] == (s.map_m + 1) ** 3
+    # the lazy fallback builds only the map vertices the failing tiles' rays read
+    assert 0 < t["map_vertices"] <= (s.map_m + 1) ** 3
     _check_tiles(img, mlp_img, exact_img, flagged)
     # a tolerance above every error keeps the network's image and builds no map
     r.set_form(B.FORM_MLP, B.mlp_options(knot=2, probe_fraction=1.0, fallback_tol=1e30))
@@ -223,3 +224,40 @@ def test_mlp_fallback_one_percent_probes(cuda_device):
     print(f"1% probes, tol {tol:.3f}: {flagged.sum()} of 9 tiles fall back; probe errors max {err.max():.3f}")
     assert 0 < flagged.sum() < 9 and t["fallback_tiles"] == flagged.sum()
     _check_tiles(img, mlp_img, exact_img, flagged)
+
+
+def test_mlp_lazy_fallback_builds_only_the_failing_tiles_vertices(cuda_device):
+    """A few failing tiles of a 256^2 image over a 64-cell map: the fallback
+    marks and marches only the map vertices those tiles' view rays read, far
+    fewer than the whole map, and the tiles still carry the exact form's pixels
+    bit for bit (every vertex they read was built)."""
+    s = scenes.small(66, n=48, image=256, m=64, kind="noise")
+    r = _renderer(s)
+    exact_img, te = r.render(s.camera())
+    r.mlp_set_params(smooth_params(11))
+    r.set_form(B.FORM_MLP, B.mlp_options(knot=2, probe_fraction=0.0))
+    mlp_img, _ = r.render(s.camera())
+    full = (s.map_m + 1) ** 3
+    P = 4  # probe fraction 1/16: probes at (4i + 2, 4j + 2)
+    n = len(range(P // 2, s.width, P))
+    for q in (0.9, 0.5):
+        r.set_form(B.FORM_MLP, B.mlp_options(knot=2, probe_fraction=1.0 / 16, fallback_tol=1e30))
+        r.render(s.camera())
+        err = r.mlp_probe_errors(n * n).reshape(n, n)
+        nt = -(-s.width // TILE)
+        tiles = np.full((nt, nt), -np.inf)
+        for j in range(n):
+            for i in range(n):
+                y, x = j * P + P // 2, i * P + P // 2
+                tiles[y // TILE, x // TILE] = max(tiles[y // TILE, x // TILE], err[j, i])
+        tol = float(np.quantile(tiles[np.isfinite(tiles)], q))
+        r.set_form(B.FORM_MLP, B.mlp_options(knot=2, probe_fraction=1.0 / 16, fallback_tol=tol))
+        img, t = r.render(s.camera())
+        flagged = tiles > tol
+        print(f"quantile {q}: {flagged.sum()} of {flagged.size} tiles fall back, "
+              f"{t['map_vertices']} of {full} map vertices built, light samples {t['light_samples']} "
+              f"(whole map: {te['light_samples']})")
+        assert t["fallback_tiles"] == flagged.sum() and flagged.sum() > 0
+        assert 0 < t["map_vertices"] < full
+        _check_tiles(img, mlp_img, exact_img, flagged)
+    r.close()

@@ -992,6 +992,7 @@ def run_bricks(args):
 #   mlp_view         learned-form view march, 1024^2
 #   mlp_frame        learned form frame: scene-light network, 1% probes
 #   mlp_tc           tcgen05 forward, 2^21 rows
+#   mlp_train        tcgen05 training steps (2^18 samples, 1 epoch, batches of 16384)
 #   batch            16-request persistent batch (--split: map-build launch, then view launch)
 #   precision_light  precision-form K1, bf16 640^3
 #   precision_view   precision-form K2, bf16 640^3, 1024^2, map cached
@@ -1000,8 +1001,8 @@ def run_bricks(args):
 # device memory stays within a few GB. The tuning is fixed (8^3 vertex bricks,
 # skipping as stated per case) so that the launch sequence is the same every run.
 # ---------------------------------------------------------------------------
-PROFILE_CASES = ["light_march", "view_march", "mlp_view", "mlp_frame", "mlp_tc", "batch", "precision_light",
-                 "precision_view", "bricks"]
+PROFILE_CASES = ["light_march", "view_march", "mlp_view", "mlp_frame", "mlp_tc", "mlp_train", "batch",
+                 "precision_light", "precision_view", "bricks"]
 
 
 def run_profile_case(a):
@@ -1040,6 +1041,16 @@ def run_profile_case(a):
             r.set_form(B.FORM_MLP, B.mlp_options(knot=4, probe_fraction=0.0))
             for _ in range(a.reps):
                 r.render(cam, out=out, timings=False)
+    elif a.profile_case == "mlp_train":
+        # training steps on the tensor cores on the config-1 field
+        s = scenes.config1()
+        fd = s.field_device()
+        r = B.Renderer(0)
+        r.set_volume(fd, origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+        s.configure(r)
+        r.render(s.camera(), timings=False)
+        for _ in range(a.reps):
+            r.mlp_train(B.mlp_options(samples_log2=18, epochs=1, batch=16384, n_lights=1, scene_light=1))
     elif a.profile_case == "mlp_tc":
         # the tcgen05 forward on 2^21 rows of device-resident features
         s = scenes.small(5, n=32, image=16, m=8)
@@ -1127,8 +1138,9 @@ def main():
     ap.add_argument("--mlp-samples-log2", type=int, default=24)
     ap.add_argument("--mlp-epochs", type=int, default=4)
     ap.add_argument("--no-quality", action="store_true", help="skip the FP64 oracle crops")
-    ap.add_argument("--crops", type=int, default=3)
-    ap.add_argument("--crop", type=int, default=128)
+    ap.add_argument("--crops", type=int, default=None, help="FP64 crops (default 3; precision form 2)")
+    ap.add_argument("--crop", type=int, default=None,
+                    help="FP64 crop edge in pixels (default 128; precision form 512, as its config states)")
     ap.add_argument("--crop-stride", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="default line: skip the learned-form records")
@@ -1148,6 +1160,10 @@ def main():
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up frames
     if args.config is None:
         args.config = 2 if args.form == "precision" else 1
+    if args.crop is None:
+        args.crop = 512 if args.form == "precision" else 128
+    if args.crops is None:
+        args.crops = 2 if args.form == "precision" else 3
     if args.impl == "reference":
         return run_reference(args)
     if args.form == "batch":

@@ -17,14 +17,14 @@
 // descriptor (version 1). A TMA tiled load of a box {8 columns, 128 rows}
 // lands exactly as one chunk, so input tiles arrive in place.
 //
-// Forward (k_mlp_fwd_tc, 256 threads, two CTAs per SM): 128-row tiles of
-// precomputed features are loaded by TMA into a double buffer (the next tile's
-// load runs under the current tile's layers); one thread issues each layer's
-// tcgen05.mma (M 128, N 64, K 16 per instruction, float32 accumulator in TMEM)
-// and commits to an mbarrier; eight warps read the accumulator back with
-// tcgen05.ld (warp w: TMEM lanes 32(w%4).. = its rows, columns 32(w/4)..),
-// add the bias, apply ReLU, round to bfloat16 and write the next layer's
-// operand over the input tile, which the first layer has finished reading.
+// Forward (k_mlp_fwd_tc, one CTA of four warpgroup pipelines per SM):
+// 128-row tiles of precomputed features are loaded by TMA; per layer one
+// thread of the pipeline issues the tcgen05.mma (M 128, N 64, K 16 per
+// instruction, float32 accumulator in TMEM) and commits to an mbarrier; the
+// pipeline's four warps read the accumulator back with tcgen05.ld (warp w:
+// TMEM lanes 32(w%4).. = its rows), add the bias, apply ReLU, round to
+// bfloat16 and write the next layer's operand. Four tiles are in flight per SM,
+// and a pipeline's next tile loads while its last three layers run.
 //
 // Training (k_mlp_train_tc, 256 threads, one CTA per SM): per tile the forward
 // keeps every layer's activations in shared memory, the head computes T, the
@@ -244,102 +244,124 @@ __device__ __forceinline__ float head_T(float b5, float p0, float p1) {
 }
 
 // ---------------------------------------------------------------------------
-// dense forward
+// dense forward: four independent tile pipelines per SM
 // ---------------------------------------------------------------------------
-constexpr int kFwdOffW = 2 * kXBytes;                 // 57344
-constexpr int kFwdOffAux = kFwdOffW + kWBytes;        // 96256
-constexpr int kAuxFloats = 5 * kHid + 1 + 2 * kTile;  // biases, w5, b5, head halves
+// One CTA of four warpgroups per SM. Warpgroup p runs its own pipeline over
+// tiles p, p + 4*grid, ...: its input tile (TMA), activation tile, two
+// mbarriers and a 64-column TMEM accumulator are its own; the weights are
+// shared. While one pipeline waits on its MMA or runs its epilogue, the other
+// three keep the tensor core busy, and each pipeline's next tile is loaded as
+// soon as its first layer has read the current one. Per-pipeline
+// synchronisation uses named barriers (ids 1..4, 128 threads).
+constexpr int kPipes = 4;
+constexpr int kFwdThreads = 128 * kPipes;
+constexpr int kAuxFloats = 5 * kHid + 1;                              // biases, w5, b5
+constexpr int kFwdPipeBytes = kXBytes + kHBytes;                      // 45056: input tile, activations
+constexpr int kFwdOffPipe = kWBytes;                                  // 38912
+constexpr int kFwdOffAux = kFwdOffPipe + kPipes * kFwdPipeBytes;      // 219136
 constexpr int kFwdOffBar = ((kFwdOffAux + kAuxFloats * 4 + 15) / 16) * 16;
-constexpr int kFwdSmem = kFwdOffBar + 32;
+constexpr int kFwdSmem = kFwdOffBar + kPipes * 16;
+static_assert(kFwdOffPipe % 128 == 0 && kFwdPipeBytes % 128 == 0, "TMA destinations on 128-byte boundaries");
+static_assert(kFwdSmem + 1024 <= 227 * 1024, "one CTA of four pipelines fits the shared memory of an SM");
 
-__global__ void __launch_bounds__(kThreads, 2) k_mlp_fwd_tc(const __grid_constant__ CUtensorMap xmap, int row0,
-                                                            int n, const float* __restrict__ P,
-                                                            float* __restrict__ T, unsigned* __restrict__ err) {
+__device__ __forceinline__ void pipe_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+// Named-barrier OR over the pipeline's 128 threads: a uniform decision.
+__device__ __forceinline__ bool pipe_sync_or(int id, bool v) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred pi, po;\n\t"
+      "setp.ne.u32 pi, %1, 0;\n\t"
+      "bar.red.or.pred po, %2, 128, pi;\n\t"
+      "selp.u32 %0, 1, 0, po;\n\t}\n"
+      : "=r"(out)
+      : "r"((uint32_t)v), "r"(id)
+      : "memory");
+  return out != 0;
+}
+
+__global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd_tc(const __grid_constant__ CUtensorMap xmap, int row0,
+                                                               int n, const float* __restrict__ P,
+                                                               float* __restrict__ T, unsigned* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   unsigned char* sm = aligned_smem(sm_raw);
   float* aux = reinterpret_cast<float*>(sm + kFwdOffAux);
-  float* part = aux + 5 * kHid + 1;  // [2][kTile]
   __shared__ uint32_t s_tmem;
-  const int tid = threadIdx.x, warp = tid >> 5, q = warp & 3, hf = warp >> 2;
-  const int r = q * 32 + (tid & 31), c0 = hf * 32;
-  const uint32_t xbase = smem_addr(sm), wbase = smem_addr(sm + kFwdOffW);
-  const uint32_t bar_load[2] = {smem_addr(sm + kFwdOffBar), smem_addr(sm + kFwdOffBar + 8)};
-  const uint32_t bar_mma = smem_addr(sm + kFwdOffBar + 16);
+  const int tid = threadIdx.x, warp = tid >> 5, pipe = warp >> 2, q = warp & 3;
+  const int ptid = tid & 127, bar_id = 1 + pipe;
+  const int r = q * 32 + (tid & 31);  // the thread's row of the tile = its TMEM lane
+  unsigned char* H = sm + kFwdOffPipe + pipe * kFwdPipeBytes + kXBytes;
+  const uint32_t wbase = smem_addr(sm);
+  const uint32_t xaddr = smem_addr(sm + kFwdOffPipe + pipe * kFwdPipeBytes), haddr = smem_addr(H);
+  const uint32_t bar_load = smem_addr(sm + kFwdOffBar + pipe * 16), bar_mma = bar_load + 8;
   const int ntiles = (n + kTile - 1) / kTile;
 
-  stage_weights(P, sm + kFwdOffW, aux);
-  if (tid == 0) {
-    mbar_init(bar_load[0], 1);
-    mbar_init(bar_load[1], 1);
+  stage_weights(P, sm, aux);
+  if (ptid == 0) {
+    mbar_init(bar_load, 1);
     mbar_init(bar_mma, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) tmem_alloc(&s_tmem, 64u);
+  if (warp == 0) tmem_alloc(&s_tmem, 64u * kPipes);
   fence_async_smem();  // the weights were written by ordinary stores
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = s_tmem;
-  const uint32_t tmem_acc = tmem + ((uint32_t)(q * 32) << 16);
+  const uint32_t tmem = s_tmem + 64u * (uint32_t)pipe;           // this pipeline's columns
+  const uint32_t tmem_acc = tmem + ((uint32_t)(q * 32) << 16);   // and this warp's lanes
 
-  int tile = blockIdx.x;
-  if (tid == 0 && tile < ntiles) tma_load_tile(xbase, &xmap, row0 + tile * kTile, bar_load[0]);
-  unsigned mphase = 0;
-  // loads issued and not yet waited for successfully, when leaving early:
-  // the current tile's (if its wait failed) and the next tile's prefetch
-  int it = 0;
-  bool cur_pending = false, next_pending = false;
-  bool ok = true;
-  for (; tile < ntiles; tile += gridDim.x, ++it) {
-    const int cur = it & 1;
-    const int next = tile + gridDim.x;
-    next_pending = next < ntiles;
-    if (next_pending && tid == 0)
-      tma_load_tile(xbase + (cur ^ 1) * kXBytes, &xmap, row0 + next * kTile, bar_load[cur ^ 1]);
-    ok = mbar_wait(bar_load[cur], (unsigned)(it >> 1) & 1u);
-    if (__syncthreads_or(!ok)) {
+  const int stride = gridDim.x * kPipes;
+  int tile = blockIdx.x * kPipes + pipe;
+  if (ptid == 0 && tile < ntiles) tma_load_tile(xaddr, &xmap, row0 + tile * kTile, bar_load);
+  bool load_pending = tile < ntiles, ok = true;
+  unsigned lph = 0, mph = 0;
+  for (; tile < ntiles; tile += stride) {
+    ok = mbar_wait(bar_load, lph);
+    if (pipe_sync_or(bar_id, !ok)) {
       ok = false;
-      cur_pending = true;
       break;
     }
-    unsigned char* buf = sm + cur * kXBytes;
-    const uint32_t a = xbase + cur * kXBytes;
-    float h[32];
+    lph ^= 1u;
+    load_pending = false;
+    float h[2][32];
     for (int l = 0; l < 4; ++l) {
-      if (tid == 0) {
+      if (ptid == 0) {
         tc_fence_after();
-        issue_fwd(tmem, a, wbase, l);
+        issue_fwd(tmem, l == 0 ? xaddr : haddr, wbase, l);
         mma_commit(bar_mma);
       }
-      ok = mbar_wait(bar_mma, mphase);
-      mphase ^= 1u;
-      if (__syncthreads_or(!ok)) {
+      ok = mbar_wait(bar_mma, mph);
+      mph ^= 1u;
+      if (pipe_sync_or(bar_id, !ok)) {
         ok = false;
         break;
       }
       tc_fence_after();
-      // layers 0-2 overwrite the tile's input (read only by layer 0) with their output
-      hidden_epilogue(tmem_acc, aux + l * kHid, r, c0, h, l < 3 ? buf : nullptr);
-      if (l == 3) part[hf * kTile + r] = head_partial(h, aux + 4 * kHid, c0);
+      if (l == 0 && tile + stride < ntiles) {
+        // the first layer has read the input tile: load the next one in its place
+        if (ptid == 0) tma_load_tile(xaddr, &xmap, row0 + (tile + stride) * kTile, bar_load);
+        load_pending = true;
+      }
+      hidden_epilogue(tmem_acc, aux + l * kHid, r, 0, h[0], l < 3 ? H : nullptr);
+      hidden_epilogue(tmem_acc, aux + l * kHid, r, 32, h[1], l < 3 ? H : nullptr);
       fence_async_smem();
       tc_fence_before();
-      __syncthreads();
+      pipe_sync(bar_id);
     }
     if (!ok) break;
     const int row = tile * kTile + r;
-    if (hf == 0 && row < n && T) T[row] = head_T(aux[5 * kHid], part[r], part[kTile + r]);
+    if (row < n && T)
+      T[row] = head_T(aux[5 * kHid], head_partial(h[0], aux + 4 * kHid, 0), head_partial(h[1], aux + 4 * kHid, 32));
   }
   if (!ok) {
-    if (tid == 0) atomicExch(err, 1u);
-    // loads still in flight land in this CTA's shared memory: wait for them (bounded)
-    if (cur_pending) mbar_wait(bar_load[it & 1], (unsigned)(it >> 1) & 1u);
-    if (next_pending) mbar_wait(bar_load[(it + 1) & 1], (unsigned)((it + 1) >> 1) & 1u);
+    if (ptid == 0) atomicExch(err, 1u);
+    // a load still in flight lands in this CTA's shared memory: wait for it (bounded)
+    if (load_pending) mbar_wait(bar_load, lph);
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    tmem_dealloc(tmem, 64u);
+    tmem_dealloc(s_tmem, 64u * kPipes);
   }
 }
 
@@ -350,7 +372,7 @@ constexpr int kTrOffX = kWBytes;                       // 38912
 constexpr int kTrOffH = kTrOffX + kXBytes;             // 67584: H0..H3
 constexpr int kTrOffDY = kTrOffH + 4 * kHBytes;        // 133120
 constexpr int kTrOffAux = kTrOffDY + kHBytes;          // 149504
-constexpr int kTrAuxFloats = kAuxFloats + kTile;       // + dz per row
+constexpr int kTrAuxFloats = kAuxFloats + 2 * kTile + kTile;  // + head halves, dz per row
 constexpr int kTrOffBar = ((kTrOffAux + kTrAuxFloats * 4 + 15) / 16) * 16;
 constexpr int kTrSmem = kTrOffBar + 16;
 // TMEM columns: forward accumulator, data gradient, weight gradients of layers 0..3
@@ -637,13 +659,10 @@ cudaError_t mlp_forward_tc_features(const __nv_bfloat16* X, int n, const float* 
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_mlp_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdSmem + 1024);
   if (e != cudaSuccess) return e;
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_fwd_tc, kThreads, kFwdSmem + 1024);
-  if (e != cudaSuccess) return e;
   const int tiles = (n + kTile - 1) / kTile;
-  int grid = sm_count() * (per_sm > 0 ? per_sm : 1);
-  if (grid > tiles) grid = tiles;
-  k_mlp_fwd_tc<<<grid, kThreads, kFwdSmem + 1024, st>>>(map, 0, n, P, T, err);
+  int grid = sm_count();
+  if (grid > (tiles + kPipes - 1) / kPipes) grid = (tiles + kPipes - 1) / kPipes;
+  k_mlp_fwd_tc<<<grid, kFwdThreads, kFwdSmem + 1024, st>>>(map, 0, n, P, T, err);
   return cudaGetLastError();
 }
 

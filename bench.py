@@ -29,7 +29,7 @@ The line carries:
               frame when a sample says it fits the budget (the sample's
               extrapolation and its error beside it), else on the sample,
   learned     the metric's second half: the learned form on the same frame,
-              with config 4's network (32 training lights) and with a network
+              with the specified network (32 training lights) and with a network
               trained for the rendered light; frames/s against the exact frame,
               PSNR against the FP64 oracle on crops, fallback tiles, tensor
               roofline (training is not timed).
@@ -462,7 +462,7 @@ def run_ours(args):
                                                 "error": c["frame_s"] / f["frame_s"] - 1.0}}
 
     # the metric's second half: the learned form on the same field, camera and
-    # light, against this run's exact frame (config 4's network as specified,
+    # light, against this run's exact frame (the network as specified,
     # trained over 32 light directions, and a network trained for the rendered
     # light); training runs before each record's timed frames
     learned = None
@@ -481,7 +481,7 @@ def run_ours(args):
                 fallback_tol=args.fallback_tol, samples_log2=args.mlp_samples_log2, epochs=args.mlp_epochs,
                 steps=max(10, min(args.steps, 50)), warmup=3, field_host=field_host, crops=args.crops,
                 crop=args.crop, crop_stride=args.crop_stride, threads=os.cpu_count() or 1)
-            rec["network"] = ("config 4 as specified: 2^24 samples over 32 light directions uniform on the sphere"
+            rec["network"] = ("as specified: 2^24 samples over 32 light directions uniform on the sphere"
                               if lights == 32 else "2^24 samples for the rendered light only (fixed light, any camera)")
             learned[name] = rec
         r.set_form(B.FORM_EXACT)
@@ -1042,7 +1042,7 @@ def run_profile_case(a):
             for _ in range(a.reps):
                 r.render(cam, out=out, timings=False)
     elif a.profile_case == "mlp_train":
-        # training steps on the tensor cores on the config-1 field
+        # training steps on the tensor cores on the 512^3 noise field
         s = scenes.config1()
         fd = s.field_device()
         r = B.Renderer(0)

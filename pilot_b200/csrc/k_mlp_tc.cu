@@ -17,14 +17,13 @@
 // descriptor (version 1). A TMA tiled load of a box {8 columns, 128 rows}
 // lands exactly as one chunk, so input tiles arrive in place.
 //
-// Forward (k_mlp_fwd_tc, one CTA of four warpgroup pipelines per SM):
+// Forward (k_mlp_fwd_tc, one CTA of six warpgroup pipelines per SM):
 // 128-row tiles of precomputed features are loaded by TMA; per layer one
 // thread of the pipeline issues the tcgen05.mma (M 128, N 64, K 16 per
 // instruction, float32 accumulator in TMEM) and commits to an mbarrier; the
 // pipeline's four warps read the accumulator back with tcgen05.ld (warp w:
 // TMEM lanes 32(w%4).. = its rows), add the bias, apply ReLU, round to
-// bfloat16 and write the next layer's operand. Four tiles are in flight per SM,
-// and a pipeline's next tile loads while its last three layers run.
+// bfloat16 and write the next layer's operand. Six tiles are in flight per SM.
 //
 // Training (k_mlp_train_tc, 256 threads, one CTA per SM): per tile the forward
 // keeps every layer's activations in shared memory, the head computes T, the
@@ -244,25 +243,30 @@ __device__ __forceinline__ float head_T(float b5, float p0, float p1) {
 }
 
 // ---------------------------------------------------------------------------
-// dense forward: four independent tile pipelines per SM
+// dense forward: six independent tile pipelines per SM
 // ---------------------------------------------------------------------------
-// One CTA of four warpgroups per SM. Warpgroup p runs its own pipeline over
-// tiles p, p + 4*grid, ...: its input tile (TMA), activation tile, two
-// mbarriers and a 64-column TMEM accumulator are its own; the weights are
-// shared. While one pipeline waits on its MMA or runs its epilogue, the other
-// three keep the tensor core busy, and each pipeline's next tile is loaded as
-// soon as its first layer has read the current one. Per-pipeline
-// synchronisation uses named barriers (ids 1..4, 128 threads).
-constexpr int kPipes = 4;
+// One CTA of six warpgroups per SM. Warpgroup p runs its own pipeline over
+// tiles p, p + 6*grid, ...: its tile buffer (the TMA-loaded input, then each
+// layer's activations over it), two mbarriers and a 64-column TMEM accumulator
+// are its own; the weights are shared. While one pipeline waits on its MMA, its
+// next tile's load or runs its epilogue, the other five keep the tensor core
+// busy; a pipeline's next tile is loaded as soon as its last layer has read the
+// activations. Per-pipeline synchronisation uses named barriers (ids 1..6,
+// 128 threads). Six pipelines with one buffer each ran 0.39 ms on 2^22 rows,
+// four with a separate activation buffer (and the next load under the last
+// three layers) 0.44 ms.
+constexpr int kPipes = 6;
 constexpr int kFwdThreads = 128 * kPipes;
 constexpr int kAuxFloats = 5 * kHid + 1;                              // biases, w5, b5
-constexpr int kFwdPipeBytes = kXBytes + kHBytes;                      // 45056: input tile, activations
+constexpr int kFwdPipeBytes = kXBytes;                                // 28672: input tile, then activations
 constexpr int kFwdOffPipe = kWBytes;                                  // 38912
-constexpr int kFwdOffAux = kFwdOffPipe + kPipes * kFwdPipeBytes;      // 219136
+constexpr int kFwdOffAux = kFwdOffPipe + kPipes * kFwdPipeBytes;      // 210944
 constexpr int kFwdOffBar = ((kFwdOffAux + kAuxFloats * 4 + 15) / 16) * 16;
 constexpr int kFwdSmem = kFwdOffBar + kPipes * 16;
 static_assert(kFwdOffPipe % 128 == 0 && kFwdPipeBytes % 128 == 0, "TMA destinations on 128-byte boundaries");
-static_assert(kFwdSmem + 1024 <= 227 * 1024, "one CTA of four pipelines fits the shared memory of an SM");
+static_assert(kFwdSmem + 1024 <= 227 * 1024, "one CTA of six pipelines fits the shared memory of an SM");
+constexpr uint32_t kFwdCols = 512;  // TMEM columns: 64 per pipeline, allocated as a power of two
+static_assert(64 * kPipes <= (int)kFwdCols, "TMEM columns");
 
 __device__ __forceinline__ void pipe_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
 // Named-barrier OR over the pipeline's 128 threads: a uniform decision.
@@ -289,7 +293,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd_tc(const __grid_cons
   const int tid = threadIdx.x, warp = tid >> 5, pipe = warp >> 2, q = warp & 3;
   const int ptid = tid & 127, bar_id = 1 + pipe;
   const int r = q * 32 + (tid & 31);  // the thread's row of the tile = its TMEM lane
-  unsigned char* H = sm + kFwdOffPipe + pipe * kFwdPipeBytes + kXBytes;
+  unsigned char* H = sm + kFwdOffPipe + pipe * kFwdPipeBytes;  // over the input tile, once layer 0 has read it
   const uint32_t wbase = smem_addr(sm);
   const uint32_t xaddr = smem_addr(sm + kFwdOffPipe + pipe * kFwdPipeBytes), haddr = smem_addr(H);
   const uint32_t bar_load = smem_addr(sm + kFwdOffBar + pipe * 16), bar_mma = bar_load + 8;
@@ -301,7 +305,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd_tc(const __grid_cons
     mbar_init(bar_mma, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) tmem_alloc(&s_tmem, 64u * kPipes);
+  if (warp == 0) tmem_alloc(&s_tmem, kFwdCols);
   fence_async_smem();  // the weights were written by ordinary stores
   tc_fence_before();
   __syncthreads();
@@ -322,7 +326,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd_tc(const __grid_cons
     }
     lph ^= 1u;
     load_pending = false;
-    float h[2][32];
+    float h[32], p0 = 0.f, p1 = 0.f;
     for (int l = 0; l < 4; ++l) {
       if (ptid == 0) {
         tc_fence_after();
@@ -336,13 +340,16 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd_tc(const __grid_cons
         break;
       }
       tc_fence_after();
-      if (l == 0 && tile + stride < ntiles) {
-        // the first layer has read the input tile: load the next one in its place
+      if (l == 3 && tile + stride < ntiles) {
+        // the last layer has read the activations: load the next tile in their place
         if (ptid == 0) tma_load_tile(xaddr, &xmap, row0 + (tile + stride) * kTile, bar_load);
         load_pending = true;
       }
-      hidden_epilogue(tmem_acc, aux + l * kHid, r, 0, h[0], l < 3 ? H : nullptr);
-      hidden_epilogue(tmem_acc, aux + l * kHid, r, 32, h[1], l < 3 ? H : nullptr);
+      // two halves of the row in turn (32 live accumulator values per thread)
+      hidden_epilogue(tmem_acc, aux + l * kHid, r, 0, h, l < 3 ? H : nullptr);
+      if (l == 3) p0 = head_partial(h, aux + 4 * kHid, 0);
+      hidden_epilogue(tmem_acc, aux + l * kHid, r, 32, h, l < 3 ? H : nullptr);
+      if (l == 3) p1 = head_partial(h, aux + 4 * kHid, 32);
       fence_async_smem();
       tc_fence_before();
       pipe_sync(bar_id);
@@ -350,7 +357,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd_tc(const __grid_cons
     if (!ok) break;
     const int row = tile * kTile + r;
     if (row < n && T)
-      T[row] = head_T(aux[5 * kHid], head_partial(h[0], aux + 4 * kHid, 0), head_partial(h[1], aux + 4 * kHid, 32));
+      T[row] = head_T(aux[5 * kHid], p0, p1);
   }
   if (!ok) {
     if (ptid == 0) atomicExch(err, 1u);
@@ -361,7 +368,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd_tc(const __grid_cons
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    tmem_dealloc(s_tmem, 64u * kPipes);
+    tmem_dealloc(s_tmem, kFwdCols);
   }
 }
 

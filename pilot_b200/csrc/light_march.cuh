@@ -61,8 +61,8 @@ template <> struct Accum<true> {
 // PIPE: sample k+1 is located and its loads issued before sample k is
 // composited (two samples' loads in flight per ray). That pays only in the
 // exact form's skipping march; elsewhere the march issues one sample at a time,
-// which needs fewer registers and instructions (the config-1 map build went
-// 2.97 -> 2.78 ms at 4 blocks per SM, 2.70 ms at 6).
+// which needs fewer registers and instructions (the 257^3-vertex map of a
+// 512^3 noise field went 2.97 -> 2.78 ms at 4 blocks per SM, 2.70 ms at 6).
 template <typename QuadT, bool PREC, bool SKIP, bool RECT = false, bool PIPE = SKIP && !PREC, typename Prefix>
 __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __restrict__ quads, const float4* T0,
                                              const float4* T1, const float4* T2, const float* s_a,

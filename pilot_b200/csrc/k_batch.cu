@@ -14,10 +14,9 @@
 //
 // The split variant runs the same items as two persistent launches, all map
 // items and then all view items (MODE 1 and 2; stream order replaces the
-// waits). The fused kernel holds the registers of both marches (80, three
-// blocks per SM); each split kernel holds only its own march's and runs four
-// blocks per SM, which pays when the requests are large enough to fill the GPU
-// on their own.
+// waits). The fused kernel holds the registers of both marches; it runs four
+// blocks per SM like the split kernels by marching light rays one sample at a
+// time (see below).
 //
 // Per item a block keeps the request's geometry and cell tables in shared
 // memory (recomputed there when the request changes, so no table buffers or
@@ -54,8 +53,14 @@ __device__ __forceinline__ int find_request(const int* off, int n, int item) {
 }
 
 // MODE 0: map and view items in one launch; 1: map items only; 2: view items only.
+// Four blocks per SM in every mode. The one-launch kernel (MODE 0) holds both
+// marches' registers, so its light march issues one sample at a time (no
+// two-sample pipeline, which it would otherwise use with SKIP): 64 registers,
+// 8 bytes of spills with SKIP. On 64 mixed requests that took the one-launch
+// plan from 98.0 ms (three blocks per SM, the pipelined skipping march) to
+// 86.7 ms, below one render at a time (88.1 ms).
 template <bool SKIP, int MODE>
-__global__ void __launch_bounds__(kBatchThreads, MODE == 0 ? 3 : 4) k_batch(const ExactGeo* __restrict__ geos,
+__global__ void __launch_bounds__(kBatchThreads, 4) k_batch(const ExactGeo* __restrict__ geos,
                                                             const BatchDesc* __restrict__ descs,
                                                             const BatchPlan* __restrict__ pl,
                                                             const float4* __restrict__ tf,
@@ -142,7 +147,7 @@ __global__ void __launch_bounds__(kBatchThreads, MODE == 0 ? 3 : 4) k_batch(cons
           light_origin(sg, V, L);
           Accum<false> acc;
           unsigned ns = 0;
-          march_vertex<float4, false, SKIP>(sg, sd.quads, s_tab + sg.ax_off[0], s_tab + sg.ax_off[1],
+          march_vertex<float4, false, SKIP, false, SKIP && MODE != 0>(sg, sd.quads, s_tab + sg.ax_off[0], s_tab + sg.ax_off[1],
                                             s_tab + sg.ax_off[2], s_a, nullptr, sd.occ, V, L,
                                             [](const float*) { return 0.f; }, acc, ns);
           acc.store(sd.map, id);

@@ -145,16 +145,18 @@ __device__ __forceinline__ void tma_load_tile(uint32_t dst, const CUtensorMap* m
   for (int j = 0; j < kIn / 8; ++j) tma_load_chunk(dst + j * kTile * 16, map, j * 8, row, bar);
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t addr, float v[16]) {
-  uint32_t r[16];
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, float v[32]) {
+  uint32_t r[32];
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
       : "r"(addr));
 #pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
@@ -206,24 +208,34 @@ __device__ __forceinline__ void issue_fwd(uint32_t d, uint32_t a, uint32_t wbase
 }
 
 // Epilogue of a hidden layer for the calling thread's row r and 32 columns
-// c0..c0+31: h = bf16(relu(acc + bias)), written as the chunked operand out.
+// c0..c0+31: bf16(relu(acc + bias)), written as the chunked operand out when
+// out is non-null; with want_h, h receives those bf16 values as floats (the
+// head and the backward's ReLU mask read them). Each pair is rounded and packed
+// once, and ReLU runs on the packed pair: max(round(x), 0) = round(max(x, 0))
+// for every x (rounding keeps the sign; NaN gives 0 either way).
 __device__ __forceinline__ void hidden_epilogue(uint32_t tmem_acc, const float* bias, int r, int c0, float h[32],
-                                                unsigned char* out) {
-  tmem_ld16(tmem_acc + c0, h);
-  tmem_ld16(tmem_acc + c0 + 16, h + 16);
+                                                unsigned char* out, bool want_h = true) {
+  tmem_ld32(tmem_acc + c0, h);
   tmem_wait_ld();
+  uint32_t w[16];
+  const __nv_bfloat162 zero = __float2bfloat162_rn(0.f);
 #pragma unroll
-  for (int j = 0; j < 32; ++j) h[j] = bf16r(fmaxf(h[j] + bias[c0 + j], 0.f));
+  for (int j = 0; j < 16; ++j) {
+    const __nv_bfloat162 b2 =
+        __hmax2(__floats2bfloat162_rn(h[2 * j] + bias[c0 + 2 * j], h[2 * j + 1] + bias[c0 + 2 * j + 1]), zero);
+    w[j] = *reinterpret_cast<const uint32_t*>(&b2);
+  }
   if (out) {
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      uint32_t w[4];
+    for (int c = 0; c < 4; ++c)
+      *reinterpret_cast<uint4*>(out + ch_off(kTile, r, c0 + c * 8)) =
+          make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
+  }
+  if (want_h) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const __nv_bfloat162 b2 = __floats2bfloat162_rn(h[c * 8 + 2 * j], h[c * 8 + 2 * j + 1]);
-        w[j] = *reinterpret_cast<const uint32_t*>(&b2);
-      }
-      *reinterpret_cast<uint4*>(out + ch_off(kTile, r, c0 + c * 8)) = make_uint4(w[0], w[1], w[2], w[3]);
+    for (int j = 0; j < 16; ++j) {
+      h[2 * j] = __uint_as_float(w[j] << 16);
+      h[2 * j + 1] = __uint_as_float(w[j] & 0xffff0000u);
     }
   }
 }
@@ -346,9 +358,9 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd_tc(const __grid_cons
         load_pending = true;
       }
       // two halves of the row in turn (32 live accumulator values per thread)
-      hidden_epilogue(tmem_acc, aux + l * kHid, r, 0, h, l < 3 ? H : nullptr);
+      hidden_epilogue(tmem_acc, aux + l * kHid, r, 0, h, l < 3 ? H : nullptr, l == 3);
       if (l == 3) p0 = head_partial(h, aux + 4 * kHid, 0);
-      hidden_epilogue(tmem_acc, aux + l * kHid, r, 32, h, l < 3 ? H : nullptr);
+      hidden_epilogue(tmem_acc, aux + l * kHid, r, 32, h, l < 3 ? H : nullptr, l == 3);
       if (l == 3) p1 = head_partial(h, aux + 4 * kHid, 32);
       fence_async_smem();
       tc_fence_before();
@@ -460,7 +472,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train_tc(const __grid_const
         break;
       }
       tc_fence_after();
-      hidden_epilogue(tmem + kColFwd + lanes, aux + l * kHid, r, c0, h, H[l]);
+      hidden_epilogue(tmem + kColFwd + lanes, aux + l * kHid, r, c0, h, H[l], l == 3);
       if (l == 3) part[hf * kTile + r] = head_partial(h, aux + 4 * kHid, c0);
       fence_async_smem();
       tc_fence_before();
@@ -540,8 +552,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train_tc(const __grid_const
       if (l == 0) break;
       tc_fence_after();
       float dx[32];
-      tmem_ld16(tmem + kColDg + lanes + c0, dx);
-      tmem_ld16(tmem + kColDg + lanes + c0 + 16, dx + 16);
+      tmem_ld32(tmem + kColDg + lanes + c0, dx);
       tmem_wait_ld();
       const unsigned char* in = H[l - 1];
 #pragma unroll
@@ -577,8 +588,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train_tc(const __grid_const
     const int oW[4] = {oW1, oW2, oW3, oW4}, Ks[4] = {kIn, kHid, kHid, kHid}, oB[4] = {oB1, oB2, oB3, oB4};
     for (int l = 0; l < 4; ++l) {
       float v[32];
-      tmem_ld16(tmem + kColWg + 64u * (uint32_t)l + lanes + c0, v);
-      tmem_ld16(tmem + kColWg + 64u * (uint32_t)l + lanes + c0 + 16, v + 16);
+      tmem_ld32(tmem + kColWg + 64u * (uint32_t)l + lanes + c0, v);
       tmem_wait_ld();
       if (r < Ks[l]) {
         float* g = G + oW[l] + r * kHid + c0;

@@ -8,7 +8,10 @@ reference behaviours the oracle restates:
     (LightedVolumeRenderer.cxx:464-481), so a constant field gives
     C.a = 1 - (1-a)^k after k samples;
   * the slab test returns the analytic entry/exit (LightedVolumeRenderer.cxx:644-718);
-  * the TF index truncates (LightedVolumeRenderer.cxx:453-454).
+  * the TF index truncates (LightedVolumeRenderer.cxx:453-454);
+  * the cell-field march (LightedVolumeRenderer.cxx:501-642) composites one
+    clamped TF entry per cell, breaks right after the composite that reaches
+    the cut-off and clamps the result to 1.
 """
 import numpy as np
 import pytest
@@ -278,3 +281,46 @@ def test_stretched_coordinates_move_the_samples():
     m, _ = Oracle(s).light_march()
     assert not np.array_equal(m, base_m)
     assert np.all((m >= 0) & (m <= 1))
+
+
+def test_cell_field_constant_closed_form():
+    """SamplerCellAssoc (LightedVolumeRenderer.cxx:501-642) on a constant cell
+    field: every sample composites the same TF entry, so C.a = 1 - (1 - A)^k
+    and rgb = tf_rgb * C.a after k samples, with k equal to the composites
+    counted, and the clamped index takes the first / last entry for values
+    below / above the range."""
+    s = const_scene(use_map=False, image=12)
+    n = s.dims[0]
+    for value, idx in ((0.45, int(np.float32(0.45) * np.float32(255))), (-3.0, 0), (7.5, 255)):
+        cells = np.full((n - 1, n - 1, n - 1), value, np.float32)
+        o = Oracle(s, field=cells)
+        img, lit = o.view_march_cells(fp64=True)
+        A = float(s.tf[idx, 3])
+        alpha = img[..., 3]
+        if A == 0.0:
+            assert np.all(img == 0) and lit > 0
+            continue
+        assert np.allclose(img[..., :3], s.tf[idx, :3][None, None, :] * alpha[..., None], atol=1e-9)
+        if A > 0.5:  # (1 - A)^k underflows double precision's distance from 1 within a few dozen samples
+            assert np.all(alpha[alpha > 0] > 1 - 1e-9)
+            continue
+        k = np.log1p(-alpha) / np.log1p(-A)
+        assert np.allclose(k, np.round(k), atol=1e-6)
+        assert int(np.round(k).sum()) == lit  # one composite per counted sample
+
+
+def test_cell_field_break_before_update_and_final_clamp():
+    """The cell march breaks on C.a >= cutoff right after compositing (no
+    further sample), and clamps every channel to 1 at the end: an opaque entry
+    (A = 1) stops each ray after exactly one composite."""
+    s = const_scene(use_map=False, image=10, cutoff=1.0)
+    s.tf = s.tf.copy()
+    s.tf[:, 3] = 1.0
+    s.tf[:, :3] = 2.0  # colours above 1: the final clamp caps them
+    n = s.dims[0]
+    cells = np.full((n - 1, n - 1, n - 1), 0.5, np.float32)
+    o = Oracle(s, field=cells)
+    img, lit = o.view_march_cells()
+    hit = img[..., 3] > 0
+    assert lit == int(hit.sum())
+    assert np.all(img[hit] == 1.0)

@@ -138,6 +138,12 @@ beams_status beams_add_directional_light(beams_renderer* r, const double dir[3],
  * LightedVolumeRenderer::SetSampleDistance (LightedVolumeRenderer.cxx:1374-1379).
  * d <= 0 returns BEAMS_ERR_INVALID_ARG, where the reference throws. */
 beams_status beams_set_sample_distance(beams_renderer* r, float d);
+/* Replaces MapperLightedVolume::SetDensityScale (MapperLightedVolume.h:51,
+ * MapperLightedVolume.cxx:86-89), which stores the value in the renderer
+ * (LightedVolumeRenderer.h:71) where nothing reads it: stored here the same way,
+ * with no effect on the image; beams_get_density_scale reads it back. */
+beams_status beams_set_density_scale(beams_renderer* r, float scale);
+beams_status beams_get_density_scale(const beams_renderer* r, float* scale);
 /* Early-termination threshold on accumulated alpha. The reference breaks at
  * alpha >= 1.0 (LightedVolumeRenderer.cxx:491-492); 1.0 is the default. */
 beams_status beams_set_termination_alpha(beams_renderer* r, float alpha);

@@ -84,7 +84,7 @@ class MapperLightedVolume {
     if (depth.size() != (size_t)width * height) throw Error(BEAMS_ERR_INVALID_ARG, "depth buffer size");
     check(beams_set_depth_buffer(r_, depth.data(), width, height, BEAMS_DEPTH_WINDOW, near_plane, far_plane, 0), r_);
   }
-  void SetDensityScale(float s) { density_scale_ = s; }  // stored, never read (as in the reference)
+  void SetDensityScale(float s) { check(beams_set_density_scale(r_, s), r_); }  // stored, never read (as in the reference)
   // SetActiveColorTable: the colour table already sampled to RGBA entries.
   void SetActiveColorTable(const std::vector<float>& rgba) {
     if (rgba.empty() || rgba.size() % 4 != 0) throw Error(BEAMS_ERR_INVALID_ARG, "colour table must be RGBA");
@@ -132,7 +132,6 @@ class MapperLightedVolume {
   beams_renderer* r_ = nullptr;
   int width_ = 0, height_ = 0;
   float sample_distance_ = -1.f;
-  float density_scale_ = 1.f;
   std::vector<float> color_map_;
 };
 

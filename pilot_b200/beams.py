@@ -174,6 +174,8 @@ def lib():
         "beams_add_directional_light": ([P, P, P, C.c_float], C.c_int),
         "beams_set_sample_distance": ([P, C.c_float], C.c_int),
         "beams_set_termination_alpha": ([P, C.c_float], C.c_int),
+        "beams_set_density_scale": ([P, C.c_float], C.c_int),
+        "beams_get_density_scale": ([P, P], C.c_int),
         "beams_set_light_steps": ([P, C.c_float], C.c_int),
         "beams_set_slab_fp64": ([P, C.c_int], C.c_int),
         "beams_set_reuse_shadow_map": ([P, C.c_int], C.c_int),
@@ -500,6 +502,15 @@ class Renderer:
     def set_sample_distance(self, d):
         self._check(self._L.beams_set_sample_distance(self._h, float(d)))
 
+    def set_density_scale(self, scale):
+        """MapperLightedVolume::SetDensityScale: stored, no effect on the image (as in the reference)."""
+        self._check(self._L.beams_set_density_scale(self._h, float(scale)))
+
+    def get_density_scale(self):
+        v = C.c_float()
+        self._check(self._L.beams_get_density_scale(self._h, C.byref(v)))
+        return v.value
+
     def set_termination_alpha(self, a):
         self._check(self._L.beams_set_termination_alpha(self._h, float(a)))
 
@@ -687,7 +698,7 @@ class MapperLightedVolume:
         self._r.set_background(on, rgba)
 
     def SetDensityScale(self, s: float):
-        self._density_scale = float(s)  # stored, never read (as in the reference)
+        self._r.set_density_scale(s)  # stored, never read (as in the reference)
 
     def SetActiveColorTable(self, rgba_table):
         self._color_map = np.asarray(rgba_table, np.float32).reshape(-1, 4)

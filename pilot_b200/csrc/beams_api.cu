@@ -900,6 +900,18 @@ beams_status beams_set_sample_distance(beams_renderer* r, float d) {
   return BEAMS_OK;
 }
 
+beams_status beams_set_density_scale(beams_renderer* r, float scale) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  r->density_scale = scale;
+  return BEAMS_OK;
+}
+
+beams_status beams_get_density_scale(const beams_renderer* r, float* scale) {
+  if (!r || !scale) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "get_density_scale: NULL argument");
+  *scale = r->density_scale;
+  return BEAMS_OK;
+}
+
 beams_status beams_set_termination_alpha(beams_renderer* r, float a) {
   if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
   if (!(a > 0.f) || !std::isfinite(a)) return fail(r, BEAMS_ERR_INVALID_ARG, "termination alpha must be positive");

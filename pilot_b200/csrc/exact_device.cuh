@@ -222,6 +222,19 @@ __device__ __forceinline__ int find_cell_bsearch_t(const float4* T, int cmax, fl
   return c;
 }
 
+// The same search for a sample already inside the volume: val >= org exactly
+// (org is the volume's first coordinate), so the guess needs no lower clamp.
+__device__ __forceinline__ int find_cell_bsearch_in(const float4* T, int cmax, float org, float invh, float val,
+                                                    float4& e) {
+  int c = trunc_small(fminf((val - org) * invh, (float)cmax));
+  e = T[c];
+  if (val <= e.x || val > e.y) {
+    while (c > 0 && val <= e.x) e = T[--c];
+    while (c < cmax && val > e.y) e = T[++c];
+  }
+  return c;
+}
+
 // Searches for explicit (non-uniform) rectilinear coordinates, where no seed
 // from a uniform spacing is close: the light march's binary search
 // (RectilinearMeshOracle.h:154-176, smallest c with val <= coord(c+1)) and the

@@ -99,6 +99,7 @@ struct beams_renderer {
   bool use_map = true;
   float sample_distance = -1.f;
   float cutoff = 1.f;
+  float density_scale = 1.f;  // SetDensityScale: stored, never read (as in the reference)
   float light_steps = 128.f;
   int slab_fp64 = 1;
   int light_brick_log2 = 3;  // beams_set_tuning (8^3-vertex bricks)

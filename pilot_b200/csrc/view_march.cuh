@@ -43,7 +43,7 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT*
   if (!ray_setup(g, x, y, o, d, minD, maxD)) return;
   hit += 1;
   const float qd = (maxD - minD) / g.sd;
-  long long budget = (qd < 1e9f) ? (long long)qd + 16 : 1000000000ll;
+  int budget = (qd < 1e9f) ? (int)qd + 16 : 1000000000;  // qd <= 1e6: the sample distance is checked on the host
   float dist = minD + g.mesh_eps;
   float p[3] = {o[0] + dist * d[0], o[1] + dist * d[1], o[2] + dist * d[2]};
   while (!inside_vol(g, p) && dist < maxD && budget-- > 0) {

@@ -327,3 +327,14 @@ def test_non_cubic_map(cuda_device):
     assert np.max(np.abs(img - oimg)) <= TOL
     assert np.mean(np.all(img == oimg, axis=-1)) > 0.999
     assert t["lit_samples"] == olit
+
+
+def test_density_scale_is_stored_and_changes_nothing(cuda_device):
+    """SetDensityScale (MapperLightedVolume.cxx:86-89) stores a value nothing reads."""
+    s = scenes.small(6, n=24, image=40, m=8)
+    img, _, _, r = gpu_render(s)
+    r.set_density_scale(3.5)
+    assert r.get_density_scale() == 3.5
+    img2, _ = r.render(s.camera())
+    assert np.array_equal(img, img2)
+    r.close()

@@ -379,6 +379,14 @@ beams_status beams_mlp_forward_tc_device(beams_renderer* r, const void* features
 /* 1 (default): training and beams_mlp_loss_grad run the hidden layers on the
  * tcgen05 tensor cores; 0: on the CUDA cores (the reference path for tests). */
 beams_status beams_mlp_set_tensor_cores(beams_renderer* r, int enable);
+/* Order of a BEAMS_FORM_MLP frame. 0: the network shades every pixel (recording
+ * the probe pixels), the probe check follows, and the failing tiles are
+ * rendered again from the exact map. 1: the network shades the probe pixels
+ * first, the check runs, and the network then shades only the tiles that
+ * passed. The images are the same; 1 is faster when many tiles fail. -1
+ * (default): 1 when more than 1/8 of the tiles failed in the last learned frame
+ * whose count has reached the host (read without waiting), else 0. */
+beams_status beams_mlp_set_probe_first(beams_renderer* r, int mode);
 /* The network's input encoding of n world positions under n light features. */
 beams_status beams_mlp_encode(beams_renderer* r, const float* pos, const float* lfeat, int n, float* out);
 /* Versioned checkpoint of parameters and Adam moments (FNV-1a checksummed). */

@@ -197,6 +197,7 @@ def lib():
         "beams_mlp_probe_errors": ([P, P, C.c_int], C.c_int),
         "beams_mlp_forward_tc": ([P, P, C.c_int, P], C.c_int),
         "beams_mlp_set_tensor_cores": ([P, C.c_int], C.c_int),
+        "beams_mlp_set_probe_first": ([P, C.c_int], C.c_int),
         "beams_mlp_forward_tc_device": ([P, P, C.c_int, P], C.c_int),
         "beams_set_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "beams_set_multi_light": ([P, C.c_int], C.c_int),
@@ -466,6 +467,10 @@ class Renderer:
 
     def mlp_set_tensor_cores(self, enable: bool):
         self._check(self._L.beams_mlp_set_tensor_cores(self._h, int(bool(enable))))
+
+    def mlp_set_probe_first(self, mode: int):
+        """Learned-frame order: 1 probe pixels first, 0 network first, -1 chosen per frame."""
+        self._check(self._L.beams_mlp_set_probe_first(self._h, int(mode)))
 
     def mlp_probe_errors(self, n):
         out = np.empty(n, np.float32)

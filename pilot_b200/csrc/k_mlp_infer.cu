@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
                                                            const float* __restrict__ aux, Encoding enc,
                                                            float lf0, float lf1, float lf2, int knot,
                                                            float4* __restrict__ out, Counters* __restrict__ cnt,
-                                                           MlpProbe probe) {
+                                                           MlpProbe probe, MlpPass pass) {
   extern __shared__ float4 s_dyn[];
   const int nfield = g.max_off[0];
   float4* s_tab = s_dyn;
@@ -236,13 +236,26 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
   __syncthreads();
   const float lf[3] = {lf0, lf1, lf2};
   const int tiles_x = (g.width + 7) >> 3;
-  const int ntiles = tiles_x * ((g.height + 3) >> 2);
+  const int nprobe = probe.nqx * probe.nqy;
+  const int ntiles = pass.probes_only ? (nprobe + 31) >> 5 : tiles_x * ((g.height + 3) >> 2);
   const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
   const int n1 = g.tf_n - 1;
   unsigned lit = 0, hit = 0, evals = 0, rows = 0;
   for (int tile = next_warp_tile_mlp(&cnt->tiles_view); tile < ntiles; tile = next_warp_tile_mlp(&cnt->tiles_view)) {
     const int lane = threadIdx.x & 31;
-    const int x = (tile % tiles_x) * 8 + (lane & 7), y = (tile / tiles_x) * 4 + (lane >> 3);
+    int x, y;
+    if (pass.probes_only) {
+      // probe q = 32 tile + lane; lanes past the grid get no pixel
+      const int q = tile * 32 + lane;
+      x = q < nprobe ? (q % probe.nqx) * probe.P + probe.h : g.width;
+      y = q < nprobe ? (q / probe.nqx) * probe.P + probe.h : g.height;
+    } else {
+      const int x0 = (tile % tiles_x) * 8, y0 = (tile / tiles_x) * 4;
+      // an 8x4 tile lies inside one fallback tile: the exact path renders it
+      if (pass.skip && pass.skip[(y0 / kFallbackTile) * pass.ftx + x0 / kFallbackTile] != 0u) continue;
+      x = x0 + (lane & 7);
+      y = y0 + (lane >> 3);
+    }
     // a probe pixel records its compositing samples for the exact-march check
     const bool is_probe = probe.P > 0 && x < g.width && y < g.height && x % probe.P == probe.h &&
                           y % probe.P == probe.h && x / probe.P < probe.nqx && y / probe.P < probe.nqy;
@@ -382,8 +395,10 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
     if (x < g.width && y < g.height) out[(size_t)y * g.width + x] = color;
     if (is_probe) probe.count[(y / probe.P) * probe.nqx + x / probe.P] = pn;
   }
-  warp_add(&cnt->lit_samples, lit);
-  warp_add(&cnt->rays_hit, hit);
+  if (!pass.probes_only) {
+    warp_add(&cnt->lit_samples, lit);
+    warp_add(&cnt->rays_hit, hit);
+  }
   warp_add(&cnt->mlp_samples, evals);
   if ((threadIdx.x & 31) == 0 && rows) atomicAdd(&cnt->mlp_rows, (unsigned long long)rows);
 }
@@ -397,8 +412,10 @@ size_t mlp_packed_bytes() { return (size_t)kPacked * sizeof(uint2) + (size_t)kAu
 
 cudaError_t launch_view_march_mlp(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                   const uint2* W, const float* aux, const Encoding& enc, const float lf[3], int knot,
-                                  float4* out, Counters* cnt, const MlpProbe& probe, cudaStream_t st) {
+                                  float4* out, Counters* cnt, const MlpProbe& probe, const MlpPass& pass,
+                                  cudaStream_t st) {
   if (knot < 1 || knot > kKnotMax) return cudaErrorInvalidValue;
+  if (pass.probes_only && (probe.P < 1 || !probe.rec || !probe.count)) return cudaErrorInvalidValue;
   const size_t smem = (size_t)g.max_off[0] * sizeof(float4) + (size_t)g.tf_n * sizeof(float4) +
                       (size_t)kPacked * sizeof(uint2) + (size_t)((kAux + 3) & ~3) * sizeof(float) +
                       (size_t)8 * kKnotMax * 32 * sizeof(unsigned short);
@@ -411,12 +428,13 @@ cudaError_t launch_view_march_mlp(const ExactGeo& g, const float4* quads, const 
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int ntiles = ((g.width + 7) >> 3) * ((g.height + 3) >> 2);
+  const int ntiles = pass.probes_only ? (probe.nqx * probe.nqy + 31) / 32 : ((g.width + 7) >> 3) * ((g.height + 3) >> 2);
   int grid = sms * per_sm;
   const int need = (ntiles + 7) / 8;
   if (grid > need) grid = need;
+  if (grid < 1) return cudaSuccess;
   k_view_march_mlp<float4><<<grid, 256, smem, st>>>(g, quads, tab, tf, W, aux, enc, lf[0], lf[1], lf[2], knot, out,
-                                                    cnt, probe);
+                                                    cnt, probe, pass);
   return cudaGetLastError();
 }
 

@@ -203,8 +203,13 @@ struct VertexMarker {
   }
 };
 
-__global__ void k_clear_mask_gated(const unsigned* __restrict__ fcount, uint4* __restrict__ mask, size_t n16) {
-  if (*fcount == 0u) return;
+// Also copies the list's length to host-mapped memory (when given) for the
+// host's choice of order in the next frame.
+__global__ void k_clear_mask_gated(const unsigned* __restrict__ fcount, uint4* __restrict__ mask, size_t n16,
+                                   volatile unsigned* host_count) {
+  const unsigned nf = *fcount;
+  if (host_count && blockIdx.x == 0 && threadIdx.x == 0) *host_count = nf;
+  if (nf == 0u) return;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n16; i += (size_t)gridDim.x * blockDim.x)
     mask[i] = make_uint4(0u, 0u, 0u, 0u);
 }
@@ -254,9 +259,9 @@ int grid_for(size_t n, int threads, int cap_blocks) {
 
 cudaError_t launch_mark_fallback_vertices(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                           const unsigned* flist, const unsigned* fcount, unsigned char* vmask,
-                                          size_t mask_bytes, cudaStream_t st) {
+                                          size_t mask_bytes, unsigned* host_count, cudaStream_t st) {
   if (mask_bytes % 16 != 0) return cudaErrorInvalidValue;
-  k_clear_mask_gated<<<148 * 4, 256, 0, st>>>(fcount, (uint4*)vmask, mask_bytes / 16);
+  k_clear_mask_gated<<<148 * 4, 256, 0, st>>>(fcount, (uint4*)vmask, mask_bytes / 16, host_count);
   const size_t smem = ((size_t)g.ntab + (size_t)g.tf_n) * sizeof(float4);
   cudaError_t e = cudaFuncSetAttribute(k_mark_fallback, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

@@ -25,13 +25,14 @@ cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const
 void occupancy_dims(const int n[3], int occ_n[3]);
 cudaError_t launch_build_occupancy(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tf,
                                    unsigned char* occ, cudaStream_t st);
-// K2 over a device list of kFallbackTile^2 pixel tiles (count in *fcount), with the map.
 // Learned form's lazy fallback (k_mlp_probe.cu): when the list of failing tiles
 // is non-empty, clears the vertex mask (nvert bytes, 16-byte multiple) and marks
-// the map vertices that the listed tiles' view rays read.
+// the map vertices that the listed tiles' view rays read. host_count (host-mapped
+// memory, or null) receives the list's length.
 cudaError_t launch_mark_fallback_vertices(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                           const unsigned* flist, const unsigned* fcount, unsigned char* vmask,
-                                          size_t mask_bytes, cudaStream_t st);
+                                          size_t mask_bytes, unsigned* host_count, cudaStream_t st);
+// K2 over a device list of kFallbackTile^2 pixel tiles (count in *fcount), with the map.
 cudaError_t launch_view_march_tiles(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                     const float* map, float4* out, Counters* cnt, const unsigned* flist,
                                     const unsigned* fcount, cudaStream_t st);
@@ -47,6 +48,16 @@ struct MlpProbe {
   int P, h, nqx, nqy, cap;
   float4* rec;
   int* count;
+};
+// Which pixels one network view march shades: every 8x4 warp tile; or the warp
+// tiles outside the kFallbackTile^2 tiles already flagged for the exact path
+// (skip = the probe check's flags, ftx tiles per row); or the probe pixels
+// only, 32 per warp (probes_only; their lit samples are not counted, the
+// later pass or the fallback renders their tiles again).
+struct MlpPass {
+  const unsigned* skip;
+  int ftx;
+  int probes_only;
 };
 ProbeLayout probe_layout(int width, int height, float fraction);
 // recorded: the network's view march already recorded the probe samples (no probe march).

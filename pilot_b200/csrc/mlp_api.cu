@@ -47,10 +47,18 @@ struct MlpState {
   beams_mlp_options render_opts{};
   bool use_tc = true;            // training forward on the tcgen05 tensor cores
   unsigned* err_slot = nullptr;  // their timeout flag in the workspace
+  // Frame order: -1 chosen from the last frame's fallback fraction, 0 network
+  // march first, 1 probe pixels first (the images are the same).
+  int probe_first = -1;
+  // Host-mapped, written by the fallback's first kernel: the failing-tile count
+  // of the last learned frame that has got that far, and that frame's tile count.
+  volatile unsigned* h_fallback = nullptr;
+  int fb_tiles = 0;
   ~MlpState() {
     for (void* p : {(void*)P, (void*)G, (void*)m, (void*)v, ws_mem, (void*)lights, (void*)lfeat, packed, probe_mem,
                     (void*)probe_err, (void*)vmask})
       if (p) cudaFree(p);
+    if (h_fallback) cudaFreeHost((void*)h_fallback);
   }
 };
 
@@ -145,7 +153,8 @@ static void init_params(std::vector<float>& h, unsigned seed) {
 
 cudaError_t launch_view_march_mlp(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                   const uint2* W, const float* aux, const Encoding& enc, const float lf[3], int knot,
-                                  float4* out, Counters* cnt, const MlpProbe& probe, cudaStream_t st);
+                                  float4* out, Counters* cnt, const MlpProbe& probe, const MlpPass& pass,
+                                  cudaStream_t st);
 
 bool mlp_ready(const beams_renderer* r) { return r->mlp && r->mlp->ready; }
 
@@ -208,22 +217,32 @@ static beams_status probe_buffers(beams_renderer* r, const ExactGeo& g, ProbeBuf
   return BEAMS_OK;
 }
 
-// Probe pixels against the exact light march, then the exact map path over the
-// tiles that failed, built lazily: the map vertices the listed tiles' view rays
-// read are marked, K1 marches only those (both gated on a non-empty list), K2
-// re-renders the listed tiles. The network's view march has already recorded
-// the probe pixels' samples. Nothing here waits on the host.
-static beams_status mlp_probe_and_fallback(beams_renderer* r, const ExactGeo& g, const ProbeBuffers& pb, float4* out,
-                                           int& launches) {
+// Probe pixels against the exact light march: the tiles that fail are flagged
+// and listed. A network view march has already shaded the probe pixels and
+// recorded their samples.
+static beams_status mlp_probe_check(beams_renderer* r, const ExactGeo& g, const ProbeBuffers& pb, float4* out,
+                                    int& launches) {
   MlpState* st = r->mlp;
   const ProbeLayout& L = pb.L;
-  if (L.stride == 0) return BEAMS_OK;  // probe fraction 0: the network's image stands
   cudaError_t e = cudaMemsetAsync(pb.flags, 0, ((size_t)L.ntiles + 1) * sizeof(unsigned), r->stream);
   if (e == cudaSuccess)
     e = launch_mlp_probe(g, L, (const float4*)r->d_quads, r->d_tab, r->d_tf, out, st->render_opts.fallback_tol, pb.rec,
                          pb.count, pb.flags, pb.flist, pb.fcount, st->probe_err, r->d_cnt, r->stream, true);
   if (e != cudaSuccess) return cuda_fail(r, e, "mlp probe launch");
-  launches += L.nprobe > 0 ? 2 : 1;
+  ++launches;
+  return BEAMS_OK;
+}
+
+// The exact map path over the listed tiles, built lazily: the map vertices the
+// listed tiles' view rays read are marked, K1 marches only those (both gated on
+// a non-empty list), K2 re-renders the listed tiles. Nothing here waits on the
+// host; the list's length is copied to pinned memory for the next frame's
+// choice of order.
+static beams_status mlp_fallback(beams_renderer* r, const ExactGeo& g, const ProbeBuffers& pb, float4* out,
+                                 int& launches) {
+  MlpState* st = r->mlp;
+  const ProbeLayout& L = pb.L;
+  cudaError_t e;
   const size_t nvert = (size_t)g.pd[0] * g.pd[1] * g.pd[2];
   beams_status s = ensure_buffer(r, (void**)&r->d_map, &r->map_cap, nvert * sizeof(float), "allocating map");
   if (s != BEAMS_OK) return s;
@@ -232,8 +251,16 @@ static beams_status mlp_probe_and_fallback(beams_renderer* r, const ExactGeo& g,
   const size_t mask_bytes = (nvert + 15) & ~(size_t)15;
   s = ensure_buffer(r, (void**)&st->vmask, &st->vmask_bytes, mask_bytes, "allocating the fallback vertex mask");
   if (s != BEAMS_OK) return s;
+  if (!st->h_fallback) {
+    unsigned* h = nullptr;
+    e = cudaHostAlloc((void**)&h, sizeof(unsigned), cudaHostAllocMapped);
+    if (e != cudaSuccess) return cuda_fail(r, e, "allocating the fallback count");
+    *h = 0u;
+    st->h_fallback = h;
+  }
+  st->fb_tiles = L.ntiles;
   e = launch_mark_fallback_vertices(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, pb.flist, pb.fcount, st->vmask,
-                                    mask_bytes, r->stream);
+                                    mask_bytes, (unsigned*)st->h_fallback, r->stream);
   if (e == cudaSuccess)
     e = launch_light_march_f32(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map, r->d_cnt, r->stream,
                                nullptr, 0, -1, pb.fcount, nullptr, st->vmask);
@@ -243,6 +270,18 @@ static beams_status mlp_probe_and_fallback(beams_renderer* r, const ExactGeo& g,
   if (e != cudaSuccess) return cuda_fail(r, e, "mlp fallback launch");
   launches += 4;
   return BEAMS_OK;
+}
+
+// Probe pixels first pays when many tiles fall back: the network then shades
+// only the tiles that passed. Chosen from the last learned frame whose count
+// has reached the host (read without waiting); the first frame marches the
+// network first.
+constexpr float kProbeFirstFraction = 0.125f;
+
+static bool choose_probe_first(const MlpState* st) {
+  if (st->probe_first >= 0) return st->probe_first == 1;
+  if (!st->h_fallback || st->fb_tiles <= 0) return false;
+  return (float)*st->h_fallback > kProbeFirstFraction * (float)st->fb_tiles;
 }
 
 // The view march shaded by the network (no map is built).
@@ -263,14 +302,39 @@ beams_status mlp_render_view(beams_renderer* r, const ExactGeo& g, float4* out, 
   ProbeBuffers pb;
   beams_status s = probe_buffers(r, g, pb);
   if (s != BEAMS_OK) return s;
-  MlpProbe probe{0, 0, 0, 0, 0, nullptr, nullptr};
+  const MlpProbe none{0, 0, 0, 0, 0, nullptr, nullptr};
+  MlpProbe probe = none;
   if (pb.L.stride > 0 && pb.L.nprobe > 0)
     probe = MlpProbe{pb.L.stride, pb.L.offset, pb.L.nqx, pb.L.nqy, pb.L.cap, pb.rec, pb.count};
-  e = launch_view_march_mlp(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, W, aux, mlp_encoding(g), lf,
-                            st->render_opts.knot, out, r->d_cnt, probe, r->stream);
+  const Encoding enc = mlp_encoding(g);
+  const int knot = st->render_opts.knot;
+  const float4* quads = (const float4*)r->d_quads;
+  if (probe.P > 0 && choose_probe_first(st)) {
+    // probe pixels, their check, then the network over the tiles that passed
+    e = launch_view_march_mlp(g, quads, r->d_tab, r->d_tf, W, aux, enc, lf, knot, out, r->d_cnt, probe,
+                              MlpPass{nullptr, 0, 1}, r->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&r->d_cnt->tiles_view, 0, sizeof(unsigned), r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "mlp probe march launch");
+    ++launches;
+    s = mlp_probe_check(r, g, pb, out, launches);
+    if (s != BEAMS_OK) return s;
+    // the network over the tiles that passed (a side stream beside the exact
+    // path over the failing tiles measured no faster)
+    const int ftx = (g.width + kFallbackTile - 1) / kFallbackTile;
+    e = launch_view_march_mlp(g, quads, r->d_tab, r->d_tf, W, aux, enc, lf, knot, out, r->d_cnt, none,
+                              MlpPass{pb.flags, ftx, 0}, r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "mlp view march launch");
+    ++launches;
+    return mlp_fallback(r, g, pb, out, launches);
+  }
+  e = launch_view_march_mlp(g, quads, r->d_tab, r->d_tf, W, aux, enc, lf, knot, out, r->d_cnt, probe,
+                            MlpPass{nullptr, 0, 0}, r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "mlp view march launch");
   ++launches;
-  return mlp_probe_and_fallback(r, g, pb, out, launches);
+  if (pb.L.stride == 0) return BEAMS_OK;  // probe fraction 0: the network's image stands
+  s = mlp_probe_check(r, g, pb, out, launches);
+  if (s != BEAMS_OK) return s;
+  return mlp_fallback(r, g, pb, out, launches);
 }
 
 }  // namespace beams
@@ -299,6 +363,13 @@ beams_status beams_mlp_set_tensor_cores(beams_renderer* r, int enable) {
   MlpState* st = mlp_state(r);
   st->use_tc = enable != 0;
   st->ws.err = (st->use_tc && st->err_slot) ? st->err_slot : nullptr;
+  return BEAMS_OK;
+}
+
+beams_status beams_mlp_set_probe_first(beams_renderer* r, int mode) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  if (mode < -1 || mode > 1) return fail(r, BEAMS_ERR_INVALID_ARG, "mlp_set_probe_first: mode must be -1, 0 or 1");
+  mlp_state(r)->probe_first = mode;
   return BEAMS_OK;
 }
 

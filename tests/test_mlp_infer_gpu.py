@@ -261,3 +261,56 @@ def test_mlp_lazy_fallback_builds_only_the_failing_tiles_vertices(cuda_device):
         assert 0 < t["map_vertices"] < full
         _check_tiles(img, mlp_img, exact_img, flagged)
     r.close()
+
+
+def test_mlp_probe_first_order_gives_the_same_image(cuda_device):
+    """Probe pixels first (the network then shades only the tiles that passed)
+    and the network first give the same image bit for bit, the same fallback
+    tiles and the same probe errors, at a tolerance where most tiles fail and
+    at one where few do. A 200^2 image: 7 x 7 tiles with a ragged edge, 400
+    probes (the last probe warp half full). The per-frame choice follows the
+    last frame's fallback fraction."""
+    s = scenes.small(67, n=40, image=200, m=24, kind="noise")
+    r = _renderer(s)
+    r.mlp_set_params(smooth_params(12))
+    P = 10
+    n = len(range(P // 2, s.width, P))
+    r.mlp_set_probe_first(0)
+    r.set_form(B.FORM_MLP, B.mlp_options(knot=4, probe_fraction=0.01, fallback_tol=1e30))
+    r.render(s.camera())
+    err = r.mlp_probe_errors(n * n).reshape(n, n)
+    nt = -(-s.width // TILE)
+    tiles = np.full((nt, nt), -np.inf)
+    for j in range(n):
+        for i in range(n):
+            y, x = j * P + P // 2, i * P + P // 2
+            tiles[y // TILE, x // TILE] = max(tiles[y // TILE, x // TILE], err[j, i])
+    rows = {}
+    for q in (0.2, 0.95):
+        tol = float(np.quantile(tiles, q))
+        flagged = int((tiles > tol).sum())
+        out = {}
+        for mode in (0, 1):
+            r.mlp_set_probe_first(mode)
+            r.set_form(B.FORM_MLP, B.mlp_options(knot=4, probe_fraction=0.01, fallback_tol=tol))
+            img, t = r.render(s.camera())
+            out[mode] = (img, t, r.mlp_probe_errors(n * n))
+        print(f"quantile {q}: {flagged} of {tiles.size} tiles fall back; network rows "
+              f"{out[0][1]['mlp_rows']} (network first) vs {out[1][1]['mlp_rows']} (probes first)")
+        assert np.array_equal(out[0][0], out[1][0])
+        assert out[0][1]["fallback_tiles"] == out[1][1]["fallback_tiles"] == flagged > 0
+        assert out[0][1]["map_vertices"] == out[1][1]["map_vertices"]
+        assert np.array_equal(out[0][2], out[1][2])
+        rows[q] = (out[0][1]["mlp_rows"], out[1][1]["mlp_rows"], out[0][0])
+    assert rows[0.2][1] < rows[0.2][0]
+    # chosen per frame from the last frame's failing-tile count (the first auto
+    # frame follows the last frame above, where few tiles failed)
+    r.mlp_set_probe_first(-1)
+    seq = []
+    for q in (0.2, 0.2, 0.95, 0.95):
+        r.set_form(B.FORM_MLP, B.mlp_options(knot=4, probe_fraction=0.01, fallback_tol=float(np.quantile(tiles, q))))
+        img, t = r.render(s.camera())
+        assert np.array_equal(img, rows[q][2])
+        seq.append(t["mlp_rows"])
+    assert seq == [rows[0.2][0], rows[0.2][1], rows[0.95][1], rows[0.95][0]]
+    r.close()

@@ -52,6 +52,21 @@ constexpr int k1_blocks_per_sm() {
   return (STITCH || PREC || SKIP || RECT) ? 4 : 6;
 }
 
+// The learned form's lazy map: vertex (x, y, z) is needed when one of the (up
+// to 8) map cells it is a corner of was marked (one byte per cell, x fastest).
+__device__ __forceinline__ bool vertex_in_marked_cell(const unsigned char* __restrict__ cm, const int pd[3], int x,
+                                                      int y, int z) {
+  const int mx = pd[0] - 1, my = pd[1] - 1, mz = pd[2] - 1;  // cells per axis
+  const int x0 = max(x - 1, 0), x1 = min(x, mx - 1);
+  const int y0 = max(y - 1, 0), y1 = min(y, my - 1);
+  const int z0 = max(z - 1, 0), z1 = min(z, mz - 1);
+  for (int k = z0; k <= z1; ++k)
+    for (int j = y0; j <= y1; ++j)
+      for (int i = x0; i <= x1; ++i)
+        if (__ldg(cm + ((size_t)k * my + j) * mx + i)) return true;
+  return false;
+}
+
 template <typename QuadT, bool STITCH, bool PREC, bool SKIP, bool RECT = false>
 __global__ void __launch_bounds__(kThreads, k1_blocks_per_sm<STITCH, PREC, SKIP, RECT>()) k_light_march(const ExactGeo g, const QuadT* __restrict__ quads,
                                                           const float4* __restrict__ tab,
@@ -64,7 +79,8 @@ __global__ void __launch_bounds__(kThreads, k1_blocks_per_sm<STITCH, PREC, SKIP,
                                                           const unsigned char* __restrict__ occ,
                                                           const unsigned char* __restrict__ vmask) {
   // gate: the learned form's fallback builds the map only when a tile failed its
-  // probes, and (vmask) only the vertices the failing tiles' view rays read
+  // probes, and (vmask: marked map cells) only the vertices the failing tiles'
+  // view rays read
   if (gate && *gate == 0u) return;
   extern __shared__ float4 s_dyn[];
   const int nfield = g.max_off[0];             // field-axis table entries only
@@ -112,15 +128,19 @@ __global__ void __launch_bounds__(kThreads, k1_blocks_per_sm<STITCH, PREC, SKIP,
       const int z = (bz << bl) + (li >> (2 * bl));
       if (x >= g.pd[0] || y >= g.pd[1] || z >= g.pd[2]) continue;
       id = (z * g.pd[1] + y) * g.pd[0] + x;
+      if (vmask && !vertex_in_marked_cell(vmask, g.pd, x, y, z)) continue;
       V[0] = vtx_coord(g, 0, x);
       V[1] = vtx_coord(g, 1, y);
       V[2] = vtx_coord(g, 2, z);
     } else {
       id = (tile << 5) + lane;
       if (id >= nvert) continue;
+      if (vmask) {
+        const int x = id % g.pd[0], yz = id / g.pd[0];
+        if (!vertex_in_marked_cell(vmask, g.pd, x, yz % g.pd[1], yz / g.pd[1])) continue;
+      }
       map_vertex(g, id, V);
     }
-    if (vmask && !vmask[id]) continue;
     ++built;
     light_origin(g, V, L);
     Accum<PREC> acc;

@@ -13,8 +13,8 @@
 //      exceeds the tolerance (or that holds no probe, or a probe past the cap)
 //      joins the fallback list.
 // The host then builds the exact map lazily, only where the listed tiles need
-// it (k_mark_fallback marks the map vertices their view rays read, and K1
-// marches the marked vertices only; both gated on the list being non-empty),
+// it (k_mark_fallback marks the map cells their view rays read, and K1 marches
+// only the vertices of marked cells; both gated on the list being non-empty),
 // and K2 re-renders the listed tiles, so a failing tile is exactly the exact
 // form's pixels.
 // Compiled with -fmad=false like every kernel file.
@@ -172,11 +172,12 @@ __global__ void __launch_bounds__(kThreadsP, 3) k_probe_check(const ExactGeo g, 
   }
 }
 
-// Marks, for every lit sample of a view ray, the 8 vertices of the map cell
-// that the shading looks up (the cell of map_interp_t: truncate
-// min(max((p - origin) / spacing, 0), pd - 2) per axis), skipping repeats of
-// the previous sample's cell.
-struct VertexMarker {
+// Marks, for every lit sample of a view ray, the map cell that the shading
+// looks up (the cell of map_interp_t: truncate min(max((p - origin) / spacing,
+// 0), pd - 2) per axis), one byte per cell, skipping repeats of the previous
+// sample's cell. K1 then builds a vertex when a cell around it is marked
+// (the same vertex set as marking the 8 corners, with one store per cell).
+struct CellMarker {
   float morig[3], minv[3];
   int pd[3];
   unsigned char* mask;
@@ -188,18 +189,11 @@ struct VertexMarker {
       const float t = (p[d] - morig[d]) * minv[d];
       c[d] = trunc_small(fminf(fmaxf(t, 0.f), (float)(pd[d] - 2)));
     }
-    const unsigned px = (unsigned)pd[0], pxy = (unsigned)pd[0] * (unsigned)pd[1];
-    const unsigned id = (unsigned)c[2] * pxy + (unsigned)c[1] * px + (unsigned)c[0];
+    const unsigned mx = (unsigned)(pd[0] - 1), mxy = mx * (unsigned)(pd[1] - 1);
+    const unsigned id = (unsigned)c[2] * mxy + (unsigned)c[1] * mx + (unsigned)c[0];
     if (id == last) return;
     last = id;
     mask[id] = 1;
-    mask[id + 1] = 1;
-    mask[id + px] = 1;
-    mask[id + px + 1] = 1;
-    mask[id + pxy] = 1;
-    mask[id + pxy + 1] = 1;
-    mask[id + pxy + px] = 1;
-    mask[id + pxy + px + 1] = 1;
   }
 };
 
@@ -215,7 +209,7 @@ __global__ void k_clear_mask_gated(const unsigned* __restrict__ fcount, uint4* _
 }
 
 // The listed tiles' view rays (the K2 march without shading: the samples and
-// their order do not depend on the map) mark the vertices they read.
+// their order do not depend on the map) mark the map cells they read.
 __global__ void __launch_bounds__(kThreadsP) k_mark_fallback(const ExactGeo g, const float4* __restrict__ quads,
                                                              const float4* __restrict__ tab,
                                                              const float4* __restrict__ tf,
@@ -239,11 +233,11 @@ __global__ void __launch_bounds__(kThreadsP) k_mark_fallback(const ExactGeo g, c
     const int x = (f % ftx) * kFallbackTile + ((sub & 3) << 3) + (lane & 7);
     const int y = (f / ftx) * kFallbackTile + ((sub >> 2) << 2) + (lane >> 3);
     if (x < g.width && y < g.height) {
-      VertexMarker m{{g.morig[0], g.morig[1], g.morig[2]}, {g.minv[0], g.minv[1], g.minv[2]},
-                     {g.pd[0], g.pd[1], g.pd[2]}, mask, 0xffffffffu};
+      CellMarker m{{g.morig[0], g.morig[1], g.morig[2]}, {g.minv[0], g.minv[1], g.minv[2]},
+                   {g.pd[0], g.pd[1], g.pd[2]}, mask, 0xffffffffu};
       float4 color;
       unsigned lit = 0, hit = 0;
-      view_march_pixel<float4, false, float, VertexMarker>(g, quads, s_tab, s_tf, nullptr, x, y, color, lit, hit, &m);
+      view_march_pixel<float4, false, float, CellMarker>(g, quads, s_tab, s_tf, nullptr, x, y, color, lit, hit, &m);
     }
   }
 }

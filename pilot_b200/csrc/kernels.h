@@ -26,8 +26,9 @@ void occupancy_dims(const int n[3], int occ_n[3]);
 cudaError_t launch_build_occupancy(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tf,
                                    unsigned char* occ, cudaStream_t st);
 // Learned form's lazy fallback (k_mlp_probe.cu): when the list of failing tiles
-// is non-empty, clears the vertex mask (nvert bytes, 16-byte multiple) and marks
-// the map vertices that the listed tiles' view rays read. host_count (host-mapped
+// is non-empty, clears the cell mask (one byte per map cell, rounded up to a
+// 16-byte multiple) and marks the map cells that the listed tiles' view rays
+// read; K1 given the mask builds the vertices of marked cells. host_count (host-mapped
 // memory, or null) receives the list's length.
 cudaError_t launch_mark_fallback_vertices(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                           const unsigned* flist, const unsigned* fcount, unsigned char* vmask,

@@ -42,7 +42,7 @@ struct MlpState {
   size_t probe_bytes = 0;
   float* probe_err = nullptr;  // per-probe max |dRGBA| of the last frame (tests)
   int probe_err_n = 0;
-  unsigned char* vmask = nullptr;  // lazy fallback: map vertices the failing tiles read
+  unsigned char* vmask = nullptr;  // lazy fallback: map cells the failing tiles read
   size_t vmask_bytes = 0;
   beams_mlp_options render_opts{};
   bool use_tc = true;            // training forward on the tcgen05 tensor cores
@@ -233,11 +233,11 @@ static beams_status mlp_probe_check(beams_renderer* r, const ExactGeo& g, const 
   return BEAMS_OK;
 }
 
-// The exact map path over the listed tiles, built lazily: the map vertices the
-// listed tiles' view rays read are marked, K1 marches only those (both gated on
+// The exact map path over the listed tiles, built lazily: the map cells the
+// listed tiles' view rays read are marked, K1 marches only their vertices (both gated on
 // a non-empty list), K2 re-renders the listed tiles. Nothing here waits on the
-// host; the list's length is copied to pinned memory for the next frame's
-// choice of order.
+// host; the first kernel writes the list's length to host-mapped memory for the
+// next frame's choice of order.
 static beams_status mlp_fallback(beams_renderer* r, const ExactGeo& g, const ProbeBuffers& pb, float4* out,
                                  int& launches) {
   MlpState* st = r->mlp;
@@ -248,8 +248,9 @@ static beams_status mlp_fallback(beams_renderer* r, const ExactGeo& g, const Pro
   if (s != BEAMS_OK) return s;
   r->map_valid = false;  // a partial map, built (or not) on the device's decision
   r->map_is_half = false;
-  const size_t mask_bytes = (nvert + 15) & ~(size_t)15;
-  s = ensure_buffer(r, (void**)&st->vmask, &st->vmask_bytes, mask_bytes, "allocating the fallback vertex mask");
+  const size_t ncell = (size_t)(g.pd[0] - 1) * (g.pd[1] - 1) * (g.pd[2] - 1);
+  const size_t mask_bytes = (ncell + 15) & ~(size_t)15;
+  s = ensure_buffer(r, (void**)&st->vmask, &st->vmask_bytes, mask_bytes, "allocating the fallback cell mask");
   if (s != BEAMS_OK) return s;
   if (!st->h_fallback) {
     unsigned* h = nullptr;

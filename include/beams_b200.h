@@ -439,7 +439,10 @@ beams_status beams_build_shadow_map(beams_renderer* r, beams_timings* t);
  * what loads the module, and so where the 8.6 MB and the kernels' code are
  * taken: make that first call (a warm-up frame) before the host framework claims
  * its memory, and outside any stream capture. The volume data must be 4-byte
- * aligned. All calls share the one array: calls that
+ * aligned. The marches are beams_render's own, on the plain field with the cell
+ * tables in shared memory (so the image equals beams_render's bit for bit); the
+ * tables limit the axes: (nx + ny + nz - 3 + 3 map_cells + 1024) * 16 bytes must
+ * stay within 200 KiB, else BEAMS_ERR_UNSUPPORTED. All calls share the one array: calls that
  * overlap on the GPU (other streams, other threads) race and corrupt each
  * other's maps; serialise them. Each call rewrites every map entry it reads, so
  * no clearing is needed between calls. Errors: beams_last_error(NULL). */

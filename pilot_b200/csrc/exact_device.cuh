@@ -440,7 +440,33 @@ __device__ __forceinline__ void pencil_brick(int bi, const int* s_bo, int& bx, i
 // Quad layout of a point field: Q[z][y][x] = {f(x,y,z), f(x+1,y,z), f(x,y+1,z),
 // f(x+1,y+1,z)} for x < nx-1, y < ny-1, so one cell is two 16-byte loads
 // (z and z+1). VTK corner order 0..7 = lo.x lo.y lo.w lo.z hi.x hi.y hi.w hi.z.
+// Cell (x, y, z) is entry qi = z qz + y qx + x; strides() gives qx and qz.
+// FieldF32 reads the float32 field itself (x fastest, eight scalar loads per
+// cell; qx = nx, qz = nx ny): the allocation-free entry point's layout.
 template <typename Q> struct QuadLoad;
+struct FieldF32 { float v; };
+__device__ __forceinline__ void quad_strides(const ExactGeo& g, unsigned& qx, unsigned& qz) {
+  qx = (unsigned)(g.n[0] - 1);
+  qz = qx * (unsigned)(g.n[1] - 1);
+}
+template <> struct QuadLoad<FieldF32> {
+  static __device__ __forceinline__ void strides(const ExactGeo& g, unsigned& qx, unsigned& qz) {
+    qx = (unsigned)g.n[0];
+    qz = qx * (unsigned)g.n[1];
+  }
+  static __device__ __forceinline__ void cell(const FieldF32* __restrict__ q, unsigned qi, unsigned qx, unsigned qz,
+                                              float v[8]) {
+    const float* f = reinterpret_cast<const float*>(q) + qi;
+    v[0] = __ldg(f);
+    v[1] = __ldg(f + 1);
+    v[2] = __ldg(f + qx + 1);
+    v[3] = __ldg(f + qx);
+    v[4] = __ldg(f + qz);
+    v[5] = __ldg(f + qz + 1);
+    v[6] = __ldg(f + qz + qx + 1);
+    v[7] = __ldg(f + qz + qx);
+  }
+};
 // 16-bit quads (precision form): four binary16 or bfloat16 values in 8 bytes.
 struct __align__(8) QuadBF16 { unsigned short v[4]; };
 struct __align__(8) QuadF16 { unsigned short v[4]; };
@@ -449,7 +475,8 @@ __device__ __forceinline__ float bf16_hi(unsigned u) { return __uint_as_float(u 
 __device__ __forceinline__ float f16_lo(unsigned u) { return __half2float(__ushort_as_half((unsigned short)(u & 0xffffu))); }
 __device__ __forceinline__ float f16_hi(unsigned u) { return __half2float(__ushort_as_half((unsigned short)(u >> 16))); }
 template <> struct QuadLoad<QuadBF16> {
-  static __device__ __forceinline__ void cell(const QuadBF16* __restrict__ q, unsigned qi, unsigned qz, float v[8]) {
+  static __device__ __forceinline__ void strides(const ExactGeo& g, unsigned& qx, unsigned& qz) { quad_strides(g, qx, qz); }
+  static __device__ __forceinline__ void cell(const QuadBF16* __restrict__ q, unsigned qi, unsigned, unsigned qz, float v[8]) {
     const uint2 a = __ldg((const uint2*)(q + qi));
     const uint2 b = __ldg((const uint2*)(q + qi + qz));
     v[0] = bf16_lo(a.x); v[1] = bf16_hi(a.x); v[2] = bf16_hi(a.y); v[3] = bf16_lo(a.y);
@@ -457,7 +484,8 @@ template <> struct QuadLoad<QuadBF16> {
   }
 };
 template <> struct QuadLoad<QuadF16> {
-  static __device__ __forceinline__ void cell(const QuadF16* __restrict__ q, unsigned qi, unsigned qz, float v[8]) {
+  static __device__ __forceinline__ void strides(const ExactGeo& g, unsigned& qx, unsigned& qz) { quad_strides(g, qx, qz); }
+  static __device__ __forceinline__ void cell(const QuadF16* __restrict__ q, unsigned qi, unsigned, unsigned qz, float v[8]) {
     const uint2 a = __ldg((const uint2*)(q + qi));
     const uint2 b = __ldg((const uint2*)(q + qi + qz));
     v[0] = f16_lo(a.x); v[1] = f16_hi(a.x); v[2] = f16_hi(a.y); v[3] = f16_lo(a.y);
@@ -465,7 +493,8 @@ template <> struct QuadLoad<QuadF16> {
   }
 };
 template <> struct QuadLoad<float4> {
-  static __device__ __forceinline__ void cell(const float4* __restrict__ q, unsigned qi, unsigned qz, float v[8]) {
+  static __device__ __forceinline__ void strides(const ExactGeo& g, unsigned& qx, unsigned& qz) { quad_strides(g, qx, qz); }
+  static __device__ __forceinline__ void cell(const float4* __restrict__ q, unsigned qi, unsigned, unsigned qz, float v[8]) {
     const float4 a = __ldg(q + qi);
     const float4 b = __ldg(q + qi + qz);
     v[0] = a.x; v[1] = a.y; v[2] = a.w; v[3] = a.z;
@@ -515,7 +544,7 @@ __device__ __forceinline__ float point_opacity(const ExactGeo& g, const float4* 
     const int c1 = find_cell_bsearch_t(T1, g.n[1] - 2, g.org[1], g.invh[1], s[1], e1);
     const int c2 = find_cell_bsearch_t(T2, g.n[2] - 2, g.org[2], g.invh[2], s[2], e2);
     float vals[8];
-    QuadLoad<float4>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qz, vals);
+    QuadLoad<float4>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qx, qz, vals);
     float scalar = hex_interp(vals, div_rn_markstein(s[0] - e0.x, e0.z, e0.w), div_rn_markstein(s[1] - e1.x, e1.z, e1.w),
                               div_rn_markstein(s[2] - e2.x, e2.z, e2.w));
     scalar = (scalar - g.min_scalar) * g.inv_delta;

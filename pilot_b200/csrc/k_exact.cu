@@ -489,7 +489,8 @@ __global__ void k_build_occupancy(const ExactGeo g, const QuadT* __restrict__ qu
                                   unsigned char* __restrict__ occ) {
   const int lane = threadIdx.x & 31;
   const int nm = g.occ_n[0] * g.occ_n[1] * g.occ_n[2];
-  const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
+  unsigned qx, qz;
+  QuadLoad<QuadT>::strides(g, qx, qz);
   for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nm; w += (gridDim.x * blockDim.x) >> 5) {
     const int m0 = w % g.occ_n[0], m1 = (w / g.occ_n[0]) % g.occ_n[1], m2 = w / (g.occ_n[0] * g.occ_n[1]);
     int lo[3], ext[3];
@@ -506,7 +507,7 @@ __global__ void k_build_occupancy(const ExactGeo g, const QuadT* __restrict__ qu
     for (int i = lane; i < count; i += 32) {
       const int x = lo[0] + i % ext[0], y = lo[1] + (i / ext[0]) % ext[1], z = lo[2] + i / (ext[0] * ext[1]);
       float v[8];
-      QuadLoad<QuadT>::cell(quads, (unsigned)z * qz + (unsigned)y * qx + (unsigned)x, qz, v);
+      QuadLoad<QuadT>::cell(quads, (unsigned)z * qz + (unsigned)y * qx + (unsigned)x, qx, qz, v);
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         nan |= (v[k] != v[k]);

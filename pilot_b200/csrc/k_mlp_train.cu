@@ -46,7 +46,7 @@ __device__ float alpha_at(const ExactGeo& g, const float4* __restrict__ quads, c
   const int c1 = find_cell_bsearch_t(T1, g.n[1] - 2, g.org[1], g.invh[1], P[1], e1);
   const int c2 = find_cell_bsearch_t(T2, g.n[2] - 2, g.org[2], g.invh[2], P[2], e2);
   float vals[8];
-  QuadLoad<float4>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qz, vals);
+  QuadLoad<float4>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qx, qz, vals);
   float scalar = hex_interp(vals, div_rn_markstein(P[0] - e0.x, e0.z, e0.w), div_rn_markstein(P[1] - e1.x, e1.z, e1.w),
                             div_rn_markstein(P[2] - e2.x, e2.z, e2.w));
   scalar = (scalar - g.min_scalar) * g.inv_delta;

@@ -10,9 +10,10 @@
 // transmittance map, in a fixed static device array below, and otherwise uses
 // the caller's input and output buffers.
 //
-// The kernels here restate the same reference arithmetic as k_exact.cu on the
-// plain field layout (eight scalar loads per cell, coordinates generated as
-// origin + spacing*i, IEEE division), so the image equals beams_render's.
+// The kernels run the same march code as beams_render's K1 and K2
+// (march_vertex, view_march_pixel) on the plain float32 field with the cell
+// tables computed into shared memory, so the image equals beams_render's bit
+// for bit.
 // Compiled with -fmad=false like every kernel file.
 #include <cuda_runtime.h>
 
@@ -21,7 +22,9 @@
 
 #include "../../include/beams_b200.h"
 #include "exact_device.cuh"
+#include "light_march.cuh"
 #include "renderer.h"
+#include "view_march.cuh"
 
 namespace beams {
 namespace {
@@ -55,216 +58,63 @@ cudaError_t scratch_address(float** out) {
 // Errors go to the thread-local text that beams_last_error(NULL) returns.
 beams_status nf(beams_status s, const char* msg) { return fail(nullptr, s, msg); }
 
-// Reference-order TF staging: RGBA in shared memory plus alpha / max alpha
-// (TransmittanceMap.h:329, GetMaxAlpha :515-525).
-__device__ void stage_tf(const float4* __restrict__ tf, int n, float4* s_tf, float* s_a, float* s_max) {
-  if (threadIdx.x == 0) {
-    float m = 0.f;
-    for (int i = 0; i < n; ++i) m = mx(m, tf[i].w);
-    *s_max = m;
-  }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s_tf[i] = tf[i];
-  __syncthreads();
-  const float m = *s_max;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s_a[i] = (m > 0.f) ? s_tf[i].w / m : 0.f;
-  __syncthreads();
+// The cell tables {lo, hi, hi - lo, RN(1/(hi - lo))} computed into shared
+// memory from the generated coordinates (the entries beams_render builds once
+// per volume into device memory), n entries from the start.
+__device__ void stage_tables(const ExactGeo& g, int n, float4* s_tab) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s_tab[i] = table_entry(g, i);
 }
 
-// The view march reads the TF colours only (no alpha / max alpha pass).
-__device__ void stage_tf_colors(const float4* __restrict__ tf, int n, float4* s_tf) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s_tf[i] = tf[i];
-  __syncthreads();
-}
-
-// Smallest cell c with val <= coord(c+1) (RectilinearMeshOracle.h:154-176).
-__device__ __forceinline__ int cell_bsearch_gen(const ExactGeo& g, int d, float val) {
-  const int cmax = g.n[d] - 2;
-  int c = (int)fminf(fmaxf((val - g.org[d]) * g.invh[d], 0.f), (float)cmax);
-  while (c > 0 && val <= coord(g, d, c)) --c;
-  while (c < cmax && val > coord(g, d, c + 1)) ++c;
-  return c;
-}
-
-// Unique cell with coord(c) <= p < coord(c+1) (LightedVolumeRenderer.cxx:119-165).
-__device__ __forceinline__ int cell_walk_gen(const ExactGeo& g, int d, float p) {
-  const int cmax = g.n[d] - 2;
-  int c = (int)fminf(fmaxf((p - g.org[d]) * g.invh[d], 0.f), (float)cmax);
-  while (c > 0 && p < coord(g, d, c)) --c;
-  while (c < cmax && p >= coord(g, d, c + 1)) ++c;
-  return c;
-}
-
-__device__ __forceinline__ void cell_values(const float* __restrict__ f, const ExactGeo& g, int c0, int c1, int c2,
-                                            float v[8]) {
-  const unsigned nx = (unsigned)g.n[0], nxy = (unsigned)g.n[0] * (unsigned)g.n[1];
-  const float* b = f + ((unsigned)c2 * nxy + (unsigned)c1 * nx + (unsigned)c0);
-  v[0] = __ldg(b);
-  v[1] = __ldg(b + 1);
-  v[2] = __ldg(b + 1 + nx);
-  v[3] = __ldg(b + nx);
-  v[4] = __ldg(b + nxy);
-  v[5] = __ldg(b + nxy + 1);
-  v[6] = __ldg(b + nxy + 1 + nx);
-  v[7] = __ldg(b + nxy + nx);
-}
-
-// Light march (TransmittanceMap.h:279-332) writing the scratch map.
-__global__ void __launch_bounds__(256) k_noalloc_light_march(const ExactGeo g, const float* __restrict__ field,
+// K1: one thread per map vertex, the light march of k_light_march
+// (march_vertex, TransmittanceMap.h:279-332) on the plain field, into the
+// scratch map. Alpha / max alpha as GetMaxAlpha (TransmittanceMap.h:515-525).
+__global__ void __launch_bounds__(256) k_noalloc_light_march(const ExactGeo g, const FieldF32* __restrict__ field,
                                                              const float4* __restrict__ tf,
                                                              float* __restrict__ map, int nvert) {
-  __shared__ float4 s_tf[kMaxTFn];
-  __shared__ float s_a[kMaxTFn];
+  extern __shared__ float4 s_dyn[];
+  float4* s_tab = s_dyn;                              // field axes' entries
+  float* s_a = reinterpret_cast<float*>(s_dyn + g.max_off[0]);
   __shared__ float s_max;
-  stage_tf(tf, g.tf_n, s_tf, s_a, &s_max);
+  if (threadIdx.x == 0) {
+    float m = 0.f;
+    for (int i = 0; i < g.tf_n; ++i) m = mx(m, tf[i].w);
+    s_max = m;
+  }
+  stage_tables(g, g.max_off[0], s_tab);
+  __syncthreads();
+  for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) s_a[i] = (s_max > 0.f) ? tf[i].w / s_max : 0.f;
+  __syncthreads();
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= nvert) return;
   float V[3], L[3];
   map_vertex(g, id, V);
   light_origin(g, V, L);
-  const float v[3] = {V[0] - L[0], V[1] - L[1], V[2] - L[2]};
-  const float rs = 1.f / sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-  const float dir[3] = {v[0] * rs, v[1] * rs, v[2] * rs};
-  float tmin, tmax;
-  segment_aabb(g, L, V, tmin, tmax);
-  const float st[3] = {L[0] + tmin * dir[0], L[1] + tmin * dir[1], L[2] + tmin * dir[2]};
-  float s[3] = {st[0], st[1], st[2]};
-  const float len2 = (tmax - tmin) * (tmax - tmin);
-  const int n1 = g.tf_n - 1;
-  float o = 0.f;
-  for (int b = g.light_budget; b > 0; --b) {
-    const float q0 = s[0] - st[0], q1 = s[1] - st[1], q2 = s[2] - st[2];
-    if (!(q0 * q0 + q1 * q1 + q2 * q2 <= len2)) break;
-    s[0] = s[0] + g.step * dir[0];
-    s[1] = s[1] + g.step * dir[1];
-    s[2] = s[2] + g.step * dir[2];
-    if (!inside_vol(g, s)) break;
-    int c[3];
-    float pc[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      c[d] = cell_bsearch_gen(g, d, s[d]);
-      const float lo = coord(g, d, c[d]), hi = coord(g, d, c[d] + 1);
-      pc[d] = (s[d] - lo) / (hi - lo);
-    }
-    float vals[8];
-    cell_values(field, g, c[0], c[1], c[2], vals);
-    float scalar = hex_interp(vals, pc[0], pc[1], pc[2]);
-    scalar = (scalar - g.min_scalar) * g.inv_delta;
-    o = o + (1.f - o) * s_a[tf_index_clamped(scalar * (float)n1, n1)];
-    if (o == 1.f) break;
-  }
-  map[id] = o;
+  Accum<false> acc;
+  unsigned ns = 0;
+  march_vertex<FieldF32, false, false>(g, field, s_tab + g.ax_off[0], s_tab + g.ax_off[1], s_tab + g.ax_off[2], s_a,
+                                       nullptr, nullptr, V, L, [](const float*) { return 0.f; }, acc, ns);
+  map[id] = acc.o;
 }
 
-__device__ __forceinline__ float map_opacity_gen(const ExactGeo& g, const float* __restrict__ map, const float p[3]) {
-  int c[3];
-  float pc[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    float t = (p[d] - g.morig[d]) * g.minv[d];
-    if (t < 0.f) t = 0.f;
-    if (t >= (float)(g.pd[d] - 1)) t = (float)(g.pd[d] - 2);
-    c[d] = (int)t;
-    const float lo = vtx_coord(g, d, c[d]), hi = vtx_coord(g, d, c[d] + 1);
-    pc[d] = (p[d] - lo) / (hi - lo);
-  }
-  const unsigned px = (unsigned)g.pd[0], pxy = (unsigned)g.pd[0] * (unsigned)g.pd[1];
-  const float* m = map + ((unsigned)c[2] * pxy + (unsigned)c[1] * px + (unsigned)c[0]);
-  float v[8] = {m[0], m[1], m[1 + px], m[px], m[pxy], m[pxy + 1], m[pxy + 1 + px], m[pxy + px]};
-  return hex_interp(v, pc[0], pc[1], pc[2]);
-}
-
-// View march (LightedVolumeRenderer.cxx:346-498) shading by the scratch map.
-__global__ void __launch_bounds__(256) k_noalloc_view_march(const ExactGeo g, const float* __restrict__ field,
+// K2: one thread per pixel in 16 x 16 blocks, the view march of k_view_march
+// (view_march_pixel, LightedVolumeRenderer.cxx:346-498) shading by the scratch map.
+__global__ void __launch_bounds__(256) k_noalloc_view_march(const ExactGeo g, const FieldF32* __restrict__ field,
                                                             const float4* __restrict__ tf,
                                                             const float* __restrict__ map,
                                                             float4* __restrict__ out) {
-  __shared__ float4 s_tf[kMaxTFn];
-  stage_tf_colors(tf, g.tf_n, s_tf);
+  extern __shared__ float4 s_dyn[];
+  float4* s_tab = s_dyn;            // field and map axes' entries
+  float4* s_tf = s_dyn + g.ntab;
+  stage_tables(g, g.ntab, s_tab);
+  for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) s_tf[i] = tf[i];
+  __syncthreads();
   const int tiles_x = (g.width + 15) >> 4;
   const int x = (blockIdx.x % tiles_x) * 16 + (threadIdx.x & 15);
   const int y = (blockIdx.x / tiles_x) * 16 + (threadIdx.x >> 4);
   if (x >= g.width || y >= g.height) return;
-  float4 color = make_float4(0.f, 0.f, 0.f, 0.f);
-  float o[3], d[3], minD, maxD;
-  if (ray_setup(g, x, y, o, d, minD, maxD)) {
-    const float qd = (maxD - minD) / g.sd;
-    long long budget = (qd < 1e9f) ? (long long)qd + 16 : 1000000000ll;
-    float dist = minD + g.mesh_eps;
-    float p[3] = {o[0] + dist * d[0], o[1] + dist * d[1], o[2] + dist * d[2]};
-    while (!inside_vol(g, p) && dist < maxD && budget-- > 0) {
-      dist += g.sd;
-      p[0] = o[0] + dist * d[0];
-      p[1] = o[1] + dist * d[1];
-      p[2] = o[2] + dist * d[2];
-    }
-    float bl[3] = {0.f, 0.f, 0.f}, inv[3] = {0.f, 0.f, 0.f};
-    bool newCell = true;
-    float tx = 0.f, ty = 0.f, tz = 0.f;
-    float s0 = 0.f, s1m0 = 0.f, s2m3 = 0.f, s3 = 0.f, s4 = 0.f, s5m4 = 0.f, s6m7 = 0.f, s7 = 0.f;
-    int c[3] = {0, 0, 0};
-    const int n1 = g.tf_n - 1;
-    while (inside_vol(g, p) && dist < maxD && budget-- > 0) {
-      const float mint = mn(tx, mn(ty, tz));
-      const float maxt = mx(tx, mx(ty, tz));
-      if (maxt > 1.f || mint < 0.f) newCell = true;
-      if (newCell) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          if (p[k] == g.maxp[k]) {
-            c[k] = g.n[k] - 2;  // the reference keeps invSpacing[k] here
-          } else {
-            c[k] = cell_walk_gen(g, k, p[k]);
-            inv[k] = 1.f / (coord(g, k, c[k] + 1) - coord(g, k, c[k]));
-          }
-          bl[k] = coord(g, k, c[k]);
-        }
-        float v[8];
-        cell_values(field, g, c[0], c[1], c[2], v);
-        s0 = v[0];
-        s3 = v[3];
-        s4 = v[4];
-        s7 = v[7];
-        s6m7 = v[6] - v[7];
-        s5m4 = v[5] - v[4];
-        s1m0 = v[1] - v[0];
-        s2m3 = v[2] - v[3];
-        tx = (p[0] - bl[0]) * inv[0];
-        ty = (p[1] - bl[1]) * inv[1];
-        tz = (p[2] - bl[2]) * inv[2];
-        newCell = false;
-      }
-      const float l76 = s7 + tx * s6m7;
-      const float l45 = s4 + tx * s5m4;
-      const float top = l45 + ty * (l76 - l45);
-      const float l01 = s0 + tx * s1m0;
-      const float l32 = s3 + tx * s2m3;
-      const float bot = l01 + ty * (l32 - l01);
-      float fs = bot + tz * (top - bot);
-      fs = (fs - g.min_scalar) * g.inv_delta;
-      const float fi = fs * (float)n1;
-      if (fi > -1.f && fi < (float)(n1 + 1)) {
-        const float4 tfc = s_tf[(int)fi];
-        const float sa = tfc.w * (1.f - color.w);
-        const float tr = 1.f - map_opacity_gen(g, map, p);
-        const float sc0 = clamp01(tfc.x * (tr * g.light_color[0]));
-        const float sc1 = clamp01(tfc.y * (tr * g.light_color[1]));
-        const float sc2 = clamp01(tfc.z * (tr * g.light_color[2]));
-        color.x = color.x + sc0 * sa;
-        color.y = color.y + sc1 * sa;
-        color.z = color.z + sc2 * sa;
-        color.w = sa + color.w;
-      }
-      dist += g.sd;
-      p[0] = p[0] + g.sd * d[0];
-      p[1] = p[1] + g.sd * d[1];
-      p[2] = p[2] + g.sd * d[2];
-      tx = (p[0] - bl[0]) * inv[0];
-      ty = (p[1] - bl[1]) * inv[1];
-      tz = (p[2] - bl[2]) * inv[2];
-      if (color.w >= g.cutoff) break;
-    }
-  }
+  float4 color;
+  unsigned lit = 0, hit = 0;
+  view_march_pixel<FieldF32, true, float>(g, field, s_tab, s_tf, map, x, y, color, lit, hit);
   out[(size_t)y * g.width + x] = color;
 }
 
@@ -291,6 +141,8 @@ extern "C" beams_status beams_render_noalloc(const beams_volume* vol, const floa
   if ((double)vol->dims[0] * vol->dims[1] * vol->dims[2] >= 4294967296.0)
     return nf(BEAMS_ERR_UNSUPPORTED, "render_noalloc: volume too large for 32-bit indexing");
   if (tf_n < 1 || tf_n > kMaxTFn) return nf(BEAMS_ERR_INVALID_ARG, "render_noalloc: tf_n must be in [1, 1024]");
+  if ((size_t)(vol->dims[0] + vol->dims[1] + vol->dims[2] - 3 + 3 * (size_t)map_cells + kMaxTFn) * 16 > 200 * 1024)
+    return nf(BEAMS_ERR_UNSUPPORTED, "render_noalloc: volume/map axes too long for the shared-memory cell tables");
   if (map_cells < 1 || map_cells > kMaxMapCells)
     return nf(BEAMS_ERR_INVALID_ARG,
               "render_noalloc: map_cells must be in [1, BEAMS_NOALLOC_MAX_MAP_CELLS = 128]; the map lives in a "
@@ -326,6 +178,18 @@ extern "C" beams_status beams_render_noalloc(const beams_volume* vol, const floa
   g.min_scalar = fmin;
   g.inv_delta = ((fmax - fmin) != 0.f) ? 1.f / (fmax - fmin) : fmin;
   g.tf_n = tf_n;
+  {
+    int off = 0;
+    for (int d = 0; d < 3; ++d) {
+      g.ax_off[d] = off;
+      off += g.n[d] - 1;
+    }
+    for (int d = 0; d < 3; ++d) {
+      g.max_off[d] = off;
+      off += map_cells;
+    }
+    g.ntab = off;
+  }
   float ext[3];
   for (int d = 0; d < 3; ++d) ext[d] = (float)(g.bmax[d] - g.bmin[d]);
   g.extent_mag = std::sqrt(ext[0] * ext[0] + ext[1] * ext[1] + ext[2] * ext[2]);
@@ -387,13 +251,19 @@ extern "C" beams_status beams_render_noalloc(const beams_volume* vol, const floa
   }
   cudaStream_t st = (cudaStream_t)cuda_stream;
   const int nvert = g.pd[0] * g.pd[1] * g.pd[2];
+  const size_t smem1 = (size_t)g.max_off[0] * sizeof(float4) + (size_t)tf_n * sizeof(float);
+  const size_t smem2 = ((size_t)g.ntab + (size_t)tf_n) * sizeof(float4);
+  e = cudaFuncSetAttribute(k_noalloc_light_march, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_noalloc_view_march, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
+  if (e != cudaSuccess) return nf(BEAMS_ERR_CUDA, cudaGetErrorString(e));
   // The light march writes every one of the nvert map entries before the view
   // march reads any, so the scratch needs no clearing between calls.
-  k_noalloc_light_march<<<(nvert + 255) / 256, 256, 0, st>>>(g, (const float*)vol->data,
-                                                            (const float4*)tf_rgba_device, map, nvert);
+  const FieldF32* field = (const FieldF32*)vol->data;
+  k_noalloc_light_march<<<(nvert + 255) / 256, 256, smem1, st>>>(g, field, (const float4*)tf_rgba_device, map, nvert);
   const int tiles = ((g.width + 15) >> 4) * ((g.height + 15) >> 4);
-  k_noalloc_view_march<<<tiles, 256, 0, st>>>(g, (const float*)vol->data, (const float4*)tf_rgba_device, map,
-                                              (float4*)rgba_out_device);
+  k_noalloc_view_march<<<tiles, 256, smem2, st>>>(g, field, (const float4*)tf_rgba_device, map,
+                                                  (float4*)rgba_out_device);
   e = cudaGetLastError();
   if (e != cudaSuccess) return nf(BEAMS_ERR_CUDA, cudaGetErrorString(e));
   return BEAMS_OK;

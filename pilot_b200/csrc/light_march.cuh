@@ -70,7 +70,8 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
                                              const float V[3], const float L[3], Prefix prefix, Accum<PREC>& acc,
                                              unsigned& ns) {
   const int cm0 = g.n[0] - 2, cm1 = g.n[1] - 2, cm2 = g.n[2] - 2;
-  const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
+  unsigned qx, qz;
+  QuadLoad<QuadT>::strides(g, qx, qz);
   const int n1 = g.tf_n - 1;
   const float v[3] = {V[0] - L[0], V[1] - L[1], V[2] - L[2]};
   const float rs = 1.f / sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
@@ -154,7 +155,7 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
         c1 = find_cell_bsearch_in(T1, cm1, g.org[1], g.invh[1], s[1], e1);
         c2 = find_cell_bsearch_in(T2, cm2, g.org[2], g.invh[2], s[2], e2);
       }
-      QuadLoad<QuadT>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qz, v8);
+      QuadLoad<QuadT>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qx, qz, v8);
       // pcoords = (p - min) / (max - min) (RectilinearMeshOracle.h:189-192)
       pc[0] = div_rn_markstein(s[0] - e0.x, e0.z, e0.w);
       pc[1] = div_rn_markstein(s[1] - e1.x, e1.z, e1.w);

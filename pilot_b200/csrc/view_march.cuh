@@ -53,7 +53,8 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT*
     p[2] = o[2] + dist * d[2];
   }
   const float sdx = g.sd * d[0], sdy = g.sd * d[1], sdz = g.sd * d[2];
-  const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
+  unsigned qx, qz;
+  QuadLoad<QuadT>::strides(g, qx, qz);
   float bl[3] = {0.f, 0.f, 0.f};
   bool newCell = true;
   float tx = 0.f, ty = 0.f, tz = 0.f;
@@ -92,7 +93,7 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT*
         bl[k] = e.x;
       }
       float v[8];
-      QuadLoad<QuadT>::cell(quads, (unsigned)c[2] * qz + (unsigned)c[1] * qx + (unsigned)c[0], qz, v);
+      QuadLoad<QuadT>::cell(quads, (unsigned)c[2] * qz + (unsigned)c[1] * qx + (unsigned)c[0], qx, qz, v);
       s0 = v[0];
       s3 = v[3];
       s4 = v[4];

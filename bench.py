@@ -486,6 +486,24 @@ def run_ours(args):
             learned[name] = rec
         r.set_form(B.FORM_EXACT)
 
+    # the other forms, each in its own configuration (one GPU, the default run only):
+    # config 2 precision (no FP64 crops here), config 3 batch, the config-1 field as bricks
+    forms = None
+    if world == 1 and not args.no_forms:
+        forms = {}
+        for name, fn, over in (("precision_config2", run_form, dict(form="precision", config=2, no_quality=True)),
+                               ("batch_config3", run_batch, dict(form="batch")),
+                               ("bricks_2x2x2", run_bricks, dict(form="bricks"))):
+            sub = argparse.Namespace(**dict(vars(args), steps=min(args.steps, 10), warmup=3, **over))
+            try:
+                rec = fn(sub, nested=True)
+                forms[name] = {k: v for k, v in rec.items()
+                               if k not in ("metric", "unit", "n_gpus", "higher_is_better", "scaling", "vs_baseline")}
+            except Exception as ex:  # a failing form must not cost the headline line
+                forms[name] = {"error": repr(ex)[:400]}
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
@@ -498,7 +516,7 @@ def run_ours(args):
                 "lit_samples_per_frame": lit_frame, "light_samples_per_frame": light_frame,
                 "gpu_launches": launches_per_frame * args.steps,
                 "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": sampler.summary(),
-                "learned": learned}
+                "learned": learned, "forms": forms}
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:
@@ -639,7 +657,9 @@ def learned_record(B, r, s, cam, out, exact_img, exact_ms, stream, world, local,
     return rec, total_ms, clocks, tm, tn
 
 
-def run_form(args):
+def run_form(args, nested=False):
+    """--form precision / mlp. nested: called from the default run (no process
+    group of its own, returns the line instead of printing it)."""
     import torch
     import torch.distributed as dist
 
@@ -648,6 +668,8 @@ def run_form(args):
     from pilot_b200 import scenes
 
     world, rank, local = dist_setup()
+    if nested:
+        world, rank = 1, 0
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
@@ -739,6 +761,9 @@ def run_form(args):
                 "data": "synthetic (seeded fields generated on the device)", "config": wl,
                 "lit_samples_per_frame": lit_frame, "gpu_launches": launches * args.steps,
                 "roofline": roofline, "clocks": clocks, **extra}
+        if nested:
+            r.close()
+            return line
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:
@@ -785,7 +810,7 @@ def batch_requests(B, vols, rng, nreq, outs):
     return reqs
 
 
-def run_batch(args):
+def run_batch(args, nested=False):
     import torch
 
     from pilot_b200 import beams as B
@@ -923,11 +948,13 @@ def run_batch(args):
                     "d2h_bytes_per_step": int(sum(w * w * 16 for w in sizes)),
                     "note": "wall clock per batch: host request set-up, graph replay, images to pinned host memory"},
             "clocks": sampler.summary()}
+    if nested:
+        return line
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_bricks(args):
+def run_bricks(args, nested=False):
     import torch
 
     from oracle.oracle import psnr
@@ -981,6 +1008,9 @@ def run_bricks(args):
             "phases_ms": {"maps_and_stitch": tb["map_build_ms"], "view_marches": tb["view_march_ms"],
                           "composite": tb["composite_ms"]},
             "undivided_ms_per_frame": whole_ms, "psnr_vs_undivided": psnr(img, whole), "clocks": clocks}
+    r.close()
+    if nested:
+        return line
     print(json.dumps(line), flush=True)
     return 0
 
@@ -1144,6 +1174,8 @@ def main():
     ap.add_argument("--crop-stride", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="default line: skip the learned-form records")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="default line: skip the precision, batch and bricks records")
     ap.add_argument("--learned-knot", type=int, default=32, help="default line: knot of the learned-form records")
     ap.add_argument("--no-autotune", action="store_true", help="fixed tuning (for launch lists under ncu)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -307,10 +307,12 @@ beams_status beams_set_batch_options(beams_renderer* r, const beams_batch_option
  * persistent kernel(s) and their staging copies, lit_samples and rays_hit summed,
  * kernel_launches 1 or 2 (split). */
 beams_status beams_render_batch(beams_renderer* r, const beams_request* reqs, int n, beams_timings* t);
-/* Tunes the batch options on these requests by coordinate descent over the
- * empty-space skip, one or two launches, the vertex order {rows, 8, 16, 32, 64 bricks} and the view
- * tile {8x8, 16x16, 32x8, 8x32, 32x32, 64x32, 64x64}; keeps the fastest (images are identical
- * under all of them) and reports it. */
+/* Tunes the batch options on these requests: for each launch plan (one launch,
+ * or map builds then view marches) a coordinate descent over the empty-space
+ * skip, the vertex order {rows, 8, 16, 32, 64 bricks} and the view tile {8x8,
+ * 16x16, 32x8, 8x32, 32x32, 64x32, 64x64}, repeated until a round changes
+ * nothing (three rounds at most); keeps the fastest (images are identical under
+ * all of them) and reports it. */
 beams_status beams_batch_autotune(beams_renderer* r, const beams_request* reqs, int n, beams_batch_options* best,
                                   float* best_ms);
 /* The autotuner's results cache: beams_batch_autotune keeps its result per batch
@@ -321,6 +323,19 @@ beams_status beams_batch_autotune(beams_renderer* r, const beams_request* reqs, 
 beams_status beams_batch_tuning_save(beams_renderer* r, const char* path);
 beams_status beams_batch_tuning_load(beams_renderer* r, const char* path);
 beams_status beams_batch_tuning_clear(beams_renderer* r);
+
+/* ---- profiling ---------------------------------------------------------------- */
+/* Replaces MapperLightedVolume::SetProfiler (MapperLightedVolume.h:57,
+ * MapperLightedVolume.cxx:305-309), whose beams::Profiler (beams/Profiler.h)
+ * records named, nested frames ("Phase 1" and its sub-frames,
+ * LightedVolumeRenderer.cxx:914-966). With a profiler set, every beams_render
+ * reports its frames after it completes (the call then synchronises the stream,
+ * as with timings): ("Render", depth 0, total) and at depth 1 "Phase 1" (layouts
+ * and map build; "Phases 1-3" for bricks: local maps and stitch), "Phase 4"
+ * (view march) and "Phase 5" (composite and copy-out), each its CUDA-event time
+ * in ms on the renderer's stream. fn = NULL removes the profiler. */
+typedef void (*beams_profile_fn)(void* user, const char* frame, int depth, double ms);
+beams_status beams_set_profiler(beams_renderer* r, beams_profile_fn fn, void* user);
 
 /* ---- learned form ------------------------------------------------------------ */
 /* No reference counterpart: a transmittance network (encoded position and light

@@ -9,7 +9,11 @@
 // raises vtkm::cont::ErrorBadValue.
 #pragma once
 
+#include <algorithm>
 #include <array>
+#include <chrono>
+#include <memory>
+#include <ostream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -43,6 +47,74 @@ struct Field {
   std::array<double, 3> spacing{1, 1, 1};
   bool cell_associated = false;
   bool on_device = false;
+};
+
+// The reference's profiler (beams/Profiler.h:12-60, Profiler.cxx): a tree of
+// named frames, each keeping its elapsed times. StartFrame/EndFrame time host
+// code; a MapperLightedVolume given the profiler adds every render's frames
+// ("Render" > "Phase 1", "Phase 4", "Phase 5", CUDA-event times) under the frame
+// open at that moment. Collect() is local here (one process; the reference
+// reduces over MPI ranks), PrintSummary writes "name: Min = a ms, Max = b ms,
+// Avg = c ms" per frame, two spaces of indent per level, as the reference does.
+class Profiler {
+ public:
+  struct Frame {
+    std::string name;
+    std::vector<double> ms;
+    std::vector<std::unique_ptr<Frame>> sub;
+    std::chrono::steady_clock::time_point start{};
+    Frame* child(const std::string& n) {
+      for (auto& f : sub)
+        if (f->name == n) return f.get();
+      sub.push_back(std::unique_ptr<Frame>(new Frame{n, {}, {}, {}}));
+      return sub.back().get();
+    }
+  };
+
+  explicit Profiler(const std::string& name) : root_(new Frame{name, {}, {}, {}}) {
+    stack_.push_back(root_.get());
+    root_->start = std::chrono::steady_clock::now();
+  }
+  void StartFrame(const std::string& name) {
+    Frame* f = stack_.empty() ? root_.get() : stack_.back()->child(name);
+    stack_.push_back(f);
+    f->start = std::chrono::steady_clock::now();
+  }
+  void EndFrame() {
+    if (stack_.empty()) return;
+    Frame* f = stack_.back();
+    stack_.pop_back();
+    f->ms.push_back(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - f->start).count());
+  }
+  // A frame timed elsewhere: depth 0 under the frame open now, depth d under the
+  // last frame recorded at depth d - 1.
+  void Record(const std::string& name, int depth, double ms) {
+    Frame* parent = depth <= 0 || (size_t)depth > last_.size() ? (stack_.empty() ? root_.get() : stack_.back())
+                                                                : last_[(size_t)depth - 1];
+    Frame* f = parent->child(name);
+    f->ms.push_back(ms);
+    last_.resize((size_t)std::max(depth, 0) + 1);
+    last_[(size_t)std::max(depth, 0)] = f;
+  }
+  void Collect() {}
+  void PrintSummary(std::ostream& os) const { print(os, *root_, 0); }
+  const Frame& Root() const { return *root_; }
+
+ private:
+  static void print(std::ostream& os, const Frame& f, int level) {
+    double mn = 0.0, mx = 0.0, sum = 0.0;
+    if (!f.ms.empty()) {
+      mn = *std::min_element(f.ms.begin(), f.ms.end());
+      mx = *std::max_element(f.ms.begin(), f.ms.end());
+      for (double v : f.ms) sum += v;
+    }
+    os << std::string((size_t)level * 2, ' ') << f.name << ": Min = " << mn << " ms, Max = " << mx
+       << " ms, Avg = " << (f.ms.empty() ? 0.0 : sum / (double)f.ms.size()) << " ms\n";
+    for (const auto& c : f.sub) print(os, *c, level + 1);
+  }
+  std::unique_ptr<Frame> root_;
+  std::vector<Frame*> stack_;
+  std::vector<Frame*> last_;
 };
 
 class MapperLightedVolume {
@@ -85,6 +157,11 @@ class MapperLightedVolume {
     check(beams_set_depth_buffer(r_, depth.data(), width, height, BEAMS_DEPTH_WINDOW, near_plane, far_plane, 0), r_);
   }
   void SetDensityScale(float s) { check(beams_set_density_scale(r_, s), r_); }  // stored, never read (as in the reference)
+  // SetProfiler (MapperLightedVolume.cxx:305-309): every RenderCells adds its frames to p.
+  void SetProfiler(std::shared_ptr<Profiler> p) {
+    check(beams_set_profiler(r_, p ? &MapperLightedVolume::record : nullptr, p.get()), r_);
+    profiler_ = std::move(p);
+  }
   // SetActiveColorTable: the colour table already sampled to RGBA entries.
   void SetActiveColorTable(const std::vector<float>& rgba) {
     if (rgba.empty() || rgba.size() % 4 != 0) throw Error(BEAMS_ERR_INVALID_ARG, "colour table must be RGBA");
@@ -129,7 +206,11 @@ class MapperLightedVolume {
   beams_renderer* handle() { return r_; }
 
  private:
+  static void record(void* user, const char* frame, int depth, double ms) {
+    static_cast<Profiler*>(user)->Record(frame, depth, ms);
+  }
   beams_renderer* r_ = nullptr;
+  std::shared_ptr<Profiler> profiler_;
   int width_ = 0, height_ = 0;
   float sample_distance_ = -1.f;
   std::vector<float> color_map_;

@@ -67,6 +67,10 @@ class Volume(C.Structure):
                 ("assoc", C.c_int), ("on_device", C.c_int)]
 
 
+# beams_profile_fn: (user, frame name, depth, ms)
+PROFILE_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_char_p, C.c_int, C.c_double)
+
+
 class Camera(C.Structure):
     _fields_ = [("position", C.c_double * 3), ("look_at", C.c_double * 3), ("up", C.c_double * 3),
                 ("fov_y_deg", C.c_double), ("width", C.c_int), ("height", C.c_int)]
@@ -198,6 +202,7 @@ def lib():
         "beams_mlp_forward_tc": ([P, P, C.c_int, P], C.c_int),
         "beams_mlp_set_tensor_cores": ([P, C.c_int], C.c_int),
         "beams_mlp_set_probe_first": ([P, C.c_int], C.c_int),
+        "beams_set_profiler": ([P, P, P], C.c_int),
         "beams_mlp_forward_tc_device": ([P, P, C.c_int, P], C.c_int),
         "beams_set_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "beams_set_multi_light": ([P, C.c_int], C.c_int),
@@ -464,6 +469,17 @@ class Renderer:
     def mlp_forward_tc_device(self, features_bf16, T):
         """tcgen05 forward on torch CUDA tensors: features (n, 112) bfloat16, T (n,) float32."""
         self._check(self._L.beams_mlp_forward_tc_device(self._h, _ptr(features_bf16), int(T.numel()), _ptr(T)))
+
+    def set_profiler(self, fn):
+        """fn(frame: str, depth: int, ms: float) after every render (the reference's
+        SetProfiler frames: Render > Phase 1 / Phase 4 / Phase 5); None removes it."""
+        if fn is None:
+            self._profile_cb = None
+            self._check(self._L.beams_set_profiler(self._h, None, None))
+            return
+        cb = PROFILE_FN(lambda _user, frame, depth, ms: fn(frame.decode(), depth, ms))
+        self._profile_cb = cb  # kept alive while set
+        self._check(self._L.beams_set_profiler(self._h, C.cast(cb, C.c_void_p), None))
 
     def mlp_set_tensor_cores(self, enable: bool):
         self._check(self._L.beams_mlp_set_tensor_cores(self._h, int(bool(enable))))

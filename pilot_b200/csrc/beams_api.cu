@@ -1175,8 +1175,33 @@ beams_status beams_get_shadow_map(beams_renderer* r, float* dst, size_t count, i
   return BEAMS_OK;
 }
 
+static beams_status render_frame(beams_renderer* r, const beams_camera* cam, float* rgba_out, int out_on_device,
+                                 beams_timings* t);
+
+beams_status beams_set_profiler(beams_renderer* r, beams_profile_fn fn, void* user) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  r->profile_fn = fn;
+  r->profile_user = fn ? user : nullptr;
+  return BEAMS_OK;
+}
+
 beams_status beams_render(beams_renderer* r, const beams_camera* cam, float* rgba_out, int out_on_device,
                           beams_timings* t) {
+  if (!r || !r->profile_fn) return render_frame(r, cam, rgba_out, out_on_device, t);
+  // a profiler needs the frame's event times: take the timings path
+  beams_timings local{};
+  beams_timings* tt = t ? t : &local;
+  const beams_status s = render_frame(r, cam, rgba_out, out_on_device, tt);
+  if (s != BEAMS_OK) return s;
+  r->profile_fn(r->profile_user, "Render", 0, tt->total_ms);
+  r->profile_fn(r->profile_user, r->brick_mode ? "Phases 1-3" : "Phase 1", 1, tt->map_build_ms);
+  r->profile_fn(r->profile_user, "Phase 4", 1, tt->view_march_ms);
+  r->profile_fn(r->profile_user, "Phase 5", 1, tt->composite_ms);
+  return BEAMS_OK;
+}
+
+static beams_status render_frame(beams_renderer* r, const beams_camera* cam, float* rgba_out, int out_on_device,
+                                 beams_timings* t) {
   if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
   beams_status s = validate_camera(r, cam);
   if (s != BEAMS_OK) return s;

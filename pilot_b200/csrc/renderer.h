@@ -118,6 +118,8 @@ struct beams_renderer {
   float* d_raymax = nullptr;
   size_t raymax_cap = 0;
   int form = BEAMS_FORM_EXACT;
+  beams_profile_fn profile_fn = nullptr;  // beams_set_profiler
+  void* profile_user = nullptr;
 
   // transmittance map
   float* d_map = nullptr;

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <iostream>
 #include <string>
 #include <vector>
 
@@ -57,9 +58,16 @@ int main(int argc, char** argv) {
     f.point_dims = {nx, ny, nz};
     f.origin = {0.0, 0.0, 0.0};
     f.spacing = {1.0 / (nx - 1), 1.0 / (ny - 1), 1.0 / (nz - 1)};
+    auto profiler = std::make_shared<beams::Profiler>("Beams");
+    mapper.SetProfiler(profiler);
     beams_timings t{};
     std::vector<float> rgba = mapper.RenderCells(f, {0.0, 1.0}, camera, &t);
     // ---------------------------------------------------------------------------
+    profiler->StartFrame("Second render");
+    mapper.RenderCells(f, {0.0, 1.0}, camera);
+    profiler->EndFrame();
+    profiler->Collect();
+    profiler->PrintSummary(std::cerr);  // the reference prints to a stream as well
 
     std::ofstream out(dir + "/rgba.bin", std::ios::binary);
     out.write(reinterpret_cast<const char*>(rgba.data()), (std::streamsize)(rgba.size() * sizeof(float)));

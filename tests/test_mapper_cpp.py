@@ -6,7 +6,8 @@ and links libbeams_b200.so.
 CPU: the snippet compiles with g++ -Wall -Werror against the adapter and links.
 GPU: it renders a small seeded scene whose image matches the oracle within the
 exact form's bar (max |dRGBA| <= 2e-3, >= 99.9% of pixels bit-identical) with
-the oracle's lit-sample count.
+the oracle's lit-sample count, and the profiler set with SetProfiler holds the
+two renders' frames in the reference's summary format.
 """
 import subprocess
 from pathlib import Path
@@ -61,3 +62,9 @@ def test_mapper_snippet_renders_like_the_oracle(cuda_device, tmp_path):
     assert err <= TOL, f"max |d| {err}"
     assert np.mean(np.all(img == oimg, axis=-1)) >= 0.999
     assert int(p.stdout.split()[0]) == lit
+    # SetProfiler: the profiler's summary, one line per frame, indented per level
+    lines = p.stderr.splitlines()
+    names = [ln.split(":")[0] for ln in lines]
+    assert names[:6] == ["Beams", "  Render", "    Phase 1", "    Phase 4", "    Phase 5", "  Second render"]
+    assert names[6:] == ["    Render", "      Phase 1", "      Phase 4", "      Phase 5"]
+    assert all("Min = " in ln and "Avg = " in ln for ln in lines)

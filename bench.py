@@ -2,7 +2,7 @@
 """Benchmark of the Beams lighted volume renderer hot path on B200.
 
 One step = one frame of the exact path at the 512^3 noise / 1024x1024 / M = 256
-configuration: the light march that builds the 257^3
+configuration (config 1): the light march that builds the 257^3
 transmittance map (K1) and the view march that shades by it (K2), with the
 field already resident in HBM. Synthetic seeded input; the 512 MiB field is
 larger than L2, so no flush is needed between steps.

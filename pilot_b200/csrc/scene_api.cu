@@ -274,7 +274,7 @@ static beams_status generate_scene(beams_renderer* r, const beams_scene_desc* d,
     }
     s = beams_generate_spheres(f, pts, org, sp, e.data(), 1, def, floor, -0.01f, 0.7f, r->stream);
   } else if (type == "blobs") {
-    // 8 seeded blobs as in the BASELINE configs (centres U[0.2,0.8], sigma U[0.05,0.15], amplitude U[0.5,1])
+    // 8 seeded blobs as in the 128^3 blob workload (centres U[0.2,0.8], sigma U[0.05,0.15], amplitude U[0.5,1])
     std::vector<float> prm;
     unsigned x = d->seed * 2654435761u + 12345u;
     auto u01 = [&]() {

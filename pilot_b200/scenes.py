@@ -1,6 +1,6 @@
 """Seeded synthetic scenes for the Beams renderer (tests and benchmarks).
 
-The reference's data files are not shipped and the BASELINE configurations use
+The reference's data files are not shipped and the benchmark workloads use
 synthetic fields, so every scene here is generated from a seed:
 
 * ``config0``: 128^3 float32 sum of 8 Gaussian blobs (centres U[0.2,0.8]^3,

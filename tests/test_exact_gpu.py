@@ -86,7 +86,7 @@ def test_no_shadow_map(cuda_device):
 
 
 def test_config0_parity(cuda_device):
-    """BASELINE config 0 at full size: 128^3 blobs, 512^2, M = 128, directional light."""
+    """The 128^3 blob workload (config 0) at full size: 512^2, M = 128, directional light."""
     s = scenes.config0()
     img, m, t, _ = gpu_render(s)
     o = Oracle(s)
@@ -104,7 +104,7 @@ def test_config0_parity(cuda_device):
 
 
 def test_config1_full_size_properties(cuda_device):
-    """BASELINE config 1 (512^3 noise, 1024^2, M = 256): properties at full size
+    """The 512^3 noise workload (config 1: 1024^2, M = 256): properties at full size
     plus oracle parity on a random vertex subset and an image crop."""
     import torch
     s = scenes.config1()

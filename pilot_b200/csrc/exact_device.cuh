@@ -222,17 +222,21 @@ __device__ __forceinline__ int find_cell_bsearch_t(const float4* T, int cmax, fl
   return c;
 }
 
-// The same search for a sample already inside the volume: val >= org exactly
-// (org is the volume's first coordinate), so the guess needs no lower clamp.
-__device__ __forceinline__ int find_cell_bsearch_in(const float4* T, int cmax, float org, float invh, float val,
-                                                    float4& e) {
-  int c = trunc_small(fminf((val - org) * invh, (float)cmax));
-  e = T[c];
-  if (val <= e.x || val > e.y) {
-    while (c > 0 && val <= e.x) e = T[--c];
-    while (c < cmax && val > e.y) e = T[++c];
-  }
+// The bounded walk that settles a seeded light-march cell guess (the smallest
+// c with val <= coord(c+1), RectilinearMeshOracle.h:154-176), for the rare
+// sample within an ulp of a cell face; kept out of line (noinline) so that the
+// march's common path carries none of its code.
+static __device__ __noinline__ int walk_cell_bsearch(const float4* T, int cmax, float val, int c) {
+  float4 e = T[c];
+  while (c > 0 && val <= e.x) e = T[--c];
+  while (c < cmax && val > e.y) e = T[++c];
   return c;
+}
+static __device__ __noinline__ int3 walk_cells_bsearch(const float4* T0, const float4* T1, const float4* T2, int m0,
+                                                       int m1, int m2, float v0, float v1, float v2, int c0, int c1,
+                                                       int c2) {
+  return make_int3(walk_cell_bsearch(T0, m0, v0, c0), walk_cell_bsearch(T1, m1, v1, c1),
+                   walk_cell_bsearch(T2, m2, v2, c2));
 }
 
 // Searches for explicit (non-uniform) rectilinear coordinates, where no seed
@@ -273,6 +277,57 @@ __device__ __forceinline__ int find_cell_walk_t(const float4* T, int cmax, float
     while (c < cmax && p >= e.y) e = T[++c];
   }
   return c;
+}
+
+// The view march's walk (the unique c with coord(c) <= p < coord(c+1)) that
+// settles seeded guesses off by a face, out of line like walk_cells_bsearch.
+static __device__ __noinline__ int walk_cell_view(const float4* T, int cmax, float p, int c) {
+  float4 e = T[c];
+  while (c > 0 && p < e.x) e = T[--c];
+  while (c < cmax && p >= e.y) e = T[++c];
+  return c;
+}
+static __device__ __noinline__ int3 walk_cells_view(const float4* T0, const float4* T1, const float4* T2, int m0,
+                                                    int m1, int m2, float v0, float v1, float v2, int c0, int c1,
+                                                    int c2) {
+  return make_int3(walk_cell_view(T0, m0, v0, c0), walk_cell_view(T1, m1, v1, c1), walk_cell_view(T2, m2, v2, c2));
+}
+
+// The view march's cell location on a uniform grid when a sample leaves its
+// cell (RectilinearLocator::LocateCell, LightedVolumeRenderer.cxx:119-165):
+// seeded guesses, one branch testing the three axes, the rare walk out of line.
+// On a max face the cell is the last one and inv[k] is left as it was (the
+// reference keeps the previous invSpacing there); bl[k] = the cell's lower
+// coordinate.
+__device__ __forceinline__ void locate_view_cell(const ExactGeo& g, const float4* s_tab, const float p[3], int c[3],
+                                                 float inv[3], float bl[3]) {
+  float4 e[3];
+  bool off = false;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    c[k] = trunc_small(fminf(fmaxf((p[k] - g.org[k]) * g.invh[k], 0.f), (float)(g.n[k] - 2)));
+    e[k] = s_tab[g.ax_off[k] + c[k]];
+    off = off | (p[k] < e[k].x) | (p[k] >= e[k].y);
+  }
+  if (off) {
+    const int3 cc = walk_cells_view(s_tab + g.ax_off[0], s_tab + g.ax_off[1], s_tab + g.ax_off[2], g.n[0] - 2,
+                                    g.n[1] - 2, g.n[2] - 2, p[0], p[1], p[2], c[0], c[1], c[2]);
+    c[0] = cc.x;
+    c[1] = cc.y;
+    c[2] = cc.z;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) e[k] = s_tab[g.ax_off[k] + c[k]];
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (p[k] == g.maxp[k]) {
+      c[k] = g.n[k] - 2;
+      e[k] = s_tab[g.ax_off[k] + c[k]];
+    } else {
+      inv[k] = e[k].w;  // 1.f / (coord(c+1) - coord(c)), IEEE
+    }
+    bl[k] = e[k].x;
+  }
 }
 
 // TF index of the light march (TransmittanceMap.h:322-326): truncate, clamp to

@@ -305,19 +305,7 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
         if (maxt > 1.f || mint < 0.f) newCell = true;
         if (newCell) {
           int c[3];
-#pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            const float4* T = s_tab + g.ax_off[k];
-            float4 e;
-            if (p[k] == g.maxp[k]) {
-              c[k] = g.n[k] - 2;
-              e = T[c[k]];
-            } else {
-              c[k] = find_cell_walk_t(T, g.n[k] - 2, g.org[k], g.invh[k], p[k], e);
-              inv[k] = e.w;
-            }
-            bl[k] = e.x;
-          }
+          locate_view_cell(g, s_tab, p, c, inv, bl);
           float v[8];
           QuadLoad<QuadT>::cell(quads, (unsigned)c[2] * qz + (unsigned)c[1] * qx + (unsigned)c[0], qx, qz, v);
           s0 = v[0];

@@ -78,19 +78,22 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT*
     const float maxt = mx(tx, mx(ty, tz));
     if (maxt > 1.f || mint < 0.f) newCell = true;
     if (newCell) {
+      if constexpr (RECT) {
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const float4* T = s_tab + g.ax_off[k];
-        float4 e;
-        if (p[k] == g.maxp[k]) {
-          c[k] = g.n[k] - 2;  // the reference leaves invSpacing[k] unchanged here
-          e = T[c[k]];
-        } else {
-          if constexpr (RECT) c[k] = find_cell_walk_rect(T, g.n[k] - 2, p[k], e);
-          else c[k] = find_cell_walk_t(T, g.n[k] - 2, g.org[k], g.invh[k], p[k], e);
-          inv[k] = e.w;  // 1.f / (coord(c+1) - coord(c)), IEEE
+        for (int k = 0; k < 3; ++k) {
+          const float4* T = s_tab + g.ax_off[k];
+          float4 e;
+          if (p[k] == g.maxp[k]) {
+            c[k] = g.n[k] - 2;  // the reference leaves invSpacing[k] unchanged here
+            e = T[c[k]];
+          } else {
+            c[k] = find_cell_walk_rect(T, g.n[k] - 2, p[k], e);
+            inv[k] = e.w;  // 1.f / (coord(c+1) - coord(c)), IEEE
+          }
+          bl[k] = e.x;
         }
-        bl[k] = e.x;
+      } else {
+        locate_view_cell(g, s_tab, p, c, inv, bl);
       }
       float v[8];
       QuadLoad<QuadT>::cell(quads, (unsigned)c[2] * qz + (unsigned)c[1] * qx + (unsigned)c[0], qx, qz, v);

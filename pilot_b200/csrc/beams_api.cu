@@ -179,6 +179,7 @@ beams_status make_geo_vol(beams_renderer* r, const beams_volume& v, const beams_
     off += r->map_m[d];
   }
   g.ntab = off;
+  geo_loop_constants(g);
   g.slab_fp64 = r->slab_fp64;
   g.use_map = r->use_map ? 1 : 0;
   g.assoc_cells = (v.assoc == BEAMS_ASSOC_CELLS) ? 1 : 0;

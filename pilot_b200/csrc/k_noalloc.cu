@@ -190,6 +190,7 @@ extern "C" beams_status beams_render_noalloc(const beams_volume* vol, const floa
     }
     g.ntab = off;
   }
+  geo_loop_constants(g);
   float ext[3];
   for (int d = 0; d < 3; ++d) ext[d] = (float)(g.bmax[d] - g.bmin[d]);
   g.extent_mag = std::sqrt(ext[0] * ext[0] + ext[1] * ext[1] + ext[2] * ext[2]);

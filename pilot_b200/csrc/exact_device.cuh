@@ -336,6 +336,10 @@ __device__ __forceinline__ void locate_view_cell(const ExactGeo& g, const float4
 __device__ __forceinline__ int tf_index_clamped(float fi, int n1) {
   return trunc_small(fminf(fmaxf(fi, 0.f), (float)n1));
 }
+// The same with the top index given as a float (n1f = (float)n1).
+__device__ __forceinline__ int tf_index_clamped_f(float fi, float n1f) {
+  return trunc_small(fminf(fmaxf(fi, 0.f), n1f));
+}
 
 // Pinhole camera ray through pixel centre (x, y).
 __device__ __forceinline__ void camera_ray(const ExactGeo& g, int x, int y, float o[3], float d[3]) {

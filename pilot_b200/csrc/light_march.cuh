@@ -192,16 +192,26 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
   float va[8], pa[3];
   unsigned ska;
   if constexpr (!PIPE) {
+    // Every gen() call takes one step (fast or b), so the samples marched are
+    // the steps taken less a failing last one: the precision march counts them
+    // so at the end (its 640^3 build 6.06 -> 5.96 ms); the exact march counts
+    // per sample, which runs faster there (2.38 against 2.42 ms).
+    const int steps0 = fast + b;
     for (;;) {
       if (!gen(va, pa, ska)) {
-        ns += ska;  // skipped samples before the end of the ray
+        if constexpr (PREC) ns += (unsigned)(steps0 - (fast + b) - 1);
+        else ns += ska;  // skipped samples before the end of the ray
         break;
       }
       float scalar = hex_interp(va, pa[0], pa[1], pa[2]);
       scalar = (scalar - g.min_scalar) * g.inv_delta;
-      ns += 1 + ska;
+      if constexpr (!PREC) ns += 1 + ska;
       // Stop when the accumulated value can no longer change (see Accum).
-      if (acc.add(s_a, s_tau, tf_index_clamped(scalar * (PREC ? (float)n1 : g.n1f), n1))) break;
+      const int ti = PREC ? tf_index_clamped(scalar * (float)n1, n1) : tf_index_clamped_f(scalar * g.n1f, g.n1f);
+      if (acc.add(s_a, s_tau, ti)) {
+        if constexpr (PREC) ns += (unsigned)(steps0 - (fast + b));
+        break;
+      }
     }
     return;
   }
@@ -216,7 +226,7 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
     {
       float scalar = hex_interp(va, pa[0], pa[1], pa[2]);
       scalar = (scalar - g.min_scalar) * g.inv_delta;
-      done = acc.add(s_a, s_tau, tf_index_clamped(scalar * (PREC ? (float)n1 : g.n1f), n1));
+      done = acc.add(s_a, s_tau, (PREC ? tf_index_clamped(scalar * (float)n1, n1) : tf_index_clamped_f(scalar * g.n1f, g.n1f)));
       ns += 1 + ska;
     }
     // Stop when the accumulated value can no longer change (see Accum).
@@ -229,7 +239,7 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
     {
       float scalar = hex_interp(vb, pb[0], pb[1], pb[2]);
       scalar = (scalar - g.min_scalar) * g.inv_delta;
-      done = acc.add(s_a, s_tau, tf_index_clamped(scalar * (PREC ? (float)n1 : g.n1f), n1));
+      done = acc.add(s_a, s_tau, (PREC ? tf_index_clamped(scalar * (float)n1, n1) : tf_index_clamped_f(scalar * g.n1f, g.n1f)));
       ns += 1 + skb;
     }
     if (done) break;

@@ -305,7 +305,7 @@ __device__ __forceinline__ void locate_view_cell(const ExactGeo& g, const float4
   bool off = false;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    c[k] = trunc_small(fminf(fmaxf((p[k] - g.org[k]) * g.invh[k], 0.f), g.cmaxf[k]));
+    c[k] = trunc_small(fminf(fmaxf((p[k] - g.org[k]) * g.invh[k], 0.f), (float)(g.n[k] - 2)));
     e[k] = s_tab[g.ax_off[k] + c[k]];
     off = off | (p[k] < e[k].x) | (p[k] >= e[k].y);
   }
@@ -534,10 +534,7 @@ __device__ __forceinline__ float bf16_hi(unsigned u) { return __uint_as_float(u 
 __device__ __forceinline__ float f16_lo(unsigned u) { return __half2float(__ushort_as_half((unsigned short)(u & 0xffffu))); }
 __device__ __forceinline__ float f16_hi(unsigned u) { return __half2float(__ushort_as_half((unsigned short)(u >> 16))); }
 template <> struct QuadLoad<QuadBF16> {
-  static __device__ __forceinline__ void strides(const ExactGeo& g, unsigned& qx, unsigned& qz) {
-    qx = g.qxs;
-    qz = g.qzs;
-  }
+  static __device__ __forceinline__ void strides(const ExactGeo& g, unsigned& qx, unsigned& qz) { quad_strides(g, qx, qz); }
   static __device__ __forceinline__ void cell(const QuadBF16* __restrict__ q, unsigned qi, unsigned, unsigned qz, float v[8]) {
     const uint2 a = __ldg((const uint2*)(q + qi));
     const uint2 b = __ldg((const uint2*)(q + qi + qz));
@@ -546,10 +543,7 @@ template <> struct QuadLoad<QuadBF16> {
   }
 };
 template <> struct QuadLoad<QuadF16> {
-  static __device__ __forceinline__ void strides(const ExactGeo& g, unsigned& qx, unsigned& qz) {
-    qx = g.qxs;
-    qz = g.qzs;
-  }
+  static __device__ __forceinline__ void strides(const ExactGeo& g, unsigned& qx, unsigned& qz) { quad_strides(g, qx, qz); }
   static __device__ __forceinline__ void cell(const QuadF16* __restrict__ q, unsigned qi, unsigned, unsigned qz, float v[8]) {
     const uint2 a = __ldg((const uint2*)(q + qi));
     const uint2 b = __ldg((const uint2*)(q + qi + qz));
@@ -558,10 +552,7 @@ template <> struct QuadLoad<QuadF16> {
   }
 };
 template <> struct QuadLoad<float4> {
-  static __device__ __forceinline__ void strides(const ExactGeo& g, unsigned& qx, unsigned& qz) {
-    qx = g.qxs;
-    qz = g.qzs;
-  }
+  static __device__ __forceinline__ void strides(const ExactGeo& g, unsigned& qx, unsigned& qz) { quad_strides(g, qx, qz); }
   static __device__ __forceinline__ void cell(const float4* __restrict__ q, unsigned qi, unsigned, unsigned qz, float v[8]) {
     const float4 a = __ldg(q + qi);
     const float4 b = __ldg(q + qi + qz);

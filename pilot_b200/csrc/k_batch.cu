@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch(const ExactGeo* __re
           light_origin(sg, V, L);
           Accum<false> acc;
           unsigned ns = 0;
-          march_vertex<float4, false, SKIP, false, SKIP && MODE != 0>(sg, sd.quads, s_tab + sg.ax_off[0], s_tab + sg.ax_off[1],
+          march_vertex<float4, false, SKIP, false, SKIP && MODE != 0, true>(sg, sd.quads, s_tab + sg.ax_off[0], s_tab + sg.ax_off[1],
                                             s_tab + sg.ax_off[2], s_a, nullptr, sd.occ, V, L,
                                             [](const float*) { return 0.f; }, acc, ns);
           acc.store(sd.map, id);

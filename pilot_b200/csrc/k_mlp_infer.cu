@@ -238,6 +238,8 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
   const int tiles_x = (g.width + 7) >> 3;
   const int nprobe = probe.nqx * probe.nqy;
   const int ntiles = pass.probes_only ? (nprobe + 31) >> 5 : tiles_x * ((g.height + 3) >> 2);
+  const unsigned qx = (unsigned)(g.n[0] - 1), qz = (unsigned)(g.n[0] - 1) * (unsigned)(g.n[1] - 1);
+  const int n1 = g.tf_n - 1;
   unsigned lit = 0, hit = 0, evals = 0, rows = 0;
   for (int tile = next_warp_tile_mlp(&cnt->tiles_view); tile < ntiles; tile = next_warp_tile_mlp(&cnt->tiles_view)) {
     const int lane = threadIdx.x & 31;
@@ -305,8 +307,7 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
           int c[3];
           locate_view_cell(g, s_tab, p, c, inv, bl);
           float v[8];
-          QuadLoad<QuadT>::cell(quads, (unsigned)c[2] * g.qzs + (unsigned)c[1] * g.qxs + (unsigned)c[0], g.qxs,
-                                g.qzs, v);
+          QuadLoad<QuadT>::cell(quads, (unsigned)c[2] * qz + (unsigned)c[1] * qx + (unsigned)c[0], qx, qz, v);
           s0 = v[0];
           s3 = v[3];
           s4 = v[4];
@@ -328,8 +329,8 @@ __global__ void __launch_bounds__(256, 2) k_view_march_mlp(const ExactGeo g, con
         const float bot = l01 + ty * (l32 - l01);
         float fs = bot + tz * (top - bot);
         fs = (fs - g.min_scalar) * g.inv_delta;
-        const float fi = fs * g.n1f;
-        if (fi > -1.f && fi < g.n1f + 1.f) {
+        const float fi = fs * (float)n1;
+        if (fi > -1.f && fi < (float)(n1 + 1)) {
           const int ti = trunc_small(fmaxf(fi, 0.f));  // (int)fi: fi in (-1, n1 + 1)
           const float4 tfc = s_tf[ti];
           const float sa = tfc.w * (1.f - color.w);

@@ -65,20 +65,21 @@ template <> struct Accum<true> {
 // exact form's skipping march; elsewhere the march issues one sample at a time,
 // which needs fewer registers and instructions (the 257^3-vertex map of a
 // 512^3 noise field went 2.97 -> 2.78 ms at 4 blocks per SM, 2.70 ms at 6).
-template <typename QuadT, bool PREC, bool SKIP, bool RECT = false, bool PIPE = SKIP && !PREC, typename Prefix>
+template <typename QuadT, bool PREC, bool SKIP, bool RECT = false, bool PIPE = SKIP && !PREC, bool REG_CONSTS = PREC,
+          typename Prefix>
 __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __restrict__ quads, const float4* T0,
                                              const float4* T1, const float4* T2, const float* s_a,
                                              const float* s_tau, const unsigned char* __restrict__ occ,
                                              const float V[3], const float L[3], Prefix prefix, Accum<PREC>& acc,
                                              unsigned& ns) {
   const int cm0 = g.n[0] - 2, cm1 = g.n[1] - 2, cm2 = g.n[2] - 2;
-  unsigned qx, qz;  // FieldF32 and the precision form; the exact form's quads read g.qxs, g.qzs
-  if constexpr (PREC) {
-    qx = (unsigned)(g.n[0] - 1);
-    qz = qx * (unsigned)(g.n[1] - 1);
-  } else {
-    QuadLoad<QuadT>::strides(g, qx, qz);
-  }
+  // Loop constants: with REG_CONSTS derived here (held in registers), else read
+  // at each use from g's loop-constant fields, which in a kernel's parameter
+  // block cost no registers (the exact light march: 2.59 -> 2.38 ms at six
+  // blocks per SM). The precision march (1.5% faster so) and the batch kernel,
+  // whose geometry lives in shared memory, derive them.
+  unsigned qx, qz;  // FieldF32, and quads with REG_CONSTS
+  QuadLoad<QuadT>::strides(g, qx, qz);
   const int n1 = g.tf_n - 1;
   const float v[3] = {V[0] - L[0], V[1] - L[1], V[2] - L[2]};
   const float rs = 1.f / sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
@@ -148,11 +149,9 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
         // code (the 257^3-vertex map of a 512^3 noise field: 2.66 -> 2.59 ms;
         // the same walks inline behind one branch ran 2.75 ms, and three
         // separate per-axis branches 2.66 ms)
-        // the clamps from the parameter space in the exact form (kept in
-        // registers, the precision march's 640^3 build ran 1.5% faster)
-        c0 = trunc_small(fminf((s[0] - g.org[0]) * g.invh[0], PREC ? (float)cm0 : g.cmaxf[0]));
-        c1 = trunc_small(fminf((s[1] - g.org[1]) * g.invh[1], PREC ? (float)cm1 : g.cmaxf[1]));
-        c2 = trunc_small(fminf((s[2] - g.org[2]) * g.invh[2], PREC ? (float)cm2 : g.cmaxf[2]));
+        c0 = trunc_small(fminf((s[0] - g.org[0]) * g.invh[0], REG_CONSTS ? (float)cm0 : g.cmaxf[0]));
+        c1 = trunc_small(fminf((s[1] - g.org[1]) * g.invh[1], REG_CONSTS ? (float)cm1 : g.cmaxf[1]));
+        c2 = trunc_small(fminf((s[2] - g.org[2]) * g.invh[2], REG_CONSTS ? (float)cm2 : g.cmaxf[2]));
         e0 = T0[c0];
         e1 = T1[c1];
         e2 = T2[c2];
@@ -177,7 +176,7 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
           }
         }
       }
-      if constexpr (PREC || std::is_same<QuadT, FieldF32>::value)
+      if constexpr (REG_CONSTS || std::is_same<QuadT, FieldF32>::value)
         QuadLoad<QuadT>::cell(quads, (unsigned)c2 * qz + (unsigned)c1 * qx + (unsigned)c0, qx, qz, v8);
       else  // the quad strides straight from the parameter space
         QuadLoad<QuadT>::cell(quads, (unsigned)c2 * g.qzs + (unsigned)c1 * g.qxs + (unsigned)c0, g.qxs, g.qzs, v8);
@@ -207,7 +206,7 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
       scalar = (scalar - g.min_scalar) * g.inv_delta;
       if constexpr (!PREC) ns += 1 + ska;
       // Stop when the accumulated value can no longer change (see Accum).
-      const int ti = PREC ? tf_index_clamped(scalar * (float)n1, n1) : tf_index_clamped_f(scalar * g.n1f, g.n1f);
+      const int ti = REG_CONSTS ? tf_index_clamped(scalar * (float)n1, n1) : tf_index_clamped_f(scalar * g.n1f, g.n1f);
       if (acc.add(s_a, s_tau, ti)) {
         if constexpr (PREC) ns += (unsigned)(steps0 - (fast + b));
         break;
@@ -226,7 +225,7 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
     {
       float scalar = hex_interp(va, pa[0], pa[1], pa[2]);
       scalar = (scalar - g.min_scalar) * g.inv_delta;
-      done = acc.add(s_a, s_tau, (PREC ? tf_index_clamped(scalar * (float)n1, n1) : tf_index_clamped_f(scalar * g.n1f, g.n1f)));
+      done = acc.add(s_a, s_tau, (REG_CONSTS ? tf_index_clamped(scalar * (float)n1, n1) : tf_index_clamped_f(scalar * g.n1f, g.n1f)));
       ns += 1 + ska;
     }
     // Stop when the accumulated value can no longer change (see Accum).
@@ -239,7 +238,7 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
     {
       float scalar = hex_interp(vb, pb[0], pb[1], pb[2]);
       scalar = (scalar - g.min_scalar) * g.inv_delta;
-      done = acc.add(s_a, s_tau, (PREC ? tf_index_clamped(scalar * (float)n1, n1) : tf_index_clamped_f(scalar * g.n1f, g.n1f)));
+      done = acc.add(s_a, s_tau, (REG_CONSTS ? tf_index_clamped(scalar * (float)n1, n1) : tf_index_clamped_f(scalar * g.n1f, g.n1f)));
       ns += 1 + skb;
     }
     if (done) break;

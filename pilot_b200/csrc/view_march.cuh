@@ -63,6 +63,7 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT*
   float s0 = 0.f, s1m0 = 0.f, s2m3 = 0.f, s3 = 0.f, s4 = 0.f, s5m4 = 0.f, s6m7 = 0.f, s7 = 0.f;
   int c[3] = {0, 0, 0};
   float inv[3] = {0.f, 0.f, 0.f};
+  const int n1 = g.tf_n - 1;
   while (inside_vol(g, p) && dist < maxD && budget-- > 0) {
     if (SKIP && !occupied(g, occ, p)) {
       ++lit;
@@ -97,11 +98,7 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT*
         locate_view_cell(g, s_tab, p, c, inv, bl);
       }
       float v[8];
-      if constexpr (std::is_same<QuadT, FieldF32>::value)
-        QuadLoad<QuadT>::cell(quads, (unsigned)c[2] * qz + (unsigned)c[1] * qx + (unsigned)c[0], qx, qz, v);
-      else  // the quad strides straight from the parameter space
-        QuadLoad<QuadT>::cell(quads, (unsigned)c[2] * g.qzs + (unsigned)c[1] * g.qxs + (unsigned)c[0], g.qxs, g.qzs,
-                              v);
+      QuadLoad<QuadT>::cell(quads, (unsigned)c[2] * qz + (unsigned)c[1] * qx + (unsigned)c[0], qx, qz, v);
       s0 = v[0];
       s3 = v[3];
       s4 = v[4];
@@ -123,8 +120,8 @@ __device__ __forceinline__ void view_march_pixel(const ExactGeo& g, const QuadT*
     const float bot = l01 + ty * (l32 - l01);
     float fs = bot + tz * (top - bot);
     fs = (fs - g.min_scalar) * g.inv_delta;
-    const float fi = fs * g.n1f;
-    if (fi > -1.f && fi < g.n1f + 1.f) {
+    const float fi = fs * (float)n1;
+    if (fi > -1.f && fi < (float)(n1 + 1)) {
       const float4 tfc = s_tf[trunc_small(fmaxf(fi, 0.f))];  // (int)fi: fi in (-1, n1 + 1)
       float sc0 = tfc.x, sc1 = tfc.y, sc2 = tfc.z;
       const float sa = tfc.w * (1.f - color.w);

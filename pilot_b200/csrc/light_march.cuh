@@ -187,6 +187,10 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
       return true;
     }
   };
+  // TF index of a normalised scalar (TransmittanceMap.h:322-326)
+  auto tf_idx = [&](float scalar) {
+    return REG_CONSTS ? tf_index_clamped(scalar * (float)n1, n1) : tf_index_clamped_f(scalar * g.n1f, g.n1f);
+  };
   acc.init(prefix(dir));
   float va[8], pa[3];
   unsigned ska;
@@ -206,8 +210,7 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
       scalar = (scalar - g.min_scalar) * g.inv_delta;
       if constexpr (!PREC) ns += 1 + ska;
       // Stop when the accumulated value can no longer change (see Accum).
-      const int ti = REG_CONSTS ? tf_index_clamped(scalar * (float)n1, n1) : tf_index_clamped_f(scalar * g.n1f, g.n1f);
-      if (acc.add(s_a, s_tau, ti)) {
+      if (acc.add(s_a, s_tau, tf_idx(scalar))) {
         if constexpr (PREC) ns += (unsigned)(steps0 - (fast + b));
         break;
       }
@@ -225,7 +228,7 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
     {
       float scalar = hex_interp(va, pa[0], pa[1], pa[2]);
       scalar = (scalar - g.min_scalar) * g.inv_delta;
-      done = acc.add(s_a, s_tau, (REG_CONSTS ? tf_index_clamped(scalar * (float)n1, n1) : tf_index_clamped_f(scalar * g.n1f, g.n1f)));
+      done = acc.add(s_a, s_tau, tf_idx(scalar));
       ns += 1 + ska;
     }
     // Stop when the accumulated value can no longer change (see Accum).
@@ -238,7 +241,7 @@ __device__ __forceinline__ void march_vertex(const ExactGeo& g, const QuadT* __r
     {
       float scalar = hex_interp(vb, pb[0], pb[1], pb[2]);
       scalar = (scalar - g.min_scalar) * g.inv_delta;
-      done = acc.add(s_a, s_tau, (REG_CONSTS ? tf_index_clamped(scalar * (float)n1, n1) : tf_index_clamped_f(scalar * g.n1f, g.n1f)));
+      done = acc.add(s_a, s_tau, tf_idx(scalar));
       ns += 1 + skb;
     }
     if (done) break;

@@ -261,7 +261,9 @@ beams_status beams_set_form(beams_renderer* r, int form, const void* opts);
  * share their face plane. Up to 32 blocks. beams_set_volume leaves this mode. */
 beams_status beams_set_bricks(beams_renderer* r, const beams_volume* bricks, int nbricks);
 /* Copies brick `brick`'s map after the last render: stage 0 = Phase 1 (local),
- * stage 1 = stitched. For tests and tools. */
+ * stage 1 = stitched. When no two bricks overlap, Phase 1 builds only the
+ * vertices within one layer of a brick face (the only ones the stitch reads);
+ * the other stage-0 entries are then unspecified. For tests and tools. */
 beams_status beams_get_brick_map(beams_renderer* r, int brick, int stage, float* dst, size_t count,
                                  int dst_on_device);
 

@@ -14,6 +14,13 @@ pytestmark = pytest.mark.gpu
 TOL = 2e-3
 
 
+def shell_mask(pd):
+    """Vertices (x fastest) with an index in {0, 1, pd-2, pd-1} on some axis."""
+    i = np.arange(pd)
+    edge = (i <= 1) | (i >= pd - 2)
+    return (edge[:, None, None] | edge[None, :, None] | edge[None, None, :]).ravel()
+
+
 def gpu_bricks(bricks):
     r = B.Renderer(0)
     r.set_bricks([(b.field_numpy(), b.origin, b.spacing, b.value_range) for b in bricks])
@@ -31,7 +38,10 @@ def test_bricks_match_oracle(cuda_device, kind, light_kind, splits):
     orgba, _, olocal, ofinal, olit = render_bricks(bricks)
     for i, b in enumerate(bricks):
         nv = (b.map_m + 1) ** 3
-        assert np.array_equal(r.get_brick_map(i, 0, nv), olocal[i]), f"brick {i} local map"
+        # Phase 1 builds the vertices the stitch reads: those within one layer of a brick face
+        shell = shell_mask(b.map_m + 1)
+        assert np.array_equal(r.get_brick_map(i, 0, nv)[shell], np.asarray(olocal[i]).ravel()[shell]), \
+            f"brick {i} local map"
         assert np.array_equal(r.get_brick_map(i, 1, nv), ofinal[i]), f"brick {i} stitched map"
     err = np.abs(img - orgba)
     assert err.max() <= TOL and np.mean(np.all(img == orgba, axis=-1)) > 0.999

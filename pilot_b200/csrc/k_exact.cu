@@ -42,14 +42,14 @@ __device__ __forceinline__ void load_tables(float4* s_tab, const float4* __restr
 // STITCH: the multi-brick Phase 3 — the march starts from the cross-brick
 // prefix (stitch_prefix) instead of zero, as GenerateEstimator is re-run on
 // the prefix opacities (LightedVolumeRenderer.cxx:1241-1252).
-// Blocks per SM: 6 (40 registers) for the plain exact march, which then issues
-// one sample at a time (the 257^3-vertex map of a 512^3 noise field: 2.70 ms
-// against 2.78 ms at 4 blocks); the
-// skipping, precision, stitching and rectilinear marches keep 4 (at 6 they
+// Blocks per SM: 6 (40 registers) for the plain and the stitching exact march,
+// which issue one sample at a time (the 257^3-vertex map of a 512^3 noise
+// field: 2.70 ms against 2.78 ms at 4 blocks; the 2x2x2-brick frame 0.7% faster
+// than at 4); the skipping, precision and rectilinear marches keep 4 (at 6 they
 // spill: the 640^3 precision build went 6.4 -> 9.5 ms).
 template <bool STITCH, bool PREC, bool SKIP, bool RECT>
 constexpr int k1_blocks_per_sm() {
-  return (STITCH || PREC || SKIP || RECT) ? 4 : 6;
+  return (PREC || SKIP || RECT) ? 4 : 6;
 }
 
 // Multi-brick Phase 1: the vertex lies within one layer of a face of the map.

@@ -524,6 +524,27 @@ static cudaError_t brick_lanes_join(beams_renderer* r) {
 
 // One frame of a multi-block scene: Phase 1 local maps, Phases 2-3 stitched
 // maps, Phase 4 per-brick view marches, Phase 5 depth-ordered composite.
+// Cell mask of the outer cell layer of a pd[0] x pd[1] x pd[2]-vertex map
+// (cells with index 0 or pd-2 on some axis), built on the host once per map
+// size: a masked K1 then builds exactly the vertices within one layer of a face.
+static beams_status brick_shell_mask(beams_renderer* r, const int pd[3]) {
+  if (r->d_shell_mask && std::memcmp(r->shell_pd, pd, sizeof(r->shell_pd)) == 0) return BEAMS_OK;
+  const int mx = pd[0] - 1, my = pd[1] - 1, mz = pd[2] - 1;
+  std::vector<unsigned char> h((size_t)mx * my * mz);
+  for (int z = 0; z < mz; ++z)
+    for (int y = 0; y < my; ++y)
+      for (int x = 0; x < mx; ++x)
+        h[((size_t)z * my + y) * mx + x] =
+            (x == 0 || y == 0 || z == 0 || x == mx - 1 || y == my - 1 || z == mz - 1) ? 1 : 0;
+  beams_status s = ensure_buffer(r, (void**)&r->d_shell_mask, &r->shell_cap, h.size(), "allocating the shell mask");
+  if (s != BEAMS_OK) return s;
+  cudaError_t e = cudaMemcpyAsync(r->d_shell_mask, h.data(), h.size(), cudaMemcpyHostToDevice, r->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(r->stream);  // h goes out of scope
+  if (e != cudaSuccess) return cuda_fail(r, e, "copying the shell mask");
+  std::memcpy(r->shell_pd, pd, sizeof(r->shell_pd));
+  return BEAMS_OK;
+}
+
 // Within a phase the bricks' launches are independent and run on the lanes;
 // the phases are joined on r->stream (Phase 3 reads every Phase-1 map, Phase 5
 // every brick image).
@@ -588,13 +609,20 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
           inside = inside && G[a].bmin[d] < G[b].bmax[d] && G[b].bmin[d] < G[a].bmax[d];
         disjoint = !inside;
       }
+    // the outer cell layer marked: its corners are those vertices (one mask for
+    // every brick, the map size is shared)
+    const unsigned char* shell = nullptr;
+    if (disjoint && nb > 1) {
+      s = brick_shell_mask(r, G[0].pd);
+      if (s != BEAMS_OK) return s;
+      shell = r->d_shell_mask;
+    }
     s = brick_lanes_fork(r);
     if (s != BEAMS_OK) return s;
     for (int b = 0; b < nb; ++b) {
       Brick& B = r->bricks[b];
-      ExactGeo g1 = G[b];
-      g1.shell_only = (disjoint && nb > 1) ? 1 : 0;
-      e = launch_light_march_f32(g1, B.d_quads, B.d_tab, r->d_tf, B.d_map_local, r->d_brick_cnt + b, lane(b));
+      e = launch_light_march_f32(G[b], B.d_quads, B.d_tab, r->d_tf, B.d_map_local, r->d_brick_cnt + b, lane(b),
+                                 nullptr, 0, -1, nullptr, nullptr, shell);
       if (e != cudaSuccess) return lane_fail(e, "brick light march");
       ++launches;
     }

@@ -47,11 +47,6 @@ struct ExactGeo {
   // bricks of 2^b vertices per edge in brick order (rays in flight stay in a
   // narrow cone towards the light, so the field they read stays in L2).
   int light_brick_log2;
-  // Multi-brick Phase 1 (the local maps): the stitch reads another brick's
-  // local map only at the exit point of a light segment from that brick, on
-  // its boundary, so K1 builds only the vertices within one layer of a face
-  // (index 0, 1, pd-2 or pd-1 on some axis). 0: every vertex.
-  int shell_only;
   // Brick order that follows the light: bricks are visited in pencils along
   // bo_axis[0] (the axis the light travels most along, in map-vertex units),
   // the two other brick coordinates (bo_axis[1], bo_axis[2]) sheared by

@@ -52,13 +52,9 @@ constexpr int k1_blocks_per_sm() {
   return (PREC || SKIP || RECT) ? 4 : 6;
 }
 
-// Multi-brick Phase 1: the vertex lies within one layer of a face of the map.
-__device__ __forceinline__ bool vertex_on_shell(const int pd[3], int x, int y, int z) {
-  return x <= 1 || y <= 1 || z <= 1 || x >= pd[0] - 2 || y >= pd[1] - 2 || z >= pd[2] - 2;
-}
-
-// The learned form's lazy map: vertex (x, y, z) is needed when one of the (up
-// to 8) map cells it is a corner of was marked (one byte per cell, x fastest).
+// A masked map build (the learned form's lazy map, the multi-brick Phase 1):
+// vertex (x, y, z) is built when one of the (up to 8) map cells it is a corner
+// of is marked (one byte per cell, x fastest).
 __device__ __forceinline__ bool vertex_in_marked_cell(const unsigned char* __restrict__ cm, const int pd[3], int x,
                                                       int y, int z) {
   const int mx = pd[0] - 1, my = pd[1] - 1, mz = pd[2] - 1;  // cells per axis
@@ -133,7 +129,6 @@ __global__ void __launch_bounds__(kThreads, k1_blocks_per_sm<STITCH, PREC, SKIP,
       const int z = (bz << bl) + (li >> (2 * bl));
       if (x >= g.pd[0] || y >= g.pd[1] || z >= g.pd[2]) continue;
       id = (z * g.pd[1] + y) * g.pd[0] + x;
-      if (g.shell_only && !vertex_on_shell(g.pd, x, y, z)) continue;
       if (vmask && !vertex_in_marked_cell(vmask, g.pd, x, y, z)) continue;
       V[0] = vtx_coord(g, 0, x);
       V[1] = vtx_coord(g, 1, y);
@@ -141,10 +136,9 @@ __global__ void __launch_bounds__(kThreads, k1_blocks_per_sm<STITCH, PREC, SKIP,
     } else {
       id = (tile << 5) + lane;
       if (id >= nvert) continue;
-      if (vmask || g.shell_only) {
-        const int x = id % g.pd[0], yz = id / g.pd[0], y = yz % g.pd[1], z = yz / g.pd[1];
-        if (g.shell_only && !vertex_on_shell(g.pd, x, y, z)) continue;
-        if (vmask && !vertex_in_marked_cell(vmask, g.pd, x, y, z)) continue;
+      if (vmask) {
+        const int x = id % g.pd[0], yz = id / g.pd[0];
+        if (!vertex_in_marked_cell(vmask, g.pd, x, yz % g.pd[1], yz / g.pd[1])) continue;
       }
       map_vertex(g, id, V);
     }

@@ -163,6 +163,9 @@ struct beams_renderer {
   // idle; each brick has its own work counters (d_brick_cnt[b]).
   static constexpr int kBrickLanes = 4;
   cudaStream_t brick_lane[kBrickLanes] = {nullptr, nullptr, nullptr, nullptr};
+  unsigned char* d_shell_mask = nullptr;  // Phase 1's outer-cell-layer mask
+  size_t shell_cap = 0;
+  int shell_pd[3] = {0, 0, 0};
   cudaEvent_t brick_fork = nullptr;
   cudaEvent_t brick_join[kBrickLanes] = {nullptr, nullptr, nullptr, nullptr};
   beams::Counters* d_brick_cnt = nullptr;  // kMaxBricks entries
@@ -193,6 +196,7 @@ struct beams_renderer {
     if (d_refs) cudaFree(d_refs);
     if (d_brick_imgs) cudaFree(d_brick_imgs);
     if (d_brick_cnt) cudaFree(d_brick_cnt);
+    if (d_shell_mask) cudaFree(d_shell_mask);
     for (auto& s : brick_lane)
       if (s) cudaStreamDestroy(s);
     for (auto& e : brick_join)

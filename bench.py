@@ -461,6 +461,29 @@ def run_ours(args):
                    "extrapolated_from_sample": {"ms_per_frame": c["frame_s"] * 1e3, "sample": c["sample"],
                                                 "error": c["frame_s"] / f["frame_s"] - 1.0}}
 
+    # the exact form with the lazy map (beams_set_lazy_shadow_map): the same
+    # frame with only the map vertices the view rays read built; the image must
+    # equal the full map's bit for bit
+    lazy = None
+    exact_img = None
+    if not args.no_lazy:
+        r.set_reuse_shadow_map(False)
+        r.render(cam, out=out, timings=False)
+        exact_img = out.cpu().numpy()
+        r.set_lazy_shadow_map(True)
+        _, tl = r.render(cam, out=out, timings=True)
+        same = bool(np.array_equal(out.cpu().numpy(), exact_img))
+        lms, lclk = time_frames(lambda: r.render(cam, out=out, timings=False), args.steps, args.warmup, stream,
+                                world, local)
+        r.set_lazy_shadow_map(False)
+        lazy = {"ms_per_frame": lms / args.steps, "value": replica_value(world, args.steps, lit_frame, lms),
+                "unit": UNIT, "map_build_ms": tl["map_build_ms"], "view_march_ms": tl["view_march_ms"],
+                "map_vertices_built": tl["map_vertices"], "map_vertices": nvert,
+                "lit_samples_equal": tl["lit_samples"] == lit_frame, "image_equals_full_map": same,
+                "speedup_vs_full_map": (max_ms / args.steps) / (lms / args.steps), "clocks": lclk,
+                "note": "a view march without shading marks the map cells the rays read, the light march builds "
+                        "the marked cells' corners, then the view march; map_build_ms covers the marking"}
+
     # the metric's second half: the learned form on the same field, camera and
     # light, against this run's exact frame (the network as specified,
     # trained over 32 light directions, and a network trained for the rendered
@@ -468,8 +491,9 @@ def run_ours(args):
     learned = None
     if not args.no_learned:
         r.set_reuse_shadow_map(False)
-        r.render(cam, out=out, timings=False)
-        exact_img = out.cpu().numpy()
+        if exact_img is None:
+            r.render(cam, out=out, timings=False)
+            exact_img = out.cpu().numpy()
         field_host = None
         if rank == 0 and not args.no_quality:
             field_host = field if cpu is not None else fd.cpu().numpy()
@@ -483,6 +507,8 @@ def run_ours(args):
                 crop=args.crop, crop_stride=args.crop_stride, threads=os.cpu_count() or 1)
             rec["network"] = ("as specified: 2^24 samples over 32 light directions uniform on the sphere"
                               if lights == 32 else "2^24 samples for the rendered light only (fixed light, any camera)")
+            if lazy is not None:
+                rec["speedup_vs_exact_lazy_map"] = lazy["ms_per_frame"] / rec["ms_per_frame"]
             learned[name] = rec
         r.set_form(B.FORM_EXACT)
 
@@ -516,7 +542,7 @@ def run_ours(args):
                 "lit_samples_per_frame": lit_frame, "light_samples_per_frame": light_frame,
                 "gpu_launches": launches_per_frame * args.steps,
                 "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": sampler.summary(),
-                "learned": learned, "forms": forms}
+                "exact_lazy_map": lazy, "learned": learned, "forms": forms}
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:
@@ -1019,6 +1045,7 @@ def run_bricks(args, nested=False):
 # --profile-case: fixed small cases for profiling one kernel at a time (ncu -k):
 #   light_march      K1, 512^3 noise, M = 256
 #   view_march       K2, 512^3 noise, 1024^2, map cached
+#   lazy_frame       exact frame with the lazy map: cell marking, masked K1, K2
 #   mlp_view         learned-form view march, 1024^2
 #   mlp_frame        learned form frame: scene-light network, 1% probes
 #   mlp_frame32      learned form frame: the 32-light network, 1% probes (probe pixels first)
@@ -1032,7 +1059,7 @@ def run_bricks(args, nested=False):
 # device memory stays within a few GB. The tuning is fixed (8^3 vertex bricks,
 # skipping as stated per case) so that the launch sequence is the same every run.
 # ---------------------------------------------------------------------------
-PROFILE_CASES = ["light_march", "view_march", "mlp_view", "mlp_frame", "mlp_frame32", "mlp_tc", "mlp_train", "batch",
+PROFILE_CASES = ["light_march", "view_march", "lazy_frame", "mlp_view", "mlp_frame", "mlp_frame32", "mlp_tc", "mlp_train", "batch",
                  "precision_light", "precision_view", "bricks"]
 
 
@@ -1044,7 +1071,7 @@ def run_profile_case(a):
     from pilot_b200 import scenes
 
     torch.cuda.set_device(0)
-    if a.profile_case in ("light_march", "view_march", "mlp_view", "mlp_frame", "mlp_frame32"):
+    if a.profile_case in ("light_march", "view_march", "lazy_frame", "mlp_view", "mlp_frame", "mlp_frame32"):
         s = scenes.config1()
         fd = s.field_device()
         r = B.Renderer(0)
@@ -1059,6 +1086,10 @@ def run_profile_case(a):
         elif a.profile_case == "view_march":
             r.build_shadow_map(timings=False)
             r.set_reuse_shadow_map(True)
+            for _ in range(a.reps):
+                r.render(cam, out=out, timings=False)
+        elif a.profile_case == "lazy_frame":
+            r.set_lazy_shadow_map(True)
             for _ in range(a.reps):
                 r.render(cam, out=out, timings=False)
         elif a.profile_case == "mlp_frame":
@@ -1182,6 +1213,7 @@ def main():
     ap.add_argument("--crop-stride", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="default line: skip the learned-form records")
+    ap.add_argument("--no-lazy", action="store_true", help="default line: skip the lazy-map record")
     ap.add_argument("--no-forms", action="store_true",
                     help="default line: skip the precision, batch and bricks records")
     ap.add_argument("--learned-knot", type=int, default=32, help="default line: knot of the learned-form records")

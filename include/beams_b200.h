@@ -94,7 +94,8 @@ typedef struct beams_timings {
   unsigned long long lit_samples;    /* view samples composited */
   unsigned long long rays_hit;       /* view rays that entered the volume */
   unsigned long long mlp_samples;    /* view samples shaded by the MLP */
-  int map_vertices;                  /* (M+1)^3 of the map built this frame, 0 if reused */
+  int map_vertices;                  /* map vertices built this frame ((M+1)^3 per light, 0 if reused;
+                                        fewer under the lazy map and the learned form's fallback) */
   int fallback_tiles;                /* MLP form: tiles that used the exact map */
   int kernel_launches;               /* kernels this call launched */
   unsigned long long mlp_rows;       /* learned form: network rows computed, idle lanes included */
@@ -156,6 +157,17 @@ beams_status beams_set_slab_fp64(beams_renderer* r, int enable);
 /* Keep the last map when its inputs (volume, colour map, light, map size) did not
  * change. Off by default: the reference rebuilds the map every frame. */
 beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable);
+/* Extension (no reference counterpart; the reference builds every vertex,
+ * TransmittanceMap.h:565-621): the exact form builds only the map vertices that
+ * the frame's view rays read. A view march without shading (the samples and
+ * their order do not depend on the map: early termination reads only the
+ * colour map's alpha) marks the map cells the shading will interpolate, then
+ * the light march builds the corners of the marked cells. The image is the
+ * full map's bit for bit; the map is partial, so beams_get_shadow_map returns
+ * BEAMS_ERR_STATE after such a frame and the map is never reused.
+ * beams_timings.map_vertices reports the vertices built. Off by default; the
+ * precision and learned forms and multi-block scenes ignore it. */
+beams_status beams_set_lazy_shadow_map(beams_renderer* r, int enable);
 /* ---- legacy VTK files ---------------------------------------------------------
  * Replaces the reference's dataset read (pilot/io/DataSetUtils.cxx:13-42, VTK-m's
  * legacy reader) for structured volumes: DATASET STRUCTURED_POINTS or

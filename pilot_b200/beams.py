@@ -183,6 +183,7 @@ def lib():
         "beams_set_light_steps": ([P, C.c_float], C.c_int),
         "beams_set_slab_fp64": ([P, C.c_int], C.c_int),
         "beams_set_reuse_shadow_map": ([P, C.c_int], C.c_int),
+        "beams_set_lazy_shadow_map": ([P, C.c_int], C.c_int),
         "beams_set_background": ([P, C.c_int, P], C.c_int),
         "beams_set_form": ([P, C.c_int, P], C.c_int),
         "beams_render": ([P, C.POINTER(Camera), P, C.c_int, C.POINTER(Timings)], C.c_int),
@@ -543,6 +544,10 @@ class Renderer:
 
     def set_reuse_shadow_map(self, on: bool):
         self._check(self._L.beams_set_reuse_shadow_map(self._h, int(bool(on))))
+
+    def set_lazy_shadow_map(self, on: bool):
+        """Build only the map vertices the frame's view rays read (exact form)."""
+        self._check(self._L.beams_set_lazy_shadow_map(self._h, int(bool(on))))
 
     def set_background(self, on: bool, rgba=(1, 1, 1, 1)):
         c = (C.c_float * 4)(*rgba)

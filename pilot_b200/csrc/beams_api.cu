@@ -429,6 +429,49 @@ beams_status build_map(beams_renderer* r, const ExactGeo& g, int& launches, bool
   return BEAMS_OK;
 }
 
+// The exact form's lazy map (beams_set_lazy_shadow_map). The view rays' samples
+// and their order do not depend on the map (early termination reads only the
+// colour map's alpha), so a view march without shading marks the map cells
+// the frame reads, and the light march builds only the vertices of marked
+// cells: the image equals the full map's bit for bit. The map itself is
+// partial, so it is neither kept for reuse nor readable.
+static beams_status build_map_lazy(beams_renderer* r, const ExactGeo& g, int& launches) {
+  const size_t nvert = (size_t)g.pd[0] * g.pd[1] * g.pd[2];
+  const int nl = g.n_lights > 1 ? g.n_lights : 1;
+  beams_status s = ensure_buffer(r, (void**)&r->d_map, &r->map_cap, nl * nvert * sizeof(float), "allocating map");
+  if (s != BEAMS_OK) return s;
+  r->map_valid = false;
+  r->map_is_half = false;
+  const size_t ncell = (size_t)(g.pd[0] - 1) * (g.pd[1] - 1) * (g.pd[2] - 1);
+  s = ensure_buffer(r, (void**)&r->d_cell_mask, &r->cell_mask_cap, ncell, "allocating the map cell mask");
+  if (s != BEAMS_OK) return s;
+  const unsigned char* occ = nullptr;
+  if (r->empty_skip && !g.rect) {
+    s = prepare_occupancy(r, g, launches);
+    if (s != BEAMS_OK) return s;
+    occ = r->d_occ;
+  }
+  s = ensure_buffer(r, (void**)&r->d_vlist, &r->vlist_cap, (nvert + 1) * sizeof(unsigned),
+                    "allocating the map vertex list");
+  if (s != BEAMS_OK) return s;
+  const float4* quads = (const float4*)r->d_quads;
+  cudaError_t e = cudaMemsetAsync(r->d_cell_mask, 0, ncell, r->stream);
+  if (e == cudaSuccess)
+    e = launch_mark_view_cells(g, quads, r->d_tab, r->d_tf, r->d_cell_mask, r->d_cnt, nullptr, nullptr, r->stream);
+  if (e == cudaSuccess) e = launch_list_marked_vertices(g, r->d_cell_mask, nullptr, r->d_vlist, r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "map cell marking launch");
+  launches += 2;
+  for (int l = 0; l < nl; ++l) {
+    ExactGeo gl = g;
+    if (l > 0) geo_set_light(gl, r->lights[l]);
+    e = launch_light_march_f32(gl, quads, r->d_tab, r->d_tf, r->d_map + (size_t)l * nvert, r->d_cnt, r->stream,
+                               nullptr, 0, -1, nullptr, occ, r->d_vlist);
+    if (e != cudaSuccess) return cuda_fail(r, e, "light_march launch");
+    ++launches;
+  }
+  return BEAMS_OK;
+}
+
 static beams_status check_sizes(beams_renderer* r, const beams_volume& v) {
   const double nq = (double)(v.dims[0] - 1) * (v.dims[1] - 1) * v.dims[2];
   if (nq >= 4294967296.0) return fail(r, BEAMS_ERR_UNSUPPORTED, "volume too large for 32-bit cell indexing");
@@ -617,12 +660,24 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
       if (s != BEAMS_OK) return s;
       shell = r->d_shell_mask;
     }
+    // the shell's vertices listed once (the bricks' maps share their size)
+    const unsigned* shell_list = nullptr;
+    if (shell) {
+      const size_t nv = (size_t)G[0].pd[0] * G[0].pd[1] * G[0].pd[2];
+      s = ensure_buffer(r, (void**)&r->d_vlist, &r->vlist_cap, (nv + 1) * sizeof(unsigned),
+                        "allocating the map vertex list");
+      if (s != BEAMS_OK) return s;
+      e = launch_list_marked_vertices(G[0], shell, nullptr, r->d_vlist, r->stream);
+      if (e != cudaSuccess) return cuda_fail(r, e, "listing the shell vertices");
+      ++launches;
+      shell_list = r->d_vlist;
+    }
     s = brick_lanes_fork(r);
     if (s != BEAMS_OK) return s;
     for (int b = 0; b < nb; ++b) {
       Brick& B = r->bricks[b];
       e = launch_light_march_f32(G[b], B.d_quads, B.d_tab, r->d_tf, B.d_map_local, r->d_brick_cnt + b, lane(b),
-                                 nullptr, 0, -1, nullptr, nullptr, shell);
+                                 nullptr, 0, -1, nullptr, nullptr, shell_list);
       if (e != cudaSuccess) return lane_fail(e, "brick light march");
       ++launches;
     }
@@ -1018,6 +1073,12 @@ beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable) {
   return BEAMS_OK;
 }
 
+beams_status beams_set_lazy_shadow_map(beams_renderer* r, int enable) {
+  if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  r->lazy_map = enable != 0;
+  return BEAMS_OK;
+}
+
 beams_status beams_set_background(beams_renderer* r, int enable, const float rgba[4]) {
   if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
   r->bg = enable != 0;
@@ -1266,7 +1327,13 @@ static beams_status render_frame(beams_renderer* r, const beams_camera* cam, flo
   if (s != BEAMS_OK) return s;
   const bool use_mlp = r->form == BEAMS_FORM_MLP;
   const bool need_map = r->use_map && r->vol.assoc == BEAMS_ASSOC_POINTS && !use_mlp;
-  if (need_map) {
+  const bool lazy = need_map && r->lazy_map && r->form == BEAMS_FORM_EXACT;
+  if (lazy) {
+    // the marking pass clips rays to the canvas depth like the view march
+    s = prepare_ray_limits(r, g, launches);
+    if (s == BEAMS_OK) s = build_map_lazy(r, g, launches);
+    if (s != BEAMS_OK) return s;
+  } else if (need_map) {
     s = build_map(r, g, launches, built);
     if (s != BEAMS_OK) return s;
   }
@@ -1279,8 +1346,10 @@ static beams_status render_frame(beams_renderer* r, const beams_camera* cam, flo
     if (s != BEAMS_OK) return s;
     dst = r->d_rgba;
   }
-  s = prepare_ray_limits(r, g, launches);
-  if (s != BEAMS_OK) return s;
+  if (!lazy) {
+    s = prepare_ray_limits(r, g, launches);
+    if (s != BEAMS_OK) return s;
+  }
   if (use_mlp) {
     s = mlp_render_view(r, g, dst, launches);
     if (s != BEAMS_OK) return s;
@@ -1329,8 +1398,8 @@ static beams_status render_frame(beams_renderer* r, const beams_camera* cam, flo
     t->mlp_samples = c.mlp_samples;
     t->mlp_rows = c.mlp_rows;
     t->fallback_tiles = (int)c.fallback_tiles;
-    // the learned form's fallback builds only the vertices its failing tiles read
-    t->map_vertices = use_mlp ? (int)c.map_vertices : (built ? (int)((size_t)g.pd[0] * g.pd[1] * g.pd[2]) : 0);
+    // the learned form's fallback and the lazy map build only the vertices their view rays read
+    t->map_vertices = (use_mlp || lazy) ? (int)c.map_vertices : (built ? (int)r->map_count : 0);
     t->kernel_launches = launches;
   } else if (out_on_device == BEAMS_OUT_HOST) {
     // The caller reads rgba_out on return.

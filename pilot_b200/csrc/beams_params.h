@@ -116,6 +116,8 @@ struct Counters {
   unsigned int tiles_view;
   unsigned long long mlp_rows;  // network rows computed (idle lanes included)
   unsigned long long map_vertices;  // vertices a masked (lazy) light march built
+  unsigned int tiles_mark;  // the map-cell marking pass's tile counter (zeroed by its launcher)
+  unsigned int reserved;
 };
 
 // Derives ExactGeo's loop constants from n[] and tf_n.

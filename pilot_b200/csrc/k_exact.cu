@@ -52,23 +52,78 @@ constexpr int k1_blocks_per_sm() {
   return (PREC || SKIP || RECT) ? 4 : 6;
 }
 
-// A masked map build (the learned form's lazy map, the multi-brick Phase 1):
-// vertex (x, y, z) is built when one of the (up to 8) map cells it is a corner
-// of is marked (one byte per cell, x fastest).
+// A masked map build (the exact form's lazy map, the learned form's fallback,
+// the multi-brick Phase 1): vertex (x, y, z) is built when one of the (up to 8)
+// map cells it is a corner of is marked (one byte per cell, x fastest). The
+// eight loads (clamped at the faces, where a vertex has fewer cells) are
+// issued together.
 __device__ __forceinline__ bool vertex_in_marked_cell(const unsigned char* __restrict__ cm, const int pd[3], int x,
                                                       int y, int z) {
-  const int mx = pd[0] - 1, my = pd[1] - 1, mz = pd[2] - 1;  // cells per axis
-  const int x0 = max(x - 1, 0), x1 = min(x, mx - 1);
-  const int y0 = max(y - 1, 0), y1 = min(y, my - 1);
-  const int z0 = max(z - 1, 0), z1 = min(z, mz - 1);
-  for (int k = z0; k <= z1; ++k)
-    for (int j = y0; j <= y1; ++j)
-      for (int i = x0; i <= x1; ++i)
-        if (__ldg(cm + ((size_t)k * my + j) * mx + i)) return true;
-  return false;
+  const unsigned mx = pd[0] - 1, mxy = mx * (unsigned)(pd[1] - 1);  // cells per row, per slice
+  const unsigned x0 = max(x - 1, 0), x1 = min(x, pd[0] - 2);
+  const unsigned y0 = max(y - 1, 0), y1 = min(y, pd[1] - 2);
+  const unsigned z0 = max(z - 1, 0), z1 = min(z, pd[2] - 2);
+  const unsigned r00 = z0 * mxy + y0 * mx, r01 = z0 * mxy + y1 * mx;
+  const unsigned r10 = z1 * mxy + y0 * mx, r11 = z1 * mxy + y1 * mx;
+  const unsigned m = __ldg(cm + r00 + x0) | __ldg(cm + r00 + x1) | __ldg(cm + r01 + x0) | __ldg(cm + r01 + x1) |
+                     __ldg(cm + r10 + x0) | __ldg(cm + r10 + x1) | __ldg(cm + r11 + x0) | __ldg(cm + r11 + x1);
+  return m != 0u;
 }
 
-template <typename QuadT, bool STITCH, bool PREC, bool SKIP, bool RECT = false>
+// The work list of a masked map build: the vertices of marked cells
+// (vertex_in_marked_cell) in the light march's vertex order, list[1 + i] their
+// ids, list[0] their count (zeroed before the launch). A masked build over this
+// list takes one tile-counter atomic per 32 listed vertices, where testing every
+// vertex took one per 32 vertices of the whole map (the 257^3-vertex map of a
+// 512^3 field seen through a 30-degree camera: 31,073 vertices built, 0.41 ms
+// for the per-vertex test, most of it atomics on the one counter). One warp per
+// 32-vertex tile of the order at a static stride, one append per warp that
+// finds a vertex (lane order kept inside the warp).
+__global__ void __launch_bounds__(256) k_list_marked_vertices(const ExactGeo g, const unsigned char* __restrict__ cm,
+                                                              const unsigned* __restrict__ gate,
+                                                              unsigned* __restrict__ list) {
+  if (gate && *gate == 0u) return;
+  __shared__ int s_bo[8];
+  const int bl = g.light_brick_log2;
+  if (threadIdx.x == 0 && bl) brick_order_setup(g, bl, s_bo);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int nvert = g.pd[0] * g.pd[1] * g.pd[2];
+  const int ntiles = bl ? (s_bo[0] * s_bo[1] * s_bo[2]) << (3 * bl - 5) : (nvert + 31) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < ntiles; tile += nwarps) {
+    int x, y, z;
+    bool in;
+    if (bl) {  // the brick order of k_light_march
+      const int bi = tile >> (3 * bl - 5);
+      const int li = ((tile & ((1 << (3 * bl - 5)) - 1)) << 5) + lane;
+      const int m = (1 << bl) - 1;
+      int bx, by, bz;
+      pencil_brick(bi, s_bo, bx, by, bz);
+      x = (bx << bl) + (li & m);
+      y = (by << bl) + ((li >> bl) & m);
+      z = (bz << bl) + (li >> (2 * bl));
+      in = x < g.pd[0] && y < g.pd[1] && z < g.pd[2];
+    } else {
+      const int id = (tile << 5) + lane;
+      in = id < nvert;
+      x = id % g.pd[0];
+      y = (id / g.pd[0]) % g.pd[1];
+      z = id / (g.pd[0] * g.pd[1]);
+    }
+    const bool take = in && vertex_in_marked_cell(cm, g.pd, x, y, z);
+    const unsigned b = __ballot_sync(0xffffffffu, take);
+    if (b == 0u) continue;
+    unsigned base = 0;
+    if (lane == 0) base = atomicAdd(list, (unsigned)__popc(b));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (take) list[1 + base + __popc(b & ((1u << lane) - 1u))] = (unsigned)((z * g.pd[1] + y) * g.pd[0] + x);
+  }
+}
+
+// LIST: the vertices come from a work list (k_list_marked_vertices) instead of
+// the whole map's vertex order.
+template <typename QuadT, bool STITCH, bool PREC, bool SKIP, bool RECT = false, bool LIST = false>
 __global__ void __launch_bounds__(kThreads, k1_blocks_per_sm<STITCH, PREC, SKIP, RECT>()) k_light_march(const ExactGeo g, const QuadT* __restrict__ quads,
                                                           const float4* __restrict__ tab,
                                                           const float4* __restrict__ tf,
@@ -78,10 +133,9 @@ __global__ void __launch_bounds__(kThreads, k1_blocks_per_sm<STITCH, PREC, SKIP,
                                                           const BrickRef* __restrict__ refs, int nrefs,
                                                           int self, const unsigned* __restrict__ gate,
                                                           const unsigned char* __restrict__ occ,
-                                                          const unsigned char* __restrict__ vmask) {
+                                                          const unsigned* __restrict__ vlist) {
   // gate: the learned form's fallback builds the map only when a tile failed its
-  // probes, and (vmask: marked map cells) only the vertices the failing tiles'
-  // view rays read
+  // probes, and (LIST) only the vertices the failing tiles' view rays read
   if (gate && *gate == 0u) return;
   extern __shared__ float4 s_dyn[];
   const int nfield = g.max_off[0];             // field-axis table entries only
@@ -109,6 +163,7 @@ __global__ void __launch_bounds__(kThreads, k1_blocks_per_sm<STITCH, PREC, SKIP,
   if (threadIdx.x == 0) brick_order_setup(g, g.light_brick_log2, s_bo);
   __syncthreads();
   const int ntiles = [&] {
+    if (LIST) return (int)((vlist[0] + 31u) >> 5);
     const int b0 = g.light_brick_log2;
     return b0 ? (s_bo[0] * s_bo[1] * s_bo[2]) << (3 * b0 - 5) : (nvert + 31) >> 5;
   }();
@@ -118,7 +173,12 @@ __global__ void __launch_bounds__(kThreads, k1_blocks_per_sm<STITCH, PREC, SKIP,
     int id;
     float V[3], L[3];
     const int bl = g.light_brick_log2;
-    if (bl) {
+    if (LIST) {
+      const unsigned i = ((unsigned)tile << 5) + lane;
+      if (i >= vlist[0]) continue;
+      id = (int)vlist[1 + i];
+      map_vertex(g, id, V);
+    } else if (bl) {
       // tile -> brick (light-aligned order), lane -> vertex of the brick (x fastest inside the brick)
       const int bi = tile >> (3 * bl - 5);
       const int li = ((tile & ((1 << (3 * bl - 5)) - 1)) << 5) + lane;
@@ -129,17 +189,12 @@ __global__ void __launch_bounds__(kThreads, k1_blocks_per_sm<STITCH, PREC, SKIP,
       const int z = (bz << bl) + (li >> (2 * bl));
       if (x >= g.pd[0] || y >= g.pd[1] || z >= g.pd[2]) continue;
       id = (z * g.pd[1] + y) * g.pd[0] + x;
-      if (vmask && !vertex_in_marked_cell(vmask, g.pd, x, y, z)) continue;
       V[0] = vtx_coord(g, 0, x);
       V[1] = vtx_coord(g, 1, y);
       V[2] = vtx_coord(g, 2, z);
     } else {
       id = (tile << 5) + lane;
       if (id >= nvert) continue;
-      if (vmask) {
-        const int x = id % g.pd[0], yz = id / g.pd[0];
-        if (!vertex_in_marked_cell(vmask, g.pd, x, yz % g.pd[1], yz / g.pd[1])) continue;
-      }
       map_vertex(g, id, V);
     }
     ++built;
@@ -153,7 +208,7 @@ __global__ void __launch_bounds__(kThreads, k1_blocks_per_sm<STITCH, PREC, SKIP,
     acc.store(map, id);
   }
   warp_add(&cnt->light_samples, ns);
-  if (vmask) warp_add(&cnt->map_vertices, built);
+  if (LIST) warp_add(&cnt->map_vertices, built);
 }
 
 // ---------------------------------------------------------------------------
@@ -204,6 +259,53 @@ __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const
   }
   warp_add(&cnt->lit_samples, lit);
   warp_add(&cnt->rays_hit, hit);
+}
+
+// The masked map builds' marking pass: the view march without shading (the
+// samples and their order do not depend on the map, since early termination
+// reads only the colour map's alpha), CellMarker observing every lit sample.
+// K2's warp tiles in K2's order over the window, or (LIST) over the listed
+// kFallbackTile^2 tiles while *fcount > 0; tile counter cnt->tiles_mark. The
+// march reads no map, so only the field axes' cell tables are staged.
+template <bool RECT, bool LIST>
+__global__ void __launch_bounds__(kThreads) k_mark_view_cells(const ExactGeo g, const float4* __restrict__ quads,
+                                                              const float4* __restrict__ tab,
+                                                              const float4* __restrict__ tf,
+                                                              unsigned char* __restrict__ mask,
+                                                              Counters* __restrict__ cnt,
+                                                              const unsigned* __restrict__ flist,
+                                                              const unsigned* __restrict__ fcount) {
+  if (LIST && *fcount == 0u) return;
+  extern __shared__ float4 s_dyn[];
+  const int nfield = g.max_off[0];
+  float4* s_tab = s_dyn;
+  float4* s_tf = s_dyn + nfield;
+  load_tables(s_tab, tab, nfield);
+  for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) s_tf[i] = tf[i];
+  __syncthreads();
+  const int tiles_x = (g.win[2] + 7) >> 3;
+  const int ntiles = LIST ? (int)(*fcount) * 32 : tiles_x * ((g.win[3] + 3) >> 2);
+  const int ftx = (g.width + kFallbackTile - 1) / kFallbackTile;
+  for (int tile = next_warp_tile(&cnt->tiles_mark); tile < ntiles; tile = next_warp_tile(&cnt->tiles_mark)) {
+    int x, y;
+    if (LIST) {
+      const int f = (int)flist[tile >> 5], sub = tile & 31, lane = threadIdx.x & 31;
+      x = (f % ftx) * kFallbackTile + ((sub & 3) << 3) + (lane & 7);
+      y = (f / ftx) * kFallbackTile + ((sub >> 2) << 2) + (lane >> 3);
+    } else {
+      tile_pixel(tiles_x, tile, x, y);
+      x = (x < g.win[2]) ? x + g.win[0] : g.width;
+      y = (y < g.win[3]) ? y + g.win[1] : g.height;
+    }
+    if (x < g.width && y < g.height) {
+      CellMarker m{{g.morig[0], g.morig[1], g.morig[2]}, {g.minv[0], g.minv[1], g.minv[2]},
+                   {g.pd[0], g.pd[1], g.pd[2]}, mask, 0xffffffffu};
+      float4 color;
+      unsigned lit = 0, hit = 0;
+      view_march_pixel<float4, false, float, CellMarker, false, false, RECT>(g, quads, s_tab, s_tf, nullptr, x, y,
+                                                                             color, lit, hit, &m);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -420,7 +522,7 @@ template <typename QuadT, bool STITCH, bool PREC>
 static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4* tab, const float4* tf,
                              const float* tau, void* map, Counters* cnt, cudaStream_t st, const BrickRef* refs,
                              int nrefs, int self, const unsigned* gate = nullptr,
-                             const unsigned char* occ = nullptr, const unsigned char* vmask = nullptr) {
+                             const unsigned char* occ = nullptr, const unsigned* vlist = nullptr) {
   const int nvert = g.pd[0] * g.pd[1] * g.pd[2];
   const size_t smem = (size_t)g.max_off[0] * sizeof(float4) + 2 * (size_t)g.tf_n * sizeof(float);
   const int ntiles = (nvert + kThreads - 1) / kThreads;
@@ -434,39 +536,97 @@ static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4*
     // empty-space skipping (the precision form keeps the seeded walk, correct for
     // any increasing coordinates)
     if constexpr (!STITCH && !PREC && std::is_same<QuadT, float4>::value) {
+      if (vlist) {
+        e = persistent_grid(k_light_march<float4, false, false, false, true, true>, smem, ntiles, grid);
+        if (e != cudaSuccess) return e;
+        k_light_march<float4, false, false, false, true, true><<<grid, kThreads, smem, st>>>(
+            g, (const float4*)quads, tab, tf, tau, map, nvert, cnt, refs, nrefs, self, gate, nullptr, vlist);
+        return cudaGetLastError();
+      }
       e = persistent_grid(k_light_march<float4, false, false, false, true>, smem, ntiles, grid);
       if (e != cudaSuccess) return e;
       k_light_march<float4, false, false, false, true><<<grid, kThreads, smem, st>>>(
-          g, (const float4*)quads, tab, tf, tau, map, nvert, cnt, refs, nrefs, self, gate, nullptr, vmask);
+          g, (const float4*)quads, tab, tf, tau, map, nvert, cnt, refs, nrefs, self, gate, nullptr, nullptr);
       return cudaGetLastError();
     } else {
       return cudaErrorInvalidValue;
     }
+  }
+  if constexpr (!STITCH && !PREC) {
+    if (vlist) {
+      if (occ) {
+        e = persistent_grid(k_light_march<QuadT, false, false, true, false, true>, smem, ntiles, grid);
+        if (e != cudaSuccess) return e;
+        k_light_march<QuadT, false, false, true, false, true><<<grid, kThreads, smem, st>>>(
+            g, (const QuadT*)quads, tab, tf, tau, map, nvert, cnt, refs, nrefs, self, gate, occ, vlist);
+      } else {
+        e = persistent_grid(k_light_march<QuadT, false, false, false, false, true>, smem, ntiles, grid);
+        if (e != cudaSuccess) return e;
+        k_light_march<QuadT, false, false, false, false, true><<<grid, kThreads, smem, st>>>(
+            g, (const QuadT*)quads, tab, tf, tau, map, nvert, cnt, refs, nrefs, self, gate, nullptr, vlist);
+      }
+      return cudaGetLastError();
+    }
+  } else {
+    if (vlist) return cudaErrorInvalidValue;
   }
   if (occ) {
     e = persistent_grid(k_light_march<QuadT, STITCH, PREC, true>, smem, ntiles, grid);
     if (e != cudaSuccess) return e;
     k_light_march<QuadT, STITCH, PREC, true><<<grid, kThreads, smem, st>>>(g, (const QuadT*)quads, tab, tf, tau, map,
                                                                            nvert, cnt, refs, nrefs, self, gate, occ,
-                                                                           vmask);
+                                                                           nullptr);
   } else {
     e = persistent_grid(k_light_march<QuadT, STITCH, PREC, false>, smem, ntiles, grid);
     if (e != cudaSuccess) return e;
     k_light_march<QuadT, STITCH, PREC, false><<<grid, kThreads, smem, st>>>(g, (const QuadT*)quads, tab, tf, tau,
                                                                             map, nvert, cnt, refs, nrefs, self, gate,
-                                                                            nullptr, vmask);
+                                                                            nullptr, nullptr);
   }
+  return cudaGetLastError();
+}
+
+template <bool RECT, bool LIST>
+static cudaError_t launch_mark(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
+                               unsigned char* cell_mask, Counters* cnt, const unsigned* flist,
+                               const unsigned* fcount, cudaStream_t st) {
+  const size_t smem = ((size_t)g.max_off[0] + (size_t)g.tf_n) * sizeof(float4);
+  const int ntiles = ((g.win[2] + 7) >> 3) * ((g.win[3] + 3) >> 2);
+  int grid = 0;
+  cudaError_t e = persistent_grid(k_mark_view_cells<RECT, LIST>, smem, ntiles, grid);
+  if (e != cudaSuccess) return e;
+  k_mark_view_cells<RECT, LIST><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, cell_mask, cnt, flist, fcount);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mark_view_cells(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
+                                   unsigned char* cell_mask, Counters* cnt, const unsigned* flist,
+                                   const unsigned* fcount, cudaStream_t st) {
+  if (flist && !fcount) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(&cnt->tiles_mark, 0, sizeof(unsigned), st);
+  if (e != cudaSuccess) return e;
+  if (g.rect)
+    return flist ? launch_mark<true, true>(g, quads, tab, tf, cell_mask, cnt, flist, fcount, st)
+                 : launch_mark<true, false>(g, quads, tab, tf, cell_mask, cnt, nullptr, nullptr, st);
+  return flist ? launch_mark<false, true>(g, quads, tab, tf, cell_mask, cnt, flist, fcount, st)
+               : launch_mark<false, false>(g, quads, tab, tf, cell_mask, cnt, nullptr, nullptr, st);
+}
+
+cudaError_t launch_list_marked_vertices(const ExactGeo& g, const unsigned char* cell_mask, const unsigned* gate,
+                                        unsigned* list, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(list, 0, sizeof(unsigned), st);
+  if (e != cudaSuccess) return e;
+  k_list_marked_vertices<<<num_sms() * 8, 256, 0, st>>>(g, cell_mask, gate, list);
   return cudaGetLastError();
 }
 
 cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    float* map, Counters* cnt, cudaStream_t st, const BrickRef* refs, int nrefs,
-                                   int self, const unsigned* gate, const unsigned char* occ,
-                                   const unsigned char* vmask) {
+                                   int self, const unsigned* gate, const unsigned char* occ, const unsigned* vlist) {
   if (refs)
     return launch_k1<float4, true, false>(g, quads, tab, tf, nullptr, map, cnt, st, refs, nrefs, self, gate, occ,
-                                          vmask);
-  return launch_k1<float4, false, false>(g, quads, tab, tf, nullptr, map, cnt, st, nullptr, 0, -1, gate, occ, vmask);
+                                          vlist);
+  return launch_k1<float4, false, false>(g, quads, tab, tf, nullptr, map, cnt, st, nullptr, 0, -1, gate, occ, vlist);
 }
 
 cudaError_t launch_light_march_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,

@@ -13,8 +13,9 @@
 //      exceeds the tolerance (or that holds no probe, or a probe past the cap)
 //      joins the fallback list.
 // The host then builds the exact map lazily, only where the listed tiles need
-// it (k_mark_fallback marks the map cells their view rays read, and K1 marches
-// only the vertices of marked cells; both gated on the list being non-empty),
+// it (k_mark_view_cells marks the map cells their view rays read,
+// k_list_marked_vertices lists the corners of marked cells and K1 marches only
+// those; all gated on the list being non-empty),
 // and K2 re-renders the listed tiles, so a failing tile is exactly the exact
 // form's pixels.
 // Compiled with -fmad=false like every kernel file.
@@ -172,31 +173,6 @@ __global__ void __launch_bounds__(kThreadsP, 3) k_probe_check(const ExactGeo g, 
   }
 }
 
-// Marks, for every lit sample of a view ray, the map cell that the shading
-// looks up (the cell of map_interp_t: truncate min(max((p - origin) / spacing,
-// 0), pd - 2) per axis), one byte per cell, skipping repeats of the previous
-// sample's cell. K1 then builds a vertex when a cell around it is marked
-// (the same vertex set as marking the 8 corners, with one store per cell).
-struct CellMarker {
-  float morig[3], minv[3];
-  int pd[3];
-  unsigned char* mask;
-  unsigned last;
-  __device__ __forceinline__ void operator()(const float* p, const float4&, float) {
-    int c[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const float t = (p[d] - morig[d]) * minv[d];
-      c[d] = trunc_small(fminf(fmaxf(t, 0.f), (float)(pd[d] - 2)));
-    }
-    const unsigned mx = (unsigned)(pd[0] - 1), mxy = mx * (unsigned)(pd[1] - 1);
-    const unsigned id = (unsigned)c[2] * mxy + (unsigned)c[1] * mx + (unsigned)c[0];
-    if (id == last) return;
-    last = id;
-    mask[id] = 1;
-  }
-};
-
 // Also copies the list's length to host-mapped memory (when given) for the
 // host's choice of order in the next frame.
 __global__ void k_clear_mask_gated(const unsigned* __restrict__ fcount, uint4* __restrict__ mask, size_t n16,
@@ -206,40 +182,6 @@ __global__ void k_clear_mask_gated(const unsigned* __restrict__ fcount, uint4* _
   if (nf == 0u) return;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n16; i += (size_t)gridDim.x * blockDim.x)
     mask[i] = make_uint4(0u, 0u, 0u, 0u);
-}
-
-// The listed tiles' view rays (the K2 march without shading: the samples and
-// their order do not depend on the map) mark the map cells they read.
-__global__ void __launch_bounds__(kThreadsP) k_mark_fallback(const ExactGeo g, const float4* __restrict__ quads,
-                                                             const float4* __restrict__ tab,
-                                                             const float4* __restrict__ tf,
-                                                             const unsigned* __restrict__ flist,
-                                                             const unsigned* __restrict__ fcount,
-                                                             unsigned char* __restrict__ mask) {
-  const int nf = (int)*fcount;
-  if (nf == 0) return;
-  extern __shared__ float4 s_dyn[];
-  float4* s_tab = s_dyn;
-  float4* s_tf = s_dyn + g.ntab;
-  for (int i = threadIdx.x; i < g.ntab; i += blockDim.x) s_tab[i] = tab[i];
-  for (int i = threadIdx.x; i < g.tf_n; i += blockDim.x) s_tf[i] = tf[i];
-  __syncthreads();
-  const int ftx = (g.width + kFallbackTile - 1) / kFallbackTile;
-  const int lane = threadIdx.x & 31;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  // a kFallbackTile^2 tile is 32 warp tiles of 8 x 4 pixels (the LIST order of k_view_march)
-  for (int wt = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; wt < nf * 32; wt += nwarps) {
-    const int f = (int)flist[wt >> 5], sub = wt & 31;
-    const int x = (f % ftx) * kFallbackTile + ((sub & 3) << 3) + (lane & 7);
-    const int y = (f / ftx) * kFallbackTile + ((sub >> 2) << 2) + (lane >> 3);
-    if (x < g.width && y < g.height) {
-      CellMarker m{{g.morig[0], g.morig[1], g.morig[2]}, {g.minv[0], g.minv[1], g.minv[2]},
-                   {g.pd[0], g.pd[1], g.pd[2]}, mask, 0xffffffffu};
-      float4 color;
-      unsigned lit = 0, hit = 0;
-      view_march_pixel<float4, false, float, CellMarker>(g, quads, s_tab, s_tf, nullptr, x, y, color, lit, hit, &m);
-    }
-  }
 }
 
 int grid_for(size_t n, int threads, int cap_blocks) {
@@ -253,14 +195,10 @@ int grid_for(size_t n, int threads, int cap_blocks) {
 
 cudaError_t launch_mark_fallback_vertices(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                           const unsigned* flist, const unsigned* fcount, unsigned char* vmask,
-                                          size_t mask_bytes, unsigned* host_count, cudaStream_t st) {
+                                          size_t mask_bytes, unsigned* host_count, Counters* cnt, cudaStream_t st) {
   if (mask_bytes % 16 != 0) return cudaErrorInvalidValue;
   k_clear_mask_gated<<<148 * 4, 256, 0, st>>>(fcount, (uint4*)vmask, mask_bytes / 16, host_count);
-  const size_t smem = ((size_t)g.ntab + (size_t)g.tf_n) * sizeof(float4);
-  cudaError_t e = cudaFuncSetAttribute(k_mark_fallback, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  k_mark_fallback<<<148 * 4, kThreadsP, smem, st>>>(g, quads, tab, tf, flist, fcount, vmask);
-  return cudaGetLastError();
+  return launch_mark_view_cells(g, quads, tab, tf, vmask, cnt, flist, fcount, st);
 }
 
 ProbeLayout probe_layout(int width, int height, float fraction) {

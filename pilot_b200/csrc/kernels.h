@@ -20,7 +20,13 @@ cudaError_t launch_view_march_prec(const ExactGeo& g, int quad_dtype, const void
 cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    float* map, Counters* cnt, cudaStream_t st, const BrickRef* refs = nullptr,
                                    int nrefs = 0, int self = -1, const unsigned* gate = nullptr,
-                                   const unsigned char* occ = nullptr, const unsigned char* vmask = nullptr);
+                                   const unsigned char* occ = nullptr, const unsigned* vlist = nullptr);
+// The work list of a masked map build (vlist above): zeroes list[0], then lists
+// in list[1..] the vertices of the cells marked in cell_mask (one byte per map
+// cell, x fastest), list[0] their count. list holds (M+1)^3 + 1 entries.
+// gate (non-null): nothing is listed while *gate is 0.
+cudaError_t launch_list_marked_vertices(const ExactGeo& g, const unsigned char* cell_mask, const unsigned* gate,
+                                        unsigned* list, cudaStream_t st);
 // Empty-space occupancy of 8^3-cell macro-cells for the light march's skip.
 void occupancy_dims(const int n[3], int occ_n[3]);
 cudaError_t launch_build_occupancy(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tf,
@@ -32,7 +38,14 @@ cudaError_t launch_build_occupancy(const ExactGeo& g, int quad_dtype, const void
 // memory, or null) receives the list's length.
 cudaError_t launch_mark_fallback_vertices(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                           const unsigned* flist, const unsigned* fcount, unsigned char* vmask,
-                                          size_t mask_bytes, unsigned* host_count, cudaStream_t st);
+                                          size_t mask_bytes, unsigned* host_count, Counters* cnt, cudaStream_t st);
+// Marks (one byte per map cell, x fastest; the mask is not cleared here) every
+// map cell that the view rays of the frame's window read, or (flist given) of
+// the listed kFallbackTile^2 tiles, *fcount of them (nothing while it is 0).
+// Zeroes and uses cnt->tiles_mark.
+cudaError_t launch_mark_view_cells(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
+                                   unsigned char* cell_mask, Counters* cnt, const unsigned* flist,
+                                   const unsigned* fcount, cudaStream_t st);
 // K2 over a device list of kFallbackTile^2 pixel tiles (count in *fcount), with the map.
 cudaError_t launch_view_march_tiles(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                     const float* map, float4* out, Counters* cnt, const unsigned* flist,

@@ -259,17 +259,21 @@ static beams_status mlp_fallback(beams_renderer* r, const ExactGeo& g, const Pro
     *h = 0u;
     st->h_fallback = h;
   }
+  s = ensure_buffer(r, (void**)&r->d_vlist, &r->vlist_cap, (nvert + 1) * sizeof(unsigned),
+                    "allocating the map vertex list");
+  if (s != BEAMS_OK) return s;
   st->fb_tiles = L.ntiles;
   e = launch_mark_fallback_vertices(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, pb.flist, pb.fcount, st->vmask,
-                                    mask_bytes, (unsigned*)st->h_fallback, r->stream);
+                                    mask_bytes, (unsigned*)st->h_fallback, r->d_cnt, r->stream);
+  if (e == cudaSuccess) e = launch_list_marked_vertices(g, st->vmask, pb.fcount, r->d_vlist, r->stream);
   if (e == cudaSuccess)
     e = launch_light_march_f32(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map, r->d_cnt, r->stream,
-                               nullptr, 0, -1, pb.fcount, nullptr, st->vmask);
+                               nullptr, 0, -1, pb.fcount, nullptr, r->d_vlist);
   if (e == cudaSuccess)
     e = launch_view_march_tiles(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map, out, r->d_cnt + 1,
                                 pb.flist, pb.fcount, r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "mlp fallback launch");
-  launches += 4;
+  launches += 5;
   return BEAMS_OK;
 }
 

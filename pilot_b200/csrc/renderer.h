@@ -104,6 +104,15 @@ struct beams_renderer {
   int slab_fp64 = 1;
   int light_brick_log2 = 3;  // beams_set_tuning (8^3-vertex bricks)
   bool reuse_map = false;
+  // beams_set_lazy_shadow_map: the exact form builds only the map vertices
+  // that the frame's view rays read (d_cell_mask marks their cells)
+  bool lazy_map = false;
+  unsigned char* d_cell_mask = nullptr;
+  size_t cell_mask_cap = 0;
+  // the masked map builds' vertex list ((M+1)^3 + 1 entries: count, then ids),
+  // shared by the lazy map, the learned form's fallback and the bricks' Phase 1
+  unsigned* d_vlist = nullptr;
+  size_t vlist_cap = 0;
   bool bg = false;
   float bg_rgba[4] = {1.f, 1.f, 1.f, 1.f};
   // explicit rectilinear coordinates of the volume's point axes (beams_set_volume_coordinates)
@@ -197,6 +206,8 @@ struct beams_renderer {
     if (d_brick_imgs) cudaFree(d_brick_imgs);
     if (d_brick_cnt) cudaFree(d_brick_cnt);
     if (d_shell_mask) cudaFree(d_shell_mask);
+    if (d_cell_mask) cudaFree(d_cell_mask);
+    if (d_vlist) cudaFree(d_vlist);
     for (auto& s : brick_lane)
       if (s) cudaStreamDestroy(s);
     for (auto& e : brick_join)

@@ -30,6 +30,32 @@ struct NoRecord {
   __device__ __forceinline__ void operator()(const float*, const float4&, float) {}
 };
 
+// A view-march observer that marks, for every lit sample, the map cell that the
+// shading looks up (the cell of map_interp_t: truncate min(max((p - origin) / spacing,
+// 0), pd - 2) per axis), one byte per cell, skipping repeats of the previous
+// sample's cell. A masked map build then lists every vertex with a marked cell
+// around it (the same vertex set as marking the 8 corners, with one store per
+// cell).
+struct CellMarker {
+  float morig[3], minv[3];
+  int pd[3];
+  unsigned char* mask;
+  unsigned last;
+  __device__ __forceinline__ void operator()(const float* p, const float4&, float) {
+    int c[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float t = (p[d] - morig[d]) * minv[d];
+      c[d] = trunc_small(fminf(fmaxf(t, 0.f), (float)(pd[d] - 2)));
+    }
+    const unsigned mx = (unsigned)(pd[0] - 1), mxy = mx * (unsigned)(pd[1] - 1);
+    const unsigned id = (unsigned)c[2] * mxy + (unsigned)c[1] * mx + (unsigned)c[0];
+    if (id == last) return;
+    last = id;
+    mask[id] = 1;
+  }
+};
+
 // SKIP: samples in macro-cells whose occupancy is 0 (every value there maps to
 // an in-range TF entry of alpha 0) only advance and count as lit: their
 // premultiplied alpha is 0, so they change neither colour nor alpha.

@@ -66,6 +66,11 @@ int main(int argc, char** argv) {
     profiler->StartFrame("Second render");
     mapper.RenderCells(f, {0.0, 1.0}, camera);
     profiler->EndFrame();
+    // the lazy map extension gives the same image bit for bit
+    mapper.SetLazyShadowMap(true);
+    const std::vector<float> lazy = mapper.RenderCells(f, {0.0, 1.0}, camera);
+    mapper.SetLazyShadowMap(false);
+    if (lazy != rgba) return 5;
     profiler->Collect();
     profiler->PrintSummary(std::cerr);  // the reference prints to a stream as well
 

@@ -1,0 +1,196 @@
+"""The exact form's lazy map (beams_set_lazy_shadow_map): a view march without
+shading marks the map cells the frame's rays read and the light march builds
+only their corners. The reference builds every vertex (TransmittanceMap.h:565-621)
+and reads the map only at lit samples (LightedVolumeRenderer.cxx:456-475), whose
+set and order do not depend on the map, so the image must equal the full map's
+bit for bit.
+
+Each lazy frame follows a frame that left other lights' maps in the map
+buffer, so a vertex that the lazy build skips but the view march reads would
+change the image.
+
+Bars: lazy image == full-map image (np.array_equal) with equal lit-sample
+counts, on uniform and rectilinear fields, point and directional lights, the
+multi-light extension, canvas depth limits and both empty-skip settings; fewer
+vertices built than (M+1)^3 when the view sees part of the volume; one lazy
+image also checked directly against the oracle (max |dRGBA| <= 2e-3, >= 99.9%
+bit-identical pixels, the exact form's bar).
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from pilot_b200 import beams as B
+from pilot_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+TOL = 2e-3
+
+
+def renderer(s, coords=None):
+    r = B.Renderer(0)
+    r.set_volume(s.field_numpy(), origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+    if coords is not None:
+        r.set_volume_coordinates(*coords)
+    s.configure(r)
+    return r
+
+
+POISON_LIGHTS = [((0.3, 0.9, -0.3), (1.0, 0.2, 0.2), 1.0), ((-0.8, 0.1, 0.6), (0.2, 1.0, 0.2), 1.0),
+                 ((0.1, -0.7, -0.7), (0.2, 0.2, 1.0), 1.0)]
+
+
+def poison(r, cam, nlights=1):
+    """Leaves other directional lights' full maps in the map buffer, so that a
+    vertex the lazy build skips but the view march reads changes the image."""
+    r.set_lazy_shadow_map(False)
+    r.clear_lights()
+    for d, c, i in POISON_LIGHTS[:nlights]:
+        r.add_directional_light(d, c, i)
+    r.render(cam)
+
+
+def full_and_lazy(r, cam, restore, nlights=1):
+    """restore(r) puts back the scene's lights after the poisoning frame."""
+    r.set_lazy_shadow_map(False)
+    full, tf = r.render(cam)
+    poison(r, cam, nlights)
+    restore(r)
+    r.set_lazy_shadow_map(True)
+    lazy, tl = r.render(cam)
+    r.set_lazy_shadow_map(False)
+    return full, tf, lazy, tl
+
+
+def assert_same(full, tf, lazy, tl, nvert):
+    assert np.array_equal(lazy, full), f"lazy image differs by {np.max(np.abs(lazy - full))}"
+    assert tl["lit_samples"] == tf["lit_samples"]
+    assert tf["map_vertices"] == nvert
+    assert 0 < tl["map_vertices"] <= nvert
+
+
+CASES = [
+    dict(seed=0, kind="blobs", light_kind=0, fov=30.0),
+    dict(seed=1, kind="blobs", light_kind=1, fov=30.0),
+    dict(seed=2, kind="noise", light_kind=0, fov=9.0),
+    dict(seed=3, kind="noise", light_kind=1, fov=6.0),
+]
+
+
+@pytest.mark.parametrize("c", CASES, ids=lambda c: f"{c['kind']}-L{c['light_kind']}-fov{c['fov']:g}")
+def test_lazy_map_image_equals_full_map_image(cuda_device, c):
+    s = scenes.small(c["seed"], n=40, image=96, m=20, kind=c["kind"], light_kind=c["light_kind"])
+    s.fov_y_deg = c["fov"]
+    r = renderer(s)
+    nv = (s.map_m + 1) ** 3
+    full, tf, lazy, tl = full_and_lazy(r, s.camera(), s.configure)
+    assert_same(full, tf, lazy, tl, nv)
+    if c["fov"] < 10:  # a zoomed view reads part of the volume
+        assert tl["map_vertices"] < nv
+    print(f"{c}: built {tl['map_vertices']} of {nv} vertices")
+
+
+def test_lazy_map_image_matches_oracle(cuda_device):
+    s = scenes.small(4, n=40, image=96, m=20, kind="noise", light_kind=0)
+    s.fov_y_deg = 12.0
+    r = renderer(s)
+    poison(r, s.camera())
+    s.configure(r)
+    r.set_lazy_shadow_map(True)
+    img, t = r.render(s.camera())
+    o = Oracle(s)
+    om, _ = o.light_march()
+    oimg, olit = o.view_march(om)
+    err = np.abs(img - oimg)
+    assert err.max() <= TOL, f"max |d| {err.max()}"
+    assert np.mean(np.all(img == oimg, axis=-1)) > 0.999
+    assert t["lit_samples"] == olit
+
+
+def test_lazy_map_is_not_readable_or_reused(cuda_device):
+    s = scenes.small(5, n=32, image=64, m=16)
+    r = renderer(s)
+    r.set_reuse_shadow_map(True)
+    r.set_lazy_shadow_map(True)
+    a, ta = r.render(s.camera())
+    with pytest.raises(B.BeamsError):
+        r.get_shadow_map((s.map_m + 1) ** 3)
+    b, tb = r.render(s.camera())  # rebuilt, never reused
+    assert tb["map_vertices"] == ta["map_vertices"] > 0
+    assert np.array_equal(a, b)
+    r.set_lazy_shadow_map(False)
+    c, tc = r.render(s.camera())  # a full map again, readable
+    assert np.array_equal(a, c)
+    assert tc["map_vertices"] == (s.map_m + 1) ** 3
+    assert r.get_shadow_map((s.map_m + 1) ** 3).size == (s.map_m + 1) ** 3
+
+
+@pytest.mark.parametrize("skip", [True, False])
+def test_lazy_map_with_and_without_empty_skip(cuda_device, skip):
+    s = scenes.small(6, n=48, image=80, m=24, kind="blobs", light_kind=0)
+    s.fov_y_deg = 14.0
+    r = renderer(s)
+    r.set_tuning(light_brick=8, empty_skip=skip, view_skip=skip)
+    full, tf, lazy, tl = full_and_lazy(r, s.camera(), s.configure)
+    assert_same(full, tf, lazy, tl, (s.map_m + 1) ** 3)
+
+
+def test_lazy_map_rectilinear(cuda_device):
+    s = scenes.small(21, n=40, image=80, m=16, kind="noise", light_kind=1)
+    rng = np.random.default_rng(21)
+    coords = []
+    for _ in range(3):
+        w = rng.uniform(0.4, 1.6, s.dims[0] - 1)
+        cc = np.concatenate([[0.0], np.cumsum(w)])
+        coords.append(np.float32(cc / cc[-1]))
+    s.fov_y_deg = 10.0
+    r = renderer(s, coords)
+    full, tf, lazy, tl = full_and_lazy(r, s.camera(), s.configure)
+    assert_same(full, tf, lazy, tl, (s.map_m + 1) ** 3)
+
+
+def test_lazy_map_multi_light(cuda_device):
+    s = scenes.small(2, n=40, image=96, m=20, kind="noise")
+    s.fov_y_deg = 12.0
+    r = renderer(s)
+
+    def lights(q):
+        s.configure(q)
+        q.add_point_light((1.6, 0.2, -0.4), (0.9, 0.5, 0.2), 0.8)
+        q.add_directional_light((-0.3, -1.0, 0.2), (0.2, 0.4, 1.0), 0.6)
+
+    lights(r)
+    r.set_multi_light(True)
+    nv = (s.map_m + 1) ** 3
+    full, tf, lazy, tl = full_and_lazy(r, s.camera(), lights, nlights=3)
+    assert np.array_equal(lazy, full)
+    assert tl["lit_samples"] == tf["lit_samples"]
+    assert tf["map_vertices"] == 3 * nv
+    assert 0 < tl["map_vertices"] < 3 * nv and tl["map_vertices"] % 3 == 0
+
+
+def test_lazy_map_with_depth_limits(cuda_device):
+    s = scenes.small(3, n=40, image=96, m=20, kind="noise", light_kind=1)
+    r = renderer(s)
+    rng = np.random.default_rng(3)
+    c = float(np.linalg.norm(np.asarray(s.cam_pos) - 0.5))
+    lim = rng.uniform(c - 0.6, c, (s.height, s.width)).astype(np.float32)  # most rays end inside
+    lim[rng.random(lim.shape) < 0.1] = np.inf
+    r.set_lazy_shadow_map(True)
+    _, t_nolim = r.render(s.camera())
+    r.set_depth_buffer(lim, B.DEPTH_RAY_DISTANCE)
+    full, tf, lazy, tl = full_and_lazy(r, s.camera(), s.configure)
+    assert_same(full, tf, lazy, tl, (s.map_m + 1) ** 3)
+    assert tl["map_vertices"] < t_nolim["map_vertices"]  # clipped rays read fewer cells
+
+
+def test_lazy_map_ignored_by_the_precision_form(cuda_device):
+    s = scenes.small(7, n=32, image=64, m=16)
+    r = renderer(s)
+    r.set_form(B.FORM_PRECISION, field_dtype=B.BF16)
+    a, ta = r.render(s.camera())
+    r.set_lazy_shadow_map(True)
+    b, tb = r.render(s.camera())
+    assert np.array_equal(a, b)
+    assert tb["map_vertices"] == ta["map_vertices"] == (s.map_m + 1) ** 3
+    assert r.get_shadow_map((s.map_m + 1) ** 3).size == (s.map_m + 1) ** 3

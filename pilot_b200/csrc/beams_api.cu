@@ -451,7 +451,7 @@ static beams_status build_map_lazy(beams_renderer* r, const ExactGeo& g, int& la
     if (s != BEAMS_OK) return s;
     occ = r->d_occ;
   }
-  s = ensure_buffer(r, (void**)&r->d_vlist, &r->vlist_cap, (nvert + 1) * sizeof(unsigned),
+  s = ensure_buffer(r, (void**)&r->d_vlist, &r->vlist_cap, marked_list_bytes(g.pd),
                     "allocating the map vertex list");
   if (s != BEAMS_OK) return s;
   const float4* quads = (const float4*)r->d_quads;
@@ -663,8 +663,7 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
     // the shell's vertices listed once (the bricks' maps share their size)
     const unsigned* shell_list = nullptr;
     if (shell) {
-      const size_t nv = (size_t)G[0].pd[0] * G[0].pd[1] * G[0].pd[2];
-      s = ensure_buffer(r, (void**)&r->d_vlist, &r->vlist_cap, (nv + 1) * sizeof(unsigned),
+      s = ensure_buffer(r, (void**)&r->d_vlist, &r->vlist_cap, marked_list_bytes(G[0].pd),
                         "allocating the map vertex list");
       if (s != BEAMS_OK) return s;
       e = launch_list_marked_vertices(G[0], shell, nullptr, r->d_vlist, r->stream);

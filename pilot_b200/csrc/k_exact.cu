@@ -79,45 +79,92 @@ __device__ __forceinline__ bool vertex_in_marked_cell(const unsigned char* __res
 // for the per-vertex test, most of it atomics on the one counter). One warp per
 // 32-vertex tile of the order at a static stride, one append per warp that
 // finds a vertex (lane order kept inside the warp).
+// Blocks of 8^3 map cells: cb[d] = ceil((pd[d] - 1) / 8) per axis.
+__host__ __device__ inline void cell_blocks(const int pd[3], int cb[3]) {
+  for (int d = 0; d < 3; ++d) cb[d] = (pd[d] - 1 + 7) >> 3;
+}
+
+// One byte per 8^3-cell block: 1 when a cell of the block is marked (every
+// block written, so nothing needs clearing). One warp per block, 16 cells a lane.
+__global__ void __launch_bounds__(256) k_mark_cell_blocks(const ExactGeo g, const unsigned char* __restrict__ cm,
+                                                          const unsigned* __restrict__ gate,
+                                                          unsigned char* __restrict__ blocks) {
+  if (gate && *gate == 0u) return;
+  int cb[3];
+  cell_blocks(g.pd, cb);
+  const int nb = cb[0] * cb[1] * cb[2];
+  const unsigned mx = g.pd[0] - 1, my = g.pd[1] - 1, mz = g.pd[2] - 1;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += nwarps) {
+    const unsigned bx = b % cb[0], by = (b / cb[0]) % cb[1], bz = b / (cb[0] * cb[1]);
+    unsigned any = 0;
+#pragma unroll 4
+    for (int k = lane; k < 512; k += 32) {
+      const unsigned x = (bx << 3) + (k & 7), y = (by << 3) + ((k >> 3) & 7), z = (bz << 3) + (k >> 6);
+      if (x < mx && y < my && z < mz) any |= __ldg(cm + (z * my + y) * mx + x);
+    }
+    any = __any_sync(0xffffffffu, any != 0u);
+    if (lane == 0) blocks[b] = any ? 1 : 0;
+  }
+}
+
 __global__ void __launch_bounds__(256) k_list_marked_vertices(const ExactGeo g, const unsigned char* __restrict__ cm,
+                                                              const unsigned char* __restrict__ blocks,
                                                               const unsigned* __restrict__ gate,
                                                               unsigned* __restrict__ list) {
   if (gate && *gate == 0u) return;
+  int cb[3];
+  cell_blocks(g.pd, cb);
   __shared__ int s_bo[8];
   const int bl = g.light_brick_log2;
   if (threadIdx.x == 0 && bl) brick_order_setup(g, bl, s_bo);
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int nvert = g.pd[0] * g.pd[1] * g.pd[2];
-  const int ntiles = bl ? (s_bo[0] * s_bo[1] * s_bo[2]) << (3 * bl - 5) : (nvert + 31) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < ntiles; tile += nwarps) {
-    int x, y, z;
-    bool in;
-    if (bl) {  // the brick order of k_light_march
-      const int bi = tile >> (3 * bl - 5);
-      const int li = ((tile & ((1 << (3 * bl - 5)) - 1)) << 5) + lane;
-      const int m = (1 << bl) - 1;
-      int bx, by, bz;
-      pencil_brick(bi, s_bo, bx, by, bz);
-      x = (bx << bl) + (li & m);
-      y = (by << bl) + ((li >> bl) & m);
-      z = (bz << bl) + (li >> (2 * bl));
-      in = x < g.pd[0] && y < g.pd[1] && z < g.pd[2];
-    } else {
-      const int id = (tile << 5) + lane;
-      in = id < nvert;
-      x = id % g.pd[0];
-      y = (id / g.pd[0]) % g.pd[1];
-      z = id / (g.pd[0] * g.pd[1]);
-    }
-    const bool take = in && vertex_in_marked_cell(cm, g.pd, x, y, z);
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  auto append = [&](bool take, int x, int y, int z) {
     const unsigned b = __ballot_sync(0xffffffffu, take);
-    if (b == 0u) continue;
+    if (b == 0u) return;
     unsigned base = 0;
     if (lane == 0) base = atomicAdd(list, (unsigned)__popc(b));
     base = __shfl_sync(0xffffffffu, base, 0);
     if (take) list[1 + base + __popc(b & ((1u << lane) - 1u))] = (unsigned)((z * g.pd[1] + y) * g.pd[0] + x);
+  };
+  if (bl == 0) {  // row order: 32-vertex tiles of the rows
+    const int nvert = g.pd[0] * g.pd[1] * g.pd[2];
+    for (int tile = warp; tile < (nvert + 31) >> 5; tile += nwarps) {
+      const int id = (tile << 5) + lane;
+      const int x = id % g.pd[0], y = (id / g.pd[0]) % g.pd[1], z = id / (g.pd[0] * g.pd[1]);
+      append(id < nvert && vertex_in_marked_cell(cm, g.pd, x, y, z), x, y, z);
+    }
+    return;
+  }
+  // one warp per vertex brick of the order: the 8^3-cell blocks around the
+  // brick's vertices first (a brick with none marked is skipped whole), then
+  // the brick's 32-vertex tiles, each vertex tested against its own cells
+  const int E = 1 << bl, m = E - 1;
+  const int nbricks = s_bo[0] * s_bo[1] * s_bo[2];
+  for (int bi = warp; bi < nbricks; bi += nwarps) {
+    int v[3];
+    pencil_brick(bi, s_bo, v[0], v[1], v[2]);
+    int lo[3], n[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int c0 = max(v[d] * E - 1, 0), c1 = min(v[d] * E + m, g.pd[d] - 2);  // cells around the vertices
+      lo[d] = c0 >> 3;
+      n[d] = (c1 >> 3) - lo[d] + 1;
+    }
+    bool any = false;
+    for (int k = lane; k < n[0] * n[1] * n[2]; k += 32) {
+      const int i = k % n[0], j = (k / n[0]) % n[1], l = k / (n[0] * n[1]);
+      any |= blocks[((lo[2] + l) * cb[1] + lo[1] + j) * cb[0] + lo[0] + i] != 0;
+    }
+    if (!__any_sync(0xffffffffu, any)) continue;
+    for (int li = lane; li < E * E * E; li += 32) {
+      const int x = (v[0] << bl) + (li & m), y = (v[1] << bl) + ((li >> bl) & m), z = (v[2] << bl) + (li >> (2 * bl));
+      append(x < g.pd[0] && y < g.pd[1] && z < g.pd[2] && vertex_in_marked_cell(cm, g.pd, x, y, z), x, y, z);
+    }
   }
 }
 
@@ -612,11 +659,21 @@ cudaError_t launch_mark_view_cells(const ExactGeo& g, const float4* quads, const
                : launch_mark<false, false>(g, quads, tab, tf, cell_mask, cnt, nullptr, nullptr, st);
 }
 
+size_t marked_list_bytes(const int pd[3]) {
+  int cb[3];
+  cell_blocks(pd, cb);
+  const size_t nvert = (size_t)pd[0] * pd[1] * pd[2];
+  return (nvert + 1) * sizeof(unsigned) + (size_t)cb[0] * cb[1] * cb[2];
+}
+
 cudaError_t launch_list_marked_vertices(const ExactGeo& g, const unsigned char* cell_mask, const unsigned* gate,
                                         unsigned* list, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(list, 0, sizeof(unsigned), st);
   if (e != cudaSuccess) return e;
-  k_list_marked_vertices<<<num_sms() * 8, 256, 0, st>>>(g, cell_mask, gate, list);
+  const size_t nvert = (size_t)g.pd[0] * g.pd[1] * g.pd[2];
+  unsigned char* blocks = (unsigned char*)(list + nvert + 1);
+  k_mark_cell_blocks<<<num_sms() * 8, 256, 0, st>>>(g, cell_mask, gate, blocks);
+  k_list_marked_vertices<<<num_sms() * 8, 256, 0, st>>>(g, cell_mask, blocks, gate, list);
   return cudaGetLastError();
 }
 

@@ -23,8 +23,10 @@ cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const
                                    const unsigned char* occ = nullptr, const unsigned* vlist = nullptr);
 // The work list of a masked map build (vlist above): zeroes list[0], then lists
 // in list[1..] the vertices of the cells marked in cell_mask (one byte per map
-// cell, x fastest), list[0] their count. list holds (M+1)^3 + 1 entries.
+// cell, x fastest), list[0] their count. list spans marked_list_bytes(pd):
+// (M+1)^3 + 1 entries, then one byte per 8^3-cell block (scratch).
 // gate (non-null): nothing is listed while *gate is 0.
+size_t marked_list_bytes(const int pd[3]);
 cudaError_t launch_list_marked_vertices(const ExactGeo& g, const unsigned char* cell_mask, const unsigned* gate,
                                         unsigned* list, cudaStream_t st);
 // Empty-space occupancy of 8^3-cell macro-cells for the light march's skip.

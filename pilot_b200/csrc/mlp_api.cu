@@ -259,7 +259,7 @@ static beams_status mlp_fallback(beams_renderer* r, const ExactGeo& g, const Pro
     *h = 0u;
     st->h_fallback = h;
   }
-  s = ensure_buffer(r, (void**)&r->d_vlist, &r->vlist_cap, (nvert + 1) * sizeof(unsigned),
+  s = ensure_buffer(r, (void**)&r->d_vlist, &r->vlist_cap, marked_list_bytes(g.pd),
                     "allocating the map vertex list");
   if (s != BEAMS_OK) return s;
   st->fb_tiles = L.ntiles;

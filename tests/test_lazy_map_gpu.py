@@ -135,6 +135,18 @@ def test_lazy_map_with_and_without_empty_skip(cuda_device, skip):
     assert_same(full, tf, lazy, tl, (s.map_m + 1) ** 3)
 
 
+@pytest.mark.parametrize("brick", [0, 16, 32])
+def test_lazy_map_under_every_vertex_order(cuda_device, brick):
+    """The vertex list follows the light march's order: rows, or cubic bricks."""
+    s = scenes.small(8, n=56, image=96, m=40, kind="noise", light_kind=0)
+    s.fov_y_deg = 11.0
+    r = renderer(s)
+    r.set_tuning(light_brick=brick, empty_skip=False, view_skip=False)
+    full, tf, lazy, tl = full_and_lazy(r, s.camera(), s.configure)
+    assert_same(full, tf, lazy, tl, (s.map_m + 1) ** 3)
+    assert tl["map_vertices"] < (s.map_m + 1) ** 3
+
+
 def test_lazy_map_rectilinear(cuda_device):
     s = scenes.small(21, n=40, image=80, m=16, kind="noise", light_kind=1)
     rng = np.random.default_rng(21)

@@ -475,12 +475,35 @@ def run_ours(args):
         same = bool(np.array_equal(out.cpu().numpy(), exact_img))
         lms, lclk = time_frames(lambda: r.render(cam, out=out, timings=False), args.steps, args.warmup, stream,
                                 world, local)
+        # the same field and light seen from 2 and 3 units instead of 1 (the
+        # whole volume in view): full against lazy, a few frames each
+        views = {}
+        cdir = np.asarray(s.cam_pos, np.float64) - 0.5
+        for dist in (2.0, 3.0):
+            vpos = tuple(float(v) for v in 0.5 + cdir / np.linalg.norm(cdir) * dist)
+            vcam = B.Renderer.camera(vpos, s.cam_look, s.cam_up, s.fov_y_deg, s.width, s.height)
+            rec = {}
+            for lz in (False, True):
+                r.set_lazy_shadow_map(lz)
+                _, tv = r.render(vcam, out=out, timings=True)
+                rec["lazy" if lz else "full"] = out.cpu().numpy()
+                vms, _ = time_frames(lambda: r.render(vcam, out=out, timings=False), 5, 2, stream, world, local)
+                rec[("lazy" if lz else "full") + "_ms"] = vms / 5
+                if lz:
+                    rec["map_vertices_built"] = tv["map_vertices"]
+                else:
+                    rec["lit_samples"] = tv["lit_samples"]
+            views[f"distance_{dist:g}"] = {"full_ms_per_frame": rec["full_ms"], "lazy_ms_per_frame": rec["lazy_ms"],
+                                          "map_vertices_built": rec["map_vertices_built"],
+                                          "lit_samples": rec["lit_samples"],
+                                          "image_equals_full_map": bool(np.array_equal(rec["lazy"], rec["full"]))}
         r.set_lazy_shadow_map(False)
         lazy = {"ms_per_frame": lms / args.steps, "value": replica_value(world, args.steps, lit_frame, lms),
                 "unit": UNIT, "map_build_ms": tl["map_build_ms"], "view_march_ms": tl["view_march_ms"],
                 "map_vertices_built": tl["map_vertices"], "map_vertices": nvert,
                 "lit_samples_equal": tl["lit_samples"] == lit_frame, "image_equals_full_map": same,
                 "speedup_vs_full_map": (max_ms / args.steps) / (lms / args.steps), "clocks": lclk,
+                "other_views": views,
                 "note": "a view march without shading marks the map cells the rays read, the light march builds "
                         "the marked cells' corners, then the view march; map_build_ms covers the marking"}
 
@@ -509,6 +532,19 @@ def run_ours(args):
                               if lights == 32 else "2^24 samples for the rendered light only (fixed light, any camera)")
             if lazy is not None:
                 rec["speedup_vs_exact_lazy_map"] = lazy["ms_per_frame"] / rec["ms_per_frame"]
+                # the lazy record's wider views, rendered by this network
+                rec["other_views"] = {}
+                cdir = np.asarray(s.cam_pos, np.float64) - 0.5
+                for vname, v in lazy["other_views"].items():
+                    dist = float(vname.split("_")[1])
+                    vpos = tuple(float(c) for c in 0.5 + cdir / np.linalg.norm(cdir) * dist)
+                    vcam = B.Renderer.camera(vpos, s.cam_look, s.cam_up, s.fov_y_deg, s.width, s.height)
+                    for _ in range(2):  # the frame order settles on the failing-tile count
+                        _, tv = r.render(vcam, out=out, timings=True)
+                    vms, _ = time_frames(lambda: r.render(vcam, out=out, timings=False), 5, 2, stream, world, local)
+                    rec["other_views"][vname] = {"ms_per_frame": vms / 5, "fallback_tiles": tv["fallback_tiles"],
+                                                 "speedup_vs_exact": v["full_ms_per_frame"] / (vms / 5),
+                                                 "speedup_vs_exact_lazy_map": v["lazy_ms_per_frame"] / (vms / 5)}
             learned[name] = rec
         r.set_form(B.FORM_EXACT)
 
@@ -1001,6 +1037,10 @@ def run_bricks(args, nested=False):
     whole_ms, _ = time_frames(lambda: r.render(cam, out=out, timings=False), 10, 3, stream, 1, local)
     whole_ms /= 10
     whole = out.cpu().numpy()
+    r.set_lazy_shadow_map(True)
+    whole_lazy_ms, _ = time_frames(lambda: r.render(cam, out=out, timings=False), 10, 3, stream, 1, local)
+    whole_lazy_ms /= 10
+    r.set_lazy_shadow_map(False)
     # 2x2x2 bricks; neighbours share their face plane (the reference's blocks)
     nx = s.dims[0]
     cells = nx - 1
@@ -1023,6 +1063,12 @@ def run_bricks(args, nested=False):
     frame = lambda: r.render(cam, out=out, timings=False)  # noqa: E731
     total_ms, clocks = time_frames(frame, args.steps, args.warmup, stream, 1, local)
     value = tb["lit_samples"] * args.steps / (total_ms / 1e3)
+    # the same bricks with the lazy map: only the stitched vertices the view reads
+    r.set_lazy_shadow_map(True)
+    _, tz = r.render(cam, out=out, timings=True)
+    lazy_same = bool(np.array_equal(out.cpu().numpy(), img))
+    lazy_ms, _ = time_frames(frame, args.steps, args.warmup, stream, 1, local)
+    r.set_lazy_shadow_map(False)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded 4-octave gradient noise generated on the device)",
@@ -1033,7 +1079,11 @@ def run_bricks(args, nested=False):
             "lit_samples_per_frame": tb["lit_samples"], "gpu_launches": tb["kernel_launches"] * args.steps,
             "phases_ms": {"maps_and_stitch": tb["map_build_ms"], "view_marches": tb["view_march_ms"],
                           "composite": tb["composite_ms"]},
-            "undivided_ms_per_frame": whole_ms, "psnr_vs_undivided": psnr(img, whole), "clocks": clocks}
+            "undivided_ms_per_frame": whole_ms, "psnr_vs_undivided": psnr(img, whole), "clocks": clocks,
+            "lazy_map": {"ms_per_frame": lazy_ms / args.steps, "undivided_ms_per_frame": whole_lazy_ms,
+                         "map_vertices_built": tz["map_vertices"], "stitched_map_vertices": tb["map_vertices"],
+                         "image_equals_full_maps": lazy_same,
+                         "phases_ms": {"maps_and_stitch": tz["map_build_ms"], "view_marches": tz["view_march_ms"]}}}
     r.close()
     if nested:
         return line
@@ -1055,12 +1105,13 @@ def run_bricks(args, nested=False):
 #   precision_light  precision-form K1, bf16 640^3
 #   precision_view   precision-form K2, bf16 640^3, 1024^2, map cached
 #   bricks           512^3 noise as 2x2x2 bricks: K1, K5, K2, K6
+#   bricks_lazy      the same with the lazy map (marks and lists before K5)
 # Each case sets up its scene, runs the target kernel --reps times and exits 0;
 # device memory stays within a few GB. The tuning is fixed (8^3 vertex bricks,
 # skipping as stated per case) so that the launch sequence is the same every run.
 # ---------------------------------------------------------------------------
 PROFILE_CASES = ["light_march", "view_march", "lazy_frame", "mlp_view", "mlp_frame", "mlp_frame32", "mlp_tc", "mlp_train", "batch",
-                 "precision_light", "precision_view", "bricks"]
+                 "precision_light", "precision_view", "bricks", "bricks_lazy"]
 
 
 def run_profile_case(a):
@@ -1150,7 +1201,7 @@ def run_profile_case(a):
             out = torch.empty((s.height, s.width, 4), device="cuda")
             for _ in range(a.reps):
                 r.render(s.camera(), out=out, timings=False)
-    elif a.profile_case == "bricks":
+    elif a.profile_case in ("bricks", "bricks_lazy"):
         s = scenes.config1()
         fd = s.field_device()
         cells = s.dims[0] - 1
@@ -1167,6 +1218,7 @@ def run_profile_case(a):
         r.set_bricks(bricks)
         s.configure(r)
         r.set_shadow_map_size(s.map_m // 2)
+        r.set_lazy_shadow_map(a.profile_case == "bricks_lazy")
         cam = s.camera()
         out = torch.empty((s.height, s.width, 4), device="cuda")
         for _ in range(a.reps):

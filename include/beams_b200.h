@@ -165,8 +165,11 @@ beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable);
  * the light march builds the corners of the marked cells. The image is the
  * full map's bit for bit; the map is partial, so beams_get_shadow_map returns
  * BEAMS_ERR_STATE after such a frame and the map is never reused.
- * beams_timings.map_vertices reports the vertices built. Off by default; the
- * precision and learned forms and multi-block scenes ignore it. */
+ * beams_timings.map_vertices reports the vertices built. In a multi-block
+ * scene each brick's view rays mark the cells of its stitched map (Phases 2-3)
+ * and only their corners are stitched (beams_get_brick_map's stitched stage
+ * then returns BEAMS_ERR_STATE; Phase 1 is unchanged). Off by default; the
+ * precision and learned forms ignore it. */
 beams_status beams_set_lazy_shadow_map(beams_renderer* r, int enable);
 /* ---- legacy VTK files ---------------------------------------------------------
  * Replaces the reference's dataset read (pilot/io/DataSetUtils.cxx:13-42, VTK-m's

@@ -612,6 +612,7 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
   e = cudaMemsetAsync(r->d_brick_cnt, 0, nb * sizeof(Counters), r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "clearing brick counters");
   auto lane = [&](int b) { return r->brick_lane[b % beams_renderer::kBrickLanes]; };
+  const bool lazy = r->lazy_map && r->use_map;
   auto lane_fail = [&](cudaError_t err, const char* what) {
     brick_lanes_join(r);
     return cuda_fail(r, err, what);
@@ -662,6 +663,7 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
     }
     // the shell's vertices listed once (the bricks' maps share their size)
     const unsigned* shell_list = nullptr;
+    r->shell_listed = shell != nullptr;
     if (shell) {
       s = ensure_buffer(r, (void**)&r->d_vlist, &r->vlist_cap, marked_list_bytes(G[0].pd),
                         "allocating the map vertex list");
@@ -683,12 +685,45 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
     e = brick_lanes_join(r);
     if (e != cudaSuccess) return cuda_fail(r, e, "joining brick streams");
     // Phases 2-3: stitched maps (each reads every brick's Phase-1 map)
+    // The lazy map: each brick's view rays (their limits and pixel window as in
+    // Phase 4) mark the cells of its map they read, and the stitched march
+    // builds only those cells' corners; a brick no pixel reaches needs none.
+    bool reached[kMaxBricks];
+    if (lazy) {
+      s = prepare_ray_limits(r, G[0], launches);
+      if (s != BEAMS_OK) return s;
+      for (int b = 0; b < nb; ++b) {
+        G[b].ray_max = G[0].ray_max;
+        reached[b] = brick_window(G[b], G[b].win);
+        Brick& B = r->bricks[b];
+        const size_t ncell = (size_t)(G[b].pd[0] - 1) * (G[b].pd[1] - 1) * (G[b].pd[2] - 1);
+        s = ensure_buffer(r, (void**)&B.d_cell_mask, &B.cell_mask_cap, ncell, "allocating a brick's cell mask");
+        if (s == BEAMS_OK)
+          s = ensure_buffer(r, (void**)&B.d_vlist, &B.vlist_cap, marked_list_bytes(G[b].pd),
+                            "allocating a brick's vertex list");
+        if (s != BEAMS_OK) return s;
+      }
+    }
     s = brick_lanes_fork(r);
     if (s != BEAMS_OK) return s;
     for (int b = 0; b < nb; ++b) {
       Brick& B = r->bricks[b];
+      B.final_partial = lazy;
+      const unsigned* list = nullptr;
+      if (lazy) {
+        if (!reached[b]) continue;
+        const size_t ncell = (size_t)(G[b].pd[0] - 1) * (G[b].pd[1] - 1) * (G[b].pd[2] - 1);
+        e = cudaMemsetAsync(B.d_cell_mask, 0, ncell, lane(b));
+        if (e == cudaSuccess)
+          e = launch_mark_view_cells(G[b], B.d_quads, B.d_tab, r->d_tf, B.d_cell_mask, r->d_brick_cnt + b, nullptr,
+                                     nullptr, lane(b));
+        if (e == cudaSuccess) e = launch_list_marked_vertices(G[b], B.d_cell_mask, nullptr, B.d_vlist, lane(b));
+        if (e != cudaSuccess) return lane_fail(e, "brick map cell marking");
+        launches += 3;
+        list = B.d_vlist;
+      }
       e = launch_light_march_f32(G[b], B.d_quads, B.d_tab, r->d_tf, B.d_map_final, r->d_brick_cnt + b, lane(b),
-                                 r->d_refs, nb, b);
+                                 r->d_refs, nb, b, nullptr, nullptr, list);
       if (e != cudaSuccess) return lane_fail(e, "brick stitch march");
       ++launches;
     }
@@ -696,9 +731,11 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
     if (e != cudaSuccess) return cuda_fail(r, e, "joining brick streams");
   }
   cudaEventRecord(r->ev[1], r->stream);
-  s = prepare_ray_limits(r, G[0], launches);  // one camera: the same limits for every brick
-  if (s != BEAMS_OK) return s;
-  for (int b = 1; b < nb; ++b) G[b].ray_max = G[0].ray_max;
+  if (!lazy) {
+    s = prepare_ray_limits(r, G[0], launches);  // one camera: the same limits for every brick
+    if (s != BEAMS_OK) return s;
+    for (int b = 1; b < nb; ++b) G[b].ray_max = G[0].ray_max;
+  }
   // Phase 4: view marches
   s = brick_lanes_fork(r);
   if (s != BEAMS_OK) return s;
@@ -782,8 +819,22 @@ beams_status render_bricks_frame(beams_renderer* r, const beams_camera* cam, flo
       t->lit_samples += k.lit_samples;
       t->rays_hit += k.rays_hit;
     }
+    // the stitched maps' vertices (Phase 1 is not counted); under the lazy map
+    // the listed ones: the masked builds count what they build, Phase 1's
+    // shell list (its length in the list's first entry) included, so that is
+    // taken off once per brick
     size_t nv = 0;
-    for (auto& b : r->bricks) nv += r->use_map ? b.map_count : 0;
+    if (r->lazy_map && r->use_map) {
+      for (size_t b = 1; b < c.size(); ++b) nv += c[b].map_vertices;
+      if (r->shell_listed) {
+        unsigned shell_n = 0;
+        e = cudaMemcpy(&shell_n, r->d_vlist, sizeof(unsigned), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(r, e, "reading the shell list length");
+        nv -= (size_t)shell_n * r->bricks.size();
+      }
+    } else {
+      for (auto& b : r->bricks) nv += r->use_map ? b.map_count : 0;
+    }
     t->map_vertices = (int)nv;
     t->kernel_launches = launches;
   } else if (out_on_device == BEAMS_OUT_HOST) {
@@ -1466,6 +1517,8 @@ beams_status beams_get_brick_map(beams_renderer* r, int brick, int stage, float*
   Brick& B = r->bricks[brick];
   const float* src = stage ? B.d_map_final : B.d_map_local;
   if (!src || B.map_count == 0) return fail(r, BEAMS_ERR_STATE, "brick map not built yet");
+  if (stage && B.final_partial)
+    return fail(r, BEAMS_ERR_STATE, "the lazy map built only the stitched vertices the view reads");
   if (!dst || count < B.map_count) return fail(r, BEAMS_ERR_INVALID_ARG, "destination too small for the map");
   cudaSetDevice(r->device);
   cudaError_t e = cudaMemcpyAsync(dst, src, B.map_count * sizeof(float),

@@ -614,6 +614,15 @@ static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4*
       }
       return cudaGetLastError();
     }
+  } else if constexpr (STITCH && !PREC) {
+    if (vlist) {  // the lazy map of a multi-block scene: the stitched march over a brick's list
+      if (occ) return cudaErrorInvalidValue;
+      e = persistent_grid(k_light_march<QuadT, true, false, false, false, true>, smem, ntiles, grid);
+      if (e != cudaSuccess) return e;
+      k_light_march<QuadT, true, false, false, false, true><<<grid, kThreads, smem, st>>>(
+          g, (const QuadT*)quads, tab, tf, tau, map, nvert, cnt, refs, nrefs, self, gate, nullptr, vlist);
+      return cudaGetLastError();
+    }
   } else {
     if (vlist) return cudaErrorInvalidValue;
   }

@@ -43,12 +43,24 @@ struct Brick {
   float* d_map_final = nullptr;
   size_t final_cap = 0;
   size_t map_count = 0;
+  // the lazy map (beams_set_lazy_shadow_map): the cells this brick's view rays
+  // read and their corner vertices; the stitched map is then partial
+  unsigned char* d_cell_mask = nullptr;
+  size_t cell_mask_cap = 0;
+  unsigned* d_vlist = nullptr;
+  size_t vlist_cap = 0;
+  bool final_partial = false;
   void release() {
     if (d_field_owned) cudaFree(d_field_owned);
     if (d_quads) cudaFree(d_quads);
     if (d_tab) cudaFree(d_tab);
     if (d_map_local) cudaFree(d_map_local);
     if (d_map_final) cudaFree(d_map_final);
+    if (d_cell_mask) cudaFree(d_cell_mask);
+    if (d_vlist) cudaFree(d_vlist);
+    d_cell_mask = nullptr;
+    d_vlist = nullptr;
+    cell_mask_cap = vlist_cap = 0;
     d_field_owned = d_quads = nullptr;
     d_quads = nullptr;
     d_tab = nullptr;
@@ -173,6 +185,7 @@ struct beams_renderer {
   static constexpr int kBrickLanes = 4;
   cudaStream_t brick_lane[kBrickLanes] = {nullptr, nullptr, nullptr, nullptr};
   unsigned char* d_shell_mask = nullptr;  // Phase 1's outer-cell-layer mask
+  bool shell_listed = false;              // this frame's Phase 1 ran over the shell's list (d_vlist)
   size_t shell_cap = 0;
   int shell_pd[3] = {0, 0, 0};
   cudaEvent_t brick_fork = nullptr;

@@ -87,3 +87,35 @@ def test_repeated_brick_frames_are_identical(cuda_device):
     img5, t5 = r.render(five[0].camera())
     orgba, _, _, _, olit = render_bricks(five)
     assert np.abs(img5 - orgba).max() <= TOL and t5["lit_samples"] == olit
+
+
+@pytest.mark.parametrize("splits,fov", [((2, 2, 2), 30.0), ((3, 1, 2), 30.0), ((2, 2, 2), 8.0)])
+def test_lazy_map_bricks_give_the_full_maps_image(cuda_device, splits, fov):
+    """beams_set_lazy_shadow_map in a multi-block scene: each brick's view rays
+    mark the cells of its stitched map they read and only their corners are
+    stitched; a brick no pixel reaches stitches nothing. The lazy frame follows
+    a frame under another light, so a vertex skipped but read would show."""
+    s = scenes.small(35, n=41, image=80, m=12, kind="noise", light_kind=0)
+    s.fov_y_deg = fov
+    bricks = scenes.split_bricks(s, splits)
+    for b in bricks:
+        b.fov_y_deg = fov
+    cam = bricks[0].camera()
+    r, img, t = gpu_bricks(bricks)
+    r.clear_lights()
+    r.add_directional_light((0.3, 0.9, -0.3), (1.0, 0.2, 0.2), 1.0)
+    r.render(cam)
+    bricks[0].configure(r)
+    r.set_lazy_shadow_map(True)
+    lazy, tl = r.render(cam)
+    assert np.array_equal(lazy, img), f"lazy brick frame differs by {np.max(np.abs(lazy - img))}"
+    assert tl["lit_samples"] == t["lit_samples"]
+    assert 0 < tl["map_vertices"] < t["map_vertices"]
+    nv = (bricks[0].map_m + 1) ** 3
+    with pytest.raises(B.BeamsError):
+        r.get_brick_map(0, 1, nv)  # the stitched map is partial
+    r.set_lazy_shadow_map(False)
+    again, _ = r.render(cam)
+    assert np.array_equal(again, img)
+    assert r.get_brick_map(0, 1, nv).size == nv
+    print(f"{splits} fov {fov}: {tl['map_vertices']} vertices built, full stitched maps {t['map_vertices']}")

@@ -497,13 +497,37 @@ def run_ours(args):
                                           "map_vertices_built": rec["map_vertices_built"],
                                           "lit_samples": rec["lit_samples"],
                                           "image_equals_full_map": bool(np.array_equal(rec["lazy"], rec["full"]))}
+        # a light orbit around the fixed camera (the reference driver's loop): the
+        # point light steps around the vertical axis every frame; with the marks
+        # kept (mode 2) only the listed vertices are built again
+        lpos0 = np.asarray(s.light, np.float64) - 0.5
+        orbit = {}
+        step = [0]
+
+        def orbit_frame():
+            a = 2.0 * np.pi * (step[0] % 24) / 24.0
+            step[0] += 1
+            c, sn = np.cos(a), np.sin(a)
+            lp = (0.5 + c * lpos0[0] + sn * lpos0[2], 0.5 + lpos0[1], 0.5 - sn * lpos0[0] + c * lpos0[2])
+            r.clear_lights()
+            r.add_point_light(tuple(float(v) for v in lp), s.light_color, s.light_intensity)
+            r.render(cam, out=out, timings=False)
+
+        for mode, name in ((0, "full_map"), (2, "lazy_kept_marks")):
+            if mode:
+                r.set_lazy_shadow_map(True, keep_marks=True)
+            oms, _ = time_frames(orbit_frame, 24, 3, stream, world, local)
+            orbit[name + "_ms_per_frame"] = oms / 24
+            r.set_lazy_shadow_map(False)
+        orbit["frames"] = "24 light positions around the vertical axis, 15 degrees apart, camera fixed"
+        s.configure(r)
         r.set_lazy_shadow_map(False)
         lazy = {"ms_per_frame": lms / args.steps, "value": replica_value(world, args.steps, lit_frame, lms),
                 "unit": UNIT, "map_build_ms": tl["map_build_ms"], "view_march_ms": tl["view_march_ms"],
                 "map_vertices_built": tl["map_vertices"], "map_vertices": nvert,
                 "lit_samples_equal": tl["lit_samples"] == lit_frame, "image_equals_full_map": same,
                 "speedup_vs_full_map": (max_ms / args.steps) / (lms / args.steps), "clocks": lclk,
-                "other_views": views,
+                "other_views": views, "light_orbit": orbit,
                 "note": "a view march without shading marks the map cells the rays read, the light march builds "
                         "the marked cells' corners, then the view march; map_build_ms covers the marking"}
 

@@ -169,8 +169,14 @@ beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable);
  * scene each brick's view rays mark the cells of its stitched map (Phases 2-3)
  * and only their corners are stitched (beams_get_brick_map's stitched stage
  * then returns BEAMS_ERR_STATE; Phase 1 is unchanged). Off by default; the
- * precision and learned forms ignore it. */
-beams_status beams_set_lazy_shadow_map(beams_renderer* r, int enable);
+ * precision and learned forms ignore it.
+ * mode: 0 off, 1 on (the cells are marked every frame), 2 on and the marks are
+ * kept while everything they depend on is unchanged: volume, colour map,
+ * canvas depth, camera, sample distance, termination alpha, slab mode and map
+ * size (not the light: a light orbit around a fixed camera marks once). Other
+ * values return BEAMS_ERR_INVALID_ARG. Mode 2 applies to single volumes; a
+ * multi-block scene marks every frame. */
+beams_status beams_set_lazy_shadow_map(beams_renderer* r, int mode);
 /* ---- legacy VTK files ---------------------------------------------------------
  * Replaces the reference's dataset read (pilot/io/DataSetUtils.cxx:13-42, VTK-m's
  * legacy reader) for structured volumes: DATASET STRUCTURED_POINTS or

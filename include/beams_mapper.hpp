@@ -157,8 +157,11 @@ class MapperLightedVolume {
     check(beams_set_depth_buffer(r_, depth.data(), width, height, BEAMS_DEPTH_WINDOW, near_plane, far_plane, 0), r_);
   }
   void SetDensityScale(float s) { check(beams_set_density_scale(r_, s), r_); }  // stored, never read (as in the reference)
-  // Extension: build only the map vertices the frame's view rays read (same image).
-  void SetLazyShadowMap(bool on) { check(beams_set_lazy_shadow_map(r_, on ? 1 : 0), r_); }
+  // Extension: build only the map vertices the frame's view rays read (same
+  // image); keep_marks keeps the marked cells while the view is unchanged.
+  void SetLazyShadowMap(bool on, bool keep_marks = false) {
+    check(beams_set_lazy_shadow_map(r_, on ? (keep_marks ? 2 : 1) : 0), r_);
+  }
   // SetProfiler (MapperLightedVolume.cxx:305-309): every RenderCells adds its frames to p.
   void SetProfiler(std::shared_ptr<Profiler> p) {
     check(beams_set_profiler(r_, p ? &MapperLightedVolume::record : nullptr, p.get()), r_);

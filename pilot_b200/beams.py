@@ -545,9 +545,10 @@ class Renderer:
     def set_reuse_shadow_map(self, on: bool):
         self._check(self._L.beams_set_reuse_shadow_map(self._h, int(bool(on))))
 
-    def set_lazy_shadow_map(self, on: bool):
-        """Build only the map vertices the frame's view rays read (exact form)."""
-        self._check(self._L.beams_set_lazy_shadow_map(self._h, int(bool(on))))
+    def set_lazy_shadow_map(self, on: bool, keep_marks: bool = False):
+        """Build only the map vertices the frame's view rays read (exact form);
+        keep_marks keeps the marked cells while the view's inputs are unchanged."""
+        self._check(self._L.beams_set_lazy_shadow_map(self._h, (2 if keep_marks else 1) if on else 0))
 
     def set_background(self, on: bool, rgba=(1, 1, 1, 1)):
         c = (C.c_float * 4)(*rgba)

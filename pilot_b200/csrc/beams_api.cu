@@ -435,6 +435,35 @@ beams_status build_map(beams_renderer* r, const ExactGeo& g, int& launches, bool
 // the frame reads, and the light march builds only the vertices of marked
 // cells: the image equals the full map's bit for bit. The map itself is
 // partial, so it is neither kept for reuse nor readable.
+static void mark_key(const beams_renderer* r, const ExactGeo& g, MarkKey& k) {
+  std::memset(&k, 0, sizeof(k));
+  k.volume_version = r->volume_version;
+  k.tf_version = r->tf_version;
+  k.depth_version = r->depth_set ? r->depth_version : 0;
+  for (int d = 0; d < 3; ++d) {
+    k.cam[d] = g.cam_pos[d];
+    k.cam[3 + d] = g.cf[d];
+    k.cam[6 + d] = g.cr[d];
+    k.cam[9 + d] = g.cu[d];
+    k.morig[d] = g.morig[d];
+    k.minv[d] = g.minv[d];
+    k.pd[d] = g.pd[d];
+  }
+  k.k[0] = g.kx;
+  k.k[1] = g.cx;
+  k.k[2] = g.ky;
+  k.k[3] = g.cy;
+  k.sd = g.sd;
+  k.mesh_eps = g.mesh_eps;
+  k.cutoff = g.cutoff;
+  k.min_scalar = g.min_scalar;
+  k.inv_delta = g.inv_delta;
+  k.size[0] = g.width;
+  k.size[1] = g.height;
+  for (int i = 0; i < 4; ++i) k.win[i] = g.win[i];
+  k.slab_fp64 = g.slab_fp64;
+}
+
 static beams_status build_map_lazy(beams_renderer* r, const ExactGeo& g, int& launches) {
   const size_t nvert = (size_t)g.pd[0] * g.pd[1] * g.pd[2];
   const int nl = g.n_lights > 1 ? g.n_lights : 1;
@@ -455,12 +484,24 @@ static beams_status build_map_lazy(beams_renderer* r, const ExactGeo& g, int& la
                     "allocating the map vertex list");
   if (s != BEAMS_OK) return s;
   const float4* quads = (const float4*)r->d_quads;
-  cudaError_t e = cudaMemsetAsync(r->d_cell_mask, 0, ncell, r->stream);
-  if (e == cudaSuccess)
-    e = launch_mark_view_cells(g, quads, r->d_tab, r->d_tf, r->d_cell_mask, r->d_cnt, nullptr, nullptr, r->stream);
-  if (e == cudaSuccess) e = launch_list_marked_vertices(g, r->d_cell_mask, nullptr, r->d_vlist, r->stream);
-  if (e != cudaSuccess) return cuda_fail(r, e, "map cell marking launch");
-  launches += 2;
+  // mode 2 keeps the marks while the view's inputs are unchanged (a light
+  // orbit around a fixed camera re-marks nothing)
+  MarkKey key;
+  mark_key(r, g, key);
+  cudaError_t e = cudaSuccess;
+  if (!(r->keep_marks && r->marks_valid && std::memcmp(&key, &r->mark_key, sizeof(key)) == 0)) {
+    r->marks_valid = false;
+    e = cudaMemsetAsync(r->d_cell_mask, 0, ncell, r->stream);
+    if (e == cudaSuccess)
+      e = launch_mark_view_cells(g, quads, r->d_tab, r->d_tf, r->d_cell_mask, r->d_cnt, nullptr, nullptr, r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "map cell marking launch");
+    ++launches;
+    r->mark_key = key;
+    r->marks_valid = r->keep_marks;
+  }
+  e = launch_list_marked_vertices(g, r->d_cell_mask, nullptr, r->d_vlist, r->stream);
+  if (e != cudaSuccess) return cuda_fail(r, e, "map vertex listing launch");
+  ++launches;
   for (int l = 0; l < nl; ++l) {
     ExactGeo gl = g;
     if (l > 0) geo_set_light(gl, r->lights[l]);
@@ -1123,9 +1164,11 @@ beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable) {
   return BEAMS_OK;
 }
 
-beams_status beams_set_lazy_shadow_map(beams_renderer* r, int enable) {
+beams_status beams_set_lazy_shadow_map(beams_renderer* r, int mode) {
   if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
-  r->lazy_map = enable != 0;
+  if (mode < 0 || mode > 2) return fail(r, BEAMS_ERR_INVALID_ARG, "lazy shadow map mode must be 0, 1 or 2");
+  r->lazy_map = mode != 0;
+  r->keep_marks = mode == 2;  // kept marks stay valid only while their key matches
   return BEAMS_OK;
 }
 

@@ -132,6 +132,7 @@ using namespace beams;
 extern "C" beams_status beams_set_depth_buffer(beams_renderer* r, const float* depth, int width, int height,
                                                int kind, double near_plane, double far_plane, int on_device) {
   if (!r) return fail(nullptr, BEAMS_ERR_INVALID_ARG, "renderer is NULL");
+  ++r->depth_version;  // every call may change the ray limits
   if (!depth) {
     r->depth_set = false;
     return BEAMS_OK;

@@ -68,6 +68,15 @@ struct Brick {
   }
 };
 
+// What the lazy map's cell marks depend on: the view rays and their samples
+// (volume, colour map, canvas depth, camera, window, sample distance,
+// termination, slab mode, value range) and the map grid; not the light.
+struct MarkKey {
+  unsigned long long volume_version, tf_version, depth_version;
+  float cam[12], k[4], sd, mesh_eps, cutoff, min_scalar, inv_delta, morig[3], minv[3];
+  int size[2], win[4], slab_fp64, pd[3];
+};
+
 struct MapKey {
   unsigned long long volume_version;
   unsigned long long tf_version;
@@ -119,6 +128,9 @@ struct beams_renderer {
   // beams_set_lazy_shadow_map: the exact form builds only the map vertices
   // that the frame's view rays read (d_cell_mask marks their cells)
   bool lazy_map = false;
+  bool keep_marks = false;    // mode 2: marks kept while mark_key matches
+  bool marks_valid = false;
+  beams::MarkKey mark_key{};
   unsigned char* d_cell_mask = nullptr;
   size_t cell_mask_cap = 0;
   // the masked map builds' vertex list ((M+1)^3 + 1 entries: count, then ids),
@@ -132,6 +144,7 @@ struct beams_renderer {
   std::vector<float> coords[3];
   // canvas depth buffer (beams_set_depth_buffer) and the per-pixel ray limits derived from it
   bool depth_set = false;
+  unsigned long long depth_version = 0;  // bumped by every beams_set_depth_buffer
   int depth_w = 0, depth_h = 0, depth_kind = 0;
   double depth_near = 0.0, depth_far = 0.0;
   float* d_depth = nullptr;

@@ -206,3 +206,69 @@ def test_lazy_map_ignored_by_the_precision_form(cuda_device):
     assert np.array_equal(a, b)
     assert tb["map_vertices"] == ta["map_vertices"] == (s.map_m + 1) ** 3
     assert r.get_shadow_map((s.map_m + 1) ** 3).size == (s.map_m + 1) ** 3
+
+
+def test_kept_marks_follow_every_view_input(cuda_device):
+    """Mode 2 keeps the marked cells across frames while the view's inputs are
+    unchanged: a moving light re-marks nothing (one launch fewer) and matches
+    the full map; a change of camera, colour map, canvas depth, sample distance,
+    termination alpha or volume marks again."""
+    s = scenes.small(9, n=40, image=96, m=20, kind="noise", light_kind=1)
+    s.fov_y_deg = 14.0
+    r = renderer(s)
+    q = renderer(s)  # full maps, same settings
+    for x in (r, q):  # fixed launch choices; layouts built before counting launches
+        x.set_tuning(light_brick=8, empty_skip=False, view_skip=False)
+        x.render(s.camera())
+
+    def both(cam):
+        r.set_lazy_shadow_map(True, keep_marks=True)
+        a, ta = r.render(cam)
+        b, tb = q.render(cam)
+        assert np.array_equal(a, b), f"kept-mark frame differs by {np.max(np.abs(a - b))}"
+        assert ta["lit_samples"] == tb["lit_samples"]
+        return ta
+
+    cam = s.camera()
+    t0 = both(cam)
+    t1 = both(cam)
+    assert t1["kernel_launches"] == t0["kernel_launches"] - 1  # marks kept
+    for i, d in enumerate([(0.2, 0.9, 0.3), (-0.7, 0.1, 0.7), (0.5, -0.5, -0.7)]):  # a light orbit
+        for x in (r, q):
+            x.clear_lights()
+            x.add_directional_light(d, (1.0, 0.9, 0.8), 1.2)
+        t = both(cam)
+        assert t["kernel_launches"] == t1["kernel_launches"]
+    # each view input marks again
+    s2 = scenes.small(9, n=40, image=96, m=20, kind="noise", light_kind=1)
+    s2.fov_y_deg = 9.0
+    t = both(s2.camera())
+    assert t["kernel_launches"] == t0["kernel_launches"]
+    t = both(cam)
+    assert t["kernel_launches"] == t0["kernel_launches"]
+    tf = np.array(s.tf, np.float32).copy()
+    tf[:, 3] = np.clip(tf[:, 3] * 1.7, 0, 1)
+    for x in (r, q):
+        x.set_color_map(tf)
+    assert both(cam)["kernel_launches"] == t0["kernel_launches"]
+    for x in (r, q):
+        x.set_sample_distance(0.7 / 39)
+    assert both(cam)["kernel_launches"] == t0["kernel_launches"]
+    for x in (r, q):
+        x.set_termination_alpha(0.9)
+    assert both(cam)["kernel_launches"] == t0["kernel_launches"]
+    c = float(np.linalg.norm(np.asarray(s.cam_pos) - 0.5))
+    lim = np.random.default_rng(9).uniform(c - 0.5, c + 0.3, (s.height, s.width)).astype(np.float32)
+    for x in (r, q):
+        x.set_depth_buffer(lim, B.DEPTH_RAY_DISTANCE)
+    t = both(cam)
+    assert t["kernel_launches"] == t0["kernel_launches"] + 1  # the ray-limit kernel
+    assert both(cam)["kernel_launches"] == t0["kernel_launches"]  # kept again (limits still computed)
+    f2 = s.field_numpy() * np.float32(0.8)
+    for x in (r, q):
+        x.set_depth_buffer(None)
+        x.set_volume(f2, origin=s.origin, spacing=s.spacing, value_range=s.value_range)
+    t = both(cam)
+    assert t["kernel_launches"] > t0["kernel_launches"] - 1
+    with pytest.raises(B.BeamsError):
+        r._check(r._L.beams_set_lazy_shadow_map(r._h, 3))

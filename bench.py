@@ -513,9 +513,8 @@ def run_ours(args):
             r.add_point_light(tuple(float(v) for v in lp), s.light_color, s.light_intensity)
             r.render(cam, out=out, timings=False)
 
-        for mode, name in ((0, "full_map"), (2, "lazy_kept_marks")):
-            if mode:
-                r.set_lazy_shadow_map(True, keep_marks=True)
+        for mode, name in ((0, "full_map"), (1, "lazy"), (2, "lazy_kept_marks")):
+            r.set_lazy_shadow_map(mode != 0, keep_marks=mode == 2)
             oms, _ = time_frames(orbit_frame, 24, 3, stream, world, local)
             orbit[name + "_ms_per_frame"] = oms / 24
             r.set_lazy_shadow_map(False)

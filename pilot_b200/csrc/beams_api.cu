@@ -1307,8 +1307,9 @@ beams_status beams_autotune(beams_renderer* r, const beams_camera* cam, beams_tu
   if (cam) {
     // the view march with and without its skip, on the map just chosen
     const int keep_view = r->view_skip;
-    const bool keep_reuse2 = r->reuse_map;
+    const bool keep_reuse2 = r->reuse_map, keep_lazy = r->lazy_map;
     r->reuse_map = true;  // the first render of each choice builds the map; the timed ones reuse it
+    r->lazy_map = false;  // (a lazy frame would mark and build again)
     float tv[2] = {3.4e38f, 3.4e38f};
     float4* img = nullptr;
     s = validate_camera(r, cam);
@@ -1336,6 +1337,7 @@ beams_status beams_autotune(beams_renderer* r, const beams_camera* cam, beams_tu
       }
     }
     r->reuse_map = keep_reuse2;
+    r->lazy_map = keep_lazy;
     if (s != BEAMS_OK) {
       r->view_skip = keep_view;
       return s;

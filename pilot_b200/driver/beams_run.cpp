@@ -95,12 +95,19 @@ bool arg(const char* a, const char* name, std::string& out) {
 
 int main(int argc, char** argv) {
   std::string base, config, out, frames_s, dev_s;
+  bool lazy = false;
   for (int i = 1; i < argc; ++i) {
     std::string preset;
+    if (std::strcmp(argv[i], "--lazy-shadow-map") == 0) {
+      lazy = true;  // build only the map vertices the view reads, marking once for the fixed camera
+      continue;
+    }
     if (!arg(argv[i], "--base-dir", base) && !arg(argv[i], "--config", config) && !arg(argv[i], "--out", out) &&
         !arg(argv[i], "--frames", frames_s) && !arg(argv[i], "--device", dev_s) &&
         !arg(argv[i], "--preset", preset)) {
-      std::fprintf(stderr, "usage: %s --base-dir=<dir> | --config=<file.toml> [--frames=N] [--out=<dir>] [--device=D]\n",
+      std::fprintf(stderr,
+                   "usage: %s --base-dir=<dir> | --config=<file.toml> [--frames=N] [--out=<dir>] [--device=D] "
+                   "[--lazy-shadow-map]\n",
                    argv[0]);
       return 2;
     }
@@ -129,6 +136,11 @@ int main(int argc, char** argv) {
   beams_camera cam;
   if (beams_apply_scene(r, &d, &cam) != BEAMS_OK) {
     std::fprintf(stderr, "beams_run: scene: %s\n", beams_last_error(r));
+    beams_destroy(r);
+    return 1;
+  }
+  if (lazy && beams_set_lazy_shadow_map(r, 2) != BEAMS_OK) {
+    std::fprintf(stderr, "beams_run: %s\n", beams_last_error(r));
     beams_destroy(r);
     return 1;
   }

@@ -144,6 +144,18 @@ def test_driver_runs_the_light_orbit(cuda_device, tmp_path):
     assert [x["frame"] for x in lines] == [0, 1, 2] and all(x["lit_samples"] > 0 for x in lines)
     for k in range(3):
         assert _read_png(tmp_path / f"spheres_0_{k:03d}.png") == (64, 56)
+    # the lazy map with kept marks (the camera is fixed, the light orbits): the
+    # same images byte for byte
+    lazy_dir = tmp_path / "lazy"
+    lazy_dir.mkdir()
+    p = subprocess.run([str(exe), f"--base-dir={tmp_path}", "--frames=3", f"--out={lazy_dir}", "--lazy-shadow-map"],
+                       capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    lazy_lines = [json.loads(x) for x in p.stdout.strip().splitlines()]
+    assert [x["lit_samples"] for x in lazy_lines] == [x["lit_samples"] for x in lines]
+    for k in range(3):
+        name = f"spheres_0_{k:03d}.png"
+        assert (lazy_dir / name).read_bytes() == (tmp_path / name).read_bytes(), name
 
 
 def test_vtk_file_scene_renders_like_the_oracle(cuda_device, tmp_path):

@@ -497,7 +497,7 @@ def run_ours(args):
                                           "map_vertices_built": rec["map_vertices_built"],
                                           "lit_samples": rec["lit_samples"],
                                           "image_equals_full_map": bool(np.array_equal(rec["lazy"], rec["full"]))}
-        # a light orbit around the fixed camera (the reference driver's loop): the
+        # a light orbit around the fixed camera (the loop of the reference's Beams::Run): the
         # point light steps around the vertical axis every frame; with the marks
         # kept (mode 2) only the listed vertices are built again
         lpos0 = np.asarray(s.light, np.float64) - 0.5

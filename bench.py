@@ -780,6 +780,16 @@ def run_form(args, nested=False):
     exact_ms, _ = time_frames(lambda: r.render(cam, out=out, timings=False), max(3, args.steps // 4), 2, stream,
                               world, local)
     exact_ms /= max(3, args.steps // 4)
+    # the exact form with the lazy map (only the vertices the view reads)
+    r.set_lazy_shadow_map(True)
+    _, tlz = r.render(cam, out=out, timings=True)
+    lazy_same = bool(np.array_equal(out.cpu().numpy(), exact_img))
+    exact_lazy_ms, _ = time_frames(lambda: r.render(cam, out=out, timings=False), max(3, args.steps // 4), 2,
+                                   stream, world, local)
+    exact_lazy_ms /= max(3, args.steps // 4)
+    r.set_lazy_shadow_map(False)
+    exact_lazy = {"ms_per_frame": exact_lazy_ms, "map_vertices_built": tlz["map_vertices"],
+                  "image_equals_full_map": lazy_same}
     extra, roofline = {}, None
     if args.form == "precision":
         dt = B.F16 if args.field_dtype == "f16" else B.BF16
@@ -801,6 +811,7 @@ def run_form(args, nested=False):
         dtype = args.field_dtype
         extra["precision"] = {"field_dtype": dtype, "exact_f32_ms_per_frame": exact_ms, "exact_tuning": exact_tuning,
                               "speedup_vs_exact_f32": exact_ms / (total_ms / args.steps),
+                              "exact_f32_lazy_map": exact_lazy,
                               "psnr_vs_exact_f32_full_frame": psnr(img, exact_img)}
         if not args.no_quality and rank == 0:
             extra["precision"]["vs_fp64"] = fp64_crops(s, fd.cpu().numpy(), {"precision": img, "exact_f32": exact_img},

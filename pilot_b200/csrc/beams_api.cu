@@ -68,6 +68,15 @@ beams_status ensure_buffer(beams_renderer* r, void** buf, size_t* cap, size_t by
   return BEAMS_OK;
 }
 
+beams_status ensure_masked_map(beams_renderer* r, float** buf, size_t* cap, size_t bytes, cudaStream_t st) {
+  const bool fresh = !(*buf && *cap >= bytes);
+  beams_status s = ensure_buffer(r, (void**)buf, cap, bytes, "allocating map");
+  if (s != BEAMS_OK || !fresh) return s;
+  cudaError_t e = cudaMemsetAsync(*buf, 0, bytes, st);
+  if (e != cudaSuccess) return cuda_fail(r, e, "clearing map");
+  return BEAMS_OK;
+}
+
 static bool finite3(const double* v) {
   return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]);
 }
@@ -467,18 +476,20 @@ static void mark_key(const beams_renderer* r, const ExactGeo& g, MarkKey& k) {
 static beams_status build_map_lazy(beams_renderer* r, const ExactGeo& g, int& launches) {
   const size_t nvert = (size_t)g.pd[0] * g.pd[1] * g.pd[2];
   const int nl = g.n_lights > 1 ? g.n_lights : 1;
-  beams_status s = ensure_buffer(r, (void**)&r->d_map, &r->map_cap, nl * nvert * sizeof(float), "allocating map");
+  beams_status s = ensure_masked_map(r, &r->d_map, &r->map_cap, nl * nvert * sizeof(float), r->stream);
   if (s != BEAMS_OK) return s;
   r->map_valid = false;
   r->map_is_half = false;
   const size_t ncell = (size_t)(g.pd[0] - 1) * (g.pd[1] - 1) * (g.pd[2] - 1);
   s = ensure_buffer(r, (void**)&r->d_cell_mask, &r->cell_mask_cap, ncell, "allocating the map cell mask");
   if (s != BEAMS_OK) return s;
-  const unsigned char* occ = nullptr;
-  if (r->empty_skip && !g.rect) {
+  const unsigned char* occ = nullptr;       // the light march's empty-space skip
+  const unsigned char* view_occ = nullptr;  // the marking pass skips as the view march does
+  if ((r->empty_skip || r->view_skip) && !g.rect) {
     s = prepare_occupancy(r, g, launches);
     if (s != BEAMS_OK) return s;
-    occ = r->d_occ;
+    occ = r->empty_skip ? r->d_occ : nullptr;
+    view_occ = r->view_skip ? r->d_occ : nullptr;
   }
   s = ensure_buffer(r, (void**)&r->d_vlist, &r->vlist_cap, marked_list_bytes(g.pd),
                     "allocating the map vertex list");
@@ -493,7 +504,8 @@ static beams_status build_map_lazy(beams_renderer* r, const ExactGeo& g, int& la
     r->marks_valid = false;
     e = cudaMemsetAsync(r->d_cell_mask, 0, ncell, r->stream);
     if (e == cudaSuccess)
-      e = launch_mark_view_cells(g, quads, r->d_tab, r->d_tf, r->d_cell_mask, r->d_cnt, nullptr, nullptr, r->stream);
+      e = launch_mark_view_cells(g, quads, r->d_tab, r->d_tf, r->d_cell_mask, r->d_cnt, nullptr, nullptr, r->stream,
+                                 view_occ);
     if (e != cudaSuccess) return cuda_fail(r, e, "map cell marking launch");
     ++launches;
     r->mark_key = key;
@@ -664,7 +676,7 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
       Brick& B = r->bricks[b];
       const size_t nv = (size_t)G[b].pd[0] * G[b].pd[1] * G[b].pd[2];
       s = ensure_buffer(r, (void**)&B.d_map_local, &B.local_cap, nv * sizeof(float), "allocating brick map");
-      if (s == BEAMS_OK) s = ensure_buffer(r, (void**)&B.d_map_final, &B.final_cap, nv * sizeof(float), "allocating brick map");
+      if (s == BEAMS_OK) s = ensure_masked_map(r, &B.d_map_final, &B.final_cap, nv * sizeof(float), r->stream);
       if (s != BEAMS_OK) return s;
       B.map_count = nv;
       BrickRef& R = refs[b];

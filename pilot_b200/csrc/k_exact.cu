@@ -314,14 +314,15 @@ __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const
 // K2's warp tiles in K2's order over the window, or (LIST) over the listed
 // kFallbackTile^2 tiles while *fcount > 0; tile counter cnt->tiles_mark. The
 // march reads no map, so only the field axes' cell tables are staged.
-template <bool RECT, bool LIST>
+template <bool RECT, bool LIST, bool SKIP = false>
 __global__ void __launch_bounds__(kThreads) k_mark_view_cells(const ExactGeo g, const float4* __restrict__ quads,
                                                               const float4* __restrict__ tab,
                                                               const float4* __restrict__ tf,
                                                               unsigned char* __restrict__ mask,
                                                               Counters* __restrict__ cnt,
                                                               const unsigned* __restrict__ flist,
-                                                              const unsigned* __restrict__ fcount) {
+                                                              const unsigned* __restrict__ fcount,
+                                                              const unsigned char* __restrict__ occ) {
   if (LIST && *fcount == 0u) return;
   extern __shared__ float4 s_dyn[];
   const int nfield = g.max_off[0];
@@ -349,8 +350,8 @@ __global__ void __launch_bounds__(kThreads) k_mark_view_cells(const ExactGeo g, 
                    {g.pd[0], g.pd[1], g.pd[2]}, mask, 0xffffffffu};
       float4 color;
       unsigned lit = 0, hit = 0;
-      view_march_pixel<float4, false, float, CellMarker, false, false, RECT>(g, quads, s_tab, s_tf, nullptr, x, y,
-                                                                             color, lit, hit, &m);
+      view_march_pixel<float4, false, float, CellMarker, SKIP, false, RECT>(g, quads, s_tab, s_tf, nullptr, x, y,
+                                                                            color, lit, hit, &m, occ);
     }
   }
 }
@@ -642,25 +643,28 @@ static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4*
   return cudaGetLastError();
 }
 
-template <bool RECT, bool LIST>
+template <bool RECT, bool LIST, bool SKIP = false>
 static cudaError_t launch_mark(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                unsigned char* cell_mask, Counters* cnt, const unsigned* flist,
-                               const unsigned* fcount, cudaStream_t st) {
+                               const unsigned* fcount, cudaStream_t st, const unsigned char* occ = nullptr) {
   const size_t smem = ((size_t)g.max_off[0] + (size_t)g.tf_n) * sizeof(float4);
   const int ntiles = ((g.win[2] + 7) >> 3) * ((g.win[3] + 3) >> 2);
   int grid = 0;
-  cudaError_t e = persistent_grid(k_mark_view_cells<RECT, LIST>, smem, ntiles, grid);
+  cudaError_t e = persistent_grid(k_mark_view_cells<RECT, LIST, SKIP>, smem, ntiles, grid);
   if (e != cudaSuccess) return e;
-  k_mark_view_cells<RECT, LIST><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, cell_mask, cnt, flist, fcount);
+  k_mark_view_cells<RECT, LIST, SKIP><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, cell_mask, cnt, flist, fcount,
+                                                                     occ);
   return cudaGetLastError();
 }
 
 cudaError_t launch_mark_view_cells(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    unsigned char* cell_mask, Counters* cnt, const unsigned* flist,
-                                   const unsigned* fcount, cudaStream_t st) {
+                                   const unsigned* fcount, cudaStream_t st, const unsigned char* occ) {
   if (flist && !fcount) return cudaErrorInvalidValue;
   cudaError_t e = cudaMemsetAsync(&cnt->tiles_mark, 0, sizeof(unsigned), st);
   if (e != cudaSuccess) return e;
+  if (occ && !g.rect && !flist)  // samples in empty macro-cells have alpha 0 and mark nothing
+    return launch_mark<false, false, true>(g, quads, tab, tf, cell_mask, cnt, nullptr, nullptr, st, occ);
   if (g.rect)
     return flist ? launch_mark<true, true>(g, quads, tab, tf, cell_mask, cnt, flist, fcount, st)
                  : launch_mark<true, false>(g, quads, tab, tf, cell_mask, cnt, nullptr, nullptr, st);

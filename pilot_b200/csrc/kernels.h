@@ -42,12 +42,13 @@ cudaError_t launch_mark_fallback_vertices(const ExactGeo& g, const float4* quads
                                           const unsigned* flist, const unsigned* fcount, unsigned char* vmask,
                                           size_t mask_bytes, unsigned* host_count, Counters* cnt, cudaStream_t st);
 // Marks (one byte per map cell, x fastest; the mask is not cleared here) every
-// map cell that the view rays of the frame's window read, or (flist given) of
-// the listed kFallbackTile^2 tiles, *fcount of them (nothing while it is 0).
-// Zeroes and uses cnt->tiles_mark.
+// map cell that the view rays of the frame's window read at samples of alpha
+// above 0, or (flist given) of the listed kFallbackTile^2 tiles, *fcount of
+// them (nothing while it is 0). occ (window only): the march skips empty
+// macro-cells. Zeroes and uses cnt->tiles_mark.
 cudaError_t launch_mark_view_cells(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    unsigned char* cell_mask, Counters* cnt, const unsigned* flist,
-                                   const unsigned* fcount, cudaStream_t st);
+                                   const unsigned* fcount, cudaStream_t st, const unsigned char* occ = nullptr);
 // K2 over a device list of kFallbackTile^2 pixel tiles (count in *fcount), with the map.
 cudaError_t launch_view_march_tiles(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                     const float* map, float4* out, Counters* cnt, const unsigned* flist,

@@ -30,10 +30,12 @@ struct NoRecord {
   __device__ __forceinline__ void operator()(const float*, const float4&, float) {}
 };
 
-// A view-march observer that marks, for every lit sample, the map cell that the
-// shading looks up (the cell of map_interp_t: truncate min(max((p - origin) / spacing,
-// 0), pd - 2) per axis), one byte per cell, skipping repeats of the previous
-// sample's cell. A masked map build then lists every vertex with a marked cell
+// A view-march observer that marks, for every lit sample of premultiplied
+// alpha above 0, the map cell that the shading looks up (the cell of
+// map_interp_t: truncate min(max((p - origin) / spacing, 0), pd - 2) per axis),
+// one byte per cell, skipping repeats of the previous sample's cell. A sample
+// of alpha 0 adds exactly 0 times its shading, so the map value it reads only
+// has to be finite (the masked builds zero a newly allocated map). A masked map build then lists every vertex with a marked cell
 // around it (the same vertex set as marking the 8 corners, with one store per
 // cell).
 struct CellMarker {
@@ -41,7 +43,8 @@ struct CellMarker {
   int pd[3];
   unsigned char* mask;
   unsigned last;
-  __device__ __forceinline__ void operator()(const float* p, const float4&, float) {
+  __device__ __forceinline__ void operator()(const float* p, const float4&, float sa) {
+    if (!(sa > 0.f)) return;
     int c[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {

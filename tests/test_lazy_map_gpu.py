@@ -272,3 +272,26 @@ def test_kept_marks_follow_every_view_input(cuda_device):
     assert t["kernel_launches"] > t0["kernel_launches"] - 1
     with pytest.raises(B.BeamsError):
         r._check(r._L.beams_set_lazy_shadow_map(r._h, 3))
+
+
+@pytest.mark.parametrize("skip", [True, False])
+def test_lazy_first_frame_with_transparent_colour_map_range(cuda_device, skip):
+    """Samples of alpha 0 mark no cell (they add exactly 0 whatever finite map
+    value they read; a masked build's new map buffer is zeroed): a colour map
+    transparent below 0.45 leaves many samples unmarked. The lazy frame is the
+    renderer's first, so an unbuilt vertex holds only what the allocation left,
+    and it must equal a full-map render from another renderer."""
+    s = scenes.small(10, n=48, image=96, m=24, kind="blobs", light_kind=0)
+    tf = np.array(s.tf, np.float32).copy()
+    tf[: int(0.45 * len(tf)), 3] = 0.0
+    s.tf = tf
+    lazy_r, full_r = renderer(s), renderer(s)
+    for x in (lazy_r, full_r):
+        x.set_tuning(light_brick=8, empty_skip=skip, view_skip=skip)
+    lazy_r.set_lazy_shadow_map(True)
+    lazy, tl = lazy_r.render(s.camera())
+    full, tfull = full_r.render(s.camera())
+    assert np.array_equal(lazy, full), f"differs by {np.max(np.abs(lazy - full))}"
+    assert tl["lit_samples"] == tfull["lit_samples"]
+    assert 0 < tl["map_vertices"] < tfull["map_vertices"]
+    assert np.all(np.isfinite(lazy))

@@ -801,6 +801,14 @@ def run_form(args, nested=False):
         launches = tp["kernel_launches"]
         frame = lambda: r.render(cam, out=out, timings=False)  # noqa: E731  map build + view march
         total_ms, clocks = time_frames(frame, args.steps, args.warmup, stream, world, local)
+        # the precision form with the lazy map
+        r.set_lazy_shadow_map(True)
+        _, tpl = r.render(cam, out=out, timings=True)
+        prec_lazy_same = bool(np.array_equal(out.cpu().numpy(), img))
+        prec_lazy_ms, _ = time_frames(frame, max(3, args.steps // 4), 2, stream, world, local)
+        prec_lazy = {"ms_per_frame": prec_lazy_ms / max(3, args.steps // 4), "map_vertices_built": tpl["map_vertices"],
+                     "image_equals_full_map": prec_lazy_same}
+        r.set_lazy_shadow_map(False)
         _, tk = r.render(cam, out=out, timings=True)
         nvert = (s.map_m + 1) ** 3
         kb = tk["light_samples"] * 16 + nvert * 2  # bf16/f16 quads: 8 corners x 2 B; binary16 map
@@ -811,7 +819,7 @@ def run_form(args, nested=False):
         dtype = args.field_dtype
         extra["precision"] = {"field_dtype": dtype, "exact_f32_ms_per_frame": exact_ms, "exact_tuning": exact_tuning,
                               "speedup_vs_exact_f32": exact_ms / (total_ms / args.steps),
-                              "exact_f32_lazy_map": exact_lazy,
+                              "exact_f32_lazy_map": exact_lazy, "lazy_map": prec_lazy,
                               "psnr_vs_exact_f32_full_frame": psnr(img, exact_img)}
         if not args.no_quality and rank == 0:
             extra["precision"]["vs_fp64"] = fp64_crops(s, fd.cpu().numpy(), {"precision": img, "exact_f32": exact_img},

@@ -168,8 +168,9 @@ beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable);
  * beams_timings.map_vertices reports the vertices built. In a multi-block
  * scene each brick's view rays mark the cells of its stitched map (Phases 2-3)
  * and only their corners are stitched (beams_get_brick_map's stitched stage
- * then returns BEAMS_ERR_STATE; Phase 1 is unchanged). Off by default; the
- * precision and learned forms ignore it.
+ * then returns BEAMS_ERR_STATE; Phase 1 is unchanged). The precision form
+ * builds its binary16 map the same way, marking over its 16-bit field. Off by
+ * default; the learned form ignores it (its fallback is lazy already).
  * mode: 0 off, 1 on (the cells are marked every frame), 2 on and the marks are
  * kept while everything they depend on is unchanged: volume, colour map,
  * canvas depth, camera, sample distance, termination alpha, slab mode and map

@@ -68,8 +68,9 @@ beams_status ensure_buffer(beams_renderer* r, void** buf, size_t* cap, size_t by
   return BEAMS_OK;
 }
 
-beams_status ensure_masked_map(beams_renderer* r, float** buf, size_t* cap, size_t bytes, cudaStream_t st) {
-  const bool fresh = !(*buf && *cap >= bytes);
+beams_status ensure_masked_map(beams_renderer* r, float** buf, size_t* cap, size_t bytes, cudaStream_t st,
+                               bool clear) {
+  const bool fresh = clear || !(*buf && *cap >= bytes);
   beams_status s = ensure_buffer(r, (void**)buf, cap, bytes, "allocating map");
   if (s != BEAMS_OK || !fresh) return s;
   cudaError_t e = cudaMemsetAsync(*buf, 0, bytes, st);
@@ -476,10 +477,14 @@ static void mark_key(const beams_renderer* r, const ExactGeo& g, MarkKey& k) {
 static beams_status build_map_lazy(beams_renderer* r, const ExactGeo& g, int& launches) {
   const size_t nvert = (size_t)g.pd[0] * g.pd[1] * g.pd[2];
   const int nl = g.n_lights > 1 ? g.n_lights : 1;
-  beams_status s = ensure_masked_map(r, &r->d_map, &r->map_cap, nl * nvert * sizeof(float), r->stream);
+  const bool prec = r->form == BEAMS_FORM_PRECISION;  // binary16 transmittance
+  // the buffer is cleared when its format changes too: float32 data read as
+  // binary16 can hold NaN or infinity patterns
+  beams_status s = ensure_masked_map(r, &r->d_map, &r->map_cap, nl * nvert * (prec ? 2 : sizeof(float)), r->stream,
+                                     r->map_is_half != prec);
   if (s != BEAMS_OK) return s;
   r->map_valid = false;
-  r->map_is_half = false;
+  r->map_is_half = prec;
   const size_t ncell = (size_t)(g.pd[0] - 1) * (g.pd[1] - 1) * (g.pd[2] - 1);
   s = ensure_buffer(r, (void**)&r->d_cell_mask, &r->cell_mask_cap, ncell, "allocating the map cell mask");
   if (s != BEAMS_OK) return s;
@@ -504,8 +509,10 @@ static beams_status build_map_lazy(beams_renderer* r, const ExactGeo& g, int& la
     r->marks_valid = false;
     e = cudaMemsetAsync(r->d_cell_mask, 0, ncell, r->stream);
     if (e == cudaSuccess)
-      e = launch_mark_view_cells(g, quads, r->d_tab, r->d_tf, r->d_cell_mask, r->d_cnt, nullptr, nullptr, r->stream,
-                                 view_occ);
+      e = prec ? launch_mark_view_cells_prec(g, quad_dtype(r), r->d_quads, r->d_tab, r->d_tf, r->d_cell_mask,
+                                             r->d_cnt, r->stream, view_occ)
+               : launch_mark_view_cells(g, quads, r->d_tab, r->d_tf, r->d_cell_mask, r->d_cnt, nullptr, nullptr,
+                                        r->stream, view_occ);
     if (e != cudaSuccess) return cuda_fail(r, e, "map cell marking launch");
     ++launches;
     r->mark_key = key;
@@ -514,6 +521,13 @@ static beams_status build_map_lazy(beams_renderer* r, const ExactGeo& g, int& la
   e = launch_list_marked_vertices(g, r->d_cell_mask, nullptr, r->d_vlist, r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "map vertex listing launch");
   ++launches;
+  if (prec) {
+    e = launch_light_march_prec(g, quad_dtype(r), r->d_quads, r->d_tab, r->d_tf, r->d_tau, (__half*)r->d_map,
+                                r->d_cnt, r->stream, occ, r->d_vlist);
+    if (e != cudaSuccess) return cuda_fail(r, e, "light_march launch");
+    ++launches;
+    return BEAMS_OK;
+  }
   for (int l = 0; l < nl; ++l) {
     ExactGeo gl = g;
     if (l > 0) geo_set_light(gl, r->lights[l]);
@@ -676,7 +690,7 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
       Brick& B = r->bricks[b];
       const size_t nv = (size_t)G[b].pd[0] * G[b].pd[1] * G[b].pd[2];
       s = ensure_buffer(r, (void**)&B.d_map_local, &B.local_cap, nv * sizeof(float), "allocating brick map");
-      if (s == BEAMS_OK) s = ensure_masked_map(r, &B.d_map_final, &B.final_cap, nv * sizeof(float), r->stream);
+      if (s == BEAMS_OK) s = ensure_masked_map(r, &B.d_map_final, &B.final_cap, nv * sizeof(float), r->stream, false);
       if (s != BEAMS_OK) return s;
       B.map_count = nv;
       BrickRef& R = refs[b];
@@ -1434,7 +1448,7 @@ static beams_status render_frame(beams_renderer* r, const beams_camera* cam, flo
   if (s != BEAMS_OK) return s;
   const bool use_mlp = r->form == BEAMS_FORM_MLP;
   const bool need_map = r->use_map && r->vol.assoc == BEAMS_ASSOC_POINTS && !use_mlp;
-  const bool lazy = need_map && r->lazy_map && r->form == BEAMS_FORM_EXACT;
+  const bool lazy = need_map && r->lazy_map && (r->form == BEAMS_FORM_EXACT || r->form == BEAMS_FORM_PRECISION);
   if (lazy) {
     // the marking pass clips rays to the canvas depth like the view march
     s = prepare_ray_limits(r, g, launches);

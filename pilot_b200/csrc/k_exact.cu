@@ -70,15 +70,6 @@ __device__ __forceinline__ bool vertex_in_marked_cell(const unsigned char* __res
   return m != 0u;
 }
 
-// The work list of a masked map build: the vertices of marked cells
-// (vertex_in_marked_cell) in the light march's vertex order, list[1 + i] their
-// ids, list[0] their count (zeroed before the launch). A masked build over this
-// list takes one tile-counter atomic per 32 listed vertices, where testing every
-// vertex took one per 32 vertices of the whole map (the 257^3-vertex map of a
-// 512^3 field seen through a 30-degree camera: 31,073 vertices built, 0.41 ms
-// for the per-vertex test, most of it atomics on the one counter). One warp per
-// 32-vertex tile of the order at a static stride, one append per warp that
-// finds a vertex (lane order kept inside the warp).
 // Blocks of 8^3 map cells: cb[d] = ceil((pd[d] - 1) / 8) per axis.
 __host__ __device__ inline void cell_blocks(const int pd[3], int cb[3]) {
   for (int d = 0; d < 3; ++d) cb[d] = (pd[d] - 1 + 7) >> 3;
@@ -109,6 +100,14 @@ __global__ void __launch_bounds__(256) k_mark_cell_blocks(const ExactGeo g, cons
   }
 }
 
+// The work list of a masked map build: the vertices of marked cells
+// (vertex_in_marked_cell) in the light march's vertex order, list[1 + i] their
+// ids, list[0] their count (zeroed before the launch). A masked build over this
+// list takes one tile-counter atomic per 32 listed vertices, where testing every
+// vertex took one per 32 vertices of the whole map (the 257^3-vertex map of a
+// 512^3 field seen through a 30-degree camera: 31,073 vertices built, 0.41 ms
+// for the per-vertex test, most of it atomics on the one counter). One append
+// per warp that finds a vertex (lane order kept inside the warp).
 __global__ void __launch_bounds__(256) k_list_marked_vertices(const ExactGeo g, const unsigned char* __restrict__ cm,
                                                               const unsigned char* __restrict__ blocks,
                                                               const unsigned* __restrict__ gate,
@@ -314,8 +313,8 @@ __global__ void __launch_bounds__(kThreads) k_view_march(const ExactGeo g, const
 // K2's warp tiles in K2's order over the window, or (LIST) over the listed
 // kFallbackTile^2 tiles while *fcount > 0; tile counter cnt->tiles_mark. The
 // march reads no map, so only the field axes' cell tables are staged.
-template <bool RECT, bool LIST, bool SKIP = false>
-__global__ void __launch_bounds__(kThreads) k_mark_view_cells(const ExactGeo g, const float4* __restrict__ quads,
+template <typename QuadT, bool RECT, bool LIST, bool SKIP = false>
+__global__ void __launch_bounds__(kThreads) k_mark_view_cells(const ExactGeo g, const QuadT* __restrict__ quads,
                                                               const float4* __restrict__ tab,
                                                               const float4* __restrict__ tf,
                                                               unsigned char* __restrict__ mask,
@@ -350,8 +349,8 @@ __global__ void __launch_bounds__(kThreads) k_mark_view_cells(const ExactGeo g, 
                    {g.pd[0], g.pd[1], g.pd[2]}, mask, 0xffffffffu};
       float4 color;
       unsigned lit = 0, hit = 0;
-      view_march_pixel<float4, false, float, CellMarker, SKIP, false, RECT>(g, quads, s_tab, s_tf, nullptr, x, y,
-                                                                            color, lit, hit, &m, occ);
+      view_march_pixel<QuadT, false, float, CellMarker, SKIP, false, RECT>(g, quads, s_tab, s_tf, nullptr, x, y,
+                                                                           color, lit, hit, &m, occ);
     }
   }
 }
@@ -615,6 +614,21 @@ static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4*
       }
       return cudaGetLastError();
     }
+  } else if constexpr (!STITCH && PREC) {
+    if (vlist) {  // the precision form's lazy map
+      if (occ) {
+        e = persistent_grid(k_light_march<QuadT, false, true, true, false, true>, smem, ntiles, grid);
+        if (e != cudaSuccess) return e;
+        k_light_march<QuadT, false, true, true, false, true><<<grid, kThreads, smem, st>>>(
+            g, (const QuadT*)quads, tab, tf, tau, map, nvert, cnt, refs, nrefs, self, gate, occ, vlist);
+      } else {
+        e = persistent_grid(k_light_march<QuadT, false, true, false, false, true>, smem, ntiles, grid);
+        if (e != cudaSuccess) return e;
+        k_light_march<QuadT, false, true, false, false, true><<<grid, kThreads, smem, st>>>(
+            g, (const QuadT*)quads, tab, tf, tau, map, nvert, cnt, refs, nrefs, self, gate, nullptr, vlist);
+      }
+      return cudaGetLastError();
+    }
   } else if constexpr (STITCH && !PREC) {
     if (vlist) {  // the lazy map of a multi-block scene: the stitched march over a brick's list
       if (occ) return cudaErrorInvalidValue;
@@ -643,18 +657,37 @@ static cudaError_t launch_k1(const ExactGeo& g, const void* quads, const float4*
   return cudaGetLastError();
 }
 
-template <bool RECT, bool LIST, bool SKIP = false>
-static cudaError_t launch_mark(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
+template <bool RECT, bool LIST, bool SKIP = false, typename QuadT = float4>
+static cudaError_t launch_mark(const ExactGeo& g, const QuadT* quads, const float4* tab, const float4* tf,
                                unsigned char* cell_mask, Counters* cnt, const unsigned* flist,
                                const unsigned* fcount, cudaStream_t st, const unsigned char* occ = nullptr) {
   const size_t smem = ((size_t)g.max_off[0] + (size_t)g.tf_n) * sizeof(float4);
   const int ntiles = ((g.win[2] + 7) >> 3) * ((g.win[3] + 3) >> 2);
   int grid = 0;
-  cudaError_t e = persistent_grid(k_mark_view_cells<RECT, LIST, SKIP>, smem, ntiles, grid);
+  cudaError_t e = persistent_grid(k_mark_view_cells<QuadT, RECT, LIST, SKIP>, smem, ntiles, grid);
   if (e != cudaSuccess) return e;
-  k_mark_view_cells<RECT, LIST, SKIP><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, cell_mask, cnt, flist, fcount,
-                                                                     occ);
+  k_mark_view_cells<QuadT, RECT, LIST, SKIP><<<grid, kThreads, smem, st>>>(g, quads, tab, tf, cell_mask, cnt, flist,
+                                                                            fcount, occ);
   return cudaGetLastError();
+}
+
+// The precision form's view march reads the 16-bit quads and never takes the
+// rectilinear instantiation (its seeded walk serves both), so its marking
+// pass does the same.
+cudaError_t launch_mark_view_cells_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,
+                                        const float4* tf, unsigned char* cell_mask, Counters* cnt, cudaStream_t st,
+                                        const unsigned char* occ) {
+  cudaError_t e = cudaMemsetAsync(&cnt->tiles_mark, 0, sizeof(unsigned), st);
+  if (e != cudaSuccess) return e;
+  if (quad_dtype == 1)
+    return occ ? launch_mark<false, false, true>(g, (const QuadBF16*)quads, tab, tf, cell_mask, cnt, nullptr, nullptr,
+                                                 st, occ)
+               : launch_mark<false, false, false>(g, (const QuadBF16*)quads, tab, tf, cell_mask, cnt, nullptr,
+                                                  nullptr, st);
+  return occ ? launch_mark<false, false, true>(g, (const QuadF16*)quads, tab, tf, cell_mask, cnt, nullptr, nullptr, st,
+                                               occ)
+             : launch_mark<false, false, false>(g, (const QuadF16*)quads, tab, tf, cell_mask, cnt, nullptr, nullptr,
+                                                st);
 }
 
 cudaError_t launch_mark_view_cells(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
@@ -701,10 +734,10 @@ cudaError_t launch_light_march_f32(const ExactGeo& g, const float4* quads, const
 
 cudaError_t launch_light_march_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,
                                     const float4* tf, const float* tau, __half* map, Counters* cnt, cudaStream_t st,
-                                    const unsigned char* occ) {
+                                    const unsigned char* occ, const unsigned* vlist) {
   if (quad_dtype == 1)
-    return launch_k1<QuadBF16, false, true>(g, quads, tab, tf, tau, map, cnt, st, nullptr, 0, -1, nullptr, occ);
-  return launch_k1<QuadF16, false, true>(g, quads, tab, tf, tau, map, cnt, st, nullptr, 0, -1, nullptr, occ);
+    return launch_k1<QuadBF16, false, true>(g, quads, tab, tf, tau, map, cnt, st, nullptr, 0, -1, nullptr, occ, vlist);
+  return launch_k1<QuadF16, false, true>(g, quads, tab, tf, tau, map, cnt, st, nullptr, 0, -1, nullptr, occ, vlist);
 }
 
 // Occupancy of the 8^3-cell macro-cells: 0 when every value the trilinear

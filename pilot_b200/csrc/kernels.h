@@ -13,7 +13,7 @@ cudaError_t launch_build_quads(const void* field, int in_dtype, void* quads, int
                                cudaStream_t st);
 cudaError_t launch_light_march_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,
                                     const float4* tf, const float* tau, __half* map, Counters* cnt, cudaStream_t st,
-                                    const unsigned char* occ = nullptr);
+                                    const unsigned char* occ = nullptr, const unsigned* vlist = nullptr);
 cudaError_t launch_view_march_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,
                                    const float4* tf, const __half* map, float4* out, Counters* cnt, cudaStream_t st,
                                    const unsigned char* occ = nullptr);
@@ -49,6 +49,11 @@ cudaError_t launch_mark_fallback_vertices(const ExactGeo& g, const float4* quads
 cudaError_t launch_mark_view_cells(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                    unsigned char* cell_mask, Counters* cnt, const unsigned* flist,
                                    const unsigned* fcount, cudaStream_t st, const unsigned char* occ = nullptr);
+// The same over the precision form's 16-bit quads (quad_dtype 1: bfloat16,
+// else binary16), window only.
+cudaError_t launch_mark_view_cells_prec(const ExactGeo& g, int quad_dtype, const void* quads, const float4* tab,
+                                        const float4* tf, unsigned char* cell_mask, Counters* cnt, cudaStream_t st,
+                                        const unsigned char* occ = nullptr);
 // K2 over a device list of kFallbackTile^2 pixel tiles (count in *fcount), with the map.
 cudaError_t launch_view_march_tiles(const ExactGeo& g, const float4* quads, const float4* tab, const float4* tf,
                                     const float* map, float4* out, Counters* cnt, const unsigned* flist,

@@ -244,7 +244,7 @@ static beams_status mlp_fallback(beams_renderer* r, const ExactGeo& g, const Pro
   const ProbeLayout& L = pb.L;
   cudaError_t e;
   const size_t nvert = (size_t)g.pd[0] * g.pd[1] * g.pd[2];
-  beams_status s = ensure_masked_map(r, &r->d_map, &r->map_cap, nvert * sizeof(float), r->stream);
+  beams_status s = ensure_masked_map(r, &r->d_map, &r->map_cap, nvert * sizeof(float), r->stream, r->map_is_half);
   if (s != BEAMS_OK) return s;
   r->map_valid = false;  // a partial map, built (or not) on the device's decision
   r->map_is_half = false;

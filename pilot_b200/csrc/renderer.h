@@ -253,8 +253,10 @@ beams_status cuda_fail(beams_renderer* r, cudaError_t e, const char* what);
 beams_status ensure_buffer(beams_renderer* r, void** buf, size_t* cap, size_t bytes, const char* what);
 // The map of a masked build: the vertices it does not build are still read by
 // samples of premultiplied alpha 0 (which add 0 times their shading, exactly 0
-// for any finite value), so a newly allocated buffer is zeroed on st.
-beams_status ensure_masked_map(beams_renderer* r, float** buf, size_t* cap, size_t bytes, cudaStream_t st);
+// for any finite value), so a newly allocated buffer is zeroed on st, and so
+// is a reused one when clear is set (its data came in another format).
+beams_status ensure_masked_map(beams_renderer* r, float** buf, size_t* cap, size_t bytes, cudaStream_t st,
+                               bool clear);
 beams_status prepare_ray_limits(beams_renderer* r, ExactGeo& g, int& launches);
 beams_status blend_background(beams_renderer* r, float4* img, size_t npix, int& launches);
 }  // namespace beams

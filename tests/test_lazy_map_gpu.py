@@ -196,16 +196,41 @@ def test_lazy_map_with_depth_limits(cuda_device):
     assert tl["map_vertices"] < t_nolim["map_vertices"]  # clipped rays read fewer cells
 
 
-def test_lazy_map_ignored_by_the_precision_form(cuda_device):
-    s = scenes.small(7, n=32, image=64, m=16)
+@pytest.mark.parametrize("dt,skip", [(B.BF16, False), (B.F16, True)])
+def test_lazy_map_in_the_precision_form(cuda_device, dt, skip):
+    """The precision form marks over its 16-bit field and builds its binary16
+    map over the list: the same image as its full map, after a frame that left
+    another light's map in the buffer, and straight after an exact-form frame
+    (the buffer then held a float32 map, whose bits read as binary16 can be
+    NaN: the masked build clears it)."""
+    s = scenes.small(7, n=48, image=80, m=24, kind="noise", light_kind=0)
+    s.fov_y_deg = 12.0
     r = renderer(s)
-    r.set_form(B.FORM_PRECISION, field_dtype=B.BF16)
-    a, ta = r.render(s.camera())
+    r.set_tuning(light_brick=8, empty_skip=skip, view_skip=skip)
+    r.render(s.camera())  # exact form: a float32 map in the buffer
+    r.set_form(B.FORM_PRECISION, field_dtype=dt)
+    full, tf = r.render(s.camera())
+    poison(r, s.camera())
+    s.configure(r)
     r.set_lazy_shadow_map(True)
-    b, tb = r.render(s.camera())
-    assert np.array_equal(a, b)
-    assert tb["map_vertices"] == ta["map_vertices"] == (s.map_m + 1) ** 3
+    lazy, tl = r.render(s.camera())
+    assert np.array_equal(lazy, full), f"differs by {np.max(np.abs(lazy - full))}"
+    assert tl["lit_samples"] == tf["lit_samples"]
+    assert 0 < tl["map_vertices"] < tf["map_vertices"] == (s.map_m + 1) ** 3
+    with pytest.raises(B.BeamsError):
+        r.get_shadow_map((s.map_m + 1) ** 3)
+    r.set_lazy_shadow_map(False)
+    again, _ = r.render(s.camera())
+    assert np.array_equal(again, full)
     assert r.get_shadow_map((s.map_m + 1) ** 3).size == (s.map_m + 1) ** 3
+    # straight from an exact-form frame (a float32 map) to a lazy precision frame
+    q = renderer(s)
+    q.set_tuning(light_brick=8, empty_skip=skip, view_skip=skip)
+    q.render(s.camera())
+    q.set_form(B.FORM_PRECISION, field_dtype=dt)
+    q.set_lazy_shadow_map(True)
+    direct, _ = q.render(s.camera())
+    assert np.array_equal(direct, full), f"differs by {np.max(np.abs(direct - full))}"
 
 
 def test_kept_marks_follow_every_view_input(cuda_device):

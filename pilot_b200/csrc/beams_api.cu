@@ -472,6 +472,8 @@ static void mark_key(const beams_renderer* r, const ExactGeo& g, MarkKey& k) {
   k.size[1] = g.height;
   for (int i = 0; i < 4; ++i) k.win[i] = g.win[i];
   k.slab_fp64 = g.slab_fp64;
+  k.form = r->form;
+  k.quad_dtype = quad_dtype(r);
 }
 
 static beams_status build_map_lazy(beams_renderer* r, const ExactGeo& g, int& launches) {

@@ -70,11 +70,12 @@ struct Brick {
 
 // What the lazy map's cell marks depend on: the view rays and their samples
 // (volume, colour map, canvas depth, camera, window, sample distance,
-// termination, slab mode, value range) and the map grid; not the light.
+// termination, slab mode, value range, and the form with its field's type,
+// whose rounding moves the samples' values) and the map grid; not the light.
 struct MarkKey {
   unsigned long long volume_version, tf_version, depth_version;
   float cam[12], k[4], sd, mesh_eps, cutoff, min_scalar, inv_delta, morig[3], minv[3];
-  int size[2], win[4], slab_fp64, pd[3];
+  int size[2], win[4], slab_fp64, pd[3], form, quad_dtype;
 };
 
 struct MapKey {

@@ -295,6 +295,14 @@ def test_kept_marks_follow_every_view_input(cuda_device):
         x.set_volume(f2, origin=s.origin, spacing=s.spacing, value_range=s.value_range)
     t = both(cam)
     assert t["kernel_launches"] > t0["kernel_launches"] - 1
+    # the form and its field's type move the samples: the precision form marks
+    # again, and again after its dtype changes
+    for dt in (B.BF16, B.F16):
+        for x in (r, q):
+            x.set_form(B.FORM_PRECISION, field_dtype=dt)
+        both(cam)  # a new quad copy and marks
+        t = both(cam)
+        assert t["kernel_launches"] == t0["kernel_launches"] - 1  # marks kept within the form
     with pytest.raises(B.BeamsError):
         r._check(r._L.beams_set_lazy_shadow_map(r._h, 3))
 

@@ -1146,6 +1146,7 @@ def run_bricks(args, nested=False):
 #   batch            16-request persistent batch (--split: map-build launch, then view launch)
 #   precision_light  precision-form K1, bf16 640^3
 #   precision_view   precision-form K2, bf16 640^3, 1024^2, map cached
+#   precision_lazy   precision-form frame with the lazy map, bf16 640^3, 1024^2
 #   bricks           512^3 noise as 2x2x2 bricks: K1, K5, K2, K6
 #   bricks_lazy      the same with the lazy map (marks and lists before K5)
 # Each case sets up its scene, runs the target kernel --reps times and exits 0;
@@ -1153,7 +1154,7 @@ def run_bricks(args, nested=False):
 # skipping as stated per case) so that the launch sequence is the same every run.
 # ---------------------------------------------------------------------------
 PROFILE_CASES = ["light_march", "view_march", "lazy_frame", "mlp_view", "mlp_frame", "mlp_frame32", "mlp_tc", "mlp_train", "batch",
-                 "precision_light", "precision_view", "bricks", "bricks_lazy"]
+                 "precision_light", "precision_view", "precision_lazy", "bricks", "bricks_lazy"]
 
 
 def run_profile_case(a):
@@ -1226,7 +1227,7 @@ def run_profile_case(a):
         T = torch.empty(n, device="cuda")
         for _ in range(a.reps):
             r.mlp_forward_tc_device(X, T)
-    elif a.profile_case in ("precision_light", "precision_view"):
+    elif a.profile_case in ("precision_light", "precision_view", "precision_lazy"):
         s = scenes.config2(n=640, image=1024, m=320)
         fd = s.field_device()
         r = B.Renderer(0)
@@ -1237,6 +1238,11 @@ def run_profile_case(a):
         if a.profile_case == "precision_light":
             for _ in range(a.reps):
                 r.build_shadow_map(timings=False)
+        elif a.profile_case == "precision_lazy":
+            r.set_lazy_shadow_map(True)
+            out = torch.empty((s.height, s.width, 4), device="cuda")
+            for _ in range(a.reps):
+                r.render(s.camera(), out=out, timings=False)
         else:
             r.build_shadow_map(timings=False)
             r.set_reuse_shadow_map(True)

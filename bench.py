@@ -1110,6 +1110,25 @@ def run_bricks(args, nested=False):
     _, tz = r.render(cam, out=out, timings=True)
     lazy_same = bool(np.array_equal(out.cpu().numpy(), img))
     lazy_ms, _ = time_frames(frame, args.steps, args.warmup, stream, 1, local)
+    # a light orbit around the fixed camera: 12 point-light positions 30 degrees
+    # apart, full maps, lazy maps, and lazy maps with each brick's marks kept
+    lpos0 = np.asarray(s.light, np.float64) - 0.5
+    step = [0]
+
+    def orbit_frame():
+        a = 2.0 * np.pi * (step[0] % 12) / 12.0
+        step[0] += 1
+        c, sn = np.cos(a), np.sin(a)
+        lp = (0.5 + c * lpos0[0] + sn * lpos0[2], 0.5 + lpos0[1], 0.5 - sn * lpos0[0] + c * lpos0[2])
+        r.clear_lights()
+        r.add_point_light(tuple(float(v) for v in lp), s.light_color, s.light_intensity)
+        r.render(cam, out=out, timings=False)
+
+    orbit = {"frames": "12 light positions around the vertical axis, 30 degrees apart, camera fixed"}
+    for mode, name in ((0, "full_maps"), (1, "lazy"), (2, "lazy_kept_marks")):
+        r.set_lazy_shadow_map(mode != 0, keep_marks=mode == 2)
+        oms, _ = time_frames(orbit_frame, 12, 3, stream, 1, local)
+        orbit[name + "_ms_per_frame"] = oms / 12
     r.set_lazy_shadow_map(False)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -1124,7 +1143,7 @@ def run_bricks(args, nested=False):
             "undivided_ms_per_frame": whole_ms, "psnr_vs_undivided": psnr(img, whole), "clocks": clocks,
             "lazy_map": {"ms_per_frame": lazy_ms / args.steps, "undivided_ms_per_frame": whole_lazy_ms,
                          "map_vertices_built": tz["map_vertices"], "stitched_map_vertices": tb["map_vertices"],
-                         "image_equals_full_maps": lazy_same,
+                         "image_equals_full_maps": lazy_same, "light_orbit": orbit,
                          "phases_ms": {"maps_and_stitch": tz["map_build_ms"], "view_marches": tz["view_march_ms"]}}}
     r.close()
     if nested:

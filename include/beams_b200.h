@@ -175,8 +175,8 @@ beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable);
  * kept while everything they depend on is unchanged: volume, colour map,
  * canvas depth, camera, sample distance, termination alpha, slab mode and map
  * size (not the light: a light orbit around a fixed camera marks once). Other
- * values return BEAMS_ERR_INVALID_ARG. Mode 2 applies to single volumes; a
- * multi-block scene marks every frame. */
+ * values return BEAMS_ERR_INVALID_ARG. In a multi-block scene each brick
+ * keeps its own marks the same way. */
 beams_status beams_set_lazy_shadow_map(beams_renderer* r, int mode);
 /* ---- legacy VTK files ---------------------------------------------------------
  * Replaces the reference's dataset read (pilot/io/DataSetUtils.cxx:13-42, VTK-m's

@@ -522,7 +522,7 @@ static beams_status build_map_lazy(beams_renderer* r, const ExactGeo& g, int& la
   }
   e = launch_list_marked_vertices(g, r->d_cell_mask, nullptr, r->d_vlist, r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "map vertex listing launch");
-  ++launches;
+  launches += 2;  // the block pass and the list
   if (prec) {
     e = launch_light_march_prec(g, quad_dtype(r), r->d_quads, r->d_tab, r->d_tf, r->d_tau, (__half*)r->d_map,
                                 r->d_cnt, r->stream, occ, r->d_vlist);
@@ -739,7 +739,7 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
       if (s != BEAMS_OK) return s;
       e = launch_list_marked_vertices(G[0], shell, nullptr, r->d_vlist, r->stream);
       if (e != cudaSuccess) return cuda_fail(r, e, "listing the shell vertices");
-      ++launches;
+      launches += 2;  // the block pass and the list
       shell_list = r->d_vlist;
     }
     s = brick_lanes_fork(r);
@@ -781,14 +781,25 @@ beams_status render_bricks(beams_renderer* r, const beams_camera* cam, float4* o
       const unsigned* list = nullptr;
       if (lazy) {
         if (!reached[b]) continue;
-        const size_t ncell = (size_t)(G[b].pd[0] - 1) * (G[b].pd[1] - 1) * (G[b].pd[2] - 1);
-        e = cudaMemsetAsync(B.d_cell_mask, 0, ncell, lane(b));
-        if (e == cudaSuccess)
-          e = launch_mark_view_cells(G[b], B.d_quads, B.d_tab, r->d_tf, B.d_cell_mask, r->d_brick_cnt + b, nullptr,
-                                     nullptr, lane(b));
-        if (e == cudaSuccess) e = launch_list_marked_vertices(G[b], B.d_cell_mask, nullptr, B.d_vlist, lane(b));
-        if (e != cudaSuccess) return lane_fail(e, "brick map cell marking");
-        launches += 3;
+        // mode 2 keeps a brick's marks while its view's inputs are unchanged
+        MarkKey key;
+        mark_key(r, G[b], key);
+        key.volume_version = B.version;
+        if (!(r->keep_marks && B.marks_valid && std::memcmp(&key, &B.mark_key, sizeof(key)) == 0)) {
+          B.marks_valid = false;
+          const size_t ncell = (size_t)(G[b].pd[0] - 1) * (G[b].pd[1] - 1) * (G[b].pd[2] - 1);
+          e = cudaMemsetAsync(B.d_cell_mask, 0, ncell, lane(b));
+          if (e == cudaSuccess)
+            e = launch_mark_view_cells(G[b], B.d_quads, B.d_tab, r->d_tf, B.d_cell_mask, r->d_brick_cnt + b,
+                                       nullptr, nullptr, lane(b));
+          if (e != cudaSuccess) return lane_fail(e, "brick map cell marking");
+          ++launches;
+          B.mark_key = key;
+          B.marks_valid = r->keep_marks;
+        }
+        e = launch_list_marked_vertices(G[b], B.d_cell_mask, nullptr, B.d_vlist, lane(b));
+        if (e != cudaSuccess) return lane_fail(e, "brick map vertex listing");
+        launches += 2;  // the block pass and the list
         list = B.d_vlist;
       }
       e = launch_light_march_f32(G[b], B.d_quads, B.d_tab, r->d_tf, B.d_map_final, r->d_brick_cnt + b, lane(b),

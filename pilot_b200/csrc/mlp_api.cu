@@ -273,7 +273,7 @@ static beams_status mlp_fallback(beams_renderer* r, const ExactGeo& g, const Pro
     e = launch_view_march_tiles(g, (const float4*)r->d_quads, r->d_tab, r->d_tf, r->d_map, out, r->d_cnt + 1,
                                 pb.flist, pb.fcount, r->stream);
   if (e != cudaSuccess) return cuda_fail(r, e, "mlp fallback launch");
-  launches += 5;
+  launches += 6;  // mask clear, marks, block pass, list, light march, view march
   return BEAMS_OK;
 }
 

@@ -26,6 +26,16 @@ struct Light {
 
 // One block of a multi-block scene: its own field and derived buffers (the
 // reference holds one block per MPI rank; here all blocks share one GPU).
+// What the lazy map's cell marks depend on: the view rays and their samples
+// (volume, colour map, canvas depth, camera, window, sample distance,
+// termination, slab mode, value range, and the form with its field's type,
+// whose rounding moves the samples' values) and the map grid; not the light.
+struct MarkKey {
+  unsigned long long volume_version, tf_version, depth_version;
+  float cam[12], k[4], sd, mesh_eps, cutoff, min_scalar, inv_delta, morig[3], minv[3];
+  int size[2], win[4], slab_fp64, pd[3], form, quad_dtype;
+};
+
 struct Brick {
   beams_volume vol{};
   void* d_field_owned = nullptr;
@@ -50,6 +60,8 @@ struct Brick {
   unsigned* d_vlist = nullptr;
   size_t vlist_cap = 0;
   bool final_partial = false;
+  bool marks_valid = false;  // mode 2: this brick's marks kept while mark_key matches
+  MarkKey mark_key{};
   void release() {
     if (d_field_owned) cudaFree(d_field_owned);
     if (d_quads) cudaFree(d_quads);
@@ -66,16 +78,6 @@ struct Brick {
     d_tab = nullptr;
     d_map_local = d_map_final = nullptr;
   }
-};
-
-// What the lazy map's cell marks depend on: the view rays and their samples
-// (volume, colour map, canvas depth, camera, window, sample distance,
-// termination, slab mode, value range, and the form with its field's type,
-// whose rounding moves the samples' values) and the map grid; not the light.
-struct MarkKey {
-  unsigned long long volume_version, tf_version, depth_version;
-  float cam[12], k[4], sd, mesh_eps, cutoff, min_scalar, inv_delta, morig[3], minv[3];
-  int size[2], win[4], slab_fp64, pd[3], form, quad_dtype;
 };
 
 struct MapKey {

@@ -119,3 +119,30 @@ def test_lazy_map_bricks_give_the_full_maps_image(cuda_device, splits, fov):
     assert np.array_equal(again, img)
     assert r.get_brick_map(0, 1, nv).size == nv
     print(f"{splits} fov {fov}: {tl['map_vertices']} vertices built, full stitched maps {t['map_vertices']}")
+
+
+def test_kept_brick_marks_over_a_light_orbit(cuda_device):
+    """Mode 2 in a multi-block scene: each brick keeps its marks while the view
+    is unchanged, so a moving light re-marks no brick (one launch fewer per
+    brick the view reaches) and every frame equals the full stitched maps'."""
+    s = scenes.small(36, n=41, image=72, m=12, kind="noise", light_kind=1)
+    bricks = scenes.split_bricks(s, (2, 2, 2))
+    cam = bricks[0].camera()
+    r, _, _ = gpu_bricks(bricks)
+    q, _, _ = gpu_bricks(bricks)
+    r.set_lazy_shadow_map(True, keep_marks=True)
+    counts = []
+    for d in [(0.2, 0.9, 0.3), (-0.7, 0.1, 0.7), (0.5, -0.5, -0.7), (0.1, 0.2, -0.97)]:
+        for x in (r, q):
+            x.clear_lights()
+            x.add_directional_light(d, (1.0, 0.9, 0.8), 1.2)
+        a, ta = r.render(cam)
+        b, tb = q.render(cam)
+        assert np.array_equal(a, b), f"light {d}: differs by {np.max(np.abs(a - b))}"
+        assert ta["lit_samples"] == tb["lit_samples"]
+        counts.append(ta["kernel_launches"])
+    assert counts[1] < counts[0] and counts[1] == counts[2] == counts[3]  # marked once
+    cam2 = scenes.split_bricks(scenes.small(37, n=41, image=72, m=12, kind="noise"), (2, 2, 2))[0].camera()
+    a, ta = r.render(cam2)  # a new view marks again
+    b, _ = q.render(cam2)
+    assert np.array_equal(a, b)

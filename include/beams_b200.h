@@ -161,8 +161,9 @@ beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable);
  * TransmittanceMap.h:565-621): the exact form builds only the map vertices that
  * the frame's view rays read. A view march without shading (the samples and
  * their order do not depend on the map: early termination reads only the
- * colour map's alpha) marks the map cells the shading will interpolate, then
- * the light march builds the corners of the marked cells. The image is the
+ * colour map's alpha) marks the map cells the shading will interpolate at
+ * samples of alpha above 0 (the others add 0 times their shading), then the
+ * light march builds the corners of the marked cells. The image is the
  * full map's bit for bit; the map is partial, so beams_get_shadow_map returns
  * BEAMS_ERR_STATE after such a frame and the map is never reused.
  * beams_timings.map_vertices reports the vertices built. In a multi-block
@@ -173,8 +174,9 @@ beams_status beams_set_reuse_shadow_map(beams_renderer* r, int enable);
  * default; the learned form ignores it (its fallback is lazy already).
  * mode: 0 off, 1 on (the cells are marked every frame), 2 on and the marks are
  * kept while everything they depend on is unchanged: volume, colour map,
- * canvas depth, camera, sample distance, termination alpha, slab mode and map
- * size (not the light: a light orbit around a fixed camera marks once). Other
+ * canvas depth, camera, sample distance, termination alpha, slab mode, form and
+ * field type, and map size (not the light: a light orbit around a fixed camera
+ * marks once). Other
  * values return BEAMS_ERR_INVALID_ARG. In a multi-block scene each brick
  * keeps its own marks the same way. */
 beams_status beams_set_lazy_shadow_map(beams_renderer* r, int mode);
